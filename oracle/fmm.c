@@ -1,0 +1,426 @@
+/*
+ * Oracle (test infrastructure only): the reference's host FMM on one rank, restated:
+ *   - build: fmm-exec/src/fmm.rs:17-93 steps 3-8 (domain, keys of sources ++ targets,
+ *     octree, points in leaf order = caller order within a leaf, leaf-scaled
+ *     coordinates per fmm-exec/src/geometry.rs:291-298);
+ *   - lists: fmm-plan/src/interaction_manager.rs:15-27, found by neighbour lookups
+ *     (the brute-force search of tree.c checks them in the tests);
+ *   - evaluation order: fmm-plan/src/evaluator.rs:368-527 (upward L..0: p2m then m2m;
+ *     downward 1..L: l2l, m2l by offset index, p2l by source leaf; leaves 0..L: l2p,
+ *     m2p by box index, p2p by source leaf), accumulation rule operator.rs:34-45;
+ *   - operators: fmm-ref leaf/direct/p2p restated in operators.c, M2M/L2L/M2L by
+ *     tables applied as fmm-tables/src/matrix_set.rs:128;
+ *   - frames: CONVENTIONS 3.13 "Relative frames" (integer centres, exact dyadics);
+ *   - output: fmm-exec/src/fmm.rs:4750-4778 (phi / (4 pi r), g / ((4 pi r) r)).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "fmm_oracle.h"
+
+#define DEEPEST 16
+
+static int cmp_u64(const void *a, const void *b) {
+    uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+typedef struct {
+    int nlevels;
+    size_t nboxes;
+    uint64_t *key;      /* level-major key order */
+    int *level;
+    uint32_t (*idx)[3];
+    uint8_t *leaf;
+    size_t *level_start; /* nlevels + 1 */
+    uint64_t *sorted;    /* keys sorted by value, with their box index */
+    size_t *sorted_box;
+} boxes_t;
+
+static long find(const boxes_t *b, uint64_t k) {
+    uint64_t *p = (uint64_t *)bsearch(&k, b->sorted, b->nboxes, sizeof(uint64_t), cmp_u64);
+    return p ? (long)b->sorted_box[p - b->sorted] : -1;
+}
+
+static int is_anc(uint64_t a, uint64_t b) {
+    int la = (int)(a & 0x7FFF), lb = (int)(b & 0x7FFF);
+    if (la >= lb) return 0;
+    uint64_t mask = ~0ULL << (15 + 3 * (DEEPEST - la));
+    return ((a ^ b) & mask) == 0;
+}
+
+static int adjacent_boxes(const boxes_t *B, size_t a, size_t b) {
+    if (a == b || is_anc(B->key[a], B->key[b]) || is_anc(B->key[b], B->key[a])) return 0;
+    int la = B->level[a], lb = B->level[b], L = la > lb ? la : lb;
+    for (int k = 0; k < 3; ++k) {
+        long a0 = (long)B->idx[a][k] << (L - la), a1 = (long)(B->idx[a][k] + 1) << (L - la);
+        long b0 = (long)B->idx[b][k] << (L - lb), b1 = (long)(B->idx[b][k] + 1) << (L - lb);
+        if ((a0 > b0 ? a0 : b0) > (a1 < b1 ? a1 : b1)) return 0;
+    }
+    return 1;
+}
+
+static long neighbour(const boxes_t *B, size_t b, int dx, int dy, int dz) {
+    int l = B->level[b];
+    long size = 1L << l;
+    long n[3] = {(long)B->idx[b][0] + dx, (long)B->idx[b][1] + dy, (long)B->idx[b][2] + dz};
+    for (int k = 0; k < 3; ++k)
+        if (n[k] < 0 || n[k] >= size) return -2; /* outside the domain */
+    uint32_t ni[3] = {(uint32_t)n[0], (uint32_t)n[1], (uint32_t)n[2]};
+    return find(B, orc_key_from_index(ni, l));
+}
+
+static long parent_box(const boxes_t *B, size_t b) {
+    if (B->level[b] == 0) return -1;
+    uint32_t pi[3] = {B->idx[b][0] >> 1, B->idx[b][1] >> 1, B->idx[b][2] >> 1};
+    return find(B, orc_key_from_index(pi, B->level[b] - 1));
+}
+
+static long child_box(const boxes_t *B, size_t b, int o) {
+    uint32_t ci[3] = {2 * B->idx[b][0] + ((o >> 2) & 1), 2 * B->idx[b][1] + ((o >> 1) & 1),
+                      2 * B->idx[b][2] + (o & 1)};
+    return find(B, orc_key_from_index(ci, B->level[b] + 1));
+}
+
+typedef struct { size_t *data; size_t len, cap; } vecz;
+static void zpush(vecz *v, size_t x) {
+    if (v->len == v->cap) {
+        v->cap = v->cap ? 2 * v->cap : 32;
+        v->data = (size_t *)realloc(v->data, v->cap * sizeof(size_t));
+    }
+    v->data[v->len++] = x;
+}
+static int cmp_z(const void *a, const void *b) {
+    size_t x = *(const size_t *)a, y = *(const size_t *)b;
+    return x < y ? -1 : x > y;
+}
+static void sort_unique(vecz *v) {
+    qsort(v->data, v->len, sizeof(size_t), cmp_z);
+    size_t n = 0;
+    for (size_t i = 0; i < v->len; ++i)
+        if (n == 0 || v->data[n - 1] != v->data[i]) v->data[n++] = v->data[i];
+    v->len = n;
+}
+
+/* relative frame of box s seen from box t (CONVENTIONS 3.13 "Relative frames") */
+static void rel_frame(const boxes_t *B, size_t s, size_t t, double c[3], double *r) {
+    int ls = B->level[s], lt = B->level[t], L = ls > lt ? ls : lt;
+    for (int k = 0; k < 3; ++k) {
+        long Cs = (2L * B->idx[s][k] + 1) << (L - ls);
+        long Ct = (2L * B->idx[t][k] + 1) << (L - lt);
+        c[k] = ldexp((double)(Cs - Ct), lt - L);
+    }
+    *r = ldexp(1.0, lt - ls);
+}
+
+static int offset_of(const boxes_t *B, size_t t, size_t s) {
+    return orc_offset_index((int64_t)B->idx[t][0] - (int64_t)B->idx[s][0],
+                            (int64_t)B->idx[t][1] - (int64_t)B->idx[s][1],
+                            (int64_t)B->idx[t][2] - (int64_t)B->idx[s][2]);
+}
+
+static int cmp_pair(const void *a, const void *b) {
+    const size_t *x = (const size_t *)a, *y = (const size_t *)b;
+    return x[0] < y[0] ? -1 : x[0] > y[0] ? 1 : (x[1] < y[1] ? -1 : x[1] > y[1]);
+}
+
+int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+            int p, int max_keys, int gradients, int threads, double *phi_out, double *grad_out) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+    int nc = (p + 1) * (p + 1);
+    orc_tree *tree = orc_tree_build(ns, src, nt, tgt, DEEPEST, max_keys);
+    boxes_t B;
+    memset(&B, 0, sizeof(B));
+    B.nlevels = orc_tree_nlevels(tree);
+    B.nboxes = orc_tree_nboxes(tree);
+    B.key = (uint64_t *)malloc(B.nboxes * sizeof(uint64_t));
+    B.leaf = (uint8_t *)malloc(B.nboxes);
+    orc_tree_boxes(tree, B.key, B.leaf);
+    double lower[3], side;
+    orc_tree_domain(tree, lower, &side);
+    double box6[6];
+    { double lw[3], sd; orc_domain(ns, src, nt, tgt, lw, &sd, box6); }
+    orc_tree_free(tree);
+    B.level = (int *)malloc(B.nboxes * sizeof(int));
+    B.idx = malloc(B.nboxes * sizeof(*B.idx));
+    B.level_start = (size_t *)calloc(B.nlevels + 1, sizeof(size_t));
+    for (size_t b = 0; b < B.nboxes; ++b) {
+        orc_key_decode(B.key[b], &B.level[b], B.idx[b]);
+        B.level_start[B.level[b] + 1] = b + 1;
+    }
+    for (int l = 1; l <= B.nlevels; ++l)
+        if (B.level_start[l] < B.level_start[l - 1]) B.level_start[l] = B.level_start[l - 1];
+    B.sorted = (uint64_t *)malloc(B.nboxes * sizeof(uint64_t));
+    B.sorted_box = (size_t *)malloc(B.nboxes * sizeof(size_t));
+    {
+        size_t *pr = (size_t *)malloc(2 * B.nboxes * sizeof(size_t));
+        for (size_t b = 0; b < B.nboxes; ++b) { pr[2 * b] = (size_t)B.key[b]; pr[2 * b + 1] = b; }
+        qsort(pr, B.nboxes, 2 * sizeof(size_t), cmp_pair);
+        for (size_t i = 0; i < B.nboxes; ++i) { B.sorted[i] = pr[2 * i]; B.sorted_box[i] = pr[2 * i + 1]; }
+        free(pr);
+    }
+    /* leaves in level-major order (the leaf numbering); box -> leaf */
+    size_t nleaves = 0;
+    long *leaf_of_box = (long *)malloc(B.nboxes * sizeof(long));
+    for (size_t b = 0; b < B.nboxes; ++b) leaf_of_box[b] = B.leaf[b] ? (long)nleaves++ : -1;
+    size_t *leaf_box = (size_t *)malloc(nleaves * sizeof(size_t));
+    for (size_t b = 0; b < B.nboxes; ++b)
+        if (B.leaf[b]) leaf_box[leaf_of_box[b]] = b;
+
+    /* points -> leaves, caller order within each leaf */
+    size_t *s_leaf = (size_t *)malloc((ns + 1) * sizeof(size_t));
+    size_t *t_leaf = (size_t *)malloc((nt + 1) * sizeof(size_t));
+    for (int s = 0; s < 2; ++s) {
+        size_t n = s ? nt : ns;
+        const double *x = s ? tgt : src;
+        size_t *out = s ? t_leaf : s_leaf;
+        for (size_t i = 0; i < n; ++i) {
+            uint64_t fine = orc_point_key(x + 3 * i, box6, DEEPEST);
+            long found = -1;
+            for (int l = B.nlevels - 1; l >= 0 && found < 0; --l) {
+                int fl;
+                uint32_t fi[3];
+                orc_key_decode(fine, &fl, fi);
+                uint32_t ai[3] = {fi[0] >> (DEEPEST - l), fi[1] >> (DEEPEST - l), fi[2] >> (DEEPEST - l)};
+                long b = find(&B, orc_key_from_index(ai, l));
+                if (b >= 0 && B.leaf[b]) found = leaf_of_box[b];
+            }
+            out[i] = (size_t)found;
+        }
+    }
+    size_t *s_off = (size_t *)calloc(nleaves + 1, sizeof(size_t));
+    size_t *t_off = (size_t *)calloc(nleaves + 1, sizeof(size_t));
+    for (size_t i = 0; i < ns; ++i) s_off[s_leaf[i] + 1]++;
+    for (size_t i = 0; i < nt; ++i) t_off[t_leaf[i] + 1]++;
+    for (size_t j = 0; j < nleaves; ++j) { s_off[j + 1] += s_off[j]; t_off[j + 1] += t_off[j]; }
+    size_t *s_perm = (size_t *)malloc((ns + 1) * sizeof(size_t)); /* leaf-order pos -> caller */
+    size_t *t_perm = (size_t *)malloc((nt + 1) * sizeof(size_t));
+    {
+        size_t *fill = (size_t *)calloc(nleaves + 1, sizeof(size_t));
+        for (size_t i = 0; i < ns; ++i) s_perm[s_off[s_leaf[i]] + fill[s_leaf[i]]++] = i;
+        memset(fill, 0, (nleaves + 1) * sizeof(size_t));
+        for (size_t i = 0; i < nt; ++i) t_perm[t_off[t_leaf[i]] + fill[t_leaf[i]]++] = i;
+        free(fill);
+    }
+    /* leaf-scaled coordinates and charges in leaf order */
+    double *us = (double *)malloc((3 * ns + 1) * sizeof(double));
+    double *qs = (double *)malloc((ns * m + 1) * sizeof(double));
+    double *ut = (double *)malloc((3 * nt + 1) * sizeof(double));
+    for (size_t j = 0; j < nleaves; ++j) {
+        size_t b = leaf_box[j];
+        for (size_t a = s_off[j]; a < s_off[j + 1]; ++a) {
+            size_t i = s_perm[a];
+            for (int k = 0; k < 3; ++k)
+                us[3 * a + k] = orc_leaf_coordinate(src[3 * i + k], lower[k], side, B.level[b], B.idx[b][k]);
+            for (int v = 0; v < m; ++v) qs[a * m + v] = q[i * m + v];
+        }
+        for (size_t a = t_off[j]; a < t_off[j + 1]; ++a) {
+            size_t i = t_perm[a];
+            for (int k = 0; k < 3; ++k)
+                ut[3 * a + k] = orc_leaf_coordinate(tgt[3 * i + k], lower[k], side, B.level[b], B.idx[b][k]);
+        }
+    }
+
+    /* tables */
+    double *m2l_t = (double *)malloc((size_t)316 * nc * nc * sizeof(double));
+    double *m2m_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
+    double *l2l_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
+    orc_build_m2l_tables(p, m2l_t);
+    orc_build_m2m_tables(p, m2m_t);
+    orc_build_l2l_tables(p, l2l_t);
+
+    double *M = (double *)calloc(B.nboxes * m * nc, sizeof(double));
+    double *Lc = (double *)calloc(B.nboxes * m * nc, sizeof(double));
+    double *phi = (double *)calloc(nt * m + 1, sizeof(double));
+    double *grad = (double *)calloc(3 * nt * m + 1, sizeof(double));
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    int L = B.nlevels - 1;
+
+    /* ---- upward: for l = L..0: p2m(l); m2m(l-1) ---- */
+    for (int l = L; l >= 0; --l) {
+#pragma omp parallel for schedule(dynamic, 4)
+        for (long b = (long)B.level_start[l]; b < (long)B.level_start[l + 1]; ++b) {
+            if (!B.leaf[b]) continue;
+            size_t j = (size_t)leaf_of_box[b];
+            size_t n = s_off[j + 1] - s_off[j];
+            orc_p2m(p, zero3, 1.0, n, us + 3 * s_off[j], qs + m * s_off[j], m, M + (size_t)b * m * nc);
+        }
+        if (l > 0) {
+#pragma omp parallel for schedule(dynamic, 4)
+            for (long b = (long)B.level_start[l - 1]; b < (long)B.level_start[l]; ++b) {
+                if (B.leaf[b]) continue;
+                for (int o = 0; o < 8; ++o) {
+                    long c = child_box(&B, (size_t)b, o);
+                    for (int v = 0; v < m; ++v)
+                        orc_matvec(nc, m2m_t + (size_t)o * nc * nc, M + ((size_t)c * m + v) * nc,
+                                   M + ((size_t)b * m + v) * nc);
+                }
+            }
+        }
+    }
+
+    /* ---- downward: for l = 1..L: l2l, m2l (V by offset), p2l (X by source leaf) ---- */
+    for (int l = 1; l <= L; ++l) {
+#pragma omp parallel for schedule(dynamic, 4)
+        for (long b = (long)B.level_start[l]; b < (long)B.level_start[l + 1]; ++b) {
+            long P = parent_box(&B, (size_t)b);
+            int o = (int)(((B.idx[b][0] & 1) << 2) | ((B.idx[b][1] & 1) << 1) | (B.idx[b][2] & 1));
+            double *Lb = Lc + (size_t)b * m * nc;
+            for (int v = 0; v < m; ++v)
+                orc_matvec(nc, l2l_t + (size_t)o * nc * nc, Lc + ((size_t)P * m + v) * nc, Lb + v * nc);
+            /* V: children of the parent's colleagues, not adjacent to b, by offset index */
+            size_t vl[189][2];
+            int nv = 0;
+            for (int dx = -1; dx <= 1; ++dx)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dz = -1; dz <= 1; ++dz) {
+                        if (!dx && !dy && !dz) continue;
+                        long C = neighbour(&B, (size_t)P, dx, dy, dz);
+                        if (C < 0 || B.leaf[C]) continue;
+                        for (int co = 0; co < 8; ++co) {
+                            long s = child_box(&B, (size_t)C, co);
+                            if (adjacent_boxes(&B, (size_t)s, (size_t)b)) continue;
+                            vl[nv][0] = (size_t)offset_of(&B, (size_t)b, (size_t)s);
+                            vl[nv][1] = (size_t)s;
+                            ++nv;
+                        }
+                    }
+            qsort(vl, nv, sizeof(vl[0]), cmp_pair);
+            for (int e = 0; e < nv; ++e)
+                for (int v = 0; v < m; ++v)
+                    orc_matvec(nc, m2l_t + vl[e][0] * nc * nc, M + (vl[e][1] * m + v) * nc, Lb + v * nc);
+            /* X: leaves among the parent's colleagues, not adjacent to b, by leaf index */
+            vecz xl = {0, 0, 0};
+            for (int dx = -1; dx <= 1; ++dx)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dz = -1; dz <= 1; ++dz) {
+                        if (!dx && !dy && !dz) continue;
+                        long C = neighbour(&B, (size_t)P, dx, dy, dz);
+                        if (C < 0 || !B.leaf[C] || adjacent_boxes(&B, (size_t)C, (size_t)b)) continue;
+                        zpush(&xl, (size_t)leaf_of_box[C]);
+                    }
+            sort_unique(&xl);
+            for (size_t e = 0; e < xl.len; ++e) {
+                size_t j = xl.data[e], s = leaf_box[j];
+                double c[3], r;
+                rel_frame(&B, (size_t)b, s, c, &r); /* (c(t|s), r(t|s)) */
+                orc_p2l(p, c, r, s_off[j + 1] - s_off[j], us + 3 * s_off[j], qs + m * s_off[j], m, Lb);
+            }
+            free(xl.data);
+        }
+    }
+
+    /* ---- leaves: for l = 0..L: l2p, m2p (W by box index), p2p (near by source leaf) ---- */
+    for (int l = 0; l <= L; ++l) {
+#pragma omp parallel for schedule(dynamic, 2)
+        for (long b = (long)B.level_start[l]; b < (long)B.level_start[l + 1]; ++b) {
+            if (!B.leaf[b]) continue;
+            size_t j = (size_t)leaf_of_box[b];
+            size_t n = t_off[j + 1] - t_off[j];
+            if (n == 0) continue;
+            /* chunk-local outputs: phi[v][n], grad[v][n][3] */
+            double *cphi = (double *)calloc(m * n, sizeof(double));
+            double *cg = gradients ? (double *)calloc(3 * m * n, sizeof(double)) : NULL;
+            const double *u = ut + 3 * t_off[j];
+            orc_l2p(p, zero3, 1.0, Lc + (size_t)b * m * nc, m, n, u, cphi, cg);
+            vecz wl = {0, 0, 0}, near = {0, 0, 0};
+            for (int dx = -1; dx <= 1; ++dx)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dz = -1; dz <= 1; ++dz) {
+                        if (!dx && !dy && !dz) continue;
+                        long N = neighbour(&B, (size_t)b, dx, dy, dz);
+                        if (N == -2) continue;
+                        if (N >= 0 && !B.leaf[N]) {
+                            for (int co = 0; co < 8; ++co) {
+                                long c = child_box(&B, (size_t)N, co);
+                                if (adjacent_boxes(&B, (size_t)c, (size_t)b)) zpush(&near, (size_t)leaf_of_box[c]);
+                                else zpush(&wl, (size_t)c);
+                            }
+                        } else if (N >= 0) {
+                            zpush(&near, (size_t)leaf_of_box[N]);
+                        } else {
+                            /* the neighbour cell is not a box: its parent is a coarser leaf */
+                            int l1 = B.level[b];
+                            uint32_t ni[3] = {(uint32_t)((long)B.idx[b][0] + dx) >> 1,
+                                              (uint32_t)((long)B.idx[b][1] + dy) >> 1,
+                                              (uint32_t)((long)B.idx[b][2] + dz) >> 1};
+                            long C = find(&B, orc_key_from_index(ni, l1 - 1));
+                            if (C >= 0 && B.leaf[C]) zpush(&near, (size_t)leaf_of_box[C]);
+                        }
+                    }
+            zpush(&near, j);
+            sort_unique(&wl);
+            sort_unique(&near);
+            for (size_t e = 0; e < wl.len; ++e) {
+                size_t s = wl.data[e];
+                double c[3], r;
+                rel_frame(&B, s, (size_t)b, c, &r); /* (c(s|t), r(s|t)) */
+                orc_m2p(p, c, r, M + s * m * nc, m, n, u, cphi, cg);
+            }
+            double *ys = NULL;
+            size_t ys_cap = 0;
+            for (size_t e = 0; e < near.len; ++e) {
+                size_t sj = near.data[e], s = leaf_box[sj];
+                size_t nsrc = s_off[sj + 1] - s_off[sj];
+                const double *y = us + 3 * s_off[sj];
+                if (sj != j) {
+                    if (nsrc > ys_cap) { ys_cap = nsrc; ys = (double *)realloc(ys, 3 * nsrc * sizeof(double)); }
+                    double c[3], r;
+                    rel_frame(&B, s, (size_t)b, c, &r);
+                    for (size_t a = 0; a < nsrc; ++a)
+                        for (int k = 0; k < 3; ++k) ys[3 * a + k] = c[k] + r * us[3 * (s_off[sj] + a) + k];
+                    y = ys;
+                }
+                double *qv = (double *)malloc((nsrc + 1) * sizeof(double));
+                for (int v = 0; v < m; ++v) {
+                    for (size_t a = 0; a < nsrc; ++a) qv[a] = qs[(s_off[sj] + a) * m + v];
+                    orc_p2p(nsrc, y, qv, n, u, cphi + v * n, cg ? cg + 3 * v * n : NULL);
+                }
+                free(qv);
+            }
+            free(ys);
+            free(wl.data);
+            free(near.data);
+            for (int v = 0; v < m; ++v)
+                for (size_t a = 0; a < n; ++a) {
+                    phi[v * nt + t_off[j] + a] = cphi[v * n + a];
+                    if (cg)
+                        for (int k = 0; k < 3; ++k) grad[3 * (v * nt + t_off[j] + a) + k] = cg[3 * (v * n + a) + k];
+                }
+            free(cphi);
+            free(cg);
+        }
+    }
+
+    /* ---- output pass ---- */
+    for (size_t j = 0; j < nleaves; ++j) {
+        double r = ldexp(side, -(B.level[leaf_box[j]] + 1));
+        double ps = 4.0 * M_PI * r, gs = 4.0 * M_PI * r * r;
+        for (size_t a = t_off[j]; a < t_off[j + 1]; ++a) {
+            size_t i = t_perm[a];
+            for (int v = 0; v < m; ++v) {
+                phi_out[v * nt + i] = phi[v * nt + a] / ps;
+                if (gradients && grad_out)
+                    for (int k = 0; k < 3; ++k)
+                        grad_out[3 * (v * nt + i) + k] = grad[3 * (v * nt + a) + k] / gs;
+            }
+        }
+    }
+
+    free(M); free(Lc); free(phi); free(grad);
+    free(m2l_t); free(m2m_t); free(l2l_t);
+    free(us); free(qs); free(ut);
+    free(s_leaf); free(t_leaf); free(s_off); free(t_off); free(s_perm); free(t_perm);
+    free(leaf_of_box); free(leaf_box);
+    free(B.key); free(B.leaf); free(B.level); free(B.idx); free(B.level_start);
+    free(B.sorted); free(B.sorted_box);
+    return 0;
+}

@@ -1,0 +1,212 @@
+"""ctypes bindings of the oracle library (oracle/_build/liboracle.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py, never by the product package.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_sz = C.c_size_t
+
+
+def build():
+    """Compiles the oracle with its Makefile (gcc, no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        sig = {
+            "orc_rng_next": (C.c_uint64, [C.c_void_p]),
+            "orc_regular": (None, [C.c_int, _dp, _dp]),
+            "orc_irregular": (None, [C.c_int, _dp, _dp]),
+            "orc_regular_grad": (None, [C.c_int, _dp, _dp, _dp, _dp, _dp]),
+            "orc_irregular_grad": (None, [C.c_int, _dp, _dp, _dp, _dp, _dp]),
+            "orc_p2m": (None, [C.c_int, _dp, C.c_double, _sz, _dp, _dp, C.c_int, _dp]),
+            "orc_p2l": (None, [C.c_int, _dp, C.c_double, _sz, _dp, _dp, C.c_int, _dp]),
+            "orc_l2p": (None, [C.c_int, _dp, C.c_double, _dp, C.c_int, _sz, _dp, _dp, C.c_void_p]),
+            "orc_m2p": (None, [C.c_int, _dp, C.c_double, _dp, C.c_int, _sz, _dp, _dp, C.c_void_p]),
+            "orc_m2m": (None, [C.c_int, _dp, C.c_double, _dp, C.c_double, _dp, _dp]),
+            "orc_l2l": (None, [C.c_int, _dp, C.c_double, _dp, C.c_double, _dp, _dp]),
+            "orc_m2l": (None, [C.c_int, _dp, C.c_double, _dp, C.c_double, _dp, _dp]),
+            "orc_build_m2l_tables": (None, [C.c_int, _dp]),
+            "orc_build_m2m_tables": (None, [C.c_int, _dp]),
+            "orc_build_l2l_tables": (None, [C.c_int, _dp]),
+            "orc_offset_index": (C.c_int, [C.c_int64, C.c_int64, C.c_int64]),
+            "orc_p2p": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_direct_sum": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_direct_sum_omp": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_key_from_index": (C.c_uint64, [_u32p, C.c_int]),
+            "orc_tree_build": (C.c_void_p, [_sz, _dp, _sz, _dp, C.c_int, C.c_int]),
+            "orc_tree_free": (None, [C.c_void_p]),
+            "orc_tree_nlevels": (C.c_int, [C.c_void_p]),
+            "orc_tree_nboxes": (_sz, [C.c_void_p]),
+            "orc_tree_nleaves": (_sz, [C.c_void_p]),
+            "orc_tree_boxes": (None, [C.c_void_p, _u64p, _u8p]),
+            "orc_tree_list": (_sz, [C.c_void_p, _sz, C.c_int, _u64p, _sz]),
+            "orc_fmm": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, _dp, C.c_void_p]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def nc(p):
+    return (p + 1) ** 2
+
+
+class Rng:
+    """SplitMix64 (fmm-validate/src/rng.rs:24-45)."""
+
+    def __init__(self, seed):
+        self.state = C.c_uint64(seed)
+
+    def next_u64(self):
+        return lib().orc_rng_next(C.byref(self.state))
+
+
+def regular(p, x):
+    out = np.zeros(nc(p))
+    lib().orc_regular(p, np.ascontiguousarray(x, dtype=np.float64), out)
+    return out
+
+
+def irregular(p, x):
+    out = np.zeros(nc(p))
+    lib().orc_irregular(p, np.ascontiguousarray(x, dtype=np.float64), out)
+    return out
+
+
+def regular_grad(p, x):
+    v, gx, gy, gz = (np.zeros(nc(p)) for _ in range(4))
+    lib().orc_regular_grad(p, np.ascontiguousarray(x, dtype=np.float64), v, gx, gy, gz)
+    return v, np.stack([gx, gy, gz])
+
+
+def irregular_grad(p, x):
+    v, gx, gy, gz = (np.zeros(nc(p)) for _ in range(4))
+    lib().orc_irregular_grad(p, np.ascontiguousarray(x, dtype=np.float64), v, gx, gy, gz)
+    return v, np.stack([gx, gy, gz])
+
+
+def tables(p):
+    n = nc(p)
+    m2l = np.zeros(316 * n * n)
+    m2m = np.zeros(8 * n * n)
+    l2l = np.zeros(8 * n * n)
+    lib().orc_build_m2l_tables(p, m2l)
+    lib().orc_build_m2m_tables(p, m2m)
+    lib().orc_build_l2l_tables(p, l2l)
+    return m2l.reshape(316, n, n), m2m.reshape(8, n, n), l2l.reshape(8, n, n)
+
+
+def p2p(src, q, tgt, gradients=True):
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    phi = np.zeros(len(tgt))
+    g = np.zeros((len(tgt), 3)) if gradients else None
+    lib().orc_p2p(len(src), src, q, len(tgt), tgt, phi, _ptr(g))
+    return phi, g
+
+
+def direct_sum(src, q, tgt, gradients=True, threads=True):
+    """Neumaier-compensated f64 direct sum of q/|x-y| (fmm-ref/src/p2p.rs:147-186)."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    phi = np.zeros(len(tgt))
+    g = np.zeros((len(tgt), 3)) if gradients else None
+    f = lib().orc_direct_sum_omp if threads else lib().orc_direct_sum
+    f(len(src), src, q, len(tgt), tgt, phi, _ptr(g))
+    return phi, g
+
+
+def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0):
+    """The restated host FMM; q is (N,) or (N, m); returns phi (m, Nt), grad (m, Nt, 3)
+    in caller order with 1/(4 pi) applied."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64)
+    m = 1 if q.ndim == 1 else q.shape[1]
+    q = np.ascontiguousarray(q.reshape(len(src), m))
+    phi = np.zeros(m * len(tgt))
+    g = np.zeros(3 * m * len(tgt)) if gradients else None
+    rc = lib().orc_fmm(len(src), src, q, m, len(tgt), tgt, p, max_keys, int(gradients), threads,
+                       phi, _ptr(g))
+    if rc != 0:
+        raise RuntimeError(f"oracle fmm failed: {rc}")
+    return phi.reshape(m, len(tgt)), (g.reshape(m, len(tgt), 3) if gradients else None)
+
+
+class Tree:
+    """The oracle's octree (refine + 2:1 balance) and its brute-force list rule."""
+
+    def __init__(self, src, tgt, max_level, max_keys):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+        self._t = lib().orc_tree_build(len(src), src, len(tgt), tgt, max_level, max_keys)
+        n = lib().orc_tree_nboxes(self._t)
+        self.keys = np.zeros(n, dtype=np.uint64)
+        self.is_leaf = np.zeros(n, dtype=np.uint8)
+        lib().orc_tree_boxes(self._t, self.keys, self.is_leaf)
+        self.nlevels = lib().orc_tree_nlevels(self._t)
+
+    def list(self, box, kind):
+        out = np.zeros(4096, dtype=np.uint64)
+        n = lib().orc_tree_list(self._t, box, kind, out, len(out))
+        return out[:n].copy()
+
+    def __del__(self):
+        if getattr(self, "_t", None):
+            lib().orc_tree_free(self._t)
+            self._t = None
+
+
+def point_sets(kind, n, seed):
+    """Seeded inputs via the restated generators (fmm-validate/src/points.rs)."""
+    L = lib()
+    st = C.c_uint64(seed)
+    xyz = np.zeros(3 * n)
+    c = np.array([0.5, 0.5, 0.5])
+    fns = {
+        "cube": ("orc_points_cube", [c.ctypes.data_as(C.c_void_p), C.c_double(0.5)]),
+    }
+    if kind == "cube":
+        f = L.orc_points_cube
+        f.argtypes = [C.c_void_p, _sz, _dp, C.c_double, _dp]
+        f(C.byref(st), n, c, 0.5, xyz)
+    elif kind == "sphere":
+        f = L.orc_points_sphere_gauss
+        f.argtypes = [C.c_void_p, _sz, _dp, C.c_double, _dp]
+        f(C.byref(st), n, np.zeros(3), 1.0, xyz)
+    else:
+        raise ValueError(kind)
+    del fns
+    q = np.zeros(n)
+    L.orc_charges.argtypes = [C.c_void_p, _sz, _dp]
+    L.orc_charges(C.byref(st), n, q)
+    return xyz.reshape(n, 3), q
