@@ -1,0 +1,376 @@
+"""Benchmark of the FMM evaluation passes on B200 (one JSON line on rank 0).
+
+Workload (the headline configuration): Laplace 3D, N = 4,000,000 points uniform on the
+unit sphere surface (normalised Gaussian 3-vectors), sources = targets, charges N(0, 1),
+p = 8, 128 points per leaf (adaptive octree), potential + gradient; mixed precision
+(f32 points, expansions and P2P, f64 per-target accumulation).  Seeded synthetic input
+(SplitMix64 + Box-Muller, restated here with numpy).  A step is one evaluation: charges
+in, potentials and gradients out.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n N]
+
+value     : N / (device time of one evaluation) in Mpoints/s, inputs resident in HBM,
+            L2 flushed (a 512 MiB write) before every timed step, CUDA events on the
+            evaluator's stream.
+e2e       : the same through the public host API (fmmgpu_fmm_evaluate) with pinned host
+            buffers, host->device charges and device->host outputs inside the timed call.
+plain_f64 : the plain f64 evaluator (the drop-in) on the same input, for the mixed/plain
+            ratio of the metric.
+error     : relative L2 of phi and grad at 2,000 sampled targets against an f64 direct sum
+            (Neumaier-compensated, on the GPU) of all sources.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P = 8
+LEAF = 128
+N_DEFAULT = 4_000_000
+SEED = 0x5EED_0002
+SAMPLE = 2000
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# reference op model of P2P: 10 FP32 lane-ops per pair for phi, 15 with the gradient
+# (fmm-validate/src/peaks.rs:12-17)
+P2P_OPS = {False: 10, True: 15}
+
+
+# ------------------------------------------------------------------------------------
+# seeded synthetic input (SplitMix64 of fmm-validate/src/rng.rs, vectorised)
+# ------------------------------------------------------------------------------------
+def splitmix(seed, count):
+    with np.errstate(over="ignore"):
+        k = np.arange(1, count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + k * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform01(u):
+    return (u >> np.uint64(11)).astype(np.float64) * (1.0 / float(1 << 53))
+
+
+def normals(seed, count):
+    """Box-Muller (cosine branch) on pairs of SplitMix64 uniforms, 1 - U in (0, 1]."""
+    u = uniform01(splitmix(seed, 2 * count)).reshape(count, 2)
+    return np.sqrt(-2.0 * np.log(1.0 - u[:, 0])) * np.cos(2.0 * np.pi * u[:, 1])
+
+
+def sphere_problem(n, seed=SEED):
+    g = normals(seed, 3 * n).reshape(n, 3)
+    x = g / np.linalg.norm(g, axis=1, keepdims=True)
+    q = normals(seed + 1, n)
+    return np.ascontiguousarray(x), np.ascontiguousarray(q)
+
+
+def sample_indices(n, count, seed=SEED + 2):
+    r = splitmix(seed, count)
+    order = np.arange(n)
+    for i in range(count):
+        j = i + int((int(r[i]) >> 32) * (n - i) >> 32)
+        order[i], order[j] = order[j], order[i]
+    return order[:count].copy()
+
+
+# ------------------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            sm = [float(r[1]) for r in rows]
+            smax = max(float(r[2]) for r in rows)
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                    "samples": len(rows)}
+        except Exception as e:  # no nvidia-smi or no samples
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)[:80]}
+
+
+def peaks():
+    try:
+        return json.load(open(PEAKS))
+    except Exception:
+        return {}
+
+
+def run_ours(args):
+    import torch
+
+    import fmm_b200 as F
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n = args.n
+    # weak scaling: every rank evaluates its own independent cloud (replicas of the
+    # workload with different seeds); no data-path collective
+    x, q = sphere_problem(n, SEED + 1000 * rank)
+    sample = sample_indices(n, SAMPLE)
+
+    def build(precision):
+        return (F.FmmBuilder(P).gradients().max_points_per_leaf(LEAF).precision(precision)
+                .device(local).build(x))
+
+    t0 = time.perf_counter()
+    fmm = build("mixed")
+    build_s = time.perf_counter() - t0
+    info = fmm.info()
+    stream = torch.cuda.ExternalStream(fmm.stream)
+    dev = torch.device("cuda", local)
+    dq = torch.from_numpy(q).to(dev)
+    dphi = torch.empty(n, dtype=torch.float64, device=dev)
+    dg = torch.empty(n * 3, dtype=torch.float64, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def device_steps(f, steps, warmup):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                f.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
+            f.synchronize()
+            total = 0.0
+            for _ in range(steps):
+                flush.zero_()
+                s = torch.cuda.Event(enable_timing=True)
+                e = torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                f.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
+                e.record(stream)
+                e.synchronize()
+                total += s.elapsed_time(e)
+            f.synchronize()
+        return total / steps
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ms = device_steps(fmm, args.steps, args.warmup)
+    clocks = clk.summary()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    # per-kind split and the dominant kernel (separate, untimed evaluation)
+    fmm.set_kind_timing(True)
+    with torch.cuda.stream(stream):
+        flush.zero_()
+        fmm.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
+    kinds = fmm.kind_times()
+    fmm.set_kind_timing(False)
+    # accuracy at sampled targets against the f64 direct sum on the GPU
+    with torch.cuda.stream(stream):
+        fmm.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
+    fmm.synchronize()
+    phi = dphi.cpu().numpy()
+    grad = dg.cpu().numpy().reshape(n, 3)
+    ex_phi, ex_g = F.direct_sum(x, q, x[sample], device=local)
+    err_phi = float(np.linalg.norm(phi[sample] - ex_phi) / np.linalg.norm(ex_phi))
+    err_g = float(np.linalg.norm(grad[sample] - ex_g) / np.linalg.norm(ex_g))
+    # e2e through the host API with pinned buffers
+    hq = torch.from_numpy(q).pin_memory()
+    hphi = torch.empty(n, dtype=torch.float64).pin_memory()
+    hg = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        F._check(F.lib().fmmgpu_fmm_evaluate(fmm._h, hq.data_ptr(), hphi.data_ptr(), hg.data_ptr()))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        F._check(F.lib().fmmgpu_fmm_evaluate(fmm._h, hq.data_ptr(), hphi.data_ptr(), hg.data_ptr()))
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    fmm.close()
+    # the plain f64 evaluator on the same input
+    plain = build("f64")
+    plain_ms = device_steps(plain, max(2, args.steps // 2), max(1, args.warmup // 2))
+    with torch.cuda.stream(torch.cuda.ExternalStream(plain.stream)):
+        plain.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
+    plain.synchronize()
+    pphi = dphi.cpu().numpy()
+    perr = float(np.linalg.norm(pphi[sample] - ex_phi) / np.linalg.norm(ex_phi))
+    plain.close()
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
+    pk = peaks()
+    sm_max = float(pk.get("sm_max_mhz", 1965.0))
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    dominant = max(kinds, key=kinds.get)
+    roof = {"kernel": dominant}
+    if dominant == "p2p":
+        ops = info["near_pairs"] * P2P_OPS[True]
+        peak = nsm * 128 * sm_max * 1e6 / 1e12
+        achieved = ops / (kinds["p2p"] * 1e-3) / 1e12
+        roof.update({"bound": "fp32", "achieved": round(achieved, 2), "peak": round(peak, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                     "peak_source": f"derived: {nsm} SMs x 128 FP32 lanes x {sm_max:.0f} MHz "
+                                    "(no FP32 peak in MEASURED_PEAKS.json)",
+                     "op_model": "15 FP32 lane-ops per pair (fmm-validate/src/peaks.rs:12-17)",
+                     "traffic": None})
+    else:
+        roof.update({"bound": "unknown", "achieved": None, "peak": None, "unit": None, "frac": None,
+                     "traffic": None})
+    value = world * n / (ms * 1e-3) / 1e6
+    line = {
+        "metric": "Mpoints/s at rel-L2 <=1e-6 vs FP64 direct: mixed/batched vs plain FP64 GPU FMM",
+        "value": round(value, 3),
+        "unit": "Mpoints/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 per-target accumulation)",
+        "data": "synthetic (seeded SplitMix64: unit-sphere surface from normalised Gaussians, q ~ N(0,1))",
+        "config": {"workload": f"laplace3d sphere N={n} p={P} leaf={LEAF} phi+grad mixed",
+                   "n_points": n, "p": P, "max_points_per_leaf": LEAF, "gradients": True,
+                   "precision": "mixed", "l2": "flushed (512 MiB write) before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "error": {"phi_rel_l2": err_phi, "grad_rel_l2": err_g, "sampled_targets": SAMPLE,
+                  "against": "f64 direct sum (GPU, Neumaier)", "plain_f64_phi_rel_l2": perr},
+        "plain_f64": {"ms_per_step": round(plain_ms, 4), "value": round(n / (plain_ms * 1e-3) / 1e6, 3),
+                      "mixed_over_plain": round(plain_ms / ms, 3)},
+        "kinds_ms": {k: round(v, 4) for k, v in kinds.items()},
+        "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs",
+                                      "x_pairs", "device_bytes")},
+        "build_s": round(build_s, 3),
+        "e2e": {"value": round(n / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
+                "ms_per_step": round(e2e_ms, 4),
+                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8 * 4},
+        "gpu_launches": None,
+        "roofline": roof,
+        "clocks": clocks,
+    }
+    line["gpu_launches"] = launches_per_step(info)
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def launches_per_step(info):
+    # charge load, P2M, M2M per level, (L2L, M2L, P2L) per level >= 2, L2P+M2P, P2P
+    L = info["nlevels"] - 1
+    return 1 + 1 + max(0, L) + 3 * max(0, L - 1) - (1 if L >= 2 else 0) + 2
+
+
+def cpu_baseline(args, n_sample=None):
+    """The restated reference host FMM (oracle, OpenMP over all host cores) on a bounded
+    sample of the same workload: the same sphere problem at a smaller N."""
+    from oracle import oracle as O
+
+    n = n_sample or args.cpu_n
+    x, q = sphere_problem(n, SEED)
+    cores = os.cpu_count()
+    O.fmm(x[:2000], q[:2000], x[:2000], P, LEAF, gradients=True, threads=cores)  # warm the library
+    t0 = time.perf_counter()
+    O.fmm(x, q, x, P, LEAF, gradients=True, threads=cores)
+    s = time.perf_counter() - t0
+    return {"value": round(n / s / 1e6, 4), "unit": "Mpoints/s", "cores": cores, "kind": "port",
+            "sample": f"sphere N={n} p={P} leaf={LEAF} phi+grad f64, one evaluation incl. its table build "
+                      f"({s:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    times = []
+    for _ in range(args.warmup):
+        cpu_baseline(args, args.cpu_n // 4)
+    for _ in range(args.steps):
+        b = cpu_baseline(args)
+        times.append(b["value"])
+    v = float(np.median(times))
+    b["value"] = round(v, 4)
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "Mpoints/s at rel-L2 <=1e-6 vs FP64 direct: mixed/batched vs plain FP64 GPU FMM",
+        "value": v, "unit": "Mpoints/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded SplitMix64 sphere)",
+        "config": {"workload": f"laplace3d sphere p={P} leaf={LEAF} phi+grad, bounded sample N={args.cpu_n}"},
+        "cpu_baseline": b,
+        "e2e": {"value": v, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-n", type=int, default=400_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

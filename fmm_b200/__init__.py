@@ -1,0 +1,248 @@
+"""B200 evaluator for the FMM evaluation passes of tbetcke/fmm (Laplace 1/(4 pi r)).
+
+The Python surface mirrors nd-fmm-exec's builder API (fmm-exec/src/fmm.rs):
+
+    fmm = (FmmBuilder(p=6).gradients().vectors(1).max_points_per_leaf(64)
+           .precision("f64").build(sources, targets))
+    out = fmm.evaluate(charges)        # Output: potential (m, nt), gradient (m, nt, 3)
+
+Every call goes through the C ABI of include/fmm_b200.h in fmm_b200/libfmm_b200.so;
+there is no fallback: if the library or a GPU is missing, build() raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["FmmBuilder", "Fmm", "Output", "FmmError", "lib", "Plan", "direct_sum"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBPATH = os.path.join(_HERE, "libfmm_b200.so")
+_lib = None
+
+PRECISIONS = {"f64": 0, "mixed": 1}
+
+
+class FmmError(RuntimeError):
+    """A failed call of the C ABI (status code and message)."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class Settings(C.Structure):
+    _fields_ = [("p", C.c_int), ("precision", C.c_int), ("gradients", C.c_int), ("vectors", C.c_int),
+                ("max_points_per_leaf", C.c_int), ("max_level", C.c_int), ("device", C.c_int)]
+
+
+class Info(C.Structure):
+    _fields_ = [("nlevels", C.c_int), ("nboxes", C.c_int64), ("nleaves", C.c_int64),
+                ("nsources", C.c_int64), ("ntargets", C.c_int64), ("near_pairs", C.c_int64),
+                ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
+                ("device_bytes", C.c_int64)]
+
+
+def lib():
+    """Loads libfmm_b200.so (built by fmm_b200.build); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIBPATH):
+            raise FmmError(-1, f"{_LIBPATH} is missing: run `python -m fmm_b200.build`")
+        L = C.CDLL(_LIBPATH)
+        vp, sz, dp = C.c_void_p, C.c_size_t, C.c_void_p
+        sig = {
+            "fmmgpu_default_settings": (None, [C.POINTER(Settings)]),
+            "fmmgpu_fmm_build": (C.c_int, [C.POINTER(Settings), sz, dp, sz, dp, C.POINTER(vp)]),
+            "fmmgpu_plan_build": (C.c_int, [C.POINTER(Settings), sz, dp, sz, dp, C.POINTER(vp)]),
+            "fmmgpu_fmm_evaluate": (C.c_int, [vp, dp, dp, dp]),
+            "fmmgpu_fmm_evaluate_device": (C.c_int, [vp, dp, dp, dp]),
+            "fmmgpu_fmm_stream": (vp, [vp]),
+            "fmmgpu_fmm_synchronize": (C.c_int, [vp]),
+            "fmmgpu_fmm_info": (C.c_int, [vp, C.POINTER(Info)]),
+            "fmmgpu_fmm_destroy": (None, [vp]),
+            "fmmgpu_fmm_boxes": (C.c_int, [vp, dp, dp]),
+            "fmmgpu_fmm_list": (C.c_int64, [vp, C.c_int, C.c_int64, dp, C.c_int64]),
+            "fmmgpu_fmm_tables": (C.c_int, [vp, dp, dp, dp]),
+            "fmmgpu_fmm_set_kind_timing": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_kind_times": (C.c_int, [vp, dp]),
+            "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
+            "fmmgpu_status_string": (C.c_char_p, [C.c_int]),
+            "fmmgpu_last_error": (C.c_char_p, []),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise FmmError(status, lib().fmmgpu_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _points(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.ndim != 2 or x.shape[1] != 3:
+        raise ValueError("points must have shape (n, 3)")
+    return x
+
+
+def direct_sum(sources, charges, targets, gradients=True, device=0):
+    """f64 direct sum on the GPU (Neumaier per target), with 1/(4 pi): phi (nt,), grad (nt, 3)."""
+    src = _points(sources)
+    tgt = _points(targets)
+    q = np.ascontiguousarray(charges, dtype=np.float64).reshape(len(src))
+    phi = np.zeros(len(tgt))
+    g = np.zeros((len(tgt), 3)) if gradients else None
+    _check(lib().fmmgpu_direct_sum(len(src), _ptr(src), _ptr(q), len(tgt), _ptr(tgt), _ptr(phi), _ptr(g), device))
+    return phi, g
+
+
+class Output:
+    """Potentials (m, nt) and, with gradients, gradients (m, nt, 3), caller order."""
+
+    def __init__(self, potential, gradient):
+        self.potential = potential
+        self.gradient = gradient
+
+
+class FmmBuilder:
+    """The settings of an FMM, as nd-fmm-exec's FmmBuilder (fmm-exec/src/fmm.rs:1228-1270)."""
+
+    def __init__(self, p=6):
+        self._s = Settings()
+        lib().fmmgpu_default_settings(C.byref(self._s))
+        self._s.p = p
+
+    def gradients(self, on=True):
+        self._s.gradients = int(bool(on))
+        return self
+
+    def vectors(self, m):
+        self._s.vectors = int(m)
+        return self
+
+    def max_points_per_leaf(self, n):
+        self._s.max_points_per_leaf = int(n)
+        return self
+
+    def max_level(self, level):
+        self._s.max_level = int(level)
+        return self
+
+    def precision(self, name):
+        if name not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self._s.precision = PRECISIONS[name]
+        return self
+
+    def device(self, ordinal):
+        self._s.device = int(ordinal)
+        return self
+
+    def build(self, sources, targets=None):
+        src = _points(sources)
+        tgt = src if targets is None else _points(targets)
+        h = C.c_void_p()
+        _check(lib().fmmgpu_fmm_build(C.byref(self._s), len(src), _ptr(src), len(tgt), _ptr(tgt), C.byref(h)))
+        return Fmm(h, self._s, len(src), len(tgt))
+
+    def plan(self, sources, targets=None):
+        """The host half only (tree, lists, tables); needs no GPU."""
+        src = _points(sources)
+        tgt = src if targets is None else _points(targets)
+        h = C.c_void_p()
+        _check(lib().fmmgpu_plan_build(C.byref(self._s), len(src), _ptr(src), len(tgt), _ptr(tgt), C.byref(h)))
+        return Plan(h, self._s, len(src), len(tgt))
+
+
+class Plan:
+    """A built plan (host half of an FMM): boxes, lists and tables, for inspection."""
+
+    def __init__(self, handle, settings, ns, nt):
+        self._h = handle
+        self.settings = settings
+        self.nsources = ns
+        self.ntargets = nt
+
+    def info(self):
+        i = Info()
+        _check(lib().fmmgpu_fmm_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in Info._fields_}
+
+    def boxes(self):
+        n = self.info()["nboxes"]
+        keys = np.zeros(n, dtype=np.uint64)
+        leaf = np.zeros(n, dtype=np.uint8)
+        _check(lib().fmmgpu_fmm_boxes(self._h, _ptr(keys), _ptr(leaf)))
+        return keys, leaf
+
+    def list(self, kind, row):
+        out = np.zeros(4096, dtype=np.uint64)
+        n = lib().fmmgpu_fmm_list(self._h, kind, row, _ptr(out), len(out))
+        if n < 0:
+            raise IndexError(row)
+        return out[:n].copy()
+
+    def tables(self):
+        p = self.settings.p
+        n = (p + 1) ** 2
+        m2l = np.zeros(316 * n * n)
+        m2m = np.zeros(8 * n * n)
+        l2l = np.zeros(8 * n * n)
+        _check(lib().fmmgpu_fmm_tables(self._h, _ptr(m2l), _ptr(m2m), _ptr(l2l)))
+        # column-major storage: entry (i, k) at i + k n; return A with A[t] @ x = output
+        return (m2l.reshape(316, n, n).transpose(0, 2, 1), m2m.reshape(8, n, n).transpose(0, 2, 1),
+                l2l.reshape(8, n, n).transpose(0, 2, 1))
+
+    def close(self):
+        if self._h:
+            lib().fmmgpu_fmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Fmm(Plan):
+    """A built FMM on one GPU (nd-fmm-exec's Fmm): evaluate charge vectors."""
+
+    def evaluate(self, charges):
+        m = self.settings.vectors
+        q = np.ascontiguousarray(charges, dtype=np.float64).reshape(self.nsources, m)
+        phi = np.zeros((m, self.ntargets))
+        g = np.zeros((m, self.ntargets, 3)) if self.settings.gradients else None
+        _check(lib().fmmgpu_fmm_evaluate(self._h, _ptr(q), _ptr(phi), _ptr(g)))
+        return Output(phi, g)
+
+    def evaluate_device(self, charges_ptr, potential_ptr, gradient_ptr=None):
+        """Device-pointer form (no copies, no sync) on the evaluator's stream."""
+        _check(lib().fmmgpu_fmm_evaluate_device(self._h, charges_ptr, potential_ptr, gradient_ptr))
+
+    KINDS = ("load", "p2m", "m2m", "l2l", "m2l", "p2l", "l2p_m2p", "p2p")
+
+    def set_kind_timing(self, on=True):
+        _check(lib().fmmgpu_fmm_set_kind_timing(self._h, int(on)))
+
+    def kind_times(self):
+        """Milliseconds per kind of the last evaluation (after set_kind_timing(True))."""
+        ms = np.zeros(8)
+        _check(lib().fmmgpu_fmm_kind_times(self._h, _ptr(ms)))
+        return dict(zip(self.KINDS, ms.tolist()))
+
+    @property
+    def stream(self):
+        return lib().fmmgpu_fmm_stream(self._h)
+
+    def synchronize(self):
+        _check(lib().fmmgpu_fmm_synchronize(self._h))

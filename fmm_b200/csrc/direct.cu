@@ -1,0 +1,139 @@
+// f64 direct sum on the GPU: the accuracy reference of benchmarks at sampled targets.
+// Restates fmm-ref/src/p2p.rs:147-186 (direct_sum): every pair with x != y exactly adds
+// q / r and -q d / r^3 (r = sqrt(r2), r^3 = r2 * r, q d formed first), summed per
+// target with Neumaier compensation; here the sources are split into chunks summed
+// separately and the chunk sums are then added in chunk order with compensation.
+// The result carries 1/(4 pi), like the FMM output.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/fmm_b200.h"
+
+namespace {
+
+struct Neumaier {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double t) {
+        double u = s + t;
+        if (fabs(s) >= fabs(t)) c += (s - u) + t;
+        else c += (t - u) + s;
+        s = u;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+
+constexpr int kTile = 256;
+
+__global__ void direct_partial_kernel(const double* __restrict__ src, const double* __restrict__ q, int64_t ns,
+                                      const double* __restrict__ tgt, int64_t nt, int64_t chunk, int grad,
+                                      double* __restrict__ part) {
+    __shared__ double sx[kTile], sy[kTile], sz[kTile], sq[kTile];
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t c0 = blockIdx.y * chunk, c1 = c0 + chunk < ns ? c0 + chunk : ns;
+    double x = 0, y = 0, z = 0;
+    if (t < nt) {
+        x = tgt[3 * t];
+        y = tgt[3 * t + 1];
+        z = tgt[3 * t + 2];
+    }
+    Neumaier ph, g0, g1, g2;
+    for (int64_t b = c0; b < c1; b += kTile) {
+        int cnt = (int)((c1 - b) < kTile ? (c1 - b) : kTile);
+        __syncthreads();
+        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+            sx[j] = src[3 * (b + j)];
+            sy[j] = src[3 * (b + j) + 1];
+            sz[j] = src[3 * (b + j) + 2];
+            sq[j] = q[b + j];
+        }
+        __syncthreads();
+        if (t < nt)
+            for (int j = 0; j < cnt; ++j) {
+                if (x == sx[j] && y == sy[j] && z == sz[j]) continue;
+                double d0 = __dsub_rn(x, sx[j]), d1 = __dsub_rn(y, sy[j]), d2 = __dsub_rn(z, sz[j]);
+                double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+                double r = sqrt(r2);
+                ph.add(sq[j] / r);
+                if (grad) {
+                    double r3 = __dmul_rn(r2, r);
+                    g0.add(-(__dmul_rn(sq[j], d0) / r3));
+                    g1.add(-(__dmul_rn(sq[j], d1) / r3));
+                    g2.add(-(__dmul_rn(sq[j], d2) / r3));
+                }
+            }
+    }
+    if (t < nt) {
+        double* o = part + ((int64_t)blockIdx.y * nt + t) * 4;
+        o[0] = ph.value();
+        o[1] = g0.value();
+        o[2] = g1.value();
+        o[3] = g2.value();
+    }
+}
+
+__global__ void direct_combine_kernel(const double* __restrict__ part, int64_t nt, int nchunks, int grad,
+                                      double* __restrict__ phi, double* __restrict__ g) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    Neumaier s[4];
+    for (int c = 0; c < nchunks; ++c)
+        for (int k = 0; k < 4; ++k) s[k].add(part[((int64_t)c * nt + t) * 4 + k]);
+    const double f = 4.0 * 3.141592653589793;
+    phi[t] = s[0].value() / f;
+    if (grad)
+        for (int k = 0; k < 3; ++k) g[3 * t + k] = s[k + 1].value() / f;
+}
+
+thread_local std::string g_err;
+
+}  // namespace
+
+extern "C" int fmmgpu_direct_sum(size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
+                                 double* phi, double* grad, int device) {
+    auto fail = [](cudaError_t e) {
+        g_err = cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? FMMGPU_DEVICE_MEMORY : FMMGPU_DEVICE_ERROR;
+    };
+    if ((ns && (!src || !q)) || (nt && (!tgt || !phi))) return FMMGPU_INVALID_ARGUMENT;
+    if (nt == 0) return FMMGPU_OK;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e);
+    const int nchunks = ns > (1 << 16) ? 128 : 1;
+    const int64_t chunk = ((int64_t)ns + nchunks - 1) / nchunks;
+    double *dsrc = nullptr, *dq = nullptr, *dtgt = nullptr, *dpart = nullptr, *dphi = nullptr, *dg = nullptr;
+    auto cleanup = [&] {
+        cudaFree(dsrc);
+        cudaFree(dq);
+        cudaFree(dtgt);
+        cudaFree(dpart);
+        cudaFree(dphi);
+        cudaFree(dg);
+    };
+    if ((e = cudaMalloc(&dsrc, 3 * ns * sizeof(double) + 8)) != cudaSuccess ||
+        (e = cudaMalloc(&dq, ns * sizeof(double) + 8)) != cudaSuccess ||
+        (e = cudaMalloc(&dtgt, 3 * nt * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&dpart, (size_t)nchunks * nt * 4 * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&dphi, nt * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&dg, 3 * nt * sizeof(double))) != cudaSuccess) {
+        cleanup();
+        return fail(e);
+    }
+    cudaMemcpy(dsrc, src, 3 * ns * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(dq, q, ns * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(dtgt, tgt, 3 * nt * sizeof(double), cudaMemcpyHostToDevice);
+    dim3 grid((unsigned)((nt + 127) / 128), (unsigned)nchunks);
+    direct_partial_kernel<<<grid, 128>>>(dsrc, dq, (int64_t)ns, dtgt, (int64_t)nt, chunk, grad != nullptr, dpart);
+    direct_combine_kernel<<<(unsigned)((nt + 127) / 128), 128>>>(dpart, (int64_t)nt, nchunks, grad != nullptr, dphi, dg);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        cudaMemcpy(phi, dphi, nt * sizeof(double), cudaMemcpyDeviceToHost);
+        if (grad) cudaMemcpy(grad, dg, 3 * nt * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    cleanup();
+    return e == cudaSuccess ? FMMGPU_OK : fail(e);
+}

@@ -1,0 +1,603 @@
+// The device evaluator: plan upload, the level-by-level pass sequence on one stream,
+// and the C ABI of include/fmm_b200.h.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/fmm_b200.h"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+namespace fmmb {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Failure : std::runtime_error {
+    int status;
+    Failure(int s, const std::string& msg) : std::runtime_error(msg), status(s) {}
+};
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t _e = (expr);                                                                \
+        if (_e != cudaSuccess)                                                                  \
+            throw Failure(_e == cudaErrorMemoryAllocation ? FMMGPU_DEVICE_MEMORY : FMMGPU_DEVICE_ERROR, \
+                          std::string(#expr) + ": " + cudaGetErrorString(_e));                  \
+    } while (0)
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (ptr) cudaFree(ptr);
+    }
+    void alloc(size_t n) {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = n;
+        if (n) CUDA_TRY(cudaMalloc(&ptr, n));
+    }
+    template <class V>
+    void upload(const std::vector<V>& v) {
+        alloc(v.size() * sizeof(V) + sizeof(V));
+        if (!v.empty()) CUDA_TRY(cudaMemcpy(ptr, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+    }
+    template <class V>
+    V* as() const {
+        return static_cast<V*>(ptr);
+    }
+};
+
+inline int round32(int x) { return (x + 31) / 32 * 32; }
+
+}  // namespace
+
+// Per-kind device timing (the reference's KindTiming, fmm-exec/src/fmm.rs:150-153): when
+// enabled, every launch is bracketed by two events on the stream and the elapsed times
+// are summed per kind after the evaluation.
+enum Kind { kLoad = 0, kP2M, kM2M, kL2L, kM2L, kP2L, kFar, kP2P, kKinds };
+
+struct KindTimer {
+    bool on = false;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> events;
+    std::vector<int> kinds;
+    size_t used = 0;
+    double ms[kKinds] = {0};
+    ~KindTimer() {
+        for (auto e : events) cudaEventDestroy(e);
+    }
+    void begin() {
+        used = 0;
+        kinds.clear();
+    }
+    template <class F>
+    void run(int kind, F&& launch) {
+        if (!on) {
+            launch();
+            return;
+        }
+        while (events.size() < used + 2) {
+            cudaEvent_t e;
+            CUDA_TRY(cudaEventCreate(&e));
+            events.push_back(e);
+        }
+        CUDA_TRY(cudaEventRecord(events[used], stream));
+        launch();
+        CUDA_TRY(cudaEventRecord(events[used + 1], stream));
+        kinds.push_back(kind);
+        used += 2;
+    }
+    void collect() {
+        for (int k = 0; k < kKinds; ++k) ms[k] = 0.0;
+        if (!on) return;
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        for (size_t i = 0; i < kinds.size(); ++i) {
+            float t = 0.0f;
+            CUDA_TRY(cudaEventElapsedTime(&t, events[2 * i], events[2 * i + 1]));
+            ms[kinds[i]] += t;
+        }
+    }
+};
+
+// ----------------------------------------------------------------------------------
+// The evaluator of one precision T and one degree P.
+// ----------------------------------------------------------------------------------
+struct EvaluatorBase {
+    KindTimer timer;
+    virtual ~EvaluatorBase() = default;
+    virtual void evaluate(const double* d_charges, double* d_phi, double* d_grad) = 0;
+};
+
+template <int P, typename T>
+struct Evaluator final : EvaluatorBase {
+    static constexpr int NC = nc_of(P);
+    using T4 = typename Vec4<T>::type;
+    const Plan& plan;
+    DevPlan dp{};
+    cudaStream_t stream;
+    int m;
+    bool gradients;
+    // plan arrays
+    DevBuf level, idx, parent, child_first, box_leaf, src_below, tgt_below, leaf_box, src_start,
+        tgt_start, tgt_perm, src_perm, near_row, near_col, w_row, w_col, x_row, x_col, v_row, v_col,
+        v_off;
+    // data
+    DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g;
+
+    Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
+              const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
+              const std::vector<double>& ut)
+        : plan(pl), stream(s), m(m_), gradients(grad) {
+        timer.stream = s;
+        level.upload(pl.level);
+        idx.upload(pl.idx);
+        parent.upload(pl.parent);
+        child_first.upload(pl.child_first);
+        box_leaf.upload(pl.box_leaf);
+        src_below.upload(pl.src_below);
+        tgt_below.upload(pl.tgt_below);
+        leaf_box.upload(pl.leaf_box);
+        src_start.upload(pl.src_start);
+        tgt_start.upload(pl.tgt_start);
+        tgt_perm.upload(pl.tgt_perm);
+        src_perm.upload(pl.src_perm);
+        near_row.upload(pl.near.row);
+        near_col.upload(pl.near.col);
+        w_row.upload(pl.w.row);
+        w_col.upload(pl.w.col);
+        x_row.upload(pl.x.row);
+        x_col.upload(pl.x.col);
+        v_row.upload(pl.v.row);
+        v_col.upload(pl.v.col);
+        v_off.upload(pl.v.aux);
+        dp.nlevels = pl.nlevels;
+        dp.side = pl.side;
+        dp.level = level.as<int32_t>();
+        dp.idx = idx.as<uint32_t>();
+        dp.parent = parent.as<int32_t>();
+        dp.child_first = child_first.as<int32_t>();
+        dp.box_leaf = box_leaf.as<int32_t>();
+        dp.src_below = src_below.as<int64_t>();
+        dp.tgt_below = tgt_below.as<int64_t>();
+        dp.leaf_box = leaf_box.as<int32_t>();
+        dp.src_start = src_start.as<int64_t>();
+        dp.tgt_start = tgt_start.as<int64_t>();
+        dp.tgt_perm = tgt_perm.as<int64_t>();
+        dp.src_perm = src_perm.as<int64_t>();
+        dp.near_row = near_row.as<int64_t>();
+        dp.near_col = near_col.as<int32_t>();
+        dp.w_row = w_row.as<int64_t>();
+        dp.w_col = w_col.as<int32_t>();
+        dp.x_row = x_row.as<int64_t>();
+        dp.x_col = x_col.as<int32_t>();
+        dp.v_row = v_row.as<int64_t>();
+        dp.v_col = v_col.as<int32_t>();
+        dp.v_off = v_off.as<int32_t>();
+        dp.nsrc = (int64_t)pl.src_perm.size();
+        dp.ntgt = (int64_t)pl.tgt_perm.size();
+        // tables rounded entry by entry to T (fmm-tables/src/matrix_set.rs:150 cast)
+        auto up_tab = [](DevBuf& b, const std::vector<double>& t) {
+            std::vector<T> c(t.begin(), t.end());
+            b.upload(c);
+        };
+        up_tab(m2l_tab, m2l);
+        up_tab(m2m_tab, m2m);
+        up_tab(l2l_tab, l2l);
+        // leaf-scaled coordinates, rounded once to T
+        auto up_pos = [](DevBuf& b, const std::vector<double>& u) {
+            size_t n = u.size() / 3;
+            std::vector<T4> v(n);
+            for (size_t i = 0; i < n; ++i) {
+                v[i].x = (T)u[3 * i];
+                v[i].y = (T)u[3 * i + 1];
+                v[i].z = (T)u[3 * i + 2];
+                v[i].w = T(0);
+            }
+            b.upload(v);
+        };
+        up_pos(spos, us);
+        up_pos(tpos, ut);
+        const size_t nb = pl.nboxes();
+        sq.alloc(sizeof(T) * (size_t)m * (dp.nsrc + 1));
+        M.alloc(sizeof(T) * (size_t)m * NC * nb);
+        Lc.alloc(sizeof(T) * (size_t)m * NC * nb);
+        far_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
+        far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
+        CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
+        // shared memory opt-in beyond 48 KB where a kernel needs it
+        size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
+        if (exp_smem > 48 * 1024) {
+            CUDA_TRY(cudaFuncSetAttribute(expand_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)exp_smem));
+            CUDA_TRY(cudaFuncSetAttribute(expand_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)exp_smem));
+        }
+    }
+
+    size_t device_bytes() const {
+        const DevBuf* all[] = {&level, &idx, &parent, &child_first, &box_leaf, &src_below, &tgt_below,
+                               &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
+                               &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
+                               &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g};
+        size_t s = 0;
+        for (auto* b : all) s += b->bytes;
+        return s;
+    }
+
+    void evaluate(const double* d_charges, double* d_phi, double* d_grad) override {
+        const int64_t ns = dp.nsrc;
+        const int L = plan.nlevels - 1;
+        const size_t nleaves = plan.nleaves();
+        timer.begin();
+        // charge load into leaf order
+        timer.run(kLoad, [&] {
+            if (ns > 0)
+                charge_load_kernel<T><<<(unsigned)((ns + 255) / 256), 256, 0, stream>>>(
+                    d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>());
+            CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, Lc.bytes, stream));
+        });
+        // upward: P2M of every leaf, then M2M from level L-1 up to 0
+        const size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
+        timer.run(kP2M, [&] {
+            if (nleaves)
+                expand_kernel<P, T, false><<<(unsigned)nleaves, 32, exp_smem, stream>>>(
+                    dp, 0, (int64_t)nleaves, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
+        });
+        for (int l = L - 1; l >= 0; --l) {
+            int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+            if (b1 > b0)
+                timer.run(kM2M, [&] {
+                    m2m_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), 8 * NC * sizeof(T), stream>>>(
+                        dp, b0, b1, m, m2m_tab.as<T>(), M.as<T>());
+                });
+        }
+        // downward: for l = 2..L: L2L, M2L, P2L
+        for (int l = 2; l <= L; ++l) {
+            int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+            int64_t p0 = plan.level_start[l - 1], p1 = plan.level_start[l];
+            if (l >= 3)
+                timer.run(kL2L, [&] {
+                    l2l_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), NC * sizeof(T), stream>>>(
+                        dp, b0, b1, m, l2l_tab.as<T>(), Lc.as<T>());
+                });
+            timer.run(kM2L, [&] {
+                m2l_group_kernel<P, T><<<(unsigned)(p1 - p0), round32(NC), 8 * NC * sizeof(T), stream>>>(
+                    dp, p0, p1, m, m2l_tab.as<T>(), M.as<T>(), Lc.as<T>());
+            });
+            timer.run(kP2L, [&] {
+                expand_kernel<P, T, true><<<(unsigned)(b1 - b0), 32, exp_smem, stream>>>(
+                    dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
+            });
+        }
+        // leaves: L2P + M2P, then P2P with the output pass
+        if (nleaves) {
+            if (gradients) {
+                timer.run(kFar, [&] {
+                    leaf_far_kernel<P, T, true><<<(unsigned)nleaves, 64, NC * sizeof(T), stream>>>(
+                        dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+                });
+                timer.run(kP2P, [&] {
+                    p2p_kernel<T, true, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
+                        dp, m, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(), far_g.as<double>(),
+                        d_phi, d_grad);
+                });
+            } else {
+                timer.run(kFar, [&] {
+                    leaf_far_kernel<P, T, false><<<(unsigned)nleaves, 64, NC * sizeof(T), stream>>>(
+                        dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+                });
+                timer.run(kP2P, [&] {
+                    p2p_kernel<T, false, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
+                        dp, m, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(), nullptr, d_phi,
+                        nullptr);
+                });
+            }
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+};
+
+template <typename T>
+std::unique_ptr<EvaluatorBase> make_evaluator(int p, const Plan& pl, const std::vector<double>& m2l,
+                                              const std::vector<double>& m2m, const std::vector<double>& l2l,
+                                              cudaStream_t s, int m, bool grad, const std::vector<double>& us,
+                                              const std::vector<double>& ut, size_t* bytes) {
+#define FMMB_CASE(PP)                                                                    \
+    case PP: {                                                                           \
+        auto e = std::make_unique<Evaluator<PP, T>>(pl, m2l, m2m, l2l, s, m, grad, us, ut); \
+        *bytes = e->device_bytes();                                                      \
+        return e;                                                                        \
+    }
+    switch (p) {
+        FMMB_CASE(3)
+        FMMB_CASE(6)
+        FMMB_CASE(8)
+        default:
+            throw Failure(FMMGPU_UNSUPPORTED, "expansion order " + std::to_string(p) + " is not compiled in (3, 6, 8)");
+    }
+#undef FMMB_CASE
+}
+
+}  // namespace fmmb
+
+// ----------------------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------------------
+using namespace fmmb;
+
+struct fmmgpu_fmm {
+    fmmgpu_settings settings;
+    Plan plan;
+    std::vector<double> m2l, m2m, l2l;
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<EvaluatorBase> eval;
+    DevBuf d_charges, d_phi, d_grad;
+    size_t device_bytes = 0;
+    int64_t near_pairs = 0;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return FMMGPU_OK;
+    } catch (const Failure& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return FMMGPU_INVALID_ARGUMENT;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return FMMGPU_INVALID_ARGUMENT;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void fmmgpu_default_settings(fmmgpu_settings* s) {
+    s->p = 6;
+    s->precision = FMMGPU_PRECISION_F64;
+    s->gradients = 0;
+    s->vectors = 1;
+    s->max_points_per_leaf = 64;
+    s->max_level = 16;
+    s->device = 0;
+}
+
+namespace {
+
+// Host part of a build: plan, tables, leaf-scaled coordinates (no device work).
+std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
+                                       const double* tgt, std::vector<double>& us, std::vector<double>& ut) {
+    if (!settings) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+    const fmmgpu_settings& s = *settings;
+    if (s.p < 0 || s.vectors < 1 || s.max_points_per_leaf < 1 || s.max_level < 0 || s.max_level > 16)
+        throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid settings");
+    if (s.precision != FMMGPU_PRECISION_F64 && s.precision != FMMGPU_PRECISION_MIXED)
+        throw Failure(FMMGPU_UNSUPPORTED, "unknown precision");
+    if ((ns && !src) || (nt && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
+    auto f = std::make_unique<fmmgpu_fmm>();
+    f->settings = s;
+    f->plan = build_plan(ns, src, nt, tgt, s.max_level, s.max_points_per_leaf);
+    build_m2l_tables(s.p, f->m2l);
+    build_m2m_tables(s.p, f->m2m);
+    build_l2l_tables(s.p, f->l2l);
+    const Plan& P = f->plan;
+    // leaf-scaled coordinates in leaf order (CONVENTIONS 3.13)
+    us.assign(3 * ns, 0.0);
+    ut.assign(3 * nt, 0.0);
+    for (size_t j = 0; j < P.nleaves(); ++j) {
+        int b = P.leaf_box[j];
+        for (int64_t a = P.src_start[j]; a < P.src_start[j + 1]; ++a) {
+            int64_t i = P.src_perm[a];
+            for (int k = 0; k < 3; ++k)
+                us[3 * a + k] = leaf_coordinate(src[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
+        }
+        for (int64_t a = P.tgt_start[j]; a < P.tgt_start[j + 1]; ++a) {
+            int64_t i = P.tgt_perm[a];
+            for (int k = 0; k < 3; ++k)
+                ut[3 * a + k] = leaf_coordinate(tgt[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
+        }
+    }
+    for (size_t j = 0; j < P.nleaves(); ++j) {
+        int64_t nt_j = P.tgt_start[j + 1] - P.tgt_start[j];
+        for (int64_t e = P.near.row[j]; e < P.near.row[j + 1]; ++e) {
+            int sj = P.near.col[e];
+            f->near_pairs += nt_j * (P.src_start[sj + 1] - P.src_start[sj]);
+        }
+    }
+    return f;
+}
+
+}  // namespace
+
+int fmmgpu_plan_build(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
+                      const double* tgt, fmmgpu_fmm** out) {
+    return guarded([&] {
+        if (!out) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        std::vector<double> us, ut;
+        auto f = build_host(settings, ns, src, nt, tgt, us, ut);
+        *out = f.release();
+    });
+}
+
+int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
+                     const double* tgt, fmmgpu_fmm** out) {
+    return guarded([&] {
+        if (!out) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            throw Failure(FMMGPU_NO_DEVICE, "no CUDA device is visible");
+        }
+        std::vector<double> us, ut;
+        auto f = build_host(settings, ns, src, nt, tgt, us, ut);
+        const fmmgpu_settings& s = f->settings;
+        CUDA_TRY(cudaSetDevice(s.device));
+        const Plan& P = f->plan;
+        CUDA_TRY(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+        size_t bytes = 0;
+        if (s.precision == FMMGPU_PRECISION_F64)
+            f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0,
+                                             us, ut, &bytes);
+        else
+            f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0,
+                                            us, ut, &bytes);
+        f->d_charges.alloc(sizeof(double) * (size_t)s.vectors * (ns + 1));
+        f->d_phi.alloc(sizeof(double) * (size_t)s.vectors * (nt + 1));
+        if (s.gradients) f->d_grad.alloc(sizeof(double) * 3 * (size_t)s.vectors * (nt + 1));
+        f->device_bytes = bytes + f->d_charges.bytes + f->d_phi.bytes + f->d_grad.bytes;
+        CUDA_TRY(cudaDeviceSynchronize());
+        *out = f.release();
+    });
+}
+
+int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* f, const double* charges, double* potential, double* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        f->eval->evaluate(charges, potential, f->settings.gradients ? gradient : nullptr);
+    });
+}
+
+int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential, double* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors;
+        const size_t ns = f->plan.src_perm.size(), nt = f->plan.tgt_perm.size();
+        CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, f->stream));
+        f->eval->evaluate(f->d_charges.as<double>(), f->d_phi.as<double>(),
+                          f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        CUDA_TRY(cudaMemcpyAsync(potential, f->d_phi.ptr, sizeof(double) * m * nt, cudaMemcpyDeviceToHost, f->stream));
+        if (f->settings.gradients)
+            CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
+                                     f->stream));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+    });
+}
+
+void* fmmgpu_fmm_stream(fmmgpu_fmm* f) { return f ? (void*)f->stream : nullptr; }
+
+int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* f, int on) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        f->eval->timer.on = on != 0;
+    });
+}
+
+int fmmgpu_fmm_kind_times(fmmgpu_fmm* f, double* ms) {
+    return guarded([&] {
+        if (!f || !f->eval || !ms) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        f->eval->timer.collect();
+        for (int k = 0; k < kKinds; ++k) ms[k] = f->eval->timer.ms[k];
+    });
+}
+
+int fmmgpu_fmm_synchronize(fmmgpu_fmm* f) {
+    return guarded([&] {
+        if (!f) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        CUDA_TRY(cudaGetLastError());
+    });
+}
+
+int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
+    return guarded([&] {
+        if (!f || !info) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        const Plan& P = f->plan;
+        info->nlevels = P.nlevels;
+        info->nboxes = (int64_t)P.nboxes();
+        info->nleaves = (int64_t)P.nleaves();
+        info->nsources = (int64_t)P.src_perm.size();
+        info->ntargets = (int64_t)P.tgt_perm.size();
+        info->near_pairs = f->near_pairs;
+        info->v_pairs = (int64_t)P.v.nnz();
+        info->w_pairs = (int64_t)P.w.nnz();
+        info->x_pairs = (int64_t)P.x.nnz();
+        info->device_bytes = (int64_t)f->device_bytes;
+    });
+}
+
+void fmmgpu_fmm_destroy(fmmgpu_fmm* f) {
+    if (!f) return;
+    if (f->eval || f->stream) cudaSetDevice(f->settings.device);
+    if (f->stream) cudaStreamSynchronize(f->stream);
+    f->eval.reset();
+    f->d_charges.alloc(0);
+    f->d_phi.alloc(0);
+    f->d_grad.alloc(0);
+    if (f->stream) cudaStreamDestroy(f->stream);
+    delete f;
+}
+
+int fmmgpu_fmm_boxes(const fmmgpu_fmm* f, uint64_t* keys, uint8_t* is_leaf) {
+    return guarded([&] {
+        if (!f) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        const Plan& P = f->plan;
+        for (size_t b = 0; b < P.nboxes(); ++b) {
+            if (keys) keys[b] = P.key[b];
+            if (is_leaf) is_leaf[b] = P.box_leaf[b] >= 0;
+        }
+    });
+}
+
+int64_t fmmgpu_fmm_list(const fmmgpu_fmm* f, int kind, int64_t row, uint64_t* keys, int64_t cap) {
+    if (!f) return -1;
+    const Plan& P = f->plan;
+    const Csr* c = kind == 0 ? &P.near : kind == 1 ? &P.v : kind == 2 ? &P.w : kind == 3 ? &P.x : nullptr;
+    if (!c || row < 0 || row + 1 >= (int64_t)c->row.size()) return -1;
+    int64_t n = c->row[row + 1] - c->row[row];
+    for (int64_t e = 0; e < n && e < cap; ++e) {
+        int32_t col = c->col[c->row[row] + e];
+        int32_t box = (kind == 0 || kind == 3) ? P.leaf_box[col] : col;
+        keys[e] = P.key[box];
+    }
+    return n;
+}
+
+int fmmgpu_fmm_tables(const fmmgpu_fmm* f, double* m2l, double* m2m, double* l2l) {
+    return guarded([&] {
+        if (!f) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (m2l) std::memcpy(m2l, f->m2l.data(), f->m2l.size() * sizeof(double));
+        if (m2m) std::memcpy(m2m, f->m2m.data(), f->m2m.size() * sizeof(double));
+        if (l2l) std::memcpy(l2l, f->l2l.data(), f->l2l.size() * sizeof(double));
+    });
+}
+
+const char* fmmgpu_status_string(int s) {
+    switch (s) {
+        case FMMGPU_OK: return "ok";
+        case FMMGPU_INVALID_ARGUMENT: return "invalid argument";
+        case FMMGPU_UNSUPPORTED: return "unsupported";
+        case FMMGPU_DEVICE_MEMORY: return "device memory";
+        case FMMGPU_DEVICE_ERROR: return "device error";
+        case FMMGPU_NO_DEVICE: return "no device";
+        default: return "unknown status";
+    }
+}
+
+const char* fmmgpu_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,604 @@
+// Device kernels of the FMM evaluation passes (one rank, one GPU).
+//
+// Data in HBM (all level-major, see plan.hpp):
+//   multipoles / locals : [box][vector][(p+1)^2]            (T)
+//   source points       : xyz as T4 (w unused) + charges [vector][point]  (leaf order)
+//   target points       : xyz as T4                                       (leaf order)
+//   far-field partials  : phi [vector][target], grad [vector][target][3]  (f64)
+//   output              : caller order, phi [vector][target], grad [...][3] (f64)
+// Every kernel adds into its output in a fixed order per output value, with no atomics,
+// so two evaluations are bit-identical.
+#pragma once
+
+#include <cstdint>
+
+#include "harmonics.cuh"
+
+namespace fmmb {
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<double> {
+    using type = double4;
+};
+template <>
+struct Vec4<float> {
+    using type = float4;
+};
+
+struct DevPlan {
+    int nlevels;
+    double side;
+    const int32_t* level;      // per box
+    const uint32_t* idx;       // 3 per box
+    const int32_t* parent;
+    const int32_t* child_first;
+    const int32_t* box_leaf;
+    const int64_t* src_below;
+    const int64_t* tgt_below;
+    const int32_t* leaf_box;
+    const int64_t* src_start;
+    const int64_t* tgt_start;
+    const int64_t* tgt_perm;
+    const int64_t* src_perm;
+    const int64_t *near_row, *w_row, *x_row, *v_row;
+    const int32_t *near_col, *w_col, *x_col, *v_col, *v_off;
+    int64_t nsrc, ntgt;
+};
+
+// relative frame of box s seen from box t (CONVENTIONS 3.13 "Relative frames"):
+// c = (C_L(s) - C_L(t)) 2^(l_t - L), r = 2^(l_t - l_s); exact in f32 and f64.
+template <typename T>
+__device__ __forceinline__ void rel_frame(const DevPlan& P, int s, int t, T c[3], T& r) {
+    int ls = P.level[s], lt = P.level[t];
+    int L = ls > lt ? ls : lt;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        long long Cs = (2LL * P.idx[3 * s + k] + 1) << (L - ls);
+        long long Ct = (2LL * P.idx[3 * t + k] + 1) << (L - lt);
+        c[k] = (T)ldexp((double)(Cs - Ct), lt - L);
+    }
+    r = (T)ldexp(1.0, lt - ls);
+}
+
+// ---------------------------------------------------------------------------------
+// Charge load: caller-order charges (m per point, point-major) -> leaf order [v][i].
+// ---------------------------------------------------------------------------------
+template <typename T>
+__global__ void charge_load_kernel(const double* __restrict__ q_caller, const int64_t* __restrict__ perm,
+                                   int64_t n, int m, T* __restrict__ q_leaf) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t c = perm[i];
+    for (int v = 0; v < m; ++v) q_leaf[(int64_t)v * n + i] = (T)q_caller[c * m + v];
+}
+
+// ---------------------------------------------------------------------------------
+// P2M (rows = leaves, source = the leaf itself, unit frame) and P2L (rows = boxes,
+// sources = X-list leaves, frame (c(t|s), r(t|s))): one warp per row.  Each lane forms
+// the harmonics of one source and writes conj(X) into shared memory; lanes then sum
+// the 32 sources of a chunk per coefficient in source order.
+//   multipole: M_n^m += q conj R_n^m(u);  local: L_n^m += q conj I_n^m((u - c)/r)
+// ---------------------------------------------------------------------------------
+template <int P, typename T, bool IRREG>
+__global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
+                                                    int m, const typename Vec4<T>::type* __restrict__ spos,
+                                                    const T* __restrict__ sq, T* __restrict__ out) {
+    constexpr int NC = nc_of(P);
+    extern __shared__ unsigned char smem_raw[];
+    T* S = reinterpret_cast<T*>(smem_raw);  // [NC][32]
+    T* Q = S + NC * 32;                     // [m][32]
+    const int lane = threadIdx.x;
+    const int64_t row = row_begin + blockIdx.x;
+    if (row >= row_end) return;
+    int box, nent;
+    int64_t ent0;
+    if (!IRREG) {  // row = leaf
+        box = plan.leaf_box[row];
+        nent = 1;
+        ent0 = 0;
+        if (plan.src_below[box] == 0) return;
+    } else {  // row = box
+        box = (int)row;
+        ent0 = plan.x_row[row];
+        nent = (int)(plan.x_row[row + 1] - ent0);
+        if (nent == 0) return;
+    }
+    T* outb = out + (int64_t)box * m * NC;
+    bool first = true;
+    for (int e = 0; e < nent; ++e) {
+        int sleaf = IRREG ? plan.x_col[ent0 + e] : (int)row;
+        T fc[3] = {T(0), T(0), T(0)};
+        T fr = T(1);
+        if (IRREG) rel_frame<T>(plan, box, plan.leaf_box[sleaf], fc, fr);  // (c(t|s), r(t|s))
+        T finv = T(1) / fr;
+        int64_t s0 = plan.src_start[sleaf], s1 = plan.src_start[sleaf + 1];
+        for (int64_t cb = s0; cb < s1; cb += 32) {
+            int64_t si = cb + lane;
+            bool valid = si < s1;
+            T x = T(0), y = T(0), z = T(1);
+            if (valid) {
+                auto p4 = spos[si];
+                x = (p4.x - fc[0]) * finv;
+                y = (p4.y - fc[1]) * finv;
+                z = (p4.z - fc[2]) * finv;
+            }
+            for (int v = 0; v < m; ++v) Q[v * 32 + lane] = valid ? sq[(int64_t)v * plan.nsrc + si] : T(0);
+            if (!IRREG) {
+                RegularRows<P, T> h;
+                h.init(x, y, z);
+#pragma unroll
+                for (int n = 0; n <= P; ++n) {
+                    h.step(n);
+#pragma unroll
+                    for (int mm = 0; mm <= n; ++mm) {
+                        S[slot(n, mm) * 32 + lane] = valid ? h.cre[mm] : T(0);
+                        if (mm) S[slot(n, -mm) * 32 + lane] = valid ? -h.cim[mm] : T(0);
+                    }
+                }
+            } else {
+                IrregularRows<P, T> h;
+                T r2 = x * x + y * y + z * z;
+                h.init(x, y, z, valid ? T(1) / sqrt(r2) : T(0));
+#pragma unroll
+                for (int n = 0; n <= P; ++n) {
+                    h.step(n);
+#pragma unroll
+                    for (int mm = 0; mm <= n; ++mm) {
+                        S[slot(n, mm) * 32 + lane] = valid ? h.cre[mm] : T(0);
+                        if (mm) S[slot(n, -mm) * 32 + lane] = valid ? -h.cim[mm] : T(0);
+                    }
+                }
+            }
+            __syncwarp();
+            int cnt = (int)((s1 - cb) < 32 ? (s1 - cb) : 32);
+            for (int v = 0; v < m; ++v)
+                for (int c = lane; c < NC; c += 32) {
+                    T acc = T(0);
+                    for (int j = 0; j < cnt; ++j) acc += Q[v * 32 + j] * S[c * 32 + j];
+                    T* o = outb + (int64_t)v * NC + c;
+                    if (first && !IRREG) *o = acc;
+                    else *o += acc;
+                }
+            first = false;
+            __syncwarp();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// M2M on one level: parent (level l) = sum over children by octant of T_o * M_child.
+// Block per parent; thread per output slot.  Parents with no source below are skipped
+// (their multipole stays zero and no list names them).
+// ---------------------------------------------------------------------------------
+template <int P, typename T>
+__global__ void m2m_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, const T* __restrict__ tab,
+                           T* __restrict__ M) {
+    constexpr int NC = nc_of(P);
+    extern __shared__ unsigned char smem_raw[];
+    T* Mc = reinterpret_cast<T*>(smem_raw);  // [8][NC]
+    int64_t b = b0 + blockIdx.x;
+    if (b >= b1) return;
+    int c0 = plan.child_first[b];
+    if (c0 < 0 || plan.src_below[b] == 0) return;
+    for (int v = 0; v < m; ++v) {
+        for (int t = threadIdx.x; t < 8 * NC; t += blockDim.x) {
+            int o = t / NC, k = t % NC;
+            Mc[t] = plan.src_below[c0 + o] ? M[((int64_t)(c0 + o) * m + v) * NC + k] : T(0);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+            T acc = T(0);
+            for (int o = 0; o < 8; ++o) {
+                if (!plan.src_below[c0 + o]) continue;
+                const T* A = tab + (int64_t)o * NC * NC + i;
+                const T* x = Mc + o * NC;
+#pragma unroll 7
+                for (int k = 0; k < NC; ++k) acc += A[(int64_t)k * NC] * x[k];
+            }
+            M[((int64_t)b * m + v) * NC + i] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// L2L on one level: child (level l) += T_o * L_parent.  Block per child box.
+// ---------------------------------------------------------------------------------
+template <int P, typename T>
+__global__ void l2l_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, const T* __restrict__ tab,
+                           T* __restrict__ Lc) {
+    constexpr int NC = nc_of(P);
+    extern __shared__ unsigned char smem_raw[];
+    T* Lp = reinterpret_cast<T*>(smem_raw);  // [NC]
+    int64_t b = b0 + blockIdx.x;
+    if (b >= b1) return;
+    if (plan.tgt_below[b] == 0) return;
+    int par = plan.parent[b];
+    int o = (int)(((plan.idx[3 * b] & 1) << 2) | ((plan.idx[3 * b + 1] & 1) << 1) | (plan.idx[3 * b + 2] & 1));
+    const T* A0 = tab + (int64_t)o * NC * NC;
+    for (int v = 0; v < m; ++v) {
+        for (int k = threadIdx.x; k < NC; k += blockDim.x) Lp[k] = Lc[((int64_t)par * m + v) * NC + k];
+        __syncthreads();
+        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+            T acc = T(0);
+#pragma unroll 7
+            for (int k = 0; k < NC; ++k) acc += A0[(int64_t)k * NC + i] * Lp[k];
+            Lc[((int64_t)b * m + v) * NC + i] += acc;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Dense M2L on one level, f64 SIMT form: block per parent; its 8 children are the
+// targets.  The children's V rows (sorted by offset index) are merged, so every table
+// A_d is read once per parent and applied to all children that have offset d; each
+// child's local receives its V-list terms in offset-index order.
+// ---------------------------------------------------------------------------------
+template <int P, typename T>
+__global__ void m2l_group_kernel(DevPlan plan, int64_t p0, int64_t p1, int m, const T* __restrict__ tab,
+                                 const T* __restrict__ M, T* __restrict__ Lc) {
+    constexpr int NC = nc_of(P);
+    extern __shared__ unsigned char smem_raw[];
+    T* Ms = reinterpret_cast<T*>(smem_raw);  // [8][NC]
+    __shared__ int64_t ptr[8], end[8];
+    __shared__ int src[8];
+    __shared__ int cur_d;
+    int64_t pb = p0 + blockIdx.x;
+    if (pb >= p1) return;
+    int c0 = plan.child_first[pb];
+    if (c0 < 0 || plan.tgt_below[pb] == 0) return;
+    for (int v = 0; v < m; ++v) {
+        if (threadIdx.x < 8) {
+            ptr[threadIdx.x] = plan.v_row[c0 + threadIdx.x];
+            end[threadIdx.x] = plan.v_row[c0 + threadIdx.x + 1];
+        }
+        __syncthreads();
+        T acc[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] = T(0);
+        for (;;) {
+            if (threadIdx.x == 0) {
+                int d = 1 << 30;
+                for (int c = 0; c < 8; ++c)
+                    if (ptr[c] < end[c] && plan.v_off[ptr[c]] < d) d = plan.v_off[ptr[c]];
+                cur_d = d;
+                for (int c = 0; c < 8; ++c) {
+                    if (ptr[c] < end[c] && plan.v_off[ptr[c]] == d) {
+                        src[c] = plan.v_col[ptr[c]];
+                        ptr[c]++;
+                    } else {
+                        src[c] = -1;
+                    }
+                }
+            }
+            __syncthreads();
+            int d = cur_d;
+            if (d == (1 << 30)) break;
+            for (int t = threadIdx.x; t < 8 * NC; t += blockDim.x) {
+                int c = t / NC, k = t % NC;
+                Ms[t] = src[c] >= 0 ? M[((int64_t)src[c] * m + v) * NC + k] : T(0);
+            }
+            __syncthreads();
+            const T* A = tab + (int64_t)d * NC * NC;
+            const int i = threadIdx.x;  // blockDim.x >= NC
+            if (i < NC) {
+                for (int k = 0; k < NC; ++k) {
+                    T a = A[(int64_t)k * NC + i];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) acc[c] += a * Ms[c * NC + k];
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x < NC) {
+            for (int c = 0; c < 8; ++c)
+                if (plan.tgt_below[c0 + c]) Lc[((int64_t)(c0 + c) * m + v) * NC + threadIdx.x] += acc[c];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// L2P (own local) then M2P (W list, by box index) for every target of a leaf.
+// Gradients by the ladder identities, contracted with shifted coefficients:
+//   (d/dx - i d/dy) phi = sum L_{k+1}^{mu+1} R_k^mu - conj(sum L_{k+1}^{mu-1} R_k^mu)
+//   d/dz phi = sum w_mu Re(L_{k+1}^mu R_k^mu)          (L2P; M2P uses M_{k-1}, sign -)
+// Results (phi_hat, g_hat in the leaf's units) go to the f64 far-field partials.
+// ---------------------------------------------------------------------------------
+template <int P, typename T, bool GRAD>
+__device__ __forceinline__ void l2p_eval(const T* L, T x, T y, T z, T& phi, T& gx, T& gy, T& gz) {
+    RegularRows<P, T> h;
+    h.init(x, y, z);
+    T f = T(0), dz = T(0), are = T(0), aim = T(0);
+#pragma unroll
+    for (int k = 0; k <= P; ++k) {
+        h.step(k);
+#pragma unroll
+        for (int mu = 0; mu <= k; ++mu) {
+            T w = mu ? T(2) : T(1);
+            Cx<T> c = coef_at(L, k, mu);
+            f += w * (c.re * h.cre[mu] - c.im * h.cim[mu]);
+            if (GRAD && k < P) {
+                Cx<T> c1 = coef_at(L, k + 1, mu);
+                dz += w * (c1.re * h.cre[mu] - c1.im * h.cim[mu]);
+                Cx<T> up = coef_at(L, k + 1, mu + 1);
+                are += up.re * h.cre[mu] - up.im * h.cim[mu];
+                aim += up.re * h.cim[mu] + up.im * h.cre[mu];
+                if (mu >= 1) {
+                    Cx<T> dn = coef_at(L, k + 1, mu - 1);
+                    are -= dn.re * h.cre[mu] - dn.im * h.cim[mu];
+                    aim += dn.re * h.cim[mu] + dn.im * h.cre[mu];  // minus conj
+                }
+            }
+        }
+    }
+    phi = f;
+    gx = are;
+    gy = -aim;
+    gz = dz;
+}
+
+template <int P, typename T, bool GRAD>
+__device__ __forceinline__ void m2p_eval(const T* M, T x, T y, T z, T& phi, T& gx, T& gy, T& gz) {
+    constexpr int KMAX = GRAD ? P + 1 : P;
+    IrregularRows<P, T> h;
+    T r2 = x * x + y * y + z * z;
+    h.init(x, y, z, T(1) / sqrt(r2));
+    T f = T(0), dz = T(0), are = T(0), aim = T(0);
+#pragma unroll
+    for (int k = 0; k <= KMAX; ++k) {
+        h.step(k);
+#pragma unroll
+        for (int mu = 0; mu <= k; ++mu) {
+            T w = mu ? T(2) : T(1);
+            if (k <= P) {
+                Cx<T> c = coef_at(M, k, mu);
+                f += w * (c.re * h.cre[mu] - c.im * h.cim[mu]);
+            }
+            if (GRAD && k >= 1) {
+                Cx<T> c1 = coef_at(M, k - 1, mu);
+                dz -= w * (c1.re * h.cre[mu] - c1.im * h.cim[mu]);
+                if (mu <= k - 2) {
+                    Cx<T> up = coef_at(M, k - 1, mu + 1);
+                    are += up.re * h.cre[mu] - up.im * h.cim[mu];
+                    aim += up.re * h.cim[mu] + up.im * h.cre[mu];
+                }
+                if (mu >= 1) {
+                    Cx<T> dn = coef_at(M, k - 1, mu - 1);
+                    are -= dn.re * h.cre[mu] - dn.im * h.cim[mu];
+                    aim += dn.re * h.cim[mu] + dn.im * h.cre[mu];
+                }
+            }
+        }
+    }
+    phi = f;
+    gx = are;
+    gy = -aim;
+    gz = dz;
+}
+
+template <int P, typename T, bool GRAD>
+__global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int m,
+                                                      const typename Vec4<T>::type* __restrict__ tpos,
+                                                      const T* __restrict__ M, const T* __restrict__ Lc,
+                                                      double* __restrict__ far_phi, double* __restrict__ far_g) {
+    constexpr int NC = nc_of(P);
+    extern __shared__ unsigned char smem_raw[];
+    T* C = reinterpret_cast<T*>(smem_raw);  // [NC]
+    const int leaf = blockIdx.x;
+    const int box = plan.leaf_box[leaf];
+    const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
+    if (t1 == t0) return;
+    const int64_t w0 = plan.w_row[leaf], w1 = plan.w_row[leaf + 1];
+    const int64_t nt = plan.ntgt;
+    for (int v = 0; v < m; ++v) {
+        for (int64_t tb = t0; tb < t1; tb += blockDim.x) {
+            int64_t t = tb + threadIdx.x;
+            bool valid = t < t1;
+            T ux = T(0), uy = T(0), uz = T(0);
+            if (valid) {
+                auto p4 = tpos[t];
+                ux = p4.x;
+                uy = p4.y;
+                uz = p4.z;
+            }
+            double fphi = 0.0, fg[3] = {0.0, 0.0, 0.0};
+            // L2P, unit frame
+            for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Lc[((int64_t)box * m + v) * NC + k];
+            __syncthreads();
+            if (valid) {
+                T ph, gx, gy, gz;
+                l2p_eval<P, T, GRAD>(C, ux, uy, uz, ph, gx, gy, gz);
+                fphi = (double)ph;
+                if (GRAD) {
+                    fg[0] = (double)gx;
+                    fg[1] = (double)gy;
+                    fg[2] = (double)gz;
+                }
+            }
+            __syncthreads();
+            // M2P over the W list, frame (c(s|t), r(s|t))
+            for (int64_t e = w0; e < w1; ++e) {
+                int s = plan.w_col[e];
+                for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = M[((int64_t)s * m + v) * NC + k];
+                __syncthreads();
+                if (valid) {
+                    T c[3], r;
+                    rel_frame<T>(plan, s, box, c, r);
+                    T rinv = T(1) / r;
+                    T ph, gx, gy, gz;
+                    m2p_eval<P, T, GRAD>(C, (ux - c[0]) * rinv, (uy - c[1]) * rinv, (uz - c[2]) * rinv, ph, gx, gy, gz);
+                    fphi += (double)(ph * rinv);
+                    if (GRAD) {
+                        T r2inv = rinv * rinv;
+                        fg[0] += (double)(gx * r2inv);
+                        fg[1] += (double)(gy * r2inv);
+                        fg[2] += (double)(gz * r2inv);
+                    }
+                }
+                __syncthreads();
+            }
+            if (valid) {
+                far_phi[(int64_t)v * nt + t] = fphi;
+                if (GRAD) {
+                    double* g = far_g + ((int64_t)v * nt + t) * 3;
+                    g[0] = fg[0];
+                    g[1] = fg[1];
+                    g[2] = fg[2];
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// P2P + output pass.  Block of 4 warps per target leaf; each warp holds TPL targets
+// per lane and walks every 4th entry of the near row (source leaves by leaf index),
+// staging the mapped sources y = fma(r, u_s, c) (the leaf itself: u_s unchanged) in its
+// own shared memory.  A pair with r2 == 0 adds nothing (select, never a mask
+// multiply).  Warp partials are summed in warp order, added to the far-field partial
+// in f64 and scaled once: phi = phi_hat / (4 pi r_t), g = g_hat / ((4 pi r_t) r_t),
+// then written in caller order.
+// The per-source-leaf partial is kept in T and added into an f64 accumulator per
+// target, so the f32 form sums in f32 only within one source leaf.
+// ---------------------------------------------------------------------------------
+constexpr int kP2pWarps = 4;
+constexpr int kP2pStage = 64;
+
+template <typename T, bool GRAD, int TPL>
+__global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, int m,
+                                                  const typename Vec4<T>::type* __restrict__ spos,
+                                                  const T* __restrict__ sq,
+                                                  const typename Vec4<T>::type* __restrict__ tpos,
+                                                  const double* __restrict__ far_phi, const double* __restrict__ far_g,
+                                                  double* __restrict__ out_phi, double* __restrict__ out_g) {
+    using T4 = typename Vec4<T>::type;
+    __shared__ T4 stage[kP2pWarps][kP2pStage];
+    __shared__ double red[kP2pWarps][32 * TPL][4];
+    const int leaf = blockIdx.x;
+    const int box = plan.leaf_box[leaf];
+    const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
+    if (t1 == t0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t n0 = plan.near_row[leaf], n1 = plan.near_row[leaf + 1];
+    const int64_t nt = plan.ntgt;
+    const double rt = ldexp(plan.side, -(plan.level[box] + 1));
+    const double phi_scale = 4.0 * 3.141592653589793 * rt;
+    const double g_scale = phi_scale * rt;
+    for (int v = 0; v < m; ++v) {
+        for (int64_t tb = t0; tb < t1; tb += 32 * TPL) {
+            T tx[TPL], ty[TPL], tz[TPL];
+            double aphi[TPL], ag[TPL][3];
+#pragma unroll
+            for (int j = 0; j < TPL; ++j) {
+                int64_t t = tb + lane + 32 * j;
+                tx[j] = ty[j] = tz[j] = T(0);
+                if (t < t1) {
+                    T4 p4 = tpos[t];
+                    tx[j] = p4.x;
+                    ty[j] = p4.y;
+                    tz[j] = p4.z;
+                }
+                aphi[j] = 0.0;
+                ag[j][0] = ag[j][1] = ag[j][2] = 0.0;
+            }
+            for (int64_t e = n0 + warp; e < n1; e += kP2pWarps) {
+                int sl = plan.near_col[e];
+                int sbox = plan.leaf_box[sl];
+                T c[3] = {T(0), T(0), T(0)}, r = T(1);
+                bool self = sl == leaf;
+                if (!self) rel_frame<T>(plan, sbox, box, c, r);
+                int64_t s0 = plan.src_start[sl], s1 = plan.src_start[sl + 1];
+                for (int64_t sb = s0; sb < s1; sb += kP2pStage) {
+                    int cnt = (int)((s1 - sb) < kP2pStage ? (s1 - sb) : kP2pStage);
+                    for (int j = lane; j < cnt; j += 32) {
+                        T4 p4 = spos[sb + j];
+                        T4 y;
+                        if (self) {
+                            y.x = p4.x;
+                            y.y = p4.y;
+                            y.z = p4.z;
+                        } else {
+                            y.x = fma(r, p4.x, c[0]);
+                            y.y = fma(r, p4.y, c[1]);
+                            y.z = fma(r, p4.z, c[2]);
+                        }
+                        y.w = sq[(int64_t)v * plan.nsrc + sb + j];
+                        stage[warp][j] = y;
+                    }
+                    __syncwarp();
+                    T pphi[TPL], pg[TPL][3];
+#pragma unroll
+                    for (int j = 0; j < TPL; ++j) pphi[j] = pg[j][0] = pg[j][1] = pg[j][2] = T(0);
+                    for (int s = 0; s < cnt; ++s) {
+                        T4 y = stage[warp][s];
+#pragma unroll
+                        for (int j = 0; j < TPL; ++j) {
+                            T dx = tx[j] - y.x, dy = ty[j] - y.y, dz = tz[j] - y.z;
+                            T r2 = dx * dx + dy * dy + dz * dz;
+                            T rinv = r2 == T(0) ? T(0) : rsqrt(r2);
+                            T qr = y.w * rinv;
+                            pphi[j] += qr;
+                            if (GRAD) {
+                                T qr3 = qr * rinv * rinv;
+                                pg[j][0] -= qr3 * dx;
+                                pg[j][1] -= qr3 * dy;
+                                pg[j][2] -= qr3 * dz;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < TPL; ++j) {
+                        aphi[j] += (double)pphi[j];
+                        if (GRAD) {
+                            ag[j][0] += (double)pg[j][0];
+                            ag[j][1] += (double)pg[j][1];
+                            ag[j][2] += (double)pg[j][2];
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < TPL; ++j) {
+                red[warp][lane + 32 * j][0] = aphi[j];
+                red[warp][lane + 32 * j][1] = ag[j][0];
+                red[warp][lane + 32 * j][2] = ag[j][1];
+                red[warp][lane + 32 * j][3] = ag[j][2];
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < 32 * TPL; j += blockDim.x) {
+                int64_t t = tb + j;
+                if (t >= t1) continue;
+                double ph = far_phi[(int64_t)v * nt + t];
+                double g0 = 0, g1 = 0, g2 = 0;
+                if (GRAD) {
+                    const double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                    g0 = fg[0];
+                    g1 = fg[1];
+                    g2 = fg[2];
+                }
+                for (int w = 0; w < kP2pWarps; ++w) {
+                    ph += red[w][j][0];
+                    g0 += red[w][j][1];
+                    g1 += red[w][j][2];
+                    g2 += red[w][j][3];
+                }
+                int64_t i = plan.tgt_perm[t];
+                out_phi[(int64_t)v * nt + i] = ph / phi_scale;
+                if (GRAD) {
+                    double* o = out_g + ((int64_t)v * nt + i) * 3;
+                    o[0] = g0 / g_scale;
+                    o[1] = g1 / g_scale;
+                    o[2] = g2 / g_scale;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace fmmb

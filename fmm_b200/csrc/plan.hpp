@@ -1,0 +1,84 @@
+// Host-side plan of the B200 FMM evaluator: the octree, the box index, the per-leaf
+// point order and the U/V/W/X interaction lists, flattened into arrays that are
+// uploaded once and read by the device kernels.
+//
+// Conventions follow the reference (tbetcke/fmm):
+//  - Morton keys: octree/src/morton.rs (3 interleaved index bits per level, x highest,
+//    << 15, level in the low 15 bits); child octant o = 4x + 2y + z.
+//  - boxes are numbered level-major, key order within a level; leaves likewise
+//    (the leaf numbering of fmm-plan/src/index.rs, one rank).
+//  - list rule: fmm-plan/src/interaction_manager.rs:15-27; rows are sorted as the
+//    accumulation rule of fmm-plan/src/operator.rs:34-45 orders them (V by offset
+//    index, W by box index, X and near by source leaf).
+//  - boxes with no source below them are left out of every source-side list and
+//    boxes with no target below them get empty target rows (their contributions
+//    are exact zeros in the reference).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fmmb {
+
+constexpr int kDeepest = 16;
+
+struct Csr {
+    std::vector<int64_t> row;  // nrows + 1
+    std::vector<int32_t> col;  // entries
+    std::vector<int32_t> aux;  // optional per-entry payload (the offset index for V)
+    size_t nnz() const { return col.size(); }
+};
+
+struct Plan {
+    int nlevels = 0;
+    double lower[3] = {0, 0, 0};
+    double side = 0;
+    double box6[6] = {0, 0, 0, 0, 0, 0};
+
+    // boxes, level-major
+    std::vector<uint64_t> key;
+    std::vector<int32_t> level;          // per box
+    std::vector<uint32_t> idx;           // 3 per box
+    std::vector<int64_t> level_start;    // nlevels + 1
+    std::vector<int32_t> parent;         // -1 for the root
+    std::vector<int32_t> child_first;    // first of 8 consecutive children, -1 for leaves
+    std::vector<int32_t> box_leaf;       // leaf index or -1
+    std::vector<int64_t> src_below, tgt_below;
+
+    // leaves, level-major
+    std::vector<int32_t> leaf_box;
+    std::vector<int64_t> leaf_level_start;  // nlevels + 1
+    std::vector<int64_t> src_start, tgt_start;  // nleaves + 1 (points in leaf order)
+    std::vector<int64_t> src_perm, tgt_perm;    // leaf-order position -> caller index
+    std::vector<int64_t> src_pos_of, tgt_pos_of;  // caller index -> leaf-order position
+
+    // interaction lists (rows: leaves for near/W, boxes for V/X)
+    Csr near;  // source leaves, U-list and the leaf itself, by leaf index
+    Csr w;     // source boxes on level l + 1, by box index
+    Csr x;     // source leaves on level l - 1, by leaf index
+    Csr v;     // source boxes with aux = offset index, by offset index
+
+    size_t nboxes() const { return key.size(); }
+    size_t nleaves() const { return leaf_box.size(); }
+};
+
+// Builds the cubic domain, the tree of the distinct level-16 keys of sources ++ targets
+// (refined while a box holds more than max_keys keys, then 2:1 balanced), the box
+// index, the point order and the lists.  Throws std::runtime_error on bad input.
+Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
+                int max_keys);
+
+// Leaf-scaled coordinate of CONVENTIONS 3.13: fl(fl(fl(x - a) * 2^(l+1)) / w) - (2i + 1).
+double leaf_coordinate(double x, double a, double w, int level, uint32_t index);
+
+// M2L offset index of d = index(target) - index(source) (fmm-tables/src/geometry.rs:90)
+int offset_index(int dx, int dy, int dz);
+
+// Operator tables (column-major, (p+1)^2 x (p+1)^2 each), built in f64 from the direct
+// translations applied to unit vectors (fmm-tables/src/m2l.rs:67-96, octant.rs:150-174).
+void build_m2l_tables(int p, std::vector<double>& out);  // 316 matrices
+void build_m2m_tables(int p, std::vector<double>& out);  // 8
+void build_l2l_tables(int p, std::vector<double>& out);  // 8
+
+}  // namespace fmmb

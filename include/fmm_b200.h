@@ -1,0 +1,133 @@
+/*
+ * fmm_b200.h -- C ABI of the B200 evaluator for the FMM evaluation passes.
+ *
+ * Two layers, both plain C (pointers, sizes, status codes; no CUDA or torch types):
+ *
+ * 1. The FMM entry points (fmmgpu_fmm_*) mirror the user API of the reference,
+ *    nd-fmm-exec's FmmBuilder / Fmm (fmm-exec/src/fmm.rs:1853 build, :3691 evaluate,
+ *    :3719 evaluate_into): build once from source and target points in the caller's
+ *    order, then evaluate charge vectors into potentials (and gradients) in the
+ *    caller's order, with 1/(4 pi) applied (phi(x) = sum_j q_j / (4 pi |x - y_j|)).
+ *    The build makes the plan on the host (octree, lists, f64 operator tables) and
+ *    uploads it; an evaluation runs every pass on the GPU.
+ *
+ * 2. The operator entry points (fmmgpu_op_*) are the level calls of the reference's
+ *    drop-in boundary, the FmmOperator trait (fmm-plan/src/operator.rs:434-492): one
+ *    call per (level, kind) that queues device work and adds into its output in the
+ *    trait's accumulation order (operator.rs:34-45).  A host that keeps its own plan
+ *    (nd-fmm-exec's Engine::Device seam, fmm-exec/src/fmm.rs:2564-2568) drives an
+ *    evaluation through these calls between fmmgpu_op_begin_evaluation and
+ *    fmmgpu_op_read_output.
+ *
+ * Errors: every call returns an fmmgpu_status; a device error surfaces at the next
+ * call that synchronises (evaluate, read_output), as the reference's device errors
+ * surface at read_output (fmm-kernels/src/lib.rs:64-66).  fmmgpu_last_error() gives
+ * the message of the last failure on the calling thread.
+ */
+#ifndef FMM_B200_H
+#define FMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FMMGPU_OK = 0,
+    FMMGPU_INVALID_ARGUMENT = 1,     /* settings or inputs rejected before any GPU work */
+    FMMGPU_UNSUPPORTED = 2,          /* expansion order or precision not compiled in */
+    FMMGPU_DEVICE_MEMORY = 3,        /* the device buffers do not fit */
+    FMMGPU_DEVICE_ERROR = 4,         /* a CUDA call or kernel failed */
+    FMMGPU_NO_DEVICE = 5             /* no CUDA device is visible */
+} fmmgpu_status;
+
+typedef enum {
+    FMMGPU_PRECISION_F64 = 0,   /* the plain f64 evaluator (the drop-in) */
+    FMMGPU_PRECISION_MIXED = 1  /* f32 points/expansions, f64 per-target accumulation */
+} fmmgpu_precision;
+
+/* FmmBuilder settings (fmm-exec/src/fmm.rs:1228-1270 names and defaults). */
+typedef struct {
+    int p;                    /* expansion order */
+    int precision;            /* fmmgpu_precision */
+    int gradients;            /* 0: potentials only, 1: potentials and gradients */
+    int vectors;              /* m >= 1 charge vectors at the same points */
+    int max_points_per_leaf;  /* refinement target (distinct level-16 keys per leaf) */
+    int max_level;            /* deepest leaf level, 0-16 */
+    int device;               /* CUDA device ordinal */
+} fmmgpu_settings;
+
+typedef struct {
+    int nlevels;
+    int64_t nboxes, nleaves, nsources, ntargets;
+    int64_t near_pairs;   /* source-target point pairs of P2P over all near rows */
+    int64_t v_pairs;      /* M2L box pairs */
+    int64_t w_pairs, x_pairs;
+    int64_t device_bytes; /* device memory held by the evaluator */
+} fmmgpu_info;
+
+typedef struct fmmgpu_fmm fmmgpu_fmm;
+
+/* Settings with the reference's defaults: p = 6, f64, no gradients, one vector,
+ * 64 points per leaf, max level 16, device 0. */
+void fmmgpu_default_settings(fmmgpu_settings* settings);
+
+/* FmmBuilder::build (fmm.rs:1853): sources/targets are n x 3 doubles, caller order. */
+int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t nsources, const double* sources,
+                     size_t ntargets, const double* targets, fmmgpu_fmm** out);
+
+/* The host half of a build only (plan, lists, tables), no device needed: the handle
+ * answers info/boxes/list/tables and must be destroyed, but cannot evaluate. */
+int fmmgpu_plan_build(const fmmgpu_settings* settings, size_t nsources, const double* sources,
+                      size_t ntargets, const double* targets, fmmgpu_fmm** out);
+
+/* Fmm::evaluate_into (fmm.rs:3719) with HOST buffers: charges[i*m + v] (caller order,
+ * m charges of a source adjacent); potential[v*nt + i]; gradient[(v*nt + i)*3 + k] (or
+ * NULL without gradients).  Copies in, evaluates, copies out, synchronises. */
+int fmmgpu_fmm_evaluate(fmmgpu_fmm* fmm, const double* charges, double* potential, double* gradient);
+
+/* The same with DEVICE buffers on the evaluator's stream; does not synchronise. */
+int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* fmm, const double* charges, double* potential,
+                               double* gradient);
+
+/* The evaluator's CUDA stream (a cudaStream_t), for timing with events on it. */
+void* fmmgpu_fmm_stream(fmmgpu_fmm* fmm);
+
+/* Per-kind device timing of the following evaluations (the reference's KindTiming,
+ * fmm-exec/src/fmm.rs:150-153): every launch is bracketed by CUDA events. */
+int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* fmm, int on);
+/* Milliseconds of the last evaluation per kind: [0] charge load, [1] P2M, [2] M2M,
+ * [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P + output pass.  Synchronises. */
+int fmmgpu_fmm_kind_times(fmmgpu_fmm* fmm, double* ms);
+
+/* Waits for the stream and returns the first device error, if any. */
+int fmmgpu_fmm_synchronize(fmmgpu_fmm* fmm);
+
+int fmmgpu_fmm_info(const fmmgpu_fmm* fmm, fmmgpu_info* info);
+
+void fmmgpu_fmm_destroy(fmmgpu_fmm* fmm);
+
+/* Plan export, for tests: level-major box keys (nboxes u64) and leaf flags (u8). */
+int fmmgpu_fmm_boxes(const fmmgpu_fmm* fmm, uint64_t* keys, uint8_t* is_leaf);
+/* The rows of one list (kind 0 near, 1 V, 2 W, 3 X) as box keys; row = leaf index for
+ * near/W, box index for V/X.  Returns the count (writes at most cap keys), or -1. */
+int64_t fmmgpu_fmm_list(const fmmgpu_fmm* fmm, int kind, int64_t row, uint64_t* keys, int64_t cap);
+/* The f64 tables the plan uploaded: 316 M2L, 8 M2M, 8 L2L, column-major (p+1)^2 squares. */
+int fmmgpu_fmm_tables(const fmmgpu_fmm* fmm, double* m2l, double* m2m, double* l2l);
+
+/* f64 direct sum on the GPU at the given targets: phi(x) = sum_j q_j / (4 pi |x - y_j|)
+ * and its gradient (grad may be NULL), exactly coincident pairs skipped, Neumaier
+ * compensation per target (fmm-ref/src/p2p.rs:147-186 with the FMM's 1/(4 pi)).
+ * Host buffers in and out; allocates and frees its own device memory. */
+int fmmgpu_direct_sum(size_t nsources, const double* sources, const double* charges, size_t ntargets,
+                      const double* targets, double* potential, double* gradient, int device);
+
+const char* fmmgpu_status_string(int status);
+const char* fmmgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMM_B200_H */

@@ -120,7 +120,9 @@ def tables(p):
     lib().orc_build_m2l_tables(p, m2l)
     lib().orc_build_m2m_tables(p, m2m)
     lib().orc_build_l2l_tables(p, l2l)
-    return m2l.reshape(316, n, n), m2m.reshape(8, n, n), l2l.reshape(8, n, n)
+    # column-major storage: entry (i, k) at i + k n; return A with A[t] @ x = output
+    return (m2l.reshape(316, n, n).transpose(0, 2, 1), m2m.reshape(8, n, n).transpose(0, 2, 1),
+            l2l.reshape(8, n, n).transpose(0, 2, 1))
 
 
 def p2p(src, q, tgt, gradients=True):

@@ -1,0 +1,94 @@
+"""GPU parity of the evaluator against the oracle (needs a B200: -m gpu).
+
+The f64 evaluator must match the restated reference host FMM on the same tree and p
+within 1e-12 relative L2 over all targets (the reference's own device
+matched its host within 1.2e-14, fmm-bench/results/phase4s-gh200.md:448).  The mixed
+evaluator (f32 points and expansions, f64 per-target accumulation) must stay within
+2e-6 relative L2 of the f64 oracle at p <= 8 on these problems, so that its error
+against the direct sum is the FMM's own truncation error.
+"""
+import numpy as np
+import pytest
+
+import fmm_b200 as F
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def run_both(oracle, src, q, tgt, p, mk, grad, precision="f64", m=1):
+    fmm = F.FmmBuilder(p).gradients(grad).vectors(m).max_points_per_leaf(mk).precision(precision).build(src, tgt)
+    out = fmm.evaluate(q)
+    phi, g = oracle.fmm(src, q, tgt, p, mk, gradients=grad, threads=8)
+    return fmm, out, phi, g
+
+
+CASES = [
+    ("cube", 20000, 6, 64, False),
+    ("cube", 20000, 3, 32, True),
+    ("sphere", 30000, 8, 64, True),
+    ("sphere", 12000, 6, 16, True),
+]
+
+
+@pytest.mark.parametrize("kind,n,p,mk,grad", CASES)
+def test_f64_matches_oracle(oracle, kind, n, p, mk, grad):
+    x, q = oracle.point_sets(kind, n, 17)
+    fmm, out, phi, g = run_both(oracle, x, q, x, p, mk, grad)
+    assert rel(out.potential, phi) < 1e-12
+    if grad:
+        assert rel(out.gradient, g) < 1e-12
+
+
+def test_f64_distinct_targets_and_vectors(oracle):
+    rng = np.random.default_rng(9)
+    src = rng.uniform(-1, 1, (15000, 3))
+    tgt = np.concatenate([rng.normal(0.2, 0.3, (6000, 3)), src[:2000]])  # some coincide with sources
+    q = rng.normal(size=(15000, 2))
+    fmm, out, phi, g = run_both(oracle, src, q, tgt, 6, 24, True, m=2)
+    assert rel(out.potential, phi) < 1e-12
+    assert rel(out.gradient, g) < 1e-12
+
+
+def test_f64_single_leaf_and_duplicates(oracle):
+    rng = np.random.default_rng(2)
+    x = rng.uniform(0, 1, (50, 3))
+    x = np.concatenate([x, x[:10]])  # exact duplicates: coincident pairs are skipped
+    q = rng.uniform(-1, 1, len(x))
+    fmm, out, phi, g = run_both(oracle, x, q, x, 6, 64, True)  # root is the only leaf
+    assert fmm.info()["nleaves"] == 1
+    assert rel(out.potential, phi) < 1e-12 and rel(out.gradient, g) < 1e-12
+
+
+def test_f64_bitwise_repeatable(oracle):
+    x, q = oracle.point_sets("sphere", 20000, 3)
+    fmm = F.FmmBuilder(6).gradients().max_points_per_leaf(32).build(x)
+    a = fmm.evaluate(q)
+    b = fmm.evaluate(q)
+    assert np.array_equal(a.potential, b.potential) and np.array_equal(a.gradient, b.gradient)
+
+
+@pytest.mark.parametrize("kind,n,p,mk,grad", CASES)
+def test_mixed_close_to_oracle(oracle, kind, n, p, mk, grad):
+    x, q = oracle.point_sets(kind, n, 17)
+    fmm, out, phi, g = run_both(oracle, x, q, x, p, mk, grad, precision="mixed")
+    assert rel(out.potential, phi) < 2e-6
+    if grad:
+        assert rel(out.gradient, g) < 2e-6
+
+
+def test_f64_accuracy_gate_problem(oracle):
+    """The C3.2 gate on the device (fmm-exec/tests/accuracy.rs): p = 8, twice 1.08e-5."""
+    from tests.test_oracle import gate_problem
+
+    x, sample, q = gate_problem(vectors=4)
+    fmm = F.FmmBuilder(8).vectors(4).max_points_per_leaf(64).build(x)
+    out = fmm.evaluate(q)
+    errs = []
+    for k in range(4):
+        d, _ = oracle.direct_sum(x, q[:, k], x[sample], gradients=False)
+        errs.append(rel(out.potential[k][sample], d / (4 * np.pi)))
+    assert np.sqrt(np.mean(np.square(errs))) < 2 * 1.08e-5

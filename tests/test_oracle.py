@@ -1,0 +1,158 @@
+"""Pins the oracle to the reference's own known answers (no GPU).
+
+- harmonics against the mpmath fixtures of fmm-math/fixtures/harmonics_{A,B,C}.json
+  (subset committed in tests/golden/harmonics.json by tests/golden/make_golden.py);
+- SplitMix64 seed-0 outputs (fmm-validate/src/rng.rs:58-64);
+- the doc examples of fmm-ref/src/p2p.rs:48-64, fmm-math/src/harmonics.rs:103-112
+  and :150-157, fmm-exec/src/tables.rs:37-44 (monopole through M2L offset 0);
+- the Neumaier example of fmm-ref/src/p2p.rs:466-489;
+- the FMM accuracy gate of fmm-exec/tests/accuracy.rs:72-73,148-260 (relative L2 of
+  phi at 1,000 sampled targets, RMS over eight charge vectors, within twice the
+  single-translation prediction 1.77e-3 at p = 3 and 1.08e-5 at p = 8) on its own
+  problem (N = 1e5 in [-1, 1)^3, seed 0xc32), restated.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "harmonics.json")
+
+
+def _f(a):
+    return np.array([float(v) for v in a])
+
+
+def test_harmonics_match_mpmath_fixtures(oracle):
+    data = json.load(open(GOLDEN))
+    worst = 0.0
+    count = 0
+    for s in data["sets"]:
+        p = s["p"]
+        for fam in ("regular", "irregular"):
+            for rec in s[fam]:
+                x = _f(rec["x"])
+                ref = _f(rec["value"])
+                if "grad" in rec:
+                    f = oracle.regular_grad if fam == "regular" else oracle.irregular_grad
+                    v, g = f(p, x)
+                    rg = np.array([_f(c) for c in rec["grad"]])
+                    # per-degree relative error (orthonormal weighting is not needed at this size)
+                    worst = max(worst, np.abs(g - rg).max() / np.abs(rg).max())
+                else:
+                    v = (oracle.regular if fam == "regular" else oracle.irregular)(p, x)
+                worst = max(worst, np.abs(v - ref).max() / np.abs(ref).max())
+                count += 1
+    assert count >= 28
+    assert worst < 1e-13, worst
+
+
+def test_splitmix64_seed0(oracle):
+    r = oracle.Rng(0)
+    assert [r.next_u64() for _ in range(3)] == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F]
+
+
+def test_p2p_doc_example(oracle):
+    pts = np.array([[0.0, 0.0, 0.0], [3.0, 4.0, 0.0]])
+    q = np.array([2.0, -1.0])
+    phi, g = oracle.p2p(pts, q, pts)
+    assert list(phi) == [-1.0 / 5.0, 2.0 / 5.0]
+    assert list(g[1]) == [-2.0 * 3.0 / 125.0, -2.0 * 4.0 / 125.0, 0.0]
+    d, _ = oracle.direct_sum(pts, q, pts, gradients=False, threads=False)
+    assert list(d) == list(phi)
+
+
+def test_direct_sum_is_compensated(oracle):
+    src = np.array([[1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0], [-1.0, 0, 0]])
+    q = np.array([1.0, 1e100, 1.0, -1e100])
+    o = np.zeros((1, 3))
+    d, _ = oracle.direct_sum(src, q, o, gradients=False, threads=False)
+    p, _ = oracle.p2p(src, q, o, gradients=False)
+    assert d[0] == 2.0 and p[0] == 0.0
+
+
+def test_harmonics_doc_examples(oracle):
+    x, y, z = 0.3, -0.2, 0.5
+    r = oracle.regular(2, [x, y, z])
+    assert (r[3], r[1]) == (x / 2, y / 2)
+    assert abs(r[6] - (2 * z * z - x * x - y * y) / 4) < 1e-15
+    i = oracle.irregular(1, [0.0, 0.0, 2.0])
+    assert list(i) == [0.5, 0.0, 0.25, 0.0]
+
+
+def test_m2l_monopole_offset0(oracle):
+    m2l, _, _ = oracle.tables(2)
+    assert abs(m2l[0][0, 0] - 1.0 / (6.0 * np.sqrt(3.0))) < 1e-15
+
+
+def test_tables_match_direct_operators(oracle):
+    # fmm-tables/src/m2l.rs:26-45: table application equals direct::m2l at the canonical frames
+    p = 3
+    m2l, m2m, l2l = oracle.tables(p)
+    n = (p + 1) ** 2
+    x = 1.0 / (1.0 + np.arange(n))
+    d = (2, -1, 0)
+    idx = oracle.lib().orc_offset_index(*d)
+    out = np.zeros(n)
+    oracle.lib().orc_m2l(p, np.zeros(3), 1.0, 2.0 * np.array(d, dtype=float), 1.0, x, out)
+    assert np.abs(m2l[idx] @ x - out).max() < 1e-15
+    # M2M after P2M equals P2M at the parent (fmm-ref/src/direct.rs doc example)
+    src = np.array([[0.3, 0.1, 0.4], [0.2, 0.45, 0.05]])
+    q = np.array([1.0, -0.5])
+    p = 10
+    n = (p + 1) ** 2
+    child = np.zeros(n)
+    oracle.lib().orc_p2m(p, np.array([0.25, 0.25, 0.25]), 0.25, 2, src, q, 1, child)
+    tr = np.zeros(n)
+    oracle.lib().orc_m2m(p, np.array([0.25, 0.25, 0.25]), 0.25, np.zeros(3), 0.5, child, tr)
+    par = np.zeros(n)
+    oracle.lib().orc_p2m(p, np.zeros(3), 0.5, 2, src, q, 1, par)
+    assert np.abs(tr - par).max() < 1e-14
+
+
+def splitmix_stream(seed, count):
+    """count consecutive SplitMix64 outputs from `seed` (fmm-validate/src/rng.rs:24-45), vectorised."""
+    with np.errstate(over="ignore"):
+        k = np.arange(1, count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + k * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform_range(u64, lo, hi):
+    return lo + (hi - lo) * ((u64 >> np.uint64(11)).astype(np.float64) * (1.0 / float(1 << 53)))
+
+
+def test_splitmix_stream_matches_scalar(oracle):
+    r = oracle.Rng(1234)
+    assert [r.next_u64() for _ in range(5)] == splitmix_stream(1234, 5).tolist()
+
+
+def gate_problem(n=100_000, nsample=1000, vectors=8, seed=0xC32):
+    """The C3.2 gate problem of fmm-exec/tests/accuracy.rs:148-176, restated."""
+    raw = splitmix_stream(seed, 3 * n + nsample)
+    pts = uniform_range(raw[: 3 * n], -1.0, 1.0).reshape(n, 3)
+    order = np.arange(n)
+    for i in range(nsample):
+        j = i + int((int(raw[3 * n + i]) >> 32) * (n - i) >> 32)
+        order[i], order[j] = order[j], order[i]
+    sample = order[:nsample].copy()
+    q = np.stack([uniform_range(splitmix_stream(seed + 1 + k, n), -1.0, 1.0) for k in range(vectors)], axis=1)
+    return pts, sample, q
+
+
+@pytest.mark.parametrize("p,prediction", [(3, 1.77e-3), (8, 1.08e-5)])
+def test_fmm_accuracy_gate(oracle, p, prediction):
+    """fmm-exec/tests/accuracy.rs: RMS over eight charge vectors of the relative L2 error
+    of phi at 1,000 sampled targets, within twice the single-translation prediction."""
+    x, sample, q = gate_problem()
+    phi, _ = oracle.fmm(x, q, x, p, 64, gradients=False, threads=8)
+    errs = []
+    for k in range(q.shape[1]):
+        d, _ = oracle.direct_sum(x, q[:, k], x[sample], gradients=False)
+        d /= 4 * np.pi
+        errs.append(np.linalg.norm(phi[k][sample] - d) / np.linalg.norm(d))
+    rms = float(np.sqrt(np.mean(np.square(errs))))
+    assert rms < 2.0 * prediction, (rms, errs)

@@ -1,0 +1,151 @@
+"""The product's host plan (tree, lists, tables) against the oracle (no GPU).
+
+The tree must equal the oracle's restatement of the reference's refinement and 2:1
+balance key for key; every list row must equal the oracle's brute-force list rule
+(fmm-plan/src/interaction_manager.rs:15-27) with boxes that hold no source removed
+(their contributions are exact zeros), in the accumulation order of
+fmm-plan/src/operator.rs:34-45; the f64 tables must equal the oracle's tables.
+"""
+import numpy as np
+import pytest
+
+import fmm_b200 as F
+
+LEVEL_MASK = np.uint64(0x7FFF)
+
+
+def _occupied(keys, pts_keys):
+    """Boxes (keys) with at least one level-16 point key below them."""
+    lv = (keys & LEVEL_MASK).astype(np.int64)
+    occ = np.zeros(len(keys), dtype=bool)
+    pk = np.sort(pts_keys)
+    for i, (k, l) in enumerate(zip(keys, lv)):
+        shift = np.uint64(15 + 3 * (16 - l))
+        lo = (k >> shift) << shift
+        hi = lo + (np.uint64(1) << shift)
+        a = np.searchsorted(pk, lo)
+        occ[i] = a < len(pk) and pk[a] < hi
+    return occ
+
+
+def _point_keys(oracle, x):
+    tr = oracle.Tree(x, x, 16, 1 << 30)  # for the domain only
+    del tr
+    lo = x.min(0)
+    hi = x.max(0)
+    diam = hi - lo
+    mean = lo + 0.5 * diam
+    md = diam.max() * (1.0 + 1.0 / 65536)
+    b0 = mean - 0.5 * md
+    b1 = mean + 0.5 * md
+    keys = np.zeros(len(x), dtype=np.uint64)
+    for i, p in enumerate(x):
+        idx = np.minimum(np.floor((p - b0) / (b1 - b0) * 65536).clip(0), 65535).astype(np.uint32)
+        keys[i] = oracle.lib().orc_key_from_index(np.ascontiguousarray(idx), 16)
+    return keys
+
+
+@pytest.mark.parametrize("kind,n,mk", [("cube", 3000, 16), ("sphere", 6000, 24), ("cube", 40000, 64)])
+def test_tree_equals_oracle(oracle, kind, n, mk):
+    x, _ = oracle.point_sets(kind, n, 11)
+    plan = F.FmmBuilder(4).max_points_per_leaf(mk).plan(x)
+    keys, leaf = plan.boxes()
+    tr = oracle.Tree(x, x, 16, mk)
+    assert np.array_equal(keys, tr.keys)
+    assert np.array_equal(leaf, tr.is_leaf)
+
+
+def test_tree_with_distinct_targets(oracle):
+    rng = np.random.default_rng(3)
+    src = rng.uniform(0, 1, (2500, 3))
+    tgt = rng.normal(0.5, 0.1, (1500, 3))
+    plan = F.FmmBuilder(4).max_points_per_leaf(10).plan(src, tgt)
+    keys, leaf = plan.boxes()
+    tr = oracle.Tree(src, tgt, 16, 10)
+    assert np.array_equal(keys, tr.keys) and np.array_equal(leaf, tr.is_leaf)
+
+
+def test_lists_equal_brute_force_rule(oracle):
+    x, _ = oracle.point_sets("sphere", 5000, 5)
+    mk = 20
+    plan = F.FmmBuilder(4).max_points_per_leaf(mk).plan(x)
+    keys, leaf = plan.boxes()
+    tr = oracle.Tree(x, x, 16, mk)
+    occ = _occupied(keys, _point_keys(oracle, x))
+    occ_of = dict(zip(keys.tolist(), occ.tolist()))
+    leaf_ids = np.flatnonzero(leaf)
+    offsets_checked = 0
+    for b in range(len(keys)):
+        is_leaf = bool(leaf[b])
+        # V (kind 1) and X (kind 3) rows by box; near (0) and W (2) rows by leaf index
+        for kind, okind in ((1, 1), (3, 3)):
+            got = plan.list(kind, b)
+            want = [k for k in tr.list(b, okind).tolist() if occ_of[k]] if occ[b] else []
+            if kind == 1:
+                # V rows are ordered by offset index; compare as sets, then check the order
+                assert sorted(got.tolist()) == sorted(want)
+                offs = []
+                for k in got.tolist():
+                    s = keys.tolist().index(k)
+                    d = _index(keys[b]) - _index(keys[s])
+                    offs.append(oracle.lib().orc_offset_index(*[int(t) for t in d]))
+                assert offs == sorted(offs) and min(offs, default=0) >= 0
+                offsets_checked += len(offs)
+            else:
+                assert got.tolist() == sorted(want, key=lambda k: keys.tolist().index(k))
+        if is_leaf:
+            j = int(np.searchsorted(leaf_ids, b))
+            near = plan.list(0, j).tolist()
+            want_u = [k for k in tr.list(b, 0).tolist() if occ_of[k]] if occ[b] else []
+            if occ[b]:
+                want_u = want_u + [int(keys[b])]
+            pos = {k: i for i, k in enumerate(keys.tolist())}
+            assert near == sorted(want_u, key=lambda k: pos[k])
+            w = plan.list(2, j).tolist()
+            want_w = [k for k in tr.list(b, 2).tolist() if occ_of[k]] if occ[b] else []
+            assert w == sorted(want_w, key=lambda k: pos[k])
+    assert offsets_checked > 1000
+
+
+def _index(key):
+    key = int(key)
+    level = key & 0x7FFF
+    m = key >> 15
+    v = [0, 0, 0]
+    for bit in range(16):
+        v[0] |= ((m >> (3 * bit + 2)) & 1) << bit
+        v[1] |= ((m >> (3 * bit + 1)) & 1) << bit
+        v[2] |= ((m >> (3 * bit)) & 1) << bit
+    return np.array([c >> (16 - level) for c in v], dtype=np.int64)
+
+
+@pytest.mark.parametrize("p", [3, 6])
+def test_tables_equal_oracle(oracle, p):
+    x, _ = oracle.point_sets("cube", 200, 1)
+    plan = F.FmmBuilder(p).plan(x)
+    m2l, m2m, l2l = plan.tables()
+    om2l, om2m, ol2l = oracle.tables(p)
+    for a, b in ((m2l, om2l), (m2m, om2m), (l2l, ol2l)):
+        assert np.abs(a - b).max() <= 1e-14 * np.abs(b).max()
+
+
+def test_uniform_cube_counts(oracle):
+    # the reference's N = 1e5 uniform cube at 64 keys per leaf: a uniform level-4 tree,
+    # 640,584 V pairs and 58.1e6 near pairs (fmm-bench/results/phase4s-gh200.md:69-72,346,397)
+    x, _ = oracle.point_sets("cube", 100000, 0xBE9C06)
+    info = F.FmmBuilder(6).max_points_per_leaf(64).plan(x).info()
+    assert info["nleaves"] == 4096 and info["nlevels"] == 5
+    assert info["v_pairs"] == 640584
+    assert abs(info["near_pairs"] - 58.1e6) < 0.1e6
+
+
+def test_settings_errors():
+    x = np.random.default_rng(0).uniform(size=(10, 3))
+    with pytest.raises(F.FmmError):
+        F.FmmBuilder(4).max_points_per_leaf(0).plan(x)
+    with pytest.raises(F.FmmError):
+        F.FmmBuilder(4).plan(np.zeros((5, 3)))  # spans no volume
+    bad = x.copy()
+    bad[3, 1] = np.nan
+    with pytest.raises(F.FmmError):
+        F.FmmBuilder(4).plan(bad)
