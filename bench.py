@@ -29,6 +29,10 @@ import time
 
 import numpy as np
 
+import faulthandler
+
+faulthandler.enable()
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -144,6 +148,10 @@ def peaks():
         return {}
 
 
+def log(msg):
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 def run_ours(args):
     import torch
 
@@ -167,11 +175,12 @@ def run_ours(args):
         return (F.FmmBuilder(P).gradients().max_points_per_leaf(LEAF).precision(precision)
                 .device(local).build(x))
 
+    log(f"problem n={n} generated")
     t0 = time.perf_counter()
     fmm = build("mixed")
     build_s = time.perf_counter() - t0
     info = fmm.info()
-    stream = torch.cuda.ExternalStream(fmm.stream)
+    log(f"built in {time.perf_counter() - t0:.2f} s: {info}")
     dev = torch.device("cuda", local)
     dq = torch.from_numpy(q).to(dev)
     dphi = torch.empty(n, dtype=torch.float64, device=dev)
@@ -180,6 +189,7 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     def device_steps(f, steps, warmup):
+        stream = torch.cuda.ExternalStream(f.stream)  # the evaluator's own stream
         with torch.cuda.stream(stream):
             for _ in range(warmup):
                 f.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
@@ -203,16 +213,19 @@ def run_ours(args):
     with Clocks(local) as clk:
         ms = device_steps(fmm, args.steps, args.warmup)
     clocks = clk.summary()
+    log(f"timed: {ms:.3f} ms/step")
     if world > 1:
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     # per-kind split and the dominant kernel (separate, untimed evaluation)
     fmm.set_kind_timing(True)
+    stream = torch.cuda.ExternalStream(fmm.stream)
     with torch.cuda.stream(stream):
         flush.zero_()
         fmm.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
     kinds = fmm.kind_times()
+    log(f"kinds: {kinds}")
     fmm.set_kind_timing(False)
     # accuracy at sampled targets against the f64 direct sum on the GPU
     with torch.cuda.stream(stream):
@@ -220,7 +233,9 @@ def run_ours(args):
     fmm.synchronize()
     phi = dphi.cpu().numpy()
     grad = dg.cpu().numpy().reshape(n, 3)
+    log("direct sum")
     ex_phi, ex_g = F.direct_sum(x, q, x[sample], device=local)
+    log("e2e")
     err_phi = float(np.linalg.norm(phi[sample] - ex_phi) / np.linalg.norm(ex_phi))
     err_g = float(np.linalg.norm(grad[sample] - ex_g) / np.linalg.norm(ex_g))
     # e2e through the host API with pinned buffers
@@ -234,6 +249,7 @@ def run_ours(args):
         F._check(F.lib().fmmgpu_fmm_evaluate(fmm._h, hq.data_ptr(), hphi.data_ptr(), hg.data_ptr()))
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     fmm.close()
+    log(f"e2e {e2e_ms:.3f} ms")
     # the plain f64 evaluator on the same input
     plain = build("f64")
     plain_ms = device_steps(plain, max(2, args.steps // 2), max(1, args.warmup // 2))

@@ -66,6 +66,7 @@ def lib():
             "fmmgpu_fmm_tables": (C.c_int, [vp, dp, dp, dp]),
             "fmmgpu_fmm_set_kind_timing": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_kind_times": (C.c_int, [vp, dp]),
+            "fmmgpu_fmm_set_kinds": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_status_string": (C.c_char_p, [C.c_int]),
             "fmmgpu_last_error": (C.c_char_p, []),
@@ -233,6 +234,10 @@ class Fmm(Plan):
 
     def set_kind_timing(self, on=True):
         _check(lib().fmmgpu_fmm_set_kind_timing(self._h, int(on)))
+
+    def set_kinds(self, kinds):
+        """Test hook: bit 0 near field, bit 1 far field (3, the default, is the FMM)."""
+        _check(lib().fmmgpu_fmm_set_kinds(self._h, int(kinds)))
 
     def kind_times(self):
         """Milliseconds per kind of the last evaluation (after set_kind_timing(True))."""

@@ -115,6 +115,7 @@ struct KindTimer {
 // ----------------------------------------------------------------------------------
 struct EvaluatorBase {
     KindTimer timer;
+    int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
     virtual ~EvaluatorBase() = default;
     virtual void evaluate(const double* d_charges, double* d_phi, double* d_grad) = 0;
 };
@@ -133,7 +134,10 @@ struct Evaluator final : EvaluatorBase {
         tgt_start, tgt_perm, src_perm, near_row, near_col, w_row, w_col, x_row, x_col, v_row, v_col,
         v_off;
     // data
-    DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g;
+    DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g, Y;
+    // M2L batches: pairs of all levels grouped by offset, in tiles
+    DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
+    int64_t ntiles = 0;
 
     Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
               const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
@@ -215,6 +219,11 @@ struct Evaluator final : EvaluatorBase {
         far_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
+        build_m2l_batches(kGemmPairs);
+        Y.alloc(sizeof(T) * (size_t)m * NC * (pl.v.nnz() + 1));
+        gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
+        if (gemm_smem > 48 * 1024)
+            CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
         // shared memory opt-in beyond 48 KB where a kernel needs it
         size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
         if (exp_smem > 48 * 1024) {
@@ -223,11 +232,48 @@ struct Evaluator final : EvaluatorBase {
         }
     }
 
+    size_t gemm_smem = 0;
+
+    // V pairs of every level grouped by offset index, then by target box; tiles of up
+    // to `tile` pairs never straddle two offsets.
+    void build_m2l_batches(int tile) {
+        const Plan& pl = plan;
+        const size_t nnz = pl.v.nnz();
+        std::vector<int64_t> cnt(317, 0);
+        for (size_t e2 = 0; e2 < nnz; ++e2) cnt[pl.v.aux[e2] + 1]++;
+        for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+        std::vector<int64_t> pe(nnz);
+        std::vector<int32_t> ps(nnz);
+        std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+        // rows are boxes in order, so pairs of one offset come out ordered by target
+        for (size_t b = 0; b + 1 < pl.v.row.size(); ++b)
+            for (int64_t e2 = pl.v.row[b]; e2 < pl.v.row[b + 1]; ++e2) {
+                int64_t pos = fill[pl.v.aux[e2]]++;
+                pe[pos] = e2;
+                ps[pos] = pl.v.col[e2];
+            }
+        std::vector<int32_t> td, tc;
+        std::vector<int64_t> tb;
+        for (int d = 0; d < 316; ++d)
+            for (int64_t b = cnt[d]; b < cnt[d + 1]; b += tile) {
+                td.push_back(d);
+                tb.push_back(b);
+                tc.push_back((int32_t)std::min<int64_t>(tile, cnt[d + 1] - b));
+            }
+        ntiles = (int64_t)td.size();
+        tile_d.upload(td);
+        tile_begin.upload(tb);
+        tile_count.upload(tc);
+        pair_e.upload(pe);
+        pair_src.upload(ps);
+    }
+
     size_t device_bytes() const {
         const DevBuf* all[] = {&level, &idx, &parent, &child_first, &box_leaf, &src_below, &tgt_below,
                                &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
                                &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
-                               &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g};
+                               &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
+                               &Y, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -243,8 +289,24 @@ struct Evaluator final : EvaluatorBase {
             if (ns > 0)
                 charge_load_kernel<T><<<(unsigned)((ns + 255) / 256), 256, 0, stream>>>(
                     d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>());
-            CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, Lc.bytes, stream));
+            // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
+            int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
+            CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * NC * top, stream));
         });
+        if (!(kinds & 2)) {
+            // far field off: zero partials, then the near field and the output pass only
+            CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
+            CUDA_TRY(cudaMemsetAsync(far_g.ptr, 0, far_g.bytes, stream));
+        } else {
+            run_far();
+        }
+        run_near(d_phi, d_grad);
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    void run_far() {
+        const int L = plan.nlevels - 1;
+        const size_t nleaves = plan.nleaves();
         // upward: P2M of every leaf, then M2M from level L-1 up to 0
         const size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
         timer.run(kP2M, [&] {
@@ -260,49 +322,55 @@ struct Evaluator final : EvaluatorBase {
                         dp, b0, b1, m, m2m_tab.as<T>(), M.as<T>());
                 });
         }
-        // downward: for l = 2..L: L2L, M2L, P2L
+        // M2L products of every level at once (all multipoles are final here)
+        if (ntiles)
+            timer.run(kM2L, [&] {
+                m2l_gemm_kernel<P, T><<<(unsigned)ntiles, 256, gemm_smem, stream>>>(
+                    tile_d.as<int32_t>(), tile_begin.as<int64_t>(), tile_count.as<int32_t>(), pair_e.as<int64_t>(),
+                    pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
+            });
+        // downward: for l = 2..L: L2L + V (one kernel), then P2L
         for (int l = 2; l <= L; ++l) {
             int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
-            int64_t p0 = plan.level_start[l - 1], p1 = plan.level_start[l];
-            if (l >= 3)
-                timer.run(kL2L, [&] {
-                    l2l_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), NC * sizeof(T), stream>>>(
-                        dp, b0, b1, m, l2l_tab.as<T>(), Lc.as<T>());
-                });
-            timer.run(kM2L, [&] {
-                m2l_group_kernel<P, T><<<(unsigned)(p1 - p0), round32(NC), 8 * NC * sizeof(T), stream>>>(
-                    dp, p0, p1, m, m2l_tab.as<T>(), M.as<T>(), Lc.as<T>());
+            timer.run(kL2L, [&] {
+                local_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), NC * sizeof(T), stream>>>(
+                    dp, b0, b1, m, l >= 3, l2l_tab.as<T>(), Y.as<T>(), Lc.as<T>());
             });
             timer.run(kP2L, [&] {
                 expand_kernel<P, T, true><<<(unsigned)(b1 - b0), 32, exp_smem, stream>>>(
                     dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
             });
         }
-        // leaves: L2P + M2P, then P2P with the output pass
-        if (nleaves) {
-            if (gradients) {
-                timer.run(kFar, [&] {
+        // leaves: L2P + M2P
+        if (nleaves)
+            timer.run(kFar, [&] {
+                if (gradients)
                     leaf_far_kernel<P, T, true><<<(unsigned)nleaves, 64, NC * sizeof(T), stream>>>(
                         dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
-                });
-                timer.run(kP2P, [&] {
-                    p2p_kernel<T, true, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
-                        dp, m, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(), far_g.as<double>(),
-                        d_phi, d_grad);
-                });
-            } else {
-                timer.run(kFar, [&] {
+                else
                     leaf_far_kernel<P, T, false><<<(unsigned)nleaves, 64, NC * sizeof(T), stream>>>(
                         dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+            });
+    }
+
+    void run_near(double* d_phi, double* d_grad) {
+        const size_t nleaves = plan.nleaves();
+        const int near = kinds & 1;
+        if (nleaves) {
+            if (gradients) {
+                timer.run(kP2P, [&] {
+                    p2p_kernel<T, true, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
+                        dp, m, near, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(),
+                        far_g.as<double>(), d_phi, d_grad);
                 });
+            } else {
                 timer.run(kP2P, [&] {
                     p2p_kernel<T, false, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
-                        dp, m, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(), nullptr, d_phi,
-                        nullptr);
+                        dp, m, near, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(), nullptr,
+                        d_phi, nullptr);
                 });
             }
         }
-        CUDA_TRY(cudaGetLastError());
     }
 };
 
@@ -503,6 +571,13 @@ int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* f, int on) {
     return guarded([&] {
         if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
         f->eval->timer.on = on != 0;
+    });
+}
+
+int fmmgpu_fmm_set_kinds(fmmgpu_fmm* f, int kinds) {
+    return guarded([&] {
+        if (!f || !f->eval || kinds < 1 || kinds > 3) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid kinds");
+        f->eval->kinds = kinds;
     });
 }
 

@@ -204,100 +204,110 @@ __global__ void m2m_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, const T*
 }
 
 // ---------------------------------------------------------------------------------
-// L2L on one level: child (level l) += T_o * L_parent.  Block per child box.
+// Dense M2L as batched GEMM, SIMT form (f64 path): the V pairs of every level are
+// grouped by offset index d (fmm-kernels/src/translate.rs:61-74 batches them the same
+// way); a block takes a tile of up to 64 pairs of one offset, stages A_d (column-major,
+// so row k of the staged array holds column k) and the tile's source multipoles in
+// shared memory, and writes the products Y[e] = A_d M_s (e = the pair's position in
+// the target's V row).  Each thread holds 4 pairs x 6 output slots in registers.
 // ---------------------------------------------------------------------------------
+constexpr int kGemmPairs = 64;
+
 template <int P, typename T>
-__global__ void l2l_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, const T* __restrict__ tab,
-                           T* __restrict__ Lc) {
+__global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict__ tile_d,
+                                                       const int64_t* __restrict__ tile_begin,
+                                                       const int32_t* __restrict__ tile_count,
+                                                       const int64_t* __restrict__ pair_e,
+                                                       const int32_t* __restrict__ pair_src, int m,
+                                                       const T* __restrict__ tab, const T* __restrict__ M,
+                                                       T* __restrict__ Y) {
     constexpr int NC = nc_of(P);
+    constexpr int NCP = 96 > NC ? 96 : ((NC + 15) / 16) * 16;
+    constexpr int JN = NCP / 16;
     extern __shared__ unsigned char smem_raw[];
-    T* Lp = reinterpret_cast<T*>(smem_raw);  // [NC]
-    int64_t b = b0 + blockIdx.x;
-    if (b >= b1) return;
-    if (plan.tgt_below[b] == 0) return;
-    int par = plan.parent[b];
-    int o = (int)(((plan.idx[3 * b] & 1) << 2) | ((plan.idx[3 * b + 1] & 1) << 1) | (plan.idx[3 * b + 2] & 1));
-    const T* A0 = tab + (int64_t)o * NC * NC;
+    T* At = reinterpret_cast<T*>(smem_raw);  // [NC][NCP]: At[k][n] = A_d[n][k]
+    T* Xs = At + NC * NCP;                   // [NC][64]:  Xs[k][pair]
+    const int tile = blockIdx.x;
+    const int d = tile_d[tile];
+    const int64_t p0 = tile_begin[tile];
+    const int cnt = tile_count[tile];
+    const T* A = tab + (int64_t)d * NC * NC;
+    for (int t = threadIdx.x; t < NC * NCP; t += blockDim.x) {
+        int k = t / NCP, n = t % NCP;
+        At[t] = n < NC ? A[(int64_t)k * NC + n] : T(0);
+    }
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int v = 0; v < m; ++v) {
-        for (int k = threadIdx.x; k < NC; k += blockDim.x) Lp[k] = Lc[((int64_t)par * m + v) * NC + k];
         __syncthreads();
-        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
-            T acc = T(0);
-#pragma unroll 7
-            for (int k = 0; k < NC; ++k) acc += A0[(int64_t)k * NC + i] * Lp[k];
-            Lc[((int64_t)b * m + v) * NC + i] += acc;
+        for (int t = threadIdx.x; t < NC * kGemmPairs; t += blockDim.x) {
+            int pr = t / NC, k = t % NC;
+            Xs[k * kGemmPairs + pr] = pr < cnt ? M[((int64_t)pair_src[p0 + pr] * m + v) * NC + k] : T(0);
         }
         __syncthreads();
+        T acc[4][JN];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < JN; ++j) acc[i][j] = T(0);
+#pragma unroll 3
+        for (int k = 0; k < NC; ++k) {
+            T xv[4], av[JN];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) xv[i] = Xs[k * kGemmPairs + ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < JN; ++j) av[j] = At[k * NCP + tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < JN; ++j) acc[i][j] += av[j] * xv[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            int pr = ty * 4 + i;
+            if (pr >= cnt) continue;
+            T* y = Y + (pair_e[p0 + pr] * m + v) * NC;
+#pragma unroll
+            for (int j = 0; j < JN; ++j) {
+                int n = tx + 16 * j;
+                if (n < NC) y[n] = acc[i][j];
+            }
+        }
     }
 }
 
 // ---------------------------------------------------------------------------------
-// Dense M2L on one level, f64 SIMT form: block per parent; its 8 children are the
-// targets.  The children's V rows (sorted by offset index) are merged, so every table
-// A_d is read once per parent and applied to all children that have offset d; each
-// child's local receives its V-list terms in offset-index order.
+// The local of every box of one level (l >= 2) that has a target below it:
+//   L_t = L2L_o(L_parent) (l >= 3) + sum over its V row, in offset-index order, of Y[e]
+// written once (the accumulation order of fmm-plan/src/operator.rs:34-45: the L2L
+// from the parent, then the V list by offset index; the X list is added after).
 // ---------------------------------------------------------------------------------
 template <int P, typename T>
-__global__ void m2l_group_kernel(DevPlan plan, int64_t p0, int64_t p1, int m, const T* __restrict__ tab,
-                                 const T* __restrict__ M, T* __restrict__ Lc) {
+__global__ void local_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l,
+                             const T* __restrict__ l2l_tab, const T* __restrict__ Y, T* __restrict__ Lc) {
     constexpr int NC = nc_of(P);
     extern __shared__ unsigned char smem_raw[];
-    T* Ms = reinterpret_cast<T*>(smem_raw);  // [8][NC]
-    __shared__ int64_t ptr[8], end[8];
-    __shared__ int src[8];
-    __shared__ int cur_d;
-    int64_t pb = p0 + blockIdx.x;
-    if (pb >= p1) return;
-    int c0 = plan.child_first[pb];
-    if (c0 < 0 || plan.tgt_below[pb] == 0) return;
+    T* Lp = reinterpret_cast<T*>(smem_raw);  // [NC]
+    int64_t b = b0 + blockIdx.x;
+    if (b >= b1 || plan.tgt_below[b] == 0) return;
+    const int par = plan.parent[b];
+    const int o = (int)(((plan.idx[3 * b] & 1) << 2) | ((plan.idx[3 * b + 1] & 1) << 1) | (plan.idx[3 * b + 2] & 1));
+    const T* A0 = l2l_tab + (int64_t)o * NC * NC;
+    const int64_t e0 = plan.v_row[b], e1 = plan.v_row[b + 1];
     for (int v = 0; v < m; ++v) {
-        if (threadIdx.x < 8) {
-            ptr[threadIdx.x] = plan.v_row[c0 + threadIdx.x];
-            end[threadIdx.x] = plan.v_row[c0 + threadIdx.x + 1];
-        }
-        __syncthreads();
-        T acc[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = T(0);
-        for (;;) {
-            if (threadIdx.x == 0) {
-                int d = 1 << 30;
-                for (int c = 0; c < 8; ++c)
-                    if (ptr[c] < end[c] && plan.v_off[ptr[c]] < d) d = plan.v_off[ptr[c]];
-                cur_d = d;
-                for (int c = 0; c < 8; ++c) {
-                    if (ptr[c] < end[c] && plan.v_off[ptr[c]] == d) {
-                        src[c] = plan.v_col[ptr[c]];
-                        ptr[c]++;
-                    } else {
-                        src[c] = -1;
-                    }
-                }
-            }
+        if (with_l2l) {
             __syncthreads();
-            int d = cur_d;
-            if (d == (1 << 30)) break;
-            for (int t = threadIdx.x; t < 8 * NC; t += blockDim.x) {
-                int c = t / NC, k = t % NC;
-                Ms[t] = src[c] >= 0 ? M[((int64_t)src[c] * m + v) * NC + k] : T(0);
-            }
-            __syncthreads();
-            const T* A = tab + (int64_t)d * NC * NC;
-            const int i = threadIdx.x;  // blockDim.x >= NC
-            if (i < NC) {
-                for (int k = 0; k < NC; ++k) {
-                    T a = A[(int64_t)k * NC + i];
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) acc[c] += a * Ms[c * NC + k];
-                }
-            }
+            for (int k = threadIdx.x; k < NC; k += blockDim.x) Lp[k] = Lc[((int64_t)par * m + v) * NC + k];
             __syncthreads();
         }
-        if (threadIdx.x < NC) {
-            for (int c = 0; c < 8; ++c)
-                if (plan.tgt_below[c0 + c]) Lc[((int64_t)(c0 + c) * m + v) * NC + threadIdx.x] += acc[c];
+        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+            T acc = T(0);
+            if (with_l2l) {
+#pragma unroll 7
+                for (int k = 0; k < NC; ++k) acc += A0[(int64_t)k * NC + i] * Lp[k];
+            }
+            for (int64_t e = e0; e < e1; ++e) acc += Y[(e * m + v) * NC + i];
+            Lc[((int64_t)b * m + v) * NC + i] = acc;
         }
-        __syncthreads();
     }
 }
 
@@ -469,7 +479,7 @@ constexpr int kP2pWarps = 4;
 constexpr int kP2pStage = 64;
 
 template <typename T, bool GRAD, int TPL>
-__global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, int m,
+__global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, int m, int near,
                                                   const typename Vec4<T>::type* __restrict__ spos,
                                                   const T* __restrict__ sq,
                                                   const typename Vec4<T>::type* __restrict__ tpos,
@@ -483,7 +493,7 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, int m,
     const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
     if (t1 == t0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t n0 = plan.near_row[leaf], n1 = plan.near_row[leaf + 1];
+    const int64_t n0 = plan.near_row[leaf], n1 = near ? plan.near_row[leaf + 1] : n0;
     const int64_t nt = plan.ntgt;
     const double rt = ldexp(plan.side, -(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;

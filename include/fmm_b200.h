@@ -98,6 +98,9 @@ void* fmmgpu_fmm_stream(fmmgpu_fmm* fmm);
 /* Per-kind device timing of the following evaluations (the reference's KindTiming,
  * fmm-exec/src/fmm.rs:150-153): every launch is bracketed by CUDA events. */
 int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* fmm, int on);
+/* Which parts the following evaluations run, for tests: bit 0 the near field (P2P),
+ * bit 1 the far field (everything that reaches L2P and M2P); 3, the default, is the FMM. */
+int fmmgpu_fmm_set_kinds(fmmgpu_fmm* fmm, int kinds);
 /* Milliseconds of the last evaluation per kind: [0] charge load, [1] P2M, [2] M2M,
  * [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P + output pass.  Synchronises. */
 int fmmgpu_fmm_kind_times(fmmgpu_fmm* fmm, double* ms);

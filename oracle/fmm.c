@@ -130,6 +130,12 @@ static int cmp_pair(const void *a, const void *b) {
 
 int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
             int p, int max_keys, int gradients, int threads, double *phi_out, double *grad_out) {
+    return orc_fmm_kinds(ns, src, q, m, nt, tgt, p, max_keys, gradients, threads, 3, phi_out, grad_out);
+}
+
+int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+                  int p, int max_keys, int gradients, int threads, int kinds, double *phi_out,
+                  double *grad_out) {
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -330,7 +336,7 @@ int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, con
             double *cphi = (double *)calloc(m * n, sizeof(double));
             double *cg = gradients ? (double *)calloc(3 * m * n, sizeof(double)) : NULL;
             const double *u = ut + 3 * t_off[j];
-            orc_l2p(p, zero3, 1.0, Lc + (size_t)b * m * nc, m, n, u, cphi, cg);
+            if (kinds & 2) orc_l2p(p, zero3, 1.0, Lc + (size_t)b * m * nc, m, n, u, cphi, cg);
             vecz wl = {0, 0, 0}, near = {0, 0, 0};
             for (int dx = -1; dx <= 1; ++dx)
                 for (int dy = -1; dy <= 1; ++dy)
@@ -359,7 +365,7 @@ int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, con
             zpush(&near, j);
             sort_unique(&wl);
             sort_unique(&near);
-            for (size_t e = 0; e < wl.len; ++e) {
+            for (size_t e = 0; e < ((kinds & 2) ? wl.len : 0); ++e) {
                 size_t s = wl.data[e];
                 double c[3], r;
                 rel_frame(&B, s, (size_t)b, c, &r); /* (c(s|t), r(s|t)) */
@@ -367,7 +373,7 @@ int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, con
             }
             double *ys = NULL;
             size_t ys_cap = 0;
-            for (size_t e = 0; e < near.len; ++e) {
+            for (size_t e = 0; e < ((kinds & 1) ? near.len : 0); ++e) {
                 size_t sj = near.data[e], s = leaf_box[sj];
                 size_t nsrc = s_off[sj + 1] - s_off[sj];
                 const double *y = us + 3 * s_off[sj];

@@ -118,6 +118,12 @@ size_t orc_tree_list(const orc_tree *t, size_t box, int kind, uint64_t *out, siz
 int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
             int p, int max_keys, int gradients, int threads, double *phi, double *grad);
 
+/* the same with a kinds mask: bit 0 the near field (P2P), bit 1 the far field (L2P, M2P
+ * and everything upstream of them); 3 is the whole FMM */
+int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t nt,
+                  const double *tgt, int p, int max_keys, int gradients, int threads, int kinds,
+                  double *phi, double *grad);
+
 /* the oracle's own scaling of one leaf-scaled coordinate (fmm-exec/src/geometry.rs:291) */
 double orc_leaf_coordinate(double x, double lower, double side, int level, uint32_t index);
 

@@ -61,6 +61,8 @@ def lib():
             "orc_tree_list": (_sz, [C.c_void_p, _sz, C.c_int, _u64p, _sz]),
             "orc_fmm": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
                                   C.c_int, _dp, C.c_void_p]),
+            "orc_fmm_kinds": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, C.c_int, _dp, C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -147,9 +149,9 @@ def direct_sum(src, q, tgt, gradients=True, threads=True):
     return phi, g
 
 
-def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0):
+def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0, kinds=3):
     """The restated host FMM; q is (N,) or (N, m); returns phi (m, Nt), grad (m, Nt, 3)
-    in caller order with 1/(4 pi) applied."""
+    in caller order with 1/(4 pi) applied.  kinds: bit 0 near field, bit 1 far field."""
     src = np.ascontiguousarray(src, dtype=np.float64)
     tgt = np.ascontiguousarray(tgt, dtype=np.float64)
     q = np.asarray(q, dtype=np.float64)
@@ -157,8 +159,8 @@ def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0):
     q = np.ascontiguousarray(q.reshape(len(src), m))
     phi = np.zeros(m * len(tgt))
     g = np.zeros(3 * m * len(tgt)) if gradients else None
-    rc = lib().orc_fmm(len(src), src, q, m, len(tgt), tgt, p, max_keys, int(gradients), threads,
-                       phi, _ptr(g))
+    rc = lib().orc_fmm_kinds(len(src), src, q, m, len(tgt), tgt, p, max_keys, int(gradients), threads,
+                             kinds, phi, _ptr(g))
     if rc != 0:
         raise RuntimeError(f"oracle fmm failed: {rc}")
     return phi.reshape(m, len(tgt)), (g.reshape(m, len(tgt), 3) if gradients else None)

@@ -92,3 +92,19 @@ def test_f64_accuracy_gate_problem(oracle):
         d, _ = oracle.direct_sum(x, q[:, k], x[sample], gradients=False)
         errs.append(rel(out.potential[k][sample], d / (4 * np.pi)))
     assert np.sqrt(np.mean(np.square(errs))) < 2 * 1.08e-5
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-12), ("mixed", 1e-4)])
+def test_near_and_far_fields_separately(oracle, precision, tol):
+    """Near field (P2P) alone and far field alone against the oracle's same split."""
+    x, q = oracle.point_sets("sphere", 30000, 17)
+    fmm = F.FmmBuilder(8).gradients().max_points_per_leaf(64).precision(precision).build(x)
+    errs = {}
+    for kinds, name in ((1, "near"), (2, "far")):
+        fmm.set_kinds(kinds)
+        out = fmm.evaluate(q)
+        phi, g = oracle.fmm(x, q, x, 8, 64, gradients=True, threads=8, kinds=kinds)
+        errs[name] = (rel(out.potential, phi), rel(out.gradient, g))
+    print(precision, errs)
+    for name, (ep, eg) in errs.items():
+        assert ep < tol and eg < tol, (name, ep, eg)
