@@ -307,7 +307,7 @@ def run_ours(args):
                       "mixed_over_plain": round(plain_ms / ms, 3)},
         "kinds_ms": {k: round(v, 4) for k, v in kinds.items()},
         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs",
-                                      "x_pairs", "device_bytes")},
+                                      "x_pairs", "device_bytes", "close_pairs")},
         "build_s": round(build_s, 3),
         "e2e": {"value": round(n / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
                 "ms_per_step": round(e2e_ms, 4),

@@ -2,6 +2,7 @@
 // and the C ABI of include/fmm_b200.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -115,6 +116,7 @@ struct KindTimer {
 // ----------------------------------------------------------------------------------
 struct EvaluatorBase {
     KindTimer timer;
+    int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
     virtual ~EvaluatorBase() = default;
     virtual void evaluate(const double* d_charges, double* d_phi, double* d_grad) = 0;
@@ -138,6 +140,15 @@ struct Evaluator final : EvaluatorBase {
     // M2L batches: pairs of all levels grouped by offset, in tiles
     DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
     int64_t ntiles = 0;
+    // P2P work items (32 targets of one leaf each) and, for the mixed form, the
+    // near-singular pairs evaluated in f64
+    DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64;
+    P2pItems items{};
+    ClosePairs close{};
+    int64_t nclose = 0;
+    static constexpr bool kMixed = sizeof(T) == 4;
+    // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
+    static constexpr float kTheta2 = 0.0625f;
 
     Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
               const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
@@ -220,6 +231,9 @@ struct Evaluator final : EvaluatorBase {
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
         build_m2l_batches(kGemmPairs);
+        build_p2p_items();
+        if (kMixed) build_close_pairs(us, ut);
+        close_pairs = nclose;
         Y.alloc(sizeof(T) * (size_t)m * NC * (pl.v.nnz() + 1));
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
         if (gemm_smem > 48 * 1024)
@@ -268,12 +282,90 @@ struct Evaluator final : EvaluatorBase {
         pair_src.upload(ps);
     }
 
+    void build_p2p_items() {
+        std::vector<int32_t> il;
+        std::vector<int64_t> it;
+        for (size_t j = 0; j < plan.nleaves(); ++j)
+            for (int64_t t = plan.tgt_start[j]; t < plan.tgt_start[j + 1]; t += 32) {
+                il.push_back((int32_t)j);
+                it.push_back(t);
+            }
+        item_leaf.upload(il);
+        item_t0.upload(it);
+        items.leaf = item_leaf.as<int32_t>();
+        items.t0 = item_t0.as<int64_t>();
+        items.count = (int64_t)il.size();
+    }
+
+    // The mixed form's f64 pairs: found on the device with the f32 arithmetic of the P2P
+    // kernel itself, then sorted per target (source order) into a CSR.
+    void build_close_pairs(const std::vector<double>& us, const std::vector<double>& ut) {
+        auto up64 = [](DevBuf& b, const std::vector<double>& u) {
+            size_t n = u.size() / 3;
+            std::vector<double4> v(n);
+            for (size_t i = 0; i < n; ++i) v[i] = make_double4(u[3 * i], u[3 * i + 1], u[3 * i + 2], 0.0);
+            b.upload(v);
+        };
+        up64(spos64, us);
+        up64(tpos64, ut);
+        sq64.alloc(sizeof(double) * (size_t)m * (dp.nsrc + 1));
+        int64_t cap = std::max<int64_t>(1 << 20, dp.ntgt * 2);
+        DevBuf cnt, ot, os, ol;
+        cnt.alloc(sizeof(unsigned long long));
+        unsigned long long found = 0;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            ot.alloc(sizeof(int64_t) * cap);
+            os.alloc(sizeof(int64_t) * cap);
+            ol.alloc(sizeof(int32_t) * cap);
+            CUDA_TRY(cudaMemset(cnt.ptr, 0, sizeof(unsigned long long)));
+            if (items.count)
+                close_pairs_kernel<T><<<(unsigned)((items.count + kP2pWarps - 1) / kP2pWarps), 32 * kP2pWarps>>>(
+                    dp, items, (T)kTheta2, spos.as<T4>(), tpos.as<T4>(), cnt.as<unsigned long long>(), cap,
+                    ot.as<int64_t>(), os.as<int64_t>(), ol.as<int32_t>());
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaMemcpy(&found, cnt.ptr, sizeof(found), cudaMemcpyDeviceToHost));
+            if ((int64_t)found <= cap) break;
+            cap = (int64_t)found + 1024;
+        }
+        nclose = (int64_t)found;
+        std::vector<int64_t> ht(nclose), hs(nclose);
+        std::vector<int32_t> hl(nclose);
+        if (nclose) {
+            CUDA_TRY(cudaMemcpy(ht.data(), ot.ptr, sizeof(int64_t) * nclose, cudaMemcpyDeviceToHost));
+            CUDA_TRY(cudaMemcpy(hs.data(), os.ptr, sizeof(int64_t) * nclose, cudaMemcpyDeviceToHost));
+            CUDA_TRY(cudaMemcpy(hl.data(), ol.ptr, sizeof(int32_t) * nclose, cudaMemcpyDeviceToHost));
+        }
+        std::vector<int64_t> order(nclose);
+        for (int64_t i = 0; i < nclose; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+            return ht[a] != ht[b] ? ht[a] < ht[b] : hs[a] < hs[b];
+        });
+        std::vector<int64_t> row(dp.ntgt + 1, 0), src(nclose);
+        std::vector<int32_t> lf(nclose);
+        for (int64_t i = 0; i < nclose; ++i) {
+            row[ht[order[i]] + 1]++;
+            src[i] = hs[order[i]];
+            lf[i] = hl[order[i]];
+        }
+        for (int64_t t = 0; t < dp.ntgt; ++t) row[t + 1] += row[t];
+        close_row.upload(row);
+        close_src.upload(src);
+        close_leaf.upload(lf);
+        close.row = close_row.as<int64_t>();
+        close.src = close_src.as<int64_t>();
+        close.leaf = close_leaf.as<int32_t>();
+        close.spos = spos64.as<double4>();
+        close.tpos = tpos64.as<double4>();
+        close.q = sq64.as<double>();
+    }
+
     size_t device_bytes() const {
         const DevBuf* all[] = {&level, &idx, &parent, &child_first, &box_leaf, &src_below, &tgt_below,
                                &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
                                &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
                                &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
-                               &Y, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src};
+                               &Y, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
+                               &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -288,7 +380,7 @@ struct Evaluator final : EvaluatorBase {
         timer.run(kLoad, [&] {
             if (ns > 0)
                 charge_load_kernel<T><<<(unsigned)((ns + 255) / 256), 256, 0, stream>>>(
-                    d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>());
+                    d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
             // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
             int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
             CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * NC * top, stream));
@@ -354,23 +446,19 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void run_near(double* d_phi, double* d_grad) {
-        const size_t nleaves = plan.nleaves();
         const int near = kinds & 1;
-        if (nleaves) {
-            if (gradients) {
-                timer.run(kP2P, [&] {
-                    p2p_kernel<T, true, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
-                        dp, m, near, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(),
-                        far_g.as<double>(), d_phi, d_grad);
-                });
-            } else {
-                timer.run(kP2P, [&] {
-                    p2p_kernel<T, false, 2><<<(unsigned)nleaves, 128, 0, stream>>>(
-                        dp, m, near, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), far_phi.as<double>(), nullptr,
-                        d_phi, nullptr);
-                });
-            }
-        }
+        if (!items.count) return;
+        const unsigned grid = (unsigned)((items.count + kP2pWarps - 1) / kP2pWarps);
+        timer.run(kP2P, [&] {
+            if (gradients)
+                p2p_kernel<T, true, kMixed><<<grid, 32 * kP2pWarps, 0, stream>>>(
+                    dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
+                    far_phi.as<double>(), far_g.as<double>(), d_phi, d_grad);
+            else
+                p2p_kernel<T, false, kMixed><<<grid, 32 * kP2pWarps, 0, stream>>>(
+                    dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
+                    far_phi.as<double>(), nullptr, d_phi, nullptr);
+        });
     }
 };
 
@@ -612,6 +700,7 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->w_pairs = (int64_t)P.w.nnz();
         info->x_pairs = (int64_t)P.x.nnz();
         info->device_bytes = (int64_t)f->device_bytes;
+        info->close_pairs = f->eval ? f->eval->close_pairs : 0;
     });
 }
 

@@ -67,11 +67,15 @@ __device__ __forceinline__ void rel_frame(const DevPlan& P, int s, int t, T c[3]
 // ---------------------------------------------------------------------------------
 template <typename T>
 __global__ void charge_load_kernel(const double* __restrict__ q_caller, const int64_t* __restrict__ perm,
-                                   int64_t n, int m, T* __restrict__ q_leaf) {
+                                   int64_t n, int m, T* __restrict__ q_leaf, double* __restrict__ q64) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t c = perm[i];
-    for (int v = 0; v < m; ++v) q_leaf[(int64_t)v * n + i] = (T)q_caller[c * m + v];
+    for (int v = 0; v < m; ++v) {
+        double q = q_caller[c * m + v];
+        q_leaf[(int64_t)v * n + i] = (T)q;
+        if (q64) q64[(int64_t)v * n + i] = q;  // the mixed form keeps f64 charges for its f64 pairs
+    }
 }
 
 // ---------------------------------------------------------------------------------
@@ -465,148 +469,236 @@ __global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int m,
 }
 
 // ---------------------------------------------------------------------------------
-// P2P + output pass.  Block of 4 warps per target leaf; each warp holds TPL targets
-// per lane and walks every 4th entry of the near row (source leaves by leaf index),
-// staging the mapped sources y = fma(r, u_s, c) (the leaf itself: u_s unchanged) in its
-// own shared memory.  A pair with r2 == 0 adds nothing (select, never a mask
-// multiply).  Warp partials are summed in warp order, added to the far-field partial
-// in f64 and scaled once: phi = phi_hat / (4 pi r_t), g = g_hat / ((4 pi r_t) r_t),
-// then written in caller order.
-// The per-source-leaf partial is kept in T and added into an f64 accumulator per
-// target, so the f32 form sums in f32 only within one source leaf.
+// P2P + output pass.  One warp per work item = up to 32 targets of one leaf (lane =
+// target); the warp walks the leaf's near row (source leaves by leaf index) and stages
+// each source leaf's points in its own shared memory, mapped to the target leaf's
+// frame: y = fma(r, u_s, c) (CONVENTIONS 3.13 "Device kernels", rule 1), the leaf
+// itself unchanged.  Per pair d = u_t - y, r2 by explicit fma (rules 2-3), and the
+// pair is skipped by a select before rho meets a charge (rule 4).
+//   f64 (plain): skipped iff r2 == 0, the coincidence rule of the reference.
+//   f32 (mixed): skipped iff r2 < theta2; those near-singular pairs (found once at
+//   build time with the same arithmetic, pair_r2 below) are added in f64 from the f64
+//   coordinates at the end, with the f64 coincidence rule.
+// The f32 partial of one source leaf is added into an f64 accumulator per target.  The
+// sum is then added to the far-field partial and scaled once, phi = phi_hat/(4 pi r_t)
+// and g = g_hat/((4 pi r_t) r_t) (fmm-exec/src/fmm.rs:4750-4778), in caller order.
 // ---------------------------------------------------------------------------------
 constexpr int kP2pWarps = 4;
 constexpr int kP2pStage = 64;
 
-template <typename T, bool GRAD, int TPL>
-__global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, int m, int near,
+template <typename T>
+__device__ __forceinline__ T map_coord(T r, T u, T c);
+template <>
+__device__ __forceinline__ float map_coord<float>(float r, float u, float c) { return __fmaf_rn(r, u, c); }
+template <>
+__device__ __forceinline__ double map_coord<double>(double r, double u, double c) { return __fma_rn(r, u, c); }
+
+template <typename T>
+__device__ __forceinline__ T pair_r2(T dx, T dy, T dz);
+template <>
+__device__ __forceinline__ float pair_r2<float>(float dx, float dy, float dz) {
+    return __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+}
+template <>
+__device__ __forceinline__ double pair_r2<double>(double dx, double dy, double dz) {
+    return __fma_rn(dx, dx, __fma_rn(dy, dy, __dmul_rn(dz, dz)));
+}
+template <typename T>
+__device__ __forceinline__ T sub_rn(T a, T b);
+template <>
+__device__ __forceinline__ float sub_rn<float>(float a, float b) { return __fsub_rn(a, b); }
+template <>
+__device__ __forceinline__ double sub_rn<double>(double a, double b) { return __dsub_rn(a, b); }
+
+struct P2pItems {
+    const int32_t* leaf;  // work item -> target leaf
+    const int64_t* t0;    // work item -> first target (leaf order)
+    int64_t count;
+};
+
+struct ClosePairs {  // near-singular pairs of the mixed form, CSR by target (leaf order)
+    const int64_t* row;
+    const int64_t* src;   // source point (leaf order)
+    const int32_t* leaf;  // its source leaf
+    const double4* spos;  // f64 leaf-scaled coordinates
+    const double4* tpos;
+    const double* q;      // f64 charges in leaf order [vector][point]
+};
+
+template <typename T, bool GRAD, bool CLOSE>
+__global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, int m, int near, T theta2,
                                                   const typename Vec4<T>::type* __restrict__ spos,
                                                   const T* __restrict__ sq,
-                                                  const typename Vec4<T>::type* __restrict__ tpos,
+                                                  const typename Vec4<T>::type* __restrict__ tpos, ClosePairs close,
                                                   const double* __restrict__ far_phi, const double* __restrict__ far_g,
                                                   double* __restrict__ out_phi, double* __restrict__ out_g) {
     using T4 = typename Vec4<T>::type;
     __shared__ T4 stage[kP2pWarps][kP2pStage];
-    __shared__ double red[kP2pWarps][32 * TPL][4];
-    const int leaf = blockIdx.x;
-    const int box = plan.leaf_box[leaf];
-    const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
-    if (t1 == t0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * kP2pWarps + warp;
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int box = plan.leaf_box[leaf];
+    const int64_t t1 = plan.tgt_start[leaf + 1];
+    const int64_t t = items.t0[item] + lane;
+    const bool valid = t < t1;
     const int64_t n0 = plan.near_row[leaf], n1 = near ? plan.near_row[leaf + 1] : n0;
     const int64_t nt = plan.ntgt;
+    T tx = T(0), ty = T(0), tz = T(0);
+    if (valid) {
+        T4 p4 = tpos[t];
+        tx = p4.x;
+        ty = p4.y;
+        tz = p4.z;
+    }
     const double rt = ldexp(plan.side, -(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;
     const double g_scale = phi_scale * rt;
     for (int v = 0; v < m; ++v) {
-        for (int64_t tb = t0; tb < t1; tb += 32 * TPL) {
-            T tx[TPL], ty[TPL], tz[TPL];
-            double aphi[TPL], ag[TPL][3];
-#pragma unroll
-            for (int j = 0; j < TPL; ++j) {
-                int64_t t = tb + lane + 32 * j;
-                tx[j] = ty[j] = tz[j] = T(0);
-                if (t < t1) {
-                    T4 p4 = tpos[t];
-                    tx[j] = p4.x;
-                    ty[j] = p4.y;
-                    tz[j] = p4.z;
+        double aphi = 0.0, ag0 = 0.0, ag1 = 0.0, ag2 = 0.0;
+        for (int64_t e = n0; e < n1; ++e) {
+            const int sl = plan.near_col[e];
+            T c[3] = {T(0), T(0), T(0)}, r = T(1);
+            const bool self = sl == leaf;
+            if (!self) rel_frame<T>(plan, plan.leaf_box[sl], box, c, r);
+            const int64_t s0 = plan.src_start[sl], s1 = plan.src_start[sl + 1];
+            for (int64_t sb = s0; sb < s1; sb += kP2pStage) {
+                const int cnt = (int)((s1 - sb) < kP2pStage ? (s1 - sb) : kP2pStage);
+                for (int j = lane; j < cnt; j += 32) {
+                    T4 p4 = spos[sb + j];
+                    T4 y;
+                    y.x = self ? p4.x : map_coord<T>(r, p4.x, c[0]);
+                    y.y = self ? p4.y : map_coord<T>(r, p4.y, c[1]);
+                    y.z = self ? p4.z : map_coord<T>(r, p4.z, c[2]);
+                    y.w = sq[(int64_t)v * plan.nsrc + sb + j];
+                    stage[warp][j] = y;
                 }
-                aphi[j] = 0.0;
-                ag[j][0] = ag[j][1] = ag[j][2] = 0.0;
-            }
-            for (int64_t e = n0 + warp; e < n1; e += kP2pWarps) {
-                int sl = plan.near_col[e];
-                int sbox = plan.leaf_box[sl];
-                T c[3] = {T(0), T(0), T(0)}, r = T(1);
-                bool self = sl == leaf;
-                if (!self) rel_frame<T>(plan, sbox, box, c, r);
-                int64_t s0 = plan.src_start[sl], s1 = plan.src_start[sl + 1];
-                for (int64_t sb = s0; sb < s1; sb += kP2pStage) {
-                    int cnt = (int)((s1 - sb) < kP2pStage ? (s1 - sb) : kP2pStage);
-                    for (int j = lane; j < cnt; j += 32) {
-                        T4 p4 = spos[sb + j];
-                        T4 y;
-                        if (self) {
-                            y.x = p4.x;
-                            y.y = p4.y;
-                            y.z = p4.z;
-                        } else {
-                            y.x = fma(r, p4.x, c[0]);
-                            y.y = fma(r, p4.y, c[1]);
-                            y.z = fma(r, p4.z, c[2]);
-                        }
-                        y.w = sq[(int64_t)v * plan.nsrc + sb + j];
-                        stage[warp][j] = y;
+                __syncwarp();
+                T pphi = T(0), pg0 = T(0), pg1 = T(0), pg2 = T(0);
+#pragma unroll 4
+                for (int s = 0; s < cnt; ++s) {
+                    const T4 y = stage[warp][s];
+                    const T dx = sub_rn<T>(tx, y.x), dy = sub_rn<T>(ty, y.y), dz = sub_rn<T>(tz, y.z);
+                    const T r2 = pair_r2<T>(dx, dy, dz);
+                    const bool skip = CLOSE ? (r2 < theta2) : (r2 == T(0));
+                    const T rinv = skip ? T(0) : rsqrt(r2);
+                    const T qr = y.w * rinv;
+                    pphi += qr;
+                    if (GRAD) {
+                        const T qr3 = qr * rinv * rinv;
+                        pg0 -= qr3 * dx;
+                        pg1 -= qr3 * dy;
+                        pg2 -= qr3 * dz;
                     }
-                    __syncwarp();
-                    T pphi[TPL], pg[TPL][3];
-#pragma unroll
-                    for (int j = 0; j < TPL; ++j) pphi[j] = pg[j][0] = pg[j][1] = pg[j][2] = T(0);
-                    for (int s = 0; s < cnt; ++s) {
-                        T4 y = stage[warp][s];
-#pragma unroll
-                        for (int j = 0; j < TPL; ++j) {
-                            T dx = tx[j] - y.x, dy = ty[j] - y.y, dz = tz[j] - y.z;
-                            T r2 = dx * dx + dy * dy + dz * dz;
-                            T rinv = r2 == T(0) ? T(0) : rsqrt(r2);
-                            T qr = y.w * rinv;
-                            pphi[j] += qr;
-                            if (GRAD) {
-                                T qr3 = qr * rinv * rinv;
-                                pg[j][0] -= qr3 * dx;
-                                pg[j][1] -= qr3 * dy;
-                                pg[j][2] -= qr3 * dz;
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < TPL; ++j) {
-                        aphi[j] += (double)pphi[j];
-                        if (GRAD) {
-                            ag[j][0] += (double)pg[j][0];
-                            ag[j][1] += (double)pg[j][1];
-                            ag[j][2] += (double)pg[j][2];
-                        }
-                    }
-                    __syncwarp();
                 }
-            }
-#pragma unroll
-            for (int j = 0; j < TPL; ++j) {
-                red[warp][lane + 32 * j][0] = aphi[j];
-                red[warp][lane + 32 * j][1] = ag[j][0];
-                red[warp][lane + 32 * j][2] = ag[j][1];
-                red[warp][lane + 32 * j][3] = ag[j][2];
-            }
-            __syncthreads();
-            for (int j = threadIdx.x; j < 32 * TPL; j += blockDim.x) {
-                int64_t t = tb + j;
-                if (t >= t1) continue;
-                double ph = far_phi[(int64_t)v * nt + t];
-                double g0 = 0, g1 = 0, g2 = 0;
+                aphi += (double)pphi;
                 if (GRAD) {
-                    const double* fg = far_g + ((int64_t)v * nt + t) * 3;
-                    g0 = fg[0];
-                    g1 = fg[1];
-                    g2 = fg[2];
+                    ag0 += (double)pg0;
+                    ag1 += (double)pg1;
+                    ag2 += (double)pg2;
                 }
-                for (int w = 0; w < kP2pWarps; ++w) {
-                    ph += red[w][j][0];
-                    g0 += red[w][j][1];
-                    g1 += red[w][j][2];
-                    g2 += red[w][j][3];
-                }
-                int64_t i = plan.tgt_perm[t];
-                out_phi[(int64_t)v * nt + i] = ph / phi_scale;
+                __syncwarp();
+            }
+        }
+        if (!valid) continue;
+        if (CLOSE && near) {
+            // near-singular pairs in f64: the f64 map and the reference's coincidence rule
+            const double4 u = close.tpos[t];
+            for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
+                const int64_t sp = close.src[c2];
+                const int sl = close.leaf[c2];
+                double cc[3] = {0.0, 0.0, 0.0}, rr = 1.0;
+                if (sl != leaf) rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
+                const double4 ps = close.spos[sp];
+                const double yx = sl != leaf ? __fma_rn(rr, ps.x, cc[0]) : ps.x;
+                const double yy = sl != leaf ? __fma_rn(rr, ps.y, cc[1]) : ps.y;
+                const double yz = sl != leaf ? __fma_rn(rr, ps.z, cc[2]) : ps.z;
+                if (u.x == yx && u.y == yy && u.z == yz) continue;
+                const double dx = u.x - yx, dy = u.y - yy, dz = u.z - yz;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const double rinv = rsqrt(r2);
+                const double qr = close.q[(int64_t)v * plan.nsrc + sp] * rinv;
+                aphi += qr;
                 if (GRAD) {
-                    double* o = out_g + ((int64_t)v * nt + i) * 3;
-                    o[0] = g0 / g_scale;
-                    o[1] = g1 / g_scale;
-                    o[2] = g2 / g_scale;
+                    const double qr3 = qr * rinv * rinv;
+                    ag0 -= qr3 * dx;
+                    ag1 -= qr3 * dy;
+                    ag2 -= qr3 * dz;
                 }
             }
-            __syncthreads();
+        }
+        const double ph = far_phi[(int64_t)v * nt + t] + aphi;
+        const int64_t i = plan.tgt_perm[t];
+        out_phi[(int64_t)v * nt + i] = ph / phi_scale;
+        if (GRAD) {
+            const double* fg = far_g + ((int64_t)v * nt + t) * 3;
+            double* o = out_g + ((int64_t)v * nt + i) * 3;
+            o[0] = (fg[0] + ag0) / g_scale;
+            o[1] = (fg[1] + ag1) / g_scale;
+            o[2] = (fg[2] + ag2) / g_scale;
+        }
+    }
+}
+
+// Build time (mixed form): every near pair whose f32 r2, formed exactly as p2p_kernel
+// forms it, is below theta2.  Appends (target, source point, source leaf); *count may
+// exceed cap, in which case the caller enlarges the buffer and runs it again.
+template <typename T>
+__global__ void __launch_bounds__(128) close_pairs_kernel(DevPlan plan, P2pItems items, T theta2,
+                                                          const typename Vec4<T>::type* __restrict__ spos,
+                                                          const typename Vec4<T>::type* __restrict__ tpos,
+                                                          unsigned long long* count, int64_t cap,
+                                                          int64_t* __restrict__ out_t, int64_t* __restrict__ out_s,
+                                                          int32_t* __restrict__ out_leaf) {
+    using T4 = typename Vec4<T>::type;
+    __shared__ T4 stage[kP2pWarps][kP2pStage];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * kP2pWarps + warp;
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int box = plan.leaf_box[leaf];
+    const int64_t t1 = plan.tgt_start[leaf + 1];
+    const int64_t t = items.t0[item] + lane;
+    const bool valid = t < t1;
+    T tx = T(0), ty = T(0), tz = T(0);
+    if (valid) {
+        T4 p4 = tpos[t];
+        tx = p4.x;
+        ty = p4.y;
+        tz = p4.z;
+    }
+    for (int64_t e = plan.near_row[leaf]; e < plan.near_row[leaf + 1]; ++e) {
+        const int sl = plan.near_col[e];
+        T c[3] = {T(0), T(0), T(0)}, r = T(1);
+        const bool self = sl == leaf;
+        if (!self) rel_frame<T>(plan, plan.leaf_box[sl], box, c, r);
+        const int64_t s0 = plan.src_start[sl], s1 = plan.src_start[sl + 1];
+        for (int64_t sb = s0; sb < s1; sb += kP2pStage) {
+            const int cnt = (int)((s1 - sb) < kP2pStage ? (s1 - sb) : kP2pStage);
+            for (int j = lane; j < cnt; j += 32) {
+                T4 p4 = spos[sb + j];
+                T4 y;
+                y.x = self ? p4.x : map_coord<T>(r, p4.x, c[0]);
+                y.y = self ? p4.y : map_coord<T>(r, p4.y, c[1]);
+                y.z = self ? p4.z : map_coord<T>(r, p4.z, c[2]);
+                y.w = T(0);
+                stage[warp][j] = y;
+            }
+            __syncwarp();
+            if (valid)
+                for (int s = 0; s < cnt; ++s) {
+                    const T4 y = stage[warp][s];
+                    const T dx = sub_rn<T>(tx, y.x), dy = sub_rn<T>(ty, y.y), dz = sub_rn<T>(tz, y.z);
+                    if (pair_r2<T>(dx, dy, dz) < theta2) {
+                        unsigned long long k = atomicAdd(count, 1ULL);
+                        if ((int64_t)k < cap) {
+                            out_t[k] = t;
+                            out_s[k] = sb + s;
+                            out_leaf[k] = sl;
+                        }
+                    }
+                }
+            __syncwarp();
         }
     }
 }

@@ -66,6 +66,7 @@ typedef struct {
     int64_t v_pairs;      /* M2L box pairs */
     int64_t w_pairs, x_pairs;
     int64_t device_bytes; /* device memory held by the evaluator */
+    int64_t close_pairs;  /* near-singular P2P pairs the mixed form evaluates in f64 */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;
