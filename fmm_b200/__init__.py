@@ -67,6 +67,7 @@ def lib():
             "fmmgpu_fmm_set_kind_timing": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_kind_times": (C.c_int, [vp, dp]),
             "fmmgpu_fmm_set_kinds": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_status_string": (C.c_char_p, [C.c_int]),
             "fmmgpu_last_error": (C.c_char_p, []),
@@ -238,6 +239,10 @@ class Fmm(Plan):
     def set_kinds(self, kinds):
         """Test hook: bit 0 near field, bit 1 far field (3, the default, is the FMM)."""
         _check(lib().fmmgpu_fmm_set_kinds(self._h, int(kinds)))
+
+    def set_m2l_path(self, path):
+        """Test hook: 1 tensor-core M2L (mixed, p <= 8; the default), 0 SIMT M2L."""
+        _check(lib().fmmgpu_fmm_set_m2l_path(self._h, int(path)))
 
     def kind_times(self):
         """Milliseconds per kind of the last evaluation (after set_kind_timing(True))."""

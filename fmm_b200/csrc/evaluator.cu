@@ -12,6 +12,7 @@
 
 #include "../../include/fmm_b200.h"
 #include "kernels.cuh"
+#include "m2l_tc.cuh"
 #include "plan.hpp"
 
 namespace fmmb {
@@ -116,6 +117,8 @@ struct KindTimer {
 // ----------------------------------------------------------------------------------
 struct EvaluatorBase {
     KindTimer timer;
+    int m2l_path = 1;  // 1: tensor cores where the form has them (mixed, p <= 8), 0: SIMT
+    virtual int device_status() { return 0; }
     int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
     virtual ~EvaluatorBase() = default;
@@ -140,6 +143,10 @@ struct Evaluator final : EvaluatorBase {
     // M2L batches: pairs of all levels grouped by offset, in tiles
     DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
     int64_t ntiles = 0;
+    // tensor-core M2L (mixed form, p <= 8): tiles of 128 pairs and the table images
+    static constexpr bool kTensor = sizeof(T) == 4 && P <= 8;
+    DevBuf tc_tile_d, tc_tile_begin, tc_tile_count, tc_pair_e, tc_pair_src, tc_bimg, tc_error;
+    int64_t tc_ntiles = 0;
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64;
@@ -231,6 +238,7 @@ struct Evaluator final : EvaluatorBase {
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
         build_m2l_batches(kGemmPairs);
+        if (kTensor) build_tensor_m2l(m2l);
         build_p2p_items();
         if (kMixed) build_close_pairs(us, ut);
         close_pairs = nclose;
@@ -248,16 +256,38 @@ struct Evaluator final : EvaluatorBase {
 
     size_t gemm_smem = 0;
 
+    void build_tensor_m2l(const std::vector<double>& m2l) {
+        if constexpr (kTensor) {
+            std::vector<int32_t> td, tc, ps;
+            std::vector<int64_t> tb, pe;
+            batches(kTcRows, td, tb, tc, pe, ps);
+            tc_ntiles = (int64_t)td.size();
+            tc_tile_d.upload(td);
+            tc_tile_begin.upload(tb);
+            tc_tile_count.upload(tc);
+            tc_pair_e.upload(pe);
+            tc_pair_src.upload(ps);
+            std::vector<uint32_t> img;
+            build_tc_table_images<P>(m2l, img);
+            tc_bimg.upload(img);
+            tc_error.alloc(sizeof(int));
+            CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
+            CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          TcShape<P>::SMEM));
+        }
+    }
+
     // V pairs of every level grouped by offset index, then by target box; tiles of up
     // to `tile` pairs never straddle two offsets.
-    void build_m2l_batches(int tile) {
+    void batches(int tile, std::vector<int32_t>& td, std::vector<int64_t>& tb, std::vector<int32_t>& tc,
+                 std::vector<int64_t>& pe, std::vector<int32_t>& ps) {
         const Plan& pl = plan;
         const size_t nnz = pl.v.nnz();
         std::vector<int64_t> cnt(317, 0);
         for (size_t e2 = 0; e2 < nnz; ++e2) cnt[pl.v.aux[e2] + 1]++;
         for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
-        std::vector<int64_t> pe(nnz);
-        std::vector<int32_t> ps(nnz);
+        pe.assign(nnz, 0);
+        ps.assign(nnz, 0);
         std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
         // rows are boxes in order, so pairs of one offset come out ordered by target
         for (size_t b = 0; b + 1 < pl.v.row.size(); ++b)
@@ -266,14 +296,21 @@ struct Evaluator final : EvaluatorBase {
                 pe[pos] = e2;
                 ps[pos] = pl.v.col[e2];
             }
-        std::vector<int32_t> td, tc;
-        std::vector<int64_t> tb;
+        td.clear();
+        tb.clear();
+        tc.clear();
         for (int d = 0; d < 316; ++d)
             for (int64_t b = cnt[d]; b < cnt[d + 1]; b += tile) {
                 td.push_back(d);
                 tb.push_back(b);
                 tc.push_back((int32_t)std::min<int64_t>(tile, cnt[d + 1] - b));
             }
+    }
+
+    void build_m2l_batches(int tile) {
+        std::vector<int32_t> td, tc, ps;
+        std::vector<int64_t> tb, pe;
+        batches(tile, td, tb, tc, pe, ps);
         ntiles = (int64_t)td.size();
         tile_d.upload(td);
         tile_begin.upload(tb);
@@ -359,13 +396,23 @@ struct Evaluator final : EvaluatorBase {
         close.q = sq64.as<double>();
     }
 
+    int device_status() override {
+        if constexpr (kTensor) {
+            int err = 0;
+            CUDA_TRY(cudaMemcpy(&err, tc_error.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+            return err;
+        }
+        return 0;
+    }
+
     size_t device_bytes() const {
         const DevBuf* all[] = {&level, &idx, &parent, &child_first, &box_leaf, &src_below, &tgt_below,
                                &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
                                &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
                                &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
                                &Y, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
-                               &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64};
+                               &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
+                               &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -415,7 +462,18 @@ struct Evaluator final : EvaluatorBase {
                 });
         }
         // M2L products of every level at once (all multipoles are final here)
-        if (ntiles)
+        if (kTensor && m2l_path == 1) {
+            if constexpr (kTensor) {
+                if (tc_ntiles)
+                    timer.run(kM2L, [&] {
+                        m2l_tc_kernel<P><<<(unsigned)tc_ntiles, 128, TcShape<P>::SMEM, stream>>>(
+                            tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
+                            tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, tc_bimg.as<uint4>(),
+                            reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Y.ptr),
+                            tc_error.as<int>());
+                    });
+            }
+        } else if (ntiles)
             timer.run(kM2L, [&] {
                 m2l_gemm_kernel<P, T><<<(unsigned)ntiles, 256, gemm_smem, stream>>>(
                     tile_d.as<int32_t>(), tile_begin.as<int64_t>(), tile_count.as<int32_t>(), pair_e.as<int64_t>(),
@@ -650,6 +708,7 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
             CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
                                      f->stream));
         CUDA_TRY(cudaStreamSynchronize(f->stream));
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
     });
 }
 
@@ -659,6 +718,13 @@ int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* f, int on) {
     return guarded([&] {
         if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
         f->eval->timer.on = on != 0;
+    });
+}
+
+int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* f, int path) {
+    return guarded([&] {
+        if (!f || !f->eval || path < 0 || path > 1) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid M2L path");
+        f->eval->m2l_path = path;
     });
 }
 
@@ -683,6 +749,7 @@ int fmmgpu_fmm_synchronize(fmmgpu_fmm* f) {
         if (!f) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
         CUDA_TRY(cudaStreamSynchronize(f->stream));
         CUDA_TRY(cudaGetLastError());
+        if (f->eval && f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
     });
 }
 

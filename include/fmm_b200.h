@@ -102,6 +102,9 @@ int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* fmm, int on);
 /* Which parts the following evaluations run, for tests: bit 0 the near field (P2P),
  * bit 1 the far field (everything that reaches L2P and M2P); 3, the default, is the FMM. */
 int fmmgpu_fmm_set_kinds(fmmgpu_fmm* fmm, int kinds);
+/* Which M2L kernel the following evaluations use, for tests: 1 (default) the tensor-core
+ * kernel where the form has one (mixed precision, p <= 8), 0 the SIMT kernel. */
+int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* fmm, int path);
 /* Milliseconds of the last evaluation per kind: [0] charge load, [1] P2M, [2] M2M,
  * [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P + output pass.  Synchronises. */
 int fmmgpu_fmm_kind_times(fmmgpu_fmm* fmm, double* ms);

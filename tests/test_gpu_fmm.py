@@ -108,3 +108,22 @@ def test_near_and_far_fields_separately(oracle, precision, tol):
     print(precision, errs)
     for name, (ep, eg) in errs.items():
         assert ep < tol and eg < tol, (name, ep, eg)
+
+
+@pytest.mark.parametrize("p,mk", [(3, 32), (6, 32), (8, 64)])
+def test_mixed_tensor_core_m2l_matches_simt_and_oracle(oracle, p, mk):
+    """The tcgen05 (3xTF32) M2L against the f32 SIMT M2L and the f64 oracle."""
+    x, q = oracle.point_sets("sphere", 30000, 5)
+    fmm = F.FmmBuilder(p).gradients().max_points_per_leaf(mk).precision("mixed").build(x)
+    fmm.set_kinds(2)  # far field only: M2L dominates it
+    fmm.set_m2l_path(0)
+    simt = fmm.evaluate(q)
+    fmm.set_m2l_path(1)
+    tc = fmm.evaluate(q)
+    phi, g = oracle.fmm(x, q, x, p, mk, gradients=True, threads=8, kinds=2)
+    d_simt = rel(tc.potential, simt.potential)
+    e_tc, e_simt = rel(tc.potential, phi), rel(simt.potential, phi)
+    print(f"p={p}: tc vs simt {d_simt:.2e}, tc vs oracle {e_tc:.2e}, simt vs oracle {e_simt:.2e}, "
+          f"grad tc {rel(tc.gradient, g):.2e}")
+    assert d_simt < 2e-6
+    assert e_tc < 2e-6 and rel(tc.gradient, g) < 2e-6
