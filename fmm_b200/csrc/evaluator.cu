@@ -147,6 +147,7 @@ struct Evaluator final : EvaluatorBase {
     static constexpr bool kTensor = sizeof(T) == 4 && P <= 8;
     DevBuf tc_tile_d, tc_tile_begin, tc_tile_count, tc_pair_e, tc_pair_src, tc_bimg, tc_error;
     int64_t tc_ntiles = 0;
+    int num_sms = 148;
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64;
@@ -273,7 +274,10 @@ struct Evaluator final : EvaluatorBase {
             tc_error.alloc(sizeof(int));
             CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
             CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          TcShape<P>::SMEM));
+                                          TcShape2<P>::SMEM2));
+            int dev = 0;
+            CUDA_TRY(cudaGetDevice(&dev));
+            CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
         }
     }
 
@@ -466,11 +470,13 @@ struct Evaluator final : EvaluatorBase {
             if constexpr (kTensor) {
                 if (tc_ntiles)
                     timer.run(kM2L, [&] {
-                        m2l_tc_kernel<P><<<(unsigned)tc_ntiles, 128, TcShape<P>::SMEM, stream>>>(
-                            tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
-                            tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, tc_bimg.as<uint4>(),
-                            reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Y.ptr),
-                            tc_error.as<int>());
+                        const unsigned grid = (unsigned)std::min<int64_t>(tc_ntiles, num_sms);
+                        for (int v = 0; v < m; ++v)
+                            m2l_tc_kernel<P><<<grid, 128, TcShape2<P>::SMEM2, stream>>>(
+                                tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
+                                tc_ntiles, tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v,
+                                tc_bimg.as<uint4>(), reinterpret_cast<const float*>(M.ptr),
+                                reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
                     });
             }
         } else if (ntiles)

@@ -127,62 +127,127 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
     return false;
 }
 
+// Persistent form: CTA c takes the contiguous range of tiles [c T / G, (c + 1) T / G) of
+// the offset-sorted tile list, so the table image changes only a few times per CTA.
+// Per tile i, in order:
+//   wait MMA(i-1) (A and TMEM buffer (i-1)&1 are then readable / reusable),
+//   convert the raw rows of tile i (staging, arrived by cp.async) to hi/lo SW128 A,
+//   issue the cp.async gather of tile i+1 into staging,
+//   thread 0 issues MMA(i) into TMEM buffer i&1 and commits to the barrier,
+//   epilogue of tile i-1 from TMEM buffer (i-1)&1 to Y, overlapping MMA(i).
+// One vector per launch (the caller launches once per charge vector).
+template <int P>
+struct TcShape2 : TcShape<P> {
+    static constexpr int NCS = ((TcShape<P>::NC + 3) / 4) * 4;          // staging row stride (floats)
+    static constexpr int STAGE_BYTES = kTcRows * NCS * 4;
+    static constexpr int SMEM2 = 2 * TcShape<P>::A_BYTES + 2 * TcShape<P>::B_BYTES + STAGE_BYTES + 1024 + 64;
+};
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <int P>
 __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
                                                         const int64_t* __restrict__ tile_begin,
                                                         const int32_t* __restrict__ tile_count,
-                                                        const int64_t* __restrict__ pair_e,
-                                                        const int32_t* __restrict__ pair_src, int m,
+                                                        int64_t ntiles, const int64_t* __restrict__ pair_e,
+                                                        const int32_t* __restrict__ pair_src, int m, int v,
                                                         const uint4* __restrict__ bimg,  // [316][2][B_BYTES/16]
                                                         const float* __restrict__ M, float* __restrict__ Y,
                                                         int* __restrict__ error) {
-    using S = TcShape<P>;
+    using S = TcShape2<P>;
     constexpr int NC = S::NC;
     extern __shared__ unsigned char smem_raw[];
-    // 1024-byte aligned operand region (the swizzle repeats every 1024 B)
     unsigned char* base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     unsigned char* a_hi = base;
     unsigned char* a_lo = a_hi + S::A_BYTES;
     unsigned char* b_hi = a_lo + S::A_BYTES;
     unsigned char* b_lo = b_hi + S::B_BYTES;
+    float* stage = reinterpret_cast<float*>(b_lo + S::B_BYTES);
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
-    const int d = tile_d[tile];
-    const int64_t p0 = tile_begin[tile];
-    const int cnt = tile_count[tile];
+    const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
+    const int64_t i1 = (int64_t)(blockIdx.x + 1) * ntiles / gridDim.x;
+    if (i0 >= i1) return;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                     "r"(S::TMEM_COLS));
+                     "r"(2 * S::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    // table images: a verbatim copy (hi then lo), 16 B per thread per step
-    {
-        const uint4* src = bimg + (size_t)d * (2 * S::B_BYTES / 16);
-        uint4* dst = reinterpret_cast<uint4*>(b_hi);  // b_lo follows b_hi
-        for (int i = tid; i < 2 * S::B_BYTES / 16; i += 128) dst[i] = src[i];
-    }
+    const uint32_t stage_s = smem_u32(stage);
+    auto gather = [&](int64_t it) {  // raw rows of tile `it` into staging (async)
+        const int64_t p0 = tile_begin[it];
+        const int cnt = tile_count[it];
+        for (int r = warp; r < cnt; r += 4) {
+            const float* src = M + ((int64_t)pair_src[p0 + r] * m + v) * NC;
+            for (int k = lane; k < NC; k += 32) cp_async4(stage_s + (uint32_t)(r * S::NCS + k) * 4, src + k);
+        }
+        cp_async_commit();
+    };
+    gather(i0);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = tf32_idesc<S::NP>();
+    int cur_d = -1;
+    uint32_t phase = 0;
     bool failed = false;
+    int64_t prev_p0 = 0;
+    int prev_cnt = 0;
 
-    for (int v = 0; v < m; ++v) {
-        // gather: warp w fills rows w, w+4, ...; lane = column within a 32-column atom
+    auto epilogue = [&](int buf, int64_t p0, int cnt) {
+        const int r = 32 * warp + lane;
+        float* y = r < cnt ? Y + (pair_e[p0 + r] * m + v) * NC : nullptr;
+#pragma unroll
+        for (int c0 = 0; c0 < S::NP; c0 += 16) {
+            float vals[16];
+            tmem_ld16(tmem + (uint32_t)(buf * S::TMEM_COLS) + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, vals);
+            if (y) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (c0 + i < NC) y[c0 + i] = vals[i];
+            }
+        }
+    };
+
+    for (int64_t it = i0; it < i1 && !failed; ++it) {
+        const int buf = (int)((it - i0) & 1);
+        // MMA(it-1) must be done before A (and, on an offset change, B) is overwritten
+        if (it > i0) {
+            const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
+            if (__syncthreads_or(!ok)) {  // the CTA leaves together, so no barrier is left waiting
+                failed = true;
+                if (tid == 0) atomicExch(error, 1);
+                break;
+            }
+            phase ^= 1;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+        }
+        const int d = tile_d[it];
+        if (d != cur_d) {
+            const uint4* src = bimg + (size_t)d * (2 * S::B_BYTES / 16);
+            uint4* dst = reinterpret_cast<uint4*>(b_hi);
+            for (int i = tid; i < 2 * S::B_BYTES / 16; i += 128) dst[i] = src[i];
+            cur_d = d;
+        }
+        cp_async_wait_all();
+        __syncthreads();  // staging of tile `it` complete for every thread
+        const int cnt = tile_count[it];
         for (int r = warp; r < kTcRows; r += 4) {
-            const float* src = r < cnt ? M + ((int64_t)pair_src[p0 + r] * m + v) * NC : nullptr;
 #pragma unroll
             for (int a = 0; a < S::KA; ++a) {
                 const int k = a * 32 + lane;
-                const float x = (src && k < NC) ? src[k] : 0.0f;
+                const float x = (r < cnt && k < NC) ? stage[r * S::NCS + k] : 0.0f;
                 const uint32_t hi = cvt_tf32(x);
                 const uint32_t lo = cvt_tf32(x - __uint_as_float(hi));
                 const uint32_t off = sw128_offset(r, k, kTcRows);
@@ -191,13 +256,15 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();  // A complete; staging free
+        if (it + 1 < i1) gather(it + 1);
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t sa_hi = smem_u32(a_hi), sa_lo = smem_u32(a_lo);
             const uint32_t sb_hi = smem_u32(b_hi), sb_lo = smem_u32(b_lo);
+            const uint32_t dcol = tmem + (uint32_t)(buf * S::TMEM_COLS);
             uint32_t acc = 0;
-            // lo * hi, hi * lo, then hi * hi
             const uint32_t As[3] = {sa_lo, sa_hi, sa_hi}, Bs[3] = {sb_hi, sb_lo, sb_hi};
 #pragma unroll
             for (int t = 0; t < 3; ++t)
@@ -205,7 +272,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
                 for (int s = 0; s < S::KSTEPS; ++s) {
                     const uint32_t ka = (uint32_t)((s >> 2) * kTcRows * 128 + (s & 3) * 32);
                     const uint32_t kb = (uint32_t)((s >> 2) * S::NP * 128 + (s & 3) * 32);
-                    umma_tf32(tmem, sw128_desc(As[t] + ka), sw128_desc(Bs[t] + kb), idesc, acc);
+                    umma_tf32(dcol, sw128_desc(As[t] + ka), sw128_desc(Bs[t] + kb), idesc, acc);
                     acc = 1;
                 }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -213,33 +280,26 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
                          : "memory");
         }
         __syncwarp();
-        if (!mbar_wait_bounded(smem_u32(&mbar), (uint32_t)(v & 1), 4000000000LL)) {  // ~2 s
-            failed = true;
-            if (lane == 0) atomicExch(error, 1);
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        if (!failed) {
-            // epilogue: warp w reads TMEM lanes 32w..32w+31 (= pairs), 16 columns at a time
-            const int r = 32 * warp + lane;
-            float* y = r < cnt ? Y + (pair_e[p0 + r] * m + v) * NC : nullptr;
-#pragma unroll
-            for (int c0 = 0; c0 < S::NP; c0 += 16) {
-                float vals[16];
-                tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, vals);
-                if (y) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                        if (c0 + i < NC) y[c0 + i] = vals[i];
-                }
-            }
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();  // TMEM and A are reused by the next vector
-        if (failed) break;
+        // epilogue of the previous tile overlaps this tile's MMA
+        if (it > i0) epilogue(buf ^ 1, prev_p0, prev_cnt);
+        prev_p0 = tile_begin[it];
+        prev_cnt = cnt;
     }
+    if (!failed) {
+        const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(error, 1);
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            epilogue((int)((i1 - 1 - i0) & 1), prev_p0, prev_cnt);
+        }
+    }
+    cp_async_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * S::TMEM_COLS));
     }
 }
 
