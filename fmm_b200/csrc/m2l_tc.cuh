@@ -140,8 +140,12 @@ template <int P>
 struct TcShape2 : TcShape<P> {
     static constexpr int NCS = ((TcShape<P>::NC + 3) / 4) * 4;          // staging row stride (floats)
     static constexpr int STAGE_BYTES = kTcRows * NCS * 4;
-    static constexpr int SMEM2 = 2 * TcShape<P>::A_BYTES + 2 * TcShape<P>::B_BYTES + STAGE_BYTES + 1024 + 64;
+    static constexpr int OUT_BYTES = 4 * 32 * 17 * 4;                    // per-warp 32 x 16 epilogue tiles
+    static constexpr int SMEM2 =
+        2 * TcShape<P>::A_BYTES + 2 * TcShape<P>::B_BYTES + STAGE_BYTES + OUT_BYTES + 1024 + 64;
 };
+
+__device__ __forceinline__ int warp_of_thread() { return threadIdx.x >> 5; }
 
 __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
@@ -167,6 +171,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
     unsigned char* b_hi = a_lo + S::A_BYTES;
     unsigned char* b_lo = b_hi + S::B_BYTES;
     float* stage = reinterpret_cast<float*>(b_lo + S::B_BYTES);
+    float* outw = reinterpret_cast<float*>(b_lo + S::B_BYTES + S::STAGE_BYTES) + warp_of_thread() * 32 * 17;
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -205,18 +210,27 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
     int64_t prev_p0 = 0;
     int prev_cnt = 0;
 
+    // epilogue: warp w owns TMEM lanes (pairs) 32w..32w+31.  Each 32 x 16 block of D goes
+    // through the warp's shared tile so that stores run along Y rows (two rows of 16
+    // floats per instruction) instead of one 324-byte row per lane.
     auto epilogue = [&](int buf, int64_t p0, int cnt) {
-        const int r = 32 * warp + lane;
-        float* y = r < cnt ? Y + (pair_e[p0 + r] * m + v) * NC : nullptr;
-#pragma unroll
+        const int rw = 32 * warp;
+        const int half = lane >> 4, col = lane & 15;
+#pragma unroll 1
         for (int c0 = 0; c0 < S::NP; c0 += 16) {
             float vals[16];
-            tmem_ld16(tmem + (uint32_t)(buf * S::TMEM_COLS) + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, vals);
-            if (y) {
+            tmem_ld16(tmem + (uint32_t)(buf * S::TMEM_COLS) + ((uint32_t)rw << 16) + (uint32_t)c0, vals);
 #pragma unroll
-                for (int i = 0; i < 16; ++i)
-                    if (c0 + i < NC) y[c0 + i] = vals[i];
+            for (int i = 0; i < 16; ++i) outw[lane * 17 + i] = vals[i];
+            __syncwarp();
+            if (c0 + col < NC) {
+#pragma unroll 4
+                for (int rr = half; rr < 32; rr += 2) {
+                    const int r = rw + rr;
+                    if (r < cnt) Y[(pair_e[p0 + r] * m + v) * NC + c0 + col] = outw[rr * 17 + col];
+                }
             }
+            __syncwarp();
         }
     };
 
