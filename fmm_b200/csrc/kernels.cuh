@@ -47,19 +47,31 @@ struct DevPlan {
     int64_t nsrc, ntgt;
 };
 
+// 2^e for |e| <= 126, built from the exponent field (exact, no library call)
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
+__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
+template <typename T>
+__device__ __forceinline__ T pow2(int e);
+template <>
+__device__ __forceinline__ float pow2<float>(int e) { return pow2f(e); }
+template <>
+__device__ __forceinline__ double pow2<double>(int e) { return pow2d(e); }
+
 // relative frame of box s seen from box t (CONVENTIONS 3.13 "Relative frames"):
-// c = (C_L(s) - C_L(t)) 2^(l_t - L), r = 2^(l_t - l_s); exact in f32 and f64.
+// c = (C_L(s) - C_L(t)) 2^(l_t - L), r = 2^(l_t - l_s); exact in f32 and f64 (the
+// integer difference has at most 17 bits and the scale is a power of two).
 template <typename T>
 __device__ __forceinline__ void rel_frame(const DevPlan& P, int s, int t, T c[3], T& r) {
     int ls = P.level[s], lt = P.level[t];
     int L = ls > lt ? ls : lt;
+    const T scale = pow2<T>(lt - L);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        long long Cs = (2LL * P.idx[3 * s + k] + 1) << (L - ls);
-        long long Ct = (2LL * P.idx[3 * t + k] + 1) << (L - lt);
-        c[k] = (T)ldexp((double)(Cs - Ct), lt - L);
+        int Cs = (int)((2u * P.idx[3 * s + k] + 1u) << (L - ls));
+        int Ct = (int)((2u * P.idx[3 * t + k] + 1u) << (L - lt));
+        c[k] = (T)(Cs - Ct) * scale;
     }
-    r = (T)ldexp(1.0, lt - ls);
+    r = pow2<T>(lt - ls);
 }
 
 // ---------------------------------------------------------------------------------
@@ -551,7 +563,7 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
         ty = p4.y;
         tz = p4.z;
     }
-    const double rt = ldexp(plan.side, -(plan.level[box] + 1));
+    const double rt = plan.side * pow2d(-(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;
     const double g_scale = phi_scale * rt;
     for (int v = 0; v < m; ++v) {

@@ -174,6 +174,8 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
     float* outw = reinterpret_cast<float*>(b_lo + S::B_BYTES + S::STAGE_BYTES) + warp_of_thread() * 32 * 17;
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
+    __shared__ int32_t row_src[kTcRows];   // source box of each row of the tile being gathered
+    __shared__ int64_t row_e[2][kTcRows];  // Y row of each row, per TMEM buffer
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
     const int64_t i1 = (int64_t)(blockIdx.x + 1) * ntiles / gridDim.x;
@@ -189,11 +191,15 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     const uint32_t stage_s = smem_u32(stage);
-    auto gather = [&](int64_t it) {  // raw rows of tile `it` into staging (async)
+    // raw rows of tile `it` into staging (async); the rows' source boxes are loaded once,
+    // coalesced, into shared memory (one thread per row) before any copy is issued
+    auto gather = [&](int64_t it) {
         const int64_t p0 = tile_begin[it];
         const int cnt = tile_count[it];
+        row_src[tid] = tid < cnt ? pair_src[p0 + tid] : 0;
+        __syncthreads();
         for (int r = warp; r < cnt; r += 4) {
-            const float* src = M + ((int64_t)pair_src[p0 + r] * m + v) * NC;
+            const float* src = M + ((int64_t)row_src[r] * m + v) * NC;
             for (int k = lane; k < NC; k += 32) cp_async4(stage_s + (uint32_t)(r * S::NCS + k) * 4, src + k);
         }
         cp_async_commit();
@@ -207,13 +213,12 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
     int cur_d = -1;
     uint32_t phase = 0;
     bool failed = false;
-    int64_t prev_p0 = 0;
     int prev_cnt = 0;
 
     // epilogue: warp w owns TMEM lanes (pairs) 32w..32w+31.  Each 32 x 16 block of D goes
     // through the warp's shared tile so that stores run along Y rows (two rows of 16
     // floats per instruction) instead of one 324-byte row per lane.
-    auto epilogue = [&](int buf, int64_t p0, int cnt) {
+    auto epilogue = [&](int buf, int cnt) {
         const int rw = 32 * warp;
         const int half = lane >> 4, col = lane & 15;
 #pragma unroll 1
@@ -227,7 +232,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
 #pragma unroll 4
                 for (int rr = half; rr < 32; rr += 2) {
                     const int r = rw + rr;
-                    if (r < cnt) Y[(pair_e[p0 + r] * m + v) * NC + c0 + col] = outw[rr * 17 + col];
+                    if (r < cnt) Y[(row_e[buf][r] * m + v) * NC + c0 + col] = outw[rr * 17 + col];
                 }
             }
             __syncwarp();
@@ -269,6 +274,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
                 *reinterpret_cast<uint32_t*>(a_lo + off) = lo;
             }
         }
+        row_e[buf][tid] = tid < cnt ? pair_e[tile_begin[it] + tid] : 0;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();  // A complete; staging free
@@ -295,8 +301,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
         }
         __syncwarp();
         // epilogue of the previous tile overlaps this tile's MMA
-        if (it > i0) epilogue(buf ^ 1, prev_p0, prev_cnt);
-        prev_p0 = tile_begin[it];
+        if (it > i0) epilogue(buf ^ 1, prev_cnt);
         prev_cnt = cnt;
     }
     if (!failed) {
@@ -305,7 +310,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
             if (tid == 0) atomicExch(error, 1);
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            epilogue((int)((i1 - 1 - i0) & 1), prev_p0, prev_cnt);
+            epilogue((int)((i1 - 1 - i0) & 1), prev_cnt);
         }
     }
     cp_async_wait_all();
