@@ -472,7 +472,7 @@ struct Evaluator final : EvaluatorBase {
                     timer.run(kM2L, [&] {
                         const unsigned grid = (unsigned)std::min<int64_t>(tc_ntiles, num_sms);
                         for (int v = 0; v < m; ++v)
-                            m2l_tc_kernel<P><<<grid, 128, TcShape2<P>::SMEM2, stream>>>(
+                            m2l_tc_kernel<P><<<grid, 32 * kTcWarps, TcShape2<P>::SMEM2, stream>>>(
                                 tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
                                 tc_ntiles, tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v,
                                 tc_bimg.as<uint4>(), reinterpret_cast<const float*>(M.ptr),

@@ -129,54 +129,42 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
 
 // Persistent form: CTA c takes the contiguous range of tiles [c T / G, (c + 1) T / G) of
 // the offset-sorted tile list, so the table image changes only a few times per CTA.
-// Per tile i, in order:
-//   wait MMA(i-1) (A and TMEM buffer (i-1)&1 are then readable / reusable),
-//   convert the raw rows of tile i (staging, arrived by cp.async) to hi/lo SW128 A,
-//   issue the cp.async gather of tile i+1 into staging,
-//   thread 0 issues MMA(i) into TMEM buffer i&1 and commits to the barrier,
-//   epilogue of tile i-1 from TMEM buffer (i-1)&1 to Y, overlapping MMA(i).
-// One vector per launch (the caller launches once per charge vector).
+// 16 warps: all of them gather (loads of a warp's 8 rows issued before use) and convert
+// A; thread 0 issues the MMAs; the epilogue of tile i-1 (TMEM buffer (i-1)&1, read by
+// the 4 warps of each TMEM lane quarter, 16 columns at a time, staged per warp so that
+// stores run along Y rows) overlaps MMA(i) into buffer i&1.  One vector per launch.
+constexpr int kTcWarps = 16;
+
 template <int P>
 struct TcShape2 : TcShape<P> {
-    static constexpr int NCS = ((TcShape<P>::NC + 3) / 4) * 4;          // staging row stride (floats)
-    static constexpr int STAGE_BYTES = kTcRows * NCS * 4;
-    static constexpr int OUT_BYTES = 4 * 32 * 17 * 4;                    // per-warp 32 x 16 epilogue tiles
-    static constexpr int SMEM2 =
-        2 * TcShape<P>::A_BYTES + 2 * TcShape<P>::B_BYTES + STAGE_BYTES + OUT_BYTES + 1024 + 64;
+    static constexpr int OUT_BYTES = kTcWarps * 32 * 17 * 4;  // per-warp 32 x 16 epilogue tiles
+    static constexpr int SMEM2 = 2 * TcShape<P>::A_BYTES + 2 * TcShape<P>::B_BYTES + OUT_BYTES + 1024 + 64;
 };
 
-__device__ __forceinline__ int warp_of_thread() { return threadIdx.x >> 5; }
-
-__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 template <int P>
-__global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
-                                                        const int64_t* __restrict__ tile_begin,
-                                                        const int32_t* __restrict__ tile_count,
-                                                        int64_t ntiles, const int64_t* __restrict__ pair_e,
-                                                        const int32_t* __restrict__ pair_src, int m, int v,
-                                                        const uint4* __restrict__ bimg,  // [316][2][B_BYTES/16]
-                                                        const float* __restrict__ M, float* __restrict__ Y,
-                                                        int* __restrict__ error) {
+__global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
+                                                                  const int64_t* __restrict__ tile_begin,
+                                                                  const int32_t* __restrict__ tile_count,
+                                                                  int64_t ntiles, const int64_t* __restrict__ pair_e,
+                                                                  const int32_t* __restrict__ pair_src, int m, int v,
+                                                                  const uint4* __restrict__ bimg,
+                                                                  const float* __restrict__ M, float* __restrict__ Y,
+                                                                  int* __restrict__ error) {
     using S = TcShape2<P>;
     constexpr int NC = S::NC;
+    constexpr int RPW = kTcRows / kTcWarps;  // rows per warp in the gather
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     unsigned char* a_hi = base;
     unsigned char* a_lo = a_hi + S::A_BYTES;
     unsigned char* b_hi = a_lo + S::A_BYTES;
     unsigned char* b_lo = b_hi + S::B_BYTES;
-    float* stage = reinterpret_cast<float*>(b_lo + S::B_BYTES);
-    float* outw = reinterpret_cast<float*>(b_lo + S::B_BYTES + S::STAGE_BYTES) + warp_of_thread() * 32 * 17;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float* outw = reinterpret_cast<float*>(b_lo + S::B_BYTES) + warp * 32 * 17;
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __shared__ int32_t row_src[kTcRows];   // source box of each row of the tile being gathered
-    __shared__ int64_t row_e[2][kTcRows];  // Y row of each row, per TMEM buffer
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    __shared__ int32_t row_src[kTcRows];
+    __shared__ int64_t row_e[2][kTcRows];
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
     const int64_t i1 = (int64_t)(blockIdx.x + 1) * ntiles / gridDim.x;
     if (i0 >= i1) return;
@@ -190,21 +178,6 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    const uint32_t stage_s = smem_u32(stage);
-    // raw rows of tile `it` into staging (async); the rows' source boxes are loaded once,
-    // coalesced, into shared memory (one thread per row) before any copy is issued
-    auto gather = [&](int64_t it) {
-        const int64_t p0 = tile_begin[it];
-        const int cnt = tile_count[it];
-        row_src[tid] = tid < cnt ? pair_src[p0 + tid] : 0;
-        __syncthreads();
-        for (int r = warp; r < cnt; r += 4) {
-            const float* src = M + ((int64_t)row_src[r] * m + v) * NC;
-            for (int k = lane; k < NC; k += 32) cp_async4(stage_s + (uint32_t)(r * S::NCS + k) * 4, src + k);
-        }
-        cp_async_commit();
-    };
-    gather(i0);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -215,14 +188,11 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
     bool failed = false;
     int prev_cnt = 0;
 
-    // epilogue: warp w owns TMEM lanes (pairs) 32w..32w+31.  Each 32 x 16 block of D goes
-    // through the warp's shared tile so that stores run along Y rows (two rows of 16
-    // floats per instruction) instead of one 324-byte row per lane.
     auto epilogue = [&](int buf, int cnt) {
-        const int rw = 32 * warp;
+        const int quarter = warp & 3;        // TMEM lanes 32 quarter .. + 31
+        const int rw = 32 * quarter;
         const int half = lane >> 4, col = lane & 15;
-#pragma unroll 1
-        for (int c0 = 0; c0 < S::NP; c0 += 16) {
+        for (int c0 = 16 * (warp >> 2); c0 < S::NP; c0 += 16 * (kTcWarps / 4)) {
             float vals[16];
             tmem_ld16(tmem + (uint32_t)(buf * S::TMEM_COLS) + ((uint32_t)rw << 16) + (uint32_t)c0, vals);
 #pragma unroll
@@ -241,8 +211,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
 
     for (int64_t it = i0; it < i1 && !failed; ++it) {
         const int buf = (int)((it - i0) & 1);
-        // MMA(it-1) must be done before A (and, on an offset change, B) is overwritten
-        if (it > i0) {
+        if (it > i0) {  // MMA(it-1) done: A and B may be overwritten
             const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
             if (__syncthreads_or(!ok)) {  // the CTA leaves together, so no barrier is left waiting
                 failed = true;
@@ -253,32 +222,47 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
             asm volatile("tcgen05.fence::after_thread_sync;");
         }
         const int d = tile_d[it];
+        const int64_t p0 = tile_begin[it];
+        const int cnt = tile_count[it];
         if (d != cur_d) {
             const uint4* src = bimg + (size_t)d * (2 * S::B_BYTES / 16);
             uint4* dst = reinterpret_cast<uint4*>(b_hi);
-            for (int i = tid; i < 2 * S::B_BYTES / 16; i += 128) dst[i] = src[i];
+            for (int i = tid; i < 2 * S::B_BYTES / 16; i += 32 * kTcWarps) dst[i] = src[i];
             cur_d = d;
         }
-        cp_async_wait_all();
-        __syncthreads();  // staging of tile `it` complete for every thread
-        const int cnt = tile_count[it];
-        for (int r = warp; r < kTcRows; r += 4) {
+        if (tid < kTcRows) {
+            row_src[tid] = tid < cnt ? pair_src[p0 + tid] : 0;
+            row_e[buf][tid] = tid < cnt ? pair_e[p0 + tid] : 0;
+        }
+        __syncthreads();
+        // gather + split: warp w holds rows w + 16 j; every load is issued before any use
+        float x[RPW][S::KA];
+#pragma unroll
+        for (int j = 0; j < RPW; ++j) {
+            const int r = warp + kTcWarps * j;
+            const float* src = M + ((int64_t)row_src[r] * m + v) * NC;
 #pragma unroll
             for (int a = 0; a < S::KA; ++a) {
                 const int k = a * 32 + lane;
-                const float x = (r < cnt && k < NC) ? stage[r * S::NCS + k] : 0.0f;
-                const uint32_t hi = cvt_tf32(x);
-                const uint32_t lo = cvt_tf32(x - __uint_as_float(hi));
+                x[j][a] = (r < cnt && k < NC) ? __ldg(src + k) : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RPW; ++j) {
+            const int r = warp + kTcWarps * j;
+#pragma unroll
+            for (int a = 0; a < S::KA; ++a) {
+                const int k = a * 32 + lane;
+                const uint32_t hi = cvt_tf32(x[j][a]);
+                const uint32_t lo = cvt_tf32(x[j][a] - __uint_as_float(hi));
                 const uint32_t off = sw128_offset(r, k, kTcRows);
                 *reinterpret_cast<uint32_t*>(a_hi + off) = hi;
                 *reinterpret_cast<uint32_t*>(a_lo + off) = lo;
             }
         }
-        row_e[buf][tid] = tid < cnt ? pair_e[tile_begin[it] + tid] : 0;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();  // A complete; staging free
-        if (it + 1 < i1) gather(it + 1);
+        __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t sa_hi = smem_u32(a_hi), sa_lo = smem_u32(a_lo);
@@ -300,8 +284,7 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
                          : "memory");
         }
         __syncwarp();
-        // epilogue of the previous tile overlaps this tile's MMA
-        if (it > i0) epilogue(buf ^ 1, prev_cnt);
+        if (it > i0) epilogue(buf ^ 1, prev_cnt);  // overlaps MMA(it)
         prev_cnt = cnt;
     }
     if (!failed) {
@@ -313,7 +296,6 @@ __global__ void __launch_bounds__(128, 1) m2l_tc_kernel(const int32_t* __restric
             epilogue((int)((i1 - 1 - i0) & 1), prev_cnt);
         }
     }
-    cp_async_wait_all();
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) {
