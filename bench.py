@@ -109,7 +109,7 @@ class Clocks:
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -139,6 +139,15 @@ class Clocks:
                     "samples": len(rows)}
         except Exception as e:  # no nvidia-smi or no samples
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)[:80]}
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per work unit of `kernel` from a committed ncu summary (profiles/), or None."""
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))[kernel]
+        return t
+    except Exception:
+        return None
 
 
 def peaks():
@@ -280,6 +289,10 @@ def run_ours(args):
                                     "(no FP32 peak in MEASURED_PEAKS.json)",
                      "op_model": "15 FP32 lane-ops per pair (fmm-validate/src/peaks.rs:12-17)",
                      "traffic": None})
+        t = ncu_traffic("p2p_kernel")
+        if t:
+            roof["traffic"] = round(t["dram_bytes_per_unit"] * info["near_pairs"])
+            roof["traffic_source"] = t["source"]
     else:
         roof.update({"bound": "unknown", "achieved": None, "peak": None, "unit": None, "frac": None,
                      "traffic": None})
@@ -375,8 +388,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--cpu-n", type=int, default=400_000)

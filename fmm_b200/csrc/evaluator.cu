@@ -155,6 +155,8 @@ struct Evaluator final : EvaluatorBase {
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
+    static constexpr bool kBfly = sizeof(T) == 4;  // register P2M/P2L (f32, one vector)
+    static constexpr size_t group_smem = sizeof(T) * ((size_t)NC * NC + (size_t)kGroup * NC);
     // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
     static constexpr float kTheta2 = 0.0625f;
 
@@ -245,6 +247,10 @@ struct Evaluator final : EvaluatorBase {
         close_pairs = nclose;
         Y.alloc(sizeof(T) * (size_t)m * NC * (pl.v.nnz() + 1));
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
+        if (group_smem > 48 * 1024) {
+            CUDA_TRY(cudaFuncSetAttribute(m2m_group_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
+            CUDA_TRY(cudaFuncSetAttribute(local_group_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
+        }
         if (gemm_smem > 48 * 1024)
             CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
         // shared memory opt-in beyond 48 KB where a kernel needs it
@@ -453,15 +459,21 @@ struct Evaluator final : EvaluatorBase {
         // upward: P2M of every leaf, then M2M from level L-1 up to 0
         const size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
         timer.run(kP2M, [&] {
-            if (nleaves)
-                expand_kernel<P, T, false><<<(unsigned)nleaves, 32, exp_smem, stream>>>(
-                    dp, 0, (int64_t)nleaves, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
+            if (nleaves) {
+                if (kBfly && m == 1)
+                    expand_bfly_kernel<P, false><<<(unsigned)nleaves, 32, 0, stream>>>(
+                        dp, 0, (int64_t)nleaves, reinterpret_cast<const float4*>(spos.ptr),
+                        reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
+                else
+                    expand_kernel<P, T, false><<<(unsigned)nleaves, 32, exp_smem, stream>>>(
+                        dp, 0, (int64_t)nleaves, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
+            }
         });
         for (int l = L - 1; l >= 0; --l) {
             int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
             if (b1 > b0)
                 timer.run(kM2M, [&] {
-                    m2m_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), 8 * NC * sizeof(T), stream>>>(
+                    m2m_group_kernel<P, T><<<(unsigned)((b1 - b0 + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
                         dp, b0, b1, m, m2m_tab.as<T>(), M.as<T>());
                 });
         }
@@ -488,13 +500,19 @@ struct Evaluator final : EvaluatorBase {
         // downward: for l = 2..L: L2L + V (one kernel), then P2L
         for (int l = 2; l <= L; ++l) {
             int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+            int64_t p0 = plan.level_start[l - 1], p1 = plan.level_start[l];
             timer.run(kL2L, [&] {
-                local_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), NC * sizeof(T), stream>>>(
-                    dp, b0, b1, m, l >= 3, l2l_tab.as<T>(), Y.as<T>(), Lc.as<T>());
+                local_group_kernel<P, T><<<(unsigned)((p1 - p0 + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
+                    dp, p0, p1, m, l >= 3, l2l_tab.as<T>(), Y.as<T>(), Lc.as<T>());
             });
             timer.run(kP2L, [&] {
-                expand_kernel<P, T, true><<<(unsigned)(b1 - b0), 32, exp_smem, stream>>>(
-                    dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
+                if (kBfly && m == 1)
+                    expand_bfly_kernel<P, true><<<(unsigned)(b1 - b0), 32, 0, stream>>>(
+                        dp, b0, b1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
+                        reinterpret_cast<float*>(Lc.ptr));
+                else
+                    expand_kernel<P, T, true><<<(unsigned)(b1 - b0), 32, exp_smem, stream>>>(
+                        dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
             });
         }
         // leaves: L2P + M2P

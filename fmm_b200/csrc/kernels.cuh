@@ -184,38 +184,208 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
 }
 
 // ---------------------------------------------------------------------------------
-// M2M on one level: parent (level l) = sum over children by octant of T_o * M_child.
-// Block per parent; thread per output slot.  Parents with no source below are skipped
-// (their multipole stays zero and no list names them).
+// P2M / P2L, f32 single-vector form: one warp per row; lane j takes source points
+// j, j+32, ... of every entry and accumulates q conj(X) for all (p+1)^2 slots in
+// registers; one butterfly reduce-scatter per row then leaves every lane with
+// NCP/32 finished slots (NCP = slots padded to a multiple of 32).  The summation order
+// is fixed (per-lane partial sums, then a fixed tree), so results are repeatable.
 // ---------------------------------------------------------------------------------
+template <int P, bool IRREG>
+__global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
+                                                         const float4* __restrict__ spos,
+                                                         const float* __restrict__ sq, float* __restrict__ out) {
+    constexpr int NC = nc_of(P);
+    constexpr int NCP = ((NC + 31) / 32) * 32;
+    const int lane = threadIdx.x;
+    const int64_t row = row_begin + blockIdx.x;
+    if (row >= row_end) return;
+    int box, nent;
+    int64_t ent0;
+    if (!IRREG) {
+        box = plan.leaf_box[row];
+        nent = 1;
+        ent0 = 0;
+        if (plan.src_below[box] == 0) return;
+    } else {
+        box = (int)row;
+        ent0 = plan.x_row[row];
+        nent = (int)(plan.x_row[row + 1] - ent0);
+        if (nent == 0) return;
+    }
+    float w[NCP];
+#pragma unroll
+    for (int c = 0; c < NCP; ++c) w[c] = 0.0f;
+    for (int e = 0; e < nent; ++e) {
+        const int sleaf = IRREG ? plan.x_col[ent0 + e] : (int)row;
+        float fc[3] = {0.0f, 0.0f, 0.0f}, fr = 1.0f;
+        if (IRREG) rel_frame<float>(plan, box, plan.leaf_box[sleaf], fc, fr);  // (c(t|s), r(t|s))
+        const float finv = 1.0f / fr;
+        const int64_t s1 = plan.src_start[sleaf + 1];
+        for (int64_t si = plan.src_start[sleaf] + lane; si < s1; si += 32) {
+            const float4 p4 = spos[si];
+            const float q = sq[si];
+            const float x = (p4.x - fc[0]) * finv, y = (p4.y - fc[1]) * finv, z = (p4.z - fc[2]) * finv;
+            if (!IRREG) {
+                RegularRows<P, float> h;
+                h.init(x, y, z);
+#pragma unroll
+                for (int n = 0; n <= P; ++n) {
+                    h.step(n);
+#pragma unroll
+                    for (int mm = 0; mm <= n; ++mm) {
+                        w[slot(n, mm)] += q * h.cre[mm];
+                        if (mm) w[slot(n, -mm)] -= q * h.cim[mm];
+                    }
+                }
+            } else {
+                IrregularRows<P, float> h;
+                h.init(x, y, z, rsqrtf(x * x + y * y + z * z));
+#pragma unroll
+                for (int n = 0; n <= P; ++n) {
+                    h.step(n);
+#pragma unroll
+                    for (int mm = 0; mm <= n; ++mm) {
+                        w[slot(n, mm)] += q * h.cre[mm];
+                        if (mm) w[slot(n, -mm)] -= q * h.cim[mm];
+                    }
+                }
+            }
+        }
+    }
+    // reduce-scatter: after the step with offset s a lane keeps the half of its slots
+    // selected by its bit s and adds the partner's copy of that half
+#pragma unroll
+    for (int s = 16, len = NCP / 2; s >= 1; s >>= 1, len >>= 1) {
+        const bool upper = lane & s;
+#pragma unroll
+        for (int i = 0; i < len; ++i) {
+            const float send = upper ? w[i] : w[i + len];
+            const float keep = upper ? w[i + len] : w[i];
+            w[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+        }
+    }
+    int base = 0;
+#pragma unroll
+    for (int s = 16, len = NCP / 2; s >= 1; s >>= 1, len >>= 1)
+        if (lane & s) base += len;
+    float* o = out + (int64_t)box * NC;
+#pragma unroll
+    for (int i = 0; i < NCP / 32; ++i) {
+        const int c = base + i;
+        if (c < NC) {
+            if (IRREG) o[c] += w[i];
+            else o[c] = w[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// M2M on one level for a group of 8 parents (consecutive boxes of level l): for each
+// octant o the table T_o is staged in shared memory once and applied to the 8 parents'
+// child o; parent = sum over octants of T_o M_child(o), octants in order.
+// ---------------------------------------------------------------------------------
+constexpr int kGroup = 8;
+
 template <int P, typename T>
-__global__ void m2m_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, const T* __restrict__ tab,
-                           T* __restrict__ M) {
+__global__ void __launch_bounds__(128) m2m_group_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
+                                                        const T* __restrict__ tab, T* __restrict__ M) {
     constexpr int NC = nc_of(P);
     extern __shared__ unsigned char smem_raw[];
-    T* Mc = reinterpret_cast<T*>(smem_raw);  // [8][NC]
-    int64_t b = b0 + blockIdx.x;
-    if (b >= b1) return;
-    int c0 = plan.child_first[b];
-    if (c0 < 0 || plan.src_below[b] == 0) return;
+    T* A = reinterpret_cast<T*>(smem_raw);  // [NC][NC] column-major table of one octant
+    T* X = A + NC * NC;                     // [kGroup][NC] child multipoles
+    __shared__ int child[kGroup];
+    const int64_t g0 = b0 + (int64_t)blockIdx.x * kGroup;
+    if (threadIdx.x < kGroup) {
+        const int64_t b = g0 + threadIdx.x;
+        child[threadIdx.x] = (b < b1 && plan.child_first[b] >= 0 && plan.src_below[b] > 0) ? plan.child_first[b] : -1;
+    }
+    __syncthreads();
+    const int i = threadIdx.x;
     for (int v = 0; v < m; ++v) {
-        for (int t = threadIdx.x; t < 8 * NC; t += blockDim.x) {
-            int o = t / NC, k = t % NC;
-            Mc[t] = plan.src_below[c0 + o] ? M[((int64_t)(c0 + o) * m + v) * NC + k] : T(0);
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
-            T acc = T(0);
-            for (int o = 0; o < 8; ++o) {
-                if (!plan.src_below[c0 + o]) continue;
-                const T* A = tab + (int64_t)o * NC * NC + i;
-                const T* x = Mc + o * NC;
-#pragma unroll 7
-                for (int k = 0; k < NC; ++k) acc += A[(int64_t)k * NC] * x[k];
+        T acc[kGroup];
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) acc[g] = T(0);
+        for (int o = 0; o < 8; ++o) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < NC * NC; t += blockDim.x) A[t] = tab[(int64_t)o * NC * NC + t];
+            for (int t = threadIdx.x; t < kGroup * NC; t += blockDim.x) {
+                const int g = t / NC, k = t % NC;
+                const int c = child[g] >= 0 ? child[g] + o : -1;
+                X[t] = (c >= 0 && plan.src_below[c] > 0) ? M[((int64_t)c * m + v) * NC + k] : T(0);
             }
-            M[((int64_t)b * m + v) * NC + i] = acc;
+            __syncthreads();
+            if (i < NC) {
+                for (int k = 0; k < NC; ++k) {
+                    const T a = A[k * NC + i];
+#pragma unroll
+                    for (int g = 0; g < kGroup; ++g) acc[g] += a * X[g * NC + k];
+                }
+            }
         }
-        __syncthreads();
+        if (i < NC)
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g)
+                if (child[g] >= 0) M[((g0 + g) * m + v) * NC + i] = acc[g];
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// The locals of level l (>= 2), for the children of a group of 8 parents (consecutive
+// boxes of level l - 1): per octant o, T_o is staged once; child o of each parent gets
+//   L = L2L_o(L_parent) (l >= 3) + its V row's products in offset-index order,
+// written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X follows).
+// ---------------------------------------------------------------------------------
+template <int P, typename T>
+__global__ void __launch_bounds__(128) local_group_kernel(DevPlan plan, int64_t p0, int64_t p1, int m,
+                                                          int with_l2l, const T* __restrict__ l2l_tab,
+                                                          const T* __restrict__ Y, T* __restrict__ Lc) {
+    constexpr int NC = nc_of(P);
+    extern __shared__ unsigned char smem_raw[];
+    T* A = reinterpret_cast<T*>(smem_raw);  // [NC][NC]
+    T* Lp = A + NC * NC;                    // [kGroup][NC] parent locals
+    __shared__ int first[kGroup];
+    const int64_t g0 = p0 + (int64_t)blockIdx.x * kGroup;
+    if (threadIdx.x < kGroup) {
+        const int64_t b = g0 + threadIdx.x;
+        first[threadIdx.x] = (b < p1 && plan.child_first[b] >= 0 && plan.tgt_below[b] > 0) ? plan.child_first[b] : -1;
+    }
+    __syncthreads();
+    const int i = threadIdx.x;
+    for (int v = 0; v < m; ++v) {
+        if (with_l2l) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < kGroup * NC; t += blockDim.x) {
+                const int g = t / NC, k = t % NC;
+                Lp[t] = first[g] >= 0 ? Lc[((g0 + g) * m + v) * NC + k] : T(0);
+            }
+        }
+        for (int o = 0; o < 8; ++o) {
+            if (with_l2l) {
+                __syncthreads();
+                for (int t = threadIdx.x; t < NC * NC; t += blockDim.x) A[t] = l2l_tab[(int64_t)o * NC * NC + t];
+                __syncthreads();
+            }
+            if (i >= NC) continue;
+            T acc[kGroup];
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g) acc[g] = T(0);
+            if (with_l2l) {
+                for (int k = 0; k < NC; ++k) {
+                    const T a = A[k * NC + i];
+#pragma unroll
+                    for (int g = 0; g < kGroup; ++g) acc[g] += a * Lp[g * NC + k];
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g) {
+                if (first[g] < 0) continue;
+                const int c = first[g] + o;
+                if (plan.tgt_below[c] == 0) continue;
+                T s = acc[g];
+                for (int64_t e = plan.v_row[c]; e < plan.v_row[c + 1]; ++e) s += Y[(e * m + v) * NC + i];
+                Lc[((int64_t)c * m + v) * NC + i] = s;
+            }
+        }
     }
 }
 
@@ -287,42 +457,6 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
                 int n = tx + 16 * j;
                 if (n < NC) y[n] = acc[i][j];
             }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------------
-// The local of every box of one level (l >= 2) that has a target below it:
-//   L_t = L2L_o(L_parent) (l >= 3) + sum over its V row, in offset-index order, of Y[e]
-// written once (the accumulation order of fmm-plan/src/operator.rs:34-45: the L2L
-// from the parent, then the V list by offset index; the X list is added after).
-// ---------------------------------------------------------------------------------
-template <int P, typename T>
-__global__ void local_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l,
-                             const T* __restrict__ l2l_tab, const T* __restrict__ Y, T* __restrict__ Lc) {
-    constexpr int NC = nc_of(P);
-    extern __shared__ unsigned char smem_raw[];
-    T* Lp = reinterpret_cast<T*>(smem_raw);  // [NC]
-    int64_t b = b0 + blockIdx.x;
-    if (b >= b1 || plan.tgt_below[b] == 0) return;
-    const int par = plan.parent[b];
-    const int o = (int)(((plan.idx[3 * b] & 1) << 2) | ((plan.idx[3 * b + 1] & 1) << 1) | (plan.idx[3 * b + 2] & 1));
-    const T* A0 = l2l_tab + (int64_t)o * NC * NC;
-    const int64_t e0 = plan.v_row[b], e1 = plan.v_row[b + 1];
-    for (int v = 0; v < m; ++v) {
-        if (with_l2l) {
-            __syncthreads();
-            for (int k = threadIdx.x; k < NC; k += blockDim.x) Lp[k] = Lc[((int64_t)par * m + v) * NC + k];
-            __syncthreads();
-        }
-        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
-            T acc = T(0);
-            if (with_l2l) {
-#pragma unroll 7
-                for (int k = 0; k < NC; ++k) acc += A0[(int64_t)k * NC + i] * Lp[k];
-            }
-            for (int64_t e = e0; e < e1; ++e) acc += Y[(e * m + v) * NC + i];
-            Lc[((int64_t)b * m + v) * NC + i] = acc;
         }
     }
 }
