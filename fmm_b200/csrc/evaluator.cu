@@ -140,6 +140,9 @@ struct Evaluator final : EvaluatorBase {
         v_off;
     // data
     DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g, Y;
+    // interior boxes per level with a source below (M2M) / a target below (L2L), CSR by level
+    DevBuf m2m_par, l2l_par;
+    std::vector<int64_t> m2m_start, l2l_start;
     // M2L batches: pairs of all levels grouped by offset, in tiles
     DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
     int64_t ntiles = 0;
@@ -240,6 +243,7 @@ struct Evaluator final : EvaluatorBase {
         far_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
+        build_parent_lists();
         build_m2l_batches(kGemmPairs);
         if (kTensor) build_tensor_m2l(m2l);
         build_p2p_items();
@@ -327,6 +331,23 @@ struct Evaluator final : EvaluatorBase {
         tile_count.upload(tc);
         pair_e.upload(pe);
         pair_src.upload(ps);
+    }
+
+    void build_parent_lists() {
+        std::vector<int32_t> a, b;
+        m2m_start.assign(plan.nlevels + 1, 0);
+        l2l_start.assign(plan.nlevels + 1, 0);
+        for (int l = 0; l < plan.nlevels; ++l) {
+            for (int64_t x = plan.level_start[l]; x < plan.level_start[l + 1]; ++x) {
+                if (plan.child_first[x] < 0) continue;
+                if (plan.src_below[x] > 0) a.push_back((int32_t)x);
+                if (plan.tgt_below[x] > 0) b.push_back((int32_t)x);
+            }
+            m2m_start[l + 1] = (int64_t)a.size();
+            l2l_start[l + 1] = (int64_t)b.size();
+        }
+        m2m_par.upload(a);
+        l2l_par.upload(b);
     }
 
     void build_p2p_items() {
@@ -420,7 +441,7 @@ struct Evaluator final : EvaluatorBase {
                                &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
                                &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
                                &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
-                               &Y, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
+                               &Y, &m2m_par, &l2l_par, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error};
         size_t s = 0;
@@ -473,8 +494,10 @@ struct Evaluator final : EvaluatorBase {
             int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
             if (b1 > b0)
                 timer.run(kM2M, [&] {
-                    m2m_group_kernel<P, T><<<(unsigned)((b1 - b0 + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
-                        dp, b0, b1, m, m2m_tab.as<T>(), M.as<T>());
+                    const int64_t n = m2m_start[l + 1] - m2m_start[l];
+                    if (n)
+                        m2m_group_kernel<P, T><<<(unsigned)((n + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
+                            dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, m2m_tab.as<T>(), M.as<T>());
                 });
         }
         // M2L products of every level at once (all multipoles are final here)
@@ -500,10 +523,12 @@ struct Evaluator final : EvaluatorBase {
         // downward: for l = 2..L: L2L + V (one kernel), then P2L
         for (int l = 2; l <= L; ++l) {
             int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
-            int64_t p0 = plan.level_start[l - 1], p1 = plan.level_start[l];
             timer.run(kL2L, [&] {
-                local_group_kernel<P, T><<<(unsigned)((p1 - p0 + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
-                    dp, p0, p1, m, l >= 3, l2l_tab.as<T>(), Y.as<T>(), Lc.as<T>());
+                const int64_t n = l2l_start[l] - l2l_start[l - 1];
+                if (n)
+                    local_group_kernel<P, T><<<(unsigned)((n + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
+                        dp, l2l_par.as<int32_t>() + l2l_start[l - 1], n, m, l >= 3, l2l_tab.as<T>(), Y.as<T>(),
+                        Lc.as<T>());
             });
             timer.run(kP2L, [&] {
                 if (kBfly && m == 1)

@@ -280,24 +280,27 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
 }
 
 // ---------------------------------------------------------------------------------
-// M2M on one level for a group of 8 parents (consecutive boxes of level l): for each
+// M2M on one level for a group of 8 parents (from the level's list of interior boxes
+// with a source below them): for each
 // octant o the table T_o is staged in shared memory once and applied to the 8 parents'
 // child o; parent = sum over octants of T_o M_child(o), octants in order.
 // ---------------------------------------------------------------------------------
 constexpr int kGroup = 8;
 
 template <int P, typename T>
-__global__ void __launch_bounds__(128) m2m_group_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
-                                                        const T* __restrict__ tab, T* __restrict__ M) {
+__global__ void __launch_bounds__(128) m2m_group_kernel(DevPlan plan, const int32_t* __restrict__ parents,
+                                                        int64_t n, int m, const T* __restrict__ tab,
+                                                        T* __restrict__ M) {
     constexpr int NC = nc_of(P);
     extern __shared__ unsigned char smem_raw[];
     T* A = reinterpret_cast<T*>(smem_raw);  // [NC][NC] column-major table of one octant
     T* X = A + NC * NC;                     // [kGroup][NC] child multipoles
-    __shared__ int child[kGroup];
-    const int64_t g0 = b0 + (int64_t)blockIdx.x * kGroup;
+    __shared__ int child[kGroup], parent[kGroup];
+    const int64_t g0 = (int64_t)blockIdx.x * kGroup;
     if (threadIdx.x < kGroup) {
-        const int64_t b = g0 + threadIdx.x;
-        child[threadIdx.x] = (b < b1 && plan.child_first[b] >= 0 && plan.src_below[b] > 0) ? plan.child_first[b] : -1;
+        const int64_t j = g0 + threadIdx.x;
+        parent[threadIdx.x] = j < n ? parents[j] : -1;
+        child[threadIdx.x] = j < n ? plan.child_first[parents[j]] : -1;
     }
     __syncthreads();
     const int i = threadIdx.x;
@@ -325,29 +328,32 @@ __global__ void __launch_bounds__(128) m2m_group_kernel(DevPlan plan, int64_t b0
         if (i < NC)
 #pragma unroll
             for (int g = 0; g < kGroup; ++g)
-                if (child[g] >= 0) M[((g0 + g) * m + v) * NC + i] = acc[g];
+                if (child[g] >= 0) M[((int64_t)parent[g] * m + v) * NC + i] = acc[g];
     }
 }
 
 // ---------------------------------------------------------------------------------
-// The locals of level l (>= 2), for the children of a group of 8 parents (consecutive
-// boxes of level l - 1): per octant o, T_o is staged once; child o of each parent gets
+// The locals of level l (>= 2), for the children of a group of 8 parents (from the list
+// of interior boxes of level l - 1 with a target below): per octant o, T_o is staged
+// once; child o of each parent gets
 //   L = L2L_o(L_parent) (l >= 3) + its V row's products in offset-index order,
 // written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X follows).
 // ---------------------------------------------------------------------------------
 template <int P, typename T>
-__global__ void __launch_bounds__(128) local_group_kernel(DevPlan plan, int64_t p0, int64_t p1, int m,
-                                                          int with_l2l, const T* __restrict__ l2l_tab,
-                                                          const T* __restrict__ Y, T* __restrict__ Lc) {
+__global__ void __launch_bounds__(128) local_group_kernel(DevPlan plan, const int32_t* __restrict__ parents,
+                                                          int64_t n, int m, int with_l2l,
+                                                          const T* __restrict__ l2l_tab, const T* __restrict__ Y,
+                                                          T* __restrict__ Lc) {
     constexpr int NC = nc_of(P);
     extern __shared__ unsigned char smem_raw[];
     T* A = reinterpret_cast<T*>(smem_raw);  // [NC][NC]
     T* Lp = A + NC * NC;                    // [kGroup][NC] parent locals
-    __shared__ int first[kGroup];
-    const int64_t g0 = p0 + (int64_t)blockIdx.x * kGroup;
+    __shared__ int first[kGroup], parent[kGroup];
+    const int64_t g0 = (int64_t)blockIdx.x * kGroup;
     if (threadIdx.x < kGroup) {
-        const int64_t b = g0 + threadIdx.x;
-        first[threadIdx.x] = (b < p1 && plan.child_first[b] >= 0 && plan.tgt_below[b] > 0) ? plan.child_first[b] : -1;
+        const int64_t j = g0 + threadIdx.x;
+        parent[threadIdx.x] = j < n ? parents[j] : -1;
+        first[threadIdx.x] = j < n ? plan.child_first[parents[j]] : -1;
     }
     __syncthreads();
     const int i = threadIdx.x;
@@ -356,7 +362,7 @@ __global__ void __launch_bounds__(128) local_group_kernel(DevPlan plan, int64_t 
             __syncthreads();
             for (int t = threadIdx.x; t < kGroup * NC; t += blockDim.x) {
                 const int g = t / NC, k = t % NC;
-                Lp[t] = first[g] >= 0 ? Lc[((g0 + g) * m + v) * NC + k] : T(0);
+                Lp[t] = first[g] >= 0 ? Lc[((int64_t)parent[g] * m + v) * NC + k] : T(0);
             }
         }
         for (int o = 0; o < 8; ++o) {
