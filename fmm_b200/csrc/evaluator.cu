@@ -140,9 +140,13 @@ struct Evaluator final : EvaluatorBase {
         v_off;
     // data
     DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g, Y;
-    // interior boxes per level with a source below (M2M) / a target below (L2L), CSR by level
-    DevBuf m2m_par, l2l_par;
-    std::vector<int64_t> m2m_start, l2l_start;
+    // interior boxes per level with a source below (M2M parents), CSR by level
+    DevBuf m2m_par;
+    std::vector<int64_t> m2m_start;
+    // per-level octant batches of the M2M (children with a source) and L2L (children with a
+    // target) products, tiles of kGemmPairs; Yo holds one product row per child box
+    DevBuf oct_tile_d, oct_tile_begin, oct_tile_count, oct_pair_e, oct_pair_src, Yo;
+    std::vector<int64_t> m2m_tiles, l2l_tiles;  // tile ranges per level (nlevels + 1)
     // M2L batches: pairs of all levels grouped by offset, in tiles
     DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
     int64_t ntiles = 0;
@@ -159,7 +163,7 @@ struct Evaluator final : EvaluatorBase {
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
     static constexpr bool kBfly = sizeof(T) == 4;  // register P2M/P2L (f32, one vector)
-    static constexpr size_t group_smem = sizeof(T) * ((size_t)NC * NC + (size_t)kGroup * NC);
+
     // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
     static constexpr float kTheta2 = 0.0625f;
 
@@ -251,10 +255,6 @@ struct Evaluator final : EvaluatorBase {
         close_pairs = nclose;
         Y.alloc(sizeof(T) * (size_t)m * NC * (pl.v.nnz() + 1));
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
-        if (group_smem > 48 * 1024) {
-            CUDA_TRY(cudaFuncSetAttribute(m2m_group_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
-            CUDA_TRY(cudaFuncSetAttribute(local_group_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
-        }
         if (gemm_smem > 48 * 1024)
             CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
         // shared memory opt-in beyond 48 KB where a kernel needs it
@@ -334,20 +334,55 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void build_parent_lists() {
-        std::vector<int32_t> a, b;
+        std::vector<int32_t> a;
         m2m_start.assign(plan.nlevels + 1, 0);
-        l2l_start.assign(plan.nlevels + 1, 0);
         for (int l = 0; l < plan.nlevels; ++l) {
-            for (int64_t x = plan.level_start[l]; x < plan.level_start[l + 1]; ++x) {
-                if (plan.child_first[x] < 0) continue;
-                if (plan.src_below[x] > 0) a.push_back((int32_t)x);
-                if (plan.tgt_below[x] > 0) b.push_back((int32_t)x);
-            }
+            for (int64_t x = plan.level_start[l]; x < plan.level_start[l + 1]; ++x)
+                if (plan.child_first[x] >= 0 && plan.src_below[x] > 0) a.push_back((int32_t)x);
             m2m_start[l + 1] = (int64_t)a.size();
-            l2l_start[l + 1] = (int64_t)b.size();
         }
         m2m_par.upload(a);
-        l2l_par.upload(b);
+        // octant batches: M2M of level l takes children (level l + 1) with a source, L2L of
+        // level l takes children (level l) with a target; pairs grouped by octant per level
+        std::vector<int32_t> td, tc, ps;
+        std::vector<int64_t> tb, pe;
+        m2m_tiles.assign(plan.nlevels + 1, 0);
+        l2l_tiles.assign(plan.nlevels + 1, 0);
+        auto octant = [&](int64_t c) {
+            return (int)(((plan.idx[3 * c] & 1) << 2) | ((plan.idx[3 * c + 1] & 1) << 1) | (plan.idx[3 * c + 2] & 1));
+        };
+        for (int pass = 0; pass < 2; ++pass) {
+            std::vector<int64_t>& ranges = pass == 0 ? m2m_tiles : l2l_tiles;
+            for (int l = 0; l < plan.nlevels; ++l) {
+                ranges[l] = (int64_t)td.size();
+                const int cl = pass == 0 ? l + 1 : l;  // level of the children
+                if (cl >= plan.nlevels || (pass == 1 && l < 3)) continue;
+                std::vector<std::vector<int64_t>> by(8);
+                for (int64_t c = plan.level_start[cl]; c < plan.level_start[cl + 1]; ++c) {
+                    if (pass == 0 ? plan.src_below[c] == 0 : plan.tgt_below[c] == 0) continue;
+                    by[octant(c)].push_back(c);
+                }
+                for (int o = 0; o < 8; ++o)
+                    for (size_t s0 = 0; s0 < by[o].size(); s0 += kGemmPairs) {
+                        td.push_back(o);
+                        tb.push_back((int64_t)pe.size());
+                        const size_t cnt = std::min<size_t>(kGemmPairs, by[o].size() - s0);
+                        tc.push_back((int32_t)cnt);
+                        for (size_t q = s0; q < s0 + cnt; ++q) {
+                            const int64_t c = by[o][q];
+                            pe.push_back(c);
+                            ps.push_back(pass == 0 ? (int32_t)c : plan.parent[c]);
+                        }
+                    }
+            }
+            ranges[plan.nlevels] = (int64_t)td.size();
+        }
+        oct_tile_d.upload(td);
+        oct_tile_begin.upload(tb);
+        oct_tile_count.upload(tc);
+        oct_pair_e.upload(pe);
+        oct_pair_src.upload(ps);
+        Yo.alloc(sizeof(T) * (size_t)m * NC * plan.nboxes());
     }
 
     void build_p2p_items() {
@@ -441,7 +476,8 @@ struct Evaluator final : EvaluatorBase {
                                &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
                                &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
                                &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
-                               &Y, &m2m_par, &l2l_par, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
+                               &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e,
+                               &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error};
         size_t s = 0;
@@ -491,14 +527,18 @@ struct Evaluator final : EvaluatorBase {
             }
         });
         for (int l = L - 1; l >= 0; --l) {
-            int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
-            if (b1 > b0)
-                timer.run(kM2M, [&] {
-                    const int64_t n = m2m_start[l + 1] - m2m_start[l];
-                    if (n)
-                        m2m_group_kernel<P, T><<<(unsigned)((n + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
-                            dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, m2m_tab.as<T>(), M.as<T>());
-                });
+            timer.run(kM2M, [&] {
+                const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
+                const int64_t n = m2m_start[l + 1] - m2m_start[l];
+                if (nt)
+                    m2l_gemm_kernel<P, T><<<(unsigned)nt, 256, gemm_smem, stream>>>(
+                        oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
+                        oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
+                        m2m_tab.as<T>(), M.as<T>(), Yo.as<T>());
+                if (n)
+                    m2m_reduce_kernel<P, T><<<(unsigned)n, round32(NC), 0, stream>>>(
+                        dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, Yo.as<T>(), M.as<T>());
+            });
         }
         // M2L products of every level at once (all multipoles are final here)
         if (kTensor && m2l_path == 1) {
@@ -520,15 +560,18 @@ struct Evaluator final : EvaluatorBase {
                     tile_d.as<int32_t>(), tile_begin.as<int64_t>(), tile_count.as<int32_t>(), pair_e.as<int64_t>(),
                     pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
             });
-        // downward: for l = 2..L: L2L + V (one kernel), then P2L
+        // downward: for l = 2..L: L2L products, the local (L2L + V in offset order), then P2L
         for (int l = 2; l <= L; ++l) {
             int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
             timer.run(kL2L, [&] {
-                const int64_t n = l2l_start[l] - l2l_start[l - 1];
-                if (n)
-                    local_group_kernel<P, T><<<(unsigned)((n + kGroup - 1) / kGroup), 128, group_smem, stream>>>(
-                        dp, l2l_par.as<int32_t>() + l2l_start[l - 1], n, m, l >= 3, l2l_tab.as<T>(), Y.as<T>(),
-                        Lc.as<T>());
+                const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
+                if (nt)
+                    m2l_gemm_kernel<P, T><<<(unsigned)nt, 256, gemm_smem, stream>>>(
+                        oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
+                        oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
+                        l2l_tab.as<T>(), Lc.as<T>(), Yo.as<T>());
+                local_reduce_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), 0, stream>>>(
+                    dp, b0, b1, m, l >= 3, Yo.as<T>(), Y.as<T>(), Lc.as<T>());
             });
             timer.run(kP2L, [&] {
                 if (kBfly && m == 1)

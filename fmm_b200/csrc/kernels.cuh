@@ -280,119 +280,57 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
 }
 
 // ---------------------------------------------------------------------------------
-// M2M on one level for a group of 8 parents (from the level's list of interior boxes
-// with a source below them): for each
-// octant o the table T_o is staged in shared memory once and applied to the 8 parents'
-// child o; parent = sum over octants of T_o M_child(o), octants in order.
+// M2M and L2L run as batched GEMMs too (m2l_gemm_kernel with the 8 octant tables): the
+// product for child c is written to row c of Yo (M2M: T_o M_c; L2L: T_o L_parent(c)).
+// The reduces below then add rows in the reference's order.
 // ---------------------------------------------------------------------------------
-constexpr int kGroup = 8;
 
+// M2M reduce for the parents of one level: M_p = sum over octants o (in order) of the
+// products of its children that hold a source.  Block per parent, thread per slot.
 template <int P, typename T>
-__global__ void __launch_bounds__(128) m2m_group_kernel(DevPlan plan, const int32_t* __restrict__ parents,
-                                                        int64_t n, int m, const T* __restrict__ tab,
-                                                        T* __restrict__ M) {
+__global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ parents, int64_t n, int m,
+                                  const T* __restrict__ Yo, T* __restrict__ M) {
     constexpr int NC = nc_of(P);
-    extern __shared__ unsigned char smem_raw[];
-    T* A = reinterpret_cast<T*>(smem_raw);  // [NC][NC] column-major table of one octant
-    T* X = A + NC * NC;                     // [kGroup][NC] child multipoles
-    __shared__ int child[kGroup], parent[kGroup];
-    const int64_t g0 = (int64_t)blockIdx.x * kGroup;
-    if (threadIdx.x < kGroup) {
-        const int64_t j = g0 + threadIdx.x;
-        parent[threadIdx.x] = j < n ? parents[j] : -1;
-        child[threadIdx.x] = j < n ? plan.child_first[parents[j]] : -1;
-    }
-    __syncthreads();
-    const int i = threadIdx.x;
-    for (int v = 0; v < m; ++v) {
-        T acc[kGroup];
+    const int64_t j = blockIdx.x;
+    if (j >= n) return;
+    const int p = parents[j];
+    const int c0 = plan.child_first[p];
+    for (int v = 0; v < m; ++v)
+        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+            T s = T(0);
 #pragma unroll
-        for (int g = 0; g < kGroup; ++g) acc[g] = T(0);
-        for (int o = 0; o < 8; ++o) {
-            __syncthreads();
-            for (int t = threadIdx.x; t < NC * NC; t += blockDim.x) A[t] = tab[(int64_t)o * NC * NC + t];
-            for (int t = threadIdx.x; t < kGroup * NC; t += blockDim.x) {
-                const int g = t / NC, k = t % NC;
-                const int c = child[g] >= 0 ? child[g] + o : -1;
-                X[t] = (c >= 0 && plan.src_below[c] > 0) ? M[((int64_t)c * m + v) * NC + k] : T(0);
-            }
-            __syncthreads();
-            if (i < NC) {
-                for (int k = 0; k < NC; ++k) {
-                    const T a = A[k * NC + i];
-#pragma unroll
-                    for (int g = 0; g < kGroup; ++g) acc[g] += a * X[g * NC + k];
-                }
-            }
+            for (int o = 0; o < 8; ++o)
+                if (plan.src_below[c0 + o]) s += Yo[((int64_t)(c0 + o) * m + v) * NC + i];
+            M[((int64_t)p * m + v) * NC + i] = s;
         }
-        if (i < NC)
-#pragma unroll
-            for (int g = 0; g < kGroup; ++g)
-                if (child[g] >= 0) M[((int64_t)parent[g] * m + v) * NC + i] = acc[g];
-    }
 }
 
-// ---------------------------------------------------------------------------------
-// The locals of level l (>= 2), for the children of a group of 8 parents (from the list
-// of interior boxes of level l - 1 with a target below): per octant o, T_o is staged
-// once; child o of each parent gets
-//   L = L2L_o(L_parent) (l >= 3) + its V row's products in offset-index order,
-// written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X follows).
-// ---------------------------------------------------------------------------------
+// The locals of one level (>= 2), for every box with a target below it:
+//   L = (l >= 3 ? T_o L_parent : 0) + the V row's products in offset-index order,
+// written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X is added after).
+// Block per box, thread per slot; the V loop issues four loads before adding them in order.
 template <int P, typename T>
-__global__ void __launch_bounds__(128) local_group_kernel(DevPlan plan, const int32_t* __restrict__ parents,
-                                                          int64_t n, int m, int with_l2l,
-                                                          const T* __restrict__ l2l_tab, const T* __restrict__ Y,
-                                                          T* __restrict__ Lc) {
+__global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l,
+                                    const T* __restrict__ Yo, const T* __restrict__ Yv, T* __restrict__ Lc) {
     constexpr int NC = nc_of(P);
-    extern __shared__ unsigned char smem_raw[];
-    T* A = reinterpret_cast<T*>(smem_raw);  // [NC][NC]
-    T* Lp = A + NC * NC;                    // [kGroup][NC] parent locals
-    __shared__ int first[kGroup], parent[kGroup];
-    const int64_t g0 = (int64_t)blockIdx.x * kGroup;
-    if (threadIdx.x < kGroup) {
-        const int64_t j = g0 + threadIdx.x;
-        parent[threadIdx.x] = j < n ? parents[j] : -1;
-        first[threadIdx.x] = j < n ? plan.child_first[parents[j]] : -1;
-    }
-    __syncthreads();
-    const int i = threadIdx.x;
-    for (int v = 0; v < m; ++v) {
-        if (with_l2l) {
-            __syncthreads();
-            for (int t = threadIdx.x; t < kGroup * NC; t += blockDim.x) {
-                const int g = t / NC, k = t % NC;
-                Lp[t] = first[g] >= 0 ? Lc[((int64_t)parent[g] * m + v) * NC + k] : T(0);
+    const int64_t b = b0 + blockIdx.x;
+    if (b >= b1 || plan.tgt_below[b] == 0) return;
+    const int64_t e0 = plan.v_row[b], e1 = plan.v_row[b + 1];
+    for (int v = 0; v < m; ++v)
+        for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+            T s = with_l2l ? Yo[(b * m + v) * NC + i] : T(0);
+            int64_t e = e0;
+            for (; e + 4 <= e1; e += 4) {
+                const T y0 = Yv[(e * m + v) * NC + i], y1 = Yv[((e + 1) * m + v) * NC + i];
+                const T y2 = Yv[((e + 2) * m + v) * NC + i], y3 = Yv[((e + 3) * m + v) * NC + i];
+                s += y0;
+                s += y1;
+                s += y2;
+                s += y3;
             }
+            for (; e < e1; ++e) s += Yv[(e * m + v) * NC + i];
+            Lc[(b * m + v) * NC + i] = s;
         }
-        for (int o = 0; o < 8; ++o) {
-            if (with_l2l) {
-                __syncthreads();
-                for (int t = threadIdx.x; t < NC * NC; t += blockDim.x) A[t] = l2l_tab[(int64_t)o * NC * NC + t];
-                __syncthreads();
-            }
-            if (i >= NC) continue;
-            T acc[kGroup];
-#pragma unroll
-            for (int g = 0; g < kGroup; ++g) acc[g] = T(0);
-            if (with_l2l) {
-                for (int k = 0; k < NC; ++k) {
-                    const T a = A[k * NC + i];
-#pragma unroll
-                    for (int g = 0; g < kGroup; ++g) acc[g] += a * Lp[g * NC + k];
-                }
-            }
-#pragma unroll
-            for (int g = 0; g < kGroup; ++g) {
-                if (first[g] < 0) continue;
-                const int c = first[g] + o;
-                if (plan.tgt_below[c] == 0) continue;
-                T s = acc[g];
-                for (int64_t e = plan.v_row[c]; e < plan.v_row[c + 1]; ++e) s += Y[(e * m + v) * NC + i];
-                Lc[((int64_t)c * m + v) * NC + i] = s;
-            }
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------------
