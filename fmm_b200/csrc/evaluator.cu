@@ -284,7 +284,7 @@ struct Evaluator final : EvaluatorBase {
             tc_error.alloc(sizeof(int));
             CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
             CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          TcShape2<P>::SMEM2));
+                                          TcTs<P>::SMEM));
             int dev = 0;
             CUDA_TRY(cudaGetDevice(&dev));
             CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -547,10 +547,10 @@ struct Evaluator final : EvaluatorBase {
                     timer.run(kM2L, [&] {
                         const unsigned grid = (unsigned)std::min<int64_t>(tc_ntiles, num_sms);
                         for (int v = 0; v < m; ++v)
-                            m2l_tc_kernel<P><<<grid, 32 * kTcWarps, TcShape2<P>::SMEM2, stream>>>(
+                            m2l_tc_kernel<P><<<grid, 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
                                 tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
                                 tc_ntiles, tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v,
-                                tc_bimg.as<uint4>(), reinterpret_cast<const float*>(M.ptr),
+                                tc_bimg.as<uint32_t>(), reinterpret_cast<const float*>(M.ptr),
                                 reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
                     });
             }

@@ -127,19 +127,59 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
     return false;
 }
 
-// Persistent form: CTA c takes the contiguous range of tiles [c T / G, (c + 1) T / G) of
-// the offset-sorted tile list, so the table image changes only a few times per CTA.
-// 16 warps: all of them gather (loads of a warp's 8 rows issued before use) and convert
-// A; thread 0 issues the MMAs; the epilogue of tile i-1 (TMEM buffer (i-1)&1, read by
-// the 4 warps of each TMEM lane quarter, 16 columns at a time, staged per warp so that
-// stores run along Y rows) overlaps MMA(i) into buffer i&1.  One vector per launch.
+// Persistent form.  CTA c takes the contiguous range of tiles [c T / G, (c + 1) T / G) of
+// the offset-sorted tile list.  The table of the current offset lives in tensor memory
+// as the MMA's A operand (M = 128 lanes = output slots, K = input slots in columns; hi
+// and lo parts), so the MMA is D[slot][pair] = A_d . X^T with the gathered multipoles X
+// as the shared-memory B operand (N = 128 pairs, K-major, 128-byte swizzled), double
+// buffered.  Per tile i (16 warps):
+//   gather + split X(i) into buffer i&1 (its last reader, MMA(i-2), has completed),
+//   wait MMA(i-1); if the offset changes, warps 0-3 store the new table into TMEM,
+//   thread 0 issues MMA(i) into accumulator i&1 and commits to the barrier,
+//   epilogue(i-1): each thread holds one slot of 16 pairs per TMEM load, so the stores
+//   of one pair's row are contiguous across the warp's lanes.
+// One vector per launch.
 constexpr int kTcWarps = 16;
 
 template <int P>
-struct TcShape2 : TcShape<P> {
-    static constexpr int OUT_BYTES = kTcWarps * 32 * 17 * 4;  // per-warp 32 x 16 epilogue tiles
-    static constexpr int SMEM2 = 2 * TcShape<P>::A_BYTES + 2 * TcShape<P>::B_BYTES + OUT_BYTES + 1024 + 64;
+struct TcTs {
+    static constexpr int NC = nc_of(P);
+    static constexpr int KA = (NC + 31) / 32;
+    static constexpr int KP = 32 * KA;             // padded K (input slots)
+    static constexpr int KSTEPS = KP / 8;
+    static constexpr int NT = kTcRows;             // pairs per tile (UMMA N)
+    static constexpr int X_BYTES = NT * KP * 4;    // one part of one buffer
+    static constexpr int SMEM = 4 * X_BYTES + 1024 + 64;
+    static constexpr int COL_AHI = 0, COL_ALO = KP, COL_D0 = 2 * KP;  // TMEM columns
+    static constexpr int TMEM_COLS = 512;
+    static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per offset (hi, lo)
+    static_assert(NC <= 128, "UMMA M = 128 output slots");
+    static_assert(2 * KP + 2 * NT <= TMEM_COLS, "TMEM budget");
 };
+
+template <int NTILE>
+__host__ __device__ constexpr uint32_t tf32_idesc_ts() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NTILE >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]));
+}
 
 template <int P>
 __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
@@ -147,31 +187,27 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   const int32_t* __restrict__ tile_count,
                                                                   int64_t ntiles, const int64_t* __restrict__ pair_e,
                                                                   const int32_t* __restrict__ pair_src, int m, int v,
-                                                                  const uint4* __restrict__ bimg,
+                                                                  const uint32_t* __restrict__ timg,
                                                                   const float* __restrict__ M, float* __restrict__ Y,
                                                                   int* __restrict__ error) {
-    using S = TcShape2<P>;
+    using S = TcTs<P>;
     constexpr int NC = S::NC;
-    constexpr int RPW = kTcRows / kTcWarps;  // rows per warp in the gather
+    constexpr int RPW = S::NT / kTcWarps;  // gathered rows per warp
     extern __shared__ unsigned char smem_raw[];
-    unsigned char* base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-    unsigned char* a_hi = base;
-    unsigned char* a_lo = a_hi + S::A_BYTES;
-    unsigned char* b_hi = a_lo + S::A_BYTES;
-    unsigned char* b_lo = b_hi + S::B_BYTES;
+    unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 bufs][hi, lo]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    float* outw = reinterpret_cast<float*>(b_lo + S::B_BYTES) + warp * 32 * 17;
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __shared__ int32_t row_src[kTcRows];
-    __shared__ int64_t row_e[2][kTcRows];
+    __shared__ int32_t row_src[2][S::NT];
+    __shared__ int64_t row_e[2][S::NT];
+    __shared__ int32_t row_cnt[2];
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
     const int64_t i1 = (int64_t)(blockIdx.x + 1) * ntiles / gridDim.x;
     if (i0 >= i1) return;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                     "r"(2 * S::TMEM_COLS));
+                     "r"(S::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
@@ -182,65 +218,26 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-    const uint32_t idesc = tf32_idesc<S::NP>();
-    int cur_d = -1;
-    uint32_t phase = 0;
-    bool failed = false;
-    int prev_cnt = 0;
+    constexpr uint32_t idesc = tf32_idesc_ts<S::NT>();
 
-    auto epilogue = [&](int buf, int cnt) {
-        const int quarter = warp & 3;        // TMEM lanes 32 quarter .. + 31
-        const int rw = 32 * quarter;
-        const int half = lane >> 4, col = lane & 15;
-        for (int c0 = 16 * (warp >> 2); c0 < S::NP; c0 += 16 * (kTcWarps / 4)) {
-            float vals[16];
-            tmem_ld16(tmem + (uint32_t)(buf * S::TMEM_COLS) + ((uint32_t)rw << 16) + (uint32_t)c0, vals);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) outw[lane * 17 + i] = vals[i];
-            __syncwarp();
-            if (c0 + col < NC) {
-#pragma unroll 4
-                for (int rr = half; rr < 32; rr += 2) {
-                    const int r = rw + rr;
-                    if (r < cnt) Y[(row_e[buf][r] * m + v) * NC + c0 + col] = outw[rr * 17 + col];
-                }
-            }
-            __syncwarp();
-        }
-    };
-
-    for (int64_t it = i0; it < i1 && !failed; ++it) {
-        const int buf = (int)((it - i0) & 1);
-        if (it > i0) {  // MMA(it-1) done: A and B may be overwritten
-            const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
-            if (__syncthreads_or(!ok)) {  // the CTA leaves together, so no barrier is left waiting
-                failed = true;
-                if (tid == 0) atomicExch(error, 1);
-                break;
-            }
-            phase ^= 1;
-            asm volatile("tcgen05.fence::after_thread_sync;");
-        }
-        const int d = tile_d[it];
+    // gather + split X(it) into buffer b: row indices first (one coalesced load per row),
+    // then each warp issues all loads of its rows before converting and storing them
+    auto gather = [&](int64_t it, int b) {
         const int64_t p0 = tile_begin[it];
         const int cnt = tile_count[it];
-        if (d != cur_d) {
-            const uint4* src = bimg + (size_t)d * (2 * S::B_BYTES / 16);
-            uint4* dst = reinterpret_cast<uint4*>(b_hi);
-            for (int i = tid; i < 2 * S::B_BYTES / 16; i += 32 * kTcWarps) dst[i] = src[i];
-            cur_d = d;
+        if (tid < S::NT) {
+            row_src[b][tid] = tid < cnt ? pair_src[p0 + tid] : 0;
+            row_e[b][tid] = tid < cnt ? pair_e[p0 + tid] : 0;
         }
-        if (tid < kTcRows) {
-            row_src[tid] = tid < cnt ? pair_src[p0 + tid] : 0;
-            row_e[buf][tid] = tid < cnt ? pair_e[p0 + tid] : 0;
-        }
+        if (tid == 0) row_cnt[b] = cnt;
         __syncthreads();
-        // gather + split: warp w holds rows w + 16 j; every load is issued before any use
+        unsigned char* xh = xbuf + (size_t)b * 2 * S::X_BYTES;
+        unsigned char* xl = xh + S::X_BYTES;
         float x[RPW][S::KA];
 #pragma unroll
         for (int j = 0; j < RPW; ++j) {
             const int r = warp + kTcWarps * j;
-            const float* src = M + ((int64_t)row_src[r] * m + v) * NC;
+            const float* src = M + ((int64_t)row_src[b][r] * m + v) * NC;
 #pragma unroll
             for (int a = 0; a < S::KA; ++a) {
                 const int k = a * 32 + lane;
@@ -255,37 +252,109 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 const int k = a * 32 + lane;
                 const uint32_t hi = cvt_tf32(x[j][a]);
                 const uint32_t lo = cvt_tf32(x[j][a] - __uint_as_float(hi));
-                const uint32_t off = sw128_offset(r, k, kTcRows);
-                *reinterpret_cast<uint32_t*>(a_hi + off) = hi;
-                *reinterpret_cast<uint32_t*>(a_lo + off) = lo;
+                const uint32_t off = sw128_offset(r, k, S::NT);
+                *reinterpret_cast<uint32_t*>(xh + off) = hi;
+                *reinterpret_cast<uint32_t*>(xl + off) = lo;
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    };
+    // the table of offset d into TMEM columns [COL_AHI, COL_AHI + KP) and [COL_ALO, ...):
+    // warp q (< 4) writes lanes 32q .. 32q + 31 (output slots)
+    auto load_table = [&](int d) {
+        if (warp < 4) {
+            const uint32_t* src = timg + (size_t)d * S::IMG_WORDS;
+#pragma unroll 1
+            for (int part = 0; part < 2; ++part)
+#pragma unroll 1
+                for (int k0 = 0; k0 < S::KP; k0 += 16) {
+                    uint32_t r[16];
+                    const uint4* row = reinterpret_cast<const uint4*>(src + ((size_t)part * 128 + 32 * warp + lane) * S::KP + k0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const uint4 u = __ldg(row + q);
+                        r[4 * q] = u.x;
+                        r[4 * q + 1] = u.y;
+                        r[4 * q + 2] = u.z;
+                        r[4 * q + 3] = u.w;
+                    }
+                    tmem_st16(tmem + ((uint32_t)(32 * warp) << 16) +
+                                  (uint32_t)((part ? S::COL_ALO : S::COL_AHI) + k0),
+                              r);
+                }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        }
+    };
+    auto issue = [&](int b) {  // thread 0: MMA of buffer b into accumulator b, then commit
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t xh = smem_u32(xbuf + (size_t)b * 2 * S::X_BYTES), xl = xh + S::X_BYTES;
+        const uint32_t dcol = tmem + (uint32_t)(S::COL_D0 + b * S::NT);
+        const uint32_t As[3] = {(uint32_t)S::COL_AHI, (uint32_t)S::COL_ALO, (uint32_t)S::COL_AHI};
+        const uint32_t Bs[3] = {xl, xh, xh};  // A_hi X_lo, A_lo X_hi, then A_hi X_hi
+        uint32_t acc = 0;
+#pragma unroll
+        for (int t = 0; t < 3; ++t)
+#pragma unroll
+            for (int s = 0; s < S::KSTEPS; ++s) {
+                const uint32_t kb = (uint32_t)((s >> 2) * S::NT * 128 + (s & 3) * 32);
+                umma_tf32_ts(dcol, tmem + As[t] + (uint32_t)(8 * s), sw128_desc(Bs[t] + kb), idesc, acc);
+                acc = 1;
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    };
+    // accumulator b: lanes = slots, columns = pairs; warp (quarter q, column group g)
+    auto epilogue = [&](int b) {
+        const int q = warp & 3, g = warp >> 2;
+        const int n = 32 * q + lane;  // slot of this thread
+        if (32 * q >= NC) return;     // the whole quarter is padding
+        const int cnt = row_cnt[b];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c0 = 32 * g + 16 * h;  // first pair of this load
+            if (c0 >= cnt) break;
+            float vals[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + b * S::NT + c0), vals);
+            if (n < NC) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (c0 + i < cnt) Y[(row_e[b][c0 + i] * m + v) * NC + n] = vals[i];
+            }
+        }
+    };
+
+    int cur_d = tile_d[i0];
+    uint32_t phase = 0;
+    bool failed = false;
+    gather(i0, 0);
+    load_table(cur_d);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (tid == 0) issue(0);
+    __syncwarp();
+    for (int64_t it = i0 + 1; it < i1; ++it) {
+        const int b = (int)((it - i0) & 1);
+        gather(it, b);
+        const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
+        if (__syncthreads_or(!ok)) {  // the CTA leaves together, so no barrier is left waiting
+            failed = true;
+            if (tid == 0) atomicExch(error, 1);
+            break;
+        }
+        phase ^= 1;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const int d = tile_d[it];
+        if (d != cur_d) {
+            load_table(d);
+            cur_d = d;
+        }
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t sa_hi = smem_u32(a_hi), sa_lo = smem_u32(a_lo);
-            const uint32_t sb_hi = smem_u32(b_hi), sb_lo = smem_u32(b_lo);
-            const uint32_t dcol = tmem + (uint32_t)(buf * S::TMEM_COLS);
-            uint32_t acc = 0;
-            const uint32_t As[3] = {sa_lo, sa_hi, sa_hi}, Bs[3] = {sb_hi, sb_lo, sb_hi};
-#pragma unroll
-            for (int t = 0; t < 3; ++t)
-#pragma unroll
-                for (int s = 0; s < S::KSTEPS; ++s) {
-                    const uint32_t ka = (uint32_t)((s >> 2) * kTcRows * 128 + (s & 3) * 32);
-                    const uint32_t kb = (uint32_t)((s >> 2) * S::NP * 128 + (s & 3) * 32);
-                    umma_tf32(dcol, sw128_desc(As[t] + ka), sw128_desc(Bs[t] + kb), idesc, acc);
-                    acc = 1;
-                }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&mbar))
-                         : "memory");
-        }
+        if (tid == 0) issue(b);
         __syncwarp();
-        if (it > i0) epilogue(buf ^ 1, prev_cnt);  // overlaps MMA(it)
-        prev_cnt = cnt;
+        epilogue(b ^ 1);  // overlaps MMA(it)
+        __syncthreads();   // TMEM loads of accumulator b^1 and row_e[b^1] are done
     }
     if (!failed) {
         const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
@@ -293,25 +362,25 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             if (tid == 0) atomicExch(error, 1);
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            epilogue((int)((i1 - 1 - i0) & 1), prev_cnt);
+            epilogue((int)((i1 - 1 - i0) & 1));
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * S::TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS));
     }
 }
 
-// Host: the table images, hi and lo parts per offset, in the SW128 K-major layout with
-// B[n][k] = A_d[n][k] (output slot n, input slot k), zero padding.
+// Host: the table images for tensor memory, per offset a hi and a lo part, each
+// [128 output slots][KP input slots] of tf32 bits (round to nearest, ties away),
+// zero-padded: image[d][part][n][k] = A_d[n][k].
 template <int P>
 void build_tc_table_images(const std::vector<double>& m2l, std::vector<uint32_t>& img) {
-    using S = TcShape<P>;
+    using S = TcTs<P>;
     constexpr int NC = S::NC;
-    const size_t part = S::B_BYTES / 4;
-    img.assign(316 * 2 * part, 0u);
+    img.assign((size_t)316 * S::IMG_WORDS, 0u);
     for (int d = 0; d < 316; ++d)
         for (int n = 0; n < NC; ++n)
             for (int k = 0; k < NC; ++k) {
@@ -325,9 +394,9 @@ void build_tc_table_images(const std::vector<double>& m2l, std::vector<uint32_t>
                 uint32_t rb;
                 std::memcpy(&rb, &rem, 4);
                 uint32_t lo = tf32_round_bits(rb);
-                size_t o = sw128_offset(n, k, S::NP) / 4;
-                img[(size_t)d * 2 * part + o] = hi;
-                img[(size_t)d * 2 * part + part + o] = lo;
+                size_t base = (size_t)d * S::IMG_WORDS + (size_t)n * S::KP + k;
+                img[base] = hi;
+                img[base + (size_t)128 * S::KP] = lo;
             }
 }
 
