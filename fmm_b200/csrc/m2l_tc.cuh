@@ -192,15 +192,18 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   int* __restrict__ error) {
     using S = TcTs<P>;
     constexpr int NC = S::NC;
-    constexpr int RPW = S::NT / kTcWarps;  // gathered rows per warp
+    constexpr int kGather = kTcWarps / 2;     // warps 8..15 gather, warps 0..7 run the epilogue
+    constexpr int RPW = S::NT / kGather;      // gathered rows per gather warp
     extern __shared__ unsigned char smem_raw[];
     unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 bufs][hi, lo]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    __shared__ uint64_t mbar;
+    __shared__ uint64_t mbar[2];  // MMA(k) commits to mbar[k & 1] (k counted from the CTA's first tile)
     __shared__ uint32_t tmem_base;
-    __shared__ int32_t row_src[2][S::NT];
-    __shared__ int64_t row_e[2][S::NT];
-    __shared__ int32_t row_cnt[2];
+    // tile k's row indices live from its gather (iteration k-1) to its epilogue
+    // (iteration k+1): three slots, slot (k - i0) % 3
+    __shared__ int32_t row_src[3][S::NT];
+    __shared__ int64_t row_e[3][S::NT];
+    __shared__ int32_t row_cnt[3];
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
     const int64_t i1 = (int64_t)(blockIdx.x + 1) * ntiles / gridDim.x;
     if (i0 >= i1) return;
@@ -211,7 +214,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -220,9 +224,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     const uint32_t tmem = tmem_base;
     constexpr uint32_t idesc = tf32_idesc_ts<S::NT>();
 
-    // gather + split X(it) into buffer b: row indices first (one coalesced load per row),
-    // then each warp issues all loads of its rows before converting and storing them
-    auto gather = [&](int64_t it, int b) {
+    auto rows = [&](int64_t it, int b) {  // threads 0..127: the tile's row indices into meta slot b
         const int64_t p0 = tile_begin[it];
         const int cnt = tile_count[it];
         if (tid < S::NT) {
@@ -230,13 +232,17 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             row_e[b][tid] = tid < cnt ? pair_e[p0 + tid] : 0;
         }
         if (tid == 0) row_cnt[b] = cnt;
-        __syncthreads();
-        unsigned char* xh = xbuf + (size_t)b * 2 * S::X_BYTES;
+    };
+    // gather + split X into buffer xb from meta slot b (gather warps, gw = 0..kGather-1):
+    // every load of a warp's rows is issued before any is converted and stored
+    auto gather = [&](int xb, int b, int gw) {
+        const int cnt = row_cnt[b];
+        unsigned char* xh = xbuf + (size_t)xb * 2 * S::X_BYTES;
         unsigned char* xl = xh + S::X_BYTES;
         float x[RPW][S::KA];
 #pragma unroll
         for (int j = 0; j < RPW; ++j) {
-            const int r = warp + kTcWarps * j;
+            const int r = gw + kGather * j;
             const float* src = M + ((int64_t)row_src[b][r] * m + v) * NC;
 #pragma unroll
             for (int a = 0; a < S::KA; ++a) {
@@ -246,7 +252,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         }
 #pragma unroll
         for (int j = 0; j < RPW; ++j) {
-            const int r = warp + kTcWarps * j;
+            const int r = gw + kGather * j;
 #pragma unroll
             for (int a = 0; a < S::KA; ++a) {
                 const int k = a * 32 + lane;
@@ -259,8 +265,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     };
-    // the table of offset d into TMEM columns [COL_AHI, COL_AHI + KP) and [COL_ALO, ...):
-    // warp q (< 4) writes lanes 32q .. 32q + 31 (output slots)
+    // the table of offset d into TMEM (warps 0..3, one per lane quarter)
     auto load_table = [&](int d) {
         if (warp < 4) {
             const uint32_t* src = timg + (size_t)d * S::IMG_WORDS;
@@ -269,7 +274,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
 #pragma unroll 1
                 for (int k0 = 0; k0 < S::KP; k0 += 16) {
                     uint32_t r[16];
-                    const uint4* row = reinterpret_cast<const uint4*>(src + ((size_t)part * 128 + 32 * warp + lane) * S::KP + k0);
+                    const uint4* row =
+                        reinterpret_cast<const uint4*>(src + ((size_t)part * 128 + 32 * warp + lane) * S::KP + k0);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const uint4 u = __ldg(row + q);
@@ -278,14 +284,13 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                         r[4 * q + 2] = u.z;
                         r[4 * q + 3] = u.w;
                     }
-                    tmem_st16(tmem + ((uint32_t)(32 * warp) << 16) +
-                                  (uint32_t)((part ? S::COL_ALO : S::COL_AHI) + k0),
+                    tmem_st16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((part ? S::COL_ALO : S::COL_AHI) + k0),
                               r);
                 }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         }
     };
-    auto issue = [&](int b) {  // thread 0: MMA of buffer b into accumulator b, then commit
+    auto issue = [&](int b) {  // thread 0: MMA of X buffer b into accumulator b, commit to mbar[b]
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t xh = smem_u32(xbuf + (size_t)b * 2 * S::X_BYTES), xl = xh + S::X_BYTES;
         const uint32_t dcol = tmem + (uint32_t)(S::COL_D0 + b * S::NT);
@@ -301,21 +306,21 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 acc = 1;
             }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(&mbar))
+                         smem_u32(&mbar[b]))
                      : "memory");
     };
-    // accumulator b: lanes = slots, columns = pairs; warp (quarter q, column group g)
-    auto epilogue = [&](int b) {
-        const int q = warp & 3, g = warp >> 2;
-        const int n = 32 * q + lane;  // slot of this thread
-        if (32 * q >= NC) return;     // the whole quarter is padding
+    // accumulator db with meta slot b (epilogue warps 0..7): lanes = slots, columns = pairs
+    auto epilogue = [&](int db, int b) {
+        const int q = warp & 3, g = warp >> 2;  // lane quarter, column group (64 pairs)
+        const int n = 32 * q + lane;
+        if (32 * q >= NC) return;  // the whole quarter is padding
         const int cnt = row_cnt[b];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c0 = 32 * g + 16 * h;  // first pair of this load
+        for (int h = 0; h < 4; ++h) {
+            const int c0 = 64 * g + 16 * h;
             if (c0 >= cnt) break;
             float vals[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + b * S::NT + c0), vals);
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + db * S::NT + c0), vals);
             if (n < NC) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
@@ -323,47 +328,62 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             }
         }
     };
-
-    int cur_d = tile_d[i0];
-    uint32_t phase = 0;
+    // MMA(k) done: all threads wait, the CTA agrees on the outcome
     bool failed = false;
-    gather(i0, 0);
+    auto wait_mma = [&](int64_t k) {
+        const int b = (int)((k - i0) & 1);
+        const uint32_t parity = (uint32_t)(((k - i0) >> 1) & 1);
+        const bool ok = mbar_wait_bounded(smem_u32(&mbar[b]), parity, 4000000000LL);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            if (tid == 0) atomicExch(error, 1);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+    };
+
+    auto meta = [&](int64_t k) { return (int)((k - i0) % 3); };
+    int cur_d = tile_d[i0];
+    rows(i0, 0);
+    __syncthreads();
+    if (warp >= kGather) gather(0, 0, warp - kGather);
     load_table(cur_d);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (tid == 0) issue(0);
     __syncwarp();
-    for (int64_t it = i0 + 1; it < i1; ++it) {
+    for (int64_t it = i0; it < i1; ++it) {
         const int b = (int)((it - i0) & 1);
-        gather(it, b);
-        const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
-        if (__syncthreads_or(!ok)) {  // the CTA leaves together, so no barrier is left waiting
-            failed = true;
-            if (tid == 0) atomicExch(error, 1);
-            break;
+        if (it > i0) {
+            wait_mma(it - 1);  // X buffer b^1 and accumulator b^1 are free / readable
+            if (failed) break;
         }
-        phase ^= 1;
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const int d = tile_d[it];
-        if (d != cur_d) {
-            load_table(d);
-            cur_d = d;
+        const bool next = it + 1 < i1;
+        if (next) rows(it + 1, meta(it + 1));
+        __syncthreads();
+        if (warp >= kGather) {
+            if (next) gather(b ^ 1, meta(it + 1), warp - kGather);
+        } else if (it > i0) {
+            epilogue(b ^ 1, meta(it - 1));
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
-        if (tid == 0) issue(b);
-        __syncwarp();
-        epilogue(b ^ 1);  // overlaps MMA(it)
-        __syncthreads();   // TMEM loads of accumulator b^1 and row_e[b^1] are done
+        if (next) {
+            const int d = tile_d[it + 1];
+            if (d != cur_d) {  // MMA(it) still reads the old table: wait for it first
+                wait_mma(it);
+                if (failed) break;
+                load_table(d);
+                cur_d = d;
+                asm volatile("tcgen05.fence::before_thread_sync;");
+                __syncthreads();
+            }
+            if (tid == 0) issue(b ^ 1);
+            __syncwarp();
+        }
     }
     if (!failed) {
-        const bool ok = mbar_wait_bounded(smem_u32(&mbar), phase, 4000000000LL);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(error, 1);
-        } else {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            epilogue((int)((i1 - 1 - i0) & 1));
-        }
+        wait_mma(i1 - 1);
+        if (!failed && warp < kGather) epilogue((int)((i1 - 1 - i0) & 1), meta(i1 - 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
