@@ -321,14 +321,14 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
             T s = with_l2l ? Yo[(b * m + v) * NC + i] : T(0);
             int64_t e = e0;
             for (; e + 4 <= e1; e += 4) {
-                const T y0 = Yv[(e * m + v) * NC + i], y1 = Yv[((e + 1) * m + v) * NC + i];
-                const T y2 = Yv[((e + 2) * m + v) * NC + i], y3 = Yv[((e + 3) * m + v) * NC + i];
+                const T y0 = __ldcs(Yv + (e * m + v) * NC + i), y1 = __ldcs(Yv + ((e + 1) * m + v) * NC + i);
+                const T y2 = __ldcs(Yv + ((e + 2) * m + v) * NC + i), y3 = __ldcs(Yv + ((e + 3) * m + v) * NC + i);
                 s += y0;
                 s += y1;
                 s += y2;
                 s += y3;
             }
-            for (; e < e1; ++e) s += Yv[(e * m + v) * NC + i];
+            for (; e < e1; ++e) s += __ldcs(Yv + (e * m + v) * NC + i);
             Lc[(b * m + v) * NC + i] = s;
         }
 }
@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
 #pragma unroll
             for (int j = 0; j < JN; ++j) {
                 int n = tx + 16 * j;
-                if (n < NC) y[n] = acc[i][j];
+                if (n < NC) __stcs(y + n, acc[i][j]);  // read once by the reduce: stream past L2
             }
         }
     }

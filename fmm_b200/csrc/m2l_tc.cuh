@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             if (n < NC) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
-                    if (c0 + i < cnt) Y[(row_e[b][c0 + i] * m + v) * NC + n] = vals[i];
+                    if (c0 + i < cnt) __stcs(Y + (row_e[b][c0 + i] * m + v) * NC + n, vals[i]);  // streamed
             }
         }
     };
