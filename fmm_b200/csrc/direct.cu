@@ -88,17 +88,22 @@ __global__ void direct_combine_kernel(const double* __restrict__ part, int64_t n
         for (int k = 0; k < 3; ++k) g[3 * t + k] = s[k + 1].value() / f;
 }
 
-thread_local std::string g_err;
-
 }  // namespace
+
+namespace fmmb {
+void set_last_error(const std::string& message);  // evaluator.cu
+}
 
 extern "C" int fmmgpu_direct_sum(size_t ns, const double* src, const double* q, size_t nt, const double* tgt,
                                  double* phi, double* grad, int device) {
     auto fail = [](cudaError_t e) {
-        g_err = cudaGetErrorString(e);
+        fmmb::set_last_error(std::string("fmmgpu_direct_sum: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? FMMGPU_DEVICE_MEMORY : FMMGPU_DEVICE_ERROR;
     };
-    if ((ns && (!src || !q)) || (nt && (!tgt || !phi))) return FMMGPU_INVALID_ARGUMENT;
+    if ((ns && (!src || !q)) || (nt && (!tgt || !phi))) {
+        fmmb::set_last_error("fmmgpu_direct_sum: null buffer");
+        return FMMGPU_INVALID_ARGUMENT;
+    }
     if (nt == 0) return FMMGPU_OK;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(e);

@@ -21,6 +21,13 @@ namespace {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+// The message fmmgpu_last_error returns on this thread (also set by direct.cu).
+void set_last_error(const std::string& message) { g_last_error = message; }
+
+namespace {
+
 struct Failure : std::runtime_error {
     int status;
     Failure(int s, const std::string& msg) : std::runtime_error(msg), status(s) {}
