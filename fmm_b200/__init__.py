@@ -69,6 +69,7 @@ def lib():
             "fmmgpu_fmm_set_kinds": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
+            "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
             "fmmgpu_status_string": (C.c_char_p, [C.c_int]),
             "fmmgpu_last_error": (C.c_char_p, []),
         }

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -88,6 +89,15 @@ __global__ void direct_combine_kernel(const double* __restrict__ part, int64_t n
         for (int k = 0; k < 3; ++k) g[3 * t + k] = s[k + 1].value() / f;
 }
 
+// Chunking of the sources shared by both entry points (same chunks, same bits).
+int direct_chunks(size_t ns) { return ns > (1 << 16) ? 128 : 1; }
+
+// Scratch of fmmgpu_direct_sum_noalloc: the per-chunk partial sums, nchunks x nt x 4
+// doubles.  A module-scope array, so that the call allocates nothing; one per device.
+__device__ __align__(256) double g_noalloc_part[FMMGPU_DIRECT_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+constexpr int kMaxDevices = 64;
+
 }  // namespace
 
 namespace fmmb {
@@ -107,7 +117,7 @@ extern "C" int fmmgpu_direct_sum(size_t ns, const double* src, const double* q, 
     if (nt == 0) return FMMGPU_OK;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(e);
-    const int nchunks = ns > (1 << 16) ? 128 : 1;
+    const int nchunks = direct_chunks(ns);
     const int64_t chunk = ((int64_t)ns + nchunks - 1) / nchunks;
     double *dsrc = nullptr, *dq = nullptr, *dtgt = nullptr, *dpart = nullptr, *dphi = nullptr, *dg = nullptr;
     auto cleanup = [&] {
@@ -141,4 +151,60 @@ extern "C" int fmmgpu_direct_sum(size_t ns, const double* src, const double* q, 
     }
     cleanup();
     return e == cudaSuccess ? FMMGPU_OK : fail(e);
+}
+
+// The same sums on device buffers with the scratch in g_noalloc_part: no device or host
+// allocation, no synchronisation.  Its address on each device is looked up once, under a
+// lock, by the first call there.  Every scratch slot the combine reads is written by the
+// partial kernel earlier in the same call, so nothing in it has to start at zero.
+extern "C" int fmmgpu_direct_sum_noalloc(size_t ns, const double* src, const double* q, size_t nt,
+                                         const double* tgt, double* phi, double* grad, int device,
+                                         void* stream) {
+    if ((ns && (!src || !q)) || (nt && (!tgt || !phi))) {
+        fmmb::set_last_error("fmmgpu_direct_sum_noalloc: null buffer");
+        return FMMGPU_INVALID_ARGUMENT;
+    }
+    if (device < 0 || device >= kMaxDevices) {
+        fmmb::set_last_error("fmmgpu_direct_sum_noalloc: device ordinal out of range");
+        return FMMGPU_INVALID_ARGUMENT;
+    }
+    const int nchunks = direct_chunks(ns);
+    const size_t capacity = FMMGPU_DIRECT_NOALLOC_SCRATCH_BYTES / (4 * sizeof(double));  // (chunk, target) slots
+    if (nt > capacity / (size_t)nchunks) {
+        fmmb::set_last_error("fmmgpu_direct_sum_noalloc: " + std::to_string(nt) + " targets x " +
+                             std::to_string(nchunks) + " source chunks need " +
+                             std::to_string((unsigned long long)nt * nchunks * 4 * sizeof(double)) +
+                             " bytes of scratch; the static scratch holds " +
+                             std::to_string((unsigned long long)FMMGPU_DIRECT_NOALLOC_SCRATCH_BYTES) +
+                             " bytes (at most " + std::to_string(capacity / nchunks) + " targets here)");
+        return FMMGPU_INVALID_ARGUMENT;
+    }
+    if (nt == 0) return FMMGPU_OK;
+    auto fail = [](const char* what, cudaError_t e) {
+        fmmb::set_last_error(std::string("fmmgpu_direct_sum_noalloc: ") + what + ": " + cudaGetErrorString(e));
+        return FMMGPU_DEVICE_ERROR;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail("cudaSetDevice", e);
+    static std::mutex mu;
+    static double* scratch[kMaxDevices] = {};
+    double* part;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!scratch[device]) {
+            void* addr = nullptr;
+            e = cudaGetSymbolAddress(&addr, g_noalloc_part);
+            if (e != cudaSuccess) return fail("cudaGetSymbolAddress", e);
+            scratch[device] = static_cast<double*>(addr);
+        }
+        part = scratch[device];
+    }
+    const int64_t chunk = ((int64_t)ns + nchunks - 1) / nchunks;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    dim3 grid((unsigned)((nt + 127) / 128), (unsigned)nchunks);
+    direct_partial_kernel<<<grid, 128, 0, s>>>(src, q, (int64_t)ns, tgt, (int64_t)nt, chunk, grad != nullptr, part);
+    direct_combine_kernel<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(part, (int64_t)nt, nchunks, grad != nullptr,
+                                                                       phi, grad);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? FMMGPU_OK : fail("launch", e);
 }

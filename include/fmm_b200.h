@@ -131,6 +131,32 @@ int fmmgpu_fmm_tables(const fmmgpu_fmm* fmm, double* m2l, double* m2m, double* l
 int fmmgpu_direct_sum(size_t nsources, const double* sources, const double* charges, size_t ntargets,
                       const double* targets, double* potential, double* gradient, int device);
 
+/* The same direct sum on DEVICE buffers, allocating nothing.  No counterpart in the
+ * reference (its direct_sum, fmm-ref/src/p2p.rs:147-186, is host code); the results are
+ * bit-identical to fmmgpu_direct_sum's.
+ *
+ * For callers that cannot allocate: code that runs beside a built FMM whose plan and
+ * stores fill the device (a cudaMalloc there fails or takes memory the evaluator needs),
+ * and code on a stream that must not be stalled (cudaFree synchronises the whole device,
+ * so the allocating entry point waits for every stream, the evaluator's included).
+ *
+ * Its scratch is one module-scope device array of FMMGPU_DIRECT_NOALLOC_SCRATCH_BYTES
+ * (16 MiB) per device: ntargets x (128 if nsources > 65536, else 1) x 32 bytes must fit,
+ * i.e. at most 4096 targets above 65536 sources and 524288 otherwise; larger calls
+ * return FMMGPU_INVALID_ARGUMENT before any device work.  No part of the scratch has to
+ * start at zero.  Queued on `stream` (a cudaStream_t; NULL = the default stream), not
+ * synchronised; device errors surface at the caller's next synchronisation.
+ *
+ * Calls share that one scratch: two calls in flight at once on one device (different
+ * streams, or threads without ordering) race on it and give wrong results.  Calls
+ * queued one after another on one stream are safe.  The first call on each device does
+ * one-time setup (cudaSetDevice and the lookup of the scratch address, which may load
+ * the library's module there): make that call before any stream capture begins. */
+#define FMMGPU_DIRECT_NOALLOC_SCRATCH_BYTES (16u << 20)
+int fmmgpu_direct_sum_noalloc(size_t nsources, const double* sources, const double* charges, size_t ntargets,
+                              const double* targets, double* potential, double* gradient, int device,
+                              void* stream);
+
 const char* fmmgpu_status_string(int status);
 const char* fmmgpu_last_error(void);
 
