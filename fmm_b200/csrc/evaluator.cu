@@ -13,6 +13,7 @@
 #include "../../include/fmm_b200.h"
 #include "kernels.cuh"
 #include "m2l_tc.cuh"
+#include "p2p_x2.cuh"
 #include "plan.hpp"
 
 namespace fmmb {
@@ -164,7 +165,7 @@ struct Evaluator final : EvaluatorBase {
     int num_sms = 148;
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
-    DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64;
+    DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec;
     P2pItems items{};
     ClosePairs close{};
     int64_t nclose = 0;
@@ -258,7 +259,15 @@ struct Evaluator final : EvaluatorBase {
         build_m2l_batches(kGemmPairs);
         if (kTensor) build_tensor_m2l(m2l);
         build_p2p_items();
-        if (kMixed) build_close_pairs(us, ut);
+        if (kMixed) {
+            build_close_pairs(us, ut);
+            near_rec.alloc(sizeof(NearRec) * (pl.near.nnz() + 1));
+            if (pl.nleaves())
+                near_record_kernel<<<(unsigned)((pl.nleaves() + 127) / 128), 128>>>(dp, (int64_t)pl.nleaves(),
+                                                                                   near_rec.as<NearRec>());
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaDeviceSynchronize());
+        }
         close_pairs = nclose;
         Y.alloc(sizeof(T) * (size_t)m * NC * (pl.v.nnz() + 1));
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
@@ -486,7 +495,7 @@ struct Evaluator final : EvaluatorBase {
                                &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e,
                                &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
-                               &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error};
+                               &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -607,6 +616,21 @@ struct Evaluator final : EvaluatorBase {
         if (!items.count) return;
         const unsigned grid = (unsigned)((items.count + kP2pWarps - 1) / kP2pWarps);
         timer.run(kP2P, [&] {
+            if constexpr (kMixed) {
+                const unsigned gx2 = (unsigned)((items.count + kX2Warps - 1) / kX2Warps);
+                const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
+                const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
+                const auto* q = reinterpret_cast<const float*>(sq.ptr);
+                if (gradients)
+                    p2p_x2_kernel<true><<<gx2, 32 * kX2Warps, 0, stream>>>(
+                        dp, items, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(),
+                        far_g.as<double>(), d_phi, d_grad);
+                else
+                    p2p_x2_kernel<false><<<gx2, 32 * kX2Warps, 0, stream>>>(
+                        dp, items, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(),
+                        nullptr, d_phi, nullptr);
+                return;
+            }
             if (gradients)
                 p2p_kernel<T, true, kMixed><<<grid, 32 * kP2pWarps, 0, stream>>>(
                     dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
