@@ -40,7 +40,7 @@ class Info(C.Structure):
     _fields_ = [("nlevels", C.c_int), ("nboxes", C.c_int64), ("nleaves", C.c_int64),
                 ("nsources", C.c_int64), ("ntargets", C.c_int64), ("near_pairs", C.c_int64),
                 ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
-                ("device_bytes", C.c_int64), ("close_pairs", C.c_int64)]
+                ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64)]
 
 
 def lib():

@@ -129,6 +129,11 @@ struct EvaluatorBase {
     virtual int device_status() { return 0; }
     int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
+    int64_t launches = 0;  // kernels launched by the last evaluation
+    unsigned counted(unsigned grid) {  // wraps the grid of every evaluation launch
+        ++launches;
+        return grid;
+    }
     virtual ~EvaluatorBase() = default;
     virtual void evaluate(const double* d_charges, double* d_phi, double* d_grad) = 0;
 };
@@ -506,10 +511,11 @@ struct Evaluator final : EvaluatorBase {
         const int L = plan.nlevels - 1;
         const size_t nleaves = plan.nleaves();
         timer.begin();
+        launches = 0;
         // charge load into leaf order
         timer.run(kLoad, [&] {
             if (ns > 0)
-                charge_load_kernel<T><<<(unsigned)((ns + 255) / 256), 256, 0, stream>>>(
+                charge_load_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
                     d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
             // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
             int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
@@ -534,11 +540,11 @@ struct Evaluator final : EvaluatorBase {
         timer.run(kP2M, [&] {
             if (nleaves) {
                 if (kBfly && m == 1)
-                    expand_bfly_kernel<P, false><<<(unsigned)nleaves, 32, 0, stream>>>(
+                    expand_bfly_kernel<P, false><<<counted((unsigned)nleaves), 32, 0, stream>>>(
                         dp, 0, (int64_t)nleaves, reinterpret_cast<const float4*>(spos.ptr),
                         reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
                 else
-                    expand_kernel<P, T, false><<<(unsigned)nleaves, 32, exp_smem, stream>>>(
+                    expand_kernel<P, T, false><<<counted((unsigned)nleaves), 32, exp_smem, stream>>>(
                         dp, 0, (int64_t)nleaves, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
             }
         });
@@ -547,12 +553,12 @@ struct Evaluator final : EvaluatorBase {
                 const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
                 const int64_t n = m2m_start[l + 1] - m2m_start[l];
                 if (nt)
-                    m2l_gemm_kernel<P, T><<<(unsigned)nt, 256, gemm_smem, stream>>>(
+                    m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
                         oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
                         oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
                         m2m_tab.as<T>(), M.as<T>(), Yo.as<T>());
                 if (n)
-                    m2m_reduce_kernel<P, T><<<(unsigned)n, round32(NC), 0, stream>>>(
+                    m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
                         dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, Yo.as<T>(), M.as<T>());
             });
         }
@@ -563,7 +569,7 @@ struct Evaluator final : EvaluatorBase {
                     timer.run(kM2L, [&] {
                         const unsigned grid = (unsigned)std::min<int64_t>(tc_ntiles, num_sms);
                         for (int v = 0; v < m; ++v)
-                            m2l_tc_kernel<P><<<grid, 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                            m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
                                 tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
                                 tc_ntiles, tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v,
                                 tc_bimg.as<uint32_t>(), reinterpret_cast<const float*>(M.ptr),
@@ -572,7 +578,7 @@ struct Evaluator final : EvaluatorBase {
             }
         } else if (ntiles)
             timer.run(kM2L, [&] {
-                m2l_gemm_kernel<P, T><<<(unsigned)ntiles, 256, gemm_smem, stream>>>(
+                m2l_gemm_kernel<P, T><<<counted((unsigned)ntiles), 256, gemm_smem, stream>>>(
                     tile_d.as<int32_t>(), tile_begin.as<int64_t>(), tile_count.as<int32_t>(), pair_e.as<int64_t>(),
                     pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
             });
@@ -582,20 +588,20 @@ struct Evaluator final : EvaluatorBase {
             timer.run(kL2L, [&] {
                 const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
                 if (nt)
-                    m2l_gemm_kernel<P, T><<<(unsigned)nt, 256, gemm_smem, stream>>>(
+                    m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
                         oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
                         oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
                         l2l_tab.as<T>(), Lc.as<T>(), Yo.as<T>());
-                local_reduce_kernel<P, T><<<(unsigned)(b1 - b0), round32(NC), 0, stream>>>(
+                local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
                     dp, b0, b1, m, l >= 3, Yo.as<T>(), Y.as<T>(), Lc.as<T>());
             });
             timer.run(kP2L, [&] {
                 if (kBfly && m == 1)
-                    expand_bfly_kernel<P, true><<<(unsigned)(b1 - b0), 32, 0, stream>>>(
+                    expand_bfly_kernel<P, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
                         dp, b0, b1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
                         reinterpret_cast<float*>(Lc.ptr));
                 else
-                    expand_kernel<P, T, true><<<(unsigned)(b1 - b0), 32, exp_smem, stream>>>(
+                    expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem, stream>>>(
                         dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
             });
         }
@@ -603,10 +609,10 @@ struct Evaluator final : EvaluatorBase {
         if (nleaves)
             timer.run(kFar, [&] {
                 if (gradients)
-                    leaf_far_kernel<P, T, true><<<(unsigned)nleaves, 64, NC * sizeof(T), stream>>>(
+                    leaf_far_kernel<P, T, true><<<counted((unsigned)nleaves), 64, NC * sizeof(T), stream>>>(
                         dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
                 else
-                    leaf_far_kernel<P, T, false><<<(unsigned)nleaves, 64, NC * sizeof(T), stream>>>(
+                    leaf_far_kernel<P, T, false><<<counted((unsigned)nleaves), 64, NC * sizeof(T), stream>>>(
                         dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
             });
     }
@@ -622,21 +628,21 @@ struct Evaluator final : EvaluatorBase {
                 const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
                 const auto* q = reinterpret_cast<const float*>(sq.ptr);
                 if (gradients)
-                    p2p_x2_kernel<true><<<gx2, 32 * kX2Warps, 0, stream>>>(
+                    p2p_x2_kernel<true><<<counted(gx2), 32 * kX2Warps, 0, stream>>>(
                         dp, items, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(),
                         far_g.as<double>(), d_phi, d_grad);
                 else
-                    p2p_x2_kernel<false><<<gx2, 32 * kX2Warps, 0, stream>>>(
+                    p2p_x2_kernel<false><<<counted(gx2), 32 * kX2Warps, 0, stream>>>(
                         dp, items, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(),
                         nullptr, d_phi, nullptr);
                 return;
             }
             if (gradients)
-                p2p_kernel<T, true, kMixed><<<grid, 32 * kP2pWarps, 0, stream>>>(
+                p2p_kernel<T, true, kMixed><<<counted(grid), 32 * kP2pWarps, 0, stream>>>(
                     dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
                     far_phi.as<double>(), far_g.as<double>(), d_phi, d_grad);
             else
-                p2p_kernel<T, false, kMixed><<<grid, 32 * kP2pWarps, 0, stream>>>(
+                p2p_kernel<T, false, kMixed><<<counted(grid), 32 * kP2pWarps, 0, stream>>>(
                     dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
                     far_phi.as<double>(), nullptr, d_phi, nullptr);
         });
@@ -891,6 +897,7 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->x_pairs = (int64_t)P.x.nnz();
         info->device_bytes = (int64_t)f->device_bytes;
         info->close_pairs = f->eval ? f->eval->close_pairs : 0;
+        info->launches = f->eval ? f->eval->launches : 0;
     });
 }
 

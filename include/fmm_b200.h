@@ -67,6 +67,7 @@ typedef struct {
     int64_t w_pairs, x_pairs;
     int64_t device_bytes; /* device memory held by the evaluator */
     int64_t close_pairs;  /* near-singular P2P pairs the mixed form evaluates in f64 */
+    int64_t launches;     /* kernels the last evaluation launched (0 before the first) */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;
