@@ -70,6 +70,17 @@ def lib():
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
+            "fmmgpu_op_begin_evaluation": (C.c_int, [vp, dp]),
+            "fmmgpu_op_p2m": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_m2m": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_l2l": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_m2l": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_p2l": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_l2p": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_m2p": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_p2p": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_host_data": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_op_read_output": (C.c_int, [vp, dp, dp]),
             "fmmgpu_status_string": (C.c_char_p, [C.c_int]),
             "fmmgpu_last_error": (C.c_char_p, []),
         }
@@ -226,6 +237,34 @@ class Fmm(Plan):
         phi = np.zeros((m, self.ntargets))
         g = np.zeros((m, self.ntargets, 3)) if self.settings.gradients else None
         _check(lib().fmmgpu_fmm_evaluate(self._h, _ptr(q), _ptr(phi), _ptr(g)))
+        return Output(phi, g)
+
+    def evaluate_levels(self, charges, calls=None):
+        """The same evaluation driven by the level calls of the operator ABI, in the
+        reference evaluator's schedule (fmm-plan/src/evaluator.rs:368-440): upward
+        P2M(l), M2M(l-1) for l = L..0; downward L2L, M2L, P2L for l = 1..L; leaves L2P,
+        M2P, P2P for l = 0..L.  `calls`, if given, overrides that list of
+        (kind, level) pairs."""
+        L = lib()
+        m = self.settings.vectors
+        nl = self.info()["nlevels"]
+        q = np.ascontiguousarray(charges, dtype=np.float64).reshape(self.nsources, m)
+        _check(L.fmmgpu_op_begin_evaluation(self._h, _ptr(q)))
+        if calls is None:
+            calls = []
+            for lv in range(nl - 1, -1, -1):
+                calls.append(("p2m", lv))
+                if lv > 0:
+                    calls.append(("m2m", lv - 1))
+            for lv in range(1, nl):
+                calls += [("l2l", lv), ("m2l", lv), ("p2l", lv)]
+            for lv in range(nl):
+                calls += [("l2p", lv), ("m2p", lv), ("p2p", lv)]
+        for kind, lv in calls:
+            _check(getattr(L, "fmmgpu_op_" + kind)(self._h, lv))
+        phi = np.zeros((m, self.ntargets))
+        g = np.zeros((m, self.ntargets, 3)) if self.settings.gradients else None
+        _check(L.fmmgpu_op_read_output(self._h, _ptr(phi), _ptr(g)))
         return Output(phi, g)
 
     def evaluate_device(self, charges_ptr, potential_ptr, gradient_ptr=None):

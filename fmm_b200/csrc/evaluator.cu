@@ -136,6 +136,9 @@ struct EvaluatorBase {
     }
     virtual ~EvaluatorBase() = default;
     virtual void evaluate(const double* d_charges, double* d_phi, double* d_grad) = 0;
+    virtual void op_begin(const double* d_charges) = 0;
+    virtual void op_level(int kind, int level) = 0;
+    virtual void op_output(double* d_phi, double* d_grad) = 0;
 };
 
 template <int P, typename T>
@@ -163,15 +166,21 @@ struct Evaluator final : EvaluatorBase {
     // M2L batches: pairs of all levels grouped by offset, in tiles
     DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
     int64_t ntiles = 0;
+    // the same pairs in per-level tiles, for the level calls
+    DevBuf ltile_d, ltile_begin, ltile_count;
+    std::vector<int64_t> lvl_tiles;
     // tensor-core M2L (mixed form, p <= 8): tiles of 128 pairs and the table images
     static constexpr bool kTensor = sizeof(T) == 4 && P <= 8;
     DevBuf tc_tile_d, tc_tile_begin, tc_tile_count, tc_pair_e, tc_pair_src, tc_bimg, tc_error;
+    DevBuf tc_ltile_d, tc_ltile_begin, tc_ltile_count;
+    std::vector<int64_t> tc_lvl_tiles;
     int64_t tc_ntiles = 0;
     int num_sms = 148;
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec;
     P2pItems items{};
+    std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
@@ -290,13 +299,17 @@ struct Evaluator final : EvaluatorBase {
 
     void build_tensor_m2l(const std::vector<double>& m2l) {
         if constexpr (kTensor) {
-            std::vector<int32_t> td, tc, ps;
-            std::vector<int64_t> tb, pe;
-            batches(kTcRows, td, tb, tc, pe, ps);
-            tc_ntiles = (int64_t)td.size();
-            tc_tile_d.upload(td);
-            tc_tile_begin.upload(tb);
-            tc_tile_count.upload(tc);
+            Tiles all, lvl;
+            std::vector<int64_t> pe;
+            std::vector<int32_t> ps;
+            batches(kTcRows, all, lvl, tc_lvl_tiles, pe, ps);
+            tc_ntiles = (int64_t)all.d.size();
+            tc_tile_d.upload(all.d);
+            tc_tile_begin.upload(all.begin);
+            tc_tile_count.upload(all.count);
+            tc_ltile_d.upload(lvl.d);
+            tc_ltile_begin.upload(lvl.begin);
+            tc_ltile_count.upload(lvl.count);
             tc_pair_e.upload(pe);
             tc_pair_src.upload(ps);
             std::vector<uint32_t> img;
@@ -312,10 +325,24 @@ struct Evaluator final : EvaluatorBase {
         }
     }
 
-    // V pairs of every level grouped by offset index, then by target box; tiles of up
-    // to `tile` pairs never straddle two offsets.
-    void batches(int tile, std::vector<int32_t>& td, std::vector<int64_t>& tb, std::vector<int32_t>& tc,
-                 std::vector<int64_t>& pe, std::vector<int32_t>& ps) {
+    // Tile lists over the V pairs grouped by offset index, then by target box (pair
+    // positions pe/ps shared by both lists):
+    //  - the evaluation's list: tiles of up to `tile` pairs of one offset, all levels;
+    //  - the level calls' list: the same pairs cut at level boundaries too, ordered by
+    //    (level, offset), with its tile range per level in lstart.
+    struct Tiles {
+        std::vector<int32_t> d, count;
+        std::vector<int64_t> begin;
+        void add(int dd, int64_t b, int64_t n, int tile) {
+            for (int64_t x = b; x < b + n; x += tile) {
+                d.push_back(dd);
+                begin.push_back(x);
+                count.push_back((int32_t)std::min<int64_t>(tile, b + n - x));
+            }
+        }
+    };
+    void batches(int tile, Tiles& all, Tiles& lvl, std::vector<int64_t>& lstart, std::vector<int64_t>& pe,
+                 std::vector<int32_t>& ps) {
         const Plan& pl = plan;
         const size_t nnz = pl.v.nnz();
         std::vector<int64_t> cnt(317, 0);
@@ -323,6 +350,7 @@ struct Evaluator final : EvaluatorBase {
         for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
         pe.assign(nnz, 0);
         ps.assign(nnz, 0);
+        std::vector<int64_t> tbox(nnz, 0);
         std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
         // rows are boxes in order, so pairs of one offset come out ordered by target
         for (size_t b = 0; b + 1 < pl.v.row.size(); ++b)
@@ -330,26 +358,33 @@ struct Evaluator final : EvaluatorBase {
                 int64_t pos = fill[pl.v.aux[e2]]++;
                 pe[pos] = e2;
                 ps[pos] = pl.v.col[e2];
+                tbox[pos] = (int64_t)b;
             }
-        td.clear();
-        tb.clear();
-        tc.clear();
-        for (int d = 0; d < 316; ++d)
-            for (int64_t b = cnt[d]; b < cnt[d + 1]; b += tile) {
-                td.push_back(d);
-                tb.push_back(b);
-                tc.push_back((int32_t)std::min<int64_t>(tile, cnt[d + 1] - b));
+        for (int d = 0; d < 316; ++d) all.add(d, cnt[d], cnt[d + 1] - cnt[d], tile);
+        lstart.assign(pl.nlevels + 1, 0);
+        for (int l = 0; l < pl.nlevels; ++l) {
+            lstart[l] = (int64_t)lvl.d.size();
+            for (int d = 0; d < 316; ++d) {
+                auto b0 = std::lower_bound(tbox.begin() + cnt[d], tbox.begin() + cnt[d + 1], pl.level_start[l]);
+                auto b1 = std::lower_bound(b0, tbox.begin() + cnt[d + 1], pl.level_start[l + 1]);
+                lvl.add(d, b0 - tbox.begin(), b1 - b0, tile);
             }
+        }
+        lstart[pl.nlevels] = (int64_t)lvl.d.size();
     }
 
     void build_m2l_batches(int tile) {
-        std::vector<int32_t> td, tc, ps;
-        std::vector<int64_t> tb, pe;
-        batches(tile, td, tb, tc, pe, ps);
-        ntiles = (int64_t)td.size();
-        tile_d.upload(td);
-        tile_begin.upload(tb);
-        tile_count.upload(tc);
+        Tiles all, lvl;
+        std::vector<int64_t> pe;
+        std::vector<int32_t> ps;
+        batches(tile, all, lvl, lvl_tiles, pe, ps);
+        ntiles = (int64_t)all.d.size();
+        tile_d.upload(all.d);
+        tile_begin.upload(all.begin);
+        tile_count.upload(all.count);
+        ltile_d.upload(lvl.d);
+        ltile_begin.upload(lvl.begin);
+        ltile_count.upload(lvl.count);
         pair_e.upload(pe);
         pair_src.upload(ps);
     }
@@ -414,6 +449,11 @@ struct Evaluator final : EvaluatorBase {
                 il.push_back((int32_t)j);
                 it.push_back(t);
             }
+        item_lstart.assign(plan.nlevels + 1, (int64_t)il.size());
+        for (int l = plan.nlevels - 1; l >= 0; --l) {
+            int64_t first = plan.leaf_level_start[l];
+            item_lstart[l] = std::lower_bound(il.begin(), il.end(), (int32_t)first) - il.begin();
+        }
         item_leaf.upload(il);
         item_t0.upload(it);
         items.leaf = item_leaf.as<int32_t>();
@@ -500,23 +540,20 @@ struct Evaluator final : EvaluatorBase {
                                &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e,
                                &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
-                               &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec};
+                               &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
+                               &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
     }
 
+    // ---- evaluation: every pass, fused where the level structure allows ----
     void evaluate(const double* d_charges, double* d_phi, double* d_grad) override {
-        const int64_t ns = dp.nsrc;
-        const int L = plan.nlevels - 1;
-        const size_t nleaves = plan.nleaves();
         timer.begin();
         launches = 0;
         // charge load into leaf order
         timer.run(kLoad, [&] {
-            if (ns > 0)
-                charge_load_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
-                    d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
+            load_charges(d_charges);
             // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
             int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
             CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * NC * top, stream));
@@ -528,124 +565,203 @@ struct Evaluator final : EvaluatorBase {
         } else {
             run_far();
         }
-        run_near(d_phi, d_grad);
+        if (items.count) timer.run(kP2P, [&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
         CUDA_TRY(cudaGetLastError());
     }
 
     void run_far() {
         const int L = plan.nlevels - 1;
-        const size_t nleaves = plan.nleaves();
         // upward: P2M of every leaf, then M2M from level L-1 up to 0
-        const size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
-        timer.run(kP2M, [&] {
-            if (nleaves) {
-                if (kBfly && m == 1)
-                    expand_bfly_kernel<P, false><<<counted((unsigned)nleaves), 32, 0, stream>>>(
-                        dp, 0, (int64_t)nleaves, reinterpret_cast<const float4*>(spos.ptr),
-                        reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
-                else
-                    expand_kernel<P, T, false><<<counted((unsigned)nleaves), 32, exp_smem, stream>>>(
-                        dp, 0, (int64_t)nleaves, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
-            }
-        });
-        for (int l = L - 1; l >= 0; --l) {
-            timer.run(kM2M, [&] {
-                const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
-                const int64_t n = m2m_start[l + 1] - m2m_start[l];
-                if (nt)
-                    m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
-                        oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
-                        oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
-                        m2m_tab.as<T>(), M.as<T>(), Yo.as<T>());
-                if (n)
-                    m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
-                        dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, Yo.as<T>(), M.as<T>());
-            });
-        }
+        timer.run(kP2M, [&] { p2m_rows(0, (int64_t)plan.nleaves()); });
+        for (int l = L - 1; l >= 0; --l) timer.run(kM2M, [&] { m2m_level(l); });
         // M2L products of every level at once (all multipoles are final here)
-        if (kTensor && m2l_path == 1) {
-            if constexpr (kTensor) {
-                if (tc_ntiles)
-                    timer.run(kM2L, [&] {
-                        const unsigned grid = (unsigned)std::min<int64_t>(tc_ntiles, num_sms);
-                        for (int v = 0; v < m; ++v)
-                            m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
-                                tc_tile_d.as<int32_t>(), tc_tile_begin.as<int64_t>(), tc_tile_count.as<int32_t>(),
-                                tc_ntiles, tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v,
-                                tc_bimg.as<uint32_t>(), reinterpret_cast<const float*>(M.ptr),
-                                reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
-                    });
-            }
-        } else if (ntiles)
-            timer.run(kM2L, [&] {
-                m2l_gemm_kernel<P, T><<<counted((unsigned)ntiles), 256, gemm_smem, stream>>>(
-                    tile_d.as<int32_t>(), tile_begin.as<int64_t>(), tile_count.as<int32_t>(), pair_e.as<int64_t>(),
-                    pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
-            });
+        timer.run(kM2L, [&] { m2l_products(-1); });
         // downward: for l = 2..L: L2L products, the local (L2L + V in offset order), then P2L
         for (int l = 2; l <= L; ++l) {
-            int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
             timer.run(kL2L, [&] {
-                const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
-                if (nt)
-                    m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
-                        oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
-                        oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
-                        l2l_tab.as<T>(), Lc.as<T>(), Yo.as<T>());
-                local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
-                    dp, b0, b1, m, l >= 3, Yo.as<T>(), Y.as<T>(), Lc.as<T>());
+                l2l_products(l);
+                reduce_locals(l, l >= 3, 1, 0);
             });
-            timer.run(kP2L, [&] {
-                if (kBfly && m == 1)
-                    expand_bfly_kernel<P, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
-                        dp, b0, b1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
-                        reinterpret_cast<float*>(Lc.ptr));
-                else
-                    expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem, stream>>>(
-                        dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
-            });
+            timer.run(kP2L, [&] { p2l_level(l); });
         }
         // leaves: L2P + M2P
-        if (nleaves)
-            timer.run(kFar, [&] {
-                if (gradients)
-                    leaf_far_kernel<P, T, true><<<counted((unsigned)nleaves), 64, NC * sizeof(T), stream>>>(
-                        dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
-                else
-                    leaf_far_kernel<P, T, false><<<counted((unsigned)nleaves), 64, NC * sizeof(T), stream>>>(
-                        dp, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
-            });
+        timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
     }
 
-    void run_near(double* d_phi, double* d_grad) {
-        const int near = kinds & 1;
-        if (!items.count) return;
-        const unsigned grid = (unsigned)((items.count + kP2pWarps - 1) / kP2pWarps);
-        timer.run(kP2P, [&] {
-            if constexpr (kMixed) {
-                const unsigned gx2 = (unsigned)((items.count + kX2Warps - 1) / kX2Warps);
-                const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
-                const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
-                const auto* q = reinterpret_cast<const float*>(sq.ptr);
-                if (gradients)
-                    p2p_x2_kernel<true><<<counted(gx2), 32 * kX2Warps, 0, stream>>>(
-                        dp, items, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(),
-                        far_g.as<double>(), d_phi, d_grad);
-                else
-                    p2p_x2_kernel<false><<<counted(gx2), 32 * kX2Warps, 0, stream>>>(
-                        dp, items, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(),
-                        nullptr, d_phi, nullptr);
-                return;
+    // ---- the pieces, shared by the evaluation and the level calls ----
+    void load_charges(const double* d_charges) {
+        const int64_t ns = dp.nsrc;
+        if (ns > 0)
+            charge_load_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
+                d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
+    }
+
+    size_t exp_smem() const { return sizeof(T) * (NC * 32 + (size_t)m * 32); }
+
+    void p2m_rows(int64_t r0, int64_t r1) {  // P2M of leaves [r0, r1)
+        if (r1 <= r0) return;
+        if (kBfly && m == 1)
+            expand_bfly_kernel<P, false><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
+                dp, r0, r1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
+                reinterpret_cast<float*>(M.ptr));
+        else
+            expand_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 32, exp_smem(), stream>>>(
+                dp, r0, r1, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
+    }
+
+    void m2m_level(int l) {  // parents on level l from their children on level l + 1
+        const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
+        const int64_t n = m2m_start[l + 1] - m2m_start[l];
+        if (nt)
+            m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
+                oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0, oct_tile_count.as<int32_t>() + t0,
+                oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m, m2m_tab.as<T>(), M.as<T>(), Yo.as<T>());
+        if (n)
+            m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
+                dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, Yo.as<T>(), M.as<T>());
+    }
+
+    // M2L products Y of the V pairs of level l (l < 0: every level in one launch)
+    void m2l_products(int l) {
+        if (kTensor && m2l_path == 1) {
+            if constexpr (kTensor) {
+                const int64_t t0 = l < 0 ? 0 : tc_lvl_tiles[l];
+                const int64_t nt = l < 0 ? tc_ntiles : tc_lvl_tiles[l + 1] - tc_lvl_tiles[l];
+                const DevBuf& td = l < 0 ? tc_tile_d : tc_ltile_d;
+                const DevBuf& tb = l < 0 ? tc_tile_begin : tc_ltile_begin;
+                const DevBuf& tn = l < 0 ? tc_tile_count : tc_ltile_count;
+                if (nt == 0) return;
+                const unsigned grid = (unsigned)std::min<int64_t>(nt, num_sms);
+                for (int v = 0; v < m; ++v)
+                    m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                        td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
+                        tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v, tc_bimg.as<uint32_t>(),
+                        reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
+            return;
+        }
+        const int64_t t0 = l < 0 ? 0 : lvl_tiles[l];
+        const int64_t nt = l < 0 ? ntiles : lvl_tiles[l + 1] - lvl_tiles[l];
+        const DevBuf& td = l < 0 ? tile_d : ltile_d;
+        const DevBuf& tb = l < 0 ? tile_begin : ltile_begin;
+        const DevBuf& tn = l < 0 ? tile_count : ltile_count;
+        if (nt)
+            m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
+                td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, pair_e.as<int64_t>(),
+                pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
+    }
+
+    void l2l_products(int l) {  // L2L products Yo of the children on level l (l >= 3)
+        const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
+        if (nt)
+            m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
+                oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0, oct_tile_count.as<int32_t>() + t0,
+                oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m, l2l_tab.as<T>(), Lc.as<T>(), Yo.as<T>());
+    }
+
+    void reduce_locals(int l, int with_l2l, int with_v, int accumulate) {
+        const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+        if (b1 > b0)
+            local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
+                dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), Lc.as<T>());
+    }
+
+    void p2l_level(int l) {
+        const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+        if (b1 <= b0) return;
+        if (kBfly && m == 1)
+            expand_bfly_kernel<P, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+                dp, b0, b1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
+                reinterpret_cast<float*>(Lc.ptr));
+        else
+            expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), stream>>>(
+                dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
+    }
+
+    void leaf_far(int64_t r0, int64_t r1, int mode) {  // L2P / M2P of leaves [r0, r1)
+        if (r1 <= r0) return;
+        if (gradients)
+            leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), 64, NC * sizeof(T), stream>>>(
+                dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+        else
+            leaf_far_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 64, NC * sizeof(T), stream>>>(
+                dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+    }
+
+    // P2P over work items [i0, i1); accumulate = 0 adds the far partial and writes the
+    // scaled output in caller order, 1 adds into the leaf-order store (level calls)
+    void p2p_items(int64_t i0, int64_t i1, int near, int accumulate, double* d_phi, double* d_grad) {
+        if (i1 <= i0) return;
+        P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
+        double* fg = gradients ? far_g.as<double>() : nullptr;
+        double* og = gradients ? d_grad : nullptr;
+        if constexpr (kMixed) {
+            const unsigned g = (unsigned)((it.count + kX2Warps - 1) / kX2Warps);
+            const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
+            const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
+            const auto* q = reinterpret_cast<const float*>(sq.ptr);
             if (gradients)
-                p2p_kernel<T, true, kMixed><<<counted(grid), 32 * kP2pWarps, 0, stream>>>(
-                    dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
-                    far_phi.as<double>(), far_g.as<double>(), d_phi, d_grad);
+                p2p_x2_kernel<true><<<counted(g), 32 * kX2Warps, 0, stream>>>(
+                    dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(), fg,
+                    accumulate, d_phi, og);
             else
-                p2p_kernel<T, false, kMixed><<<counted(grid), 32 * kP2pWarps, 0, stream>>>(
-                    dp, items, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
-                    far_phi.as<double>(), nullptr, d_phi, nullptr);
-        });
+                p2p_x2_kernel<false><<<counted(g), 32 * kX2Warps, 0, stream>>>(
+                    dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(), fg,
+                    accumulate, d_phi, og);
+        } else {
+            const unsigned g = (unsigned)((it.count + kP2pWarps - 1) / kP2pWarps);
+            if (gradients)
+                p2p_kernel<T, true, kMixed><<<counted(g), 32 * kP2pWarps, 0, stream>>>(
+                    dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
+                    far_phi.as<double>(), fg, accumulate, d_phi, og);
+            else
+                p2p_kernel<T, false, kMixed><<<counted(g), 32 * kP2pWarps, 0, stream>>>(
+                    dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
+                    far_phi.as<double>(), fg, accumulate, d_phi, og);
+        }
+    }
+
+    // ---- level calls (the FmmOperator trait, fmm-plan/src/operator.rs:434-492) ----
+    void op_begin(const double* d_charges) override {
+        launches = 0;
+        load_charges(d_charges);
+        CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, Lc.bytes, stream));
+        CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
+        CUDA_TRY(cudaMemsetAsync(far_g.ptr, 0, far_g.bytes, stream));
+    }
+
+    void op_level(int kind, int l) override {
+        const int L = plan.nlevels - 1;
+        const int64_t f0 = plan.leaf_level_start[l], f1 = plan.leaf_level_start[l + 1];
+        switch (kind) {
+            case FMMGPU_OP_P2M: p2m_rows(f0, f1); break;
+            case FMMGPU_OP_M2M: if (l < L) m2m_level(l); break;
+            case FMMGPU_OP_L2L:
+                if (l >= 3) {
+                    l2l_products(l);
+                    reduce_locals(l, 1, 0, 1);
+                }
+                break;
+            case FMMGPU_OP_M2L:
+                if (l >= 2) {
+                    m2l_products(l);
+                    reduce_locals(l, 0, 1, 1);
+                }
+                break;
+            case FMMGPU_OP_P2L: if (l >= 2) p2l_level(l); break;
+            case FMMGPU_OP_L2P: leaf_far(f0, f1, 5); break;
+            case FMMGPU_OP_M2P: leaf_far(f0, f1, 6); break;
+            case FMMGPU_OP_P2P: p2p_items(item_lstart[l], item_lstart[l + 1], 1, 1, nullptr, nullptr); break;
+            default: throw Failure(FMMGPU_INVALID_ARGUMENT, "unknown operator kind");
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    void op_output(double* d_phi, double* d_grad) override {
+        if (plan.nleaves())
+            output_kernel<<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
+                dp, m, far_phi.as<double>(), far_g.as<double>(), d_phi, gradients ? d_grad : nullptr);
+        CUDA_TRY(cudaGetLastError());
     }
 };
 
@@ -686,6 +802,7 @@ struct fmmgpu_fmm {
     DevBuf d_charges, d_phi, d_grad;
     size_t device_bytes = 0;
     int64_t near_pairs = 0;
+    bool op_begun = false;  // a level-call evaluation has begun
 };
 
 namespace {
@@ -837,6 +954,64 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
             CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
                                      f->stream));
         CUDA_TRY(cudaStreamSynchronize(f->stream));
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    });
+}
+
+int fmmgpu_op_begin_evaluation(fmmgpu_fmm* f, const double* charges) {
+    return guarded([&] {
+        if (!f || !charges) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors, ns = f->plan.src_perm.size();
+        CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, f->stream));
+        f->eval->op_begin(f->d_charges.as<double>());
+        f->op_begun = true;
+    });
+}
+
+static int op_call(fmmgpu_fmm* f, int kind, int level) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        if (!f->op_begun) throw Failure(FMMGPU_INVALID_ARGUMENT, "no evaluation begun (fmmgpu_op_begin_evaluation)");
+        if (level < 0 || level >= f->plan.nlevels)
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "level " + std::to_string(level) + " outside 0.." +
+                                                       std::to_string(f->plan.nlevels - 1));
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        f->eval->op_level(kind, level);
+    });
+}
+
+int fmmgpu_op_p2m(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_P2M, level); }
+int fmmgpu_op_m2m(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_M2M, level); }
+int fmmgpu_op_l2l(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_L2L, level); }
+int fmmgpu_op_m2l(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_M2L, level); }
+int fmmgpu_op_p2l(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_P2L, level); }
+int fmmgpu_op_l2p(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_L2P, level); }
+int fmmgpu_op_m2p(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_M2P, level); }
+int fmmgpu_op_p2p(fmmgpu_fmm* f, int level) { return op_call(f, FMMGPU_OP_P2P, level); }
+
+int fmmgpu_op_host_data(fmmgpu_fmm* f, int event) {
+    (void)event;
+    return guarded([&] {
+        if (!f) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+    });
+}
+
+int fmmgpu_op_read_output(fmmgpu_fmm* f, double* potential, double* gradient) {
+    return guarded([&] {
+        if (!f || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval || !f->op_begun) throw Failure(FMMGPU_INVALID_ARGUMENT, "no evaluation begun");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors, nt = f->plan.tgt_perm.size();
+        f->eval->op_output(f->d_phi.as<double>(), f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        CUDA_TRY(cudaMemcpyAsync(potential, f->d_phi.ptr, sizeof(double) * m * nt, cudaMemcpyDeviceToHost, f->stream));
+        if (f->settings.gradients)
+            CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
+                                     f->stream));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        CUDA_TRY(cudaGetLastError());
         if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
     });
 }

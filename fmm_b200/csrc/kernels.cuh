@@ -309,16 +309,21 @@ __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ pare
 //   L = (l >= 3 ? T_o L_parent : 0) + the V row's products in offset-index order,
 // written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X is added after).
 // Block per box, thread per slot; the V loop issues four loads before adding them in order.
+// The evaluation writes L = Yo + sum_V Y (accumulate = 0); the level calls add into L:
+// L2L with with_v = 0, then M2L with with_l2l = 0, which gives the same floats when the
+// L2L call comes first (L starts at zero, so 0 + Yo = Yo).
 template <int P, typename T>
-__global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l,
-                                    const T* __restrict__ Yo, const T* __restrict__ Yv, T* __restrict__ Lc) {
+__global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l, int with_v,
+                                    int accumulate, const T* __restrict__ Yo, const T* __restrict__ Yv,
+                                    T* __restrict__ Lc) {
     constexpr int NC = nc_of(P);
     const int64_t b = b0 + blockIdx.x;
     if (b >= b1 || plan.tgt_below[b] == 0) return;
-    const int64_t e0 = plan.v_row[b], e1 = plan.v_row[b + 1];
+    const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
     for (int v = 0; v < m; ++v)
         for (int i = threadIdx.x; i < NC; i += blockDim.x) {
-            T s = with_l2l ? Yo[(b * m + v) * NC + i] : T(0);
+            T s = accumulate ? Lc[(b * m + v) * NC + i] : T(0);
+            if (with_l2l) s = accumulate ? s + Yo[(b * m + v) * NC + i] : Yo[(b * m + v) * NC + i];
             int64_t e = e0;
             for (; e + 4 <= e1; e += 4) {
                 const T y0 = __ldcs(Yv + (e * m + v) * NC + i), y1 = __ldcs(Yv + ((e + 1) * m + v) * NC + i);
@@ -484,19 +489,22 @@ __device__ __forceinline__ void m2p_eval(const T* M, T x, T y, T z, T& phi, T& g
     gz = dz;
 }
 
+// mode: bit 0 L2P, bit 1 M2P, bit 2 add into far_phi / far_g (else overwrite them).
+// The evaluation runs mode 3; the level calls run 5 (L2P) then 6 (M2P) on stores that
+// start at zero, which gives the same floats.
 template <int P, typename T, bool GRAD>
-__global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int m,
+__global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int64_t leaf0, int mode, int m,
                                                       const typename Vec4<T>::type* __restrict__ tpos,
                                                       const T* __restrict__ M, const T* __restrict__ Lc,
                                                       double* __restrict__ far_phi, double* __restrict__ far_g) {
     constexpr int NC = nc_of(P);
     extern __shared__ unsigned char smem_raw[];
     T* C = reinterpret_cast<T*>(smem_raw);  // [NC]
-    const int leaf = blockIdx.x;
+    const int64_t leaf = leaf0 + blockIdx.x;
     const int box = plan.leaf_box[leaf];
     const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
     if (t1 == t0) return;
-    const int64_t w0 = plan.w_row[leaf], w1 = plan.w_row[leaf + 1];
+    const int64_t w0 = plan.w_row[leaf], w1 = (mode & 2) ? plan.w_row[leaf + 1] : plan.w_row[leaf];
     const int64_t nt = plan.ntgt;
     for (int v = 0; v < m; ++v) {
         for (int64_t tb = t0; tb < t1; tb += blockDim.x) {
@@ -510,20 +518,27 @@ __global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int m,
                 uz = p4.z;
             }
             double fphi = 0.0, fg[3] = {0.0, 0.0, 0.0};
-            // L2P, unit frame
-            for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Lc[((int64_t)box * m + v) * NC + k];
-            __syncthreads();
-            if (valid) {
-                T ph, gx, gy, gz;
-                l2p_eval<P, T, GRAD>(C, ux, uy, uz, ph, gx, gy, gz);
-                fphi = (double)ph;
-                if (GRAD) {
-                    fg[0] = (double)gx;
-                    fg[1] = (double)gy;
-                    fg[2] = (double)gz;
-                }
+            if ((mode & 4) && valid) {
+                fphi = far_phi[(int64_t)v * nt + t];
+                if (GRAD)
+                    for (int k = 0; k < 3; ++k) fg[k] = far_g[((int64_t)v * nt + t) * 3 + k];
             }
-            __syncthreads();
+            // L2P, unit frame
+            if (mode & 1) {
+                for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Lc[((int64_t)box * m + v) * NC + k];
+                __syncthreads();
+                if (valid) {
+                    T ph, gx, gy, gz;
+                    l2p_eval<P, T, GRAD>(C, ux, uy, uz, ph, gx, gy, gz);
+                    fphi = (mode & 4) ? fphi + (double)ph : (double)ph;
+                    if (GRAD) {
+                        fg[0] = (mode & 4) ? fg[0] + (double)gx : (double)gx;
+                        fg[1] = (mode & 4) ? fg[1] + (double)gy : (double)gy;
+                        fg[2] = (mode & 4) ? fg[2] + (double)gz : (double)gz;
+                    }
+                }
+                __syncthreads();
+            }
             // M2P over the W list, frame (c(s|t), r(s|t))
             for (int64_t e = w0; e < w1; ++e) {
                 int s = plan.w_col[e];
@@ -620,8 +635,9 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
                                                   const typename Vec4<T>::type* __restrict__ spos,
                                                   const T* __restrict__ sq,
                                                   const typename Vec4<T>::type* __restrict__ tpos, ClosePairs close,
-                                                  const double* __restrict__ far_phi, const double* __restrict__ far_g,
-                                                  double* __restrict__ out_phi, double* __restrict__ out_g) {
+                                                  double* __restrict__ far_phi, double* __restrict__ far_g,
+                                                  int accumulate, double* __restrict__ out_phi,
+                                                  double* __restrict__ out_g) {
     using T4 = typename Vec4<T>::type;
     __shared__ T4 stage[kP2pWarps][kP2pStage];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -718,6 +734,16 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
             }
         }
         const double ph = far_phi[(int64_t)v * nt + t] + aphi;
+        if (accumulate) {  // level calls: add into the leaf-order store, scaled by output_kernel
+            far_phi[(int64_t)v * nt + t] = ph;
+            if (GRAD) {
+                double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                fg[0] = fg[0] + ag0;
+                fg[1] = fg[1] + ag1;
+                fg[2] = fg[2] + ag2;
+            }
+            continue;
+        }
         const int64_t i = plan.tgt_perm[t];
         out_phi[(int64_t)v * nt + i] = ph / phi_scale;
         if (GRAD) {
@@ -728,6 +754,33 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
             o[2] = (fg[2] + ag2) / g_scale;
         }
     }
+}
+
+// Output pass of the level calls (fmm-kernels/src/movement.rs:411 gather_output with the
+// scaling of fmm-exec/src/fmm.rs:4750-4778): phi = phi_hat / (4 pi r_t) and
+// g = g_hat / ((4 pi r_t) r_t), leaf order -> caller order.  Block per leaf; the same
+// expressions as the P2P kernels' fused output, so both give the same floats.
+__global__ void output_kernel(DevPlan plan, int m, const double* __restrict__ far_phi,
+                              const double* __restrict__ far_g, double* __restrict__ out_phi,
+                              double* __restrict__ out_g) {
+    const int64_t leaf = blockIdx.x;
+    const int box = plan.leaf_box[leaf];
+    const double rt = plan.side * pow2d(-(plan.level[box] + 1));
+    const double phi_scale = 4.0 * 3.141592653589793 * rt;
+    const double g_scale = phi_scale * rt;
+    const int64_t nt = plan.ntgt;
+    for (int v = 0; v < m; ++v)
+        for (int64_t t = plan.tgt_start[leaf] + threadIdx.x; t < plan.tgt_start[leaf + 1]; t += blockDim.x) {
+            const int64_t i = plan.tgt_perm[t];
+            out_phi[(int64_t)v * nt + i] = far_phi[(int64_t)v * nt + t] / phi_scale;
+            if (out_g) {
+                const double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                double* o = out_g + ((int64_t)v * nt + i) * 3;
+                o[0] = fg[0] / g_scale;
+                o[1] = fg[1] / g_scale;
+                o[2] = fg[2] / g_scale;
+            }
+        }
 }
 
 // Build time (mixed form): every near pair whose f32 r2, formed exactly as p2p_kernel

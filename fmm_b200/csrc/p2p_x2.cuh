@@ -62,7 +62,7 @@ template <bool GRAD>
 __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
     DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
     const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
-    const double* __restrict__ far_phi, const double* __restrict__ far_g, double* __restrict__ out_phi,
+    double* __restrict__ far_phi, double* __restrict__ far_g, int accumulate, double* __restrict__ out_phi,
     double* __restrict__ out_g) {
     __shared__ float4 sxy[kX2Warps][kX2Stage / 2];  // (x0, x1, y0, y1)
     __shared__ float4 szq[kX2Warps][kX2Stage / 2];  // (z0, z1, q0, q1)
@@ -209,6 +209,16 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
         }
         // both gradient sums hold -sum qr3 (t - y), as p2p_kernel's
         const double ph = far_phi[(int64_t)v * nt + t] + aphi;
+        if (accumulate) {  // level calls: add into the leaf-order store, scaled by output_kernel
+            far_phi[(int64_t)v * nt + t] = ph;
+            if (GRAD) {
+                double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                fg[0] = fg[0] + ag0;
+                fg[1] = fg[1] + ag1;
+                fg[2] = fg[2] + ag2;
+            }
+            continue;
+        }
         const int64_t i = plan.tgt_perm[t];
         out_phi[(int64_t)v * nt + i] = ph / phi_scale;
         if (GRAD) {

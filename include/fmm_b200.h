@@ -125,6 +125,52 @@ int64_t fmmgpu_fmm_list(const fmmgpu_fmm* fmm, int kind, int64_t row, uint64_t* 
 /* The f64 tables the plan uploaded: 316 M2L, 8 M2M, 8 L2L, column-major (p+1)^2 squares. */
 int fmmgpu_fmm_tables(const fmmgpu_fmm* fmm, double* m2l, double* m2m, double* l2l);
 
+/* ---- Operator level calls: the FmmOperator trait (fmm-plan/src/operator.rs:434-492) ----
+ * The host drives an evaluation level by level on the plan the build made, in the
+ * reference evaluator's schedule (fmm-plan/src/evaluator.rs:368-440):
+ *   begin_evaluation(charges);
+ *   for l = L..0:  p2m(l); if l > 0: m2m(l - 1)          upward
+ *   for l = 1..L:  l2l(l); m2l(l); p2l(l)                downward
+ *   for l = 0..L:  l2p(l); m2p(l); p2p(l)                leaves
+ *   read_output(potential, gradient).
+ * Every call queues work on the evaluator's stream and adds into its output (the
+ * multipoles, the locals or the leaf-order target store) in the trait's accumulation
+ * order (operator.rs:34-45); a call with nothing to do on its level is a no-op, as the
+ * trait requires every call on every level (operator.rs:409-424).  Made in this order,
+ * the calls give the same floats as fmmgpu_fmm_evaluate.  Level calls return
+ * FMMGPU_INVALID_ARGUMENT for a level outside 0..nlevels-1 or before begin_evaluation;
+ * device errors surface at read_output (fmm-kernels/src/lib.rs:64-66). */
+typedef enum {
+    FMMGPU_OP_P2M = 0,
+    FMMGPU_OP_M2M = 1,  /* parents on `level` from their children on level + 1 */
+    FMMGPU_OP_L2L = 2,  /* boxes on `level` from their parents on level - 1 */
+    FMMGPU_OP_M2L = 3,
+    FMMGPU_OP_P2L = 4,
+    FMMGPU_OP_L2P = 5,
+    FMMGPU_OP_M2P = 6,
+    FMMGPU_OP_P2P = 7
+} fmmgpu_op_kind;
+
+/* DeviceOperator::begin_evaluation (fmm-exec/src/device.rs:4386): HOST charges in caller
+ * order (charges[i*m + v]) to the device in leaf order; multipoles, locals and the
+ * target store set to zero. */
+int fmmgpu_op_begin_evaluation(fmmgpu_fmm* fmm, const double* charges);
+int fmmgpu_op_p2m(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_m2m(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_l2l(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_m2l(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_p2l(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_l2p(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_m2p(fmmgpu_fmm* fmm, int level);
+int fmmgpu_op_p2p(fmmgpu_fmm* fmm, int level);
+/* FmmOperator::host_data (operator.rs:56-119): the exchange events of a distributed
+ * evaluation; on one rank there is nothing to exchange and every event is accepted. */
+int fmmgpu_op_host_data(fmmgpu_fmm* fmm, int event);
+/* DeviceOperator::read_output (device.rs:4687) and the output pass (movement.rs:411,
+ * fmm.rs:4750): phi = phi_hat / (4 pi r_t), g = g_hat / ((4 pi r_t) r_t) into HOST
+ * buffers in caller order (layout of fmmgpu_fmm_evaluate); synchronises. */
+int fmmgpu_op_read_output(fmmgpu_fmm* fmm, double* potential, double* gradient);
+
 /* f64 direct sum on the GPU at the given targets: phi(x) = sum_j q_j / (4 pi |x - y_j|)
  * and its gradient (grad may be NULL), exactly coincident pairs skipped, Neumaier
  * compensation per target (fmm-ref/src/p2p.rs:147-186 with the FMM's 1/(4 pi)).

@@ -3,6 +3,8 @@ import ctypes as C
 import re
 from pathlib import Path
 
+import numpy as np
+
 import fmm_b200 as F
 
 HEADER = Path(__file__).resolve().parent.parent / "include" / "fmm_b200.h"
@@ -35,3 +37,13 @@ def test_direct_sum_argument_errors_reach_last_error():
     rc = lib.fmmgpu_direct_sum(4, None, None, 1, None, None, None, 0)
     assert rc == 1
     assert b"null buffer" in lib.fmmgpu_last_error()
+
+
+def test_level_calls_need_an_evaluator():
+    """A plan-only handle (no GPU needed) answers the level calls with an argument error."""
+    x = np.random.default_rng(0).uniform(size=(500, 3))
+    plan = F.FmmBuilder(3).max_points_per_leaf(16).plan(x)
+    lib = F.lib()
+    assert lib.fmmgpu_op_p2m(plan._h, 0) == 1
+    assert b"plan-only" in lib.fmmgpu_last_error()
+    assert lib.fmmgpu_op_begin_evaluation(plan._h, None) == 1
