@@ -228,6 +228,15 @@ def run_ours(args):
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
+    # the same steps replayed from one CUDA graph of the whole sweep
+    fmm.set_graph(True)
+    graph_ms = device_steps(fmm, args.steps, args.warmup)
+    fmm.set_graph(False)
+    log(f"graph: {graph_ms:.3f} ms/step")
+    if world > 1:
+        t = torch.tensor([graph_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        graph_ms = float(t.item())
     # per-kind split and the dominant kernel (separate, untimed evaluation)
     fmm.set_kind_timing(True)
     stream = torch.cuda.ExternalStream(fmm.stream)
@@ -319,6 +328,8 @@ def run_ours(args):
                   "against": "f64 direct sum (GPU, Neumaier)", "plain_f64_phi_rel_l2": perr},
         "plain_f64": {"ms_per_step": round(plain_ms, 4), "value": round(n / (plain_ms * 1e-3) / 1e6, 3),
                       "mixed_over_plain": round(plain_ms / ms, 3)},
+        "graph": {"ms_per_step": round(graph_ms, 4), "value": round(world * n / (graph_ms * 1e-3) / 1e6, 3),
+                  "note": "the same evaluation replayed from one captured CUDA graph"},
         "kinds_ms": {k: round(v, 4) for k, v in kinds.items()},
         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs",
                                       "x_pairs", "device_bytes", "close_pairs")},

@@ -67,6 +67,7 @@ def lib():
             "fmmgpu_fmm_set_kind_timing": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_kind_times": (C.c_int, [vp, dp]),
             "fmmgpu_fmm_set_kinds": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_set_graph": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
@@ -275,6 +276,10 @@ class Fmm(Plan):
 
     def set_kind_timing(self, on=True):
         _check(lib().fmmgpu_fmm_set_kind_timing(self._h, int(on)))
+
+    def set_graph(self, on=True):
+        """Replay later evaluations from one captured CUDA graph of the whole sweep."""
+        _check(lib().fmmgpu_fmm_set_graph(self._h, int(on)))
 
     def set_kinds(self, kinds):
         """Test hook: bit 0 near field, bit 1 far field (3, the default, is the FMM)."""

@@ -803,7 +803,53 @@ struct fmmgpu_fmm {
     size_t device_bytes = 0;
     int64_t near_pairs = 0;
     bool op_begun = false;  // a level-call evaluation has begun
+    // whole-evaluation CUDA graph: captured once per (charges, potential, gradient)
+    // buffer triple, replayed while the triple and the settings stay the same
+    bool graph_on = false;
+    cudaGraphExec_t graph = nullptr;
+    const void* graph_key[3] = {nullptr, nullptr, nullptr};
+    int64_t graph_launches = 0;
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
 };
+
+namespace {
+
+// One evaluation on the handle's stream: replayed from the CUDA graph when graphs are on
+// (and per-kind timing is off), else launched directly.
+void run_evaluation(fmmgpu_fmm* f, const double* q, double* phi, double* grad) {
+    EvaluatorBase& ev = *f->eval;
+    if (!f->graph_on || ev.timer.on) {
+        ev.evaluate(q, phi, grad);
+        return;
+    }
+    if (!f->graph || f->graph_key[0] != q || f->graph_key[1] != phi || f->graph_key[2] != grad) {
+        f->drop_graph();
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            ev.evaluate(q, phi, grad);
+        } catch (...) {
+            cudaStreamEndCapture(f->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        CUDA_TRY(cudaStreamEndCapture(f->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&f->graph, g, 0);
+        cudaGraphDestroy(g);
+        CUDA_TRY(e);
+        f->graph_key[0] = q;
+        f->graph_key[1] = phi;
+        f->graph_key[2] = grad;
+        f->graph_launches = ev.launches;
+    }
+    CUDA_TRY(cudaGraphLaunch(f->graph, f->stream));
+    ev.launches = f->graph_launches;
+}
+
+}  // namespace
 
 namespace {
 
@@ -934,7 +980,7 @@ int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* f, const double* charges, double* pot
             throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
         if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
         CUDA_TRY(cudaSetDevice(f->settings.device));
-        f->eval->evaluate(charges, potential, f->settings.gradients ? gradient : nullptr);
+        run_evaluation(f, charges, potential, f->settings.gradients ? gradient : nullptr);
     });
 }
 
@@ -947,8 +993,8 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
         const size_t m = f->settings.vectors;
         const size_t ns = f->plan.src_perm.size(), nt = f->plan.tgt_perm.size();
         CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, f->stream));
-        f->eval->evaluate(f->d_charges.as<double>(), f->d_phi.as<double>(),
-                          f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(),
+                       f->settings.gradients ? f->d_grad.as<double>() : nullptr);
         CUDA_TRY(cudaMemcpyAsync(potential, f->d_phi.ptr, sizeof(double) * m * nt, cudaMemcpyDeviceToHost, f->stream));
         if (f->settings.gradients)
             CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
@@ -1029,6 +1075,7 @@ int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* f, int path) {
     return guarded([&] {
         if (!f || !f->eval || path < 0 || path > 1) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid M2L path");
         f->eval->m2l_path = path;
+        f->drop_graph();
     });
 }
 
@@ -1036,6 +1083,17 @@ int fmmgpu_fmm_set_kinds(fmmgpu_fmm* f, int kinds) {
     return guarded([&] {
         if (!f || !f->eval || kinds < 1 || kinds > 3) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid kinds");
         f->eval->kinds = kinds;
+        f->drop_graph();
+    });
+}
+
+int fmmgpu_fmm_set_graph(fmmgpu_fmm* f, int on) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->graph_on = on != 0;
+        f->drop_graph();
     });
 }
 
@@ -1080,6 +1138,7 @@ void fmmgpu_fmm_destroy(fmmgpu_fmm* f) {
     if (!f) return;
     if (f->eval || f->stream) cudaSetDevice(f->settings.device);
     if (f->stream) cudaStreamSynchronize(f->stream);
+    f->drop_graph();
     f->eval.reset();
     f->d_charges.alloc(0);
     f->d_phi.alloc(0);

@@ -97,6 +97,14 @@ int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* fmm, const double* charges, double* p
 /* The evaluator's CUDA stream (a cudaStream_t), for timing with events on it. */
 void* fmmgpu_fmm_stream(fmmgpu_fmm* fmm);
 
+/* Whole-sweep CUDA graph (on = 1): the next evaluation (fmmgpu_fmm_evaluate or
+ * _evaluate_device) is captured into one CUDA graph, every pass of it, and later
+ * evaluations with the same charge / potential / gradient buffers replay that graph
+ * (one launch from the host); new buffers, or changed settings, re-capture.  The same
+ * kernels run, so the results are the same floats.  Ignored while per-kind timing is on.
+ * Off (0) by default.  Synchronises. */
+int fmmgpu_fmm_set_graph(fmmgpu_fmm* fmm, int on);
+
 /* Per-kind device timing of the following evaluations (the reference's KindTiming,
  * fmm-exec/src/fmm.rs:150-153): every launch is bracketed by CUDA events. */
 int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* fmm, int on);
