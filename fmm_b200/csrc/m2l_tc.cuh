@@ -108,8 +108,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// returns true when the barrier's phase `parity` completed within `limit` clock cycles
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, long long limit) {
+// returns true when the barrier's phase `parity` completed within `limit` clock cycles;
+// false on timeout or when *abort is set (another role gave up)
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, long long limit,
+                                                  const volatile int* abort = nullptr) {
     const long long start = clock64();
     while (clock64() - start < limit) {
         uint32_t done;
@@ -123,23 +125,51 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done) return true;
+        if (abort && *abort) return false;
     }
     return false;
 }
 
-// Persistent form.  CTA c takes the contiguous range of tiles [c T / G, (c + 1) T / G) of
-// the offset-sorted tile list.  The table of the current offset lives in tensor memory
-// as the MMA's A operand (M = 128 lanes = output slots, K = input slots in columns; hi
-// and lo parts), so the MMA is D[slot][pair] = A_d . X^T with the gathered multipoles X
-// as the shared-memory B operand (N = 128 pairs, K-major, 128-byte swizzled), double
-// buffered.  Per tile i (16 warps):
-//   gather + split X(i) into buffer i&1 (its last reader, MMA(i-2), has completed),
-//   wait MMA(i-1); if the offset changes, warps 0-3 store the new table into TMEM,
-//   thread 0 issues MMA(i) into accumulator i&1 and commits to the barrier,
-//   epilogue(i-1): each thread holds one slot of 16 pairs per TMEM load, so the stores
-//   of one pair's row are contiguous across the warp's lanes.
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile(
+        "{\n\t"
+        ".reg .b64 st;\n\t"
+        "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t"
+        "}\n" ::"r"(mbar)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+// Persistent, warp-specialised form.  CTA c takes the contiguous range of tiles
+// [c T / G, (c + 1) T / G) of the offset-sorted tile list.  The table of the current
+// offset lives in tensor memory as the MMA's A operand (M = 128 lanes = output slots,
+// K = input slots in columns; hi and lo parts), so the MMA is D[slot][pair] = A_d . X^T
+// with the gathered multipoles X as the shared-memory B operand (N = 128 pairs,
+// K-major, 128-byte swizzled).  Roles, coupled only by mbarriers (no block barrier in
+// the loop):
+//   warps 8-15 (producers): tile k into X stage k&1 once MMA(k-2) has released it
+//     (empty[k&1]), signal full[k&1]; warps 8-11 also replace the table in tensor
+//     memory when the offset changes, after MMA(k-1) has read the old one (table);
+//   warp 16, one thread (MMA): waits full[k&1], the table and the accumulator k&1
+//     (acc_empty, released by the epilogue of tile k-2), issues the 3 x KSTEPS MMAs
+//     and commits to empty[k&1] and acc_full[k&1];
+//   warps 0-7 (epilogue): wait acc_full[k&1], read the accumulator with tcgen05.ld
+//     and stream the products Y past L2, then release acc_empty[k&1].
+// Every wait is bounded; a role that gives up sets the shared abort flag (which ends
+// the other roles' waits) and *error, and the CTA frees its tensor memory and returns.
 // One vector per launch.
-constexpr int kTcWarps = 16;
+constexpr int kTcWarps = 17;
+constexpr int kTcProd = 8;      // producer warps (8..15)
+constexpr int kTcMmaWarp = 16;  // the MMA issuer's warp
+constexpr long long kTcWait = 4000000000LL;  // clock cycles (about 2 s)
 
 template <int P>
 struct TcTs {
@@ -148,13 +178,14 @@ struct TcTs {
     static constexpr int KP = 32 * KA;             // padded K (input slots)
     static constexpr int KSTEPS = KP / 8;
     static constexpr int NT = kTcRows;             // pairs per tile (UMMA N)
-    static constexpr int X_BYTES = NT * KP * 4;    // one part of one buffer
-    static constexpr int SMEM = 4 * X_BYTES + 1024 + 64;
+    static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage
+    static constexpr int SMEM = 4 * X_BYTES + 1024;
     static constexpr int COL_AHI = 0, COL_ALO = KP, COL_D0 = 2 * KP;  // TMEM columns
     static constexpr int TMEM_COLS = 512;
     static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per offset (hi, lo)
     static_assert(NC <= 128, "UMMA M = 128 output slots");
     static_assert(2 * KP + 2 * NT <= TMEM_COLS, "TMEM budget");
+    static_assert(NT % kTcProd == 0 && NT / kTcProd <= 32, "producer rows");
 };
 
 template <int NTILE>
@@ -192,21 +223,17 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   int* __restrict__ error) {
     using S = TcTs<P>;
     constexpr int NC = S::NC;
-    constexpr int kGather = kTcWarps / 2;     // warps 8..15 gather, warps 0..7 run the epilogue
-    constexpr int RPW = S::NT / kGather;      // gathered rows per gather warp
+    constexpr int RPW = S::NT / kTcProd;  // gathered rows per producer warp
     extern __shared__ unsigned char smem_raw[];
-    unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 bufs][hi, lo]
+    unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 stages][hi, lo]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    __shared__ uint64_t mbar[2];  // MMA(k) commits to mbar[k & 1] (k counted from the CTA's first tile)
+    __shared__ uint64_t bar_full[2], bar_empty[2], bar_accf[2], bar_acce[2], bar_table;
     __shared__ uint32_t tmem_base;
-    // tile k's row indices live from its gather (iteration k-1) to its epilogue
-    // (iteration k+1): three slots, slot (k - i0) % 3
-    __shared__ int32_t row_src[3][S::NT];
-    __shared__ int64_t row_e[3][S::NT];
-    __shared__ int32_t row_cnt[3];
+    __shared__ int abort_flag;
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
     const int64_t i1 = (int64_t)(blockIdx.x + 1) * ntiles / gridDim.x;
     if (i0 >= i1) return;
+    const int64_t ntile = i1 - i0;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -214,176 +241,220 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&bar_full[b]), kTcProd);
+            mbar_init(smem_u32(&bar_empty[b]), 1);
+            mbar_init(smem_u32(&bar_accf[b]), 1);
+            mbar_init(smem_u32(&bar_acce[b]), 8);
+        }
+        mbar_init(smem_u32(&bar_table), 4);
+        abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-    constexpr uint32_t idesc = tf32_idesc_ts<S::NT>();
+    volatile int* abort = &abort_flag;
+    auto give_up = [&]() {
+        *abort = 1;
+        atomicExch(error, 1);
+    };
+    // warp-wide roles: lane 0 waits (or reads the abort flag) and the warp takes its answer,
+    // so the lanes of a warp never part ways
+    auto warp_wait = [&](uint64_t* bar, uint32_t parity) {
+        int ok = 0;
+        if (lane == 0) ok = mbar_wait_bounded(smem_u32(bar), parity, kTcWait, abort);
+        return __shfl_sync(0xffffffffu, ok, 0) != 0;
+    };
+    auto warp_aborted = [&]() {
+        int a = 0;
+        if (lane == 0) a = *abort;
+        return __shfl_sync(0xffffffffu, a, 0) != 0;
+    };
 
-    auto rows = [&](int64_t it, int b) {  // threads 0..127: the tile's row indices into meta slot b
-        const int64_t p0 = tile_begin[it];
-        const int cnt = tile_count[it];
-        if (tid < S::NT) {
-            row_src[b][tid] = tid < cnt ? pair_src[p0 + tid] : 0;
-            row_e[b][tid] = tid < cnt ? pair_e[p0 + tid] : 0;
-        }
-        if (tid == 0) row_cnt[b] = cnt;
-    };
-    // gather + split X into buffer xb from meta slot b (gather warps, gw = 0..kGather-1):
-    // every load of a warp's rows is issued before any is converted and stored
-    auto gather = [&](int xb, int b, int gw) {
-        const int cnt = row_cnt[b];
-        unsigned char* xh = xbuf + (size_t)xb * 2 * S::X_BYTES;
-        unsigned char* xl = xh + S::X_BYTES;
-        float x[RPW][S::KA];
-#pragma unroll
-        for (int j = 0; j < RPW; ++j) {
-            const int r = gw + kGather * j;
-            const float* src = M + ((int64_t)row_src[b][r] * m + v) * NC;
-#pragma unroll
-            for (int a = 0; a < S::KA; ++a) {
-                const int k = a * 32 + lane;
-                x[j][a] = (r < cnt && k < NC) ? __ldg(src + k) : 0.0f;
+    if (warp >= kTcProd && warp < kTcProd + kTcProd) {
+        // ---------------- producers ----------------
+        const int pw = warp - kTcProd;
+        const uint32_t* img_prev = nullptr;
+        // metadata of the next tile, loaded one tile ahead: lane j < RPW holds the source
+        // box of row pw + kTcProd * j
+        int64_t nb = tile_begin[i0];
+        int ncnt = tile_count[i0];
+        int nsrc = 0;
+        if (lane < RPW && pw + kTcProd * lane < ncnt) nsrc = pair_src[nb + pw + kTcProd * lane];
+        for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
+            const int64_t it = i0 + k;
+            const int st = (int)(k & 1);
+            const int cnt = ncnt;
+            const int my_src = nsrc;
+            if (k >= 2 && !warp_wait(&bar_empty[st], (uint32_t)(((k - 2) >> 1) & 1))) {
+                if (lane == 0) give_up();
+                break;
             }
-        }
+            unsigned char* xh = xbuf + (size_t)st * 2 * S::X_BYTES;
+            unsigned char* xl = xh + S::X_BYTES;
+            float x[RPW][S::KA];
 #pragma unroll
-        for (int j = 0; j < RPW; ++j) {
-            const int r = gw + kGather * j;
+            for (int j = 0; j < RPW; ++j) {
+                const int r = pw + kTcProd * j;
+                const int sb = __shfl_sync(0xffffffffu, my_src, j);
+                const float* src = M + ((int64_t)sb * m + v) * NC;
 #pragma unroll
-            for (int a = 0; a < S::KA; ++a) {
-                const int k = a * 32 + lane;
-                const uint32_t hi = cvt_tf32(x[j][a]);
-                const uint32_t lo = cvt_tf32(x[j][a] - __uint_as_float(hi));
-                const uint32_t off = sw128_offset(r, k, S::NT);
-                *reinterpret_cast<uint32_t*>(xh + off) = hi;
-                *reinterpret_cast<uint32_t*>(xl + off) = lo;
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    };
-    // the table of offset d into TMEM (warps 0..3, one per lane quarter)
-    auto load_table = [&](int d) {
-        if (warp < 4) {
-            const uint32_t* src = timg + (size_t)d * S::IMG_WORDS;
-#pragma unroll 1
-            for (int part = 0; part < 2; ++part)
-#pragma unroll 1
-                for (int k0 = 0; k0 < S::KP; k0 += 16) {
-                    uint32_t r[16];
-                    const uint4* row =
-                        reinterpret_cast<const uint4*>(src + ((size_t)part * 128 + 32 * warp + lane) * S::KP + k0);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const uint4 u = __ldg(row + q);
-                        r[4 * q] = u.x;
-                        r[4 * q + 1] = u.y;
-                        r[4 * q + 2] = u.z;
-                        r[4 * q + 3] = u.w;
-                    }
-                    tmem_st16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)((part ? S::COL_ALO : S::COL_AHI) + k0),
-                              r);
+                for (int a = 0; a < S::KA; ++a) {
+                    const int kk = a * 32 + lane;
+                    x[j][a] = (r < cnt && kk < NC) ? __ldg(src + kk) : 0.0f;
                 }
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-        }
-    };
-    auto issue = [&](int b) {  // thread 0: MMA of X buffer b into accumulator b, commit to mbar[b]
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t xh = smem_u32(xbuf + (size_t)b * 2 * S::X_BYTES), xl = xh + S::X_BYTES;
-        const uint32_t dcol = tmem + (uint32_t)(S::COL_D0 + b * S::NT);
-        const uint32_t As[3] = {(uint32_t)S::COL_AHI, (uint32_t)S::COL_ALO, (uint32_t)S::COL_AHI};
-        const uint32_t Bs[3] = {xl, xh, xh};  // A_hi X_lo, A_lo X_hi, then A_hi X_hi
-        uint32_t acc = 0;
-#pragma unroll
-        for (int t = 0; t < 3; ++t)
-#pragma unroll
-            for (int s = 0; s < S::KSTEPS; ++s) {
-                const uint32_t kb = (uint32_t)((s >> 2) * S::NT * 128 + (s & 3) * 32);
-                umma_tf32_ts(dcol, tmem + As[t] + (uint32_t)(8 * s), sw128_desc(Bs[t] + kb), idesc, acc);
-                acc = 1;
             }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(&mbar[b]))
-                     : "memory");
-    };
-    // accumulator db with meta slot b (epilogue warps 0..7): lanes = slots, columns = pairs
-    auto epilogue = [&](int db, int b) {
-        const int q = warp & 3, g = warp >> 2;  // lane quarter, column group (64 pairs)
-        const int n = 32 * q + lane;
-        if (32 * q >= NC) return;  // the whole quarter is padding
-        const int cnt = row_cnt[b];
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-            const int c0 = 64 * g + 16 * h;
-            if (c0 >= cnt) break;
-            float vals[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + db * S::NT + c0), vals);
-            if (n < NC) {
-#pragma unroll
-                for (int i = 0; i < 16; ++i)
-                    if (c0 + i < cnt) __stcs(Y + (row_e[b][c0 + i] * m + v) * NC + n, vals[i]);  // streamed
+            if (k + 1 < ntile) {  // the next tile's metadata, in flight with the loads above
+                nb = tile_begin[it + 1];
+                ncnt = tile_count[it + 1];
+                nsrc = 0;
+                if (lane < RPW && pw + kTcProd * lane < ncnt) nsrc = pair_src[nb + pw + kTcProd * lane];
             }
-        }
-    };
-    // MMA(k) done: all threads wait, the CTA agrees on the outcome
-    bool failed = false;
-    auto wait_mma = [&](int64_t k) {
-        const int b = (int)((k - i0) & 1);
-        const uint32_t parity = (uint32_t)(((k - i0) >> 1) & 1);
-        const bool ok = mbar_wait_bounded(smem_u32(&mbar[b]), parity, 4000000000LL);
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            if (tid == 0) atomicExch(error, 1);
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-    };
-
-    auto meta = [&](int64_t k) { return (int)((k - i0) % 3); };
-    int cur_d = tile_d[i0];
-    rows(i0, 0);
-    __syncthreads();
-    if (warp >= kGather) gather(0, 0, warp - kGather);
-    load_table(cur_d);
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    if (tid == 0) issue(0);
-    __syncwarp();
-    for (int64_t it = i0; it < i1; ++it) {
-        const int b = (int)((it - i0) & 1);
-        if (it > i0) {
-            wait_mma(it - 1);  // X buffer b^1 and accumulator b^1 are free / readable
-            if (failed) break;
-        }
-        const bool next = it + 1 < i1;
-        if (next) rows(it + 1, meta(it + 1));
-        __syncthreads();
-        if (warp >= kGather) {
-            if (next) gather(b ^ 1, meta(it + 1), warp - kGather);
-        } else if (it > i0) {
-            epilogue(b ^ 1, meta(it - 1));
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        if (next) {
-            const int d = tile_d[it + 1];
-            if (d != cur_d) {  // MMA(it) still reads the old table: wait for it first
-                wait_mma(it);
-                if (failed) break;
-                load_table(d);
-                cur_d = d;
-                asm volatile("tcgen05.fence::before_thread_sync;");
-                __syncthreads();
+#pragma unroll
+            for (int j = 0; j < RPW; ++j) {
+                const int r = pw + kTcProd * j;
+#pragma unroll
+                for (int a = 0; a < S::KA; ++a) {
+                    const int kk = a * 32 + lane;
+                    const uint32_t hi = cvt_tf32(x[j][a]);
+                    const uint32_t lo = cvt_tf32(x[j][a] - __uint_as_float(hi));
+                    const uint32_t off = sw128_offset(r, kk, S::NT);
+                    *reinterpret_cast<uint32_t*>(xh + off) = hi;
+                    *reinterpret_cast<uint32_t*>(xl + off) = lo;
+                }
             }
-            if (tid == 0) issue(b ^ 1);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar_full[st]));
+            // the table of tile k (warps 8-11, one per lane quarter), once MMA(k-1) is done
+            const uint32_t* img = timg + (size_t)tile_d[it] * S::IMG_WORDS;
+            if (pw < 4 && img != img_prev) {
+                if (k >= 1 && !warp_wait(&bar_empty[(k - 1) & 1], (uint32_t)(((k - 1) >> 1) & 1))) {
+                    if (lane == 0) give_up();
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+                for (int part = 0; part < 2; ++part)
+#pragma unroll 1
+                    for (int k0 = 0; k0 < S::KP; k0 += 48) {
+                        uint4 u[12];
+                        const uint4* row =
+                            reinterpret_cast<const uint4*>(img + ((size_t)part * 128 + 32 * pw + lane) * S::KP + k0);
+#pragma unroll
+                        for (int q = 0; q < 12; ++q) u[q] = (k0 + 4 * q < S::KP) ? __ldg(row + q) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                        for (int h = 0; h < 3; ++h) {
+                            if (k0 + 16 * h >= S::KP) break;
+                            uint32_t r16[16];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                r16[4 * q] = u[4 * h + q].x;
+                                r16[4 * q + 1] = u[4 * h + q].y;
+                                r16[4 * q + 2] = u[4 * h + q].z;
+                                r16[4 * q + 3] = u[4 * h + q].w;
+                            }
+                            tmem_st16(tmem + ((uint32_t)(32 * pw) << 16) +
+                                          (uint32_t)((part ? S::COL_ALO : S::COL_AHI) + k0 + 16 * h),
+                                      r16);
+                        }
+                    }
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&bar_table));
+            }
+            img_prev = img;
         }
-    }
-    if (!failed) {
-        wait_mma(i1 - 1);
-        if (!failed && warp < kGather) epilogue((int)((i1 - 1 - i0) & 1), meta(i1 - 1));
+    } else if (warp == kTcMmaWarp) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            constexpr uint32_t idesc = tf32_idesc_ts<S::NT>();
+            int cur_d = -1;
+            uint32_t nchg = 0;
+            int64_t issued = 0;
+            for (int64_t k = 0; k < ntile && !*abort; ++k) {
+                const int64_t it = i0 + k;
+                const int st = (int)(k & 1);
+                const int d = tile_d[it];
+                bool ok = true;
+                if (d != cur_d) {
+                    ok = mbar_wait_bounded(smem_u32(&bar_table), nchg & 1, kTcWait, abort);
+                    ++nchg;
+                    cur_d = d;
+                }
+                ok = ok && mbar_wait_bounded(smem_u32(&bar_full[st]), (uint32_t)((k >> 1) & 1), kTcWait, abort);
+                ok = ok && (k < 2 || mbar_wait_bounded(smem_u32(&bar_acce[st]), (uint32_t)(((k - 2) >> 1) & 1),
+                                                       kTcWait, abort));
+                if (!ok) {
+                    give_up();
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t xh = smem_u32(xbuf + (size_t)st * 2 * S::X_BYTES), xl = xh + S::X_BYTES;
+                const uint32_t dcol = tmem + (uint32_t)(S::COL_D0 + st * S::NT);
+                const uint32_t As[3] = {(uint32_t)S::COL_AHI, (uint32_t)S::COL_ALO, (uint32_t)S::COL_AHI};
+                const uint32_t Bs[3] = {xl, xh, xh};  // A_hi X_lo, A_lo X_hi, then A_hi X_hi
+                uint32_t acc = 0;
+#pragma unroll
+                for (int t = 0; t < 3; ++t)
+#pragma unroll
+                    for (int s2 = 0; s2 < S::KSTEPS; ++s2) {
+                        const uint32_t kb = (uint32_t)((s2 >> 2) * S::NT * 128 + (s2 & 3) * 32);
+                        umma_tf32_ts(dcol, tmem + As[t] + (uint32_t)(8 * s2), sw128_desc(Bs[t] + kb), idesc, acc);
+                        acc = 1;
+                    }
+                umma_commit(smem_u32(&bar_empty[st]));
+                umma_commit(smem_u32(&bar_accf[st]));
+                issued = k + 1;
+            }
+            // on a give-up, let the MMAs already issued finish before the memory is freed
+            if (*abort && issued > 0) {
+                const int64_t k = issued - 1;
+                mbar_wait_bounded(smem_u32(&bar_empty[k & 1]), (uint32_t)((k >> 1) & 1), kTcWait);
+            }
+        }
+        __syncwarp();
+    } else if (warp < 8) {
+        // ---------------- epilogue ----------------
+        const int q = warp & 3, g = warp >> 2;  // lane quarter, column half (64 pairs)
+        const int n = 32 * q + lane;
+        for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
+            const int64_t it = i0 + k;
+            const int st = (int)(k & 1);
+            const int64_t p0 = tile_begin[it];
+            const int cnt = tile_count[it];
+            // the rows' V positions of this warp's 64 columns: lane j holds columns
+            // 64 g + j and 64 g + 32 + j
+            const int c_a = 64 * g + lane, c_b = c_a + 32;
+            const int64_t e_a = c_a < cnt ? pair_e[p0 + c_a] : 0;
+            const int64_t e_b = c_b < cnt ? pair_e[p0 + c_b] : 0;
+            if (!warp_wait(&bar_accf[st], (uint32_t)((k >> 1) & 1))) {
+                if (lane == 0) give_up();
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (32 * q < NC) {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const int c0 = 64 * g + 16 * h;
+                    if (c0 >= cnt) break;
+                    float vals[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * S::NT + c0), vals);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int c = 16 * h + i;  // column within the warp's half
+                        const int64_t e = __shfl_sync(0xffffffffu, c < 32 ? e_a : e_b, c & 31);
+                        if (n < NC && c0 + i < cnt) __stcs(Y + (e * m + v) * NC + n, vals[i]);  // streamed
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar_acce[st]));
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
