@@ -68,6 +68,7 @@ def lib():
             "fmmgpu_fmm_kind_times": (C.c_int, [vp, dp]),
             "fmmgpu_fmm_set_kinds": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_graph": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_set_overlap": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
@@ -276,6 +277,10 @@ class Fmm(Plan):
 
     def set_kind_timing(self, on=True):
         _check(lib().fmmgpu_fmm_set_kind_timing(self._h, int(on)))
+
+    def set_overlap(self, on=True):
+        """Near field on a second stream beside the far field (default off)."""
+        _check(lib().fmmgpu_fmm_set_overlap(self._h, int(on)))
 
     def set_graph(self, on=True):
         """Replay later evaluations from one captured CUDA graph of the whole sweep."""

@@ -130,6 +130,7 @@ struct EvaluatorBase {
     int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
     int64_t launches = 0;  // kernels launched by the last evaluation
+    bool overlap = false;  // near field on its own stream beside the far field (measured: no gain)
     unsigned counted(unsigned grid) {  // wraps the grid of every evaluation launch
         ++launches;
         return grid;
@@ -179,6 +180,10 @@ struct Evaluator final : EvaluatorBase {
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec;
+    // the near field summed apart on a second, lower-priority stream, joined by output_kernel
+    DevBuf near_phi, near_g;
+    cudaStream_t near_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     P2pItems items{};
     std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
     ClosePairs close{};
@@ -273,6 +278,13 @@ struct Evaluator final : EvaluatorBase {
         build_m2l_batches(kGemmPairs);
         if (kTensor) build_tensor_m2l(m2l);
         build_p2p_items();
+        int least = 0, greatest = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_TRY(cudaStreamCreateWithPriority(&near_stream, cudaStreamNonBlocking, least));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        near_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
+        if (gradients) near_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         if (kMixed) {
             build_close_pairs(us, ut);
             near_rec.alloc(sizeof(NearRec) * (pl.near.nnz() + 1));
@@ -283,7 +295,7 @@ struct Evaluator final : EvaluatorBase {
             CUDA_TRY(cudaDeviceSynchronize());
         }
         close_pairs = nclose;
-        Y.alloc(sizeof(T) * (size_t)m * NC * (pl.v.nnz() + 1));
+        Y.alloc(sizeof(T) * (size_t)m * ys_of(P) * (pl.v.nnz() + 1));
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
         if (gemm_smem > 48 * 1024)
             CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
@@ -296,6 +308,15 @@ struct Evaluator final : EvaluatorBase {
     }
 
     size_t gemm_smem = 0;
+
+    ~Evaluator() override {
+        if (near_stream) {
+            cudaStreamSynchronize(near_stream);
+            cudaStreamDestroy(near_stream);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+    }
 
     void build_tensor_m2l(const std::vector<double>& m2l) {
         if constexpr (kTensor) {
@@ -438,7 +459,7 @@ struct Evaluator final : EvaluatorBase {
         oct_tile_count.upload(tc);
         oct_pair_e.upload(pe);
         oct_pair_src.upload(ps);
-        Yo.alloc(sizeof(T) * (size_t)m * NC * plan.nboxes());
+        Yo.alloc(sizeof(T) * (size_t)m * ys_of(P) * plan.nboxes());
     }
 
     void build_p2p_items() {
@@ -541,7 +562,8 @@ struct Evaluator final : EvaluatorBase {
                                &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
-                               &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count};
+                               &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
+                               &near_phi, &near_g};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -558,6 +580,21 @@ struct Evaluator final : EvaluatorBase {
             int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
             CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * NC * top, stream));
         });
+        if (overlap && !timer.on && kinds == 3 && items.count) {
+            // the near field on near_stream (it needs only the charges) beside the far-field
+            // chain on the evaluator's stream; output_kernel adds them: far + near, the same
+            // addition as the fused P2P epilogue, so the same floats
+            CUDA_TRY(cudaEventRecord(ev_fork, stream));
+            CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
+            p2p_items(0, items.count, 1, 2, near_phi.as<double>(), gradients ? near_g.as<double>() : nullptr,
+                      near_stream);
+            CUDA_TRY(cudaEventRecord(ev_join, near_stream));
+            run_far();
+            CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
+            output(d_phi, d_grad, true);
+            CUDA_TRY(cudaGetLastError());
+            return;
+        }
         if (!(kinds & 2)) {
             // far field off: zero partials, then the near field and the output pass only
             CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
@@ -567,6 +604,13 @@ struct Evaluator final : EvaluatorBase {
         }
         if (items.count) timer.run(kP2P, [&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
         CUDA_TRY(cudaGetLastError());
+    }
+
+    void output(double* d_phi, double* d_grad, bool with_near) {
+        if (plan.nleaves())
+            output_kernel<<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
+                dp, m, far_phi.as<double>(), far_g.as<double>(), with_near ? near_phi.as<double>() : nullptr,
+                with_near && gradients ? near_g.as<double>() : nullptr, d_phi, gradients ? d_grad : nullptr);
     }
 
     void run_far() {
@@ -689,9 +733,12 @@ struct Evaluator final : EvaluatorBase {
     }
 
     // P2P over work items [i0, i1); accumulate = 0 adds the far partial and writes the
-    // scaled output in caller order, 1 adds into the leaf-order store (level calls)
-    void p2p_items(int64_t i0, int64_t i1, int near, int accumulate, double* d_phi, double* d_grad) {
+    // scaled output in caller order, 1 adds into the leaf-order store (level calls), 2
+    // writes the near field alone in leaf order into d_phi / d_grad
+    void p2p_items(int64_t i0, int64_t i1, int near, int accumulate, double* d_phi, double* d_grad,
+                   cudaStream_t s = nullptr) {
         if (i1 <= i0) return;
+        if (!s) s = stream;
         P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
         double* fg = gradients ? far_g.as<double>() : nullptr;
         double* og = gradients ? d_grad : nullptr;
@@ -701,21 +748,21 @@ struct Evaluator final : EvaluatorBase {
             const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
             const auto* q = reinterpret_cast<const float*>(sq.ptr);
             if (gradients)
-                p2p_x2_kernel<true><<<counted(g), 32 * kX2Warps, 0, stream>>>(
+                p2p_x2_kernel<true><<<counted(g), 32 * kX2Warps, 0, s>>>(
                     dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(), fg,
                     accumulate, d_phi, og);
             else
-                p2p_x2_kernel<false><<<counted(g), 32 * kX2Warps, 0, stream>>>(
+                p2p_x2_kernel<false><<<counted(g), 32 * kX2Warps, 0, s>>>(
                     dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(), fg,
                     accumulate, d_phi, og);
         } else {
             const unsigned g = (unsigned)((it.count + kP2pWarps - 1) / kP2pWarps);
             if (gradients)
-                p2p_kernel<T, true, kMixed><<<counted(g), 32 * kP2pWarps, 0, stream>>>(
+                p2p_kernel<T, true, kMixed><<<counted(g), 32 * kP2pWarps, 0, s>>>(
                     dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
                     far_phi.as<double>(), fg, accumulate, d_phi, og);
             else
-                p2p_kernel<T, false, kMixed><<<counted(g), 32 * kP2pWarps, 0, stream>>>(
+                p2p_kernel<T, false, kMixed><<<counted(g), 32 * kP2pWarps, 0, s>>>(
                     dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
                     far_phi.as<double>(), fg, accumulate, d_phi, og);
         }
@@ -758,9 +805,7 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void op_output(double* d_phi, double* d_grad) override {
-        if (plan.nleaves())
-            output_kernel<<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
-                dp, m, far_phi.as<double>(), far_g.as<double>(), d_phi, gradients ? d_grad : nullptr);
+        output(d_phi, d_grad, false);
         CUDA_TRY(cudaGetLastError());
     }
 };
@@ -957,7 +1002,9 @@ int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t ns, const double* s
         const fmmgpu_settings& s = f->settings;
         CUDA_TRY(cudaSetDevice(s.device));
         const Plan& P = f->plan;
-        CUDA_TRY(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+        int least = 0, greatest = 0;  // the far-field chain is the critical path: highest priority
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_TRY(cudaStreamCreateWithPriority(&f->stream, cudaStreamNonBlocking, greatest));
         size_t bytes = 0;
         if (s.precision == FMMGPU_PRECISION_F64)
             f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0,
@@ -1083,6 +1130,16 @@ int fmmgpu_fmm_set_kinds(fmmgpu_fmm* f, int kinds) {
     return guarded([&] {
         if (!f || !f->eval || kinds < 1 || kinds > 3) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid kinds");
         f->eval->kinds = kinds;
+        f->drop_graph();
+    });
+}
+
+int fmmgpu_fmm_set_overlap(fmmgpu_fmm* f, int on) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->eval->overlap = on != 0;
         f->drop_graph();
     });
 }

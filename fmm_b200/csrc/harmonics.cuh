@@ -10,6 +10,9 @@
 namespace fmmb {
 
 __host__ __device__ constexpr int nc_of(int p) { return (p + 1) * (p + 1); }
+// row stride of the translation products (Y, Yo): (p+1)^2 rounded up to 32 slots, so that
+// a row is whole 128-byte lines and a warp's store of 32 slots writes one full line
+__host__ __device__ constexpr int ys_of(int p) { return ((nc_of(p) + 31) / 32) * 32; }
 __host__ __device__ constexpr int slot(int n, int m) { return n * n + n + m; }
 
 template <typename T>

@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
 template <int P, typename T>
 __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ parents, int64_t n, int m,
                                   const T* __restrict__ Yo, T* __restrict__ M) {
-    constexpr int NC = nc_of(P);
+    constexpr int NC = nc_of(P), YS = ys_of(P);
     const int64_t j = blockIdx.x;
     if (j >= n) return;
     const int p = parents[j];
@@ -300,7 +300,7 @@ __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ pare
             T s = T(0);
 #pragma unroll
             for (int o = 0; o < 8; ++o)
-                if (plan.src_below[c0 + o]) s += Yo[((int64_t)(c0 + o) * m + v) * NC + i];
+                if (plan.src_below[c0 + o]) s += Yo[((int64_t)(c0 + o) * m + v) * YS + i];
             M[((int64_t)p * m + v) * NC + i] = s;
         }
 }
@@ -316,24 +316,24 @@ template <int P, typename T>
 __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l, int with_v,
                                     int accumulate, const T* __restrict__ Yo, const T* __restrict__ Yv,
                                     T* __restrict__ Lc) {
-    constexpr int NC = nc_of(P);
+    constexpr int NC = nc_of(P), YS = ys_of(P);
     const int64_t b = b0 + blockIdx.x;
     if (b >= b1 || plan.tgt_below[b] == 0) return;
     const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
     for (int v = 0; v < m; ++v)
         for (int i = threadIdx.x; i < NC; i += blockDim.x) {
             T s = accumulate ? Lc[(b * m + v) * NC + i] : T(0);
-            if (with_l2l) s = accumulate ? s + Yo[(b * m + v) * NC + i] : Yo[(b * m + v) * NC + i];
+            if (with_l2l) s = accumulate ? s + Yo[(b * m + v) * YS + i] : Yo[(b * m + v) * YS + i];
             int64_t e = e0;
             for (; e + 4 <= e1; e += 4) {
-                const T y0 = __ldcs(Yv + (e * m + v) * NC + i), y1 = __ldcs(Yv + ((e + 1) * m + v) * NC + i);
-                const T y2 = __ldcs(Yv + ((e + 2) * m + v) * NC + i), y3 = __ldcs(Yv + ((e + 3) * m + v) * NC + i);
+                const T y0 = __ldcs(Yv + (e * m + v) * YS + i), y1 = __ldcs(Yv + ((e + 1) * m + v) * YS + i);
+                const T y2 = __ldcs(Yv + ((e + 2) * m + v) * YS + i), y3 = __ldcs(Yv + ((e + 3) * m + v) * YS + i);
                 s += y0;
                 s += y1;
                 s += y2;
                 s += y3;
             }
-            for (; e < e1; ++e) s += __ldcs(Yv + (e * m + v) * NC + i);
+            for (; e < e1; ++e) s += __ldcs(Yv + (e * m + v) * YS + i);
             Lc[(b * m + v) * NC + i] = s;
         }
 }
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
         for (int i = 0; i < 4; ++i) {
             int pr = ty * 4 + i;
             if (pr >= cnt) continue;
-            T* y = Y + (pair_e[p0 + pr] * m + v) * NC;
+            T* y = Y + (pair_e[p0 + pr] * m + v) * ys_of(P);
 #pragma unroll
             for (int j = 0; j < JN; ++j) {
                 int n = tx + 16 * j;
@@ -733,6 +733,16 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
                 }
             }
         }
+        if (accumulate == 2) {  // near field alone, leaf order (added to the far field by output_kernel)
+            out_phi[(int64_t)v * nt + t] = aphi;
+            if (GRAD) {
+                double* o = out_g + ((int64_t)v * nt + t) * 3;
+                o[0] = ag0;
+                o[1] = ag1;
+                o[2] = ag2;
+            }
+            continue;
+        }
         const double ph = far_phi[(int64_t)v * nt + t] + aphi;
         if (accumulate) {  // level calls: add into the leaf-order store, scaled by output_kernel
             far_phi[(int64_t)v * nt + t] = ph;
@@ -756,12 +766,15 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
     }
 }
 
-// Output pass of the level calls (fmm-kernels/src/movement.rs:411 gather_output with the
-// scaling of fmm-exec/src/fmm.rs:4750-4778): phi = phi_hat / (4 pi r_t) and
-// g = g_hat / ((4 pi r_t) r_t), leaf order -> caller order.  Block per leaf; the same
-// expressions as the P2P kernels' fused output, so both give the same floats.
+// Output pass (fmm-kernels/src/movement.rs:411 gather_output with the scaling of
+// fmm-exec/src/fmm.rs:4750-4778): phi = phi_hat / (4 pi r_t) and
+// g = g_hat / ((4 pi r_t) r_t), leaf order -> caller order, phi_hat = far + near when the
+// near field was summed apart (near_phi non-null), else the store as it is (level calls).
+// Block per leaf; the same expressions as the P2P kernels' fused output, so all of them
+// give the same floats.
 __global__ void output_kernel(DevPlan plan, int m, const double* __restrict__ far_phi,
-                              const double* __restrict__ far_g, double* __restrict__ out_phi,
+                              const double* __restrict__ far_g, const double* __restrict__ near_phi,
+                              const double* __restrict__ near_g, double* __restrict__ out_phi,
                               double* __restrict__ out_g) {
     const int64_t leaf = blockIdx.x;
     const int box = plan.leaf_box[leaf];
@@ -772,13 +785,22 @@ __global__ void output_kernel(DevPlan plan, int m, const double* __restrict__ fa
     for (int v = 0; v < m; ++v)
         for (int64_t t = plan.tgt_start[leaf] + threadIdx.x; t < plan.tgt_start[leaf + 1]; t += blockDim.x) {
             const int64_t i = plan.tgt_perm[t];
-            out_phi[(int64_t)v * nt + i] = far_phi[(int64_t)v * nt + t] / phi_scale;
+            const double ph = near_phi ? far_phi[(int64_t)v * nt + t] + near_phi[(int64_t)v * nt + t]
+                                       : far_phi[(int64_t)v * nt + t];
+            out_phi[(int64_t)v * nt + i] = ph / phi_scale;
             if (out_g) {
                 const double* fg = far_g + ((int64_t)v * nt + t) * 3;
                 double* o = out_g + ((int64_t)v * nt + i) * 3;
-                o[0] = fg[0] / g_scale;
-                o[1] = fg[1] / g_scale;
-                o[2] = fg[2] / g_scale;
+                if (near_phi) {
+                    const double* ng = near_g + ((int64_t)v * nt + t) * 3;
+                    o[0] = (fg[0] + ng[0]) / g_scale;
+                    o[1] = (fg[1] + ng[1]) / g_scale;
+                    o[2] = (fg[2] + ng[2]) / g_scale;
+                } else {
+                    o[0] = fg[0] / g_scale;
+                    o[1] = fg[1] / g_scale;
+                    o[2] = fg[2] / g_scale;
+                }
             }
         }
 }

@@ -155,14 +155,15 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 // with the gathered multipoles X as the shared-memory B operand (N = 128 pairs,
 // K-major, 128-byte swizzled).  Roles, coupled only by mbarriers (no block barrier in
 // the loop):
-//   warps 8-15 (producers): tile k into X stage k&1 once MMA(k-2) has released it
-//     (empty[k&1]), signal full[k&1]; warps 8-11 also replace the table in tensor
+//   warps 8-15 (producers): load tile k's multipoles, then split them into X stage k&1
+//     once MMA(k-2) has released it (empty[k&1]), signal full[k&1]; warps 8-11 also replace the table in tensor
 //     memory when the offset changes, after MMA(k-1) has read the old one (table);
 //   warp 16, one thread (MMA): waits full[k&1], the table and the accumulator k&1
 //     (acc_empty, released by the epilogue of tile k-2), issues the 3 x KSTEPS MMAs
 //     and commits to empty[k&1] and acc_full[k&1];
 //   warps 0-7 (epilogue): wait acc_full[k&1], read the accumulator with tcgen05.ld
-//     and stream the products Y past L2, then release acc_empty[k&1].
+//     and stream the products Y past L2 in whole 128-byte lines (rows padded to
+//     ys_of(P) slots), then release acc_empty[k&1].
 // Every wait is bounded; a role that gives up sets the shared abort flag (which ends
 // the other roles' waits) and *error, and the CTA frees its tensor memory and returns.
 // One vector per launch.
@@ -288,10 +289,6 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             const int st = (int)(k & 1);
             const int cnt = ncnt;
             const int my_src = nsrc;
-            if (k >= 2 && !warp_wait(&bar_empty[st], (uint32_t)(((k - 2) >> 1) & 1))) {
-                if (lane == 0) give_up();
-                break;
-            }
             unsigned char* xh = xbuf + (size_t)st * 2 * S::X_BYTES;
             unsigned char* xl = xh + S::X_BYTES;
             float x[RPW][S::KA];
@@ -311,6 +308,11 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 ncnt = tile_count[it + 1];
                 nsrc = 0;
                 if (lane < RPW && pw + kTcProd * lane < ncnt) nsrc = pair_src[nb + pw + kTcProd * lane];
+            }
+            // the stage is written only once MMA(k-2) has read it; the loads above need no stage
+            if (k >= 2 && !warp_wait(&bar_empty[st], (uint32_t)(((k - 2) >> 1) & 1))) {
+                if (lane == 0) give_up();
+                break;
             }
 #pragma unroll
             for (int j = 0; j < RPW; ++j) {
@@ -436,7 +438,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            if (32 * q < NC) {
+            if (32 * q < ys_of(P)) {
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     const int c0 = 64 * g + 16 * h;
@@ -447,7 +449,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                     for (int i = 0; i < 16; ++i) {
                         const int c = 16 * h + i;  // column within the warp's half
                         const int64_t e = __shfl_sync(0xffffffffu, c < 32 ? e_a : e_b, c & 31);
-                        if (n < NC && c0 + i < cnt) __stcs(Y + (e * m + v) * NC + n, vals[i]);  // streamed
+                        // whole 128-byte lines (rows >= NC of the table are zero), streamed
+                        if (c0 + i < cnt) __stcs(Y + (e * m + v) * ys_of(P) + n, vals[i]);
                     }
                 }
             }

@@ -208,6 +208,16 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
             }
         }
         // both gradient sums hold -sum qr3 (t - y), as p2p_kernel's
+        if (accumulate == 2) {  // near field alone, leaf order (added to the far field by output_kernel)
+            out_phi[(int64_t)v * nt + t] = aphi;
+            if (GRAD) {
+                double* o = out_g + ((int64_t)v * nt + t) * 3;
+                o[0] = ag0;
+                o[1] = ag1;
+                o[2] = ag2;
+            }
+            continue;
+        }
         const double ph = far_phi[(int64_t)v * nt + t] + aphi;
         if (accumulate) {  // level calls: add into the leaf-order store, scaled by output_kernel
             far_phi[(int64_t)v * nt + t] = ph;

@@ -105,6 +105,14 @@ void* fmmgpu_fmm_stream(fmmgpu_fmm* fmm);
  * Off (0) by default.  Synchronises. */
 int fmmgpu_fmm_set_graph(fmmgpu_fmm* fmm, int on);
 
+/* Near field beside the far field (on = 1): an evaluation runs P2P on a second,
+ * lower-priority stream, concurrently with the far-field passes, and one output pass adds
+ * the two (the same addition as the serial order, so the same floats).  0, the default,
+ * runs everything on one stream (on one B200 the two halves compete for the same FP32
+ * pipes and the overlap measured no faster).  Per-kind timing always runs on one stream.
+ * Synchronises. */
+int fmmgpu_fmm_set_overlap(fmmgpu_fmm* fmm, int on);
+
 /* Per-kind device timing of the following evaluations (the reference's KindTiming,
  * fmm-exec/src/fmm.rs:150-153): every launch is bracketed by CUDA events. */
 int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* fmm, int on);

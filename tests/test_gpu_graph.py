@@ -39,3 +39,21 @@ def test_graph_device_buffers_recapture(oracle):
         fmm.synchronize()
         assert np.array_equal(dphi.cpu().numpy(), want.potential[0])
         assert np.array_equal(dg.cpu().numpy().reshape(n, 3), want.gradient[0])
+
+
+@pytest.mark.parametrize("precision,m", [("f64", 1), ("mixed", 1), ("mixed", 2)])
+def test_overlapped_near_field_equals_one_stream(oracle, precision, m):
+    """P2P on its own stream beside the far field gives the floats of the one-stream order."""
+    x, q = oracle.point_sets("sphere", 30000, 6)
+    q = np.stack([q * (v + 1) for v in range(m)], axis=1)
+    fmm = F.FmmBuilder(8).gradients().vectors(m).max_points_per_leaf(64).precision(precision).build(x)
+    fmm.set_overlap(True)
+    a = fmm.evaluate(q)  # overlapped
+    fmm.set_overlap(False)
+    b = fmm.evaluate(q)
+    assert np.array_equal(a.potential, b.potential) and np.array_equal(a.gradient, b.gradient)
+    fmm.set_overlap(True)
+    fmm.set_graph(True)
+    for _ in range(2):
+        c = fmm.evaluate(q)
+        assert np.array_equal(c.potential, b.potential) and np.array_equal(c.gradient, b.gradient)
