@@ -55,6 +55,8 @@ def lib():
             "fmmgpu_default_settings": (None, [C.POINTER(Settings)]),
             "fmmgpu_fmm_build": (C.c_int, [C.POINTER(Settings), sz, dp, sz, dp, C.POINTER(vp)]),
             "fmmgpu_plan_build": (C.c_int, [C.POINTER(Settings), sz, dp, sz, dp, C.POINTER(vp)]),
+            "fmmgpu_batch_build": (C.c_int, [C.POINTER(Settings), sz, dp, dp, dp, dp, C.POINTER(vp)]),
+            "fmmgpu_batch_plan_build": (C.c_int, [C.POINTER(Settings), sz, dp, dp, dp, dp, C.POINTER(vp)]),
             "fmmgpu_fmm_evaluate": (C.c_int, [vp, dp, dp, dp]),
             "fmmgpu_fmm_evaluate_device": (C.c_int, [vp, dp, dp, dp]),
             "fmmgpu_fmm_stream": (vp, [vp]),
@@ -169,6 +171,34 @@ class FmmBuilder:
         h = C.c_void_p()
         _check(lib().fmmgpu_fmm_build(C.byref(self._s), len(src), _ptr(src), len(tgt), _ptr(tgt), C.byref(h)))
         return Fmm(h, self._s, len(src), len(tgt))
+
+    def _batch(self, fn, clouds, targets):
+        srcs = [_points(c) for c in clouds]
+        ns = np.array([len(c) for c in srcs], dtype=np.uint64)
+        src = np.ascontiguousarray(np.concatenate(srcs) if srcs else np.zeros((0, 3)))
+        if targets is None:
+            nt, tgt, ntot = None, None, int(ns.sum())
+        else:
+            tgts = [_points(c) for c in targets]
+            if len(tgts) != len(srcs):
+                raise ValueError("one target set per cloud")
+            nt = np.array([len(c) for c in tgts], dtype=np.uint64)
+            tgt = np.ascontiguousarray(np.concatenate(tgts))
+            ntot = int(nt.sum())
+        h = C.c_void_p()
+        _check(fn(C.byref(self._s), len(srcs), _ptr(ns), _ptr(src), _ptr(nt), _ptr(tgt), C.byref(h)))
+        return h, int(ns.sum()), ntot
+
+    def build_batch(self, clouds, targets=None):
+        """Many independent clouds as one forest: one launch per pass for the whole batch.
+        Charges and outputs are the clouds' arrays concatenated in cloud order."""
+        h, ns, nt = self._batch(lib().fmmgpu_batch_build, clouds, targets)
+        return Fmm(h, self._s, ns, nt)
+
+    def plan_batch(self, clouds, targets=None):
+        """The host half of build_batch (no GPU)."""
+        h, ns, nt = self._batch(lib().fmmgpu_batch_plan_build, clouds, targets)
+        return Plan(h, self._s, ns, nt)
 
     def plan(self, sources, targets=None):
         """The host half only (tree, lists, tables); needs no GPU."""

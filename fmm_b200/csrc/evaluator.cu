@@ -3,11 +3,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fmm_b200.h"
@@ -154,7 +156,7 @@ struct Evaluator final : EvaluatorBase {
     // plan arrays
     DevBuf level, idx, parent, child_first, box_leaf, src_below, tgt_below, leaf_box, src_start,
         tgt_start, tgt_perm, src_perm, near_row, near_col, w_row, w_col, x_row, x_col, v_row, v_col,
-        v_off;
+        v_off, box_side;
     // data
     DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g, Y;
     // interior boxes per level with a source below (M2M parents), CSR by level
@@ -243,6 +245,8 @@ struct Evaluator final : EvaluatorBase {
         dp.v_row = v_row.as<int64_t>();
         dp.v_col = v_col.as<int32_t>();
         dp.v_off = v_off.as<int32_t>();
+        if (!pl.box_side.empty()) box_side.upload(pl.box_side);
+        dp.box_side = pl.box_side.empty() ? nullptr : box_side.as<double>();
         dp.nsrc = (int64_t)pl.src_perm.size();
         dp.ntgt = (int64_t)pl.tgt_perm.size();
         // tables rounded entry by entry to T (fmm-tables/src/matrix_set.rs:150 cast)
@@ -563,7 +567,7 @@ struct Evaluator final : EvaluatorBase {
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
-                               &near_phi, &near_g};
+                               &near_phi, &near_g, &box_side};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -931,26 +935,20 @@ void fmmgpu_default_settings(fmmgpu_settings* s) {
 
 namespace {
 
-// Host part of a build: plan, tables, leaf-scaled coordinates (no device work).
-std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
-                                       const double* tgt, std::vector<double>& us, std::vector<double>& ut) {
+void check_settings(const fmmgpu_settings* settings) {
     if (!settings) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
     const fmmgpu_settings& s = *settings;
     if (s.p < 0 || s.vectors < 1 || s.max_points_per_leaf < 1 || s.max_level < 0 || s.max_level > 16)
         throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid settings");
     if (s.precision != FMMGPU_PRECISION_F64 && s.precision != FMMGPU_PRECISION_MIXED)
         throw Failure(FMMGPU_UNSUPPORTED, "unknown precision");
-    if ((ns && !src) || (nt && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
-    auto f = std::make_unique<fmmgpu_fmm>();
-    f->settings = s;
-    f->plan = build_plan(ns, src, nt, tgt, s.max_level, s.max_points_per_leaf);
-    build_m2l_tables(s.p, f->m2l);
-    build_m2m_tables(s.p, f->m2m);
-    build_l2l_tables(s.p, f->l2l);
-    const Plan& P = f->plan;
-    // leaf-scaled coordinates in leaf order (CONVENTIONS 3.13)
-    us.assign(3 * ns, 0.0);
-    ut.assign(3 * nt, 0.0);
+}
+
+// leaf-scaled coordinates in the plan's leaf order (CONVENTIONS 3.13)
+void leaf_scaled(const Plan& P, const double* src, const double* tgt, std::vector<double>& us,
+                 std::vector<double>& ut) {
+    us.assign(3 * P.src_perm.size(), 0.0);
+    ut.assign(3 * P.tgt_perm.size(), 0.0);
     for (size_t j = 0; j < P.nleaves(); ++j) {
         int b = P.leaf_box[j];
         for (int64_t a = P.src_start[j]; a < P.src_start[j + 1]; ++a) {
@@ -964,14 +962,114 @@ std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t n
                 ut[3 * a + k] = leaf_coordinate(tgt[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
         }
     }
+}
+
+int64_t count_near_pairs(const Plan& P) {
+    int64_t n = 0;
     for (size_t j = 0; j < P.nleaves(); ++j) {
         int64_t nt_j = P.tgt_start[j + 1] - P.tgt_start[j];
         for (int64_t e = P.near.row[j]; e < P.near.row[j + 1]; ++e) {
             int sj = P.near.col[e];
-            f->near_pairs += nt_j * (P.src_start[sj + 1] - P.src_start[sj]);
+            n += nt_j * (P.src_start[sj + 1] - P.src_start[sj]);
         }
     }
+    return n;
+}
+
+// Host part of a build: plan, tables, leaf-scaled coordinates (no device work).
+std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
+                                       const double* tgt, std::vector<double>& us, std::vector<double>& ut) {
+    check_settings(settings);
+    const fmmgpu_settings& s = *settings;
+    if ((ns && !src) || (nt && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
+    auto f = std::make_unique<fmmgpu_fmm>();
+    f->settings = s;
+    f->plan = build_plan(ns, src, nt, tgt, s.max_level, s.max_points_per_leaf);
+    build_m2l_tables(s.p, f->m2l);
+    build_m2m_tables(s.p, f->m2m);
+    build_l2l_tables(s.p, f->l2l);
+    leaf_scaled(f->plan, src, tgt, us, ut);
+    f->near_pairs = count_near_pairs(f->plan);
     return f;
+}
+
+// Host part of a batch build: every cloud's plan (in parallel over the host's threads),
+// merged into one forest; the clouds' points are consecutive in the caller's arrays.
+std::unique_ptr<fmmgpu_fmm> build_host_batch(const fmmgpu_settings* settings, size_t ncloud, const size_t* ns,
+                                             const double* src, const size_t* nt, const double* tgt,
+                                             std::vector<double>& us, std::vector<double>& ut) {
+    check_settings(settings);
+    const fmmgpu_settings& s = *settings;
+    if (ncloud == 0 || !ns) throw Failure(FMMGPU_INVALID_ARGUMENT, "no clouds");
+    const bool same = nt == nullptr;  // targets are the sources
+    std::vector<TreePart> parts(ncloud);
+    int64_t so = 0, to = 0;
+    for (size_t c = 0; c < ncloud; ++c) {
+        parts[c].src_offset = so;
+        parts[c].tgt_offset = to;
+        so += (int64_t)ns[c];
+        to += (int64_t)(same ? ns[c] : nt[c]);
+    }
+    if ((so && !src) || (to && !same && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
+    std::vector<std::string> errors(ncloud);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t c; (c = next.fetch_add(1)) < ncloud;) {
+            try {
+                TreePart& tp = parts[c];
+                const double* cs = src + 3 * tp.src_offset;
+                const double* ct = same ? cs : tgt + 3 * tp.tgt_offset;
+                const size_t cnt = same ? ns[c] : nt[c];
+                tp.plan = build_plan(ns[c], cs, cnt, ct, s.max_level, s.max_points_per_leaf);
+                leaf_scaled(tp.plan, cs, ct, tp.us, tp.ut);
+            } catch (const std::exception& e) {
+                errors[c] = e.what();
+            }
+        }
+    };
+    const unsigned nthreads = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)ncloud));
+    std::vector<std::thread> pool;
+    for (unsigned i = 1; i < nthreads; ++i) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (size_t c = 0; c < ncloud; ++c)
+        if (!errors[c].empty()) throw Failure(FMMGPU_INVALID_ARGUMENT, "cloud " + std::to_string(c) + ": " + errors[c]);
+    auto f = std::make_unique<fmmgpu_fmm>();
+    f->settings = s;
+    f->plan = merge_plans(parts, us, ut);
+    build_m2l_tables(s.p, f->m2l);
+    build_m2m_tables(s.p, f->m2m);
+    build_l2l_tables(s.p, f->l2l);
+    f->near_pairs = count_near_pairs(f->plan);
+    return f;
+}
+
+// Device part of a build: the evaluator (plan upload, tables, buffers) on the device.
+void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vector<double>& ut) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        throw Failure(FMMGPU_NO_DEVICE, "no CUDA device is visible");
+    }
+    const fmmgpu_settings& s = f->settings;
+    CUDA_TRY(cudaSetDevice(s.device));
+    const Plan& P = f->plan;
+    int least = 0, greatest = 0;  // the far-field chain is the critical path: highest priority
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CUDA_TRY(cudaStreamCreateWithPriority(&f->stream, cudaStreamNonBlocking, greatest));
+    size_t bytes = 0;
+    if (s.precision == FMMGPU_PRECISION_F64)
+        f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0, us,
+                                         ut, &bytes);
+    else
+        f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0, us,
+                                        ut, &bytes);
+    const size_t ns = P.src_perm.size(), nt = P.tgt_perm.size();
+    f->d_charges.alloc(sizeof(double) * (size_t)s.vectors * (ns + 1));
+    f->d_phi.alloc(sizeof(double) * (size_t)s.vectors * (nt + 1));
+    if (s.gradients) f->d_grad.alloc(sizeof(double) * 3 * (size_t)s.vectors * (nt + 1));
+    f->device_bytes = bytes + f->d_charges.bytes + f->d_phi.bytes + f->d_grad.bytes;
+    CUDA_TRY(cudaDeviceSynchronize());
 }
 
 }  // namespace
@@ -999,24 +1097,35 @@ int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t ns, const double* s
         }
         std::vector<double> us, ut;
         auto f = build_host(settings, ns, src, nt, tgt, us, ut);
-        const fmmgpu_settings& s = f->settings;
-        CUDA_TRY(cudaSetDevice(s.device));
-        const Plan& P = f->plan;
-        int least = 0, greatest = 0;  // the far-field chain is the critical path: highest priority
-        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        CUDA_TRY(cudaStreamCreateWithPriority(&f->stream, cudaStreamNonBlocking, greatest));
-        size_t bytes = 0;
-        if (s.precision == FMMGPU_PRECISION_F64)
-            f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0,
-                                             us, ut, &bytes);
-        else
-            f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0,
-                                            us, ut, &bytes);
-        f->d_charges.alloc(sizeof(double) * (size_t)s.vectors * (ns + 1));
-        f->d_phi.alloc(sizeof(double) * (size_t)s.vectors * (nt + 1));
-        if (s.gradients) f->d_grad.alloc(sizeof(double) * 3 * (size_t)s.vectors * (nt + 1));
-        f->device_bytes = bytes + f->d_charges.bytes + f->d_phi.bytes + f->d_grad.bytes;
-        CUDA_TRY(cudaDeviceSynchronize());
+        build_device(f.get(), us, ut);
+        *out = f.release();
+    });
+}
+
+int fmmgpu_batch_plan_build(const fmmgpu_settings* settings, size_t ncloud, const size_t* nsources,
+                            const double* sources, const size_t* ntargets, const double* targets, fmmgpu_fmm** out) {
+    return guarded([&] {
+        if (!out) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        std::vector<double> us, ut;
+        auto f = build_host_batch(settings, ncloud, nsources, sources, ntargets, targets, us, ut);
+        *out = f.release();
+    });
+}
+
+int fmmgpu_batch_build(const fmmgpu_settings* settings, size_t ncloud, const size_t* nsources, const double* sources,
+                       const size_t* ntargets, const double* targets, fmmgpu_fmm** out) {
+    return guarded([&] {
+        if (!out) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            throw Failure(FMMGPU_NO_DEVICE, "no CUDA device is visible");
+        }
+        std::vector<double> us, ut;
+        auto f = build_host_batch(settings, ncloud, nsources, sources, ntargets, targets, us, ut);
+        build_device(f.get(), us, ut);
         *out = f.release();
     });
 }

@@ -45,6 +45,7 @@ struct DevPlan {
     const int64_t *near_row, *w_row, *x_row, *v_row;
     const int32_t *near_col, *w_col, *x_col, *v_col, *v_off;
     int64_t nsrc, ntgt;
+    const double* box_side;  // forests: the domain side of each box's tree (null: `side`)
 };
 
 // 2^e for |e| <= 126, built from the exponent field (exact, no library call)
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
         ty = p4.y;
         tz = p4.z;
     }
-    const double rt = plan.side * pow2d(-(plan.level[box] + 1));
+    const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;
     const double g_scale = phi_scale * rt;
     for (int v = 0; v < m; ++v) {
@@ -778,7 +779,7 @@ __global__ void output_kernel(DevPlan plan, int m, const double* __restrict__ fa
                               double* __restrict__ out_g) {
     const int64_t leaf = blockIdx.x;
     const int box = plan.leaf_box[leaf];
-    const double rt = plan.side * pow2d(-(plan.level[box] + 1));
+    const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;
     const double g_scale = phi_scale * rt;
     const int64_t nt = plan.ntgt;

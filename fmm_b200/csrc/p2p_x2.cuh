@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
     const float2 ntx = f2(-tx, -tx), nty = f2(-ty, -ty), ntz = f2(-tz, -tz);
     float* sxy_f = reinterpret_cast<float*>(sxy[warp]);
     float* szq_f = reinterpret_cast<float*>(szq[warp]);
-    const double rt = plan.side * pow2d(-(plan.level[box] + 1));
+    const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;
     const double g_scale = phi_scale * rt;
     for (int v = 0; v < m; ++v) {

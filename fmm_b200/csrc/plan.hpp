@@ -59,9 +59,24 @@ struct Plan {
     Csr x;     // source leaves on level l - 1, by leaf index
     Csr v;     // source boxes with aux = offset index, by offset index
 
+    // forests (merge_plans): the domain side of each box's tree; empty for one tree
+    std::vector<double> box_side;
+
     size_t nboxes() const { return key.size(); }
     size_t nleaves() const { return leaf_box.size(); }
 };
+
+// One cloud of a batch: its plan, its leaf-scaled coordinates (plan leaf order) and the
+// offsets of its points in the batch's concatenated caller order.
+struct TreePart {
+    Plan plan;
+    std::vector<double> us, ut;
+    int64_t src_offset = 0, tgt_offset = 0;
+};
+
+// The forest of several clouds' plans (forest.cpp): level-major over all trees, with the
+// merged leaf-scaled coordinates in us / ut.
+Plan merge_plans(std::vector<TreePart>& parts, std::vector<double>& us, std::vector<double>& ut);
 
 // Builds the cubic domain, the tree of the distinct level-16 keys of sources ++ targets
 // (refined while a box holds more than max_keys keys, then 2:1 balanced), the box

@@ -85,6 +85,23 @@ int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t nsources, const dou
 int fmmgpu_plan_build(const fmmgpu_settings* settings, size_t nsources, const double* sources,
                       size_t ntargets, const double* targets, fmmgpu_fmm** out);
 
+/* Multi-cloud batch (no reference counterpart: the reference batches charge vectors
+ * only, FmmBuilder::vectors, fmm.rs:200-227): `ncloud` independent clouds, cloud c with
+ * nsources[c] sources and ntargets[c] targets (ntargets NULL: the targets are the
+ * sources), their points consecutive in `sources` / `targets` (n x 3 doubles).  Each
+ * cloud gets its own octree, exactly as fmmgpu_fmm_build would build it (in parallel
+ * over the host's threads); the trees are merged level by level into one forest, so every
+ * pass of an evaluation is one launch over all clouds and the M2L batches by offset span
+ * the whole batch.  The handle is an ordinary fmmgpu_fmm: charges, potentials and
+ * gradients are the clouds' arrays concatenated in cloud order, and each cloud's results
+ * are the floats its own FMM gives. */
+int fmmgpu_batch_build(const fmmgpu_settings* settings, size_t ncloud, const size_t* nsources,
+                       const double* sources, const size_t* ntargets, const double* targets, fmmgpu_fmm** out);
+/* The host half of a batch build only (no device), like fmmgpu_plan_build. */
+int fmmgpu_batch_plan_build(const fmmgpu_settings* settings, size_t ncloud, const size_t* nsources,
+                            const double* sources, const size_t* ntargets, const double* targets,
+                            fmmgpu_fmm** out);
+
 /* Fmm::evaluate_into (fmm.rs:3719) with HOST buffers: charges[i*m + v] (caller order,
  * m charges of a source adjacent); potential[v*nt + i]; gradient[(v*nt + i)*3 + k] (or
  * NULL without gradients).  Copies in, evaluates, copies out, synchronises. */

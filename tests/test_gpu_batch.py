@@ -1,0 +1,53 @@
+"""Multi-cloud batches on the device: each cloud's results in the forest are the floats
+of its own FMM (f64 and mixed, one and several charge vectors), and match the oracle."""
+import numpy as np
+import pytest
+
+import fmm_b200 as F
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def make_clouds(oracle, sizes):
+    out = []
+    for i, n in enumerate(sizes):
+        kind = ("cube", "sphere")[i % 2]
+        x, _ = oracle.point_sets(kind, n, 100 + i)
+        out.append(x * (0.5 + 0.25 * i) + i)  # different scales and places
+    return out
+
+
+@pytest.mark.parametrize("precision,p,m", [("f64", 6, 1), ("mixed", 8, 1), ("mixed", 6, 3)])
+def test_batch_equals_separate_fmms(oracle, precision, p, m):
+    cs = make_clouds(oracle, [12000, 3000, 20000, 700])
+    rng = np.random.default_rng(5)
+    qs = [rng.uniform(-1, 1, (len(c), m)) for c in cs]
+    builder = F.FmmBuilder(p).gradients().vectors(m).max_points_per_leaf(64).precision(precision)
+    batch = builder.build_batch(cs)
+    out = batch.evaluate(np.concatenate(qs))
+    off = 0
+    for c, q in zip(cs, qs):
+        single = builder.build(c).evaluate(q)
+        n = len(c)
+        assert np.array_equal(out.potential[:, off:off + n], single.potential)
+        assert np.array_equal(out.gradient[:, off:off + n], single.gradient)
+        off += n
+
+
+def test_batch_with_distinct_targets_matches_oracle(oracle):
+    cs = make_clouds(oracle, [8000, 5000])
+    rng = np.random.default_rng(8)
+    ts = [c[::3] + 1e-3 for c in cs]
+    qs = [rng.normal(size=len(c)) for c in cs]
+    batch = F.FmmBuilder(6).gradients().max_points_per_leaf(32).build_batch(cs, ts)
+    out = batch.evaluate(np.concatenate(qs))
+    off = 0
+    for c, t, q in zip(cs, ts, qs):
+        phi, g = oracle.fmm(c, q, t, 6, 32, gradients=True, threads=8)
+        assert rel(out.potential[0, off:off + len(t)], phi) < 1e-12
+        assert rel(out.gradient[0, off:off + len(t)], g) < 1e-12
+        off += len(t)
