@@ -59,6 +59,7 @@ def lib():
             "fmmgpu_batch_plan_build": (C.c_int, [C.POINTER(Settings), sz, dp, dp, dp, dp, C.POINTER(vp)]),
             "fmmgpu_fmm_evaluate": (C.c_int, [vp, dp, dp, dp]),
             "fmmgpu_fmm_evaluate_device": (C.c_int, [vp, dp, dp, dp]),
+            "fmmgpu_fmm_vjp": (C.c_int, [vp, dp, dp, dp, dp, dp]),
             "fmmgpu_fmm_stream": (vp, [vp]),
             "fmmgpu_fmm_synchronize": (C.c_int, [vp]),
             "fmmgpu_fmm_info": (C.c_int, [vp, C.POINTER(Info)]),
@@ -167,7 +168,7 @@ class FmmBuilder:
 
     def build(self, sources, targets=None):
         src = _points(sources)
-        tgt = src if targets is None else _points(targets)
+        tgt = src if targets is None else _points(targets)  # the same array: a symmetric FMM
         h = C.c_void_p()
         _check(lib().fmmgpu_fmm_build(C.byref(self._s), len(src), _ptr(src), len(tgt), _ptr(tgt), C.byref(h)))
         return Fmm(h, self._s, len(src), len(tgt))
@@ -270,6 +271,18 @@ class Fmm(Plan):
         g = np.zeros((m, self.ntargets, 3)) if self.settings.gradients else None
         _check(lib().fmmgpu_fmm_evaluate(self._h, _ptr(q), _ptr(phi), _ptr(g)))
         return Output(phi, g)
+
+    def vjp(self, charges, cotangent):
+        """Vector-Jacobian product of the potentials for the cotangent w (shape (m, nt)):
+        returns (dcharges (ns, m), dsources (ns, 3), dtargets (nt, 3))."""
+        m = self.settings.vectors
+        q = np.ascontiguousarray(charges, dtype=np.float64).reshape(self.nsources, m)
+        w = np.ascontiguousarray(cotangent, dtype=np.float64).reshape(m, self.ntargets)
+        dq = np.zeros((self.nsources, m))
+        dxs = np.zeros((self.nsources, 3))
+        dxt = np.zeros((self.ntargets, 3))
+        _check(lib().fmmgpu_fmm_vjp(self._h, _ptr(q), _ptr(w), _ptr(dq), _ptr(dxs), _ptr(dxt)))
+        return dq, dxs, dxt
 
     def evaluate_levels(self, charges, calls=None):
         """The same evaluation driven by the level calls of the operator ABI, in the

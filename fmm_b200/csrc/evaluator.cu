@@ -862,7 +862,53 @@ struct fmmgpu_fmm {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
     }
+    // vector-Jacobian products: built with targets == sources, the transpose problem is
+    // this FMM; otherwise the points are kept and the swapped FMM is built at the first VJP
+    bool symmetric = false;
+    std::vector<double> src_pts, tgt_pts;
+    fmmgpu_fmm* transpose = nullptr;
+    DevBuf d_vjp_w, d_vjp_tq, d_vjp_dq, d_vjp_dxs, d_vjp_dxt;
 };
+
+namespace fmmb {
+
+// ---- vector-Jacobian products of phi(q, sources, targets) for a cotangent w on phi ----
+// dx_t[i] = sum_v w[v][i] grad phi_v(t_i)   (w, phi in the output layout [v][nt])
+__global__ void vjp_target_kernel(int64_t nt, int m, const double* __restrict__ w, const double* __restrict__ g,
+                                  double* __restrict__ dxt) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nt) return;
+    double a[3] = {0.0, 0.0, 0.0};
+    for (int v = 0; v < m; ++v) {
+        const double wv = w[(int64_t)v * nt + i];
+        for (int k = 0; k < 3; ++k) a[k] += wv * g[((int64_t)v * nt + i) * 3 + k];
+    }
+    for (int k = 0; k < 3; ++k) dxt[3 * i + k] = a[k];
+}
+
+// [v][n] -> [i][v] (outputs of one FMM as the charges of the transpose one)
+__global__ void vjp_transpose_kernel(int64_t n, int m, const double* __restrict__ in, double* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int v = 0; v < m; ++v) out[i * m + v] = in[(int64_t)v * n + i];
+}
+
+// dq[j][v] = psi_v(s_j) and dx_s[j] = sum_v q[j][v] grad psi_v(s_j), psi the transpose FMM's
+// potentials (charges w at the targets, evaluated at the sources)
+__global__ void vjp_source_kernel(int64_t ns, int m, const double* __restrict__ q, const double* __restrict__ psi,
+                                  const double* __restrict__ gpsi, double* __restrict__ dq, double* __restrict__ dxs) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    double a[3] = {0.0, 0.0, 0.0};
+    for (int v = 0; v < m; ++v) {
+        dq[j * m + v] = psi[(int64_t)v * ns + j];
+        const double qv = q[j * m + v];
+        for (int k = 0; k < 3; ++k) a[k] += qv * gpsi[((int64_t)v * ns + j) * 3 + k];
+    }
+    for (int k = 0; k < 3; ++k) dxs[3 * j + k] = a[k];
+}
+
+}  // namespace fmmb
 
 namespace {
 
@@ -1098,6 +1144,11 @@ int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t ns, const double* s
         std::vector<double> us, ut;
         auto f = build_host(settings, ns, src, nt, tgt, us, ut);
         build_device(f.get(), us, ut);
+        f->symmetric = src == tgt && ns == nt;
+        if (!f->symmetric) {
+            f->src_pts.assign(src, src + 3 * ns);
+            f->tgt_pts.assign(tgt, tgt + 3 * nt);
+        }
         *out = f.release();
     });
 }
@@ -1157,6 +1208,63 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
                                      f->stream));
         CUDA_TRY(cudaStreamSynchronize(f->stream));
         if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    });
+}
+
+int fmmgpu_fmm_vjp(fmmgpu_fmm* f, const double* charges, const double* cotangent, double* dcharges,
+                   double* dsources, double* dtargets) {
+    return guarded([&] {
+        if (!f || !charges || !cotangent || !dcharges || !dsources || !dtargets)
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        if (!f->settings.gradients) throw Failure(FMMGPU_INVALID_ARGUMENT, "a VJP needs an FMM built with gradients");
+        if (f->plan.box_side.size()) throw Failure(FMMGPU_UNSUPPORTED, "VJPs of multi-cloud batches are not offered");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const int m = f->settings.vectors;
+        const int64_t ns = (int64_t)f->plan.src_perm.size(), nt = (int64_t)f->plan.tgt_perm.size();
+        fmmgpu_fmm* T = f;
+        if (!f->symmetric) {
+            if (!f->transpose) {  // the swapped problem: charges at the targets, evaluated at the sources
+                std::vector<double> us, ut;
+                auto t = build_host(&f->settings, (size_t)nt, f->tgt_pts.data(), (size_t)ns, f->src_pts.data(), us, ut);
+                build_device(t.get(), us, ut);
+                t->symmetric = true;  // never asked for its own transpose
+                f->transpose = t.release();
+            }
+            T = f->transpose;
+        }
+        f->d_vjp_w.alloc(sizeof(double) * (size_t)m * (nt + 1));
+        f->d_vjp_tq.alloc(sizeof(double) * (size_t)m * (nt + 1));
+        f->d_vjp_dq.alloc(sizeof(double) * (size_t)m * (ns + 1));
+        f->d_vjp_dxs.alloc(sizeof(double) * 3 * (ns + 1));
+        f->d_vjp_dxt.alloc(sizeof(double) * 3 * (nt + 1));
+        cudaStream_t s = f->stream;
+        CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(f->d_vjp_w.ptr, cotangent, sizeof(double) * m * nt, cudaMemcpyHostToDevice, s));
+        // forward pass (recomputed, nothing kept from earlier evaluations): grad phi at the targets
+        run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(), f->d_grad.as<double>());
+        const unsigned bt = (unsigned)((nt + 255) / 256), bs = (unsigned)((ns + 255) / 256);
+        if (nt) {
+            vjp_target_kernel<<<bt, 256, 0, s>>>(nt, m, f->d_vjp_w.as<double>(), f->d_grad.as<double>(),
+                                                f->d_vjp_dxt.as<double>());
+            vjp_transpose_kernel<<<bt, 256, 0, s>>>(nt, m, f->d_vjp_w.as<double>(), f->d_vjp_tq.as<double>());
+        }
+        CUDA_TRY(cudaGetLastError());
+        // transpose pass: charges w at the targets, potentials and gradients at the sources
+        if (T != f) CUDA_TRY(cudaStreamSynchronize(s));  // T runs on its own stream
+        run_evaluation(T, f->d_vjp_tq.as<double>(), T->d_phi.as<double>(), T->d_grad.as<double>());
+        if (T != f) CUDA_TRY(cudaStreamSynchronize(T->stream));
+        if (ns)
+            vjp_source_kernel<<<bs, 256, 0, s>>>(ns, m, f->d_charges.as<double>(), T->d_phi.as<double>(),
+                                                T->d_grad.as<double>(), f->d_vjp_dq.as<double>(),
+                                                f->d_vjp_dxs.as<double>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(dcharges, f->d_vjp_dq.ptr, sizeof(double) * m * ns, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(dsources, f->d_vjp_dxs.ptr, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(dtargets, f->d_vjp_dxt.ptr, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        if (f->eval->device_status() || T->eval->device_status())
+            throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
     });
 }
 
@@ -1304,6 +1412,7 @@ void fmmgpu_fmm_destroy(fmmgpu_fmm* f) {
     if (!f) return;
     if (f->eval || f->stream) cudaSetDevice(f->settings.device);
     if (f->stream) cudaStreamSynchronize(f->stream);
+    if (f->transpose) fmmgpu_fmm_destroy(f->transpose);
     f->drop_graph();
     f->eval.reset();
     f->d_charges.alloc(0);

@@ -107,6 +107,21 @@ int fmmgpu_batch_plan_build(const fmmgpu_settings* settings, size_t ncloud, cons
  * NULL without gradients).  Copies in, evaluates, copies out, synchronises. */
 int fmmgpu_fmm_evaluate(fmmgpu_fmm* fmm, const double* charges, double* potential, double* gradient);
 
+/* Vector-Jacobian product of the potentials (no reference counterpart; the reference has
+ * no adjoint): for charges q and a cotangent w on the potentials (both HOST buffers, the
+ * layouts of fmmgpu_fmm_evaluate: q[i*m + v], w[v*nt + i]) it returns
+ *   dcharges[j*m + v] = sum_i w[v][i] G(t_i - s_j)             (the transpose FMM),
+ *   dsources[3j + k]  = sum_v q[j][v] d/ds_jk sum_i w[v][i] G(t_i - s_j),
+ *   dtargets[3i + k]  = sum_v w[v][i] d phi_v / dt_ik,
+ * G = 1/(4 pi r), coincident pairs excluded as in the evaluation.  Two FMM passes, both
+ * recomputed (no expansion is stored between them): the forward one with gradients and
+ * the transpose one (charges w at the targets, evaluated with gradients at the sources),
+ * which for an FMM built with targets == sources (the same pointer) is this FMM again;
+ * otherwise the swapped FMM is built once at the first call and kept.  Needs gradients
+ * on; not offered for multi-cloud batches.  Synchronises. */
+int fmmgpu_fmm_vjp(fmmgpu_fmm* fmm, const double* charges, const double* cotangent, double* dcharges,
+                   double* dsources, double* dtargets);
+
 /* The same with DEVICE buffers on the evaluator's stream; does not synchronise. */
 int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* fmm, const double* charges, double* potential,
                                double* gradient);
