@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-__all__ = ["FmmBuilder", "Fmm", "Output", "FmmError", "lib", "Plan", "direct_sum"]
+__all__ = ["FmmBuilder", "Fmm", "Output", "FmmError", "lib", "Plan", "direct_sum", "helmholtz_direct_sum"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIBPATH = os.path.join(_HERE, "libfmm_b200.so")
@@ -75,6 +75,8 @@ def lib():
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
+            "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
+            "fmmgpu_helmholtz_near": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
             "fmmgpu_op_begin_evaluation": (C.c_int, [vp, dp]),
             "fmmgpu_op_p2m": (C.c_int, [vp, C.c_int]),
             "fmmgpu_op_m2m": (C.c_int, [vp, C.c_int]),
@@ -121,6 +123,19 @@ def direct_sum(sources, charges, targets, gradients=True, device=0):
     phi = np.zeros(len(tgt))
     g = np.zeros((len(tgt), 3)) if gradients else None
     _check(lib().fmmgpu_direct_sum(len(src), _ptr(src), _ptr(q), len(tgt), _ptr(tgt), _ptr(phi), _ptr(g), device))
+    return phi, g
+
+
+def helmholtz_direct_sum(k, sources, charges, targets, gradients=True, device=0):
+    """f64 Helmholtz direct sum on the GPU, e^{ikr}/(4 pi r): phi (nt,) complex, grad (nt, 3) complex."""
+    src = _points(sources)
+    tgt = _points(targets)
+    q = np.ascontiguousarray(charges, dtype=np.complex128).reshape(len(src))
+    phi = np.zeros(len(tgt), dtype=np.complex128)
+    g = np.zeros((len(tgt), 3), dtype=np.complex128) if gradients else None
+    k = complex(k)
+    _check(lib().fmmgpu_helmholtz_direct_sum(k.real, k.imag, len(src), _ptr(src), _ptr(q), len(tgt), _ptr(tgt),
+                                             _ptr(phi), _ptr(g), device))
     return phi, g
 
 
@@ -270,6 +285,17 @@ class Fmm(Plan):
         phi = np.zeros((m, self.ntargets))
         g = np.zeros((m, self.ntargets, 3)) if self.settings.gradients else None
         _check(lib().fmmgpu_fmm_evaluate(self._h, _ptr(q), _ptr(phi), _ptr(g)))
+        return Output(phi, g)
+
+    def helmholtz_near(self, k, charges):
+        """The Helmholtz near field (P2P of every leaf) of e^{ikr}/(4 pi r) on this FMM's
+        plan, complex charges (ns, m): Output with complex potential (m, nt) and gradient."""
+        m = self.settings.vectors
+        q = np.ascontiguousarray(charges, dtype=np.complex128).reshape(self.nsources, m)
+        phi = np.zeros((m, self.ntargets), dtype=np.complex128)
+        g = np.zeros((m, self.ntargets, 3), dtype=np.complex128) if self.settings.gradients else None
+        k = complex(k)
+        _check(lib().fmmgpu_helmholtz_near(self._h, k.real, k.imag, _ptr(q), _ptr(phi), _ptr(g)))
         return Output(phi, g)
 
     def vjp(self, charges, cotangent):

@@ -208,3 +208,120 @@ extern "C" int fmmgpu_direct_sum_noalloc(size_t ns, const double* src, const dou
     e = cudaGetLastError();
     return e == cudaSuccess ? FMMGPU_OK : fail("launch", e);
 }
+
+// ---- Helmholtz: e^{ikr}/(4 pi r), the terms of fmm-ref/src/helmholtz/p2p.rs:315-375
+// (direct_sum: Neumaier per real component, coincident pairs skipped) ----
+namespace {
+
+__global__ void helm_direct_kernel(double kre, double kim, const double* __restrict__ src,
+                                   const double* __restrict__ q, int64_t ns, const double* __restrict__ tgt,
+                                   int64_t nt, int grad, double* __restrict__ phi, double* __restrict__ g) {
+    __shared__ double sx[kTile], sy[kTile], sz[kTile], sqr[kTile], sqi[kTile];
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double x = 0, y = 0, z = 0;
+    if (t < nt) {
+        x = tgt[3 * t];
+        y = tgt[3 * t + 1];
+        z = tgt[3 * t + 2];
+    }
+    Neumaier s[8];
+    for (int64_t b = 0; b < ns; b += kTile) {
+        const int cnt = (int)((ns - b) < kTile ? (ns - b) : kTile);
+        __syncthreads();
+        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+            sx[j] = src[3 * (b + j)];
+            sy[j] = src[3 * (b + j) + 1];
+            sz[j] = src[3 * (b + j) + 2];
+            sqr[j] = q[2 * (b + j)];
+            sqi[j] = q[2 * (b + j) + 1];
+        }
+        __syncthreads();
+        if (t < nt)
+            for (int j = 0; j < cnt; ++j) {
+                if (x == sx[j] && y == sy[j] && z == sz[j]) continue;
+                const double d0 = __dsub_rn(x, sx[j]), d1 = __dsub_rn(y, sy[j]), d2 = __dsub_rn(z, sz[j]);
+                const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+                const double r = sqrt(r2);
+                const double damping = -(kim * r), phase = kre * r;
+                double sn, cs;
+                sincos(phase, &sn, &cs);
+                const double decay = exp(damping);
+                const double er = decay * cs, ei = decay * sn;
+                const double qer = __dsub_rn(__dmul_rn(sqr[j], er), __dmul_rn(sqi[j], ei));
+                const double qei = __dadd_rn(__dmul_rn(sqr[j], ei), __dmul_rn(sqi[j], er));
+                s[0].add(qer / r);
+                s[1].add(qei / r);
+                if (grad) {
+                    const double r3 = __dmul_rn(r2, r);
+                    const double fr = damping - 1.0, fi = phase;
+                    const double fer = __dsub_rn(__dmul_rn(fr, er), __dmul_rn(fi, ei));
+                    const double fei = __dadd_rn(__dmul_rn(fr, ei), __dmul_rn(fi, er));
+                    const double gr = fer / r3, gi = fei / r3;
+                    const double qgr = __dsub_rn(__dmul_rn(sqr[j], gr), __dmul_rn(sqi[j], gi));
+                    const double qgi = __dadd_rn(__dmul_rn(sqr[j], gi), __dmul_rn(sqi[j], gr));
+                    const double dd[3] = {d0, d1, d2};
+                    for (int k = 0; k < 3; ++k) {
+                        s[2 + 2 * k].add(__dmul_rn(qgr, dd[k]));
+                        s[3 + 2 * k].add(__dmul_rn(qgi, dd[k]));
+                    }
+                }
+            }
+    }
+    if (t < nt) {
+        const double f = 4.0 * 3.141592653589793;
+        phi[2 * t] = s[0].value() / f;
+        phi[2 * t + 1] = s[1].value() / f;
+        if (grad)
+            for (int k = 0; k < 6; ++k) g[6 * t + k] = s[2 + k].value() / f;
+    }
+}
+
+}  // namespace
+
+extern "C" int fmmgpu_helmholtz_direct_sum(double kre, double kim, size_t ns, const double* src, const double* q,
+                                           size_t nt, const double* tgt, double* phi, double* grad, int device) {
+    auto fail = [](cudaError_t e) {
+        fmmb::set_last_error(std::string("fmmgpu_helmholtz_direct_sum: ") + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? FMMGPU_DEVICE_MEMORY : FMMGPU_DEVICE_ERROR;
+    };
+    if ((ns && (!src || !q)) || (nt && (!tgt || !phi))) {
+        fmmb::set_last_error("fmmgpu_helmholtz_direct_sum: null buffer");
+        return FMMGPU_INVALID_ARGUMENT;
+    }
+    if (!std::isfinite(kre) || !std::isfinite(kim)) {
+        fmmb::set_last_error("fmmgpu_helmholtz_direct_sum: the wavenumber must be finite");
+        return FMMGPU_INVALID_ARGUMENT;
+    }
+    if (nt == 0) return FMMGPU_OK;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e);
+    double *dsrc = nullptr, *dq = nullptr, *dtgt = nullptr, *dphi = nullptr, *dg = nullptr;
+    auto cleanup = [&] {
+        cudaFree(dsrc);
+        cudaFree(dq);
+        cudaFree(dtgt);
+        cudaFree(dphi);
+        cudaFree(dg);
+    };
+    if ((e = cudaMalloc(&dsrc, 3 * ns * sizeof(double) + 8)) != cudaSuccess ||
+        (e = cudaMalloc(&dq, 2 * ns * sizeof(double) + 8)) != cudaSuccess ||
+        (e = cudaMalloc(&dtgt, 3 * nt * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&dphi, 2 * nt * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&dg, 6 * nt * sizeof(double))) != cudaSuccess) {
+        cleanup();
+        return fail(e);
+    }
+    cudaMemcpy(dsrc, src, 3 * ns * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(dq, q, 2 * ns * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(dtgt, tgt, 3 * nt * sizeof(double), cudaMemcpyHostToDevice);
+    helm_direct_kernel<<<(unsigned)((nt + 127) / 128), 128>>>(kre, kim, dsrc, dq, (int64_t)ns, dtgt, (int64_t)nt,
+                                                            grad != nullptr, dphi, dg);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        cudaMemcpy(phi, dphi, 2 * nt * sizeof(double), cudaMemcpyDeviceToHost);
+        if (grad) cudaMemcpy(grad, dg, 6 * nt * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    cleanup();
+    return e == cudaSuccess ? FMMGPU_OK : fail(e);
+}

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,7 @@
 #include "../../include/fmm_b200.h"
 #include "kernels.cuh"
 #include "m2l_tc.cuh"
+#include "helmholtz.cuh"
 #include "p2p_x2.cuh"
 #include "plan.hpp"
 
@@ -142,6 +144,7 @@ struct EvaluatorBase {
     virtual void op_begin(const double* d_charges) = 0;
     virtual void op_level(int kind, int level) = 0;
     virtual void op_output(double* d_phi, double* d_grad) = 0;
+    virtual void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
 };
 
 template <int P, typename T>
@@ -772,6 +775,32 @@ struct Evaluator final : EvaluatorBase {
         }
     }
 
+    // ---- the Helmholtz near field (all leaves' P2P level calls) ----
+    DevBuf hq, hq64;
+    void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) override {
+        launches = 0;
+        const int64_t ns = dp.nsrc;
+        if (!hq.ptr) {
+            hq.alloc(sizeof(Cplx<T>) * (size_t)m * (ns + 1));
+            if (kMixed) hq64.alloc(sizeof(double2) * (size_t)m * (ns + 1));
+        }
+        if (ns > 0)
+            helm_charge_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
+                d_q, src_perm.as<int64_t>(), ns, m, hq.as<Cplx<T>>(), kMixed ? hq64.as<double2>() : nullptr);
+        if (items.count) {
+            const unsigned g = (unsigned)((items.count + kHelmWarps - 1) / kHelmWarps);
+            if (gradients)
+                helm_p2p_kernel<T, true, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
+                    dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
+                    hq64.as<double2>(), d_phi, d_grad);
+            else
+                helm_p2p_kernel<T, false, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
+                    dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
+                    hq64.as<double2>(), d_phi, nullptr);
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+
     // ---- level calls (the FmmOperator trait, fmm-plan/src/operator.rs:434-492) ----
     void op_begin(const double* d_charges) override {
         launches = 0;
@@ -1265,6 +1294,31 @@ int fmmgpu_fmm_vjp(fmmgpu_fmm* f, const double* charges, const double* cotangent
         CUDA_TRY(cudaStreamSynchronize(s));
         if (f->eval->device_status() || T->eval->device_status())
             throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    });
+}
+
+int fmmgpu_helmholtz_near(fmmgpu_fmm* f, double k_re, double k_im, const double* charges, double* potential,
+                          double* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        if (!std::isfinite(k_re) || !std::isfinite(k_im))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "the wavenumber must be finite");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors;
+        const size_t ns = f->plan.src_perm.size(), nt = f->plan.tgt_perm.size();
+        DevBuf q, phi, g;
+        q.alloc(sizeof(double) * 2 * m * (ns + 1));
+        phi.alloc(sizeof(double) * 2 * m * (nt + 1));
+        if (f->settings.gradients) g.alloc(sizeof(double) * 6 * m * (nt + 1));
+        CUDA_TRY(cudaMemcpyAsync(q.ptr, charges, sizeof(double) * 2 * m * ns, cudaMemcpyHostToDevice, f->stream));
+        f->eval->helmholtz_near(k_re, k_im, q.as<double>(), phi.as<double>(),
+                                f->settings.gradients ? g.as<double>() : nullptr);
+        CUDA_TRY(cudaMemcpyAsync(potential, phi.ptr, sizeof(double) * 2 * m * nt, cudaMemcpyDeviceToHost, f->stream));
+        if (f->settings.gradients)
+            CUDA_TRY(cudaMemcpyAsync(gradient, g.ptr, sizeof(double) * 6 * m * nt, cudaMemcpyDeviceToHost, f->stream));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
     });
 }
 

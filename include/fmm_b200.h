@@ -226,6 +226,27 @@ int fmmgpu_op_read_output(fmmgpu_fmm* fmm, double* potential, double* gradient);
 int fmmgpu_direct_sum(size_t nsources, const double* sources, const double* charges, size_t ntargets,
                       const double* targets, double* potential, double* gradient, int device);
 
+/* ---- Helmholtz, e^{ikr}/(4 pi r) (fmm-ref/src/helmholtz/p2p.rs; CONVENTIONS 3.15) ----
+ * Complex values are (re, im) pairs of doubles; a complex gradient is (re x, im x, re y,
+ * im y, re z, im z).  k = k_re + i k_im, finite.
+ *
+ * The f64 direct sum on the GPU (the reference's helmholtz::p2p::direct_sum: Neumaier per
+ * real component, exactly coincident pairs skipped), with 1/(4 pi): charges[ns] complex,
+ * potential[nt] and gradient[nt][3] complex (gradient may be NULL).  Host buffers. */
+int fmmgpu_helmholtz_direct_sum(double k_re, double k_im, size_t nsources, const double* sources,
+                                const double* charges, size_t ntargets, const double* targets, double* potential,
+                                double* gradient, int device);
+
+/* The Helmholtz near field of an FMM's plan: the P2P level calls of every level
+ * (fmm-exec/src/helmholtz/operator.rs:2571-2615) on the near rows of the tree the build
+ * made, in leaf-scaled coordinates with k_l = k r_l, in the handle's precision (f64, or
+ * complex64 with the mixed form's f64 near-singular pairs).  charges[i*m + v] complex
+ * (caller order), potential[v*nt + i] and gradient[(v*nt + i)*3 + k] complex (caller
+ * order; the gradient when the FMM was built with gradients), with 1/(4 pi).  Host
+ * buffers; synchronises.  The Helmholtz far field is not offered. */
+int fmmgpu_helmholtz_near(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges, double* potential,
+                          double* gradient);
+
 /* The same direct sum on DEVICE buffers, allocating nothing.  No counterpart in the
  * reference (its direct_sum, fmm-ref/src/p2p.rs:147-186, is host code); the results are
  * bit-identical to fmmgpu_direct_sum's.

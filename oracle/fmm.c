@@ -128,58 +128,55 @@ static int cmp_pair(const void *a, const void *b) {
     return x[0] < y[0] ? -1 : x[0] > y[0] ? 1 : (x[1] < y[1] ? -1 : x[1] > y[1]);
 }
 
-int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
-            int p, int max_keys, int gradients, int threads, double *phi_out, double *grad_out) {
-    return orc_fmm_kinds(ns, src, q, m, nt, tgt, p, max_keys, gradients, threads, 3, phi_out, grad_out);
-}
-
-int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
-                  int p, int max_keys, int gradients, int threads, int kinds, double *phi_out,
-                  double *grad_out) {
-#ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#else
-    (void)threads;
-#endif
-    int nc = (p + 1) * (p + 1);
-    orc_tree *tree = orc_tree_build(ns, src, nt, tgt, DEEPEST, max_keys);
+/* The plan shared by the Laplace FMM and the Helmholtz near field: the octree (boxes
+ * level-major), the leaves, the points in leaf order and their leaf-scaled coordinates. */
+typedef struct {
     boxes_t B;
-    memset(&B, 0, sizeof(B));
-    B.nlevels = orc_tree_nlevels(tree);
-    B.nboxes = orc_tree_nboxes(tree);
-    B.key = (uint64_t *)malloc(B.nboxes * sizeof(uint64_t));
-    B.leaf = (uint8_t *)malloc(B.nboxes);
-    orc_tree_boxes(tree, B.key, B.leaf);
     double lower[3], side;
-    orc_tree_domain(tree, lower, &side);
+    size_t nleaves;
+    long *leaf_of_box;
+    size_t *leaf_box, *s_off, *t_off, *s_perm, *t_perm;
+    double *us, *ut;
+} plan_t;
+
+static void plan_setup(plan_t *P, size_t ns, const double *src, size_t nt, const double *tgt, int max_keys) {
+    memset(P, 0, sizeof(*P));
+    boxes_t *Bp = &P->B;
+    orc_tree *tree = orc_tree_build(ns, src, nt, tgt, DEEPEST, max_keys);
+    Bp->nlevels = orc_tree_nlevels(tree);
+    Bp->nboxes = orc_tree_nboxes(tree);
+    Bp->key = (uint64_t *)malloc(Bp->nboxes * sizeof(uint64_t));
+    Bp->leaf = (uint8_t *)malloc(Bp->nboxes);
+    orc_tree_boxes(tree, Bp->key, Bp->leaf);
+    orc_tree_domain(tree, P->lower, &P->side);
     double box6[6];
     { double lw[3], sd; orc_domain(ns, src, nt, tgt, lw, &sd, box6); }
     orc_tree_free(tree);
-    B.level = (int *)malloc(B.nboxes * sizeof(int));
-    B.idx = malloc(B.nboxes * sizeof(*B.idx));
-    B.level_start = (size_t *)calloc(B.nlevels + 1, sizeof(size_t));
-    for (size_t b = 0; b < B.nboxes; ++b) {
-        orc_key_decode(B.key[b], &B.level[b], B.idx[b]);
-        B.level_start[B.level[b] + 1] = b + 1;
+    Bp->level = (int *)malloc(Bp->nboxes * sizeof(int));
+    Bp->idx = malloc(Bp->nboxes * sizeof(*Bp->idx));
+    Bp->level_start = (size_t *)calloc(Bp->nlevels + 1, sizeof(size_t));
+    for (size_t b = 0; b < Bp->nboxes; ++b) {
+        orc_key_decode(Bp->key[b], &Bp->level[b], Bp->idx[b]);
+        Bp->level_start[Bp->level[b] + 1] = b + 1;
     }
-    for (int l = 1; l <= B.nlevels; ++l)
-        if (B.level_start[l] < B.level_start[l - 1]) B.level_start[l] = B.level_start[l - 1];
-    B.sorted = (uint64_t *)malloc(B.nboxes * sizeof(uint64_t));
-    B.sorted_box = (size_t *)malloc(B.nboxes * sizeof(size_t));
+    for (int l = 1; l <= Bp->nlevels; ++l)
+        if (Bp->level_start[l] < Bp->level_start[l - 1]) Bp->level_start[l] = Bp->level_start[l - 1];
+    Bp->sorted = (uint64_t *)malloc(Bp->nboxes * sizeof(uint64_t));
+    Bp->sorted_box = (size_t *)malloc(Bp->nboxes * sizeof(size_t));
     {
-        size_t *pr = (size_t *)malloc(2 * B.nboxes * sizeof(size_t));
-        for (size_t b = 0; b < B.nboxes; ++b) { pr[2 * b] = (size_t)B.key[b]; pr[2 * b + 1] = b; }
-        qsort(pr, B.nboxes, 2 * sizeof(size_t), cmp_pair);
-        for (size_t i = 0; i < B.nboxes; ++i) { B.sorted[i] = pr[2 * i]; B.sorted_box[i] = pr[2 * i + 1]; }
+        size_t *pr = (size_t *)malloc(2 * Bp->nboxes * sizeof(size_t));
+        for (size_t b = 0; b < Bp->nboxes; ++b) { pr[2 * b] = (size_t)Bp->key[b]; pr[2 * b + 1] = b; }
+        qsort(pr, Bp->nboxes, 2 * sizeof(size_t), cmp_pair);
+        for (size_t i = 0; i < Bp->nboxes; ++i) { Bp->sorted[i] = pr[2 * i]; Bp->sorted_box[i] = pr[2 * i + 1]; }
         free(pr);
     }
     /* leaves in level-major order (the leaf numbering); box -> leaf */
     size_t nleaves = 0;
-    long *leaf_of_box = (long *)malloc(B.nboxes * sizeof(long));
-    for (size_t b = 0; b < B.nboxes; ++b) leaf_of_box[b] = B.leaf[b] ? (long)nleaves++ : -1;
-    size_t *leaf_box = (size_t *)malloc(nleaves * sizeof(size_t));
-    for (size_t b = 0; b < B.nboxes; ++b)
-        if (B.leaf[b]) leaf_box[leaf_of_box[b]] = b;
+    long *leaf_of_box = (long *)malloc(Bp->nboxes * sizeof(long));
+    for (size_t b = 0; b < Bp->nboxes; ++b) leaf_of_box[b] = Bp->leaf[b] ? (long)nleaves++ : -1;
+    size_t *leaf_box = (size_t *)malloc((nleaves + 1) * sizeof(size_t));
+    for (size_t b = 0; b < Bp->nboxes; ++b)
+        if (Bp->leaf[b]) leaf_box[leaf_of_box[b]] = b;
 
     /* points -> leaves, caller order within each leaf */
     size_t *s_leaf = (size_t *)malloc((ns + 1) * sizeof(size_t));
@@ -191,13 +188,13 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
         for (size_t i = 0; i < n; ++i) {
             uint64_t fine = orc_point_key(x + 3 * i, box6, DEEPEST);
             long found = -1;
-            for (int l = B.nlevels - 1; l >= 0 && found < 0; --l) {
+            for (int l = Bp->nlevels - 1; l >= 0 && found < 0; --l) {
                 int fl;
                 uint32_t fi[3];
                 orc_key_decode(fine, &fl, fi);
                 uint32_t ai[3] = {fi[0] >> (DEEPEST - l), fi[1] >> (DEEPEST - l), fi[2] >> (DEEPEST - l)};
-                long b = find(&B, orc_key_from_index(ai, l));
-                if (b >= 0 && B.leaf[b]) found = leaf_of_box[b];
+                long b = find(Bp, orc_key_from_index(ai, l));
+                if (b >= 0 && Bp->leaf[b]) found = leaf_of_box[b];
             }
             out[i] = (size_t)found;
         }
@@ -216,24 +213,103 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
         for (size_t i = 0; i < nt; ++i) t_perm[t_off[t_leaf[i]] + fill[t_leaf[i]]++] = i;
         free(fill);
     }
-    /* leaf-scaled coordinates and charges in leaf order */
+    free(s_leaf);
+    free(t_leaf);
+    /* leaf-scaled coordinates in leaf order */
     double *us = (double *)malloc((3 * ns + 1) * sizeof(double));
-    double *qs = (double *)malloc((ns * m + 1) * sizeof(double));
     double *ut = (double *)malloc((3 * nt + 1) * sizeof(double));
     for (size_t j = 0; j < nleaves; ++j) {
         size_t b = leaf_box[j];
         for (size_t a = s_off[j]; a < s_off[j + 1]; ++a) {
             size_t i = s_perm[a];
             for (int k = 0; k < 3; ++k)
-                us[3 * a + k] = orc_leaf_coordinate(src[3 * i + k], lower[k], side, B.level[b], B.idx[b][k]);
-            for (int v = 0; v < m; ++v) qs[a * m + v] = q[i * m + v];
+                us[3 * a + k] = orc_leaf_coordinate(src[3 * i + k], P->lower[k], P->side, Bp->level[b], Bp->idx[b][k]);
         }
         for (size_t a = t_off[j]; a < t_off[j + 1]; ++a) {
             size_t i = t_perm[a];
             for (int k = 0; k < 3; ++k)
-                ut[3 * a + k] = orc_leaf_coordinate(tgt[3 * i + k], lower[k], side, B.level[b], B.idx[b][k]);
+                ut[3 * a + k] = orc_leaf_coordinate(tgt[3 * i + k], P->lower[k], P->side, Bp->level[b], Bp->idx[b][k]);
         }
     }
+    P->nleaves = nleaves;
+    P->leaf_of_box = leaf_of_box;
+    P->leaf_box = leaf_box;
+    P->s_off = s_off;
+    P->t_off = t_off;
+    P->s_perm = s_perm;
+    P->t_perm = t_perm;
+    P->us = us;
+    P->ut = ut;
+}
+
+static void plan_free(plan_t *P) {
+    free(P->B.key); free(P->B.leaf); free(P->B.level); free(P->B.idx); free(P->B.level_start);
+    free(P->B.sorted); free(P->B.sorted_box);
+    free(P->leaf_of_box); free(P->leaf_box); free(P->s_off); free(P->t_off); free(P->s_perm); free(P->t_perm);
+    free(P->us); free(P->ut);
+}
+
+/* The W list (boxes, by index) and the near list (leaves: U and the leaf itself, by leaf
+ * index) of leaf box b (fmm-plan/src/interaction_manager.rs:15-27). */
+static void leaf_lists(const plan_t *P, size_t b, vecz *wl, vecz *near) {
+    const boxes_t *Bp = &P->B;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                if (!dx && !dy && !dz) continue;
+                long N = neighbour(Bp, b, dx, dy, dz);
+                if (N == -2) continue;
+                if (N >= 0 && !Bp->leaf[N]) {
+                    for (int co = 0; co < 8; ++co) {
+                        long c = child_box(Bp, (size_t)N, co);
+                        if (adjacent_boxes(Bp, (size_t)c, b)) zpush(near, (size_t)P->leaf_of_box[c]);
+                        else zpush(wl, (size_t)c);
+                    }
+                } else if (N >= 0) {
+                    zpush(near, (size_t)P->leaf_of_box[N]);
+                } else {
+                    /* the neighbour cell is not a box: its parent is a coarser leaf */
+                    int l1 = Bp->level[b];
+                    uint32_t ni[3] = {(uint32_t)((long)Bp->idx[b][0] + dx) >> 1,
+                                      (uint32_t)((long)Bp->idx[b][1] + dy) >> 1,
+                                      (uint32_t)((long)Bp->idx[b][2] + dz) >> 1};
+                    long C = find(Bp, orc_key_from_index(ni, l1 - 1));
+                    if (C >= 0 && Bp->leaf[C]) zpush(near, (size_t)P->leaf_of_box[C]);
+                }
+            }
+    zpush(near, (size_t)P->leaf_of_box[b]);
+    sort_unique(wl);
+    sort_unique(near);
+}
+
+int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+            int p, int max_keys, int gradients, int threads, double *phi_out, double *grad_out) {
+    return orc_fmm_kinds(ns, src, q, m, nt, tgt, p, max_keys, gradients, threads, 3, phi_out, grad_out);
+}
+
+int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+                  int p, int max_keys, int gradients, int threads, int kinds, double *phi_out,
+                  double *grad_out) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+    int nc = (p + 1) * (p + 1);
+    plan_t PL;
+    plan_setup(&PL, ns, src, nt, tgt, max_keys);
+    boxes_t B = PL.B;
+    const double *lower = PL.lower;
+    const double side = PL.side;
+    (void)lower;
+    size_t nleaves = PL.nleaves;
+    long *leaf_of_box = PL.leaf_of_box;
+    size_t *leaf_box = PL.leaf_box, *s_off = PL.s_off, *t_off = PL.t_off, *t_perm = PL.t_perm, *s_perm = PL.s_perm;
+    double *us = PL.us, *ut = PL.ut;
+    /* charges in leaf order */
+    double *qs = (double *)malloc((ns * m + 1) * sizeof(double));
+    for (size_t a = 0; a < ns; ++a)
+        for (int v = 0; v < m; ++v) qs[a * m + v] = q[s_perm[a] * m + v];
 
     /* tables */
     double *m2l_t = (double *)malloc((size_t)316 * nc * nc * sizeof(double));
@@ -338,33 +414,7 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
             const double *u = ut + 3 * t_off[j];
             if (kinds & 2) orc_l2p(p, zero3, 1.0, Lc + (size_t)b * m * nc, m, n, u, cphi, cg);
             vecz wl = {0, 0, 0}, near = {0, 0, 0};
-            for (int dx = -1; dx <= 1; ++dx)
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dz = -1; dz <= 1; ++dz) {
-                        if (!dx && !dy && !dz) continue;
-                        long N = neighbour(&B, (size_t)b, dx, dy, dz);
-                        if (N == -2) continue;
-                        if (N >= 0 && !B.leaf[N]) {
-                            for (int co = 0; co < 8; ++co) {
-                                long c = child_box(&B, (size_t)N, co);
-                                if (adjacent_boxes(&B, (size_t)c, (size_t)b)) zpush(&near, (size_t)leaf_of_box[c]);
-                                else zpush(&wl, (size_t)c);
-                            }
-                        } else if (N >= 0) {
-                            zpush(&near, (size_t)leaf_of_box[N]);
-                        } else {
-                            /* the neighbour cell is not a box: its parent is a coarser leaf */
-                            int l1 = B.level[b];
-                            uint32_t ni[3] = {(uint32_t)((long)B.idx[b][0] + dx) >> 1,
-                                              (uint32_t)((long)B.idx[b][1] + dy) >> 1,
-                                              (uint32_t)((long)B.idx[b][2] + dz) >> 1};
-                            long C = find(&B, orc_key_from_index(ni, l1 - 1));
-                            if (C >= 0 && B.leaf[C]) zpush(&near, (size_t)leaf_of_box[C]);
-                        }
-                    }
-            zpush(&near, j);
-            sort_unique(&wl);
-            sort_unique(&near);
+            leaf_lists(&PL, (size_t)b, &wl, &near);
             for (size_t e = 0; e < ((kinds & 2) ? wl.len : 0); ++e) {
                 size_t s = wl.data[e];
                 double c[3], r;
@@ -423,10 +473,85 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
 
     free(M); free(Lc); free(phi); free(grad);
     free(m2l_t); free(m2m_t); free(l2l_t);
-    free(us); free(qs); free(ut);
-    free(s_leaf); free(t_leaf); free(s_off); free(t_off); free(s_perm); free(t_perm);
-    free(leaf_of_box); free(leaf_box);
-    free(B.key); free(B.leaf); free(B.level); free(B.idx); free(B.level_start);
-    free(B.sorted); free(B.sorted_box);
+    free(qs);
+    plan_free(&PL);
+    return 0;
+}
+
+/* The Helmholtz near field on the plan (see helmholtz.c for the term): charges q[i][v]
+ * complex (2 m doubles per source), outputs phi[v][nt] and grad[v][nt][3] complex, caller
+ * order, with 1/(4 pi r_t) (and r_t again for the gradient). */
+int orc_helmholtz_near(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+                       int max_keys, double kre, double kim, int gradients, int threads, double *phi_out,
+                       double *grad_out) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+    plan_t PL;
+    plan_setup(&PL, ns, src, nt, tgt, max_keys);
+    const boxes_t *Bp = &PL.B;
+    const double r0 = ldexp(PL.side, -1);
+    const double kr0[2] = {kre * r0, kim * r0};
+    int L = Bp->nlevels - 1;
+    for (int l = 0; l <= L; ++l) {
+        const double kl[2] = {ldexp(kr0[0], -l), ldexp(kr0[1], -l)};
+#pragma omp parallel for schedule(dynamic, 2)
+        for (long b = (long)Bp->level_start[l]; b < (long)Bp->level_start[l + 1]; ++b) {
+            if (!Bp->leaf[b]) continue;
+            size_t j = (size_t)PL.leaf_of_box[b];
+            size_t n = PL.t_off[j + 1] - PL.t_off[j];
+            if (n == 0) continue;
+            double *cphi = (double *)calloc(2 * m * n, sizeof(double));
+            double *cg = gradients ? (double *)calloc(6 * m * n, sizeof(double)) : NULL;
+            const double *u = PL.ut + 3 * PL.t_off[j];
+            vecz wl = {0, 0, 0}, near = {0, 0, 0};
+            leaf_lists(&PL, (size_t)b, &wl, &near);
+            double *ys = NULL, *qv = NULL;
+            size_t cap = 0;
+            for (size_t e = 0; e < near.len; ++e) {
+                size_t sj = near.data[e], s = PL.leaf_box[sj];
+                size_t nsrc = PL.s_off[sj + 1] - PL.s_off[sj];
+                if (nsrc > cap) {
+                    cap = nsrc;
+                    ys = (double *)realloc(ys, 3 * cap * sizeof(double));
+                    qv = (double *)realloc(qv, 2 * cap * sizeof(double));
+                }
+                double c[3] = {0.0, 0.0, 0.0}, r = 1.0;
+                if (sj != j) rel_frame(Bp, s, (size_t)b, c, &r);
+                for (size_t a = 0; a < nsrc; ++a)
+                    for (int k = 0; k < 3; ++k) {
+                        double uu = PL.us[3 * (PL.s_off[sj] + a) + k];
+                        ys[3 * a + k] = sj != j ? c[k] + r * uu : uu;
+                    }
+                for (int v = 0; v < m; ++v) {
+                    for (size_t a = 0; a < nsrc; ++a) {
+                        size_t i = PL.s_perm[PL.s_off[sj] + a];
+                        qv[2 * a] = q[2 * (i * m + v)];
+                        qv[2 * a + 1] = q[2 * (i * m + v) + 1];
+                    }
+                    orc_helmholtz_p2p(kl[0], kl[1], nsrc, ys, qv, n, u, cphi + 2 * v * n, cg ? cg + 6 * v * n : NULL);
+                }
+            }
+            free(ys);
+            free(qv);
+            free(wl.data);
+            free(near.data);
+            double rt = ldexp(PL.side, -(l + 1));
+            double ps = 4.0 * M_PI * rt, gs = 4.0 * M_PI * rt * rt;
+            for (int v = 0; v < m; ++v)
+                for (size_t a = 0; a < n; ++a) {
+                    size_t i = PL.t_perm[PL.t_off[j] + a];
+                    for (int c2 = 0; c2 < 2; ++c2) phi_out[2 * (v * nt + i) + c2] = cphi[2 * (v * n + a) + c2] / ps;
+                    if (cg && grad_out)
+                        for (int c2 = 0; c2 < 6; ++c2)
+                            grad_out[6 * (v * nt + i) + c2] = cg[6 * (v * n + a) + c2] / gs;
+                }
+            free(cphi);
+            free(cg);
+        }
+    }
+    plan_free(&PL);
     return 0;
 }

@@ -124,6 +124,18 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
                   const double *tgt, int p, int max_keys, int gradients, int threads, int kinds,
                   double *phi, double *grad);
 
+/* Helmholtz (helmholtz.c): complex values are (re, im) double pairs.  p2p and the
+ * Neumaier direct sum of e^{ikr}/r (no 1/(4 pi)), potential[nt] and gradient[nt][3]
+ * complex, += into the outputs */
+void orc_helmholtz_p2p(double kre, double kim, size_t ns, const double *src, const double *q, size_t nt,
+                       const double *tgt, double *potential, double *gradient);
+void orc_helmholtz_direct_sum(double kre, double kim, size_t ns, const double *src, const double *q, size_t nt,
+                              const double *tgt, double *potential, double *gradient);
+/* the Helmholtz near field on the plan (fmm.c), with 1/(4 pi) */
+int orc_helmholtz_near(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+                       int max_keys, double kre, double kim, int gradients, int threads, double *phi,
+                       double *grad);
+
 /* the oracle's own scaling of one leaf-scaled coordinate (fmm-exec/src/geometry.rs:291) */
 double orc_leaf_coordinate(double x, double lower, double side, int level, uint32_t index);
 

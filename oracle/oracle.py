@@ -63,6 +63,11 @@ def lib():
                                   C.c_int, _dp, C.c_void_p]),
             "orc_fmm_kinds": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
                                         C.c_int, C.c_int, _dp, C.c_void_p]),
+            "orc_helmholtz_p2p": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_helmholtz_direct_sum": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp,
+                                                C.c_void_p]),
+            "orc_helmholtz_near": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_double, C.c_double,
+                                             C.c_int, C.c_int, _dp, C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -147,6 +152,52 @@ def direct_sum(src, q, tgt, gradients=True, threads=True):
     f = lib().orc_direct_sum_omp if threads else lib().orc_direct_sum
     f(len(src), src, q, len(tgt), tgt, phi, _ptr(g))
     return phi, g
+
+
+def _cview(a):
+    return np.ascontiguousarray(a, dtype=np.complex128).view(np.float64)
+
+
+def helmholtz_p2p(k, src, q, tgt, gradients=True):
+    """The reference's Helmholtz p2p (fmm-ref/src/helmholtz/p2p.rs), e^{ikr}/r without
+    1/(4 pi), sources in input order: phi (nt,) complex, grad (nt, 3) complex."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    phi = np.zeros(len(tgt), dtype=np.complex128)
+    g = np.zeros((len(tgt), 3), dtype=np.complex128) if gradients else None
+    k = complex(k)
+    lib().orc_helmholtz_p2p(k.real, k.imag, len(src), src, _cview(q), len(tgt), tgt, phi.view(np.float64),
+                            None if g is None else g.view(np.float64).ctypes.data_as(C.c_void_p))
+    return phi, g
+
+
+def helmholtz_direct_sum(k, src, q, tgt, gradients=True):
+    """The Helmholtz f64 direct sum (Neumaier per real component), without 1/(4 pi)."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    phi = np.zeros(len(tgt), dtype=np.complex128)
+    g = np.zeros((len(tgt), 3), dtype=np.complex128) if gradients else None
+    k = complex(k)
+    lib().orc_helmholtz_direct_sum(k.real, k.imag, len(src), src, _cview(q), len(tgt), tgt, phi.view(np.float64),
+                                   None if g is None else g.view(np.float64).ctypes.data_as(C.c_void_p))
+    return phi, g
+
+
+def helmholtz_near(src, q, tgt, k, max_keys, gradients=True, threads=0):
+    """The Helmholtz near field on the restated plan, with 1/(4 pi): q (N,) or (N, m)
+    complex; phi (m, Nt) complex, grad (m, Nt, 3) complex, caller order."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    q = np.asarray(q, dtype=np.complex128)
+    m = 1 if q.ndim == 1 else q.shape[1]
+    q = np.ascontiguousarray(q.reshape(len(src), m))
+    phi = np.zeros(m * len(tgt), dtype=np.complex128)
+    g = np.zeros(3 * m * len(tgt), dtype=np.complex128) if gradients else None
+    k = complex(k)
+    lib().orc_helmholtz_near(len(src), src, q.view(np.float64), m, len(tgt), tgt, max_keys, k.real, k.imag,
+                             int(gradients), threads, phi.view(np.float64),
+                             None if g is None else g.view(np.float64).ctypes.data_as(C.c_void_p))
+    return phi.reshape(m, len(tgt)), (None if g is None else g.reshape(m, len(tgt), 3))
 
 
 def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0, kinds=3):

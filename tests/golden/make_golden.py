@@ -1,4 +1,5 @@
-"""Generates tests/golden/harmonics.json from the reference's mpmath fixtures.
+"""Generates tests/golden/harmonics.json from the reference's mpmath fixtures, and
+tests/golden/helmholtz_fmm3d.json from its FMM3D Helmholtz fixture (see helmholtz()).
 
 The reference ships 40-digit mpmath values of the real solid harmonics and their
 gradients (fmm-math/fixtures/harmonics_{A,B,C}.json, generator
@@ -47,5 +48,33 @@ def main(ref):
         json.dump(out, f, separators=(",", ":"))
 
 
+def helmholtz(ref):
+    """tests/golden/helmholtz_fmm3d.json: FMM3D v2.1.0's Helmholtz direct sum (h3ddirectcg,
+    with 1/(4 pi)) from fmm-ref/fixtures/helmholtz_fmm3d.json (generator
+    tools/fixtures/gen_helmholtz_fmm3d.py, seed 20261028): every source, target and charge,
+    and for seven of the twelve cases the values at the 40 targets and the first 40
+    sources (the fixture's points are the sources, then the targets)."""
+    with open(os.path.join(ref, "fmm-ref", "fixtures", "helmholtz_fmm3d.json")) as f:
+        d = json.load(f)
+    ns = len(d["sources"])
+    keep = list(range(40)) + list(range(ns, ns + len(d["targets"])))
+    cases = []
+    for i in (0, 1, 3, 5, 7, 9, 11):
+        c = d["cases"][i]
+        cases.append({"label": c["label"], "k": c["k"], "charges": c["charges"], "points": keep,
+                      "potential": [c["potential"][j] for j in keep],
+                      "gradient": [c["gradient"][j] for j in keep]})
+    out = {
+        "source": "fmm-ref/fixtures/helmholtz_fmm3d.json of tbetcke/fmm (FMM3D v2.1.0 h3ddirectcg, "
+        "17 significant digits; e^{ikr}/(4 pi r); gradient [re x, im x, re y, im y, re z, im z])",
+        "sources": d["sources"], "targets": d["targets"], "charges": d["charges"], "cases": cases,
+    }
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "helmholtz_fmm3d.json"), "w") as f:
+        json.dump(out, f, separators=(",", ":"))
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    reference = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(reference)
+    helmholtz(reference)
