@@ -170,7 +170,7 @@ struct Evaluator final : EvaluatorBase {
     DevBuf oct_tile_d, oct_tile_begin, oct_tile_count, oct_pair_e, oct_pair_src, Yo;
     std::vector<int64_t> m2m_tiles, l2l_tiles;  // tile ranges per level (nlevels + 1)
     // M2L batches: pairs of all levels grouped by offset, in tiles
-    DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src;
+    DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src, v_pos;
     int64_t ntiles = 0;
     // the same pairs in per-level tiles, for the level calls
     DevBuf ltile_d, ltile_begin, ltile_count;
@@ -338,7 +338,6 @@ struct Evaluator final : EvaluatorBase {
             tc_ltile_d.upload(lvl.d);
             tc_ltile_begin.upload(lvl.begin);
             tc_ltile_count.upload(lvl.count);
-            tc_pair_e.upload(pe);
             tc_pair_src.upload(ps);
             std::vector<uint32_t> img;
             build_tc_table_images<P>(m2l, img);
@@ -415,6 +414,10 @@ struct Evaluator final : EvaluatorBase {
         ltile_count.upload(lvl.count);
         pair_e.upload(pe);
         pair_src.upload(ps);
+        // the row of each V entry's product in Y: its position in the offset-sorted list
+        std::vector<int64_t> vp(pe.size());
+        for (size_t pos = 0; pos < pe.size(); ++pos) vp[pe[pos]] = (int64_t)pos;
+        v_pos.upload(vp);
     }
 
     void build_parent_lists() {
@@ -570,7 +573,7 @@ struct Evaluator final : EvaluatorBase {
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
-                               &near_phi, &near_g, &box_side};
+                               &near_phi, &near_g, &box_side, &v_pos};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -686,7 +689,7 @@ struct Evaluator final : EvaluatorBase {
                 for (int v = 0; v < m; ++v)
                     m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
                         td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
-                        tc_pair_e.as<int64_t>(), tc_pair_src.as<int32_t>(), m, v, tc_bimg.as<uint32_t>(),
+                        tc_pair_src.as<int32_t>(), m, v, tc_bimg.as<uint32_t>(),
                         reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
             return;
@@ -698,7 +701,7 @@ struct Evaluator final : EvaluatorBase {
         const DevBuf& tn = l < 0 ? tile_count : ltile_count;
         if (nt)
             m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
-                td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, pair_e.as<int64_t>(),
+                td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nullptr,
                 pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
     }
 
@@ -714,7 +717,8 @@ struct Evaluator final : EvaluatorBase {
         const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
         if (b1 > b0)
             local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
-                dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), Lc.as<T>());
+                dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
+                Lc.as<T>());
     }
 
     void p2l_level(int l) {

@@ -307,7 +307,8 @@ __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ pare
 }
 
 // The locals of one level (>= 2), for every box with a target below it:
-//   L = (l >= 3 ? T_o L_parent : 0) + the V row's products in offset-index order,
+//   L = (l >= 3 ? T_o L_parent : 0) + the V row's products in offset-index order
+// (the product of V entry e sits at row vpos[e] of Yv, its place in the M2L tile list),
 // written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X is added after).
 // Block per box, thread per slot; the V loop issues four loads before adding them in order.
 // The evaluation writes L = Yo + sum_V Y (accumulate = 0); the level calls add into L:
@@ -316,7 +317,7 @@ __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ pare
 template <int P, typename T>
 __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l, int with_v,
                                     int accumulate, const T* __restrict__ Yo, const T* __restrict__ Yv,
-                                    T* __restrict__ Lc) {
+                                    const int64_t* __restrict__ vpos, T* __restrict__ Lc) {
     constexpr int NC = nc_of(P), YS = ys_of(P);
     const int64_t b = b0 + blockIdx.x;
     if (b >= b1 || plan.tgt_below[b] == 0) return;
@@ -327,14 +328,14 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
             if (with_l2l) s = accumulate ? s + Yo[(b * m + v) * YS + i] : Yo[(b * m + v) * YS + i];
             int64_t e = e0;
             for (; e + 4 <= e1; e += 4) {
-                const T y0 = __ldcs(Yv + (e * m + v) * YS + i), y1 = __ldcs(Yv + ((e + 1) * m + v) * YS + i);
-                const T y2 = __ldcs(Yv + ((e + 2) * m + v) * YS + i), y3 = __ldcs(Yv + ((e + 3) * m + v) * YS + i);
+                const T y0 = __ldcs(Yv + (vpos[e] * m + v) * YS + i), y1 = __ldcs(Yv + (vpos[e + 1] * m + v) * YS + i);
+                const T y2 = __ldcs(Yv + (vpos[e + 2] * m + v) * YS + i), y3 = __ldcs(Yv + (vpos[e + 3] * m + v) * YS + i);
                 s += y0;
                 s += y1;
                 s += y2;
                 s += y3;
             }
-            for (; e < e1; ++e) s += __ldcs(Yv + (e * m + v) * YS + i);
+            for (; e < e1; ++e) s += __ldcs(Yv + (vpos[e] * m + v) * YS + i);
             Lc[(b * m + v) * NC + i] = s;
         }
 }
@@ -401,7 +402,7 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
         for (int i = 0; i < 4; ++i) {
             int pr = ty * 4 + i;
             if (pr >= cnt) continue;
-            T* y = Y + (pair_e[p0 + pr] * m + v) * ys_of(P);
+            T* y = Y + ((pair_e ? pair_e[p0 + pr] : p0 + pr) * m + v) * ys_of(P);
 #pragma unroll
             for (int j = 0; j < JN; ++j) {
                 int n = tx + 16 * j;

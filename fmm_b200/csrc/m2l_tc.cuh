@@ -96,6 +96,15 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint6
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
+// the load alone: the caller waits (tcgen05.wait::ld) before reading v
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, float (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]), "=f"(v[8]),
+          "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+        : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     uint32_t r[16];
     asm volatile(
@@ -162,8 +171,9 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 //     (acc_empty, released by the epilogue of tile k-2), issues the 3 x KSTEPS MMAs
 //     and commits to empty[k&1] and acc_full[k&1];
 //   warps 0-7 (epilogue): wait acc_full[k&1], read the accumulator with tcgen05.ld
-//     and stream the products Y past L2 in whole 128-byte lines (rows padded to
-//     ys_of(P) slots), then release acc_empty[k&1].
+//     and stream the products past L2 into Y at the pairs' positions in the tile list
+//     (a tile's rows consecutive, each padded to ys_of(P) slots: whole 128-byte lines),
+//     then release acc_empty[k&1].
 // Every wait is bounded; a role that gives up sets the shared abort flag (which ends
 // the other roles' waits) and *error, and the CTA frees its tensor memory and returns.
 // One vector per launch.
@@ -217,7 +227,7 @@ template <int P>
 __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
                                                                   const int64_t* __restrict__ tile_begin,
                                                                   const int32_t* __restrict__ tile_count,
-                                                                  int64_t ntiles, const int64_t* __restrict__ pair_e,
+                                                                  int64_t ntiles,
                                                                   const int32_t* __restrict__ pair_src, int m, int v,
                                                                   const uint32_t* __restrict__ timg,
                                                                   const float* __restrict__ M, float* __restrict__ Y,
@@ -428,30 +438,31 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             const int st = (int)(k & 1);
             const int64_t p0 = tile_begin[it];
             const int cnt = tile_count[it];
-            // the rows' V positions of this warp's 64 columns: lane j holds columns
-            // 64 g + j and 64 g + 32 + j
-            const int c_a = 64 * g + lane, c_b = c_a + 32;
-            const int64_t e_a = c_a < cnt ? pair_e[p0 + c_a] : 0;
-            const int64_t e_b = c_b < cnt ? pair_e[p0 + c_b] : 0;
             if (!warp_wait(&bar_accf[st], (uint32_t)((k >> 1) & 1))) {
                 if (lane == 0) give_up();
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (32 * q < ys_of(P)) {
+                // products at their pair positions p0 + c (a tile's rows are consecutive), whole
+                // 128-byte lines (rows >= NC of the table are zero), two TMEM loads per wait
 #pragma unroll
-                for (int h = 0; h < 4; ++h) {
+                for (int h = 0; h < 4; h += 2) {
                     const int c0 = 64 * g + 16 * h;
                     if (c0 >= cnt) break;
-                    float vals[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * S::NT + c0), vals);
+                    float v0[16], v1[16];
+                    const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * S::NT + c0);
+                    tmem_ld16_nowait(ta, v0);
+                    tmem_ld16_nowait(ta + 16u, v1);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    float* yb = Y + ((p0 + c0) * m + v) * ys_of(P) + n;
+                    const int64_t row = (int64_t)m * ys_of(P);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const int c = 16 * h + i;  // column within the warp's half
-                        const int64_t e = __shfl_sync(0xffffffffu, c < 32 ? e_a : e_b, c & 31);
-                        // whole 128-byte lines (rows >= NC of the table are zero), streamed
-                        if (c0 + i < cnt) __stcs(Y + (e * m + v) * ys_of(P) + n, vals[i]);
-                    }
+                    for (int i = 0; i < 16; ++i)
+                        if (c0 + i < cnt) __stcs(yb + i * row, v0[i]);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        if (c0 + 16 + i < cnt) __stcs(yb + (16 + i) * row, v1[i]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
