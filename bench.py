@@ -85,6 +85,42 @@ def sample_indices(n, count, seed=SEED + 2):
     return order[:count].copy()
 
 
+# the batched workload: 256 clouds, N_i log-uniform in [1e4, 5e5], geometry uniform from
+# {unit cube, unit sphere surface, Plummer sphere a = 0.1 clipped at r = 5 (resampled beyond)},
+# 16 charge vectors U[-1, 1) per cloud, p = 6, 64 points per leaf, potentials
+BATCH_CLOUDS = 256
+BATCH_VECTORS = 16
+BATCH_P = 6
+BATCH_LEAF = 64
+
+
+def batched_problem(seed=SEED + 7, clouds=BATCH_CLOUDS):
+    """The batched workload's clouds and charges (numpy PCG64, seeded): a list of (N_i, 3)
+    point arrays and the (sum N_i, 16) charges in cloud order."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1e4), np.log(5e5), clouds)).astype(np.int64)
+    kinds = rng.integers(0, 3, clouds)
+    out = []
+    for c in range(clouds):
+        n = int(sizes[c])
+        if kinds[c] == 0:
+            x = rng.uniform(0.0, 1.0, (n, 3))
+        elif kinds[c] == 1:
+            g = rng.normal(size=(n, 3))
+            x = g / np.linalg.norm(g, axis=1, keepdims=True)
+        else:  # Plummer: r = a / sqrt(U^(-2/3) - 1), isotropic, resampled beyond r = 5
+            r = np.empty(0)
+            while len(r) < n:
+                u = 1.0 - rng.uniform(size=2 * n)
+                rr = 0.1 / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+                r = np.concatenate([r, rr[rr <= 5.0]])
+            g = rng.normal(size=(n, 3))
+            x = g / np.linalg.norm(g, axis=1, keepdims=True) * r[:n, None]
+        out.append(np.ascontiguousarray(x))
+    q = rng.uniform(-1.0, 1.0, (int(sizes.sum()), BATCH_VECTORS))
+    return out, np.ascontiguousarray(q), kinds
+
+
 # ------------------------------------------------------------------------------------
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
@@ -343,12 +379,83 @@ def run_ours(args):
     }
     line["gpu_launches"] = launches_per_step * args.steps
     line["gpu_launches_per_step"] = launches_per_step
+    if not args.no_batched and world == 1:
+        try:
+            line["batched"] = run_batched(F, torch, dev, flush)
+        except Exception as e:  # reported, never fatal to the headline line
+            line["batched"] = {"error": f"{type(e).__name__}: {str(e)[:200]}"}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def run_batched(F, torch, dev, flush, steps=3, warmup=1):
+    """The batched workload (256 clouds, 16 vectors, p = 6, 64 per leaf, potentials) as one
+    forest: mixed and plain f64, device-timed like the headline, with the error of the
+    first vector at sampled targets of the first clouds against the GPU f64 direct sum."""
+    clouds, q, kinds = batched_problem()
+    n = int(sum(len(c) for c in clouds))
+    m = BATCH_VECTORS
+    log(f"batched: {len(clouds)} clouds, {n} points, {m} vectors")
+    dq = torch.from_numpy(q).to(dev)
+    dphi = torch.empty(m * n, dtype=torch.float64, device=dev)
+    res = {"workload": f"{len(clouds)} clouds, N_i log-uniform in [1e4, 5e5] (cube / sphere / Plummer a=0.1 "
+                       f"clipped at r=5), {m} vectors U[-1,1), p={BATCH_P}, {BATCH_LEAF} per leaf, potentials",
+           "n_points": n, "vectors": m, "clouds_by_geometry": [int((kinds == i).sum()) for i in range(3)],
+           "data": "synthetic (numpy PCG64, seeded)"}
+
+    def timed(f):
+        stream = torch.cuda.ExternalStream(f.stream)
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                f.evaluate_device(dq.data_ptr(), dphi.data_ptr(), None)
+            f.synchronize()
+            total = 0.0
+            for _ in range(steps):
+                flush.zero_()
+                s = torch.cuda.Event(enable_timing=True)
+                e = torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                f.evaluate_device(dq.data_ptr(), dphi.data_ptr(), None)
+                e.record(stream)
+                e.synchronize()
+                total += s.elapsed_time(e)
+            f.synchronize()
+        return total / steps
+
+    for precision in ("mixed", "f64"):
+        t0 = time.perf_counter()
+        f = (F.FmmBuilder(BATCH_P).vectors(m).max_points_per_leaf(BATCH_LEAF).precision(precision)
+             .build_batch(clouds))
+        build_s = time.perf_counter() - t0
+        info = f.info()
+        ms = timed(f)
+        log(f"batched {precision}: build {build_s:.1f} s, {ms:.2f} ms/step")
+        if precision == "mixed":
+            res.update({"ms_per_step": round(ms, 3), "value": round(n / (ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
+                        "point_vectors_per_s": round(n * m / (ms * 1e-3) / 1e6, 1), "build_s": round(build_s, 2),
+                        "launches_per_step": f.info()["launches"],
+                        "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs")}})
+            # error of vector 0 at 250 sampled targets in each of the first 4 clouds
+            phi = dphi.view(m, n)[0].cpu().numpy()
+            errs, off = [], 0
+            for c in range(4):
+                x = clouds[c]
+                pick = np.linspace(0, len(x) - 1, 250).astype(np.int64)
+                ex, _ = F.direct_sum(x, q[off:off + len(x), 0], x[pick], gradients=False)
+                errs.append(float(np.linalg.norm(phi[off + pick] - ex) / np.linalg.norm(ex)))
+                off += len(x)
+            res["phi_rel_l2_first_clouds"] = errs
+        else:
+            res["plain_f64"] = {"ms_per_step": round(ms, 3), "value": round(n / (ms * 1e-3) / 1e6, 3)}
+        f.close()
+    res["mixed_over_plain"] = round(res["plain_f64"]["ms_per_step"] / res["ms_per_step"], 3)
+    del dq, dphi
+    torch.cuda.empty_cache()
+    return res
 
 
 def cpu_baseline(args, n_sample=None):
@@ -401,6 +508,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--cpu-n", type=int, default=400_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (256 clouds) measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

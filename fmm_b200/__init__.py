@@ -33,14 +33,16 @@ class FmmError(RuntimeError):
 
 class Settings(C.Structure):
     _fields_ = [("p", C.c_int), ("precision", C.c_int), ("gradients", C.c_int), ("vectors", C.c_int),
-                ("max_points_per_leaf", C.c_int), ("max_level", C.c_int), ("device", C.c_int)]
+                ("max_points_per_leaf", C.c_int), ("max_level", C.c_int), ("device", C.c_int),
+                ("vectors_per_pass", C.c_int)]
 
 
 class Info(C.Structure):
     _fields_ = [("nlevels", C.c_int), ("nboxes", C.c_int64), ("nleaves", C.c_int64),
                 ("nsources", C.c_int64), ("ntargets", C.c_int64), ("near_pairs", C.c_int64),
                 ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
-                ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64)]
+                ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64),
+                ("vectors_per_pass", C.c_int64)]
 
 
 def lib():
@@ -165,6 +167,11 @@ class FmmBuilder:
 
     def max_points_per_leaf(self, n):
         self._s.max_points_per_leaf = int(n)
+        return self
+
+    def vectors_per_pass(self, n):
+        """Charge vectors per device pass (0: as many as fit); the results do not depend on it."""
+        self._s.vectors_per_pass = int(n)
         return self
 
     def max_level(self, level):

@@ -134,6 +134,8 @@ struct EvaluatorBase {
     int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
     int64_t launches = 0;  // kernels launched by the last evaluation
+    int qstride = 1;       // charges per point in the caller's array (all vectors)
+    bool first_pass = true;  // vectors run in passes: the first one resets timing and counts
     bool overlap = false;  // near field on its own stream beside the far field (measured: no gain)
     unsigned counted(unsigned grid) {  // wraps the grid of every evaluation launch
         ++launches;
@@ -581,8 +583,10 @@ struct Evaluator final : EvaluatorBase {
 
     // ---- evaluation: every pass, fused where the level structure allows ----
     void evaluate(const double* d_charges, double* d_phi, double* d_grad) override {
-        timer.begin();
-        launches = 0;
+        if (first_pass) {
+            timer.begin();
+            launches = 0;
+        }
         // charge load into leaf order
         timer.run(kLoad, [&] {
             load_charges(d_charges);
@@ -647,7 +651,7 @@ struct Evaluator final : EvaluatorBase {
         const int64_t ns = dp.nsrc;
         if (ns > 0)
             charge_load_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
-                d_charges, src_perm.as<int64_t>(), ns, m, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
+                d_charges, src_perm.as<int64_t>(), ns, m, qstride, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
     }
 
     size_t exp_smem() const { return sizeof(T) * (NC * 32 + (size_t)m * 32); }
@@ -782,7 +786,7 @@ struct Evaluator final : EvaluatorBase {
     // ---- the Helmholtz near field (all leaves' P2P level calls) ----
     DevBuf hq, hq64;
     void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) override {
-        launches = 0;
+        if (first_pass) launches = 0;
         const int64_t ns = dp.nsrc;
         if (!hq.ptr) {
             hq.alloc(sizeof(Cplx<T>) * (size_t)m * (ns + 1));
@@ -790,7 +794,7 @@ struct Evaluator final : EvaluatorBase {
         }
         if (ns > 0)
             helm_charge_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
-                d_q, src_perm.as<int64_t>(), ns, m, hq.as<Cplx<T>>(), kMixed ? hq64.as<double2>() : nullptr);
+                d_q, src_perm.as<int64_t>(), ns, m, qstride, hq.as<Cplx<T>>(), kMixed ? hq64.as<double2>() : nullptr);
         if (items.count) {
             const unsigned g = (unsigned)((items.count + kHelmWarps - 1) / kHelmWarps);
             if (gradients)
@@ -885,6 +889,7 @@ struct fmmgpu_fmm {
     size_t device_bytes = 0;
     int64_t near_pairs = 0;
     bool op_begun = false;  // a level-call evaluation has begun
+    int mpass = 1;          // charge vectors per evaluator pass (all of them unless memory says no)
     // whole-evaluation CUDA graph: captured once per (charges, potential, gradient)
     // buffer triple, replayed while the triple and the settings stay the same
     bool graph_on = false;
@@ -947,10 +952,22 @@ namespace {
 
 // One evaluation on the handle's stream: replayed from the CUDA graph when graphs are on
 // (and per-kind timing is off), else launched directly.
+// The evaluation in passes of f->mpass vectors (all of them when they fit on the device).
+void run_passes(fmmgpu_fmm* f, const double* q, double* phi, double* grad) {
+    EvaluatorBase& ev = *f->eval;
+    const int m = f->settings.vectors;
+    const int64_t nt = (int64_t)f->plan.tgt_perm.size();
+    for (int v0 = 0; v0 < m; v0 += f->mpass) {
+        ev.first_pass = v0 == 0;
+        ev.evaluate(q + v0, phi + (int64_t)v0 * nt, grad ? grad + 3 * (int64_t)v0 * nt : nullptr);
+    }
+    ev.first_pass = true;
+}
+
 void run_evaluation(fmmgpu_fmm* f, const double* q, double* phi, double* grad) {
     EvaluatorBase& ev = *f->eval;
     if (!f->graph_on || ev.timer.on) {
-        ev.evaluate(q, phi, grad);
+        run_passes(f, q, phi, grad);
         return;
     }
     if (!f->graph || f->graph_key[0] != q || f->graph_key[1] != phi || f->graph_key[2] != grad) {
@@ -958,7 +975,7 @@ void run_evaluation(fmmgpu_fmm* f, const double* q, double* phi, double* grad) {
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            ev.evaluate(q, phi, grad);
+            run_passes(f, q, phi, grad);
         } catch (...) {
             cudaStreamEndCapture(f->stream, &g);
             if (g) cudaGraphDestroy(g);
@@ -1010,6 +1027,7 @@ void fmmgpu_default_settings(fmmgpu_settings* s) {
     s->max_points_per_leaf = 64;
     s->max_level = 16;
     s->device = 0;
+    s->vectors_per_pass = 0;
 }
 
 namespace {
@@ -1017,7 +1035,8 @@ namespace {
 void check_settings(const fmmgpu_settings* settings) {
     if (!settings) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
     const fmmgpu_settings& s = *settings;
-    if (s.p < 0 || s.vectors < 1 || s.max_points_per_leaf < 1 || s.max_level < 0 || s.max_level > 16)
+    if (s.p < 0 || s.vectors < 1 || s.max_points_per_leaf < 1 || s.max_level < 0 || s.max_level > 16 ||
+        s.vectors_per_pass < 0)
         throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid settings");
     if (s.precision != FMMGPU_PRECISION_F64 && s.precision != FMMGPU_PRECISION_MIXED)
         throw Failure(FMMGPU_UNSUPPORTED, "unknown precision");
@@ -1136,13 +1155,33 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
     int least = 0, greatest = 0;  // the far-field chain is the critical path: highest priority
     CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     CUDA_TRY(cudaStreamCreateWithPriority(&f->stream, cudaStreamNonBlocking, greatest));
+    // vectors per pass: every per-vector buffer (expansions, translation products, partial
+    // outputs) for as many vectors as fit in 60% of the free memory
+    {
+        const size_t nc = (size_t)(s.p + 1) * (s.p + 1), ys = (nc + 31) / 32 * 32;
+        const size_t tsz = s.precision == FMMGPU_PRECISION_F64 ? 8 : 4;
+        const size_t nsrc = P.src_perm.size(), ntgt = P.tgt_perm.size();
+        const size_t per_vec = tsz * (2 * P.nboxes() * nc + P.nboxes() * ys + (P.v.nnz() + 1) * ys + nsrc) +
+                               (tsz == 4 ? 8 * nsrc : 0) + 8 * ntgt * (s.gradients ? 4 : 1) * 2 +
+                               8 * ntgt * (s.gradients ? 4 : 1) + 8 * nsrc;
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        const size_t fit = per_vec ? (size_t)(0.6 * (double)free_b) / per_vec : (size_t)s.vectors;
+        int want = (int)std::max<size_t>(1, std::min<size_t>((size_t)s.vectors, fit));
+        if (s.vectors_per_pass > 0) want = std::min(s.vectors_per_pass, s.vectors);
+        // every pass holds the same number of vectors (the buffers' and the kernels' m): the
+        // largest divisor of the vector count not above the wanted size
+        while (s.vectors % want) --want;
+        f->mpass = want;
+    }
     size_t bytes = 0;
     if (s.precision == FMMGPU_PRECISION_F64)
-        f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0, us,
+        f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, f->mpass, s.gradients != 0, us,
                                          ut, &bytes);
     else
-        f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, s.vectors, s.gradients != 0, us,
+        f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, f->mpass, s.gradients != 0, us,
                                         ut, &bytes);
+    f->eval->qstride = s.vectors;
     const size_t ns = P.src_perm.size(), nt = P.tgt_perm.size();
     f->d_charges.alloc(sizeof(double) * (size_t)s.vectors * (ns + 1));
     f->d_phi.alloc(sizeof(double) * (size_t)s.vectors * (nt + 1));
@@ -1317,8 +1356,12 @@ int fmmgpu_helmholtz_near(fmmgpu_fmm* f, double k_re, double k_im, const double*
         phi.alloc(sizeof(double) * 2 * m * (nt + 1));
         if (f->settings.gradients) g.alloc(sizeof(double) * 6 * m * (nt + 1));
         CUDA_TRY(cudaMemcpyAsync(q.ptr, charges, sizeof(double) * 2 * m * ns, cudaMemcpyHostToDevice, f->stream));
-        f->eval->helmholtz_near(k_re, k_im, q.as<double>(), phi.as<double>(),
-                                f->settings.gradients ? g.as<double>() : nullptr);
+        for (int v0 = 0; v0 < (int)m; v0 += f->mpass) {
+            f->eval->first_pass = v0 == 0;
+            f->eval->helmholtz_near(k_re, k_im, q.as<double>() + 2 * v0, phi.as<double>() + 2 * (size_t)v0 * nt,
+                                    f->settings.gradients ? g.as<double>() + 6 * (size_t)v0 * nt : nullptr);
+        }
+        f->eval->first_pass = true;
         CUDA_TRY(cudaMemcpyAsync(potential, phi.ptr, sizeof(double) * 2 * m * nt, cudaMemcpyDeviceToHost, f->stream));
         if (f->settings.gradients)
             CUDA_TRY(cudaMemcpyAsync(gradient, g.ptr, sizeof(double) * 6 * m * nt, cudaMemcpyDeviceToHost, f->stream));
@@ -1330,6 +1373,8 @@ int fmmgpu_op_begin_evaluation(fmmgpu_fmm* f, const double* charges) {
     return guarded([&] {
         if (!f || !charges) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
         if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        if (f->mpass < f->settings.vectors)
+            throw Failure(FMMGPU_UNSUPPORTED, "the level calls need every charge vector in one pass (device memory)");
         CUDA_TRY(cudaSetDevice(f->settings.device));
         const size_t m = f->settings.vectors, ns = f->plan.src_perm.size();
         CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, f->stream));
@@ -1463,6 +1508,7 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->device_bytes = (int64_t)f->device_bytes;
         info->close_pairs = f->eval ? f->eval->close_pairs : 0;
         info->launches = f->eval ? f->eval->launches : 0;
+        info->vectors_per_pass = f->eval ? f->mpass : 0;
     });
 }
 

@@ -72,12 +72,12 @@ __device__ __forceinline__ void helm_pair(T kre, T kim, T dx, T dy, T dz, T r2, 
 // ((re, im) doubles) -> leaf order [v][point] in T, and in f64 for the near-singular pairs.
 template <typename T>
 __global__ void helm_charge_kernel(const double* __restrict__ q_caller, const int64_t* __restrict__ perm, int64_t n,
-                                   int m, Cplx<T>* __restrict__ q_leaf, double2* __restrict__ q64) {
+                                   int m, int stride, Cplx<T>* __restrict__ q_leaf, double2* __restrict__ q64) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t c = perm[i];
     for (int v = 0; v < m; ++v) {
-        const double re = q_caller[2 * (c * m + v)], im = q_caller[2 * (c * m + v) + 1];
+        const double re = q_caller[2 * (c * stride + v)], im = q_caller[2 * (c * stride + v) + 1];
         q_leaf[(int64_t)v * n + i] = Cplx<T>{(T)re, (T)im};
         if (q64) q64[(int64_t)v * n + i] = make_double2(re, im);
     }

@@ -78,14 +78,16 @@ __device__ __forceinline__ void rel_frame(const DevPlan& P, int s, int t, T c[3]
 // ---------------------------------------------------------------------------------
 // Charge load: caller-order charges (m per point, point-major) -> leaf order [v][i].
 // ---------------------------------------------------------------------------------
+// (m vectors of a pass; the caller's array holds `stride` charges per point, the pass's
+// first at q_caller[0])
 template <typename T>
 __global__ void charge_load_kernel(const double* __restrict__ q_caller, const int64_t* __restrict__ perm,
-                                   int64_t n, int m, T* __restrict__ q_leaf, double* __restrict__ q64) {
+                                   int64_t n, int m, int stride, T* __restrict__ q_leaf, double* __restrict__ q64) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t c = perm[i];
     for (int v = 0; v < m; ++v) {
-        double q = q_caller[c * m + v];
+        double q = q_caller[c * stride + v];
         q_leaf[(int64_t)v * n + i] = (T)q;
         if (q64) q64[(int64_t)v * n + i] = q;  // the mixed form keeps f64 charges for its f64 pairs
     }

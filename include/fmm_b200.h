@@ -57,6 +57,9 @@ typedef struct {
     int max_points_per_leaf;  /* refinement target (distinct level-16 keys per leaf) */
     int max_level;            /* deepest leaf level, 0-16 */
     int device;               /* CUDA device ordinal */
+    int vectors_per_pass;     /* charge vectors per device pass: 0 (default) as many as fit in
+                                 60% of the free device memory; rounded down to a divisor of
+                                 `vectors`; the results do not depend on it */
 } fmmgpu_settings;
 
 typedef struct {
@@ -68,12 +71,13 @@ typedef struct {
     int64_t device_bytes; /* device memory held by the evaluator */
     int64_t close_pairs;  /* near-singular P2P pairs the mixed form evaluates in f64 */
     int64_t launches;     /* kernels the last evaluation launched (0 before the first) */
+    int64_t vectors_per_pass;  /* charge vectors per device pass (0 for a plan-only handle) */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;
 
 /* Settings with the reference's defaults: p = 6, f64, no gradients, one vector,
- * 64 points per leaf, max level 16, device 0. */
+ * 64 points per leaf, max level 16, device 0 (and vectors per pass chosen by memory). */
 void fmmgpu_default_settings(fmmgpu_settings* settings);
 
 /* FmmBuilder::build (fmm.rs:1853): sources/targets are n x 3 doubles, caller order. */

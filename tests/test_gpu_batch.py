@@ -51,3 +51,24 @@ def test_batch_with_distinct_targets_matches_oracle(oracle):
         assert rel(out.potential[0, off:off + len(t)], phi) < 1e-12
         assert rel(out.gradient[0, off:off + len(t)], g) < 1e-12
         off += len(t)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_vector_passes_give_the_same_floats(oracle, precision):
+    """Charge vectors evaluated in passes (vectors_per_pass) equal the one-pass results."""
+    x, _ = oracle.point_sets("sphere", 15000, 41)
+    q = np.random.default_rng(6).uniform(-1, 1, (len(x), 6))
+    base = F.FmmBuilder(6).gradients().vectors(6).max_points_per_leaf(64).precision(precision)
+    one = base.build(x).evaluate(q)
+    # 4 is rounded down to 3, a divisor of 6: two passes of three vectors
+    two = F.FmmBuilder(6).gradients().vectors(6).max_points_per_leaf(64).precision(precision) \
+        .vectors_per_pass(4).build(x)
+    assert two.info()["vectors_per_pass"] == 3
+    out = two.evaluate(q)
+    assert np.array_equal(out.potential, one.potential) and np.array_equal(out.gradient, one.gradient)
+    two.set_graph(True)
+    for _ in range(2):
+        out = two.evaluate(q)
+        assert np.array_equal(out.potential, one.potential)
+    hq = q + 0.5j * q[::-1]
+    assert np.array_equal(two.helmholtz_near(3.0, hq).potential, base.build(x).helmholtz_near(3.0, hq).potential)
