@@ -295,6 +295,10 @@ struct Evaluator final : EvaluatorBase {
         near_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
         if (gradients) near_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         if (kMixed) {
+            for (size_t j = 0; j < pl.nleaves(); ++j)  // a row fits the kernel's shared memory
+                if (pl.near.row[j + 1] - pl.near.row[j] > kX2Recs)
+                    throw Failure(FMMGPU_INVALID_ARGUMENT, "a near row longer than " + std::to_string(kX2Recs) +
+                                                              " leaves (the tree is not 2:1 balanced)");
             build_close_pairs(us, ut);
             near_rec.alloc(sizeof(NearRec) * (pl.near.nnz() + 1));
             if (pl.nleaves())

@@ -1,7 +1,8 @@
 // Mixed-precision P2P on the packed f32x2 pipe of sm_100 (FFMA2 / FADD2 / FMUL2).
 //
 // Same sums as p2p_kernel<float, GRAD, true> (kernels.cuh): one warp per work item of up
-// to 32 targets of one leaf (lane = target), the near row of that leaf (source leaves in
+// to 32 targets of one leaf (lane = target; an item of fewer targets splits the sources
+// over several lanes per target), the near row of that leaf (source leaves in
 // row order, points in leaf order), sources mapped into the target leaf's frame by
 // y = fma(r, u, c) (fmm-kernels/src/p2p.rs:320-340 frame_centre / frame_ratio), the pair
 // skipped iff its f32 r2 < theta2 (those pairs are added in f64 from the close-pair CSR,
@@ -15,9 +16,10 @@
 //  - the frame, start and size of every near entry are precomputed at build time
 //    (NearRec, from rel_frame<float>, the same function the close-pair search uses), so
 //    a source leaf costs no dependent index loads;
-//  - the stage is filled across source-leaf boundaries (256 sources per flush), every
-//    lane issuing four loads at a time before any of them is used.
-// The f32 partial of a flush (at most 128 sources per half) is added into the f64 sums.
+//  - the stage is filled across source-leaf boundaries (128 sources per flush), the next
+//    flush's points and charges copied asynchronously (cp.async) while one is computed;
+//  - an item of fewer than 32 targets splits the sources over several lanes per target.
+// The f32 partial of a flush (at most 64 sources per half) is added into the f64 sums.
 #pragma once
 
 #include "kernels.cuh"
@@ -52,33 +54,57 @@ __global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec* __res
 }
 
 constexpr int kX2Warps = 4;
-constexpr int kX2Stage = 256;  // sources per flush (128 pairs)
-constexpr int kX2Recs = 64;    // near entries held in shared memory at once
-constexpr int kX2Gather = 4;   // loads in flight per lane while a stage is filled
+constexpr int kX2Stage = 128;  // sources per flush (64 pairs)
+constexpr int kX2Recs = 64;    // a near row's entries, all in shared memory (2:1 balance: at most 57)
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+
+// Flushes run over (vector, position in the row's source stream); while flush f is
+// computed, the raw points and charges of flush f + 1 are in flight (cp.async), so a
+// warp does not wait on global memory for its sources.
 template <bool GRAD>
 __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
     DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
     const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
     double* __restrict__ far_phi, double* __restrict__ far_g, int accumulate, double* __restrict__ out_phi,
     double* __restrict__ out_g) {
-    __shared__ float4 sxy[kX2Warps][kX2Stage / 2];  // (x0, x1, y0, y1)
+    __shared__ float4 sxy[kX2Warps][kX2Stage / 2];  // (x0, x1, y0, y1) in the target's frame
     __shared__ float4 szq[kX2Warps][kX2Stage / 2];  // (z0, z1, q0, q1)
+    __shared__ float4 raw[kX2Warps][kX2Stage];      // the next flush's points, as loaded
+    __shared__ float rawq[kX2Warps][kX2Stage];
+    __shared__ int rawrec[kX2Warps][kX2Stage];      // their near entries
     __shared__ NearRec srec[kX2Warps][kX2Recs];
+    __shared__ double red[kX2Warps][4][32];  // the split lanes' sums, reduced per target
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t item = (int64_t)blockIdx.x * kX2Warps + warp;
     if (item >= items.count) return;
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
-    const int64_t t = items.t0[item] + lane;
-    const bool valid = t < t1;
+    // an item of ni < 32 targets splits each flush's pair-steps over K = 32 / ni lanes per
+    // target: lane = target + ni * kk takes the pair-steps i = kk (mod K); the K sums of a
+    // target are added in kk order at the end
+    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int K = 32 / ni;
+    const int kk = lane < ni * K ? lane / ni : K;  // lanes past ni * K take no pair-steps
+    const int ti = lane < ni * K ? lane % ni : 0;
+    const int64_t t = items.t0[item] + ti;
+    const bool valid = lane < ni;  // the lanes that finish their target (kk = 0)
     const int64_t n0 = plan.near_row[leaf], n1 = near ? plan.near_row[leaf + 1] : n0;
     const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (valid) {
+    if (kk < K) {
         const float4 p4 = tpos[t];
         tx = p4.x;
         ty = p4.y;
@@ -90,154 +116,171 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
     const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
     const double phi_scale = 4.0 * 3.141592653589793 * rt;
     const double g_scale = phi_scale * rt;
-    for (int v = 0; v < m; ++v) {
+    const int nr = (int)(n1 - n0);  // <= kX2Recs, checked when the plan is uploaded
+    for (int j = lane; j < nr; j += 32) srec[warp][j] = recs[n0 + j];
+    __syncwarp();
+    const int S = nr ? srec[warp][nr - 1].off + srec[warp][nr - 1].ns : 0;  // the row's sources
+    const int nfl = S > 0 ? (S + kX2Stage - 1) / kX2Stage : 1;              // flushes per vector
+    const int total = nfl * m;
+    int epf = 0;  // this lane's near entry in the prefetch walk (monotone within a vector)
+    auto issue = [&](int f) {
+        const int v = f / nfl, base = (f - v * nfl) * kX2Stage;
+        const int cnt = (S - base) < kX2Stage ? (S - base) : kX2Stage;
         const float* qv = sq + (int64_t)v * nsrc;
-        double aphi = 0.0, ag0 = 0.0, ag1 = 0.0, ag2 = 0.0;
-        for (int64_t r0 = n0; r0 < n1; r0 += kX2Recs) {
-            const int nr = (int)((n1 - r0) < kX2Recs ? (n1 - r0) : kX2Recs);
-            __syncwarp();
-            for (int j = lane; j < nr; j += 32) srec[warp][j] = recs[r0 + j];
-            __syncwarp();
-            const int base0 = srec[warp][0].off;
-            const int end = srec[warp][nr - 1].off + srec[warp][nr - 1].ns;
-            int e = 0;  // this lane's current record: monotone over the flushes
-            for (int base = base0; base < end; base += kX2Stage) {
-                const int cnt = (end - base) < kX2Stage ? (end - base) : kX2Stage;
-                // two rounds of four loads per lane, each issued before any is used
+        if (base == 0) epf = 0;
 #pragma unroll
-                for (int h = 0; h < kX2Stage / 32; h += kX2Gather) {
-                    float4 p[kX2Gather];
-                    float q[kX2Gather];
-                    const int e_first = e;
+        for (int i = 0; i < kX2Stage / 32; ++i) {
+            const int k = lane + 32 * i;
+            if (k < cnt) {
+                const int pos = base + k;
+                // the entries are contiguous in the stream and pos < S: epf stays < nr
+                while (srec[warp][epf].off + srec[warp][epf].ns <= pos) ++epf;
+                const int64_t s = srec[warp][epf].s0 + (pos - srec[warp][epf].off);
+                cp_async16(&raw[warp][k], spos + s);
+                cp_async4(&rawq[warp][k], qv + s);
+                rawrec[warp][k] = epf;
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    double aphi = 0.0, ag0 = 0.0, ag1 = 0.0, ag2 = 0.0;
+    issue(0);
+    for (int f = 0; f < total; ++f) {
+        const int v = f / nfl, base = (f - v * nfl) * kX2Stage;
+        const int cnt = (S - base) < kX2Stage ? (S - base) : kX2Stage;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+        // map the flush's sources into the target's frame, in pairs
 #pragma unroll
-                    for (int i = 0; i < kX2Gather; ++i) {
-                        const int k = lane + 32 * (h + i);
-                        if (k < cnt) {
-                            const int pos = base + k;
-                            // records are contiguous in the stream and pos < end: e stays < nr
-                            while (srec[warp][e].off + srec[warp][e].ns <= pos) ++e;
-                            const int64_t s = srec[warp][e].s0 + (pos - srec[warp][e].off);
-                            p[i] = spos[s];
-                            q[i] = qv[s];
-                        }
-                    }
-                    int e2 = e_first;  // the same walk again for the frames
-#pragma unroll
-                    for (int i = 0; i < kX2Gather; ++i) {
-                        const int k = lane + 32 * (h + i);
-                        if (k < cnt) {
-                            const int pos = base + k;
-                            while (srec[warp][e2].off + srec[warp][e2].ns <= pos) ++e2;
-                            const float4 fr = srec[warp][e2].frame;
-                            const int slot = (k >> 1) * 4 + (k & 1);
-                            sxy_f[slot] = __fmaf_rn(fr.w, p[i].x, fr.x);
-                            sxy_f[slot + 2] = __fmaf_rn(fr.w, p[i].y, fr.y);
-                            szq_f[slot] = __fmaf_rn(fr.w, p[i].z, fr.z);
-                            szq_f[slot + 2] = q[i];
-                        }
-                    }
-                }
-                if ((cnt & 1) && lane == 0) {  // odd count: a zero charge completes the last pair
-                    const int slot = (cnt >> 1) * 4 + 1;
-                    sxy_f[slot] = 0.f;
-                    sxy_f[slot + 2] = 0.f;
-                    szq_f[slot] = 0.f;
-                    szq_f[slot + 2] = 0.f;
-                }
-                __syncwarp();
-                float2 pphi = f2(0.f, 0.f), pg0 = f2(0.f, 0.f), pg1 = f2(0.f, 0.f), pg2 = f2(0.f, 0.f);
-                const int npairs = (cnt + 1) >> 1;
+        for (int i = 0; i < kX2Stage / 32; ++i) {
+            const int k = lane + 32 * i;
+            if (k < cnt) {
+                const float4 p = raw[warp][k];
+                const float4 fr = srec[warp][rawrec[warp][k]].frame;
+                const int slot = (k >> 1) * 4 + (k & 1);
+                sxy_f[slot] = __fmaf_rn(fr.w, p.x, fr.x);
+                sxy_f[slot + 2] = __fmaf_rn(fr.w, p.y, fr.y);
+                szq_f[slot] = __fmaf_rn(fr.w, p.z, fr.z);
+                szq_f[slot + 2] = rawq[warp][k];
+            }
+        }
+        if ((cnt & 1) && lane == 0) {  // odd count: a zero charge completes the last pair
+            const int slot = (cnt >> 1) * 4 + 1;
+            sxy_f[slot] = 0.f;
+            sxy_f[slot + 2] = 0.f;
+            szq_f[slot] = 0.f;
+            szq_f[slot + 2] = 0.f;
+        }
+        __syncwarp();
+        if (f + 1 < total) issue(f + 1);  // the raw buffers are free again
+        float2 pphi = f2(0.f, 0.f), pg0 = f2(0.f, 0.f), pg1 = f2(0.f, 0.f), pg2 = f2(0.f, 0.f);
+        const int npairs = (cnt + 1) >> 1;
 #pragma unroll 2
-                for (int i = 0; i < npairs; ++i) {
-                    const float4 a = sxy[warp][i];
-                    const float4 b = szq[warp][i];
-                    const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
-                    const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
-                    const float2 dz = __fadd2_rn(f2(b.x, b.y), ntz);
-                    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-                    const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
-                    const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
-                    const float2 rinv = f2(ri0, ri1);
-                    const float2 qr = __fmul2_rn(f2(b.z, b.w), rinv);
-                    pphi = __fadd2_rn(pphi, qr);
+        for (int i = kk; i < npairs; i += K) {
+            const float4 a = sxy[warp][i];
+            const float4 b = szq[warp][i];
+            const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
+            const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
+            const float2 dz = __fadd2_rn(f2(b.x, b.y), ntz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
+            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float2 rinv = f2(ri0, ri1);
+            const float2 qr = __fmul2_rn(f2(b.z, b.w), rinv);
+            pphi = __fadd2_rn(pphi, qr);
+            if (GRAD) {
+                const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, rinv), rinv);
+                pg0 = __ffma2_rn(qr3, dx, pg0);
+                pg1 = __ffma2_rn(qr3, dy, pg1);
+                pg2 = __ffma2_rn(qr3, dz, pg2);
+            }
+        }
+        aphi += (double)pphi.x;
+        aphi += (double)pphi.y;
+        if (GRAD) {
+            ag0 += (double)pg0.x;
+            ag0 += (double)pg0.y;
+            ag1 += (double)pg1.x;
+            ag1 += (double)pg1.y;
+            ag2 += (double)pg2.x;
+            ag2 += (double)pg2.y;
+        }
+        __syncwarp();  // the pairs are read before the next map overwrites them
+        if (f - v * nfl != nfl - 1) continue;
+        // ---- the last flush of vector v: finish its targets ----
+        if (K > 1) {  // the target's K partial sums, in kk order
+            red[warp][0][lane] = aphi;
+            red[warp][1][lane] = ag0;
+            red[warp][2][lane] = ag1;
+            red[warp][3][lane] = ag2;
+            __syncwarp();
+            if (valid)
+                for (int j = 1; j < K; ++j) {
+                    aphi += red[warp][0][ti + ni * j];
+                    ag0 += red[warp][1][ti + ni * j];
+                    ag1 += red[warp][2][ti + ni * j];
+                    ag2 += red[warp][3][ti + ni * j];
+                }
+            __syncwarp();
+        }
+        if (valid) {
+            if (near) {
+                // near-singular pairs in f64: the f64 map and the reference's coincidence rule
+                const double4 u = close.tpos[t];
+                for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
+                    const int64_t sp = close.src[c2];
+                    const int sl = close.leaf[c2];
+                    double cc[3] = {0.0, 0.0, 0.0}, rr = 1.0;
+                    if (sl != leaf) rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
+                    const double4 ps = close.spos[sp];
+                    const double yx = sl != leaf ? __fma_rn(rr, ps.x, cc[0]) : ps.x;
+                    const double yy = sl != leaf ? __fma_rn(rr, ps.y, cc[1]) : ps.y;
+                    const double yz = sl != leaf ? __fma_rn(rr, ps.z, cc[2]) : ps.z;
+                    if (u.x == yx && u.y == yy && u.z == yz) continue;
+                    const double dx = u.x - yx, dy = u.y - yy, dz = u.z - yz;
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    const double rinv = rsqrt(r2);
+                    const double qr = close.q[(int64_t)v * nsrc + sp] * rinv;
+                    aphi += qr;
                     if (GRAD) {
-                        const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, rinv), rinv);
-                        pg0 = __ffma2_rn(qr3, dx, pg0);
-                        pg1 = __ffma2_rn(qr3, dy, pg1);
-                        pg2 = __ffma2_rn(qr3, dz, pg2);
+                        const double qr3 = qr * rinv * rinv;
+                        ag0 -= qr3 * dx;
+                        ag1 -= qr3 * dy;
+                        ag2 -= qr3 * dz;
                     }
                 }
-                aphi += (double)pphi.x;
-                aphi += (double)pphi.y;
-                if (GRAD) {
-                    ag0 += (double)pg0.x;
-                    ag0 += (double)pg0.y;
-                    ag1 += (double)pg1.x;
-                    ag1 += (double)pg1.y;
-                    ag2 += (double)pg2.x;
-                    ag2 += (double)pg2.y;
-                }
-                __syncwarp();
             }
-        }
-        if (!valid) continue;
-        if (near) {
-            // near-singular pairs in f64: the f64 map and the reference's coincidence rule
-            const double4 u = close.tpos[t];
-            for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
-                const int64_t sp = close.src[c2];
-                const int sl = close.leaf[c2];
-                double cc[3] = {0.0, 0.0, 0.0}, rr = 1.0;
-                if (sl != leaf) rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
-                const double4 ps = close.spos[sp];
-                const double yx = sl != leaf ? __fma_rn(rr, ps.x, cc[0]) : ps.x;
-                const double yy = sl != leaf ? __fma_rn(rr, ps.y, cc[1]) : ps.y;
-                const double yz = sl != leaf ? __fma_rn(rr, ps.z, cc[2]) : ps.z;
-                if (u.x == yx && u.y == yy && u.z == yz) continue;
-                const double dx = u.x - yx, dy = u.y - yy, dz = u.z - yz;
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                const double rinv = rsqrt(r2);
-                const double qr = close.q[(int64_t)v * nsrc + sp] * rinv;
-                aphi += qr;
+            // both gradient sums hold -sum qr3 (t - y), as p2p_kernel's
+            if (accumulate == 2) {  // near field alone, leaf order (added to the far field by output_kernel)
+                out_phi[(int64_t)v * nt + t] = aphi;
                 if (GRAD) {
-                    const double qr3 = qr * rinv * rinv;
-                    ag0 -= qr3 * dx;
-                    ag1 -= qr3 * dy;
-                    ag2 -= qr3 * dz;
+                    double* o = out_g + ((int64_t)v * nt + t) * 3;
+                    o[0] = ag0;
+                    o[1] = ag1;
+                    o[2] = ag2;
+                }
+            } else if (accumulate) {  // level calls: add into the leaf-order store, scaled by output_kernel
+                far_phi[(int64_t)v * nt + t] = far_phi[(int64_t)v * nt + t] + aphi;
+                if (GRAD) {
+                    double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                    fg[0] = fg[0] + ag0;
+                    fg[1] = fg[1] + ag1;
+                    fg[2] = fg[2] + ag2;
+                }
+            } else {
+                const double ph = far_phi[(int64_t)v * nt + t] + aphi;
+                const int64_t i = plan.tgt_perm[t];
+                out_phi[(int64_t)v * nt + i] = ph / phi_scale;
+                if (GRAD) {
+                    const double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                    double* o = out_g + ((int64_t)v * nt + i) * 3;
+                    o[0] = (fg[0] + ag0) / g_scale;
+                    o[1] = (fg[1] + ag1) / g_scale;
+                    o[2] = (fg[2] + ag2) / g_scale;
                 }
             }
         }
-        // both gradient sums hold -sum qr3 (t - y), as p2p_kernel's
-        if (accumulate == 2) {  // near field alone, leaf order (added to the far field by output_kernel)
-            out_phi[(int64_t)v * nt + t] = aphi;
-            if (GRAD) {
-                double* o = out_g + ((int64_t)v * nt + t) * 3;
-                o[0] = ag0;
-                o[1] = ag1;
-                o[2] = ag2;
-            }
-            continue;
-        }
-        const double ph = far_phi[(int64_t)v * nt + t] + aphi;
-        if (accumulate) {  // level calls: add into the leaf-order store, scaled by output_kernel
-            far_phi[(int64_t)v * nt + t] = ph;
-            if (GRAD) {
-                double* fg = far_g + ((int64_t)v * nt + t) * 3;
-                fg[0] = fg[0] + ag0;
-                fg[1] = fg[1] + ag1;
-                fg[2] = fg[2] + ag2;
-            }
-            continue;
-        }
-        const int64_t i = plan.tgt_perm[t];
-        out_phi[(int64_t)v * nt + i] = ph / phi_scale;
-        if (GRAD) {
-            const double* fg = far_g + ((int64_t)v * nt + t) * 3;
-            double* o = out_g + ((int64_t)v * nt + i) * 3;
-            o[0] = (fg[0] + ag0) / g_scale;
-            o[1] = (fg[1] + ag1) / g_scale;
-            o[2] = (fg[2] + ag2) / g_scale;
-        }
+        aphi = ag0 = ag1 = ag2 = 0.0;
     }
 }
 
