@@ -186,7 +186,7 @@ struct Evaluator final : EvaluatorBase {
     int num_sms = 148;
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
-    DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec;
+    DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
     // the near field summed apart on a second, lower-priority stream, joined by output_kernel
     DevBuf near_phi, near_g;
     cudaStream_t near_stream = nullptr;
@@ -557,6 +557,10 @@ struct Evaluator final : EvaluatorBase {
         close.leaf = close_leaf.as<int32_t>();
         close.spos = spos64.as<double4>();
         close.tpos = tpos64.as<double4>();
+        close_y.alloc(sizeof(double4) * (size_t)(nclose + 1));
+        close.y = close_y.as<double4>();
+        if (plan.nleaves()) close_map_kernel<<<(unsigned)plan.nleaves(), 64>>>(dp, close, close_y.as<double4>());
+        CUDA_TRY(cudaGetLastError());
         close.q = sq64.as<double>();
     }
 
@@ -576,7 +580,7 @@ struct Evaluator final : EvaluatorBase {
                                &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
                                &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e,
                                &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
-                               &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &tc_tile_d,
+                               &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
                                &near_phi, &near_g, &box_side, &v_pos};

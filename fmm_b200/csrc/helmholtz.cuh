@@ -167,13 +167,8 @@ __global__ void __launch_bounds__(32 * kHelmWarps) helm_p2p_kernel(
             const double4 u = close.tpos[t];
             for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
                 const int64_t sp = close.src[c2];
-                const int sl = close.leaf[c2];
-                double cc[3] = {0.0, 0.0, 0.0}, rr = 1.0;
-                if (sl != leaf) rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
-                const double4 ps = close.spos[sp];
-                const double yx = sl != leaf ? __fma_rn(rr, ps.x, cc[0]) : ps.x;
-                const double yy = sl != leaf ? __fma_rn(rr, ps.y, cc[1]) : ps.y;
-                const double yz = sl != leaf ? __fma_rn(rr, ps.z, cc[2]) : ps.z;
+                const double4 yv = close.y[c2];  // the source point in the target's frame
+                const double yx = yv.x, yy = yv.y, yz = yv.z;
                 if (u.x == yx && u.y == yy && u.z == yz) continue;
                 const double dx = u.x - yx, dy = u.y - yy, dz = u.z - yz;
                 const double r2 = dx * dx + dy * dy + dz * dz;

@@ -632,7 +632,28 @@ struct ClosePairs {  // near-singular pairs of the mixed form, CSR by target (le
     const double4* spos;  // f64 leaf-scaled coordinates
     const double4* tpos;
     const double* q;      // f64 charges in leaf order [vector][point]
+    const double4* y;     // the source point in the target leaf's frame (f64), per pair
 };
+
+// Build time (mixed form): each near-singular pair's source point mapped into its target
+// leaf's frame in f64, y = fma(r, u, c) with the exact relative frame (the identity for the
+// leaf itself), as the evaluation would form it.  Block per leaf.
+__global__ void close_map_kernel(DevPlan plan, ClosePairs close, double4* __restrict__ y) {
+    const int64_t leaf = blockIdx.x;
+    const int box = plan.leaf_box[leaf];
+    for (int64_t t = plan.tgt_start[leaf] + threadIdx.x; t < plan.tgt_start[leaf + 1]; t += blockDim.x)
+        for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
+            const int sl = close.leaf[c2];
+            const double4 ps = close.spos[close.src[c2]];
+            if (sl == leaf) {
+                y[c2] = make_double4(ps.x, ps.y, ps.z, 0.0);
+            } else {
+                double cc[3], rr;
+                rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
+                y[c2] = make_double4(__fma_rn(rr, ps.x, cc[0]), __fma_rn(rr, ps.y, cc[1]), __fma_rn(rr, ps.z, cc[2]), 0.0);
+            }
+        }
+}
 
 template <typename T, bool GRAD, bool CLOSE>
 __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, int m, int near, T theta2,

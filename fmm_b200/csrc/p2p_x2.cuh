@@ -226,21 +226,15 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
         if (valid) {
             if (near) {
                 // near-singular pairs in f64: the f64 map and the reference's coincidence rule
+                // (the source points already in the target's frame, close_map_kernel)
                 const double4 u = close.tpos[t];
                 for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
-                    const int64_t sp = close.src[c2];
-                    const int sl = close.leaf[c2];
-                    double cc[3] = {0.0, 0.0, 0.0}, rr = 1.0;
-                    if (sl != leaf) rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
-                    const double4 ps = close.spos[sp];
-                    const double yx = sl != leaf ? __fma_rn(rr, ps.x, cc[0]) : ps.x;
-                    const double yy = sl != leaf ? __fma_rn(rr, ps.y, cc[1]) : ps.y;
-                    const double yz = sl != leaf ? __fma_rn(rr, ps.z, cc[2]) : ps.z;
-                    if (u.x == yx && u.y == yy && u.z == yz) continue;
-                    const double dx = u.x - yx, dy = u.y - yy, dz = u.z - yz;
+                    const double4 y = close.y[c2];
+                    if (u.x == y.x && u.y == y.y && u.z == y.z) continue;
+                    const double dx = u.x - y.x, dy = u.y - y.y, dz = u.z - y.z;
                     const double r2 = dx * dx + dy * dy + dz * dz;
                     const double rinv = rsqrt(r2);
-                    const double qr = close.q[(int64_t)v * nsrc + sp] * rinv;
+                    const double qr = close.q[(int64_t)v * nsrc + close.src[c2]] * rinv;
                     aphi += qr;
                     if (GRAD) {
                         const double qr3 = qr * rinv * rinv;
