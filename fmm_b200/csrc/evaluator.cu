@@ -748,10 +748,10 @@ struct Evaluator final : EvaluatorBase {
     void leaf_far(int64_t r0, int64_t r1, int mode) {  // L2P / M2P of leaves [r0, r1)
         if (r1 <= r0) return;
         if (gradients)
-            leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), 64, NC * sizeof(T), stream>>>(
+            leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), 64, sizeof(T) == 8 ? NC * sizeof(T) : 0, stream>>>(
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
         else
-            leaf_far_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 64, NC * sizeof(T), stream>>>(
+            leaf_far_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 64, sizeof(T) == 8 ? NC * sizeof(T) : 0, stream>>>(
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
     }
 

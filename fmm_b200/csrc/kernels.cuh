@@ -502,8 +502,12 @@ __global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int64_t leaf
                                                       const T* __restrict__ M, const T* __restrict__ Lc,
                                                       double* __restrict__ far_phi, double* __restrict__ far_g) {
     constexpr int NC = nc_of(P);
+    // f32: the expansions are read straight from global memory (every thread reads the same
+    // coefficient at the same time: one broadcast through L1, no block barrier); f64 stages
+    // each expansion in shared memory (measured faster for 8-byte coefficients)
+    constexpr bool kStage = sizeof(T) == 8;
     extern __shared__ unsigned char smem_raw[];
-    T* C = reinterpret_cast<T*>(smem_raw);  // [NC]
+    T* C = reinterpret_cast<T*>(smem_raw);  // [NC] when staged
     const int64_t leaf = leaf0 + blockIdx.x;
     const int box = plan.leaf_box[leaf];
     const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
@@ -529,11 +533,15 @@ __global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int64_t leaf
             }
             // L2P, unit frame
             if (mode & 1) {
-                for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Lc[((int64_t)box * m + v) * NC + k];
-                __syncthreads();
+                const T* Lb = Lc + ((int64_t)box * m + v) * NC;
+                if (kStage) {
+                    for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Lb[k];
+                    __syncthreads();
+                    Lb = C;
+                }
                 if (valid) {
                     T ph, gx, gy, gz;
-                    l2p_eval<P, T, GRAD>(C, ux, uy, uz, ph, gx, gy, gz);
+                    l2p_eval<P, T, GRAD>(Lb, ux, uy, uz, ph, gx, gy, gz);
                     fphi = (mode & 4) ? fphi + (double)ph : (double)ph;
                     if (GRAD) {
                         fg[0] = (mode & 4) ? fg[0] + (double)gx : (double)gx;
@@ -541,19 +549,24 @@ __global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int64_t leaf
                         fg[2] = (mode & 4) ? fg[2] + (double)gz : (double)gz;
                     }
                 }
-                __syncthreads();
+                if (kStage) __syncthreads();
             }
             // M2P over the W list, frame (c(s|t), r(s|t))
             for (int64_t e = w0; e < w1; ++e) {
                 int s = plan.w_col[e];
-                for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = M[((int64_t)s * m + v) * NC + k];
-                __syncthreads();
+                const T* Mb = M + ((int64_t)s * m + v) * NC;
+                if (kStage) {
+                    for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Mb[k];
+                    __syncthreads();
+                    Mb = C;
+                }
                 if (valid) {
                     T c[3], r;
                     rel_frame<T>(plan, s, box, c, r);
                     T rinv = T(1) / r;
                     T ph, gx, gy, gz;
-                    m2p_eval<P, T, GRAD>(C, (ux - c[0]) * rinv, (uy - c[1]) * rinv, (uz - c[2]) * rinv, ph, gx, gy, gz);
+                    m2p_eval<P, T, GRAD>(Mb, (ux - c[0]) * rinv, (uy - c[1]) * rinv, (uz - c[2]) * rinv, ph, gx,
+                                         gy, gz);
                     fphi += (double)(ph * rinv);
                     if (GRAD) {
                         T r2inv = rinv * rinv;
@@ -562,7 +575,7 @@ __global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int64_t leaf
                         fg[2] += (double)(gz * r2inv);
                     }
                 }
-                __syncthreads();
+                if (kStage) __syncthreads();
             }
             if (valid) {
                 far_phi[(int64_t)v * nt + t] = fphi;
