@@ -11,7 +11,8 @@ in, potentials and gradients out.
 
 value     : N / (device time of one evaluation) in Mpoints/s, inputs resident in HBM,
             L2 flushed (a 512 MiB write) before every timed step, CUDA events on the
-            evaluator's stream.
+            evaluator's stream; the evaluation replayed from one captured CUDA graph of the
+            whole sweep (fmmgpu_fmm_set_graph; direct launches reported beside it).
 e2e       : the same through the public host API (fmmgpu_fmm_evaluate) with pinned host
             buffers, host->device charges and device->host outputs inside the timed call.
 plain_f64 : the plain f64 evaluator (the drop-in) on the same input, for the mixed/plain
@@ -255,24 +256,26 @@ def run_ours(args):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
+    # the product's repeated-evaluation mode: the whole sweep replayed from one captured
+    # CUDA graph (the same kernels and floats as direct launches, one launch from the host)
+    fmm.set_graph(True)
     with Clocks(local) as clk:
         ms = device_steps(fmm, args.steps, args.warmup)
     clocks = clk.summary()
+    fmm.set_graph(False)
     launches_per_step = fmm.info()["launches"]  # counted by the evaluator on its last evaluation
     log(f"timed: {ms:.3f} ms/step, {launches_per_step} launches per step")
     if world > 1:
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
-    # the same steps replayed from one CUDA graph of the whole sweep
-    fmm.set_graph(True)
-    graph_ms = device_steps(fmm, args.steps, args.warmup)
-    fmm.set_graph(False)
-    log(f"graph: {graph_ms:.3f} ms/step")
+    # the same steps with every kernel launched directly from the host
+    direct_ms = device_steps(fmm, args.steps, args.warmup)
+    log(f"direct launches: {direct_ms:.3f} ms/step")
     if world > 1:
-        t = torch.tensor([graph_ms], device=dev)
+        t = torch.tensor([direct_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        graph_ms = float(t.item())
+        direct_ms = float(t.item())
     # per-kind split and the dominant kernel (separate, untimed evaluation)
     fmm.set_kind_timing(True)
     stream = torch.cuda.ExternalStream(fmm.stream)
@@ -297,6 +300,7 @@ def run_ours(args):
     hq = torch.from_numpy(q).pin_memory()
     hphi = torch.empty(n, dtype=torch.float64).pin_memory()
     hg = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+    fmm.set_graph(True)  # the host API in the same repeated-evaluation mode
     for _ in range(max(1, args.warmup)):
         F._check(F.lib().fmmgpu_fmm_evaluate(fmm._h, hq.data_ptr(), hphi.data_ptr(), hg.data_ptr()))
     t0 = time.perf_counter()
@@ -305,9 +309,11 @@ def run_ours(args):
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     fmm.close()
     log(f"e2e {e2e_ms:.3f} ms")
-    # the plain f64 evaluator on the same input
+    # the plain f64 evaluator on the same input, in the same graph mode
     plain = build("f64")
+    plain.set_graph(True)
     plain_ms = device_steps(plain, max(2, args.steps // 2), max(1, args.warmup // 2))
+    plain.set_graph(False)
     with torch.cuda.stream(torch.cuda.ExternalStream(plain.stream)):
         plain.evaluate_device(dq.data_ptr(), dphi.data_ptr(), dg.data_ptr())
     plain.synchronize()
@@ -364,8 +370,9 @@ def run_ours(args):
                   "against": "f64 direct sum (GPU, Neumaier)", "plain_f64_phi_rel_l2": perr},
         "plain_f64": {"ms_per_step": round(plain_ms, 4), "value": round(n / (plain_ms * 1e-3) / 1e6, 3),
                       "mixed_over_plain": round(plain_ms / ms, 3)},
-        "graph": {"ms_per_step": round(graph_ms, 4), "value": round(world * n / (graph_ms * 1e-3) / 1e6, 3),
-                  "note": "the same evaluation replayed from one captured CUDA graph"},
+        "direct_launches": {"ms_per_step": round(direct_ms, 4),
+                            "value": round(world * n / (direct_ms * 1e-3) / 1e6, 3),
+                            "note": "the same evaluation with every kernel launched from the host (no graph)"},
         "kinds_ms": {k: round(v, 4) for k, v in kinds.items()},
         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs",
                                       "x_pairs", "device_bytes", "close_pairs")},

@@ -55,7 +55,7 @@ __global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec* __res
 
 constexpr int kX2Warps = 4;
 constexpr int kX2Stage = 128;  // sources per flush (64 pairs)
-constexpr int kX2Recs = 64;    // a near row's entries, all in shared memory (2:1 balance: at most 57)
+constexpr int kX2Recs = 58;    // a near row's entries, all in shared memory (2:1 balance: at most 57)
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
@@ -74,7 +74,7 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 // computed, the raw points and charges of flush f + 1 are in flight (cp.async), so a
 // warp does not wait on global memory for its sources.
 template <bool GRAD>
-__global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
+__global__ void __launch_bounds__(32 * kX2Warps, 8) p2p_x2_kernel(
     DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
     const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
     double* __restrict__ far_phi, double* __restrict__ far_g, int accumulate, double* __restrict__ out_phi,
@@ -85,8 +85,10 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
     __shared__ float rawq[kX2Warps][kX2Stage];
     __shared__ int rawrec[kX2Warps][kX2Stage];      // their near entries
     __shared__ NearRec srec[kX2Warps][kX2Recs];
-    __shared__ double red[kX2Warps][4][32];  // the split lanes' sums, reduced per target
+    // 27.3 KB a block: eight blocks (32 warps) fit on an SM
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the split lanes' sums, reduced per target, in the pair buffer (idle at that point)
+    double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[warp][0]);
     const int64_t item = (int64_t)blockIdx.x * kX2Warps + warp;
     if (item >= items.count) return;
     const int leaf = items.leaf[item];
@@ -209,17 +211,17 @@ __global__ void __launch_bounds__(32 * kX2Warps, 6) p2p_x2_kernel(
         if (f - v * nfl != nfl - 1) continue;
         // ---- the last flush of vector v: finish its targets ----
         if (K > 1) {  // the target's K partial sums, in kk order
-            red[warp][0][lane] = aphi;
-            red[warp][1][lane] = ag0;
-            red[warp][2][lane] = ag1;
-            red[warp][3][lane] = ag2;
+            red[0][lane] = aphi;
+            red[1][lane] = ag0;
+            red[2][lane] = ag1;
+            red[3][lane] = ag2;
             __syncwarp();
             if (valid)
                 for (int j = 1; j < K; ++j) {
-                    aphi += red[warp][0][ti + ni * j];
-                    ag0 += red[warp][1][ti + ni * j];
-                    ag1 += red[warp][2][ti + ni * j];
-                    ag2 += red[warp][3][ti + ni * j];
+                    aphi += red[0][ti + ni * j];
+                    ag0 += red[1][ti + ni * j];
+                    ag1 += red[2][ti + ni * j];
+                    ag2 += red[3][ti + ni * j];
                 }
             __syncwarp();
         }
