@@ -187,6 +187,9 @@ struct Evaluator final : EvaluatorBase {
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
+    // boxes with a nonempty X list, level by level (the P2L launches)
+    DevBuf xbox;
+    std::vector<int64_t> xbox_start;
     // the near field summed apart on a second, lower-priority stream, joined by output_kernel
     DevBuf near_phi, near_g;
     cudaStream_t near_stream = nullptr;
@@ -287,6 +290,17 @@ struct Evaluator final : EvaluatorBase {
         build_m2l_batches(kGemmPairs);
         if (kTensor) build_tensor_m2l(m2l);
         build_p2p_items();
+        {
+            std::vector<int32_t> xb;
+            xbox_start.assign(pl.nlevels + 1, 0);
+            for (int l = 0; l < pl.nlevels; ++l) {
+                xbox_start[l] = (int64_t)xb.size();
+                for (int64_t b = pl.level_start[l]; b < pl.level_start[l + 1]; ++b)
+                    if (pl.x.row[b + 1] > pl.x.row[b]) xb.push_back((int32_t)b);
+            }
+            xbox_start[pl.nlevels] = (int64_t)xb.size();
+            xbox.upload(xb);
+        }
         int least = 0, greatest = 0;
         CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         CUDA_TRY(cudaStreamCreateWithPriority(&near_stream, cudaStreamNonBlocking, least));
@@ -583,7 +597,7 @@ struct Evaluator final : EvaluatorBase {
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
-                               &near_phi, &near_g, &box_side, &v_pos};
+                               &near_phi, &near_g, &box_side, &v_pos, &xbox};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -668,11 +682,11 @@ struct Evaluator final : EvaluatorBase {
         if (r1 <= r0) return;
         if (kBfly && m == 1)
             expand_bfly_kernel<P, false><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
-                dp, r0, r1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
+                dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
                 reinterpret_cast<float*>(M.ptr));
         else
             expand_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 32, exp_smem(), stream>>>(
-                dp, r0, r1, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
+                dp, r0, r1, nullptr, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
     }
 
     void m2m_level(int l) {  // parents on level l from their children on level l + 1
@@ -733,16 +747,16 @@ struct Evaluator final : EvaluatorBase {
                 Lc.as<T>());
     }
 
-    void p2l_level(int l) {
-        const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+    void p2l_level(int l) {  // the boxes of level l with an X list
+        const int64_t b0 = xbox_start[l], b1 = xbox_start[l + 1];
         if (b1 <= b0) return;
         if (kBfly && m == 1)
             expand_bfly_kernel<P, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
-                dp, b0, b1, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
-                reinterpret_cast<float*>(Lc.ptr));
+                dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr),
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
         else
             expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), stream>>>(
-                dp, b0, b1, m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
+                dp, b0, b1, xbox.as<int32_t>(), m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
     }
 
     void leaf_far(int64_t r0, int64_t r1, int mode) {  // L2P / M2P of leaves [r0, r1)

@@ -102,15 +102,17 @@ __global__ void charge_load_kernel(const double* __restrict__ q_caller, const in
 // ---------------------------------------------------------------------------------
 template <int P, typename T, bool IRREG>
 __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
-                                                    int m, const typename Vec4<T>::type* __restrict__ spos,
+                                                    const int32_t* __restrict__ rows, int m,
+                                                    const typename Vec4<T>::type* __restrict__ spos,
                                                     const T* __restrict__ sq, T* __restrict__ out) {
     constexpr int NC = nc_of(P);
     extern __shared__ unsigned char smem_raw[];
     T* S = reinterpret_cast<T*>(smem_raw);  // [NC][32]
     T* Q = S + NC * 32;                     // [m][32]
     const int lane = threadIdx.x;
-    const int64_t row = row_begin + blockIdx.x;
-    if (row >= row_end) return;
+    const int64_t idx = row_begin + blockIdx.x;  // rows[idx] when a row list is given
+    if (idx >= row_end) return;
+    const int64_t row = rows ? rows[idx] : idx;
     int box, nent;
     int64_t ent0;
     if (!IRREG) {  // row = leaf
@@ -195,13 +197,15 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
 // ---------------------------------------------------------------------------------
 template <int P, bool IRREG>
 __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
+                                                         const int32_t* __restrict__ rows,
                                                          const float4* __restrict__ spos,
                                                          const float* __restrict__ sq, float* __restrict__ out) {
     constexpr int NC = nc_of(P);
     constexpr int NCP = ((NC + 31) / 32) * 32;
     const int lane = threadIdx.x;
-    const int64_t row = row_begin + blockIdx.x;
-    if (row >= row_end) return;
+    const int64_t idx = row_begin + blockIdx.x;  // rows[idx] when a row list is given
+    if (idx >= row_end) return;
+    const int64_t row = rows ? rows[idx] : idx;
     int box, nent;
     int64_t ent0;
     if (!IRREG) {
