@@ -488,9 +488,9 @@ def run_reference(args):
         return
     times = []
     for _ in range(args.warmup):
-        cpu_baseline(args, args.cpu_n // 4)
+        cpu_baseline(args, args.ref_n // 4)
     for _ in range(args.steps):
-        b = cpu_baseline(args)
+        b = cpu_baseline(args, args.ref_n)
         times.append(b["value"])
     v = float(np.median(times))
     b["value"] = round(v, 4)
@@ -500,7 +500,7 @@ def run_reference(args):
         "value": v, "unit": "Mpoints/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded SplitMix64 sphere)",
-        "config": {"workload": f"laplace3d sphere p={P} leaf={LEAF} phi+grad, bounded sample N={args.cpu_n}"},
+        "config": {"workload": f"laplace3d sphere p={P} leaf={LEAF} phi+grad, bounded sample N={args.ref_n}"},
         "cpu_baseline": b,
         "e2e": {"value": v, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -513,7 +513,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
-    ap.add_argument("--cpu-n", type=int, default=400_000)
+    ap.add_argument("--cpu-n", type=int, default=N_DEFAULT, help="points of the CPU baseline's sample")
+    ap.add_argument("--ref-n", type=int, default=400_000, help="points of each reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (256 clouds) measurement")
     args = ap.parse_args()
