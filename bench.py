@@ -218,8 +218,9 @@ def run_ours(args):
     sample = sample_indices(n, SAMPLE)
 
     def build(precision):
+        # launch shapes timed at build (the results are the same bits for every shape)
         return (F.FmmBuilder(P).gradients().max_points_per_leaf(LEAF).precision(precision)
-                .device(local).build(x))
+                .device(local).autotune().build(x))
 
     log(f"problem n={n} generated")
     t0 = time.perf_counter()
@@ -311,6 +312,7 @@ def run_ours(args):
     log(f"e2e {e2e_ms:.3f} ms")
     # the plain f64 evaluator on the same input, in the same graph mode
     plain = build("f64")
+    plain_info = plain.info()
     plain.set_graph(True)
     plain_ms = device_steps(plain, max(2, args.steps // 2), max(1, args.warmup // 2))
     plain.set_graph(False)
@@ -377,6 +379,9 @@ def run_ours(args):
         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs",
                                       "x_pairs", "device_bytes", "close_pairs")},
         "build_s": round(build_s, 3),
+        "launch_shapes": {"p2p_warps": info["p2p_warps"], "leaf_block": info["leaf_block"],
+                          "plain_f64_leaf_block": plain_info["leaf_block"],
+                          "note": "timed at build (autotune); build_s includes it"},
         "e2e": {"value": round(n / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
                 "ms_per_step": round(e2e_ms, 4),
                 "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8 * 4},
@@ -436,7 +441,7 @@ def run_batched(F, torch, dev, flush, steps=3, warmup=1):
     for precision in ("mixed", "f64"):
         t0 = time.perf_counter()
         f = (F.FmmBuilder(BATCH_P).vectors(m).max_points_per_leaf(BATCH_LEAF).precision(precision)
-             .build_batch(clouds))
+             .autotune().build_batch(clouds))
         build_s = time.perf_counter() - t0
         info = f.info()
         ms = timed(f)
@@ -445,6 +450,7 @@ def run_batched(F, torch, dev, flush, steps=3, warmup=1):
             res.update({"ms_per_step": round(ms, 3), "value": round(n / (ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
                         "point_vectors_per_s": round(n * m / (ms * 1e-3) / 1e6, 1), "build_s": round(build_s, 2),
                         "launches_per_step": f.info()["launches"],
+                        "launch_shapes": {"p2p_warps": info["p2p_warps"], "leaf_block": info["leaf_block"]},
                         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs")}})
             # error of vector 0 at 250 sampled targets in each of the first 4 clouds
             phi = dphi.view(m, n)[0].cpu().numpy()

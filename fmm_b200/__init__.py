@@ -34,7 +34,7 @@ class FmmError(RuntimeError):
 class Settings(C.Structure):
     _fields_ = [("p", C.c_int), ("precision", C.c_int), ("gradients", C.c_int), ("vectors", C.c_int),
                 ("max_points_per_leaf", C.c_int), ("max_level", C.c_int), ("device", C.c_int),
-                ("vectors_per_pass", C.c_int)]
+                ("vectors_per_pass", C.c_int), ("autotune", C.c_int)]
 
 
 class Info(C.Structure):
@@ -42,7 +42,7 @@ class Info(C.Structure):
                 ("nsources", C.c_int64), ("ntargets", C.c_int64), ("near_pairs", C.c_int64),
                 ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
                 ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64),
-                ("vectors_per_pass", C.c_int64)]
+                ("vectors_per_pass", C.c_int64), ("p2p_warps", C.c_int64), ("leaf_block", C.c_int64)]
 
 
 def lib():
@@ -75,6 +75,8 @@ def lib():
             "fmmgpu_fmm_set_graph": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_overlap": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_autotune": (C.c_int, [vp, dp, dp]),
+            "fmmgpu_fmm_set_launch_shapes": (C.c_int, [vp, C.c_int, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
@@ -172,6 +174,11 @@ class FmmBuilder:
     def vectors_per_pass(self, n):
         """Charge vectors per device pass (0: as many as fit); the results do not depend on it."""
         self._s.vectors_per_pass = int(n)
+        return self
+
+    def autotune(self, on=True):
+        """Time the launch shapes at build and keep the fastest (the results are the same bits)."""
+        self._s.autotune = int(bool(on))
         return self
 
     def max_level(self, level):
@@ -361,6 +368,19 @@ class Fmm(Plan):
     def set_graph(self, on=True):
         """Replay later evaluations from one captured CUDA graph of the whole sweep."""
         _check(lib().fmmgpu_fmm_set_graph(self._h, int(on)))
+
+    def autotune(self, charges):
+        """Times the launch shapes that change no result on this plan and keeps the fastest;
+        returns {"p2p_warps": w, "leaf_block": b}.  Drops a captured graph."""
+        m = self.settings.vectors
+        q = np.ascontiguousarray(charges, dtype=np.float64).reshape(self.nsources, m)
+        choice = np.zeros(2, dtype=np.int32)
+        _check(lib().fmmgpu_fmm_autotune(self._h, _ptr(q), _ptr(choice)))
+        return {"p2p_warps": int(choice[0]), "leaf_block": int(choice[1])}
+
+    def set_launch_shapes(self, p2p_warps, leaf_block):
+        """Sets the shapes autotune chooses (e.g. a stored choice): 1, 2 or 4 and 32, 64 or 128."""
+        _check(lib().fmmgpu_fmm_set_launch_shapes(self._h, int(p2p_warps), int(leaf_block)))
 
     def set_kinds(self, kinds):
         """Test hook: bit 0 near field, bit 1 far field (3, the default, is the FMM)."""

@@ -137,6 +137,10 @@ struct EvaluatorBase {
     int qstride = 1;       // charges per point in the caller's array (all vectors)
     bool first_pass = true;  // vectors run in passes: the first one resets timing and counts
     bool overlap = false;  // near field on its own stream beside the far field (measured: no gain)
+    // launch shapes the autotuner may change: warps a block of the mixed P2P kernel
+    // (1, 2 or 4) and threads a block of the L2P / M2P kernel (32, 64 or 128)
+    int p2p_warps = kX2Warps;
+    int leaf_block = 64;
     unsigned counted(unsigned grid) {  // wraps the grid of every evaluation launch
         ++launches;
         return grid;
@@ -147,6 +151,7 @@ struct EvaluatorBase {
     virtual void op_level(int kind, int level) = 0;
     virtual void op_output(double* d_phi, double* d_grad) = 0;
     virtual void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
+    virtual void autotune(const double* d_charges, double* d_phi, double* d_grad) = 0;
 };
 
 template <int P, typename T>
@@ -642,6 +647,58 @@ struct Evaluator final : EvaluatorBase {
         CUDA_TRY(cudaGetLastError());
     }
 
+    // Times the launch shapes that change no float (every P2P target and every L2P / M2P
+    // target sums the same terms in the same order whatever the block) on this plan and
+    // device, and keeps the fastest: warps a block of the mixed P2P kernel, threads a block
+    // of the L2P / M2P kernel.  One evaluation first leaves the far partials in place; the
+    // P2P launches with accumulate 0 only read them and rewrite the output, the L2P / M2P
+    // launches rewrite the same partials.  A last evaluation leaves the output and the
+    // launch count as a plain evaluation does.
+    void autotune(const double* d_charges, double* d_phi, double* d_grad) override {
+        const bool timing = timer.on;
+        timer.on = false;
+        first_pass = true;
+        evaluate(d_charges, d_phi, d_grad);
+        cudaEvent_t e0, e1;
+        CUDA_TRY(cudaEventCreate(&e0));
+        CUDA_TRY(cudaEventCreate(&e1));
+        auto time = [&](auto&& launch) {
+            launch();  // warm-up
+            CUDA_TRY(cudaEventRecord(e0, stream));
+            for (int r = 0; r < 3; ++r) launch();
+            CUDA_TRY(cudaEventRecord(e1, stream));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            return ms;
+        };
+        if (kMixed && items.count) {
+            float best = 0.f;
+            int pick = p2p_warps;
+            for (int w : {1, 2, 4}) {
+                p2p_warps = w;
+                const float ms = time([&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
+                if (w == 1 || ms < best) best = ms, pick = w;
+            }
+            p2p_warps = pick;
+        }
+        if (plan.nleaves() && (kinds & 2)) {
+            float best = 0.f;
+            int pick = leaf_block;
+            for (int b : {32, 64, 128}) {
+                leaf_block = b;
+                const float ms = time([&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+                if (b == 32 || ms < best) best = ms, pick = b;
+            }
+            leaf_block = pick;
+        }
+        CUDA_TRY(cudaEventDestroy(e0));
+        CUDA_TRY(cudaEventDestroy(e1));
+        timer.on = timing;
+        first_pass = true;
+        evaluate(d_charges, d_phi, d_grad);
+    }
+
     void output(double* d_phi, double* d_grad, bool with_near) {
         if (plan.nleaves())
             output_kernel<<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
@@ -761,12 +818,30 @@ struct Evaluator final : EvaluatorBase {
 
     void leaf_far(int64_t r0, int64_t r1, int mode) {  // L2P / M2P of leaves [r0, r1)
         if (r1 <= r0) return;
+        const size_t smem = sizeof(T) == 8 ? NC * sizeof(T) : 0;
         if (gradients)
-            leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), 64, sizeof(T) == 8 ? NC * sizeof(T) : 0, stream>>>(
+            leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), leaf_block, smem, stream>>>(
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
         else
-            leaf_far_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 64, sizeof(T) == 8 ? NC * sizeof(T) : 0, stream>>>(
+            leaf_far_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), leaf_block, smem, stream>>>(
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+    }
+
+    template <int W>
+    void p2p_x2_launch(const P2pItems& it, int near, int accumulate, double* d_phi, double* fg, double* og,
+                       cudaStream_t s) {
+        const unsigned g = (unsigned)((it.count + W - 1) / W);
+        const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
+        const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
+        const auto* q = reinterpret_cast<const float*>(sq.ptr);
+        if (gradients)
+            p2p_x2_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp,
+                                                               q, tp, close, far_phi.as<double>(), fg, accumulate,
+                                                               d_phi, og);
+        else
+            p2p_x2_kernel<false, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(),
+                                                                sp, q, tp, close, far_phi.as<double>(), fg,
+                                                                accumulate, d_phi, og);
     }
 
     // P2P over work items [i0, i1); accumulate = 0 adds the far partial and writes the
@@ -780,18 +855,12 @@ struct Evaluator final : EvaluatorBase {
         double* fg = gradients ? far_g.as<double>() : nullptr;
         double* og = gradients ? d_grad : nullptr;
         if constexpr (kMixed) {
-            const unsigned g = (unsigned)((it.count + kX2Warps - 1) / kX2Warps);
-            const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
-            const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
-            const auto* q = reinterpret_cast<const float*>(sq.ptr);
-            if (gradients)
-                p2p_x2_kernel<true><<<counted(g), 32 * kX2Warps, 0, s>>>(
-                    dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(), fg,
-                    accumulate, d_phi, og);
+            if (p2p_warps == 1)
+                p2p_x2_launch<1>(it, near, accumulate, d_phi, fg, og, s);
+            else if (p2p_warps == 2)
+                p2p_x2_launch<2>(it, near, accumulate, d_phi, fg, og, s);
             else
-                p2p_x2_kernel<false><<<counted(g), 32 * kX2Warps, 0, s>>>(
-                    dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q, tp, close, far_phi.as<double>(), fg,
-                    accumulate, d_phi, og);
+                p2p_x2_launch<4>(it, near, accumulate, d_phi, fg, og, s);
         } else {
             const unsigned g = (unsigned)((it.count + kP2pWarps - 1) / kP2pWarps);
             if (gradients)
@@ -1050,6 +1119,7 @@ void fmmgpu_default_settings(fmmgpu_settings* s) {
     s->max_level = 16;
     s->device = 0;
     s->vectors_per_pass = 0;
+    s->autotune = 0;
 }
 
 namespace {
@@ -1058,7 +1128,7 @@ void check_settings(const fmmgpu_settings* settings) {
     if (!settings) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
     const fmmgpu_settings& s = *settings;
     if (s.p < 0 || s.vectors < 1 || s.max_points_per_leaf < 1 || s.max_level < 0 || s.max_level > 16 ||
-        s.vectors_per_pass < 0)
+        s.vectors_per_pass < 0 || s.autotune < 0 || s.autotune > 1)
         throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid settings");
     if (s.precision != FMMGPU_PRECISION_F64 && s.precision != FMMGPU_PRECISION_MIXED)
         throw Failure(FMMGPU_UNSUPPORTED, "unknown precision");
@@ -1209,6 +1279,14 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
     f->d_phi.alloc(sizeof(double) * (size_t)s.vectors * (nt + 1));
     if (s.gradients) f->d_grad.alloc(sizeof(double) * 3 * (size_t)s.vectors * (nt + 1));
     f->device_bytes = bytes + f->d_charges.bytes + f->d_phi.bytes + f->d_grad.bytes;
+    if (s.autotune) {
+        // the launch shapes timed on this plan with zero charges: the charges change no
+        // branch and no launch, so they time as any others
+        CUDA_TRY(cudaMemsetAsync(f->d_charges.ptr, 0, f->d_charges.bytes, f->stream));
+        f->eval->autotune(f->d_charges.as<double>(), f->d_phi.as<double>(),
+                          s.gradients ? f->d_grad.as<double>() : nullptr);
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    }
     CUDA_TRY(cudaDeviceSynchronize());
 }
 
@@ -1496,6 +1574,41 @@ int fmmgpu_fmm_set_graph(fmmgpu_fmm* f, int on) {
     });
 }
 
+int fmmgpu_fmm_autotune(fmmgpu_fmm* f, const double* charges, int* choice) {
+    return guarded([&] {
+        if (!f || !charges) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors, ns = f->plan.src_perm.size();
+        CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, f->stream));
+        f->drop_graph();
+        f->eval->autotune(f->d_charges.as<double>(), f->d_phi.as<double>(),
+                          f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        CUDA_TRY(cudaGetLastError());
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+        if (choice) {
+            choice[0] = f->eval->p2p_warps;
+            choice[1] = f->eval->leaf_block;
+        }
+    });
+}
+
+int fmmgpu_fmm_set_launch_shapes(fmmgpu_fmm* f, int p2p_warps, int leaf_block) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        if (p2p_warps != 1 && p2p_warps != 2 && p2p_warps != 4)
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "p2p_warps must be 1, 2 or 4");
+        if (leaf_block != 32 && leaf_block != 64 && leaf_block != 128)
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "leaf_block must be 32, 64 or 128");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->eval->p2p_warps = p2p_warps;
+        f->eval->leaf_block = leaf_block;
+        f->drop_graph();
+    });
+}
+
 int fmmgpu_fmm_kind_times(fmmgpu_fmm* f, double* ms) {
     return guarded([&] {
         if (!f || !f->eval || !ms) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
@@ -1531,6 +1644,8 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->close_pairs = f->eval ? f->eval->close_pairs : 0;
         info->launches = f->eval ? f->eval->launches : 0;
         info->vectors_per_pass = f->eval ? f->mpass : 0;
+        info->p2p_warps = f->eval ? f->eval->p2p_warps : 0;
+        info->leaf_block = f->eval ? f->eval->leaf_block : 0;
     });
 }
 

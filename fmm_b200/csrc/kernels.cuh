@@ -501,7 +501,7 @@ __device__ __forceinline__ void m2p_eval(const T* M, T x, T y, T z, T& phi, T& g
 // The evaluation runs mode 3; the level calls run 5 (L2P) then 6 (M2P) on stores that
 // start at zero, which gives the same floats.
 template <int P, typename T, bool GRAD>
-__global__ void __launch_bounds__(64) leaf_far_kernel(DevPlan plan, int64_t leaf0, int mode, int m,
+__global__ void __launch_bounds__(128) leaf_far_kernel(DevPlan plan, int64_t leaf0, int mode, int m,
                                                       const typename Vec4<T>::type* __restrict__ tpos,
                                                       const T* __restrict__ M, const T* __restrict__ Lc,
                                                       double* __restrict__ far_phi, double* __restrict__ far_g) {

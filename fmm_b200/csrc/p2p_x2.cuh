@@ -53,7 +53,7 @@ __global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec* __res
     }
 }
 
-constexpr int kX2Warps = 4;
+constexpr int kX2Warps = 4;      // warps a block until the autotuner chooses
 constexpr int kX2Stage = 128;  // sources per flush (64 pairs)
 constexpr int kX2Recs = 58;    // a near row's entries, all in shared memory (2:1 balance: at most 57)
 
@@ -73,23 +73,24 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 // Flushes run over (vector, position in the row's source stream); while flush f is
 // computed, the raw points and charges of flush f + 1 are in flight (cp.async), so a
 // warp does not wait on global memory for its sources.
-template <bool GRAD>
-__global__ void __launch_bounds__(32 * kX2Warps, 8) p2p_x2_kernel(
+// W warps a block (1, 2 or 4; the autotuner picks one): 6.8 KB of shared memory and
+// at most 64 registers a thread, so 32 warps are resident on an SM for every W.
+template <bool GRAD, int W>
+__global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
     DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
     const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
     double* __restrict__ far_phi, double* __restrict__ far_g, int accumulate, double* __restrict__ out_phi,
     double* __restrict__ out_g) {
-    __shared__ float4 sxy[kX2Warps][kX2Stage / 2];  // (x0, x1, y0, y1) in the target's frame
-    __shared__ float4 szq[kX2Warps][kX2Stage / 2];  // (z0, z1, q0, q1)
-    __shared__ float4 raw[kX2Warps][kX2Stage];      // the next flush's points, as loaded
-    __shared__ float rawq[kX2Warps][kX2Stage];
-    __shared__ int rawrec[kX2Warps][kX2Stage];      // their near entries
-    __shared__ NearRec srec[kX2Warps][kX2Recs];
-    // 27.3 KB a block: eight blocks (32 warps) fit on an SM
+    __shared__ float4 sxy[W][kX2Stage / 2];  // (x0, x1, y0, y1) in the target's frame
+    __shared__ float4 szq[W][kX2Stage / 2];  // (z0, z1, q0, q1)
+    __shared__ float4 raw[W][kX2Stage];      // the next flush's points, as loaded
+    __shared__ float rawq[W][kX2Stage];
+    __shared__ int rawrec[W][kX2Stage];      // their near entries
+    __shared__ NearRec srec[W][kX2Recs];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // the split lanes' sums, reduced per target, in the pair buffer (idle at that point)
     double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[warp][0]);
-    const int64_t item = (int64_t)blockIdx.x * kX2Warps + warp;
+    const int64_t item = (int64_t)blockIdx.x * W + warp;
     if (item >= items.count) return;
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];

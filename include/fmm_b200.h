@@ -60,6 +60,10 @@ typedef struct {
     int vectors_per_pass;     /* charge vectors per device pass: 0 (default) as many as fit in
                                  60% of the free device memory; rounded down to a divisor of
                                  `vectors`; the results do not depend on it */
+    int autotune;             /* 1: time the launch shapes at build and keep the fastest
+                                 (fmm-exec/src/fmm.rs:291-300, FmmBuilder::tuning_cache, with
+                                 no cache file); 0 (default): the static shapes.  The results
+                                 are the same bits either way */
 } fmmgpu_settings;
 
 typedef struct {
@@ -72,6 +76,8 @@ typedef struct {
     int64_t close_pairs;  /* near-singular P2P pairs the mixed form evaluates in f64 */
     int64_t launches;     /* kernels the last evaluation launched (0 before the first) */
     int64_t vectors_per_pass;  /* charge vectors per device pass (0 for a plan-only handle) */
+    int64_t p2p_warps;    /* warps a block of the mixed P2P kernel (static 4, or the tuned one) */
+    int64_t leaf_block;   /* threads a block of the L2P / M2P kernel (static 64, or the tuned one) */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;
@@ -148,6 +154,22 @@ int fmmgpu_fmm_set_graph(fmmgpu_fmm* fmm, int on);
  * pipes and the overlap measured no faster).  Per-kind timing always runs on one stream.
  * Synchronises. */
 int fmmgpu_fmm_set_overlap(fmmgpu_fmm* fmm, int on);
+
+/* Times the launch shapes that change no result on this handle's plan and device and
+ * keeps the fastest (the reference's build-time tuner, fmm-exec/src/tune.rs:1-60, with
+ * the P2P layout decision as the block of the mixed P2P kernel, 1, 2 or 4 warps, and the
+ * L2P / M2P block, 32, 64 or 128 threads).  `charges` as fmmgpu_fmm_evaluate's (host);
+ * the handle's device outputs then hold their evaluation.  choice (may be NULL) receives
+ * {p2p warps, leaf block}.  Every target sums the same terms in the same order whatever
+ * the shape, so later evaluations give the same bits as before.  Drops a captured graph.
+ * Synchronises. */
+int fmmgpu_fmm_autotune(fmmgpu_fmm* fmm, const double* charges, int* choice);
+
+/* Sets the launch shapes fmmgpu_fmm_autotune chooses (a choice kept from an earlier
+ * tuning, as the reference's tuning cache keeps one, fmm-exec/src/fmm.rs:291-300):
+ * p2p_warps 1, 2 or 4; leaf_block 32, 64 or 128.  The results are the same bits for
+ * every pair.  Drops a captured graph.  Synchronises. */
+int fmmgpu_fmm_set_launch_shapes(fmmgpu_fmm* fmm, int p2p_warps, int leaf_block);
 
 /* Per-kind device timing of the following evaluations (the reference's KindTiming,
  * fmm-exec/src/fmm.rs:150-153): every launch is bracketed by CUDA events. */

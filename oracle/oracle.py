@@ -247,9 +247,6 @@ def point_sets(kind, n, seed):
     st = C.c_uint64(seed)
     xyz = np.zeros(3 * n)
     c = np.array([0.5, 0.5, 0.5])
-    fns = {
-        "cube": ("orc_points_cube", [c.ctypes.data_as(C.c_void_p), C.c_double(0.5)]),
-    }
     if kind == "cube":
         f = L.orc_points_cube
         f.argtypes = [C.c_void_p, _sz, _dp, C.c_double, _dp]
@@ -260,7 +257,6 @@ def point_sets(kind, n, seed):
         f(C.byref(st), n, np.zeros(3), 1.0, xyz)
     else:
         raise ValueError(kind)
-    del fns
     q = np.zeros(n)
     L.orc_charges.argtypes = [C.c_void_p, _sz, _dp]
     L.orc_charges(C.byref(st), n, q)

@@ -57,3 +57,34 @@ def test_overlapped_near_field_equals_one_stream(oracle, precision, m):
     for _ in range(2):
         c = fmm.evaluate(q)
         assert np.array_equal(c.potential, b.potential) and np.array_equal(c.gradient, b.gradient)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_launch_shapes_change_speed_only(oracle, precision):
+    """Every launch shape the autotuner may pick (P2P warps a block, L2P / M2P threads a
+    block) gives the same bits, and so do the tuned handle and a handle tuned at build."""
+    x, q = oracle.point_sets("sphere", 30000, 4)
+    builder = F.FmmBuilder(6).gradients().max_points_per_leaf(32).precision(precision)
+    fmm = builder.build(x)
+    want = fmm.evaluate(q)
+    assert (fmm.info()["p2p_warps"], fmm.info()["leaf_block"]) == (4, 64)
+    for w in (1, 2, 4):
+        for b in (32, 64, 128):
+            fmm.set_launch_shapes(w, b)
+            got = fmm.evaluate(q)
+            assert np.array_equal(got.potential, want.potential), (w, b)
+            assert np.array_equal(got.gradient, want.gradient), (w, b)
+    with pytest.raises(F.FmmError):
+        fmm.set_launch_shapes(3, 64)
+    choice = fmm.autotune(q)
+    assert choice["p2p_warps"] in (1, 2, 4) and choice["leaf_block"] in (32, 64, 128)
+    assert (fmm.info()["p2p_warps"], fmm.info()["leaf_block"]) == (choice["p2p_warps"], choice["leaf_block"])
+    fmm.set_graph(True)
+    for _ in range(2):
+        got = fmm.evaluate(q)
+        assert np.array_equal(got.potential, want.potential) and np.array_equal(got.gradient, want.gradient)
+    tuned = builder.autotune().build(x)
+    got = tuned.evaluate(q)
+    assert np.array_equal(got.potential, want.potential) and np.array_equal(got.gradient, want.gradient)
+    fmm.close()
+    tuned.close()
