@@ -387,7 +387,8 @@ class Fmm(Plan):
         _check(lib().fmmgpu_fmm_set_kinds(self._h, int(kinds)))
 
     def set_m2l_path(self, path):
-        """Test hook: 1 tensor-core M2L (mixed, p <= 8; the default), 0 SIMT M2L."""
+        """M2L path (mixed, p <= 8): 1 tensor-core products then the reduce (the default),
+        2 tensor-core M2L fused with the reduce (the same bits), 0 SIMT products."""
         _check(lib().fmmgpu_fmm_set_m2l_path(self._h, int(path)))
 
     def kind_times(self):

@@ -16,6 +16,7 @@
 #include "../../include/fmm_b200.h"
 #include "kernels.cuh"
 #include "m2l_tc.cuh"
+#include "m2l_fused.cuh"
 #include "helmholtz.cuh"
 #include "p2p_x2.cuh"
 #include "plan.hpp"
@@ -129,7 +130,9 @@ struct KindTimer {
 // ----------------------------------------------------------------------------------
 struct EvaluatorBase {
     KindTimer timer;
-    int m2l_path = 1;  // 1: tensor cores where the form has them (mixed, p <= 8), 0: SIMT
+    // M2L: 1 tensor-core products then the reduce (mixed, p <= 8: the default there),
+    // 2 tensor cores fused with the local reduce (an option), 0 SIMT products then the reduce
+    int m2l_path = 0;
     virtual int device_status() { return 0; }
     int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
@@ -152,6 +155,7 @@ struct EvaluatorBase {
     virtual void op_output(double* d_phi, double* d_grad) = 0;
     virtual void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
     virtual void autotune(const double* d_charges, double* d_phi, double* d_grad) = 0;
+    virtual void set_m2l_path(int path) = 0;
 };
 
 template <int P, typename T>
@@ -189,6 +193,14 @@ struct Evaluator final : EvaluatorBase {
     std::vector<int64_t> tc_lvl_tiles;
     int64_t tc_ntiles = 0;
     int num_sms = 148;
+    // fused tensor-core M2L: per level, chunks of consecutive target boxes cut into tiles
+    // of one offset (pairs in (chunk, offset, target) order), CTA c of level l taking the
+    // tiles fu_cta[fu_lvl_cta[l] + c] .. fu_cta[fu_lvl_cta[l] + c + 1]
+    DevBuf fu_tile_d, fu_tile_begin, fu_tile_np, fu_cta, fu_pair_src, fu_pair_tgt, fu_img;
+    std::vector<int64_t> fu_lvl_cta;
+    std::vector<int> fu_lvl_grid;
+    bool product_path_built = false;  // the product paths' tiles and Y (built on first use)
+    std::vector<uint32_t> tc_img;     // host copy of the tensor-memory table images
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
@@ -211,7 +223,7 @@ struct Evaluator final : EvaluatorBase {
 
     Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
               const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
-              const std::vector<double>& ut)
+              const std::vector<double>& ut, bool fused)
         : plan(pl), stream(s), m(m_), gradients(grad) {
         timer.stream = s;
         level.upload(pl.level);
@@ -292,8 +304,14 @@ struct Evaluator final : EvaluatorBase {
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
         build_parent_lists();
-        build_m2l_batches(kGemmPairs);
         if (kTensor) build_tensor_m2l(m2l);
+        if (kTensor && fused && m <= fused_tile_columns(P)) {
+            build_fused_m2l();
+            m2l_path = 2;
+        } else {
+            m2l_path = kTensor ? 1 : 0;
+            ensure_product_path();
+        }
         build_p2p_items();
         {
             std::vector<int32_t> xb;
@@ -327,7 +345,6 @@ struct Evaluator final : EvaluatorBase {
             CUDA_TRY(cudaDeviceSynchronize());
         }
         close_pairs = nclose;
-        Y.alloc(sizeof(T) * (size_t)m * ys_of(P) * (pl.v.nnz() + 1));
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
         if (gemm_smem > 48 * 1024)
             CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
@@ -350,7 +367,11 @@ struct Evaluator final : EvaluatorBase {
         if (ev_join) cudaEventDestroy(ev_join);
     }
 
-    void build_tensor_m2l(const std::vector<double>& m2l) {
+    // The product paths (1 and 0): offset-sorted tiles, the position map and the product
+    // array Y, built when a product path is first used.
+    void ensure_product_path() {
+        if (product_path_built) return;
+        build_m2l_batches(kGemmPairs);
         if constexpr (kTensor) {
             Tiles all, lvl;
             std::vector<int64_t> pe;
@@ -364,9 +385,106 @@ struct Evaluator final : EvaluatorBase {
             tc_ltile_begin.upload(lvl.begin);
             tc_ltile_count.upload(lvl.count);
             tc_pair_src.upload(ps);
+        }
+        Y.alloc(sizeof(T) * (size_t)m * ys_of(P) * (plan.v.nnz() + 1));
+        product_path_built = true;
+    }
+
+    // The fused path's tiles (see m2l_fused.cuh).  A chunk closes once it holds about
+    // three full tiles per offset, or a 1 / (2 num_sms) share of its level's columns (so
+    // that every level spreads over the SMs), or before its locals pass kFuChunkBytes (they
+    // stay in L2 while its CTA walks the offsets); each level's chunks are dealt to at most
+    // num_sms CTAs in contiguous runs of about equal tile counts.
+    static constexpr int64_t kFuChunkBytes = 384 * 1024;
+    void build_fused_m2l() {
+        if constexpr (kTensor) {
+            using S = FuShape<P>;
+            const Plan& pl = plan;
+            const int ppt = S::NT / m;
+            const int64_t col_full = 3 * 316 * (int64_t)S::NT;
+            const int64_t box_bytes = (int64_t)m * NC * (int64_t)sizeof(float);
+            std::vector<int32_t> td, tn, ps, pt;
+            std::vector<int64_t> tb, cta;
+            fu_lvl_cta.assign(pl.nlevels + 1, 0);
+            fu_lvl_grid.assign(pl.nlevels, 0);
+            std::vector<int64_t> cnt(317), fill(316);
+            for (int l = 0; l < pl.nlevels; ++l) {
+                std::vector<int64_t> chunk_tiles{(int64_t)td.size()};
+                int64_t b = pl.level_start[l];
+                const int64_t bend = pl.level_start[l + 1];
+                const int64_t level_cols = (pl.v.row[bend] - pl.v.row[b]) * m;
+                const int64_t col_target =
+                    std::min<int64_t>(col_full, std::max<int64_t>(S::NT, level_cols / (2 * (int64_t)num_sms)));
+                while (b < bend) {
+                    int64_t e = b, cols = 0, nbox = 0;
+                    for (; e < bend; ++e) {
+                        const int64_t nv = pl.v.row[e + 1] - pl.v.row[e];
+                        if (nv == 0) continue;
+                        if (nbox > 0 && (cols >= col_target || (nbox + 1) * box_bytes > kFuChunkBytes)) break;
+                        cols += nv * m;
+                        ++nbox;
+                    }
+                    if (nbox > 0) {
+                        std::fill(cnt.begin(), cnt.end(), 0);
+                        for (int64_t x = b; x < e; ++x)
+                            for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) cnt[pl.v.aux[q] + 1]++;
+                        for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+                        const int64_t base = (int64_t)ps.size();
+                        ps.resize(base + cnt[316]);
+                        pt.resize(base + cnt[316]);
+                        for (int d = 0; d < 316; ++d) fill[d] = cnt[d];
+                        // boxes in order: each offset's pairs come out ordered by target
+                        for (int64_t x = b; x < e; ++x)
+                            for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) {
+                                const int64_t pos = base + fill[pl.v.aux[q]]++;
+                                ps[pos] = pl.v.col[q];
+                                pt[pos] = (int32_t)x;
+                            }
+                        for (int d = 0; d < 316; ++d)
+                            for (int64_t j = cnt[d]; j < cnt[d + 1]; j += ppt) {
+                                td.push_back(d);
+                                tb.push_back(base + j);
+                                tn.push_back((int32_t)std::min<int64_t>(ppt, cnt[d + 1] - j));
+                            }
+                        chunk_tiles.push_back((int64_t)td.size());
+                    }
+                    b = e;
+                }
+                const int64_t nch = (int64_t)chunk_tiles.size() - 1;
+                const int G = (int)std::min<int64_t>(num_sms, nch);
+                fu_lvl_cta[l] = (int64_t)cta.size();
+                fu_lvl_grid[l] = G;
+                if (G > 0) {
+                    const int64_t t0 = chunk_tiles[0], tt = chunk_tiles[nch] - t0;
+                    int64_t ci = 0;
+                    cta.push_back(t0);
+                    for (int c = 1; c < G; ++c) {
+                        const int64_t want = t0 + tt * c / G;
+                        while (ci < nch && chunk_tiles[ci] < want) ++ci;
+                        cta.push_back(std::max(cta.back(), chunk_tiles[ci]));
+                    }
+                    cta.push_back(chunk_tiles[nch]);
+                }
+            }
+            fu_lvl_cta[pl.nlevels] = (int64_t)cta.size();
+            fu_tile_d.upload(td);
+            fu_tile_begin.upload(tb);
+            fu_tile_np.upload(tn);
+            fu_cta.upload(cta);
+            fu_pair_src.upload(ps);
+            fu_pair_tgt.upload(pt);
             std::vector<uint32_t> img;
-            build_tc_table_images<P>(m2l, img);
-            tc_bimg.upload(img);
+            build_fused_table_images<P>(tc_img, img);
+            fu_img.upload(img);
+            CUDA_TRY(cudaFuncSetAttribute(m2l_fused_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          FuShape<P>::SMEM));
+        }
+    }
+
+    void build_tensor_m2l(const std::vector<double>& m2l) {
+        if constexpr (kTensor) {
+            build_tc_table_images<P>(m2l, tc_img);
+            tc_bimg.upload(tc_img);
             tc_error.alloc(sizeof(int));
             CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
             CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -602,7 +720,8 @@ struct Evaluator final : EvaluatorBase {
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
-                               &near_phi, &near_g, &box_side, &v_pos, &xbox};
+                               &near_phi, &near_g, &box_side, &v_pos, &xbox, &fu_tile_d, &fu_tile_begin,
+                               &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -654,6 +773,19 @@ struct Evaluator final : EvaluatorBase {
     // P2P launches with accumulate 0 only read them and rewrite the output, the L2P / M2P
     // launches rewrite the same partials.  A last evaluation leaves the output and the
     // launch count as a plain evaluation does.
+    void set_m2l_path(int path) override {
+        if (path < 0 || path > 2 || (path >= 1 && !kTensor))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "M2L path " + std::to_string(path) + " not available");
+        if (path == 2 && fu_lvl_grid.empty()) {
+            if (m > fused_tile_columns(P))
+                throw Failure(FMMGPU_INVALID_ARGUMENT, "the fused M2L takes at most " +
+                                                           std::to_string(fused_tile_columns(P)) + " vectors a pass");
+            build_fused_m2l();
+        }
+        if (path <= 1) ensure_product_path();
+        m2l_path = path;
+    }
+
     void autotune(const double* d_charges, double* d_phi, double* d_grad) override {
         const bool timing = timer.on;
         timer.on = false;
@@ -711,6 +843,20 @@ struct Evaluator final : EvaluatorBase {
         // upward: P2M of every leaf, then M2M from level L-1 up to 0
         timer.run(kP2M, [&] { p2m_rows(0, (int64_t)plan.nleaves()); });
         for (int l = L - 1; l >= 0; --l) timer.run(kM2M, [&] { m2m_level(l); });
+        if (m2l_path == 2) {
+            // downward, fused: per level the L2L part of the locals, then the V products
+            // added into them in row order, then P2L
+            for (int l = 2; l <= L; ++l) {
+                timer.run(kL2L, [&] {
+                    if (l >= 3) l2l_products(l);
+                    reduce_locals(l, l >= 3, 0, 0);
+                });
+                timer.run(kM2L, [&] { m2l_fused(l); });
+                timer.run(kP2L, [&] { p2l_level(l); });
+            }
+            timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+            return;
+        }
         // M2L products of every level at once (all multipoles are final here)
         timer.run(kM2L, [&] { m2l_products(-1); });
         // downward: for l = 2..L: L2L products, the local (L2L + V in offset order), then P2L
@@ -756,6 +902,19 @@ struct Evaluator final : EvaluatorBase {
         if (n)
             m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
                 dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, Yo.as<T>(), M.as<T>());
+    }
+
+    // fused M2L of level l: L += the V products, in row order (after the L2L part)
+    void m2l_fused(int l) {
+        if constexpr (kTensor) {
+            const int G = fu_lvl_grid[l];
+            if (G == 0) return;
+            m2l_fused_kernel<P><<<counted((unsigned)G), 32 * kFuWarps, FuShape<P>::SMEM, stream>>>(
+                fu_tile_d.as<int32_t>(), fu_tile_begin.as<int64_t>(), fu_tile_np.as<int32_t>(),
+                fu_cta.as<int64_t>() + fu_lvl_cta[l], fu_pair_src.as<int32_t>(), fu_pair_tgt.as<int32_t>(), m,
+                fu_img.as<uint32_t>(), reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Lc.ptr),
+                tc_error.as<int>());
+        }
     }
 
     // M2L products Y of the V pairs of level l (l < 0: every level in one launch)
@@ -922,7 +1081,9 @@ struct Evaluator final : EvaluatorBase {
                 }
                 break;
             case FMMGPU_OP_M2L:
-                if (l >= 2) {
+                if (l >= 2 && m2l_path == 2) {
+                    m2l_fused(l);
+                } else if (l >= 2) {
                     m2l_products(l);
                     reduce_locals(l, 0, 1, 1);
                 }
@@ -946,10 +1107,10 @@ template <typename T>
 std::unique_ptr<EvaluatorBase> make_evaluator(int p, const Plan& pl, const std::vector<double>& m2l,
                                               const std::vector<double>& m2m, const std::vector<double>& l2l,
                                               cudaStream_t s, int m, bool grad, const std::vector<double>& us,
-                                              const std::vector<double>& ut, size_t* bytes) {
+                                              const std::vector<double>& ut, bool fused, size_t* bytes) {
 #define FMMB_CASE(PP)                                                                    \
     case PP: {                                                                           \
-        auto e = std::make_unique<Evaluator<PP, T>>(pl, m2l, m2m, l2l, s, m, grad, us, ut); \
+        auto e = std::make_unique<Evaluator<PP, T>>(pl, m2l, m2m, l2l, s, m, grad, us, ut, fused); \
         *bytes = e->device_bytes();                                                      \
         return e;                                                                        \
     }
@@ -981,6 +1142,7 @@ struct fmmgpu_fmm {
     int64_t near_pairs = 0;
     bool op_begun = false;  // a level-call evaluation has begun
     int mpass = 1;          // charge vectors per evaluator pass (all of them unless memory says no)
+    bool fused = false;     // M2L fused with the local reduce on the tensor cores (mixed, p <= 8)
     // whole-evaluation CUDA graph: captured once per (charges, potential, gradient)
     // buffer triple, replayed while the triple and the settings stay the same
     bool graph_on = false;
@@ -1247,13 +1409,19 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
     int least = 0, greatest = 0;  // the far-field chain is the critical path: highest priority
     CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     CUDA_TRY(cudaStreamCreateWithPriority(&f->stream, cudaStreamNonBlocking, greatest));
+    // the fused M2L is an option (fmmgpu_fmm_set_m2l_path 2), not the default: measured slower
+    // than the product path (its scattered f32 reductions into the locals cost more than
+    // writing and re-reading the products)
+    f->fused = false;
     // vectors per pass: every per-vector buffer (expansions, translation products, partial
     // outputs) for as many vectors as fit in 60% of the free memory
     {
         const size_t nc = (size_t)(s.p + 1) * (s.p + 1), ys = (nc + 31) / 32 * 32;
         const size_t tsz = s.precision == FMMGPU_PRECISION_F64 ? 8 : 4;
         const size_t nsrc = P.src_perm.size(), ntgt = P.tgt_perm.size();
-        const size_t per_vec = tsz * (2 * P.nboxes() * nc + P.nboxes() * ys + (P.v.nnz() + 1) * ys + nsrc) +
+        // the fused M2L keeps no product array (Y: one row per V pair and vector)
+        const size_t y_rows = f->fused ? 0 : P.v.nnz() + 1;
+        const size_t per_vec = tsz * (2 * P.nboxes() * nc + P.nboxes() * ys + y_rows * ys + nsrc) +
                                (tsz == 4 ? 8 * nsrc : 0) + 8 * ntgt * (s.gradients ? 4 : 1) * 2 +
                                8 * ntgt * (s.gradients ? 4 : 1) + 8 * nsrc;
         size_t free_b = 0, total_b = 0;
@@ -1261,6 +1429,7 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
         const size_t fit = per_vec ? (size_t)(0.6 * (double)free_b) / per_vec : (size_t)s.vectors;
         int want = (int)std::max<size_t>(1, std::min<size_t>((size_t)s.vectors, fit));
         if (s.vectors_per_pass > 0) want = std::min(s.vectors_per_pass, s.vectors);
+        if (f->fused) want = std::min(want, fused_tile_columns(s.p));
         // every pass holds the same number of vectors (the buffers' and the kernels' m): the
         // largest divisor of the vector count not above the wanted size
         while (s.vectors % want) --want;
@@ -1269,10 +1438,10 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
     size_t bytes = 0;
     if (s.precision == FMMGPU_PRECISION_F64)
         f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, f->mpass, s.gradients != 0, us,
-                                         ut, &bytes);
+                                         ut, false, &bytes);
     else
         f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, f->mpass, s.gradients != 0, us,
-                                        ut, &bytes);
+                                        ut, f->fused, &bytes);
     f->eval->qstride = s.vectors;
     const size_t ns = P.src_perm.size(), nt = P.tgt_perm.size();
     f->d_charges.alloc(sizeof(double) * (size_t)s.vectors * (ns + 1));
@@ -1540,8 +1709,10 @@ int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* f, int on) {
 
 int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* f, int path) {
     return guarded([&] {
-        if (!f || !f->eval || path < 0 || path > 1) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid M2L path");
-        f->eval->m2l_path = path;
+        if (!f || !f->eval || path < 0 || path > 2) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid M2L path");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->eval->set_m2l_path(path);
         f->drop_graph();
     });
 }

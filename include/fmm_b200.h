@@ -177,8 +177,11 @@ int fmmgpu_fmm_set_kind_timing(fmmgpu_fmm* fmm, int on);
 /* Which parts the following evaluations run, for tests: bit 0 the near field (P2P),
  * bit 1 the far field (everything that reaches L2P and M2P); 3, the default, is the FMM. */
 int fmmgpu_fmm_set_kinds(fmmgpu_fmm* fmm, int kinds);
-/* Which M2L kernel the following evaluations use, for tests: 1 (default) the tensor-core
- * kernel where the form has one (mixed precision, p <= 8), 0 the SIMT kernel. */
+/* Which M2L the following evaluations use (mixed precision, p <= 8; f64 always runs 0):
+ * 1 (default) the tensor-core products then the ordered local reduce, 2 the tensor-core
+ * M2L fused with the local reduce (products added into the locals in row order, no
+ * product array; at most 128 vectors a pass, 64 at p = 8), 0 SIMT products then the
+ * reduce.  2 and 1 give the same bits.  Synchronises. */
 int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* fmm, int path);
 /* Milliseconds of the last evaluation per kind: [0] charge load, [1] P2M, [2] M2M,
  * [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P + output pass.  Synchronises. */
