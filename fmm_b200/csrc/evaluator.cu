@@ -201,6 +201,7 @@ struct Evaluator final : EvaluatorBase {
     std::vector<int> fu_lvl_grid;
     bool product_path_built = false;  // the product paths' tiles and Y (built on first use)
     std::vector<uint32_t> tc_img;     // host copy of the tensor-memory table images
+    CUtensorMap mmap{};               // the multipoles, for the tensor-core M2L's row gathers
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
@@ -298,8 +299,8 @@ struct Evaluator final : EvaluatorBase {
         up_pos(tpos, ut);
         const size_t nb = pl.nboxes();
         sq.alloc(sizeof(T) * (size_t)m * (dp.nsrc + 1));
-        M.alloc(sizeof(T) * (size_t)m * NC * nb);
-        Lc.alloc(sizeof(T) * (size_t)m * NC * nb);
+        M.alloc(sizeof(T) * (size_t)m * ms_of(P) * nb);
+        Lc.alloc(sizeof(T) * (size_t)m * ms_of(P) * nb);
         far_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
@@ -376,7 +377,7 @@ struct Evaluator final : EvaluatorBase {
             Tiles all, lvl;
             std::vector<int64_t> pe;
             std::vector<int32_t> ps;
-            batches(kTcRows, all, lvl, tc_lvl_tiles, pe, ps);
+            batches(TcTs<P>::NT, all, lvl, tc_lvl_tiles, pe, ps);
             tc_ntiles = (int64_t)all.d.size();
             tc_tile_d.upload(all.d);
             tc_tile_begin.upload(all.begin);
@@ -402,7 +403,7 @@ struct Evaluator final : EvaluatorBase {
             const Plan& pl = plan;
             const int ppt = S::NT / m;
             const int64_t col_full = 3 * 316 * (int64_t)S::NT;
-            const int64_t box_bytes = (int64_t)m * NC * (int64_t)sizeof(float);
+            const int64_t box_bytes = (int64_t)m * ms_of(P) * (int64_t)sizeof(float);
             std::vector<int32_t> td, tn, ps, pt;
             std::vector<int64_t> tb, cta;
             fu_lvl_cta.assign(pl.nlevels + 1, 0);
@@ -485,6 +486,7 @@ struct Evaluator final : EvaluatorBase {
         if constexpr (kTensor) {
             build_tc_table_images<P>(m2l, tc_img);
             tc_bimg.upload(tc_img);
+            encode_multipole_map<P>(&mmap, reinterpret_cast<const float*>(M.ptr), (int64_t)plan.nboxes() * m);
             tc_error.alloc(sizeof(int));
             CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
             CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -738,7 +740,7 @@ struct Evaluator final : EvaluatorBase {
             load_charges(d_charges);
             // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
             int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
-            CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * NC * top, stream));
+            CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * ms_of(P) * top, stream));
         });
         if (overlap && !timer.on && kinds == 3 && items.count) {
             // the near field on near_stream (it needs only the charges) beside the far-field
@@ -931,8 +933,8 @@ struct Evaluator final : EvaluatorBase {
                 for (int v = 0; v < m; ++v)
                     m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
                         td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
-                        tc_pair_src.as<int32_t>(), m, v, tc_bimg.as<uint32_t>(),
-                        reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+                        tc_pair_src.as<int32_t>(), m, v, tc_bimg.as<uint32_t>(), mmap,
+                        reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
             return;
         }

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
         nent = (int)(plan.x_row[row + 1] - ent0);
         if (nent == 0) return;
     }
-    T* outb = out + (int64_t)box * m * NC;
+    T* outb = out + (int64_t)box * m * ms_of(P);
     bool first = true;
     for (int e = 0; e < nent; ++e) {
         int sleaf = IRREG ? plan.x_col[ent0 + e] : (int)row;
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
                 for (int c = lane; c < NC; c += 32) {
                     T acc = T(0);
                     for (int j = 0; j < cnt; ++j) acc += Q[v * 32 + j] * S[c * 32 + j];
-                    T* o = outb + (int64_t)v * NC + c;
+                    T* o = outb + (int64_t)v * ms_of(P) + c;
                     if (first && !IRREG) *o = acc;
                     else *o += acc;
                 }
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
 #pragma unroll
     for (int s = 16, len = NCP / 2; s >= 1; s >>= 1, len >>= 1)
         if (lane & s) base += len;
-    float* o = out + (int64_t)box * NC;
+    float* o = out + (int64_t)box * ms_of(P);
 #pragma unroll
     for (int i = 0; i < NCP / 32; ++i) {
         const int c = base + i;
@@ -308,7 +308,7 @@ __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ pare
 #pragma unroll
             for (int o = 0; o < 8; ++o)
                 if (plan.src_below[c0 + o]) s += Yo[((int64_t)(c0 + o) * m + v) * YS + i];
-            M[((int64_t)p * m + v) * NC + i] = s;
+            M[((int64_t)p * m + v) * ms_of(P) + i] = s;
         }
 }
 
@@ -330,7 +330,7 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
     const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
     for (int v = 0; v < m; ++v)
         for (int i = threadIdx.x; i < NC; i += blockDim.x) {
-            T s = accumulate ? Lc[(b * m + v) * NC + i] : T(0);
+            T s = accumulate ? Lc[(b * m + v) * ms_of(P) + i] : T(0);
             if (with_l2l) s = accumulate ? s + Yo[(b * m + v) * YS + i] : Yo[(b * m + v) * YS + i];
             int64_t e = e0;
             for (; e + 4 <= e1; e += 4) {
@@ -342,7 +342,7 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
                 s += y3;
             }
             for (; e < e1; ++e) s += __ldcs(Yv + (vpos[e] * m + v) * YS + i);
-            Lc[(b * m + v) * NC + i] = s;
+            Lc[(b * m + v) * ms_of(P) + i] = s;
         }
 }
 
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
         __syncthreads();
         for (int t = threadIdx.x; t < NC * kGemmPairs; t += blockDim.x) {
             int pr = t / NC, k = t % NC;
-            Xs[k * kGemmPairs + pr] = pr < cnt ? M[((int64_t)pair_src[p0 + pr] * m + v) * NC + k] : T(0);
+            Xs[k * kGemmPairs + pr] = pr < cnt ? M[((int64_t)pair_src[p0 + pr] * m + v) * ms_of(P) + k] : T(0);
         }
         __syncthreads();
         T acc[4][JN];
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(128) leaf_far_kernel(DevPlan plan, int64_t lea
             }
             // L2P, unit frame
             if (mode & 1) {
-                const T* Lb = Lc + ((int64_t)box * m + v) * NC;
+                const T* Lb = Lc + ((int64_t)box * m + v) * ms_of(P);
                 if (kStage) {
                     for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Lb[k];
                     __syncthreads();
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(128) leaf_far_kernel(DevPlan plan, int64_t lea
             // M2P over the W list, frame (c(s|t), r(s|t))
             for (int64_t e = w0; e < w1; ++e) {
                 int s = plan.w_col[e];
-                const T* Mb = M + ((int64_t)s * m + v) * NC;
+                const T* Mb = M + ((int64_t)s * m + v) * ms_of(P);
                 if (kStage) {
                     for (int k = threadIdx.x; k < NC; k += blockDim.x) C[k] = Mb[k];
                     __syncthreads();

@@ -77,15 +77,6 @@ struct FuShape {
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
-__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
-    asm volatile(
-        "{\n\t"
-        ".reg .b64 st;\n\t"
-        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t"
-        "}\n" ::"r"(mbar),
-        "r"(bytes)
-        : "memory");
-}
 
 // one bulk copy global -> this CTA's shared memory, completion counted on mbar (both
 // addresses 16-byte aligned, size a multiple of 16)
@@ -179,7 +170,7 @@ __global__ void __launch_bounds__(32 * kFuWarps, 1) m2l_fused_kernel(
 #pragma unroll
             for (int j = 0; j < RPW; ++j) {
                 const long long sr = __shfl_sync(0xffffffffu, (long long)my_src, j);
-                const float* src = M + (sr < 0 ? 0 : sr) * NC;
+                const float* src = M + (sr < 0 ? 0 : sr) * ms_of(P);
 #pragma unroll
                 for (int a = 0; a < S::KA; ++a) {
                     const int kk = a * 32 + lane;
@@ -344,7 +335,7 @@ __global__ void __launch_bounds__(32 * kFuWarps, 1) m2l_fused_kernel(
             const int st = (int)(k & 1);
             const int64_t pb = tile_begin[it];
             const int ncol = tile_np[it] * m;
-            // lane j holds the local row (box * m + vector) * NC of columns j, j + 32, j + 64,
+            // lane j holds the local row (box * m + vector) * ms_of(P) of columns j, j + 32, j + 64,
             // j + 96, or -1 where the column is empty or its box has the other parity
             long long rb[(NT + 31) / 32];
 #pragma unroll
@@ -353,7 +344,7 @@ __global__ void __launch_bounds__(32 * kFuWarps, 1) m2l_fused_kernel(
                 rb[h] = -1;
                 if (cc < ncol) {
                     const int t = pair_tgt[pb + cc / m];
-                    if ((t & 1) == g) rb[h] = ((long long)t * m + cc % m) * NC;
+                    if ((t & 1) == g) rb[h] = ((long long)t * m + cc % m) * ms_of(P);
                 }
             }
             if (!warp_wait(&bar_accf[st], (uint32_t)((k >> 1) & 1))) {

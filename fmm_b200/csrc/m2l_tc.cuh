@@ -22,8 +22,14 @@
 // Waits are bounded: a CTA that gives up sets *error and skips its epilogue.
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <cstring>
+#include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "harmonics.cuh"
@@ -161,12 +167,19 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 // [c T / G, (c + 1) T / G) of the offset-sorted tile list.  The table of the current
 // offset lives in tensor memory as the MMA's A operand (M = 128 lanes = output slots,
 // K = input slots in columns; hi and lo parts), so the MMA is D[slot][pair] = A_d . X^T
-// with the gathered multipoles X as the shared-memory B operand (N = 128 pairs,
+// with the gathered multipoles X as the shared-memory B operand (N = NT pairs,
 // K-major, 128-byte swizzled).  Roles, coupled only by mbarriers (no block barrier in
 // the loop):
-//   warps 8-15 (producers): load tile k's multipoles, then split them into X stage k&1
-//     once MMA(k-2) has released it (empty[k&1]), signal full[k&1]; warps 8-11 also replace the table in tensor
-//     memory when the offset changes, after MMA(k-1) has read the old one (table);
+//   warp 17 (gather): for tile k, once the raw stage k % 2 is free, each lane fetches
+//     four multipole rows with one tensor-memory-access gather (tile::gather4; box one
+//     row of KP f32, the row's slots beyond (p+1)^2 filled with zeros by the copy
+//     engine) into the raw stage, completion counted on raw_full; the copy engine keeps
+//     the whole tile's rows in flight at once, where per-lane loads were limited by the
+//     SM's outstanding misses;
+//   warps 8-15 (converters): wait raw_full, split the raw rows into X stage k&1
+//     (x = hi + lo in tf32, 128-byte swizzled) once MMA(k-2) has released it
+//     (empty[k&1]), signal full[k&1] and raw_empty; warps 8-11 also replace the table in
+//     tensor memory when the offset changes, after MMA(k-1) has read the old one;
 //   warp 16, one thread (MMA): waits full[k&1], the table and the accumulator k&1
 //     (acc_empty, released by the epilogue of tile k-2), issues the 3 x KSTEPS MMAs
 //     and commits to empty[k&1] and acc_full[k&1];
@@ -177,9 +190,10 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 // Every wait is bounded; a role that gives up sets the shared abort flag (which ends
 // the other roles' waits) and *error, and the CTA frees its tensor memory and returns.
 // One vector per launch.
-constexpr int kTcWarps = 17;
-constexpr int kTcProd = 8;      // producer warps (8..15)
-constexpr int kTcMmaWarp = 16;  // the MMA issuer's warp
+constexpr int kTcWarps = 18;
+constexpr int kTcProd = 8;        // converter warps (8..15)
+constexpr int kTcMmaWarp = 16;    // the MMA issuer's warp
+constexpr int kTcGatherWarp = 17; // the gather issuer's warp
 constexpr long long kTcWait = 4000000000LL;  // clock cycles (about 2 s)
 
 template <int P>
@@ -188,15 +202,16 @@ struct TcTs {
     static constexpr int KA = (NC + 31) / 32;
     static constexpr int KP = 32 * KA;             // padded K (input slots)
     static constexpr int KSTEPS = KP / 8;
-    static constexpr int NT = kTcRows;             // pairs per tile (UMMA N)
-    static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage
-    static constexpr int SMEM = 4 * X_BYTES + 1024;
+    static constexpr int NT = KP > 64 ? 96 : 128;  // pairs per tile (UMMA N): shared memory bounds it at p = 8
+    static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage (also one raw stage)
+    static constexpr int SMEM = 6 * X_BYTES + 1024;  // X [2 stages][hi, lo], raw [2 stages]
     static constexpr int COL_AHI = 0, COL_ALO = KP, COL_D0 = 2 * KP;  // TMEM columns
     static constexpr int TMEM_COLS = 512;
     static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per offset (hi, lo)
     static_assert(NC <= 128, "UMMA M = 128 output slots");
     static_assert(2 * KP + 2 * NT <= TMEM_COLS, "TMEM budget");
-    static_assert(NT % kTcProd == 0 && NT / kTcProd <= 32, "producer rows");
+    static_assert(NT % 32 == 0 && NT / 4 <= 32, "gather rows: four per lane");
+    static_assert(SMEM + 256 <= 227 * 1024, "shared memory");
 };
 
 template <int NTILE>
@@ -223,6 +238,27 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
         "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]));
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t"
+        ".reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t"
+        "}\n" ::"r"(mbar),
+        "r"(bytes)
+        : "memory");
+}
+
+// four rows (r0..r3) of a 2D tensor map, one box each (KP f32 at x = 0), into dst
+// (four consecutive box rows), completion counted on mbar; no multicast
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* map, int r0, int r1, int r2, int r3,
+                                            uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(mbar)
+        : "memory");
+}
+
 template <int P>
 __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
                                                                   const int64_t* __restrict__ tile_begin,
@@ -230,15 +266,15 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   int64_t ntiles,
                                                                   const int32_t* __restrict__ pair_src, int m, int v,
                                                                   const uint32_t* __restrict__ timg,
-                                                                  const float* __restrict__ M, float* __restrict__ Y,
-                                                                  int* __restrict__ error) {
+                                                                  const __grid_constant__ CUtensorMap mmap,
+                                                                  float* __restrict__ Y, int* __restrict__ error) {
     using S = TcTs<P>;
-    constexpr int NC = S::NC;
-    constexpr int RPW = S::NT / kTcProd;  // gathered rows per producer warp
+    constexpr int NT = S::NT, KP = S::KP;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 stages][hi, lo]
+    unsigned char* rbuf = xbuf + 4 * S::X_BYTES;                                      // raw [2 stages][NT][KP]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    __shared__ uint64_t bar_full[2], bar_empty[2], bar_accf[2], bar_acce[2], bar_table;
+    __shared__ uint64_t bar_full[2], bar_empty[2], bar_accf[2], bar_acce[2], bar_table, bar_rfull[2], bar_rempty[2];
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
@@ -257,6 +293,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             mbar_init(smem_u32(&bar_empty[b]), 1);
             mbar_init(smem_u32(&bar_accf[b]), 1);
             mbar_init(smem_u32(&bar_acce[b]), 8);
+            mbar_init(smem_u32(&bar_rfull[b]), 1);
+            mbar_init(smem_u32(&bar_rempty[b]), kTcProd);
         }
         mbar_init(smem_u32(&bar_table), 4);
         abort_flag = 0;
@@ -284,62 +322,78 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         return __shfl_sync(0xffffffffu, a, 0) != 0;
     };
 
-    if (warp >= kTcProd && warp < kTcProd + kTcProd) {
-        // ---------------- producers ----------------
-        const int pw = warp - kTcProd;
-        const uint32_t* img_prev = nullptr;
-        // metadata of the next tile, loaded one tile ahead: lane j < RPW holds the source
-        // box of row pw + kTcProd * j
-        int64_t nb = tile_begin[i0];
-        int ncnt = tile_count[i0];
-        int nsrc = 0;
-        if (lane < RPW && pw + kTcProd * lane < ncnt) nsrc = pair_src[nb + pw + kTcProd * lane];
+    if (warp == kTcGatherWarp) {
+        // ---------------- gather: four rows a lane ----------------
+        int64_t issued = 0;
         for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
             const int64_t it = i0 + k;
-            const int st = (int)(k & 1);
-            const int cnt = ncnt;
-            const int my_src = nsrc;
-            unsigned char* xh = xbuf + (size_t)st * 2 * S::X_BYTES;
-            unsigned char* xl = xh + S::X_BYTES;
-            float x[RPW][S::KA];
+            const int rs = (int)(k & 1);
+            const int64_t p0 = tile_begin[it];
+            const int cnt = tile_count[it];
+            int r[4];
 #pragma unroll
-            for (int j = 0; j < RPW; ++j) {
-                const int r = pw + kTcProd * j;
-                const int sb = __shfl_sync(0xffffffffu, my_src, j);
-                const float* src = M + ((int64_t)sb * m + v) * NC;
-#pragma unroll
-                for (int a = 0; a < S::KA; ++a) {
-                    const int kk = a * 32 + lane;
-                    x[j][a] = (r < cnt && kk < NC) ? __ldg(src + kk) : 0.0f;
-                }
+            for (int j = 0; j < 4; ++j) {
+                const int row = 4 * lane + j;
+                // rows past the tile's pairs fetch row 0 (their products are never stored)
+                r[j] = (row < cnt) ? pair_src[p0 + row] * m + v : 0;
             }
-            if (k + 1 < ntile) {  // the next tile's metadata, in flight with the loads above
-                nb = tile_begin[it + 1];
-                ncnt = tile_count[it + 1];
-                nsrc = 0;
-                if (lane < RPW && pw + kTcProd * lane < ncnt) nsrc = pair_src[nb + pw + kTcProd * lane];
-            }
-            // the stage is written only once MMA(k-2) has read it; the loads above need no stage
-            if (k >= 2 && !warp_wait(&bar_empty[st], (uint32_t)(((k - 2) >> 1) & 1))) {
+            if (k >= 2 && !warp_wait(&bar_rempty[rs], (uint32_t)(((k - 2) >> 1) & 1))) {
                 if (lane == 0) give_up();
                 break;
             }
-#pragma unroll
-            for (int j = 0; j < RPW; ++j) {
-                const int r = pw + kTcProd * j;
-#pragma unroll
-                for (int a = 0; a < S::KA; ++a) {
-                    const int kk = a * 32 + lane;
-                    const uint32_t hi = cvt_tf32(x[j][a]);
-                    const uint32_t lo = cvt_tf32(x[j][a] - __uint_as_float(hi));
-                    const uint32_t off = sw128_offset(r, kk, S::NT);
-                    *reinterpret_cast<uint32_t*>(xh + off) = hi;
-                    *reinterpret_cast<uint32_t*>(xl + off) = lo;
-                }
+            if (lane == 0) mbar_expect_tx(smem_u32(&bar_rfull[rs]), (uint32_t)S::X_BYTES);
+            __syncwarp();
+            if (4 * lane < NT)
+                tma_gather4(smem_u32(rbuf + (size_t)rs * S::X_BYTES + (size_t)4 * lane * KP * 4), &mmap, r[0], r[1],
+                            r[2], r[3], smem_u32(&bar_rfull[rs]));
+            issued = k + 1;
+        }
+        // on a give-up, the gathers still in flight land before the shared memory is released
+        if (lane == 0 && *abort)
+            for (int64_t k = issued > 2 ? issued - 2 : 0; k < issued; ++k)
+                mbar_wait_bounded(smem_u32(&bar_rfull[k & 1]), (uint32_t)((k >> 1) & 1), kTcWait);
+        __syncwarp();
+    } else if (warp >= kTcProd && warp < kTcProd + kTcProd) {
+        // ---------------- converters ----------------
+        const int pw = warp - kTcProd;
+        const int ctid = tid - 32 * kTcProd;  // 0 .. 255
+        const uint32_t* img_prev = nullptr;
+        for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
+            const int64_t it = i0 + k;
+            const int st = (int)(k & 1);
+            unsigned char* xh = xbuf + (size_t)st * 2 * S::X_BYTES;
+            unsigned char* xl = xh + S::X_BYTES;
+            const float4* raw = reinterpret_cast<const float4*>(rbuf + (size_t)st * S::X_BYTES);
+            // the raw rows of tile k are in; the stage is written only once MMA(k-2) has read it
+            if (!warp_wait(&bar_rfull[st], (uint32_t)((k >> 1) & 1)) ||
+                (k >= 2 && !warp_wait(&bar_empty[st], (uint32_t)(((k - 2) >> 1) & 1)))) {
+                if (lane == 0) give_up();
+                break;
+            }
+            // raw [NT][KP] -> hi / lo, four consecutive slots (one 16-byte chunk) at a time
+#pragma unroll 4
+            for (int c = ctid; c < NT * KP / 4; c += 32 * kTcProd) {
+                const int row = c / (KP / 4), k4 = 4 * (c % (KP / 4));
+                const float4 x = raw[c];
+                uint4 hi, lo;
+                hi.x = cvt_tf32(x.x);
+                hi.y = cvt_tf32(x.y);
+                hi.z = cvt_tf32(x.z);
+                hi.w = cvt_tf32(x.w);
+                lo.x = cvt_tf32(x.x - __uint_as_float(hi.x));
+                lo.y = cvt_tf32(x.y - __uint_as_float(hi.y));
+                lo.z = cvt_tf32(x.z - __uint_as_float(hi.z));
+                lo.w = cvt_tf32(x.w - __uint_as_float(hi.w));
+                const uint32_t off = sw128_offset(row, k4, NT);
+                *reinterpret_cast<uint4*>(xh + off) = hi;
+                *reinterpret_cast<uint4*>(xl + off) = lo;
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&bar_full[st]));
+            if (lane == 0) {
+                mbar_arrive(smem_u32(&bar_full[st]));
+                mbar_arrive(smem_u32(&bar_rempty[st]));
+            }
             // the table of tile k (warps 8-11, one per lane quarter), once MMA(k-1) is done
             const uint32_t* img = timg + (size_t)tile_d[it] * S::IMG_WORDS;
             if (pw < 4 && img != img_prev) {
@@ -383,7 +437,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     } else if (warp == kTcMmaWarp) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            constexpr uint32_t idesc = tf32_idesc_ts<S::NT>();
+            constexpr uint32_t idesc = tf32_idesc_ts<NT>();
             int cur_d = -1;
             uint32_t nchg = 0;
             int64_t issued = 0;
@@ -406,7 +460,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t xh = smem_u32(xbuf + (size_t)st * 2 * S::X_BYTES), xl = xh + S::X_BYTES;
-                const uint32_t dcol = tmem + (uint32_t)(S::COL_D0 + st * S::NT);
+                const uint32_t dcol = tmem + (uint32_t)(S::COL_D0 + st * NT);
                 const uint32_t As[3] = {(uint32_t)S::COL_AHI, (uint32_t)S::COL_ALO, (uint32_t)S::COL_AHI};
                 const uint32_t Bs[3] = {xl, xh, xh};  // A_hi X_lo, A_lo X_hi, then A_hi X_hi
                 uint32_t acc = 0;
@@ -414,7 +468,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 for (int t = 0; t < 3; ++t)
 #pragma unroll
                     for (int s2 = 0; s2 < S::KSTEPS; ++s2) {
-                        const uint32_t kb = (uint32_t)((s2 >> 2) * S::NT * 128 + (s2 & 3) * 32);
+                        const uint32_t kb = (uint32_t)((s2 >> 2) * NT * 128 + (s2 & 3) * 32);
                         umma_tf32_ts(dcol, tmem + As[t] + (uint32_t)(8 * s2), sw128_desc(Bs[t] + kb), idesc, acc);
                         acc = 1;
                     }
@@ -431,7 +485,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         __syncwarp();
     } else if (warp < 8) {
         // ---------------- epilogue ----------------
-        const int q = warp & 3, g = warp >> 2;  // lane quarter, column half (64 pairs)
+        const int q = warp & 3, g = warp >> 2;  // lane quarter, column half (NT / 2 pairs)
         const int n = 32 * q + lane;
         for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
             const int64_t it = i0 + k;
@@ -445,24 +499,17 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (32 * q < ys_of(P)) {
                 // products at their pair positions p0 + c (a tile's rows are consecutive), whole
-                // 128-byte lines (rows >= NC of the table are zero), two TMEM loads per wait
-#pragma unroll
-                for (int h = 0; h < 4; h += 2) {
-                    const int c0 = 64 * g + 16 * h;
+                // 128-byte lines (rows >= NC of the table are zero), 16 columns per TMEM load
+#pragma unroll 1
+                for (int c0 = (NT / 2) * g; c0 < (NT / 2) * (g + 1); c0 += 16) {
                     if (c0 >= cnt) break;
-                    float v0[16], v1[16];
-                    const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * S::NT + c0);
-                    tmem_ld16_nowait(ta, v0);
-                    tmem_ld16_nowait(ta + 16u, v1);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    float v0[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * NT + c0), v0);
                     float* yb = Y + ((p0 + c0) * m + v) * ys_of(P) + n;
                     const int64_t row = (int64_t)m * ys_of(P);
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
                         if (c0 + i < cnt) __stcs(yb + i * row, v0[i]);
-#pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                        if (c0 + 16 + i < cnt) __stcs(yb + (16 + i) * row, v1[i]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
@@ -476,6 +523,31 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         asm volatile("tcgen05.fence::after_thread_sync;");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS));
     }
+}
+
+// Host: the tensor map of the multipoles for the gathers: 2D, rows (box * m + vector) of
+// ms_of(P) f32 (16-byte multiples), the inner extent (p+1)^2 so that a box of KP slots
+// reads zeros past the row's coefficients; boxes of one row, no swizzle.  The driver's
+// encoder is fetched through the runtime (no link against the driver library).
+template <int P>
+void encode_multipole_map(CUtensorMap* map, const float* M, int64_t rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q{};
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            throw std::runtime_error("cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dim[2] = {(cuuint64_t)nc_of(P), (cuuint64_t)(rows > 0 ? rows : 1)};
+    const cuuint64_t stride[1] = {(cuuint64_t)ms_of(P) * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)TcTs<P>::KP, 1};
+    const cuuint32_t estride[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(M), dim, stride, box,
+                              estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
 // Host: the table images for tensor memory, per offset a hi and a lo part, each
