@@ -218,9 +218,15 @@ def run_ours(args):
     sample = sample_indices(n, SAMPLE)
 
     def build(precision):
-        # launch shapes timed at build (the results are the same bits for every shape)
-        return (F.FmmBuilder(P).gradients().max_points_per_leaf(LEAF).precision(precision)
-                .device(local).autotune().build(x))
+        # launch shapes timed at build (the results are the same bits for every shape),
+        # or the ones given by --shapes
+        b = F.FmmBuilder(P).gradients().max_points_per_leaf(LEAF).precision(precision).device(local)
+        if args.shapes is None:
+            return b.autotune().build(x)
+        f = b.build(x)
+        w, blk = (int(t) for t in args.shapes.split(","))
+        f.set_launch_shapes(w, blk)
+        return f
 
     log(f"problem n={n} generated")
     t0 = time.perf_counter()
@@ -523,6 +529,9 @@ def main():
     ap.add_argument("--ref-n", type=int, default=400_000, help="points of each reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (256 clouds) measurement")
+    ap.add_argument("--shapes", default=None,
+                    help="P2P warps,L2P/M2P threads (e.g. 1,128): set instead of timed at build "
+                         "(profiler runs, whose serialised launches would mislead the timing)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
