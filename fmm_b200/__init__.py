@@ -34,7 +34,7 @@ class FmmError(RuntimeError):
 class Settings(C.Structure):
     _fields_ = [("p", C.c_int), ("precision", C.c_int), ("gradients", C.c_int), ("vectors", C.c_int),
                 ("max_points_per_leaf", C.c_int), ("max_level", C.c_int), ("device", C.c_int),
-                ("vectors_per_pass", C.c_int), ("autotune", C.c_int)]
+                ("vectors_per_pass", C.c_int), ("autotune", C.c_int), ("product_bytes", C.c_int64)]
 
 
 class Info(C.Structure):
@@ -42,7 +42,8 @@ class Info(C.Structure):
                 ("nsources", C.c_int64), ("ntargets", C.c_int64), ("near_pairs", C.c_int64),
                 ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
                 ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64),
-                ("vectors_per_pass", C.c_int64), ("p2p_warps", C.c_int64), ("leaf_block", C.c_int64)]
+                ("vectors_per_pass", C.c_int64), ("p2p_warps", C.c_int64), ("leaf_block", C.c_int64),
+                ("product_chunks", C.c_int64)]
 
 
 def lib():
@@ -179,6 +180,12 @@ class FmmBuilder:
     def autotune(self, on=True):
         """Time the launch shapes at build and keep the fastest (the results are the same bits)."""
         self._s.autotune = int(bool(on))
+        return self
+
+    def product_bytes(self, n):
+        """M2L product buffer bytes (0: automatic); smaller buffers run the products in
+        chunks of target boxes, with the same results."""
+        self._s.product_bytes = int(n)
         return self
 
     def max_level(self, level):

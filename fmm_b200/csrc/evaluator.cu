@@ -156,6 +156,7 @@ struct EvaluatorBase {
     virtual void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
     virtual void autotune(const double* d_charges, double* d_phi, double* d_grad) = 0;
     virtual void set_m2l_path(int path) = 0;
+    virtual int64_t product_chunks() const = 0;
 };
 
 template <int P, typename T>
@@ -200,8 +201,20 @@ struct Evaluator final : EvaluatorBase {
     std::vector<int64_t> fu_lvl_cta;
     std::vector<int> fu_lvl_grid;
     bool product_path_built = false;  // the product paths' tiles and Y (built on first use)
+    // chunked product path: when the products of every V pair and vector do not fit the
+    // product budget (ybudget bytes), each level's boxes are cut into chunks whose products
+    // fit; a chunk's pairs are ordered by (offset, target) at positions local to the chunk
+    // (v_pos), tensor-core tiles (NT / m pairs) and SIMT tiles (kGemmPairs pairs) per chunk
+    struct Chunk {
+        int level;
+        int64_t b0, b1, base, npairs, tc_t0, tc_nt, s_t0, s_nt;
+    };
+    std::vector<Chunk> chunks;
+    int64_t ybudget = 0;
+    DevBuf ck_tc_d, ck_tc_begin, ck_tc_count, ck_s_d, ck_s_begin, ck_s_count, ck_pair_src;
     std::vector<uint32_t> tc_img;     // host copy of the tensor-memory table images
     CUtensorMap mmap{};               // the multipoles, for the tensor-core M2L's row gathers
+    CUtensorMap vmap{};               // the same, boxes of m rows (a pair's vectors)
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
@@ -217,15 +230,15 @@ struct Evaluator final : EvaluatorBase {
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
-    static constexpr bool kBfly = sizeof(T) == 4;  // register P2M/P2L (f32, one vector)
+    static constexpr bool kBfly = sizeof(T) == 4;  // register P2M/P2L (f32, vectors one after another)
 
     // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
     static constexpr float kTheta2 = 0.0625f;
 
     Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
               const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
-              const std::vector<double>& ut, bool fused)
-        : plan(pl), stream(s), m(m_), gradients(grad) {
+              const std::vector<double>& ut, bool fused, int64_t ybudget_)
+        : plan(pl), stream(s), m(m_), gradients(grad), ybudget(ybudget_) {
         timer.stream = s;
         level.upload(pl.level);
         idx.upload(pl.idx);
@@ -372,12 +385,18 @@ struct Evaluator final : EvaluatorBase {
     // array Y, built when a product path is first used.
     void ensure_product_path() {
         if (product_path_built) return;
+        const int64_t row_bytes = (int64_t)sizeof(T) * m * ys_of(P);
+        if (ybudget > 0 && ((int64_t)plan.v.nnz() + 1) * row_bytes > ybudget) {
+            build_product_chunks(row_bytes);
+            product_path_built = true;
+            return;
+        }
         build_m2l_batches(kGemmPairs);
         if constexpr (kTensor) {
             Tiles all, lvl;
             std::vector<int64_t> pe;
             std::vector<int32_t> ps;
-            batches(TcTs<P>::NT, all, lvl, tc_lvl_tiles, pe, ps);
+            batches(TcTs<P>::NT / m, all, lvl, tc_lvl_tiles, pe, ps);
             tc_ntiles = (int64_t)all.d.size();
             tc_tile_d.upload(all.d);
             tc_tile_begin.upload(all.begin);
@@ -389,6 +408,95 @@ struct Evaluator final : EvaluatorBase {
         }
         Y.alloc(sizeof(T) * (size_t)m * ys_of(P) * (plan.v.nnz() + 1));
         product_path_built = true;
+    }
+
+    void build_product_chunks(int64_t row_bytes) {
+        const Plan& pl = plan;
+        const int ppt_tc = kTensor ? std::max(1, tc_tile_columns(P) / m) : 1;
+        const int64_t max_pairs = std::max<int64_t>(1, ybudget / row_bytes - 1);
+        std::vector<int32_t> ps, tcd, tcn, sd, sn;
+        std::vector<int64_t> tcb, sb, vp(pl.v.nnz());
+        std::vector<int64_t> cnt(317), fill(316);
+        int64_t ymax = 0;
+        chunks.clear();
+        for (int l = 0; l < pl.nlevels; ++l) {
+            int64_t b = pl.level_start[l];
+            const int64_t bend = pl.level_start[l + 1];
+            while (b < bend) {
+                int64_t e = b, np = 0;
+                for (; e < bend; ++e) {
+                    const int64_t nv = pl.v.row[e + 1] - pl.v.row[e];
+                    if (np > 0 && np + nv > max_pairs) break;
+                    np += nv;
+                }
+                Chunk c{l, b, e, (int64_t)ps.size(), np, (int64_t)tcd.size(), 0, (int64_t)sd.size(), 0};
+                if (np > 0) {
+                    std::fill(cnt.begin(), cnt.end(), 0);
+                    for (int64_t x = b; x < e; ++x)
+                        for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) cnt[pl.v.aux[q] + 1]++;
+                    for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+                    ps.resize(c.base + np);
+                    for (int d = 0; d < 316; ++d) fill[d] = cnt[d];
+                    // boxes in order: each offset's pairs come out ordered by target
+                    for (int64_t x = b; x < e; ++x)
+                        for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) {
+                            const int64_t pos = fill[pl.v.aux[q]]++;
+                            ps[c.base + pos] = pl.v.col[q];
+                            vp[q] = pos;
+                        }
+                    for (int d = 0; d < 316; ++d) {
+                        for (int64_t j = cnt[d]; j < cnt[d + 1]; j += ppt_tc) {
+                            tcd.push_back(d);
+                            tcb.push_back(j);
+                            tcn.push_back((int32_t)std::min<int64_t>(ppt_tc, cnt[d + 1] - j));
+                        }
+                        for (int64_t j = cnt[d]; j < cnt[d + 1]; j += kGemmPairs) {
+                            sd.push_back(d);
+                            sb.push_back(j);
+                            sn.push_back((int32_t)std::min<int64_t>(kGemmPairs, cnt[d + 1] - j));
+                        }
+                    }
+                    c.tc_nt = (int64_t)tcd.size() - c.tc_t0;
+                    c.s_nt = (int64_t)sd.size() - c.s_t0;
+                    ymax = std::max(ymax, np);
+                }
+                chunks.push_back(c);
+                b = e;
+            }
+        }
+        ck_tc_d.upload(tcd);
+        ck_tc_begin.upload(tcb);
+        ck_tc_count.upload(tcn);
+        ck_s_d.upload(sd);
+        ck_s_begin.upload(sb);
+        ck_s_count.upload(sn);
+        ck_pair_src.upload(ps);
+        v_pos.upload(vp);
+        Y.alloc((size_t)row_bytes * (size_t)(ymax + 1));
+    }
+
+    // M2L products of one chunk into the product buffer, then its boxes' locals
+    void m2l_chunk(const Chunk& c) {
+        if (c.npairs == 0) return;
+        if (kTensor && m2l_path == 1) {
+            if constexpr (kTensor) {
+                const unsigned grid = (unsigned)std::min<int64_t>(c.tc_nt, num_sms);
+                m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                    ck_tc_d.as<int32_t>() + c.tc_t0, ck_tc_begin.as<int64_t>() + c.tc_t0,
+                    ck_tc_count.as<int32_t>() + c.tc_t0, c.tc_nt, ck_pair_src.as<int32_t>() + c.base, m,
+                    tc_bimg.as<uint32_t>(), mmap, vmap, reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+            }
+            return;
+        }
+        m2l_gemm_kernel<P, T><<<counted((unsigned)c.s_nt), 256, gemm_smem, stream>>>(
+            ck_s_d.as<int32_t>() + c.s_t0, ck_s_begin.as<int64_t>() + c.s_t0, ck_s_count.as<int32_t>() + c.s_t0,
+            nullptr, ck_pair_src.as<int32_t>() + c.base, m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
+    }
+    void reduce_chunk(const Chunk& c, int with_l2l, int with_v, int accumulate) {
+        if (c.b1 > c.b0)
+            local_reduce_kernel<P, T><<<counted((unsigned)(c.b1 - c.b0)), round32(NC), 0, stream>>>(
+                dp, c.b0, c.b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
+                Lc.as<T>());
     }
 
     // The fused path's tiles (see m2l_fused.cuh).  A chunk closes once it holds about
@@ -487,6 +595,7 @@ struct Evaluator final : EvaluatorBase {
             build_tc_table_images<P>(m2l, tc_img);
             tc_bimg.upload(tc_img);
             encode_multipole_map<P>(&mmap, reinterpret_cast<const float*>(M.ptr), (int64_t)plan.nboxes() * m);
+            encode_multipole_map<P>(&vmap, reinterpret_cast<const float*>(M.ptr), (int64_t)plan.nboxes() * m, m);
             tc_error.alloc(sizeof(int));
             CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
             CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -723,7 +832,8 @@ struct Evaluator final : EvaluatorBase {
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
                                &near_phi, &near_g, &box_side, &v_pos, &xbox, &fu_tile_d, &fu_tile_begin,
-                               &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img};
+                               &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
+                               &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -775,6 +885,8 @@ struct Evaluator final : EvaluatorBase {
     // P2P launches with accumulate 0 only read them and rewrite the output, the L2P / M2P
     // launches rewrite the same partials.  A last evaluation leaves the output and the
     // launch count as a plain evaluation does.
+    int64_t product_chunks() const override { return (int64_t)chunks.size(); }
+
     void set_m2l_path(int path) override {
         if (path < 0 || path > 2 || (path >= 1 && !kTensor))
             throw Failure(FMMGPU_INVALID_ARGUMENT, "M2L path " + std::to_string(path) + " not available");
@@ -859,6 +971,23 @@ struct Evaluator final : EvaluatorBase {
             timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
             return;
         }
+        if (!chunks.empty()) {
+            // downward, chunked: per level the L2L products, then chunk by chunk the M2L
+            // products and the locals (L2L + V in offset order), then P2L
+            for (int l = 2; l <= L; ++l) {
+                timer.run(kL2L, [&] {
+                    if (l >= 3) l2l_products(l);
+                });
+                for (const Chunk& c : chunks) {
+                    if (c.level != l) continue;
+                    timer.run(kM2L, [&] { m2l_chunk(c); });
+                    timer.run(kL2L, [&] { reduce_chunk(c, l >= 3, 1, 0); });
+                }
+                timer.run(kP2L, [&] { p2l_level(l); });
+            }
+            timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+            return;
+        }
         // M2L products of every level at once (all multipoles are final here)
         timer.run(kM2L, [&] { m2l_products(-1); });
         // downward: for l = 2..L: L2L products, the local (L2L + V in offset order), then P2L
@@ -885,10 +1014,10 @@ struct Evaluator final : EvaluatorBase {
 
     void p2m_rows(int64_t r0, int64_t r1) {  // P2M of leaves [r0, r1)
         if (r1 <= r0) return;
-        if (kBfly && m == 1)
+        if (kBfly)
             expand_bfly_kernel<P, false><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
-                dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), reinterpret_cast<const float*>(sq.ptr),
-                reinterpret_cast<float*>(M.ptr));
+                dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
         else
             expand_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 32, exp_smem(), stream>>>(
                 dp, r0, r1, nullptr, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
@@ -930,11 +1059,9 @@ struct Evaluator final : EvaluatorBase {
                 const DevBuf& tn = l < 0 ? tc_tile_count : tc_ltile_count;
                 if (nt == 0) return;
                 const unsigned grid = (unsigned)std::min<int64_t>(nt, num_sms);
-                for (int v = 0; v < m; ++v)
-                    m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
-                        td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
-                        tc_pair_src.as<int32_t>(), m, v, tc_bimg.as<uint32_t>(), mmap,
-                        reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+                m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                    td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt, tc_pair_src.as<int32_t>(),
+                    m, tc_bimg.as<uint32_t>(), mmap, vmap, reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
             return;
         }
@@ -968,9 +1095,9 @@ struct Evaluator final : EvaluatorBase {
     void p2l_level(int l) {  // the boxes of level l with an X list
         const int64_t b0 = xbox_start[l], b1 = xbox_start[l + 1];
         if (b1 <= b0) return;
-        if (kBfly && m == 1)
+        if (kBfly)
             expand_bfly_kernel<P, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
-                dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr),
+                dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
                 reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
         else
             expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), stream>>>(
@@ -1085,6 +1212,12 @@ struct Evaluator final : EvaluatorBase {
             case FMMGPU_OP_M2L:
                 if (l >= 2 && m2l_path == 2) {
                     m2l_fused(l);
+                } else if (l >= 2 && !chunks.empty()) {
+                    for (const Chunk& c : chunks)
+                        if (c.level == l) {
+                            m2l_chunk(c);
+                            reduce_chunk(c, 0, 1, 1);
+                        }
                 } else if (l >= 2) {
                     m2l_products(l);
                     reduce_locals(l, 0, 1, 1);
@@ -1109,10 +1242,11 @@ template <typename T>
 std::unique_ptr<EvaluatorBase> make_evaluator(int p, const Plan& pl, const std::vector<double>& m2l,
                                               const std::vector<double>& m2m, const std::vector<double>& l2l,
                                               cudaStream_t s, int m, bool grad, const std::vector<double>& us,
-                                              const std::vector<double>& ut, bool fused, size_t* bytes) {
+                                              const std::vector<double>& ut, bool fused, int64_t ybudget,
+                                              size_t* bytes) {
 #define FMMB_CASE(PP)                                                                    \
     case PP: {                                                                           \
-        auto e = std::make_unique<Evaluator<PP, T>>(pl, m2l, m2m, l2l, s, m, grad, us, ut, fused); \
+        auto e = std::make_unique<Evaluator<PP, T>>(pl, m2l, m2m, l2l, s, m, grad, us, ut, fused, ybudget); \
         *bytes = e->device_bytes();                                                      \
         return e;                                                                        \
     }
@@ -1145,6 +1279,7 @@ struct fmmgpu_fmm {
     bool op_begun = false;  // a level-call evaluation has begun
     int mpass = 1;          // charge vectors per evaluator pass (all of them unless memory says no)
     bool fused = false;     // M2L fused with the local reduce on the tensor cores (mixed, p <= 8)
+    int64_t ybudget = 0;    // product buffer bytes of the chunked product path (0: not chunked)
     // whole-evaluation CUDA graph: captured once per (charges, potential, gradient)
     // buffer triple, replayed while the triple and the settings stay the same
     bool graph_on = false;
@@ -1284,6 +1419,7 @@ void fmmgpu_default_settings(fmmgpu_settings* s) {
     s->device = 0;
     s->vectors_per_pass = 0;
     s->autotune = 0;
+    s->product_bytes = 0;
 }
 
 namespace {
@@ -1292,7 +1428,7 @@ void check_settings(const fmmgpu_settings* settings) {
     if (!settings) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
     const fmmgpu_settings& s = *settings;
     if (s.p < 0 || s.vectors < 1 || s.max_points_per_leaf < 1 || s.max_level < 0 || s.max_level > 16 ||
-        s.vectors_per_pass < 0 || s.autotune < 0 || s.autotune > 1)
+        s.vectors_per_pass < 0 || s.autotune < 0 || s.autotune > 1 || s.product_bytes < 0)
         throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid settings");
     if (s.precision != FMMGPU_PRECISION_F64 && s.precision != FMMGPU_PRECISION_MIXED)
         throw Failure(FMMGPU_UNSUPPORTED, "unknown precision");
@@ -1416,34 +1552,47 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
     // writing and re-reading the products)
     f->fused = false;
     // vectors per pass: every per-vector buffer (expansions, translation products, partial
-    // outputs) for as many vectors as fit in 60% of the free memory
+    // outputs) for as many vectors as fit in 60% of the free memory.  The M2L products (Y:
+    // one row per V pair and vector) are held for every pair at once when they fit beside
+    // the rest; otherwise in a buffer of at most 20% of the free memory, filled chunk by
+    // chunk (the chunked product path: the same floats)
     {
-        const size_t nc = (size_t)(s.p + 1) * (s.p + 1), ys = (nc + 31) / 32 * 32;
+        const size_t nc = (size_t)(s.p + 1) * (s.p + 1), ys = (nc + 31) / 32 * 32, ms = (nc + 3) / 4 * 4;
         const size_t tsz = s.precision == FMMGPU_PRECISION_F64 ? 8 : 4;
         const size_t nsrc = P.src_perm.size(), ntgt = P.tgt_perm.size();
-        // the fused M2L keeps no product array (Y: one row per V pair and vector)
-        const size_t y_rows = f->fused ? 0 : P.v.nnz() + 1;
-        const size_t per_vec = tsz * (2 * P.nboxes() * nc + P.nboxes() * ys + y_rows * ys + nsrc) +
-                               (tsz == 4 ? 8 * nsrc : 0) + 8 * ntgt * (s.gradients ? 4 : 1) * 2 +
-                               8 * ntgt * (s.gradients ? 4 : 1) + 8 * nsrc;
+        const size_t y_vec = f->fused ? 0 : tsz * ys * (P.v.nnz() + 1);
+        const size_t per_vec = tsz * (2 * P.nboxes() * ms + P.nboxes() * ys + nsrc) + (tsz == 4 ? 8 * nsrc : 0) +
+                               8 * ntgt * (s.gradients ? 4 : 1) * 2 + 8 * ntgt * (s.gradients ? 4 : 1) + 8 * nsrc;
         size_t free_b = 0, total_b = 0;
         CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-        const size_t fit = per_vec ? (size_t)(0.6 * (double)free_b) / per_vec : (size_t)s.vectors;
+        const size_t budget = (size_t)(0.6 * (double)free_b);
+        const size_t y_all = y_vec * (size_t)s.vectors;
+        size_t ycap = 0;  // product buffer bytes when chunked
+        size_t fit = (size_t)s.vectors;
+        if (s.product_bytes > 0) {
+            ycap = (size_t)s.product_bytes;
+            fit = budget > ycap && per_vec ? (budget - ycap) / per_vec : 1;
+        } else if (per_vec * (size_t)s.vectors + y_all > budget) {
+            ycap = std::min(y_all, (size_t)(0.2 * (double)free_b));
+            fit = budget > ycap && per_vec ? (budget - ycap) / per_vec : 1;
+        }
         int want = (int)std::max<size_t>(1, std::min<size_t>((size_t)s.vectors, fit));
         if (s.vectors_per_pass > 0) want = std::min(s.vectors_per_pass, s.vectors);
         if (f->fused) want = std::min(want, fused_tile_columns(s.p));
+        if (s.precision == FMMGPU_PRECISION_MIXED && s.p <= 8) want = std::min(want, tc_tile_columns(s.p));
         // every pass holds the same number of vectors (the buffers' and the kernels' m): the
         // largest divisor of the vector count not above the wanted size
         while (s.vectors % want) --want;
         f->mpass = want;
+        f->ybudget = (ycap > 0 && y_vec * (size_t)want > ycap) ? (int64_t)ycap : 0;
     }
     size_t bytes = 0;
     if (s.precision == FMMGPU_PRECISION_F64)
         f->eval = make_evaluator<double>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, f->mpass, s.gradients != 0, us,
-                                         ut, false, &bytes);
+                                         ut, false, f->ybudget, &bytes);
     else
         f->eval = make_evaluator<float>(s.p, P, f->m2l, f->m2m, f->l2l, f->stream, f->mpass, s.gradients != 0, us,
-                                        ut, f->fused, &bytes);
+                                        ut, f->fused, f->ybudget, &bytes);
     f->eval->qstride = s.vectors;
     const size_t ns = P.src_perm.size(), nt = P.tgt_perm.size();
     f->d_charges.alloc(sizeof(double) * (size_t)s.vectors * (ns + 1));
@@ -1819,6 +1968,7 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->vectors_per_pass = f->eval ? f->mpass : 0;
         info->p2p_warps = f->eval ? f->eval->p2p_warps : 0;
         info->leaf_block = f->eval ? f->eval->leaf_block : 0;
+        info->product_chunks = f->eval ? f->eval->product_chunks() : 0;
     });
 }
 

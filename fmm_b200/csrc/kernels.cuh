@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
 template <int P, bool IRREG>
 __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
                                                          const int32_t* __restrict__ rows,
-                                                         const float4* __restrict__ spos,
+                                                         const float4* __restrict__ spos, int m,
                                                          const float* __restrict__ sq, float* __restrict__ out) {
     constexpr int NC = nc_of(P);
     constexpr int NCP = ((NC + 31) / 32) * 32;
@@ -219,6 +219,9 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
         nent = (int)(plan.x_row[row + 1] - ent0);
         if (nent == 0) return;
     }
+    // the charge vectors one after the other (charges [v][point], expansions [box][v])
+    for (int v = 0; v < m; ++v) {
+    const float* qv = sq + (int64_t)v * plan.nsrc;
     float w[NCP];
 #pragma unroll
     for (int c = 0; c < NCP; ++c) w[c] = 0.0f;
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
         const int64_t s1 = plan.src_start[sleaf + 1];
         for (int64_t si = plan.src_start[sleaf] + lane; si < s1; si += 32) {
             const float4 p4 = spos[si];
-            const float q = sq[si];
+            const float q = qv[si];
             const float x = (p4.x - fc[0]) * finv, y = (p4.y - fc[1]) * finv, z = (p4.z - fc[2]) * finv;
             if (!IRREG) {
                 RegularRows<P, float> h;
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
 #pragma unroll
     for (int s = 16, len = NCP / 2; s >= 1; s >>= 1, len >>= 1)
         if (lane & s) base += len;
-    float* o = out + (int64_t)box * ms_of(P);
+    float* o = out + ((int64_t)box * m + v) * ms_of(P);
 #pragma unroll
     for (int i = 0; i < NCP / 32; ++i) {
         const int c = base + i;
@@ -283,6 +286,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
             if (IRREG) o[c] += w[i];
             else o[c] = w[i];
         }
+    }
     }
 }
 

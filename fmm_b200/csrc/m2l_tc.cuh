@@ -125,6 +125,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 
 // returns true when the barrier's phase `parity` completed within `limit` clock cycles;
 // false on timeout or when *abort is set (another role gave up)
+// Each try_wait may suspend the thread until the phase completes or kWaitHintNs elapse
+// (a hint to the hardware), so a waiting warp takes few issue slots from the working ones;
+// the bound and the abort flag are checked between tries.
+constexpr uint32_t kWaitHintNs = 20000;
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, long long limit,
                                                   const volatile int* abort = nullptr) {
     const long long start = clock64();
@@ -133,11 +137,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
         asm volatile(
             "{\n\t"
             ".reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t"
             "}\n"
             : "=r"(done)
-            : "r"(mbar), "r"(parity)
+            : "r"(mbar), "r"(parity), "r"(kWaitHintNs)
             : "memory");
         if (done) return true;
         if (abort && *abort) return false;
@@ -170,12 +174,14 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 // with the gathered multipoles X as the shared-memory B operand (N = NT pairs,
 // K-major, 128-byte swizzled).  Roles, coupled only by mbarriers (no block barrier in
 // the loop):
-//   warp 17 (gather): for tile k, once the raw stage k % 2 is free, each lane fetches
-//     four multipole rows with one tensor-memory-access gather (tile::gather4; box one
-//     row of KP f32, the row's slots beyond (p+1)^2 filled with zeros by the copy
-//     engine) into the raw stage, completion counted on raw_full; the copy engine keeps
-//     the whole tile's rows in flight at once, where per-lane loads were limited by the
-//     SM's outstanding misses;
+//   warp 17 (gather): for tile k, once the raw stage k % 2 is free, the lanes fetch the
+//     tile's multipole rows with the copy engine into the raw stage, completion counted
+//     on raw_full: with fewer than four vectors each lane fetches four rows with one
+//     tile::gather4 (box one row of KP f32, the slots beyond (p+1)^2 filled with zeros);
+//     with m >= 4 the m vectors of a pair are m consecutive rows and lane j fetches pair
+//     j's with one 2D tile load (box m rows).  The copy engine keeps the whole tile's
+//     rows in flight at once, where per-lane loads were limited by the SM's outstanding
+//     misses;
 //   warps 8-15 (converters): wait raw_full, split the raw rows into X stage k&1
 //     (x = hi + lo in tf32, 128-byte swizzled) once MMA(k-2) has released it
 //     (empty[k&1]), signal full[k&1] and raw_empty; warps 8-11 also replace the table in
@@ -189,7 +195,9 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 //     then release acc_empty[k&1].
 // Every wait is bounded; a role that gives up sets the shared abort flag (which ends
 // the other roles' waits) and *error, and the CTA frees its tensor memory and returns.
-// One vector per launch.
+// A tile holds cnt <= NT / m pairs of one offset with all m charge vectors: column
+// c is pair c / m, vector c % m, its product row in Y is p0 * m + c (the pair's rows are
+// its m vectors in order).
 constexpr int kTcWarps = 18;
 constexpr int kTcProd = 8;        // converter warps (8..15)
 constexpr int kTcMmaWarp = 16;    // the MMA issuer's warp
@@ -250,6 +258,16 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
 
 // four rows (r0..r3) of a 2D tensor map, one box each (KP f32 at x = 0), into dst
 // (four consecutive box rows), completion counted on mbar; no multicast
+// one box (x = 0, first row y) of a 2D tensor map into dst, completion counted on mbar;
+// no multicast
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int y, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(mbar)
+        : "memory");
+}
+
 __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* map, int r0, int r1, int r2, int r3,
                                             uint32_t mbar) {
     asm volatile(
@@ -264,9 +282,10 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   const int64_t* __restrict__ tile_begin,
                                                                   const int32_t* __restrict__ tile_count,
                                                                   int64_t ntiles,
-                                                                  const int32_t* __restrict__ pair_src, int m, int v,
+                                                                  const int32_t* __restrict__ pair_src, int m,
                                                                   const uint32_t* __restrict__ timg,
                                                                   const __grid_constant__ CUtensorMap mmap,
+                                                                  const __grid_constant__ CUtensorMap vmap,
                                                                   float* __restrict__ Y, int* __restrict__ error) {
     using S = TcTs<P>;
     constexpr int NT = S::NT, KP = S::KP;
@@ -323,29 +342,41 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     };
 
     if (warp == kTcGatherWarp) {
-        // ---------------- gather: four rows a lane ----------------
+        // ---------------- gather ----------------
+        const bool blocks = m >= 4;        // one box of m rows a pair
+        const int ppt = NT / m;            // pairs a tile holds
+        const uint32_t tx = blocks ? (uint32_t)(ppt * m * KP * 4) : (uint32_t)S::X_BYTES;
         int64_t issued = 0;
         for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
             const int64_t it = i0 + k;
             const int rs = (int)(k & 1);
             const int64_t p0 = tile_begin[it];
-            const int cnt = tile_count[it];
+            const int ncol = tile_count[it] * m;
+            // rows past the tile's columns fetch row 0 (their products are never stored)
             int r[4];
+            if (blocks) {
+                r[0] = (lane < ppt && lane * m < ncol) ? pair_src[p0 + lane] * m : 0;
+            } else {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int row = 4 * lane + j;
-                // rows past the tile's pairs fetch row 0 (their products are never stored)
-                r[j] = (row < cnt) ? pair_src[p0 + row] * m + v : 0;
+                for (int j = 0; j < 4; ++j) {
+                    const int c = 4 * lane + j;
+                    r[j] = (c < ncol) ? pair_src[p0 + c / m] * m + c % m : 0;
+                }
             }
             if (k >= 2 && !warp_wait(&bar_rempty[rs], (uint32_t)(((k - 2) >> 1) & 1))) {
                 if (lane == 0) give_up();
                 break;
             }
-            if (lane == 0) mbar_expect_tx(smem_u32(&bar_rfull[rs]), (uint32_t)S::X_BYTES);
+            if (lane == 0) mbar_expect_tx(smem_u32(&bar_rfull[rs]), tx);
             __syncwarp();
-            if (4 * lane < NT)
-                tma_gather4(smem_u32(rbuf + (size_t)rs * S::X_BYTES + (size_t)4 * lane * KP * 4), &mmap, r[0], r[1],
-                            r[2], r[3], smem_u32(&bar_rfull[rs]));
+            unsigned char* dst = rbuf + (size_t)rs * S::X_BYTES;
+            if (blocks) {
+                if (lane < ppt)
+                    tma_load_2d(smem_u32(dst + (size_t)lane * m * KP * 4), &vmap, r[0], smem_u32(&bar_rfull[rs]));
+            } else if (4 * lane < NT) {
+                tma_gather4(smem_u32(dst + (size_t)4 * lane * KP * 4), &mmap, r[0], r[1], r[2], r[3],
+                            smem_u32(&bar_rfull[rs]));
+            }
             issued = k + 1;
         }
         // on a give-up, the gathers still in flight land before the shared memory is released
@@ -491,25 +522,24 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             const int64_t it = i0 + k;
             const int st = (int)(k & 1);
             const int64_t p0 = tile_begin[it];
-            const int cnt = tile_count[it];
+            const int ncol = tile_count[it] * m;
             if (!warp_wait(&bar_accf[st], (uint32_t)((k >> 1) & 1))) {
                 if (lane == 0) give_up();
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (32 * q < ys_of(P)) {
-                // products at their pair positions p0 + c (a tile's rows are consecutive), whole
-                // 128-byte lines (rows >= NC of the table are zero), 16 columns per TMEM load
+                // products at rows p0 * m + c (a tile's rows are consecutive), whole 128-byte
+                // lines (rows >= NC of the table are zero), 16 columns per TMEM load
 #pragma unroll 1
                 for (int c0 = (NT / 2) * g; c0 < (NT / 2) * (g + 1); c0 += 16) {
-                    if (c0 >= cnt) break;
+                    if (c0 >= ncol) break;
                     float v0[16];
                     tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * NT + c0), v0);
-                    float* yb = Y + ((p0 + c0) * m + v) * ys_of(P) + n;
-                    const int64_t row = (int64_t)m * ys_of(P);
+                    float* yb = Y + (p0 * m + c0) * ys_of(P) + n;
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
-                        if (c0 + i < cnt) __stcs(yb + i * row, v0[i]);
+                        if (c0 + i < ncol) __stcs(yb + (int64_t)i * ys_of(P), v0[i]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
@@ -525,12 +555,15 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     }
 }
 
+// columns (pairs x vectors) of a tensor-core M2L tile for the compiled degrees
+inline int tc_tile_columns(int p) { return p == 3 ? TcTs<3>::NT : p == 6 ? TcTs<6>::NT : TcTs<8>::NT; }
+
 // Host: the tensor map of the multipoles for the gathers: 2D, rows (box * m + vector) of
 // ms_of(P) f32 (16-byte multiples), the inner extent (p+1)^2 so that a box of KP slots
-// reads zeros past the row's coefficients; boxes of one row, no swizzle.  The driver's
-// encoder is fetched through the runtime (no link against the driver library).
+// reads zeros past the row's coefficients; boxes of box_rows rows, no swizzle.  The
+// driver's encoder is fetched through the runtime (no link against the driver library).
 template <int P>
-void encode_multipole_map(CUtensorMap* map, const float* M, int64_t rows) {
+void encode_multipole_map(CUtensorMap* map, const float* M, int64_t rows, int box_rows = 1) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         cudaDriverEntryPointQueryResult q{};
@@ -542,7 +575,7 @@ void encode_multipole_map(CUtensorMap* map, const float* M, int64_t rows) {
     }
     const cuuint64_t dim[2] = {(cuuint64_t)nc_of(P), (cuuint64_t)(rows > 0 ? rows : 1)};
     const cuuint64_t stride[1] = {(cuuint64_t)ms_of(P) * 4};
-    const cuuint32_t box[2] = {(cuuint32_t)TcTs<P>::KP, 1};
+    const cuuint32_t box[2] = {(cuuint32_t)TcTs<P>::KP, (cuuint32_t)box_rows};
     const cuuint32_t estride[2] = {1, 1};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(M), dim, stride, box,
                               estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

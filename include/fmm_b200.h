@@ -64,6 +64,11 @@ typedef struct {
                                  (fmm-exec/src/fmm.rs:291-300, FmmBuilder::tuning_cache, with
                                  no cache file); 0 (default): the static shapes.  The results
                                  are the same bits either way */
+    int64_t product_bytes;    /* M2L product buffer: 0 (default) every V pair's products at
+                                 once when they fit beside the rest (else at most 20% of the
+                                 free memory); > 0 at most this many bytes, the products
+                                 then made and reduced level by level in chunks of target
+                                 boxes.  The results do not depend on it */
 } fmmgpu_settings;
 
 typedef struct {
@@ -78,6 +83,7 @@ typedef struct {
     int64_t vectors_per_pass;  /* charge vectors per device pass (0 for a plan-only handle) */
     int64_t p2p_warps;    /* warps a block of the mixed P2P kernel (static 4, or the tuned one) */
     int64_t leaf_block;   /* threads a block of the L2P / M2P kernel (static 64, or the tuned one) */
+    int64_t product_chunks; /* chunks of the M2L product path (0: every product at once) */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;

@@ -83,9 +83,10 @@ def test_fused_vectors_beyond_one_tile(oracle):
 
 
 def test_fused_refuses_too_many_vectors(oracle):
+    """At p = 8 a pass holds up to a tensor-core tile's 96 columns, the fused M2L 64."""
     x, q = oracle.point_sets("cube", 3000, 14)
-    fmm = F.FmmBuilder(6).vectors(130).max_points_per_leaf(32).precision("mixed").build(x)
-    assert fmm.info()["vectors_per_pass"] == 130
-    with pytest.raises(F.FmmError, match="at most 128"):
+    fmm = F.FmmBuilder(8).vectors(96).max_points_per_leaf(32).precision("mixed").build(x)
+    assert fmm.info()["vectors_per_pass"] == 96
+    with pytest.raises(F.FmmError, match="at most 64"):
         fmm.set_m2l_path(2)
     fmm.close()
