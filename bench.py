@@ -329,6 +329,13 @@ def run_ours(args):
     perr = float(np.linalg.norm(pphi[sample] - ex_phi) / np.linalg.norm(ex_phi))
     plain.close()
 
+    # the batched workload: every rank its share of the clouds (all ranks take part)
+    batched = None
+    if not args.no_batched:
+        try:
+            batched = run_batched(F, torch, dev, flush, rank, world)
+        except Exception as e:  # reported, never fatal to the headline line
+            batched = {"error": f"{type(e).__name__}: {str(e)[:200]}"}
     if rank != 0:
         if world > 1:
             torch.distributed.barrier()
@@ -397,11 +404,8 @@ def run_ours(args):
     }
     line["gpu_launches"] = launches_per_step * args.steps
     line["gpu_launches_per_step"] = launches_per_step
-    if not args.no_batched and world == 1:
-        try:
-            line["batched"] = run_batched(F, torch, dev, flush)
-        except Exception as e:  # reported, never fatal to the headline line
-            line["batched"] = {"error": f"{type(e).__name__}: {str(e)[:200]}"}
+    if batched is not None:
+        line["batched"] = batched
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
@@ -410,20 +414,33 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
-def run_batched(F, torch, dev, flush, steps=3, warmup=1):
+def run_batched(F, torch, dev, flush, rank=0, world=1, steps=3, warmup=1):
     """The batched workload (256 clouds, 16 vectors, p = 6, 64 per leaf, potentials) as one
     forest: mixed and plain f64, device-timed like the headline, with the error of the
-    first vector at sampled targets of the first clouds against the GPU f64 direct sum."""
-    clouds, q, kinds = batched_problem()
+    first vector at sampled targets of the first clouds against the GPU f64 direct sum.
+    On several ranks each rank takes its share of the clouds (fmm_b200.multigpu), the
+    times are the slowest rank's and the value counts every rank's points.  Every rank
+    takes the same collective steps, failures included."""
+    from fmm_b200.multigpu import max_over_ranks, shard_clouds
+
+    all_clouds, all_q, kinds = batched_problem()
+    n_all = int(sum(len(c) for c in all_clouds))
+    offs = np.concatenate([[0], np.cumsum([len(c) for c in all_clouds])])
+    mine = shard_clouds([len(c) for c in all_clouds], world)[rank]
+    clouds = [all_clouds[i] for i in mine]
+    q = np.ascontiguousarray(np.concatenate([all_q[offs[i]:offs[i + 1]] for i in mine]))
     n = int(sum(len(c) for c in clouds))
     m = BATCH_VECTORS
-    log(f"batched: {len(clouds)} clouds, {n} points, {m} vectors")
+    log(f"batched: {len(clouds)} of {len(all_clouds)} clouds, {n} of {n_all} points, {m} vectors")
     dq = torch.from_numpy(q).to(dev)
     dphi = torch.empty(m * n, dtype=torch.float64, device=dev)
-    res = {"workload": f"{len(clouds)} clouds, N_i log-uniform in [1e4, 5e5] (cube / sphere / Plummer a=0.1 "
+    res = {"workload": f"{len(all_clouds)} clouds, N_i log-uniform in [1e4, 5e5] (cube / sphere / Plummer a=0.1 "
                        f"clipped at r=5), {m} vectors U[-1,1), p={BATCH_P}, {BATCH_LEAF} per leaf, potentials",
-           "n_points": n, "vectors": m, "clouds_by_geometry": [int((kinds == i).sum()) for i in range(3)],
+           "n_points": n_all, "vectors": m, "clouds_by_geometry": [int((kinds == i).sum()) for i in range(3)],
            "data": "synthetic (numpy PCG64, seeded)"}
+    if world > 1:
+        res["sharding"] = f"clouds dealt to {world} ranks by points (largest first), no data-path collective; " \
+                          "times are the slowest rank's"
 
     def timed(f):
         stream = torch.cuda.ExternalStream(f.stream)
@@ -446,30 +463,43 @@ def run_batched(F, torch, dev, flush, steps=3, warmup=1):
 
     for precision in ("mixed", "f64"):
         t0 = time.perf_counter()
-        f = (F.FmmBuilder(BATCH_P).vectors(m).max_points_per_leaf(BATCH_LEAF).precision(precision)
-             .autotune().build_batch(clouds))
-        build_s = time.perf_counter() - t0
-        info = f.info()
-        ms = timed(f)
-        log(f"batched {precision}: build {build_s:.1f} s, {ms:.2f} ms/step")
+        try:
+            f = (F.FmmBuilder(BATCH_P).vectors(m).max_points_per_leaf(BATCH_LEAF).precision(precision)
+                 .autotune().build_batch(clouds))
+            build_s = time.perf_counter() - t0
+            info = f.info()
+            ms = timed(f)
+        except Exception as e:  # this rank failed: the others still take the collective below
+            log(f"batched {precision} failed: {e}")
+            f, ms = None, float("inf")
+        ms = max_over_ranks(ms, dev)
+        if f is None or not np.isfinite(ms):
+            if f is not None:
+                f.close()
+            raise RuntimeError(f"batched {precision}: a rank failed")
+        log(f"batched {precision}: build {build_s:.1f} s, {ms:.2f} ms/step (slowest rank)")
         if precision == "mixed":
-            res.update({"ms_per_step": round(ms, 3), "value": round(n / (ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
-                        "point_vectors_per_s": round(n * m / (ms * 1e-3) / 1e6, 1), "build_s": round(build_s, 2),
+            res.update({"ms_per_step": round(ms, 3), "value": round(n_all / (ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
+                        "point_vectors_per_s": round(n_all * m / (ms * 1e-3) / 1e6, 1), "build_s": round(build_s, 2),
                         "launches_per_step": f.info()["launches"],
                         "launch_shapes": {"p2p_warps": info["p2p_warps"], "leaf_block": info["leaf_block"]},
                         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs")}})
-            # error of vector 0 at 250 sampled targets in each of the first 4 clouds
-            phi = dphi.view(m, n)[0].cpu().numpy()
-            errs, off = [], 0
-            for c in range(4):
-                x = clouds[c]
-                pick = np.linspace(0, len(x) - 1, 250).astype(np.int64)
-                ex, _ = F.direct_sum(x, q[off:off + len(x), 0], x[pick], gradients=False)
-                errs.append(float(np.linalg.norm(phi[off + pick] - ex) / np.linalg.norm(ex)))
-                off += len(x)
-            res["phi_rel_l2_first_clouds"] = errs
+            # error of vector 0 at 250 sampled targets in each of this rank's first 4 clouds
+            # (local work between collectives: a failure here is recorded, not raised)
+            try:
+                phi = dphi.view(m, n)[0].cpu().numpy()
+                errs, off = [], 0
+                for c in range(min(4, len(clouds))):
+                    x = clouds[c]
+                    pick = np.linspace(0, len(x) - 1, 250).astype(np.int64)
+                    ex, _ = F.direct_sum(x, q[off:off + len(x), 0], x[pick], gradients=False)
+                    errs.append(float(np.linalg.norm(phi[off + pick] - ex) / np.linalg.norm(ex)))
+                    off += len(x)
+                res["phi_rel_l2_first_clouds"] = errs
+            except Exception as e:
+                res["phi_rel_l2_first_clouds"] = f"failed: {type(e).__name__}: {str(e)[:120]}"
         else:
-            res["plain_f64"] = {"ms_per_step": round(ms, 3), "value": round(n / (ms * 1e-3) / 1e6, 3)}
+            res["plain_f64"] = {"ms_per_step": round(ms, 3), "value": round(n_all / (ms * 1e-3) / 1e6, 3)}
         f.close()
     res["mixed_over_plain"] = round(res["plain_f64"]["ms_per_step"] / res["ms_per_step"], 3)
     del dq, dphi
