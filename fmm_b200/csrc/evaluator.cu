@@ -1107,6 +1107,14 @@ struct Evaluator final : EvaluatorBase {
     void leaf_far(int64_t r0, int64_t r1, int mode) {  // L2P / M2P of leaves [r0, r1)
         if (r1 <= r0) return;
         const size_t smem = sizeof(T) == 8 ? NC * sizeof(T) : 0;
+        if constexpr (kMixed) {
+            if (!gradients) {  // potentials: the harmonics shared by up to 8 vectors (any m: the same floats)
+                leaf_far_mv_kernel<P, 8><<<counted((unsigned)(r1 - r0)), leaf_block, 0, stream>>>(
+                    dp, r0, mode, m, reinterpret_cast<const float4*>(tpos.ptr), reinterpret_cast<const float*>(M.ptr),
+                    reinterpret_cast<const float*>(Lc.ptr), far_phi.as<double>());
+                return;
+            }
+        }
         if (gradients)
             leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), leaf_block, smem, stream>>>(
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
@@ -1122,6 +1130,11 @@ struct Evaluator final : EvaluatorBase {
         const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
         const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
         const auto* q = reinterpret_cast<const float*>(sq.ptr);
+        if (!gradients) {  // potentials: the pair geometry shared by up to kX2Vb vectors (any m)
+            p2p_x2_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q,
+                                                             tp, close, far_phi.as<double>(), accumulate, d_phi);
+            return;
+        }
         if (gradients)
             p2p_x2_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp,
                                                                q, tp, close, far_phi.as<double>(), fg, accumulate,

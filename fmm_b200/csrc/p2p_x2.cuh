@@ -281,4 +281,188 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
     }
 }
 
+// Potentials of several charge vectors (no gradients): the flush stages the sources'
+// positions once and the charges of VB vectors; a pair-step forms the pair geometry (d, r2,
+// the rsqrt and its near-singular select) once and adds q rinv for each vector.  Per
+// vector every operation and its order are p2p_x2_kernel<false, W>'s (the same flushes,
+// the same pair-steps, the same f64 additions), so the floats do not depend on how many
+// vectors a pass holds; the evaluation uses this kernel for every vector count.
+constexpr int kX2Vb = 4;  // vectors a flush
+
+template <int W>
+__global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
+    DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
+    const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
+    double* __restrict__ far_phi, int accumulate, double* __restrict__ out_phi) {
+    constexpr int VB = kX2Vb;
+    __shared__ float4 sxy[W][kX2Stage / 2];       // (x0, x1, y0, y1) in the target's frame
+    __shared__ float2 szz[W][kX2Stage / 2];       // (z0, z1)
+    __shared__ float2 sqq[W][VB][kX2Stage / 2];   // (q0, q1) of each vector
+    __shared__ float4 raw[W][kX2Stage];           // the next flush's points, as loaded
+    __shared__ float rawq[W][VB][kX2Stage];
+    __shared__ int rawrec[W][kX2Stage];
+    __shared__ NearRec srec[W][kX2Recs];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the split lanes' sums (VB x 32 doubles), reduced per target, in the pair buffer
+    double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[warp][0]);
+    static_assert(VB * 32 * sizeof(double) <= sizeof(float4) * (kX2Stage / 2), "reduction buffer");
+    const int64_t item = (int64_t)blockIdx.x * W + warp;
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int box = plan.leaf_box[leaf];
+    const int64_t t1 = plan.tgt_start[leaf + 1];
+    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int K = 32 / ni;
+    const int kk = lane < ni * K ? lane / ni : K;
+    const int ti = lane < ni * K ? lane % ni : 0;
+    const int64_t t = items.t0[item] + ti;
+    const bool valid = lane < ni;
+    const int64_t n0 = plan.near_row[leaf], n1 = near ? plan.near_row[leaf + 1] : n0;
+    const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    if (kk < K) {
+        const float4 p4 = tpos[t];
+        tx = p4.x;
+        ty = p4.y;
+        tz = p4.z;
+    }
+    const float2 ntx = f2(-tx, -tx), nty = f2(-ty, -ty), ntz = f2(-tz, -tz);
+    float* sxy_f = reinterpret_cast<float*>(sxy[warp]);
+    float* szz_f = reinterpret_cast<float*>(szz[warp]);
+    const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
+    const double phi_scale = 4.0 * 3.141592653589793 * rt;
+    const int nr = (int)(n1 - n0);
+    for (int j = lane; j < nr; j += 32) srec[warp][j] = recs[n0 + j];
+    __syncwarp();
+    const int S = nr ? srec[warp][nr - 1].off + srec[warp][nr - 1].ns : 0;
+    const int nfl = S > 0 ? (S + kX2Stage - 1) / kX2Stage : 1;
+    const int nvb = (m + VB - 1) / VB;
+    const int total = nfl * nvb;
+    int epf = 0;
+    auto issue = [&](int f) {
+        const int vb = f / nfl, base = (f - vb * nfl) * kX2Stage;
+        const int v0 = vb * VB, nb = (m - v0) < VB ? (m - v0) : VB;
+        const int cnt = (S - base) < kX2Stage ? (S - base) : kX2Stage;
+        if (base == 0) epf = 0;
+#pragma unroll
+        for (int i = 0; i < kX2Stage / 32; ++i) {
+            const int k = lane + 32 * i;
+            if (k < cnt) {
+                const int pos = base + k;
+                while (srec[warp][epf].off + srec[warp][epf].ns <= pos) ++epf;
+                const int64_t s = srec[warp][epf].s0 + (pos - srec[warp][epf].off);
+                cp_async16(&raw[warp][k], spos + s);
+#pragma unroll
+                for (int b = 0; b < VB; ++b)
+                    if (b < nb) cp_async4(&rawq[warp][b][k], sq + (int64_t)(v0 + b) * nsrc + s);
+                rawrec[warp][k] = epf;
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    double aphi[VB];
+#pragma unroll
+    for (int b = 0; b < VB; ++b) aphi[b] = 0.0;
+    issue(0);
+    for (int f = 0; f < total; ++f) {
+        const int vb = f / nfl, base = (f - vb * nfl) * kX2Stage;
+        const int v0 = vb * VB, nb = (m - v0) < VB ? (m - v0) : VB;
+        const int cnt = (S - base) < kX2Stage ? (S - base) : kX2Stage;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kX2Stage / 32; ++i) {
+            const int k = lane + 32 * i;
+            if (k < cnt) {
+                const float4 p = raw[warp][k];
+                const float4 fr = srec[warp][rawrec[warp][k]].frame;
+                const int slot = (k >> 1) * 4 + (k & 1);
+                sxy_f[slot] = __fmaf_rn(fr.w, p.x, fr.x);
+                sxy_f[slot + 2] = __fmaf_rn(fr.w, p.y, fr.y);
+                szz_f[k] = __fmaf_rn(fr.w, p.z, fr.z);
+#pragma unroll
+                for (int b = 0; b < VB; ++b)
+                    if (b < nb) reinterpret_cast<float*>(sqq[warp][b])[k] = rawq[warp][b][k];
+            }
+        }
+        if ((cnt & 1) && lane == 0) {  // odd count: a zero charge completes the last pair
+            const int slot = (cnt >> 1) * 4 + 1;
+            sxy_f[slot] = 0.f;
+            sxy_f[slot + 2] = 0.f;
+            szz_f[cnt] = 0.f;
+#pragma unroll
+            for (int b = 0; b < VB; ++b) reinterpret_cast<float*>(sqq[warp][b])[cnt] = 0.f;
+        }
+        __syncwarp();
+        if (f + 1 < total) issue(f + 1);
+        float2 pphi[VB];
+#pragma unroll
+        for (int b = 0; b < VB; ++b) pphi[b] = f2(0.f, 0.f);
+        const int npairs = (cnt + 1) >> 1;
+#pragma unroll 2
+        for (int i = kk; i < npairs; i += K) {
+            const float4 a = sxy[warp][i];
+            const float2 zz = szz[warp][i];
+            const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
+            const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
+            const float2 dz = __fadd2_rn(zz, ntz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
+            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float2 rinv = f2(ri0, ri1);
+#pragma unroll
+            for (int b = 0; b < VB; ++b)
+                if (b < nb) pphi[b] = __fadd2_rn(pphi[b], __fmul2_rn(sqq[warp][b][i], rinv));
+        }
+#pragma unroll
+        for (int b = 0; b < VB; ++b) {
+            aphi[b] += (double)pphi[b].x;
+            aphi[b] += (double)pphi[b].y;
+        }
+        __syncwarp();  // the pairs are read before the next map overwrites them
+        if (f - vb * nfl != nfl - 1) continue;
+        // ---- the last flush of vectors v0 .. v0 + nb: finish their targets ----
+        if (K > 1) {
+#pragma unroll
+            for (int b = 0; b < VB; ++b) red[b][lane] = aphi[b];
+            __syncwarp();
+            if (valid)
+                for (int j = 1; j < K; ++j)
+#pragma unroll
+                    for (int b = 0; b < VB; ++b) aphi[b] += red[b][ti + ni * j];
+            __syncwarp();
+        }
+        if (valid) {
+            if (near) {
+                const double4 u = close.tpos[t];
+                for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
+                    const double4 y = close.y[c2];
+                    if (u.x == y.x && u.y == y.y && u.z == y.z) continue;
+                    const double dx = u.x - y.x, dy = u.y - y.y, dz = u.z - y.z;
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    const double rinv = rsqrt(r2);
+#pragma unroll
+                    for (int b = 0; b < VB; ++b)
+                        if (b < nb) aphi[b] += close.q[(int64_t)(v0 + b) * nsrc + close.src[c2]] * rinv;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < VB; ++b) {
+                if (b >= nb) break;
+                const int v = v0 + b;
+                if (accumulate == 2) {
+                    out_phi[(int64_t)v * nt + t] = aphi[b];
+                } else if (accumulate) {
+                    far_phi[(int64_t)v * nt + t] = far_phi[(int64_t)v * nt + t] + aphi[b];
+                } else {
+                    const double ph = far_phi[(int64_t)v * nt + t] + aphi[b];
+                    out_phi[(int64_t)v * nt + plan.tgt_perm[t]] = ph / phi_scale;
+                }
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < VB; ++b) aphi[b] = 0.0;
+    }
+}
+
 }  // namespace fmmb

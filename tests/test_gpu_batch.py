@@ -72,3 +72,23 @@ def test_vector_passes_give_the_same_floats(oracle, precision):
         assert np.array_equal(out.potential, one.potential)
     hq = q + 0.5j * q[::-1]
     assert np.array_equal(two.helmholtz_near(3.0, hq).potential, base.build(x).helmholtz_near(3.0, hq).potential)
+
+
+def test_potentials_multi_vector_kernels_independent_of_pass_size(oracle):
+    """Mixed potentials of 8 vectors: the P2P and L2P/M2P kernels share the pair geometry
+    and the harmonics across vectors; 1, 2 or 8 vectors a pass give the same bits, and the
+    FMM agrees with the oracle."""
+    x, q = oracle.point_sets("cube", 25000, 17)
+    m = 8
+    qq = np.stack([q * (1.0 + 0.3 * v) * (-1) ** v for v in range(m)], axis=1)
+    outs = []
+    for vpp in (1, 2, 8):
+        f = F.FmmBuilder(6).vectors(m).max_points_per_leaf(32).precision("mixed").vectors_per_pass(vpp).build(x)
+        assert f.info()["vectors_per_pass"] == vpp
+        outs.append(f.evaluate(qq).potential)
+        f.close()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    phi, _ = oracle.fmm(x, qq, x, 6, 32, gradients=False, threads=8)
+    for v in (0, 5):
+        err = np.linalg.norm(outs[2][v] - phi[v]) / np.linalg.norm(phi[v])
+        assert err < 2e-6, (v, err)
