@@ -1014,8 +1014,12 @@ struct Evaluator final : EvaluatorBase {
 
     void p2m_rows(int64_t r0, int64_t r1) {  // P2M of leaves [r0, r1)
         if (r1 <= r0) return;
-        if (kBfly)
-            expand_bfly_kernel<P, false><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
+        if (kBfly && m == 1)
+            expand_bfly_kernel<P, false, false><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
+                dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
+        else if (kBfly)
+            expand_bfly_kernel<P, false, true><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
                 dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), m,
                 reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
         else
@@ -1095,8 +1099,12 @@ struct Evaluator final : EvaluatorBase {
     void p2l_level(int l) {  // the boxes of level l with an X list
         const int64_t b0 = xbox_start[l], b1 = xbox_start[l + 1];
         if (b1 <= b0) return;
-        if (kBfly)
-            expand_bfly_kernel<P, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+        if (kBfly && m == 1)
+            expand_bfly_kernel<P, true, false><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+                dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
+        else if (kBfly)
+            expand_bfly_kernel<P, true, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
                 reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
         else

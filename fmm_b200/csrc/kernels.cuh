@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
 // NCP/32 finished slots (NCP = slots padded to a multiple of 32).  The summation order
 // is fixed (per-lane partial sums, then a fixed tree), so results are repeatable.
 // ---------------------------------------------------------------------------------
-template <int P, bool IRREG>
+template <int P, bool IRREG, bool MULTI>
 __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
                                                          const int32_t* __restrict__ rows,
                                                          const float4* __restrict__ spos, int m,
@@ -219,8 +219,9 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
         nent = (int)(plan.x_row[row + 1] - ent0);
         if (nent == 0) return;
     }
-    // the charge vectors one after the other (charges [v][point], expansions [box][v])
-    for (int v = 0; v < m; ++v) {
+    // the charge vectors one after the other (charges [v][point], expansions [box][v]);
+    // MULTI = false compiles the one-vector form (m = 1) without the loop's registers
+    for (int v = 0; v < (MULTI ? m : 1); ++v) {
     const float* qv = sq + (int64_t)v * plan.nsrc;
     float w[NCP];
 #pragma unroll

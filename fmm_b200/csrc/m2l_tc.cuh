@@ -174,7 +174,7 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 // with the gathered multipoles X as the shared-memory B operand (N = NT pairs,
 // K-major, 128-byte swizzled).  Roles, coupled only by mbarriers (no block barrier in
 // the loop):
-//   warp 17 (gather): for tile k, once the raw stage k % 2 is free, the lanes fetch the
+//   warp 17 (gather): for tile k, once the raw stage k % RS is free, the lanes fetch the
 //     tile's multipole rows with the copy engine into the raw stage, completion counted
 //     on raw_full: with fewer than four vectors each lane fetches four rows with one
 //     tile::gather4 (box one row of KP f32, the slots beyond (p+1)^2 filled with zeros);
@@ -210,15 +210,22 @@ struct TcTs {
     static constexpr int KA = (NC + 31) / 32;
     static constexpr int KP = 32 * KA;             // padded K (input slots)
     static constexpr int KSTEPS = KP / 8;
-    static constexpr int NT = KP > 64 ? 96 : 128;  // pairs per tile (UMMA N): shared memory bounds it at p = 8
+    // columns per tile (UMMA N): 96 at p = 8, where shared memory then holds two raw
+    // stages (measured faster than 64 columns with four)
+    static constexpr int NT = KP > 64 ? 96 : 128;
     static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage (also one raw stage)
-    static constexpr int SMEM = 6 * X_BYTES + 1024;  // X [2 stages][hi, lo], raw [2 stages]
+    // raw stages: as many as shared memory holds beside the two X stages, at most 4 (the
+    // copy engine's loads take several tiles' time to land)
+    static constexpr int RS_FIT = (227 * 1024 - 256 - 1024 - 4 * X_BYTES) / X_BYTES;
+    static constexpr int RS = RS_FIT < 4 ? RS_FIT : 4;
+    static constexpr int SMEM = (4 + RS) * X_BYTES + 1024;  // X [2 stages][hi, lo], raw [RS stages]
     static constexpr int COL_AHI = 0, COL_ALO = KP, COL_D0 = 2 * KP;  // TMEM columns
     static constexpr int TMEM_COLS = 512;
     static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per offset (hi, lo)
     static_assert(NC <= 128, "UMMA M = 128 output slots");
     static_assert(2 * KP + 2 * NT <= TMEM_COLS, "TMEM budget");
     static_assert(NT % 32 == 0 && NT / 4 <= 32, "gather rows: four per lane");
+    static_assert(RS >= 2, "raw stages");
     static_assert(SMEM + 256 <= 227 * 1024, "shared memory");
 };
 
@@ -291,9 +298,10 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     constexpr int NT = S::NT, KP = S::KP;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 stages][hi, lo]
-    unsigned char* rbuf = xbuf + 4 * S::X_BYTES;                                      // raw [2 stages][NT][KP]
+    unsigned char* rbuf = xbuf + 4 * S::X_BYTES;                                      // raw [RS stages][NT][KP]
+    constexpr int RS = S::RS;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    __shared__ uint64_t bar_full[2], bar_empty[2], bar_accf[2], bar_acce[2], bar_table, bar_rfull[2], bar_rempty[2];
+    __shared__ uint64_t bar_full[2], bar_empty[2], bar_accf[2], bar_acce[2], bar_table, bar_rfull[RS], bar_rempty[RS];
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
     const int64_t i0 = (int64_t)blockIdx.x * ntiles / gridDim.x;
@@ -312,6 +320,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             mbar_init(smem_u32(&bar_empty[b]), 1);
             mbar_init(smem_u32(&bar_accf[b]), 1);
             mbar_init(smem_u32(&bar_acce[b]), 8);
+        }
+        for (int b = 0; b < RS; ++b) {
             mbar_init(smem_u32(&bar_rfull[b]), 1);
             mbar_init(smem_u32(&bar_rempty[b]), kTcProd);
         }
@@ -349,13 +359,19 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         int64_t issued = 0;
         for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
             const int64_t it = i0 + k;
-            const int rs = (int)(k & 1);
+            const int rs = (int)(k % RS);
             const int64_t p0 = tile_begin[it];
             const int ncol = tile_count[it] * m;
             // rows past the tile's columns fetch row 0 (their products are never stored)
             int r[4];
             if (blocks) {
                 r[0] = (lane < ppt && lane * m < ncol) ? pair_src[p0 + lane] * m : 0;
+            } else if (m == 1) {  // the common case without the divisions
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c = 4 * lane + j;
+                    r[j] = (c < ncol) ? pair_src[p0 + c] : 0;
+                }
             } else {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -363,7 +379,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                     r[j] = (c < ncol) ? pair_src[p0 + c / m] * m + c % m : 0;
                 }
             }
-            if (k >= 2 && !warp_wait(&bar_rempty[rs], (uint32_t)(((k - 2) >> 1) & 1))) {
+            if (k >= RS && !warp_wait(&bar_rempty[rs], (uint32_t)(((k - RS) / RS) & 1))) {
                 if (lane == 0) give_up();
                 break;
             }
@@ -381,8 +397,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         }
         // on a give-up, the gathers still in flight land before the shared memory is released
         if (lane == 0 && *abort)
-            for (int64_t k = issued > 2 ? issued - 2 : 0; k < issued; ++k)
-                mbar_wait_bounded(smem_u32(&bar_rfull[k & 1]), (uint32_t)((k >> 1) & 1), kTcWait);
+            for (int64_t k = issued > RS ? issued - RS : 0; k < issued; ++k)
+                mbar_wait_bounded(smem_u32(&bar_rfull[k % RS]), (uint32_t)((k / RS) & 1), kTcWait);
         __syncwarp();
     } else if (warp >= kTcProd && warp < kTcProd + kTcProd) {
         // ---------------- converters ----------------
@@ -394,9 +410,10 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             const int st = (int)(k & 1);
             unsigned char* xh = xbuf + (size_t)st * 2 * S::X_BYTES;
             unsigned char* xl = xh + S::X_BYTES;
-            const float4* raw = reinterpret_cast<const float4*>(rbuf + (size_t)st * S::X_BYTES);
+            const int rs = (int)(k % RS);
+            const float4* raw = reinterpret_cast<const float4*>(rbuf + (size_t)rs * S::X_BYTES);
             // the raw rows of tile k are in; the stage is written only once MMA(k-2) has read it
-            if (!warp_wait(&bar_rfull[st], (uint32_t)((k >> 1) & 1)) ||
+            if (!warp_wait(&bar_rfull[rs], (uint32_t)((k / RS) & 1)) ||
                 (k >= 2 && !warp_wait(&bar_empty[st], (uint32_t)(((k - 2) >> 1) & 1)))) {
                 if (lane == 0) give_up();
                 break;
@@ -423,7 +440,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(smem_u32(&bar_full[st]));
-                mbar_arrive(smem_u32(&bar_rempty[st]));
+                mbar_arrive(smem_u32(&bar_rempty[rs]));
             }
             // the table of tile k (warps 8-11, one per lane quarter), once MMA(k-1) is done
             const uint32_t* img = timg + (size_t)tile_d[it] * S::IMG_WORDS;

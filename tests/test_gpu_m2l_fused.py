@@ -82,9 +82,13 @@ def test_fused_vectors_beyond_one_tile(oracle):
     fmm.close()
 
 
-def test_fused_refuses_too_many_vectors(oracle):
-    """At p = 8 a pass holds up to a tensor-core tile's 96 columns, the fused M2L 64."""
+def test_pass_holds_at_most_a_tile_of_vectors(oracle):
+    """A pass holds at most a tensor-core tile's columns of vectors (96 at p = 8), and the
+    fused M2L (tiles of 64 columns there) refuses a pass wider than its tile."""
     x, q = oracle.point_sets("cube", 3000, 14)
+    fmm = F.FmmBuilder(8).vectors(100).max_points_per_leaf(32).precision("mixed").build(x)
+    assert fmm.info()["vectors_per_pass"] == 50
+    fmm.close()
     fmm = F.FmmBuilder(8).vectors(96).max_points_per_leaf(32).precision("mixed").build(x)
     assert fmm.info()["vectors_per_pass"] == 96
     with pytest.raises(F.FmmError, match="at most 64"):
