@@ -194,6 +194,29 @@ def peaks():
         return {}
 
 
+def passes_hbm(info, kinds, pk):
+    """P2M, M2M, L2L and L2P+M2P as HBM passes: algorithmic bytes of one evaluation
+    (f32 points, charges and expansions of n = (p+1)^2 coefficients, f64 target partials)
+    over the kind's CUDA-event time, against the measured copy bandwidth."""
+    s, nc, m, o = 4, (P + 1) ** 2, 1, 4  # bytes a float, coefficients, vectors, outputs a target
+    nb, nl, ns, nt = info["nboxes"], info["nleaves"], info["nsources"], info["ntargets"]
+    bytes_ = {
+        "p2m": ns * (3 + m) * s + nl * m * nc * s,                 # points and charges in, leaf multipoles out
+        "m2m": 2 * nb * m * nc * s,                                # a box's multipole in (child) and out (parent)
+        "l2l": 2 * nb * m * nc * s,                                # a box's local in (parent) and out (child)
+        "l2p_m2p": nt * 3 * s + nt * o * m * 8 + (nl + info["w_pairs"]) * m * nc * s,  # targets, partials, L and W
+    }
+    peak = float(pk.get("hbm_gbs", 6650.0))
+    out = {"peak_gbs": peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
+           "note": "algorithmic bytes per evaluation / the kind's CUDA-event ms; at p = 8 these passes are "
+                   "FP32-bound (harmonic recurrences), not HBM-bound"}
+    for k, b in bytes_.items():
+        gbs = b / (kinds[k] * 1e-3) / 1e9 if kinds.get(k) else None
+        out[k] = {"bytes": int(b), "gbs": round(gbs, 1) if gbs else None,
+                  "frac": round(gbs / peak, 4) if gbs else None}
+    return out
+
+
 def log(msg):
     print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
@@ -389,6 +412,7 @@ def run_ours(args):
                             "value": round(world * n / (direct_ms * 1e-3) / 1e6, 3),
                             "note": "the same evaluation with every kernel launched from the host (no graph)"},
         "kinds_ms": {k: round(v, 4) for k, v in kinds.items()},
+        "passes_hbm": passes_hbm(info, kinds, pk),
         "plan": {k: info[k] for k in ("nlevels", "nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs",
                                       "x_pairs", "device_bytes", "close_pairs")},
         "build_s": round(build_s, 3),
