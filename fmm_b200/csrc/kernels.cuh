@@ -321,7 +321,7 @@ __global__ void m2m_reduce_kernel(DevPlan plan, const int32_t* __restrict__ pare
 //   L = (l >= 3 ? T_o L_parent : 0) + the V row's products in offset-index order
 // (the product of V entry e sits at row vpos[e] of Yv, its place in the M2L tile list),
 // written once (fmm-plan/src/operator.rs:34-45: L2L, then V by offset; X is added after).
-// Block per box, thread per slot; the V loop issues four loads before adding them in order.
+// Block per box, thread per slot; the V loop issues eight (then four) loads before adding them in order.
 // The evaluation writes L = Yo + sum_V Y (accumulate = 0); the level calls add into L:
 // L2L with with_v = 0, then M2L with with_l2l = 0, which gives the same floats when the
 // L2L call comes first (L starts at zero, so 0 + Yo = Yo).
@@ -338,6 +338,13 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
             T s = accumulate ? Lc[(b * m + v) * ms_of(P) + i] : T(0);
             if (with_l2l) s = accumulate ? s + Yo[(b * m + v) * YS + i] : Yo[(b * m + v) * YS + i];
             int64_t e = e0;
+            for (; e + 8 <= e1; e += 8) {  // eight rows in flight, added in row order
+                T y[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) y[j] = __ldcs(Yv + (vpos[e + j] * m + v) * YS + i);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) s += y[j];
+            }
             for (; e + 4 <= e1; e += 4) {
                 const T y0 = __ldcs(Yv + (vpos[e] * m + v) * YS + i), y1 = __ldcs(Yv + (vpos[e + 1] * m + v) * YS + i);
                 const T y2 = __ldcs(Yv + (vpos[e + 2] * m + v) * YS + i), y3 = __ldcs(Yv + (vpos[e + 3] * m + v) * YS + i);
