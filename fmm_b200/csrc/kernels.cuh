@@ -387,16 +387,37 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
     const int64_t p0 = tile_begin[tile];
     const int cnt = tile_count[tile];
     const T* A = tab + (int64_t)d * NC * NC;
-    for (int t = threadIdx.x; t < NC * NCP; t += blockDim.x) {
-        int k = t / NCP, n = t % NCP;
-        At[t] = n < NC ? A[(int64_t)k * NC + n] : T(0);
+    // staging: eight loads a thread in flight before their shared-memory stores (a store
+    // waits for its load, so one at a time would serialise the latencies); 256 threads
+    constexpr int SA = NC * NCP, SX = NC * kGemmPairs;
+#pragma unroll 1
+    for (int t0 = threadIdx.x; t0 < SA; t0 += 8 * 256) {
+        T r[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int t = t0 + 256 * u, k = t / NCP, n = t % NCP;
+            r[u] = (t < SA && n < NC) ? A[(int64_t)k * NC + n] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (t0 + 256 * u < SA) At[t0 + 256 * u] = r[u];
     }
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int v = 0; v < m; ++v) {
         __syncthreads();
-        for (int t = threadIdx.x; t < NC * kGemmPairs; t += blockDim.x) {
-            int pr = t / NC, k = t % NC;
-            Xs[k * kGemmPairs + pr] = pr < cnt ? M[((int64_t)pair_src[p0 + pr] * m + v) * ms_of(P) + k] : T(0);
+#pragma unroll 1
+        for (int t0 = threadIdx.x; t0 < SX; t0 += 8 * 256) {
+            T r[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + 256 * u, pr = t / NC, k = t % NC;
+                r[u] = (t < SX && pr < cnt) ? M[((int64_t)pair_src[p0 + pr] * m + v) * ms_of(P) + k] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + 256 * u;
+                if (t < SX) Xs[(t % NC) * kGemmPairs + t / NC] = r[u];
+            }
         }
         __syncthreads();
         T acc[4][JN];
