@@ -430,6 +430,11 @@ def run_ours(args):
     line["gpu_launches_per_step"] = launches_per_step
     if batched is not None:
         line["batched"] = batched
+    if not args.no_batched and world == 1:
+        try:
+            line["helmholtz_near"] = run_helmholtz(F)
+        except Exception as e:  # reported, never fatal to the headline line
+            line["helmholtz_near"] = {"error": f"{type(e).__name__}: {str(e)[:200]}"}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
@@ -528,6 +533,37 @@ def run_batched(F, torch, dev, flush, rank=0, world=1, steps=3, warmup=1):
     res["mixed_over_plain"] = round(res["plain_f64"]["ms_per_step"] / res["ms_per_step"], 3)
     del dq, dphi
     torch.cuda.empty_cache()
+    return res
+
+
+def run_helmholtz(F, n=1_000_000, k=20.0, leaf=96, reps=3):
+    """The Helmholtz near field (P2P of every leaf, e^{ikr}/(4 pi r), potential and gradient)
+    on the Helmholtz configuration's points: n uniform in the unit cube, complex charges
+    N(0,1) + i N(0,1), k = 20, 96 per leaf; f64 and mixed through the host API (charges in,
+    phi and grad out: the copies are inside the timed calls), best of `reps` after a warm
+    call, with the mixed form's relative L2 error against the f64 near field."""
+    rng = np.random.default_rng(SEED + 11)
+    x = rng.uniform(0.0, 1.0, (n, 3))
+    q = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    res = {"workload": f"Helmholtz near field (P2P), N={n} uniform in the unit cube, k={k}, {leaf} per leaf, "
+                       "phi+grad, complex charges", "data": "synthetic (numpy PCG64, seeded)",
+           "timing": "wall clock of the host call fmmgpu_helmholtz_near, copies included"}
+    outs = {}
+    for precision in ("f64", "mixed"):
+        f = F.FmmBuilder(6).gradients().max_points_per_leaf(leaf).precision(precision).build(x)
+        pairs = f.info()["near_pairs"]
+        outs[precision] = f.helmholtz_near(k, q)
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            f.helmholtz_near(k, q)
+            best = min(best, time.perf_counter() - t0)
+        res[precision] = {"ms": round(best * 1e3, 3), "near_pairs": int(pairs),
+                          "gpairs_per_s": round(pairs / best / 1e9, 3), "mpoints_per_s": round(n / best / 1e6, 3)}
+        f.close()
+    a, b = outs["mixed"], outs["f64"]
+    res["mixed_rel_l2"] = {"phi": float(np.linalg.norm(a.potential - b.potential) / np.linalg.norm(b.potential)),
+                           "grad": float(np.linalg.norm(a.gradient - b.gradient) / np.linalg.norm(b.gradient))}
     return res
 
 
