@@ -400,10 +400,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32 (f64 per-target accumulation)",
         "data": "synthetic (seeded SplitMix64: unit-sphere surface from normalised Gaussians, q ~ N(0,1))",
-        "config": {"workload": f"laplace3d sphere N={n} p={P} leaf={LEAF} phi+grad mixed",
-                   "n_points": n, "p": P, "max_points_per_leaf": LEAF, "gradients": True,
-                   "precision": "mixed", "l2": "flushed (512 MiB write) before every timed step",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "config": headline_config(n, world),
         "error": {"phi_rel_l2": err_phi, "grad_rel_l2": err_g, "sampled_targets": SAMPLE,
                   "against": "f64 direct sum (GPU, Neumaier)", "plain_f64_phi_rel_l2": perr},
         "plain_f64": {"ms_per_step": round(plain_ms, 4), "value": round(n / (plain_ms * 1e-3) / 1e6, 3),
@@ -584,6 +581,14 @@ def cpu_baseline(args, n_sample=None):
                       f"({s:.1f} s)"}
 
 
+def headline_config(n, world):
+    """The workload both arms report (the reference arm times bounded samples of it)."""
+    return {"workload": f"laplace3d sphere N={n} p={P} leaf={LEAF} phi+grad mixed",
+            "n_points": n, "p": P, "max_points_per_leaf": LEAF, "gradients": True,
+            "precision": "mixed", "l2": "flushed (512 MiB write) before every timed step",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
+
+
 def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -602,7 +607,7 @@ def run_reference(args):
         "value": v, "unit": "Mpoints/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded SplitMix64 sphere)",
-        "config": {"workload": f"laplace3d sphere p={P} leaf={LEAF} phi+grad, bounded sample N={args.ref_n}"},
+        "config": headline_config(args.n, world),
         "cpu_baseline": b,
         "e2e": {"value": v, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
