@@ -68,6 +68,35 @@ __device__ __forceinline__ void helm_pair(T kre, T kim, T dx, T dy, T dz, T r2, 
     }
 }
 
+// The same term in f32 (the mixed form's far-from-singular pairs): 1/r and 1/r^3 from one
+// rsqrt instead of divisions, and the decay exp(-Im(k) r) not formed for a real wavenumber
+// (it is exactly 1 there)
+template <bool GRAD>
+__device__ __forceinline__ void helm_pair_f32(float kre, float kim, float dx, float dy, float dz, float r2,
+                                              Cplx<float> q, Cplx<float>& phi, Cplx<float> (&g3)[3]) {
+    const float rinv = rsqrtf(r2);
+    const float r = r2 * rinv;
+    const float damping = -(kim * r), phase = kre * r;
+    float s, c;
+    sincosf(phase, &s, &c);
+    const float decay = kim == 0.0f ? 1.0f : expf(damping);
+    const Cplx<float> e{decay * c, decay * s};
+    const Cplx<float> qe = cmul(q, e);
+    phi.re += qe.re * rinv;
+    phi.im += qe.im * rinv;
+    if (GRAD) {
+        const float rinv3 = rinv * rinv * rinv;
+        const Cplx<float> fe = cmul(Cplx<float>{damping - 1.0f, phase}, e);
+        const Cplx<float> qg = cmul(q, Cplx<float>{fe.re * rinv3, fe.im * rinv3});
+        g3[0].re += qg.re * dx;
+        g3[0].im += qg.im * dx;
+        g3[1].re += qg.re * dy;
+        g3[1].im += qg.im * dy;
+        g3[2].re += qg.re * dz;
+        g3[2].im += qg.im * dz;
+    }
+}
+
 // Charges of the Helmholtz calls: caller order, m complex charges per point adjacent
 // ((re, im) doubles) -> leaf order [v][point] in T, and in f64 for the near-singular pairs.
 template <typename T>
@@ -149,7 +178,12 @@ __global__ void __launch_bounds__(32 * kHelmWarps) helm_p2p_kernel(
                     const T dx = sub_rn<T>(tx, y.x), dy = sub_rn<T>(ty, y.y), dz = sub_rn<T>(tz, y.z);
                     const T r2 = pair_r2<T>(dx, dy, dz);
                     const bool skip = CLOSE ? (r2 < theta2) : (r2 == T(0));
-                    if (!skip) helm_pair<T, GRAD>(kre, kim, dx, dy, dz, r2, qstage[warp][s], pphi, pg);
+                    if (!skip) {
+                        if constexpr (sizeof(T) == 4)
+                            helm_pair_f32<GRAD>(kre, kim, dx, dy, dz, r2, qstage[warp][s], pphi, pg);
+                        else
+                            helm_pair<T, GRAD>(kre, kim, dx, dy, dz, r2, qstage[warp][s], pphi, pg);
+                    }
                 }
                 aphi[0] += (double)pphi.re;
                 aphi[1] += (double)pphi.im;
