@@ -368,6 +368,18 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
 // ---------------------------------------------------------------------------------
 constexpr int kGemmPairs = 64;
 
+// one element global -> shared by an asynchronous copy; zero-filled when !valid (the source
+// address is then not read)
+template <typename T>
+__device__ __forceinline__ void gemm_cp_async(T* smem, const T* gmem, bool valid) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t n = valid ? (uint32_t)sizeof(T) : 0u;
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
+
 template <int P, typename T>
 __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict__ tile_d,
                                                        const int64_t* __restrict__ tile_begin,
@@ -387,38 +399,24 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
     const int64_t p0 = tile_begin[tile];
     const int cnt = tile_count[tile];
     const T* A = tab + (int64_t)d * NC * NC;
-    // staging: eight loads a thread in flight before their shared-memory stores (a store
-    // waits for its load, so one at a time would serialise the latencies); 256 threads
+    // staging by asynchronous copies (every copy of the block in flight at once; padding
+    // zero-filled): the table, then each vector's source rows once the tile's sources are
+    // known; 256 threads
     constexpr int SA = NC * NCP, SX = NC * kGemmPairs;
-#pragma unroll 1
-    for (int t0 = threadIdx.x; t0 < SA; t0 += 8 * 256) {
-        T r[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int t = t0 + 256 * u, k = t / NCP, n = t % NCP;
-            r[u] = (t < SA && n < NC) ? A[(int64_t)k * NC + n] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-            if (t0 + 256 * u < SA) At[t0 + 256 * u] = r[u];
+    __shared__ int32_t srcs[kGemmPairs];
+    if (threadIdx.x < kGemmPairs) srcs[threadIdx.x] = threadIdx.x < cnt ? pair_src[p0 + threadIdx.x] : 0;
+    for (int t = threadIdx.x; t < SA; t += 256) {
+        const int k = t / NCP, n = t % NCP;
+        gemm_cp_async<T>(At + t, A + (int64_t)k * NC + (n < NC ? n : 0), n < NC);
     }
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int v = 0; v < m; ++v) {
-        __syncthreads();
-#pragma unroll 1
-        for (int t0 = threadIdx.x; t0 < SX; t0 += 8 * 256) {
-            T r[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int t = t0 + 256 * u, pr = t / NC, k = t % NC;
-                r[u] = (t < SX && pr < cnt) ? M[((int64_t)pair_src[p0 + pr] * m + v) * ms_of(P) + k] : T(0);
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int t = t0 + 256 * u;
-                if (t < SX) Xs[(t % NC) * kGemmPairs + t / NC] = r[u];
-            }
+        __syncthreads();  // srcs written; the previous vector's Xs read
+        for (int t = threadIdx.x; t < SX; t += 256) {
+            const int pr = t / NC, k = t % NC;
+            gemm_cp_async<T>(Xs + k * kGemmPairs + pr, M + ((int64_t)srcs[pr] * m + v) * ms_of(P) + k, pr < cnt);
         }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
         __syncthreads();
         T acc[4][JN];
 #pragma unroll
