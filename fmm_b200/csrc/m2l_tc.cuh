@@ -1,18 +1,18 @@
 // Dense M2L on the tensor cores (mixed form): tcgen05.mma kind::tf32 with a 3-term
 // split, accumulators in tensor memory.
 //
-// One CTA (4 warps) takes a tile of up to 128 V pairs of one offset d (the batches of
-// m2l_gemm_kernel, 128 pairs wide) and forms D = X * A_d^T, X the 128 gathered source
-// multipoles (M = 128 rows, K = the (p+1)^2 input slots padded to KP = 32 * KA),
-// A_d^T the table (N = the output slots padded to NP).  f32 data is split as
-// x = hi + lo with hi = tf32(x), lo = tf32(x - hi), and
-//   D = X_lo A_hi^T + X_hi A_lo^T + X_hi A_hi^T
-// (the lo*lo term, 2^-22 relative, is dropped), each product an exact tf32 product
-// summed in f32 in TMEM.  Operands are K-major in 128-byte-swizzled shared memory:
-// 8-row x 128 B atoms, 16 B chunk c of row r stored at chunk c ^ (r % 8); a K-step of 8
-// tf32 (32 B) advances the descriptor start address by 32 B inside an atom, and atoms
-// of 32 K-elements follow each other.  The table images (hi and lo) are precomputed on
-// the host in exactly this layout, so the CTA copies them verbatim.
+// The V pairs of every level are grouped by offset d (the batches of m2l_gemm_kernel)
+// and cut into tiles; for a tile the MMA forms D[slot][column] = A_d[slot][k] X[column][k],
+// the table A_d (M = 128 output slots) in tensor memory and X the tile's gathered source
+// multipoles (N = the tile's columns, K = the (p+1)^2 input slots padded to KP = 32 * KA)
+// in shared memory.  f32 data is split as x = hi + lo with hi = tf32(x),
+// lo = tf32(x - hi), and D = A_hi X_lo + A_lo X_hi + A_hi X_hi (the lo*lo term, 2^-22
+// relative, is dropped), each product an exact tf32 product summed in f32 in tensor
+// memory.  The X operand is K-major in 128-byte-swizzled shared memory: 8-row x 128 B
+// atoms, 16 B chunk c of row r stored at chunk c ^ (r % 8); a K-step of 8 tf32 (32 B)
+// advances the descriptor start address by 32 B inside an atom, and atoms of 32
+// K-elements follow each other.  The table images (hi and lo) are precomputed on the host.
+// The persistent, warp-specialised kernel is described above m2l_tc_kernel.
 //
 // Descriptor fields follow cute/arch/mma_sm100_desc.hpp (CUTLASS 4.5): SmemDescriptor
 // (start>>4 [0,14), LBO>>4 [16,30), SBO>>4 [32,46), version 1 [46,48), layout [61,64),
@@ -35,22 +35,6 @@
 #include "harmonics.cuh"
 
 namespace fmmb {
-
-constexpr int kTcRows = 128;  // pairs per tile (UMMA M)
-
-template <int P>
-struct TcShape {
-    static constexpr int NC = nc_of(P);
-    static constexpr int KA = (NC + 31) / 32;                   // K atoms of 32 tf32
-    static constexpr int KP = 32 * KA;                          // padded K
-    static constexpr int NP = ((NC + 15) / 16) * 16;            // padded N (M = 128 needs N % 16 == 0)
-    static constexpr int KSTEPS = KP / 8;
-    static constexpr int A_BYTES = kTcRows * KP * 4;            // one part (hi or lo)
-    static constexpr int B_BYTES = NP * KP * 4;
-    static constexpr int TMEM_COLS = NP <= 32 ? 32 : NP <= 64 ? 64 : NP <= 128 ? 128 : 256;
-    static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 1024 + 64;
-    static_assert(NP <= 256, "UMMA N must not exceed 256");
-};
 
 // byte offset of element (row r, column k) in a K-major SW128 operand of `rows` rows
 __host__ __device__ __forceinline__ uint32_t sw128_offset(int r, int k, int rows) {
@@ -78,37 +62,10 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
-template <int NP>
-__host__ __device__ constexpr uint32_t tf32_idesc() {
-    return (1u << 4)                 // D f32
-           | (2u << 7) | (2u << 10)  // A, B tf32
-           | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
-}
-
 __device__ __forceinline__ uint32_t cvt_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return r;
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-    asm volatile(
-        "{\n\t"
-        ".reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
-        "}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-// the load alone: the caller waits (tcgen05.wait::ld) before reading v
-__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, float (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]), "=f"(v[8]),
-          "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
-        : "r"(taddr));
 }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
