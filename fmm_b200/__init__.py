@@ -43,7 +43,7 @@ class Info(C.Structure):
                 ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
                 ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64),
                 ("vectors_per_pass", C.c_int64), ("p2p_warps", C.c_int64), ("leaf_block", C.c_int64),
-                ("product_chunks", C.c_int64)]
+                ("product_chunks", C.c_int64), ("p2p_stream_bytes", C.c_int64)]
 
 
 def lib():
@@ -76,6 +76,7 @@ def lib():
             "fmmgpu_fmm_set_graph": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_overlap": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_set_m2l_path": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_set_p2p_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_autotune": (C.c_int, [vp, dp, dp]),
             "fmmgpu_fmm_set_launch_shapes": (C.c_int, [vp, C.c_int, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
@@ -397,6 +398,11 @@ class Fmm(Plan):
         """M2L path (mixed, p <= 8): 1 tensor-core products then the reduce (the default),
         2 tensor-core M2L fused with the reduce (the same bits), 0 SIMT products."""
         _check(lib().fmmgpu_fmm_set_m2l_path(self._h, int(path)))
+
+    def set_p2p_path(self, path):
+        """Mixed P2P sources (test hook): 1 the near rows' streams mapped at build time (the
+        default when built), 0 mapped per flush; the same bits."""
+        _check(lib().fmmgpu_fmm_set_p2p_path(self._h, int(path)))
 
     def kind_times(self):
         """Milliseconds per kind of the last evaluation (after set_kind_timing(True))."""

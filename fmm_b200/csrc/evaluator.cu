@@ -144,6 +144,10 @@ struct EvaluatorBase {
     // (1, 2 or 4) and threads a block of the L2P / M2P kernel (32, 64 or 128)
     int p2p_warps = kX2Warps;
     int leaf_block = 64;
+    // mixed P2P: 1 the sources from the near rows' streams mapped at build time (the
+    // default when the streams fit), 0 mapped per flush; the same floats
+    int p2p_path = 0;
+    int64_t p2p_stream_bytes = 0;
     unsigned counted(unsigned grid) {  // wraps the grid of every evaluation launch
         ++launches;
         return grid;
@@ -156,6 +160,7 @@ struct EvaluatorBase {
     virtual void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
     virtual void autotune(const double* d_charges, double* d_phi, double* d_grad) = 0;
     virtual void set_m2l_path(int path) = 0;
+    virtual void set_p2p_path(int path) = 0;
     virtual int64_t product_chunks() const = 0;
 };
 
@@ -218,6 +223,8 @@ struct Evaluator final : EvaluatorBase {
     // P2P work items (32 targets of one leaf each) and, for the mixed form, the
     // near-singular pairs evaluated in f64
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
+    // the near rows' source streams in the target leaves' frames (mixed form, P2pStream)
+    DevBuf st_rowpair, st_xy, st_zz, st_idx;
     // boxes with a nonempty X list, level by level (the P2L launches)
     DevBuf xbox;
     std::vector<int64_t> xbox_start;
@@ -357,6 +364,7 @@ struct Evaluator final : EvaluatorBase {
                                                                                    near_rec.as<NearRec>());
             CUDA_TRY(cudaGetLastError());
             CUDA_TRY(cudaDeviceSynchronize());
+            build_p2p_stream();
         }
         close_pairs = nclose;
         gemm_smem = sizeof(T) * ((size_t)NC * (NC <= 96 ? 96 : ((NC + 15) / 16) * 16) + (size_t)NC * kGemmPairs);
@@ -726,6 +734,45 @@ struct Evaluator final : EvaluatorBase {
         Yo.alloc(sizeof(T) * (size_t)m * ys_of(P) * plan.nboxes());
     }
 
+    // The near rows' source streams (P2pStream), built when they take at most a quarter of
+    // the free device memory; otherwise the P2P maps its sources per flush (the same floats).
+    void build_p2p_stream() {
+        const size_t nl = plan.nleaves();
+        std::vector<int64_t> rp(nl + 1, 0);
+        for (size_t j = 0; j < nl; ++j) {
+            int64_t S = 0;
+            for (int64_t e = plan.near.row[j]; e < plan.near.row[j + 1]; ++e) {
+                const int sl = plan.near.col[e];
+                S += plan.src_start[sl + 1] - plan.src_start[sl];
+            }
+            rp[j + 1] = rp[j] + (S + 1) / 2;
+        }
+        const size_t pairs = (size_t)rp[nl];
+        const size_t bytes = pairs * (sizeof(float4) + sizeof(float2) + sizeof(int2)) + 8 * (nl + 1);
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        if (dp.nsrc >= ((int64_t)1 << 31) || bytes > free_b / 4) return;
+        st_rowpair.upload(rp);
+        st_xy.alloc(sizeof(float4) * (pairs + 1));
+        st_zz.alloc(sizeof(float2) * (pairs + 1));
+        st_idx.alloc(sizeof(int2) * (pairs + 1));
+        if (nl)
+            near_stream_kernel<<<(unsigned)((nl + 3) / 4), 128>>>(dp, (int64_t)nl, near_rec.as<NearRec>(),
+                                                                  reinterpret_cast<const float4*>(spos.ptr),
+                                                                  st_rowpair.as<int64_t>(), st_xy.as<float4>(),
+                                                                  st_zz.as<float2>(), st_idx.as<int2>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaDeviceSynchronize());
+        p2p_stream_bytes = (int64_t)(st_rowpair.bytes + st_xy.bytes + st_zz.bytes + st_idx.bytes);
+        p2p_path = 1;
+    }
+
+    void set_p2p_path(int path) override {
+        if (path < 0 || path > 1 || (path == 1 && !p2p_stream_bytes))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "P2P path " + std::to_string(path) + " not available");
+        p2p_path = path;
+    }
+
     void build_p2p_items() {
         std::vector<int32_t> il;
         std::vector<int64_t> it;
@@ -833,7 +880,8 @@ struct Evaluator final : EvaluatorBase {
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
                                &near_phi, &near_g, &box_side, &v_pos, &xbox, &fu_tile_d, &fu_tile_begin,
                                &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
-                               &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src};
+                               &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src, &st_rowpair,
+                               &st_xy, &st_zz, &st_idx};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -1138,6 +1186,16 @@ struct Evaluator final : EvaluatorBase {
         const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
         const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
         const auto* q = reinterpret_cast<const float*>(sq.ptr);
+        if (p2p_path == 1) {
+            const P2pStream st{st_rowpair.as<int64_t>(), st_xy.as<float4>(), st_zz.as<float2>(), st_idx.as<int2>()};
+            if (!gradients)
+                p2p_st_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, st, q, tp, close,
+                                                                 far_phi.as<double>(), accumulate, d_phi);
+            else
+                p2p_st_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, st, q, tp, close,
+                                                                   far_phi.as<double>(), fg, accumulate, d_phi, og);
+            return;
+        }
         if (!gradients) {  // potentials: the pair geometry shared by up to kX2Vb vectors (any m)
             p2p_x2_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q,
                                                              tp, close, far_phi.as<double>(), accumulate, d_phi);
@@ -1889,6 +1947,16 @@ int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* f, int path) {
     });
 }
 
+int fmmgpu_fmm_set_p2p_path(fmmgpu_fmm* f, int path) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->eval->set_p2p_path(path);
+        f->drop_graph();
+    });
+}
+
 int fmmgpu_fmm_set_kinds(fmmgpu_fmm* f, int kinds) {
     return guarded([&] {
         if (!f || !f->eval || kinds < 1 || kinds > 3) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid kinds");
@@ -1988,6 +2056,7 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->launches = f->eval ? f->eval->launches : 0;
         info->vectors_per_pass = f->eval ? f->mpass : 0;
         info->p2p_warps = f->eval ? f->eval->p2p_warps : 0;
+        info->p2p_stream_bytes = f->eval ? f->eval->p2p_stream_bytes : 0;
         info->leaf_block = f->eval ? f->eval->leaf_block : 0;
         info->product_chunks = f->eval ? f->eval->product_chunks() : 0;
     });

@@ -790,12 +790,13 @@ __global__ void close_map_kernel(DevPlan plan, ClosePairs close, double4* __rest
         for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
             const int sl = close.leaf[c2];
             const double4 ps = close.spos[close.src[c2]];
+            const double sw = (double)close.src[c2];  // w: the source's index (exact below 2^53)
             if (sl == leaf) {
-                y[c2] = make_double4(ps.x, ps.y, ps.z, 0.0);
+                y[c2] = make_double4(ps.x, ps.y, ps.z, sw);
             } else {
                 double cc[3], rr;
                 rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
-                y[c2] = make_double4(__fma_rn(rr, ps.x, cc[0]), __fma_rn(rr, ps.y, cc[1]), __fma_rn(rr, ps.z, cc[2]), 0.0);
+                y[c2] = make_double4(__fma_rn(rr, ps.x, cc[0]), __fma_rn(rr, ps.y, cc[1]), __fma_rn(rr, ps.z, cc[2]), sw);
             }
         }
 }

@@ -69,6 +69,22 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
                  "l"(gmem)
                  : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+// 4 bytes, or zeros when src_bytes is 0 (the address is then not read)
+__device__ __forceinline__ void cp_async4_zf(void* smem, const void* gmem, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
 
 // Flushes run over (vector, position in the row's source stream); while flush f is
 // computed, the raw points and charges of flush f + 1 are in flight (cp.async), so a
@@ -462,6 +478,423 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
         }
 #pragma unroll
         for (int b = 0; b < VB; ++b) aphi[b] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// The streamed form.  A near row's source stream (its near entries in row order, each
+// source leaf's points in leaf order) is mapped into the target leaf's frame once, at build
+// time, with the same f32 fma as the map step above (y = fma(r, u, c), the frame of the
+// entry's NearRec), and stored in the staged pair layout: per pair of stream positions
+// (2i, 2i + 1) a float4 (x0, x1, y0, y1), a float2 (z0, z1) and the two sources' indices
+// (leaf order; an odd stream ends with a padding source at the origin, index -1, whose
+// charge is zero, as the map step pads an odd flush).  A flush is then plain copies of
+// consecutive pairs plus a gather of the flush's charges by index, double-buffered: the
+// staged floats, the pair-steps and every addition are those of p2p_x2_kernel and
+// p2p_x2_mv_kernel, so the two forms give the same bits.
+
+struct P2pStream {
+    const int64_t* row_pair;  // per leaf (nleaves + 1): the first pair of its row's stream
+    const float4* xy;         // per pair: (x0, x1, y0, y1) in the target leaf's frame
+    const float2* zz;         // per pair: (z0, z1)
+    const int2* idx;          // per pair: the sources' indices in leaf order (-1: padding)
+};
+
+// Build time: warp per leaf row, writing that row's pairs.
+__global__ void near_stream_kernel(DevPlan plan, int64_t nleaves, const NearRec* __restrict__ recs,
+                                   const float4* __restrict__ spos, const int64_t* __restrict__ row_pair,
+                                   float4* __restrict__ xy_out, float2* __restrict__ zz_out,
+                                   int2* __restrict__ idx_out) {
+    const int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (leaf >= nleaves) return;
+    const int64_t pb = row_pair[leaf];
+    float* xy = reinterpret_cast<float*>(xy_out + pb);
+    float* zz = reinterpret_cast<float*>(zz_out + pb);
+    int* ix = reinterpret_cast<int*>(idx_out + pb);
+    int S = 0;
+    for (int64_t e = plan.near_row[leaf]; e < plan.near_row[leaf + 1]; ++e) {
+        const NearRec r = recs[e];
+        for (int k = lane; k < r.ns; k += 32) {
+            const int pos = r.off + k;
+            const float4 u = spos[r.s0 + k];
+            const int slot = (pos >> 1) * 4 + (pos & 1);
+            xy[slot] = __fmaf_rn(r.frame.w, u.x, r.frame.x);
+            xy[slot + 2] = __fmaf_rn(r.frame.w, u.y, r.frame.y);
+            zz[pos] = __fmaf_rn(r.frame.w, u.z, r.frame.z);
+            ix[pos] = (int)(r.s0 + k);
+        }
+        S = r.off + r.ns;
+    }
+    if ((S & 1) && lane == 0) {
+        const int slot = (S >> 1) * 4 + 1;
+        xy[slot] = 0.f;
+        xy[slot + 2] = 0.f;
+        zz[S] = 0.f;
+        ix[S] = -1;
+    }
+}
+
+constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
+
+// The near-singular pairs of target t for vector v, added in f64 in CSR order (the
+// sums of p2p_x2_kernel's loop), their records fetched four at a time; y.w holds the
+// source's index (close_map_kernel).
+template <bool GRAD>
+__device__ __forceinline__ void close_pairs_f64(const ClosePairs& close, int64_t t, const double* __restrict__ qv,
+                                                double& aphi, double& ag0, double& ag1, double& ag2) {
+    const double4 u = close.tpos[t];
+    const int64_t c0 = close.row[t], c1 = close.row[t + 1];
+    constexpr int CB = 2;
+    for (int64_t c = c0; c < c1; c += CB) {
+        double4 y[CB];
+        double qq[CB];
+#pragma unroll
+        for (int j = 0; j < CB; ++j)
+            if (c + j < c1) y[j] = close.y[c + j];
+#pragma unroll
+        for (int j = 0; j < CB; ++j)
+            if (c + j < c1) qq[j] = qv[(int64_t)y[j].w];
+#pragma unroll
+        for (int j = 0; j < CB; ++j) {
+            if (c + j >= c1) break;
+            if (u.x == y[j].x && u.y == y[j].y && u.z == y[j].z) continue;
+            const double dx = u.x - y[j].x, dy = u.y - y[j].y, dz = u.z - y[j].z;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const double rinv = rsqrt(r2);
+            const double qr = qq[j] * rinv;
+            aphi += qr;
+            if (GRAD) {
+                const double qr3 = qr * rinv * rinv;
+                ag0 -= qr3 * dx;
+                ag1 -= qr3 * dy;
+                ag2 -= qr3 * dz;
+            }
+        }
+    }
+}
+
+template <bool GRAD, int W>
+__global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
+    DevPlan plan, P2pItems items, int m, int near, float theta2, P2pStream st, const float* __restrict__ sq,
+    const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, double* __restrict__ far_g,
+    int accumulate, double* __restrict__ out_phi, double* __restrict__ out_g) {
+    __shared__ float4 sxy[W][2][kStPairs];  // (x0, x1, y0, y1), two flushes
+    __shared__ float4 szq[W][2][kStPairs];  // (z0, z1, q0, q1)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * W + warp;
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int box = plan.leaf_box[leaf];
+    const int64_t t1 = plan.tgt_start[leaf + 1];
+    // the lanes of an item of ni < 32 targets split the pair-steps (p2p_x2_kernel)
+    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int K = 32 / ni;
+    const int kk = lane < ni * K ? lane / ni : K;
+    const int ti = lane < ni * K ? lane % ni : 0;
+    const int64_t t = items.t0[item] + ti;
+    const bool valid = lane < ni;
+    const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    if (kk < K) {
+        const float4 p4 = tpos[t];
+        tx = p4.x;
+        ty = p4.y;
+        tz = p4.z;
+    }
+    const float2 ntx = f2(-tx, -tx), nty = f2(-ty, -ty), ntz = f2(-tz, -tz);
+    const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
+    const double phi_scale = 4.0 * 3.141592653589793 * rt;
+    const double g_scale = phi_scale * rt;
+    const int64_t pb = st.row_pair[leaf];
+    const int np_row = near ? (int)(st.row_pair[leaf + 1] - pb) : 0;  // pairs in the row's stream
+    const int nfl = np_row > 0 ? (np_row + kStPairs - 1) / kStPairs : 1;  // flushes per vector
+    const int total = nfl * m;
+    // the issue pointer (vector iv, flush ifl) and the source indices of that flush
+    int iv = 0, ifl = 0;
+    int2 ix0 = make_int2(-1, -1), ix1 = make_int2(-1, -1);
+    auto load_idx = [&]() {
+        const int i0 = ifl * kStPairs + lane, i1 = i0 + 32;
+        ix0 = i0 < np_row ? st.idx[pb + i0] : make_int2(-1, -1);
+        ix1 = i1 < np_row ? st.idx[pb + i1] : make_int2(-1, -1);
+    };
+    auto issue = [&](int b) {
+        const float* qv = sq + (int64_t)iv * nsrc;
+        const int64_t base = pb + (int64_t)ifl * kStPairs;
+        const int npf = np_row - ifl * kStPairs;
+        float* zq = reinterpret_cast<float*>(&szq[warp][b][0]);
+        if (lane < npf) {
+            cp_async16_cg(&sxy[warp][b][lane], st.xy + base + lane);
+            cp_async8(zq + 4 * lane, st.zz + base + lane);
+            cp_async4_zf(zq + 4 * lane + 2, qv + (ix0.x < 0 ? 0 : ix0.x), ix0.x < 0 ? 0 : 4);
+            cp_async4_zf(zq + 4 * lane + 3, qv + (ix0.y < 0 ? 0 : ix0.y), ix0.y < 0 ? 0 : 4);
+        }
+        if (lane + 32 < npf) {
+            cp_async16_cg(&sxy[warp][b][lane + 32], st.xy + base + lane + 32);
+            cp_async8(zq + 4 * (lane + 32), st.zz + base + lane + 32);
+            cp_async4_zf(zq + 4 * (lane + 32) + 2, qv + (ix1.x < 0 ? 0 : ix1.x), ix1.x < 0 ? 0 : 4);
+            cp_async4_zf(zq + 4 * (lane + 32) + 3, qv + (ix1.y < 0 ? 0 : ix1.y), ix1.y < 0 ? 0 : 4);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        if (++ifl == nfl) {
+            ifl = 0;
+            ++iv;
+        }
+        if (iv < m) load_idx();  // lands while the flush being computed runs
+    };
+    load_idx();
+    issue(0);
+    double aphi = 0.0, ag0 = 0.0, ag1 = 0.0, ag2 = 0.0;
+    int cv = 0, cfl = 0;  // the flush being computed
+    for (int f = 0; f < total; ++f) {
+        const int b = f & 1;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+        if (f + 1 < total) issue(b ^ 1);  // buffer b ^ 1 was last read by flush f - 1
+        const int rem = np_row - cfl * kStPairs;
+        const int npairs = rem < kStPairs ? rem : kStPairs;
+        float2 pphi = f2(0.f, 0.f), pg0 = f2(0.f, 0.f), pg1 = f2(0.f, 0.f), pg2 = f2(0.f, 0.f);
+#pragma unroll 4
+        for (int i = kk; i < npairs; i += K) {
+            const float4 a = sxy[warp][b][i];
+            const float4 c = szq[warp][b][i];
+            const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
+            const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
+            const float2 dz = __fadd2_rn(f2(c.x, c.y), ntz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
+            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float2 rinv = f2(ri0, ri1);
+            const float2 qr = __fmul2_rn(f2(c.z, c.w), rinv);
+            pphi = __fadd2_rn(pphi, qr);
+            if (GRAD) {
+                const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, rinv), rinv);
+                pg0 = __ffma2_rn(qr3, dx, pg0);
+                pg1 = __ffma2_rn(qr3, dy, pg1);
+                pg2 = __ffma2_rn(qr3, dz, pg2);
+            }
+        }
+        aphi += (double)pphi.x;
+        aphi += (double)pphi.y;
+        if (GRAD) {
+            ag0 += (double)pg0.x;
+            ag0 += (double)pg0.y;
+            ag1 += (double)pg1.x;
+            ag1 += (double)pg1.y;
+            ag2 += (double)pg2.x;
+            ag2 += (double)pg2.y;
+        }
+        __syncwarp();  // buffer b is read before it is refilled or reused below
+        const int v = cv;
+        const bool last = cfl == nfl - 1;
+        if (++cfl == nfl) {
+            cfl = 0;
+            ++cv;
+        }
+        if (!last) continue;
+        // ---- the last flush of vector v: finish its targets ----
+        if (K > 1) {  // the target's K partial sums, in kk order, through buffer b
+            double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[warp][b][0]);
+            red[0][lane] = aphi;
+            red[1][lane] = ag0;
+            red[2][lane] = ag1;
+            red[3][lane] = ag2;
+            __syncwarp();
+            if (valid)
+                for (int j = 1; j < K; ++j) {
+                    aphi += red[0][ti + ni * j];
+                    ag0 += red[1][ti + ni * j];
+                    ag1 += red[2][ti + ni * j];
+                    ag2 += red[3][ti + ni * j];
+                }
+            __syncwarp();
+        }
+        if (valid) {
+            if (near) close_pairs_f64<GRAD>(close, t, close.q + (int64_t)v * nsrc, aphi, ag0, ag1, ag2);
+            if (accumulate == 2) {
+                out_phi[(int64_t)v * nt + t] = aphi;
+                if (GRAD) {
+                    double* o = out_g + ((int64_t)v * nt + t) * 3;
+                    o[0] = ag0;
+                    o[1] = ag1;
+                    o[2] = ag2;
+                }
+            } else if (accumulate) {
+                far_phi[(int64_t)v * nt + t] = far_phi[(int64_t)v * nt + t] + aphi;
+                if (GRAD) {
+                    double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                    fg[0] = fg[0] + ag0;
+                    fg[1] = fg[1] + ag1;
+                    fg[2] = fg[2] + ag2;
+                }
+            } else {
+                const double ph = far_phi[(int64_t)v * nt + t] + aphi;
+                const int64_t i = plan.tgt_perm[t];
+                out_phi[(int64_t)v * nt + i] = ph / phi_scale;
+                if (GRAD) {
+                    const double* fg = far_g + ((int64_t)v * nt + t) * 3;
+                    double* o = out_g + ((int64_t)v * nt + i) * 3;
+                    o[0] = (fg[0] + ag0) / g_scale;
+                    o[1] = (fg[1] + ag1) / g_scale;
+                    o[2] = (fg[2] + ag2) / g_scale;
+                }
+            }
+        }
+        aphi = ag0 = ag1 = ag2 = 0.0;
+    }
+}
+
+// Potentials of several vectors from the stream: p2p_x2_mv_kernel's pair-steps (the pair
+// geometry once, q rinv added per vector) on flushes copied from the stream.
+template <int W>
+__global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
+    DevPlan plan, P2pItems items, int m, int near, float theta2, P2pStream st, const float* __restrict__ sq,
+    const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, int accumulate,
+    double* __restrict__ out_phi) {
+    constexpr int VB = kX2Vb;
+    __shared__ float4 sxy[W][2][kStPairs];
+    __shared__ float2 szz[W][2][kStPairs];
+    __shared__ float2 sqq[W][2][VB][kStPairs];
+    static_assert(VB * 32 * sizeof(double) <= sizeof(float4) * kStPairs, "reduction buffer");
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * W + warp;
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int box = plan.leaf_box[leaf];
+    const int64_t t1 = plan.tgt_start[leaf + 1];
+    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int K = 32 / ni;
+    const int kk = lane < ni * K ? lane / ni : K;
+    const int ti = lane < ni * K ? lane % ni : 0;
+    const int64_t t = items.t0[item] + ti;
+    const bool valid = lane < ni;
+    const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    if (kk < K) {
+        const float4 p4 = tpos[t];
+        tx = p4.x;
+        ty = p4.y;
+        tz = p4.z;
+    }
+    const float2 ntx = f2(-tx, -tx), nty = f2(-ty, -ty), ntz = f2(-tz, -tz);
+    const double rt = (plan.box_side ? plan.box_side[box] : plan.side) * pow2d(-(plan.level[box] + 1));
+    const double phi_scale = 4.0 * 3.141592653589793 * rt;
+    const int64_t pb = st.row_pair[leaf];
+    const int np_row = near ? (int)(st.row_pair[leaf + 1] - pb) : 0;
+    const int nfl = np_row > 0 ? (np_row + kStPairs - 1) / kStPairs : 1;
+    const int nvb = (m + VB - 1) / VB;
+    const int total = nfl * nvb;
+    int ivb = 0, ifl = 0;
+    int2 ix0 = make_int2(-1, -1), ix1 = make_int2(-1, -1);
+    auto load_idx = [&]() {
+        const int i0 = ifl * kStPairs + lane, i1 = i0 + 32;
+        ix0 = i0 < np_row ? st.idx[pb + i0] : make_int2(-1, -1);
+        ix1 = i1 < np_row ? st.idx[pb + i1] : make_int2(-1, -1);
+    };
+    auto issue = [&](int b) {
+        const int v0 = ivb * VB, nb = (m - v0) < VB ? (m - v0) : VB;
+        const int64_t base = pb + (int64_t)ifl * kStPairs;
+        const int npf = np_row - ifl * kStPairs;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = lane + 32 * h;
+            const int2 ix = h ? ix1 : ix0;
+            if (i < npf) {
+                cp_async16_cg(&sxy[warp][b][i], st.xy + base + i);
+                cp_async8(&szz[warp][b][i], st.zz + base + i);
+#pragma unroll
+                for (int vb = 0; vb < VB; ++vb)
+                    if (vb < nb) {
+                        const float* qv = sq + (int64_t)(v0 + vb) * nsrc;
+                        float* d = reinterpret_cast<float*>(&sqq[warp][b][vb][i]);
+                        cp_async4_zf(d, qv + (ix.x < 0 ? 0 : ix.x), ix.x < 0 ? 0 : 4);
+                        cp_async4_zf(d + 1, qv + (ix.y < 0 ? 0 : ix.y), ix.y < 0 ? 0 : 4);
+                    }
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        if (++ifl == nfl) {
+            ifl = 0;
+            ++ivb;
+        }
+        if (ivb < nvb) load_idx();
+    };
+    load_idx();
+    issue(0);
+    double aphi[VB];
+#pragma unroll
+    for (int vb = 0; vb < VB; ++vb) aphi[vb] = 0.0;
+    int cvb = 0, cfl = 0;
+    for (int f = 0; f < total; ++f) {
+        const int b = f & 1;
+        const int v0 = cvb * VB, nb = (m - v0) < VB ? (m - v0) : VB;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+        if (f + 1 < total) issue(b ^ 1);
+        const int rem = np_row - cfl * kStPairs;
+        const int npairs = rem < kStPairs ? rem : kStPairs;
+        float2 pphi[VB];
+#pragma unroll
+        for (int vb = 0; vb < VB; ++vb) pphi[vb] = f2(0.f, 0.f);
+#pragma unroll 2
+        for (int i = kk; i < npairs; i += K) {
+            const float4 a = sxy[warp][b][i];
+            const float2 zz = szz[warp][b][i];
+            const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
+            const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
+            const float2 dz = __fadd2_rn(zz, ntz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
+            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float2 rinv = f2(ri0, ri1);
+#pragma unroll
+            for (int vb = 0; vb < VB; ++vb)
+                if (vb < nb) pphi[vb] = __fadd2_rn(pphi[vb], __fmul2_rn(sqq[warp][b][vb][i], rinv));
+        }
+#pragma unroll
+        for (int vb = 0; vb < VB; ++vb) {
+            aphi[vb] += (double)pphi[vb].x;
+            aphi[vb] += (double)pphi[vb].y;
+        }
+        __syncwarp();
+        const bool last = cfl == nfl - 1;
+        if (++cfl == nfl) {
+            cfl = 0;
+            ++cvb;
+        }
+        if (!last) continue;
+        if (K > 1) {
+            double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[warp][b][0]);
+#pragma unroll
+            for (int vb = 0; vb < VB; ++vb) red[vb][lane] = aphi[vb];
+            __syncwarp();
+            if (valid)
+                for (int j = 1; j < K; ++j)
+#pragma unroll
+                    for (int vb = 0; vb < VB; ++vb) aphi[vb] += red[vb][ti + ni * j];
+            __syncwarp();
+        }
+        if (valid) {
+#pragma unroll
+            for (int vb = 0; vb < VB; ++vb) {
+                if (vb >= nb) break;
+                const int v = v0 + vb;
+                if (near) {
+                    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+                    close_pairs_f64<false>(close, t, close.q + (int64_t)v * nsrc, aphi[vb], g0, g1, g2);
+                }
+                if (accumulate == 2) {
+                    out_phi[(int64_t)v * nt + t] = aphi[vb];
+                } else if (accumulate) {
+                    far_phi[(int64_t)v * nt + t] = far_phi[(int64_t)v * nt + t] + aphi[vb];
+                } else {
+                    const double ph = far_phi[(int64_t)v * nt + t] + aphi[vb];
+                    out_phi[(int64_t)v * nt + plan.tgt_perm[t]] = ph / phi_scale;
+                }
+            }
+        }
+#pragma unroll
+        for (int vb = 0; vb < VB; ++vb) aphi[vb] = 0.0;
     }
 }
 

@@ -84,6 +84,7 @@ typedef struct {
     int64_t p2p_warps;    /* warps a block of the mixed P2P kernel (static 4, or the tuned one) */
     int64_t leaf_block;   /* threads a block of the L2P / M2P kernel (static 64, or the tuned one) */
     int64_t product_chunks; /* chunks of the M2L product path (0: every product at once) */
+    int64_t p2p_stream_bytes; /* the mixed P2P's near-row source streams (0: mapped per flush) */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;
@@ -189,6 +190,11 @@ int fmmgpu_fmm_set_kinds(fmmgpu_fmm* fmm, int kinds);
  * product array; at most 128 vectors a pass, 64 at p = 8), 0 SIMT products then the
  * reduce.  2 and 1 give the same bits.  Synchronises. */
 int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* fmm, int path);
+/* Where the mixed P2P takes its sources from, for tests: 1 (the default when the streams
+ * were built: at most a quarter of the free device memory) every near row's sources
+ * mapped into its target leaf's frame once, at build time, and copied per flush; 0 the
+ * sources mapped per flush.  The same bits.  Synchronises. */
+int fmmgpu_fmm_set_p2p_path(fmmgpu_fmm* fmm, int path);
 /* Milliseconds of the last evaluation per kind: [0] charge load, [1] P2M, [2] M2M,
  * [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P + output pass.  Synchronises. */
 int fmmgpu_fmm_kind_times(fmmgpu_fmm* fmm, double* ms);
