@@ -225,6 +225,9 @@ struct Evaluator final : EvaluatorBase {
     DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
     // the near rows' source streams in the target leaves' frames (mixed form, P2pStream)
     DevBuf st_rowpair, st_xy, st_zz, st_idx;
+    // the near-singular pairs' weights (per pair) and, per evaluation, their f64 sums per
+    // target and vector (close_weights_kernel, close_sum_kernel)
+    DevBuf close_w, close_acc;
     // boxes with a nonempty X list, level by level (the P2L launches)
     DevBuf xbox;
     std::vector<int64_t> xbox_start;
@@ -241,6 +244,7 @@ struct Evaluator final : EvaluatorBase {
 
     // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
     static constexpr float kTheta2 = 0.0625f;
+    static constexpr float kRmax = 4.0f;  // 1 / theta: the mixed P2P's clamp of 1/r
 
     Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
               const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
@@ -857,6 +861,33 @@ struct Evaluator final : EvaluatorBase {
         if (plan.nleaves()) close_map_kernel<<<(unsigned)plan.nleaves(), 64>>>(dp, close, close_y.as<double4>());
         CUDA_TRY(cudaGetLastError());
         close.q = sq64.as<double>();
+        const size_t wd = gradients ? 4 : 1;  // doubles a pair / a target and vector
+        close_w.alloc(sizeof(double) * wd * (size_t)(nclose + 1));
+        close_acc.alloc(sizeof(double) * wd * (size_t)m * (dp.ntgt + 1));
+        close.acc = close_acc.as<double>();
+        if (plan.nleaves() && nclose) {
+            const auto* s32 = reinterpret_cast<const float4*>(spos.ptr);
+            const auto* t32 = reinterpret_cast<const float4*>(tpos.ptr);
+            if (gradients)
+                close_weights_kernel<true><<<(unsigned)plan.nleaves(), 64>>>(dp, close, s32, t32, kRmax,
+                                                                             close_w.as<double>());
+            else
+                close_weights_kernel<false><<<(unsigned)plan.nleaves(), 64>>>(dp, close, s32, t32, kRmax,
+                                                                              close_w.as<double>());
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    // The near-singular pairs' f64 sums of this pass's charges (mixed form).
+    void close_sums(cudaStream_t s) {
+        if (!kMixed || !nclose || !dp.ntgt) return;
+        const unsigned g = (unsigned)((dp.ntgt + 255) / 256);
+        if (gradients)
+            close_sum_kernel<true><<<counted(g), 256, 0, s>>>(close, close_w.as<double>(), m, dp.nsrc, dp.ntgt,
+                                                             close_acc.as<double>());
+        else
+            close_sum_kernel<false><<<counted(g), 256, 0, s>>>(close, close_w.as<double>(), m, dp.nsrc, dp.ntgt,
+                                                              close_acc.as<double>());
     }
 
     int device_status() override {
@@ -881,7 +912,7 @@ struct Evaluator final : EvaluatorBase {
                                &near_phi, &near_g, &box_side, &v_pos, &xbox, &fu_tile_d, &fu_tile_begin,
                                &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
                                &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src, &st_rowpair,
-                               &st_xy, &st_zz, &st_idx};
+                               &st_xy, &st_zz, &st_idx, &close_w, &close_acc};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;
@@ -893,9 +924,13 @@ struct Evaluator final : EvaluatorBase {
             timer.begin();
             launches = 0;
         }
+        // the near-singular sums (mixed) need only the charges: beside the far field on
+        // near_stream, or with the charge load when kinds are timed
+        const bool sums = kMixed && nclose && (kinds & 1) && items.count;
         // charge load into leaf order
         timer.run(kLoad, [&] {
             load_charges(d_charges);
+            if (sums && timer.on) close_sums(stream);
             // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
             int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
             CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * ms_of(P) * top, stream));
@@ -906,6 +941,7 @@ struct Evaluator final : EvaluatorBase {
             // addition as the fused P2P epilogue, so the same floats
             CUDA_TRY(cudaEventRecord(ev_fork, stream));
             CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
+            close_sums(near_stream);
             p2p_items(0, items.count, 1, 2, near_phi.as<double>(), gradients ? near_g.as<double>() : nullptr,
                       near_stream);
             CUDA_TRY(cudaEventRecord(ev_join, near_stream));
@@ -915,6 +951,13 @@ struct Evaluator final : EvaluatorBase {
             CUDA_TRY(cudaGetLastError());
             return;
         }
+        const bool forked = sums && !timer.on;
+        if (forked) {
+            CUDA_TRY(cudaEventRecord(ev_fork, stream));
+            CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
+            close_sums(near_stream);
+            CUDA_TRY(cudaEventRecord(ev_join, near_stream));
+        }
         if (!(kinds & 2)) {
             // far field off: zero partials, then the near field and the output pass only
             CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
@@ -922,6 +965,7 @@ struct Evaluator final : EvaluatorBase {
         } else {
             run_far();
         }
+        if (forked) CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
         if (items.count) timer.run(kP2P, [&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
         CUDA_TRY(cudaGetLastError());
     }
@@ -1189,24 +1233,24 @@ struct Evaluator final : EvaluatorBase {
         if (p2p_path == 1) {
             const P2pStream st{st_rowpair.as<int64_t>(), st_xy.as<float4>(), st_zz.as<float2>(), st_idx.as<int2>()};
             if (!gradients)
-                p2p_st_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, st, q, tp, close,
+                p2p_st_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, st, q, tp, close,
                                                                  far_phi.as<double>(), accumulate, d_phi);
             else
-                p2p_st_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, st, q, tp, close,
+                p2p_st_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, st, q, tp, close,
                                                                    far_phi.as<double>(), fg, accumulate, d_phi, og);
             return;
         }
         if (!gradients) {  // potentials: the pair geometry shared by up to kX2Vb vectors (any m)
-            p2p_x2_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp, q,
+            p2p_x2_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, near_rec.as<NearRec>(), sp, q,
                                                              tp, close, far_phi.as<double>(), accumulate, d_phi);
             return;
         }
         if (gradients)
-            p2p_x2_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(), sp,
+            p2p_x2_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, near_rec.as<NearRec>(), sp,
                                                                q, tp, close, far_phi.as<double>(), fg, accumulate,
                                                                d_phi, og);
         else
-            p2p_x2_kernel<false, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kTheta2, near_rec.as<NearRec>(),
+            p2p_x2_kernel<false, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, near_rec.as<NearRec>(),
                                                                 sp, q, tp, close, far_phi.as<double>(), fg,
                                                                 accumulate, d_phi, og);
     }
@@ -1271,6 +1315,7 @@ struct Evaluator final : EvaluatorBase {
     void op_begin(const double* d_charges) override {
         launches = 0;
         load_charges(d_charges);
+        close_sums(stream);
         CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, Lc.bytes, stream));
         CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
         CUDA_TRY(cudaMemsetAsync(far_g.ptr, 0, far_g.bytes, stream));

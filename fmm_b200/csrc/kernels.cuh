@@ -778,6 +778,9 @@ struct ClosePairs {  // near-singular pairs of the mixed form, CSR by target (le
     const double4* tpos;
     const double* q;      // f64 charges in leaf order [vector][point]
     const double4* y;     // the source point in the target leaf's frame (f64), per pair
+    // mixed Laplace P2P: per target the f64 sum over its pairs of q times the pair's
+    // weight (close_sum_kernel), [vector][target], 4 doubles (phi, grad) or 1 (phi)
+    const double* acc;
 };
 
 // Build time (mixed form): each near-singular pair's source point mapped into its target

@@ -1,23 +1,24 @@
 // Mixed-precision P2P on the packed f32x2 pipe of sm_100 (FFMA2 / FADD2 / FMUL2).
 //
-// Same sums as p2p_kernel<float, GRAD, true> (kernels.cuh): one warp per work item of up
-// to 32 targets of one leaf (lane = target; an item of fewer targets splits the sources
-// over several lanes per target), the near row of that leaf (source leaves in
-// row order, points in leaf order), sources mapped into the target leaf's frame by
-// y = fma(r, u, c) (fmm-kernels/src/p2p.rs:320-340 frame_centre / frame_ratio), the pair
-// skipped iff its f32 r2 < theta2 (those pairs are added in f64 from the close-pair CSR,
-// found at build time by close_pairs_kernel with this r2), f32 partials added into f64
-// per-target accumulators.  What differs is the schedule:
+// One warp per work item of up to 32 targets of one leaf (lane = target; an item of fewer
+// targets splits the sources over several lanes per target), the near row of that leaf
+// (source leaves in row order, points in leaf order), sources mapped into the target
+// leaf's frame by y = fma(r, u, c) (fmm-kernels/src/p2p.rs:320-340 frame_centre /
+// frame_ratio), f32 pair terms with 1/r clamped to 4 (the near-singular pairs, f32
+// r2 < theta2 = 1/16, found at build time by close_pairs_kernel with this r2, are then
+// corrected by their f64 weights: close_sum_kernel below), f32 partials added into f64
+// per-target accumulators.  The schedule:
 //  - each lane takes two sources per instruction: the stage holds sources in pairs,
 //    (x0, x1, y0, y1) and (z0, z1, q0, q1), so one LDS.128 yields aligned float2
 //    operands and every add / multiply / fma of a pair-step is one f32x2 instruction;
-//    the difference is formed as d = y + (-t) = -(t - y) exactly, so r2 is the same
-//    float as p2p_kernel's and the gradient term fma(qr3, d, g) equals g - qr3 (t - y);
+//    the difference is formed as d = y + (-t) = -(t - y) exactly, so r2 is the float the
+//    close-pair search forms and the gradient term fma(qr3, d, g) equals g - qr3 (t - y);
 //  - the frame, start and size of every near entry are precomputed at build time
 //    (NearRec, from rel_frame<float>, the same function the close-pair search uses), so
 //    a source leaf costs no dependent index loads;
 //  - the stage is filled across source-leaf boundaries (128 sources per flush), the next
 //    flush's points and charges copied asynchronously (cp.async) while one is computed;
+//    the streamed form (p2p_st_kernel) copies flushes already mapped at build time;
 //  - an item of fewer than 32 targets splits the sources over several lanes per target.
 // The f32 partial of a flush (at most 64 sources per half) is added into the f64 sums.
 #pragma once
@@ -51,6 +52,102 @@ __global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec* __res
         off += x.ns;
         rec[e] = x;
     }
+}
+
+// The near-singular pairs as a fixed sparse operator.  In the f32 pair loop every pair's
+// 1/r is clamped to rmax = 1/theta = 4: a pair with f32 r^2 >= theta^2 = 1/16 is unchanged
+// (its 1/r is at most 4), a near-singular one (f32 r^2 < 1/16, the pairs close_pairs_kernel
+// finds with the same arithmetic) contributes exactly 4 q to phi and 64 q d32 to the
+// gradient sum, d32 its f32 difference y - t.  The exact term minus that clamp term is q
+// times a weight fixed by the geometry, formed at build time in f64 from f64 coordinates
+// with the reference's coincidence rule (a coincident pair has no exact term):
+// w = (1/r - 4, (y - u)/r^3 - 64 d32).  Each evaluation forms the f64 sum of q_s w over a
+// target's near-singular pairs in CSR order (close_sum_kernel, q the f64 charges) and the
+// P2P epilogue adds it once, after the f32 partials.  The clamp terms carry the f32
+// charge and the weights the f64 one: the difference is 4 |q32 - q64| <= 2^-22 |q| a pair.
+
+// Build time: block per leaf, thread per target; w is 4 doubles a pair (GRAD) or 1.
+template <bool GRAD>
+__global__ void close_weights_kernel(DevPlan plan, ClosePairs close, const float4* __restrict__ spos32,
+                                     const float4* __restrict__ tpos32, float rmax, double* __restrict__ w) {
+    const int64_t leaf = blockIdx.x;
+    const int box = plan.leaf_box[leaf];
+    const double R = rmax, R3 = (double)rmax * rmax * rmax;
+    for (int64_t t = plan.tgt_start[leaf] + threadIdx.x; t < plan.tgt_start[leaf + 1]; t += blockDim.x) {
+        const double4 u = close.tpos[t];
+        const float4 t32 = tpos32[t];
+        for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
+            // the f32 difference of the pair loop: the near entry's frame (NearRec), y + (-t)
+            float fc[3], fr;
+            rel_frame<float>(plan, plan.leaf_box[close.leaf[c2]], box, fc, fr);
+            const float4 p = spos32[close.src[c2]];
+            const double d32x = __fadd_rn(__fmaf_rn(fr, p.x, fc[0]), -t32.x);
+            const double d32y = __fadd_rn(__fmaf_rn(fr, p.y, fc[1]), -t32.y);
+            const double d32z = __fadd_rn(__fmaf_rn(fr, p.z, fc[2]), -t32.z);
+            const double4 y = close.y[c2];
+            double rinv = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+            if (!(u.x == y.x && u.y == y.y && u.z == y.z)) {
+                dx = y.x - u.x;
+                dy = y.y - u.y;
+                dz = y.z - u.z;
+                rinv = rsqrt(dx * dx + dy * dy + dz * dz);
+            }
+            const double r3 = rinv * rinv * rinv;
+            if (GRAD)
+                reinterpret_cast<double4*>(w)[c2] =
+                    make_double4(rinv - R, r3 * dx - R3 * d32x, r3 * dy - R3 * d32y, r3 * dz - R3 * d32z);
+            else
+                w[c2] = rinv - R;
+        }
+    }
+}
+
+// Evaluation: thread per target, every vector of the pass; acc [vector][target].
+template <bool GRAD>
+__global__ void close_sum_kernel(ClosePairs close, const double* __restrict__ w, int m, int64_t nsrc, int64_t nt,
+                                 double* __restrict__ acc) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const int64_t c0 = close.row[t], c1 = close.row[t + 1];
+    for (int v = 0; v < m; ++v) {
+        const double* qv = close.q + (int64_t)v * nsrc;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll 4
+        for (int64_t c = c0; c < c1; ++c) {
+            const double q = qv[close.src[c]];
+            if (GRAD) {
+                const double4 wc = reinterpret_cast<const double4*>(w)[c];
+                a0 = __fma_rn(q, wc.x, a0);
+                a1 = __fma_rn(q, wc.y, a1);
+                a2 = __fma_rn(q, wc.z, a2);
+                a3 = __fma_rn(q, wc.w, a3);
+            } else {
+                a0 = __fma_rn(q, w[c], a0);
+            }
+        }
+        if (GRAD)
+            reinterpret_cast<double4*>(acc)[(int64_t)v * nt + t] = make_double4(a0, a1, a2, a3);
+        else
+            acc[(int64_t)v * nt + t] = a0;
+    }
+}
+
+// The P2P epilogue's addition of a target's near-singular sum (entry vt = v nt + t).
+template <bool GRAD>
+__device__ __forceinline__ void close_sum_add(const ClosePairs& close, int64_t vt, double& aphi, double& ag0,
+                                              double& ag1, double& ag2) {
+    if (GRAD) {
+        const double4 c = reinterpret_cast<const double4*>(close.acc)[vt];
+        aphi += c.x;
+        ag0 += c.y;
+        ag1 += c.z;
+        ag2 += c.w;
+    } else {
+        aphi += close.acc[vt];
+    }
+}
+__device__ __forceinline__ void close_sum_add1(const ClosePairs& close, int64_t vt, double& aphi) {
+    aphi += close.acc[vt];
 }
 
 constexpr int kX2Warps = 4;      // warps a block until the autotuner chooses
@@ -93,7 +190,7 @@ __device__ __forceinline__ void cp_async4_zf(void* smem, const void* gmem, int s
 // at most 64 registers a thread, so 32 warps are resident on an SM for every W.
 template <bool GRAD, int W>
 __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
-    DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
+    DevPlan plan, P2pItems items, int m, int near, float rmax, const NearRec* __restrict__ recs,
     const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
     double* __restrict__ far_phi, double* __restrict__ far_g, int accumulate, double* __restrict__ out_phi,
     double* __restrict__ out_g) {
@@ -202,8 +299,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
             const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
             const float2 dz = __fadd2_rn(f2(b.x, b.y), ntz);
             const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
-            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float ri0 = fminf(rsqrtf(r2.x), rmax);
+            const float ri1 = fminf(rsqrtf(r2.y), rmax);
             const float2 rinv = f2(ri0, ri1);
             const float2 qr = __fmul2_rn(f2(b.z, b.w), rinv);
             pphi = __fadd2_rn(pphi, qr);
@@ -243,26 +340,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
             __syncwarp();
         }
         if (valid) {
-            if (near) {
-                // near-singular pairs in f64: the f64 map and the reference's coincidence rule
-                // (the source points already in the target's frame, close_map_kernel)
-                const double4 u = close.tpos[t];
-                for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
-                    const double4 y = close.y[c2];
-                    if (u.x == y.x && u.y == y.y && u.z == y.z) continue;
-                    const double dx = u.x - y.x, dy = u.y - y.y, dz = u.z - y.z;
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    const double rinv = rsqrt(r2);
-                    const double qr = close.q[(int64_t)v * nsrc + close.src[c2]] * rinv;
-                    aphi += qr;
-                    if (GRAD) {
-                        const double qr3 = qr * rinv * rinv;
-                        ag0 -= qr3 * dx;
-                        ag1 -= qr3 * dy;
-                        ag2 -= qr3 * dz;
-                    }
-                }
-            }
+            if (near) close_sum_add<GRAD>(close, (int64_t)v * nt + t, aphi, ag0, ag1, ag2);
             // both gradient sums hold -sum qr3 (t - y), as p2p_kernel's
             if (accumulate == 2) {  // near field alone, leaf order (added to the far field by output_kernel)
                 out_phi[(int64_t)v * nt + t] = aphi;
@@ -307,7 +385,7 @@ constexpr int kX2Vb = 4;  // vectors a flush
 
 template <int W>
 __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
-    DevPlan plan, P2pItems items, int m, int near, float theta2, const NearRec* __restrict__ recs,
+    DevPlan plan, P2pItems items, int m, int near, float rmax, const NearRec* __restrict__ recs,
     const float4* __restrict__ spos, const float* __restrict__ sq, const float4* __restrict__ tpos, ClosePairs close,
     double* __restrict__ far_phi, int accumulate, double* __restrict__ out_phi) {
     constexpr int VB = kX2Vb;
@@ -423,8 +501,8 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
             const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
             const float2 dz = __fadd2_rn(zz, ntz);
             const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
-            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float ri0 = fminf(rsqrtf(r2.x), rmax);
+            const float ri1 = fminf(rsqrtf(r2.y), rmax);
             const float2 rinv = f2(ri0, ri1);
 #pragma unroll
             for (int b = 0; b < VB; ++b)
@@ -449,19 +527,10 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
             __syncwarp();
         }
         if (valid) {
-            if (near) {
-                const double4 u = close.tpos[t];
-                for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
-                    const double4 y = close.y[c2];
-                    if (u.x == y.x && u.y == y.y && u.z == y.z) continue;
-                    const double dx = u.x - y.x, dy = u.y - y.y, dz = u.z - y.z;
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    const double rinv = rsqrt(r2);
+            if (near)
 #pragma unroll
-                    for (int b = 0; b < VB; ++b)
-                        if (b < nb) aphi[b] += close.q[(int64_t)(v0 + b) * nsrc + close.src[c2]] * rinv;
-                }
-            }
+                for (int b = 0; b < VB; ++b)
+                    if (b < nb) close_sum_add1(close, (int64_t)(v0 + b) * nt + t, aphi[b]);
 #pragma unroll
             for (int b = 0; b < VB; ++b) {
                 if (b >= nb) break;
@@ -537,46 +606,9 @@ __global__ void near_stream_kernel(DevPlan plan, int64_t nleaves, const NearRec*
 
 constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
 
-// The near-singular pairs of target t for vector v, added in f64 in CSR order (the
-// sums of p2p_x2_kernel's loop), their records fetched four at a time; y.w holds the
-// source's index (close_map_kernel).
-template <bool GRAD>
-__device__ __forceinline__ void close_pairs_f64(const ClosePairs& close, int64_t t, const double* __restrict__ qv,
-                                                double& aphi, double& ag0, double& ag1, double& ag2) {
-    const double4 u = close.tpos[t];
-    const int64_t c0 = close.row[t], c1 = close.row[t + 1];
-    constexpr int CB = 2;
-    for (int64_t c = c0; c < c1; c += CB) {
-        double4 y[CB];
-        double qq[CB];
-#pragma unroll
-        for (int j = 0; j < CB; ++j)
-            if (c + j < c1) y[j] = close.y[c + j];
-#pragma unroll
-        for (int j = 0; j < CB; ++j)
-            if (c + j < c1) qq[j] = qv[(int64_t)y[j].w];
-#pragma unroll
-        for (int j = 0; j < CB; ++j) {
-            if (c + j >= c1) break;
-            if (u.x == y[j].x && u.y == y[j].y && u.z == y[j].z) continue;
-            const double dx = u.x - y[j].x, dy = u.y - y[j].y, dz = u.z - y[j].z;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            const double rinv = rsqrt(r2);
-            const double qr = qq[j] * rinv;
-            aphi += qr;
-            if (GRAD) {
-                const double qr3 = qr * rinv * rinv;
-                ag0 -= qr3 * dx;
-                ag1 -= qr3 * dy;
-                ag2 -= qr3 * dz;
-            }
-        }
-    }
-}
-
 template <bool GRAD, int W>
 __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
-    DevPlan plan, P2pItems items, int m, int near, float theta2, P2pStream st, const float* __restrict__ sq,
+    DevPlan plan, P2pItems items, int m, int near, float rmax, P2pStream st, const float* __restrict__ sq,
     const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, double* __restrict__ far_g,
     int accumulate, double* __restrict__ out_phi, double* __restrict__ out_g) {
     __shared__ float4 sxy[W][2][kStPairs];  // (x0, x1, y0, y1), two flushes
@@ -662,8 +694,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
             const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
             const float2 dz = __fadd2_rn(f2(c.x, c.y), ntz);
             const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
-            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float ri0 = fminf(rsqrtf(r2.x), rmax);
+            const float ri1 = fminf(rsqrtf(r2.y), rmax);
             const float2 rinv = f2(ri0, ri1);
             const float2 qr = __fmul2_rn(f2(c.z, c.w), rinv);
             pphi = __fadd2_rn(pphi, qr);
@@ -710,7 +742,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
             __syncwarp();
         }
         if (valid) {
-            if (near) close_pairs_f64<GRAD>(close, t, close.q + (int64_t)v * nsrc, aphi, ag0, ag1, ag2);
+            if (near) close_sum_add<GRAD>(close, (int64_t)v * nt + t, aphi, ag0, ag1, ag2);
             if (accumulate == 2) {
                 out_phi[(int64_t)v * nt + t] = aphi;
                 if (GRAD) {
@@ -748,7 +780,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
 // geometry once, q rinv added per vector) on flushes copied from the stream.
 template <int W>
 __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
-    DevPlan plan, P2pItems items, int m, int near, float theta2, P2pStream st, const float* __restrict__ sq,
+    DevPlan plan, P2pItems items, int m, int near, float rmax, P2pStream st, const float* __restrict__ sq,
     const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, int accumulate,
     double* __restrict__ out_phi) {
     constexpr int VB = kX2Vb;
@@ -844,8 +876,8 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
             const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
             const float2 dz = __fadd2_rn(zz, ntz);
             const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            const float ri0 = r2.x < theta2 ? 0.f : rsqrtf(r2.x);
-            const float ri1 = r2.y < theta2 ? 0.f : rsqrtf(r2.y);
+            const float ri0 = fminf(rsqrtf(r2.x), rmax);
+            const float ri1 = fminf(rsqrtf(r2.y), rmax);
             const float2 rinv = f2(ri0, ri1);
 #pragma unroll
             for (int vb = 0; vb < VB; ++vb)
@@ -879,10 +911,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
             for (int vb = 0; vb < VB; ++vb) {
                 if (vb >= nb) break;
                 const int v = v0 + vb;
-                if (near) {
-                    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-                    close_pairs_f64<false>(close, t, close.q + (int64_t)v * nsrc, aphi[vb], g0, g1, g2);
-                }
+                if (near) close_sum_add1(close, (int64_t)v * nt + t, aphi[vb]);
                 if (accumulate == 2) {
                     out_phi[(int64_t)v * nt + t] = aphi[vb];
                 } else if (accumulate) {

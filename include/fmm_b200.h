@@ -195,8 +195,10 @@ int fmmgpu_fmm_set_m2l_path(fmmgpu_fmm* fmm, int path);
  * mapped into its target leaf's frame once, at build time, and copied per flush; 0 the
  * sources mapped per flush.  The same bits.  Synchronises. */
 int fmmgpu_fmm_set_p2p_path(fmmgpu_fmm* fmm, int path);
-/* Milliseconds of the last evaluation per kind: [0] charge load, [1] P2M, [2] M2M,
- * [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P + output pass.  Synchronises. */
+/* Milliseconds of the last evaluation per kind: [0] charge load (in timed evaluations
+ * with the mixed form's f64 sums of the near-singular pairs, which otherwise run beside
+ * the far field), [1] P2M, [2] M2M, [3] L2L, [4] M2L, [5] P2L, [6] L2P + M2P, [7] P2P +
+ * output pass.  Synchronises. */
 int fmmgpu_fmm_kind_times(fmmgpu_fmm* fmm, double* ms);
 
 /* Waits for the stream and returns the first device error, if any. */
