@@ -237,6 +237,7 @@ struct Evaluator final : EvaluatorBase {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     P2pItems items{};
     std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
+    std::vector<int32_t> item_leaf_h;  // the items' leaves (host copy, ascending)
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
@@ -792,6 +793,7 @@ struct Evaluator final : EvaluatorBase {
         }
         item_leaf.upload(il);
         item_t0.upload(it);
+        item_leaf_h = il;
         items.leaf = item_leaf.as<int32_t>();
         items.t0 = item_t0.as<int64_t>();
         items.count = (int64_t)il.size();
@@ -1208,12 +1210,24 @@ struct Evaluator final : EvaluatorBase {
         if (r1 <= r0) return;
         const size_t smem = sizeof(T) == 8 ? NC * sizeof(T) : 0;
         if constexpr (kMixed) {
-            if (!gradients) {  // potentials: the harmonics shared by up to 8 vectors (any m: the same floats)
-                leaf_far_mv_kernel<P, 8><<<counted((unsigned)(r1 - r0)), leaf_block, 0, stream>>>(
-                    dp, r0, mode, m, reinterpret_cast<const float4*>(tpos.ptr), reinterpret_cast<const float*>(M.ptr),
-                    reinterpret_cast<const float*>(Lc.ptr), far_phi.as<double>());
-                return;
-            }
+            // a warp per P2P work item of these leaves (items are in leaf order); leaf_block
+            // threads a block
+            const int64_t i0 = std::lower_bound(item_leaf_h.begin(), item_leaf_h.end(), (int32_t)r0) - item_leaf_h.begin();
+            const int64_t i1 = std::lower_bound(item_leaf_h.begin(), item_leaf_h.end(), (int32_t)r1) - item_leaf_h.begin();
+            if (i1 <= i0) return;
+            const P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
+            const int wpb = leaf_block / 32;
+            const unsigned g = (unsigned)((it.count + wpb - 1) / wpb);
+            const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
+            const auto* Mf = reinterpret_cast<const float*>(M.ptr);
+            const auto* Lf = reinterpret_cast<const float*>(Lc.ptr);
+            if (!gradients)  // potentials: the harmonics shared by up to 8 vectors (any m: the same floats)
+                leaf_far_mv_items_kernel<P, 8><<<counted(g), leaf_block, 0, stream>>>(dp, it, mode, m, tp, Mf, Lf,
+                                                                                     far_phi.as<double>());
+            else
+                leaf_far_items_kernel<P, true><<<counted(g), leaf_block, 0, stream>>>(
+                    dp, it, mode, m, tp, Mf, Lf, far_phi.as<double>(), far_g.as<double>());
+            return;
         }
         if (gradients)
             leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), leaf_block, smem, stream>>>(

@@ -770,6 +770,115 @@ struct P2pItems {
     int64_t count;
 };
 
+// L2P + M2P of the f32 form over P2P work items: a warp per item (up to 32 targets of one
+// leaf, lane = target), any number of warps a block.  Each target sums exactly the terms of
+// leaf_far_kernel<P, float, GRAD> / leaf_far_mv_kernel<P, VB> in the same order, so the
+// floats are those kernels'; what changes is the occupancy: a block per leaf holds every
+// thread of its block while a leaf of few targets keeps one warp busy, a warp per item
+// leaves no idle warp resident.
+template <int P, bool GRAD>
+__global__ void __launch_bounds__(128) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
+                                                             const float4* __restrict__ tpos,
+                                                             const float* __restrict__ M, const float* __restrict__ Lc,
+                                                             double* __restrict__ far_phi, double* __restrict__ far_g) {
+    const int64_t item = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int64_t t = items.t0[item] + (threadIdx.x & 31);
+    if (t >= plan.tgt_start[leaf + 1]) return;
+    const int box = plan.leaf_box[leaf];
+    const int64_t w0 = plan.w_row[leaf], w1 = (mode & 2) ? plan.w_row[leaf + 1] : plan.w_row[leaf];
+    const int64_t nt = plan.ntgt;
+    const float4 p4 = tpos[t];
+    const float ux = p4.x, uy = p4.y, uz = p4.z;
+    for (int v = 0; v < m; ++v) {
+        double fphi = 0.0, fg[3] = {0.0, 0.0, 0.0};
+        if (mode & 4) {
+            fphi = far_phi[(int64_t)v * nt + t];
+            if (GRAD)
+                for (int k = 0; k < 3; ++k) fg[k] = far_g[((int64_t)v * nt + t) * 3 + k];
+        }
+        if (mode & 1) {
+            float ph, gx, gy, gz;
+            l2p_eval<P, float, GRAD>(Lc + ((int64_t)box * m + v) * ms_of(P), ux, uy, uz, ph, gx, gy, gz);
+            fphi = (mode & 4) ? fphi + (double)ph : (double)ph;
+            if (GRAD) {
+                fg[0] = (mode & 4) ? fg[0] + (double)gx : (double)gx;
+                fg[1] = (mode & 4) ? fg[1] + (double)gy : (double)gy;
+                fg[2] = (mode & 4) ? fg[2] + (double)gz : (double)gz;
+            }
+        }
+        for (int64_t e = w0; e < w1; ++e) {
+            const int s = plan.w_col[e];
+            float c[3], r;
+            rel_frame<float>(plan, s, box, c, r);
+            const float rinv = 1.0f / r;
+            float ph, gx, gy, gz;
+            m2p_eval<P, float, GRAD>(M + ((int64_t)s * m + v) * ms_of(P), (ux - c[0]) * rinv, (uy - c[1]) * rinv,
+                                     (uz - c[2]) * rinv, ph, gx, gy, gz);
+            fphi += (double)(ph * rinv);
+            if (GRAD) {
+                const float r2inv = rinv * rinv;
+                fg[0] += (double)(gx * r2inv);
+                fg[1] += (double)(gy * r2inv);
+                fg[2] += (double)(gz * r2inv);
+            }
+        }
+        far_phi[(int64_t)v * nt + t] = fphi;
+        if (GRAD) {
+            double* g = far_g + ((int64_t)v * nt + t) * 3;
+            g[0] = fg[0];
+            g[1] = fg[1];
+            g[2] = fg[2];
+        }
+    }
+}
+
+template <int P, int VB>
+__global__ void __launch_bounds__(128) leaf_far_mv_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
+                                                                const float4* __restrict__ tpos,
+                                                                const float* __restrict__ M,
+                                                                const float* __restrict__ Lc,
+                                                                double* __restrict__ far_phi) {
+    constexpr int MS = ms_of(P);
+    const int64_t item = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (item >= items.count) return;
+    const int leaf = items.leaf[item];
+    const int64_t t = items.t0[item] + (threadIdx.x & 31);
+    if (t >= plan.tgt_start[leaf + 1]) return;
+    const int box = plan.leaf_box[leaf];
+    const int64_t w0 = plan.w_row[leaf], w1 = (mode & 2) ? plan.w_row[leaf + 1] : plan.w_row[leaf];
+    const int64_t nt = plan.ntgt;
+    const float4 p4 = tpos[t];
+    const float ux = p4.x, uy = p4.y, uz = p4.z;
+    for (int v0 = 0; v0 < m; v0 += VB) {
+        const int nb = (m - v0) < VB ? (m - v0) : VB;
+        double fphi[VB];
+#pragma unroll
+        for (int b = 0; b < VB; ++b) fphi[b] = (b < nb && (mode & 4)) ? far_phi[(int64_t)(v0 + b) * nt + t] : 0.0;
+        if (mode & 1) {
+            float ph[VB];
+            l2p_eval_mv<P, VB>(Lc + ((int64_t)box * m + v0) * MS, nb, ux, uy, uz, ph);
+#pragma unroll
+            for (int b = 0; b < VB; ++b) fphi[b] = (mode & 4) ? fphi[b] + (double)ph[b] : (double)ph[b];
+        }
+        for (int64_t e = w0; e < w1; ++e) {
+            const int s = plan.w_col[e];
+            float c[3], r;
+            rel_frame<float>(plan, s, box, c, r);
+            const float rinv = 1.0f / r;
+            float ph[VB];
+            m2p_eval_mv<P, VB>(M + ((int64_t)s * m + v0) * MS, nb, (ux - c[0]) * rinv, (uy - c[1]) * rinv,
+                               (uz - c[2]) * rinv, ph);
+#pragma unroll
+            for (int b = 0; b < VB; ++b) fphi[b] += (double)(ph[b] * rinv);
+        }
+#pragma unroll
+        for (int b = 0; b < VB; ++b)
+            if (b < nb) far_phi[(int64_t)(v0 + b) * nt + t] = fphi[b];
+    }
+}
+
 struct ClosePairs {  // near-singular pairs of the mixed form, CSR by target (leaf order)
     const int64_t* row;
     const int64_t* src;   // source point (leaf order)
