@@ -771,13 +771,14 @@ struct P2pItems {
 };
 
 // L2P + M2P of the f32 form over P2P work items: a warp per item (up to 32 targets of one
-// leaf, lane = target), any number of warps a block.  Each target sums exactly the terms of
-// leaf_far_kernel<P, float, GRAD> / leaf_far_mv_kernel<P, VB> in the same order, so the
-// floats are those kernels'; what changes is the occupancy: a block per leaf holds every
-// thread of its block while a leaf of few targets keeps one warp busy, a warp per item
-// leaves no idle warp resident.
+// leaf, lane = target), any number of warps a block.  Each target sums the terms of
+// leaf_far_kernel<P, float, GRAD> / leaf_far_mv_kernel<P, VB> in the same order (the
+// compiler may contract products into fmas differently, so the last bits can differ);
+// what changes is the occupancy: a block per leaf holds every thread of its block while a
+// leaf of few targets keeps one warp busy, a warp per item leaves no idle warp resident.
+// The gradient form is held to 96 registers (21 warps an SM, no spills).
 template <int P, bool GRAD>
-__global__ void __launch_bounds__(128) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
+__global__ void __launch_bounds__(128, 5) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
                                                              const float4* __restrict__ tpos,
                                                              const float* __restrict__ M, const float* __restrict__ Lc,
                                                              double* __restrict__ far_phi, double* __restrict__ far_g) {
