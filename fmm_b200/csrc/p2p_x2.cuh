@@ -686,8 +686,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         const int rem = np_row - cfl * kStPairs;
         const int npairs = rem < kStPairs ? rem : kStPairs;
         float2 pphi = f2(0.f, 0.f), pg0 = f2(0.f, 0.f), pg1 = f2(0.f, 0.f), pg2 = f2(0.f, 0.f);
-#pragma unroll 4
-        for (int i = kk; i < npairs; i += K) {
+        auto step = [&](int i) {
             const float4 a = sxy[warp][b][i];
             const float4 c = szq[warp][b][i];
             const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
@@ -705,6 +704,13 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
                 pg1 = __ffma2_rn(qr3, dy, pg1);
                 pg2 = __ffma2_rn(qr3, dz, pg2);
             }
+        };
+        if (K == 1) {  // the common item of one target a lane: a unit stride (8 % faster)
+#pragma unroll 4
+            for (int i = 0; i < npairs; ++i) step(i);
+        } else {
+#pragma unroll 2
+            for (int i = kk; i < npairs; i += K) step(i);
         }
         aphi += (double)pphi.x;
         aphi += (double)pphi.y;
@@ -868,8 +874,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
         float2 pphi[VB];
 #pragma unroll
         for (int vb = 0; vb < VB; ++vb) pphi[vb] = f2(0.f, 0.f);
-#pragma unroll 2
-        for (int i = kk; i < npairs; i += K) {
+        auto step = [&](int i) {
             const float4 a = sxy[warp][b][i];
             const float2 zz = szz[warp][b][i];
             const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
@@ -882,6 +887,13 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
 #pragma unroll
             for (int vb = 0; vb < VB; ++vb)
                 if (vb < nb) pphi[vb] = __fadd2_rn(pphi[vb], __fmul2_rn(sqq[warp][b][vb][i], rinv));
+        };
+        if (K == 1) {  // the common item of one target a lane: a unit stride
+#pragma unroll 2
+            for (int i = 0; i < npairs; ++i) step(i);
+        } else {
+#pragma unroll 2
+            for (int i = kk; i < npairs; i += K) step(i);
         }
 #pragma unroll
         for (int vb = 0; vb < VB; ++vb) {
