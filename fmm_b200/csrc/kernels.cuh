@@ -677,51 +677,6 @@ __device__ __forceinline__ void m2p_eval_mv(const float* M, int nb, float x, flo
     }
 }
 
-template <int P, int VB>
-__global__ void __launch_bounds__(128) leaf_far_mv_kernel(DevPlan plan, int64_t leaf0, int mode, int m,
-                                                          const float4* __restrict__ tpos, const float* __restrict__ M,
-                                                          const float* __restrict__ Lc, double* __restrict__ far_phi) {
-    constexpr int MS = ms_of(P);
-    const int64_t leaf = leaf0 + blockIdx.x;
-    const int box = plan.leaf_box[leaf];
-    const int64_t t0 = plan.tgt_start[leaf], t1 = plan.tgt_start[leaf + 1];
-    if (t1 == t0) return;
-    const int64_t w0 = plan.w_row[leaf], w1 = (mode & 2) ? plan.w_row[leaf + 1] : plan.w_row[leaf];
-    const int64_t nt = plan.ntgt;
-    for (int v0 = 0; v0 < m; v0 += VB) {
-        const int nb = (m - v0) < VB ? (m - v0) : VB;
-        for (int64_t tb = t0; tb < t1; tb += blockDim.x) {
-            const int64_t t = tb + threadIdx.x;
-            if (t >= t1) continue;
-            const float4 p4 = tpos[t];
-            const float ux = p4.x, uy = p4.y, uz = p4.z;
-            double fphi[VB];
-#pragma unroll
-            for (int b = 0; b < VB; ++b) fphi[b] = (b < nb && (mode & 4)) ? far_phi[(int64_t)(v0 + b) * nt + t] : 0.0;
-            if (mode & 1) {
-                float ph[VB];
-                l2p_eval_mv<P, VB>(Lc + ((int64_t)box * m + v0) * MS, nb, ux, uy, uz, ph);
-#pragma unroll
-                for (int b = 0; b < VB; ++b) fphi[b] = (mode & 4) ? fphi[b] + (double)ph[b] : (double)ph[b];
-            }
-            for (int64_t e = w0; e < w1; ++e) {
-                const int s = plan.w_col[e];
-                float c[3], r;
-                rel_frame<float>(plan, s, box, c, r);
-                const float rinv = 1.0f / r;
-                float ph[VB];
-                m2p_eval_mv<P, VB>(M + ((int64_t)s * m + v0) * MS, nb, (ux - c[0]) * rinv, (uy - c[1]) * rinv,
-                                   (uz - c[2]) * rinv, ph);
-#pragma unroll
-                for (int b = 0; b < VB; ++b) fphi[b] += (double)(ph[b] * rinv);
-            }
-#pragma unroll
-            for (int b = 0; b < VB; ++b)
-                if (b < nb) far_phi[(int64_t)(v0 + b) * nt + t] = fphi[b];
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------------
 // P2P + output pass.  One warp per work item = up to 32 targets of one leaf (lane =
 // target); the warp walks the leaf's near row (source leaves by leaf index) and stages
@@ -772,10 +727,11 @@ struct P2pItems {
 
 // L2P + M2P of the f32 form over P2P work items: a warp per item (up to 32 targets of one
 // leaf, lane = target), any number of warps a block.  Each target sums the terms of
-// leaf_far_kernel<P, float, GRAD> / leaf_far_mv_kernel<P, VB> in the same order (the
-// compiler may contract products into fmas differently, so the last bits can differ);
-// what changes is the occupancy: a block per leaf holds every thread of its block while a
-// leaf of few targets keeps one warp busy, a warp per item leaves no idle warp resident.
+// leaf_far_kernel<P, float, GRAD> in the same order (the compiler may contract products
+// into fmas differently, so the last bits can differ); what changes is the occupancy: a
+// block per leaf holds every thread of its block while a leaf of few targets keeps one
+// warp busy, a warp per item leaves no idle warp resident.  leaf_far_mv_items_kernel forms
+// each target's harmonics once for up to VB vectors (l2p_eval_mv / m2p_eval_mv).
 // The gradient form is held to 96 registers (21 warps an SM, no spills).
 template <int P, bool GRAD>
 __global__ void __launch_bounds__(128, 5) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
