@@ -506,9 +506,20 @@ struct Evaluator final : EvaluatorBase {
             nullptr, ck_pair_src.as<int32_t>() + c.base, m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
     }
     void reduce_chunk(const Chunk& c, int with_l2l, int with_v, int accumulate) {
-        if (c.b1 > c.b0)
-            local_reduce_kernel<P, T><<<counted((unsigned)(c.b1 - c.b0)), round32(NC), 0, stream>>>(
-                dp, c.b0, c.b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
+        reduce_range(c.b0, c.b1, with_l2l, with_v, accumulate);
+    }
+
+    // the local reduce of boxes [b0, b1): f32 a warp per box with 16-byte accesses, f64 a
+    // block per box (the same order of additions either way)
+    void reduce_range(int64_t b0, int64_t b1, int with_l2l, int with_v, int accumulate) {
+        if (b1 <= b0) return;
+        if constexpr (kMixed)
+            local_reduce4_kernel<P><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
+                dp, b0, b1, m, with_l2l, with_v, accumulate, reinterpret_cast<const float*>(Yo.ptr),
+                reinterpret_cast<const float*>(Y.ptr), v_pos.as<int64_t>(), reinterpret_cast<float*>(Lc.ptr));
+        else
+            local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
+                dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
                 Lc.as<T>());
     }
 
@@ -1183,11 +1194,7 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void reduce_locals(int l, int with_l2l, int with_v, int accumulate) {
-        const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
-        if (b1 > b0)
-            local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
-                dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
-                Lc.as<T>());
+        reduce_range(plan.level_start[l], plan.level_start[l + 1], with_l2l, with_v, accumulate);
     }
 
     void p2l_level(int l) {  // the boxes of level l with an X list

@@ -358,6 +358,67 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
         }
 }
 
+// The same reduce for f32 expansions with 16-byte accesses: a warp per box (4 a block),
+// lane q holding coefficients 4q .. 4q + 3; every coefficient adds the same terms in the
+// same order as local_reduce_kernel, so the floats are that kernel's.  Rows are 16-byte
+// aligned (ys_of and ms_of are multiples of 4 floats); the last quad's padding is read,
+// never written.  Four blocks an SM in the launch bound leave room for the eight 16-byte
+// rows in flight (96 registers; the compiler's own choice, 32-34, spilled or held fewer).
+__device__ __forceinline__ void add4(float4& s, const float4 y) {
+    s.x += y.x;
+    s.y += y.y;
+    s.z += y.z;
+    s.w += y.w;
+}
+
+template <int P>
+__global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
+                                                            int with_l2l, int with_v, int accumulate,
+                                                            const float* __restrict__ Yo, const float* __restrict__ Yv,
+                                                            const int64_t* __restrict__ vpos, float* __restrict__ Lc) {
+    constexpr int NC = nc_of(P), YS = ys_of(P), MS = ms_of(P), NQ = (NC + 3) / 4;
+    static_assert(YS % 4 == 0 && MS % 4 == 0 && 4 * NQ <= MS && NQ <= 32, "row layout");
+    const int64_t b = b0 + (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int q = threadIdx.x & 31;
+    if (b >= b1 || q >= NQ || plan.tgt_below[b] == 0) return;
+    const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
+    for (int v = 0; v < m; ++v) {
+        float4* out = reinterpret_cast<float4*>(Lc + (b * m + v) * MS) + q;
+        float4 s = accumulate ? *out : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (with_l2l) {
+            const float4 y = reinterpret_cast<const float4*>(Yo + (b * m + v) * YS)[q];
+            if (accumulate)
+                add4(s, y);
+            else
+                s = y;
+        }
+        int64_t e = e0;
+        for (; e + 8 <= e1; e += 8) {  // eight rows in flight, added in row order
+            float4 y[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) add4(s, y[j]);
+        }
+        for (; e + 4 <= e1; e += 4) {
+            float4 y[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) add4(s, y[j]);
+        }
+        for (; e < e1; ++e) add4(s, __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e] * m + v) * YS) + q));
+        if (4 * q + 3 < NC) {
+            *out = s;
+        } else {  // the last quad: its coefficients below NC only (NC - 4q of them, 1 to 3)
+            float* o = reinterpret_cast<float*>(out);
+            o[0] = s.x;
+            if (4 * q + 1 < NC) o[1] = s.y;
+            if (4 * q + 2 < NC) o[2] = s.z;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------
 // Dense M2L as batched GEMM, SIMT form (f64 path): the V pairs of every level are
 // grouped by offset index d (fmm-kernels/src/translate.rs:61-74 batches them the same
