@@ -877,7 +877,7 @@ struct Evaluator final : EvaluatorBase {
         const size_t wd = gradients ? 4 : 1;  // doubles a pair / a target and vector
         close_w.alloc(sizeof(double) * wd * (size_t)(nclose + 1));
         close_acc.alloc(sizeof(double) * wd * (size_t)m * (dp.ntgt + 1));
-        close.acc = close_acc.as<double>();
+        close.acc = nclose ? close_acc.as<double>() : nullptr;  // no pairs: nothing to add
         if (plan.nleaves() && nclose) {
             const auto* s32 = reinterpret_cast<const float4*>(spos.ptr);
             const auto* t32 = reinterpret_cast<const float4*>(tpos.ptr);

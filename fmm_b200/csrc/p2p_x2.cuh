@@ -132,10 +132,12 @@ __global__ void close_sum_kernel(ClosePairs close, const double* __restrict__ w,
     }
 }
 
-// The P2P epilogue's addition of a target's near-singular sum (entry vt = v nt + t).
+// The P2P epilogue's addition of a target's near-singular sum (entry vt = v nt + t); no
+// sums (acc null) when the plan has no near-singular pair.
 template <bool GRAD>
 __device__ __forceinline__ void close_sum_add(const ClosePairs& close, int64_t vt, double& aphi, double& ag0,
                                               double& ag1, double& ag2) {
+    if (!close.acc) return;
     if (GRAD) {
         const double4 c = reinterpret_cast<const double4*>(close.acc)[vt];
         aphi += c.x;
@@ -147,7 +149,7 @@ __device__ __forceinline__ void close_sum_add(const ClosePairs& close, int64_t v
     }
 }
 __device__ __forceinline__ void close_sum_add1(const ClosePairs& close, int64_t vt, double& aphi) {
-    aphi += close.acc[vt];
+    if (close.acc) aphi += close.acc[vt];
 }
 
 constexpr int kX2Warps = 4;      // warps a block until the autotuner chooses

@@ -99,3 +99,20 @@ def test_p2p_path_hook_rejects_unbuilt_forms():
         fmm.set_p2p_path(2)
     fmm.set_p2p_path(0)
     fmm.close()
+
+
+def test_plan_without_near_singular_pairs(oracle):
+    """Targets apart from every source (no near-singular pair, no near pair at all): the
+    P2P adds no near-singular sums, on either path, and the result is the far field."""
+    rng = np.random.default_rng(26)
+    xs = rng.uniform(0.0, 1.0, (5000, 3))
+    xt = rng.uniform(1.5, 2.5, (3000, 3))
+    q = rng.standard_normal(5000)
+    fmm = F.FmmBuilder(6).gradients().max_points_per_leaf(32).precision("mixed").build(xs, xt)
+    assert fmm.info()["close_pairs"] == 0
+    s, p, _ = _both(fmm, q)
+    assert np.array_equal(s.potential, p.potential) and np.array_equal(s.gradient, p.gradient)
+    phi, g = oracle.fmm(xs, q, xt, 6, 32, gradients=True, threads=8)
+    assert np.linalg.norm(s.potential[0] - phi[0]) / np.linalg.norm(phi[0]) < 2e-6
+    assert np.linalg.norm(s.gradient[0] - g[0]) / np.linalg.norm(g[0]) < 2e-6
+    fmm.close()
