@@ -1296,11 +1296,11 @@ struct Evaluator final : EvaluatorBase {
         } else {
             const unsigned g = (unsigned)((it.count + kP2pWarps - 1) / kP2pWarps);
             if (gradients)
-                p2p_kernel<T, true, kMixed><<<counted(g), 32 * kP2pWarps, 0, s>>>(
+                p2p_kernel<T, true><<<counted(g), 32 * kP2pWarps, 0, s>>>(
                     dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
                     far_phi.as<double>(), fg, accumulate, d_phi, og);
             else
-                p2p_kernel<T, false, kMixed><<<counted(g), 32 * kP2pWarps, 0, s>>>(
+                p2p_kernel<T, false><<<counted(g), 32 * kP2pWarps, 0, s>>>(
                     dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
                     far_phi.as<double>(), fg, accumulate, d_phi, og);
         }

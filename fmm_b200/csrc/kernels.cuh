@@ -744,14 +744,12 @@ __device__ __forceinline__ void m2p_eval_mv(const float* M, int nb, float x, flo
 // each source leaf's points in its own shared memory, mapped to the target leaf's
 // frame: y = fma(r, u_s, c) (CONVENTIONS 3.13 "Device kernels", rule 1), the leaf
 // itself unchanged.  Per pair d = u_t - y, r2 by explicit fma (rules 2-3), and the
-// pair is skipped by a select before rho meets a charge (rule 4).
-//   f64 (plain): skipped iff r2 == 0, the coincidence rule of the reference.
-//   f32 (mixed): skipped iff r2 < theta2; those near-singular pairs (found once at
-//   build time with the same arithmetic, pair_r2 below) are added in f64 from the f64
-//   coordinates at the end, with the f64 coincidence rule.
-// The f32 partial of one source leaf is added into an f64 accumulator per target.  The
-// sum is then added to the far-field partial and scaled once, phi = phi_hat/(4 pi r_t)
-// and g = g_hat/((4 pi r_t) r_t) (fmm-exec/src/fmm.rs:4750-4778), in caller order.
+// pair is skipped by a select before rho meets a charge (rule 4): iff r2 == 0, the
+// coincidence rule of the reference.  This is the plain f64 kernel; the mixed form's
+// P2P is in p2p_x2.cuh (its near-singular pairs found by close_pairs_kernel below, whose
+// f32 r2 is formed with pair_r2).  The per-target sum is added to the far-field partial
+// and scaled once, phi = phi_hat/(4 pi r_t) and g = g_hat/((4 pi r_t) r_t)
+// (fmm-exec/src/fmm.rs:4750-4778), in caller order.
 // ---------------------------------------------------------------------------------
 constexpr int kP2pWarps = 4;
 constexpr int kP2pStage = 64;
@@ -931,7 +929,7 @@ __global__ void close_map_kernel(DevPlan plan, ClosePairs close, double4* __rest
         }
 }
 
-template <typename T, bool GRAD, bool CLOSE>
+template <typename T, bool GRAD>
 __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, int m, int near, T theta2,
                                                   const typename Vec4<T>::type* __restrict__ spos,
                                                   const T* __restrict__ sq,
@@ -987,7 +985,7 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
                     const T4 y = stage[warp][s];
                     const T dx = sub_rn<T>(tx, y.x), dy = sub_rn<T>(ty, y.y), dz = sub_rn<T>(tz, y.z);
                     const T r2 = pair_r2<T>(dx, dy, dz);
-                    const bool skip = CLOSE ? (r2 < theta2) : (r2 == T(0));
+                    const bool skip = r2 == T(0);
                     const T rinv = skip ? T(0) : rsqrt(r2);
                     const T qr = y.w * rinv;
                     pphi += qr;
@@ -1008,32 +1006,6 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
             }
         }
         if (!valid) continue;
-        if (CLOSE && near) {
-            // near-singular pairs in f64: the f64 map and the reference's coincidence rule
-            const double4 u = close.tpos[t];
-            for (int64_t c2 = close.row[t]; c2 < close.row[t + 1]; ++c2) {
-                const int64_t sp = close.src[c2];
-                const int sl = close.leaf[c2];
-                double cc[3] = {0.0, 0.0, 0.0}, rr = 1.0;
-                if (sl != leaf) rel_frame<double>(plan, plan.leaf_box[sl], box, cc, rr);
-                const double4 ps = close.spos[sp];
-                const double yx = sl != leaf ? __fma_rn(rr, ps.x, cc[0]) : ps.x;
-                const double yy = sl != leaf ? __fma_rn(rr, ps.y, cc[1]) : ps.y;
-                const double yz = sl != leaf ? __fma_rn(rr, ps.z, cc[2]) : ps.z;
-                if (u.x == yx && u.y == yy && u.z == yz) continue;
-                const double dx = u.x - yx, dy = u.y - yy, dz = u.z - yz;
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                const double rinv = rsqrt(r2);
-                const double qr = close.q[(int64_t)v * plan.nsrc + sp] * rinv;
-                aphi += qr;
-                if (GRAD) {
-                    const double qr3 = qr * rinv * rinv;
-                    ag0 -= qr3 * dx;
-                    ag1 -= qr3 * dy;
-                    ag2 -= qr3 * dz;
-                }
-            }
-        }
         if (accumulate == 2) {  // near field alone, leaf order (added to the far field by output_kernel)
             out_phi[(int64_t)v * nt + t] = aphi;
             if (GRAD) {
