@@ -68,6 +68,15 @@ def lib():
                                                 C.c_void_p]),
             "orc_helmholtz_near": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_double, C.c_double,
                                              C.c_int, C.c_int, _dp, C.c_void_p]),
+            "orc_hh_harmonics": (None, [C.c_int, _dp, _dp, C.c_void_p, C.c_void_p]),
+            "orc_hh_radial": (None, [C.c_int, C.c_double, C.c_double, _dp, C.c_void_p, C.c_void_p, C.c_void_p]),
+            "orc_hh_p2m": (None, [C.c_int, C.c_double, C.c_double, _dp, _sz, _dp, _dp, _dp]),
+            "orc_hh_p2l": (None, [C.c_int, C.c_double, C.c_double, _dp, _sz, _dp, _dp, _dp]),
+            "orc_hh_l2p": (None, [C.c_int, C.c_double, C.c_double, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_hh_m2p": (None, [C.c_int, C.c_double, C.c_double, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_hh_m2m": (None, [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp, _dp, _dp]),
+            "orc_hh_l2l": (None, [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp, _dp, _dp]),
+            "orc_hh_m2l": (None, [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -156,6 +165,73 @@ def direct_sum(src, q, tgt, gradients=True, threads=True):
 
 def _cview(a):
     return np.ascontiguousarray(a, dtype=np.complex128).view(np.float64)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+# ---- Helmholtz expansions for a real k (helmholtz_ops.c) --------------------------------
+# A complex expansion of degree p is returned as a complex array of (p + 1)^2 in the layout
+# n^2 + n + m (the C side's two real planes); a box is its centre and half-width r.
+
+def hh_harmonics(p, x, derivatives=False):
+    """Real orthonormal Y_n^m of x's direction (and d_theta Y, (1/sin theta) d_phi Y)."""
+    n = (p + 1) ** 2
+    y = np.zeros(n)
+    dt = np.zeros(n) if derivatives else None
+    df = np.zeros(n) if derivatives else None
+    lib().orc_hh_harmonics(p, np.ascontiguousarray(x, dtype=np.float64), y, _ptr(dt), _ptr(df))
+    return (y, dt, df) if derivatives else y
+
+
+def hh_radial(p, z, s=1.0, singular=True):
+    """Scaled jh_n, jh_n' (and hh_n, hh_n' complex) at z, n = 0..p."""
+    jh, jhp = np.zeros(p + 1), np.zeros(p + 1)
+    hh = np.zeros(2 * (p + 1)) if singular else None
+    hhp = np.zeros(2 * (p + 1)) if singular else None
+    lib().orc_hh_radial(p, float(z), float(s), jh, _ptr(jhp), _ptr(hh), _ptr(hhp))
+    if not singular:
+        return jh, jhp
+    return jh, jhp, hh.view(np.complex128), hhp.view(np.complex128)
+
+
+def _planes(e):
+    e = np.asarray(e, dtype=np.complex128)
+    return np.ascontiguousarray(np.concatenate([e.real, e.imag]))
+
+
+def _complex(planes):
+    n = len(planes) // 2
+    return planes[:n] + 1j * planes[n:]
+
+
+def hh_p2m(p, k, r, c, src, q, singular=False):
+    """P2M (or P2L with singular=True) of complex charges about centre c."""
+    out = np.zeros(2 * (p + 1) ** 2)
+    f = lib().orc_hh_p2l if singular else lib().orc_hh_p2m
+    f(p, float(k), float(r), np.ascontiguousarray(c, dtype=np.float64), len(src),
+      np.ascontiguousarray(src, dtype=np.float64), _cview(q), out)
+    return _complex(out)
+
+
+def hh_eval(p, k, r, c, e, tgt, singular):
+    """L2P (singular=False) or M2P: phi (nt,) and grad (nt, 3) complex."""
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    phi = np.zeros(2 * len(tgt))
+    g = np.zeros(6 * len(tgt))
+    f = lib().orc_hh_m2p if singular else lib().orc_hh_l2p
+    f(p, float(k), float(r), np.ascontiguousarray(c, dtype=np.float64), _planes(e), len(tgt), tgt, phi, _ptr(g))
+    return phi.view(np.complex128), g.view(np.complex128).reshape(len(tgt), 3)
+
+
+def hh_translate(kind, p_in, p_out, k, r_in, c_in, r_out, c_out, e):
+    """M2M, L2L or M2L by projection: the output expansion (complex, (p_out + 1)^2)."""
+    out = np.zeros(2 * (p_out + 1) ** 2)
+    f = {"m2m": lib().orc_hh_m2m, "l2l": lib().orc_hh_l2l, "m2l": lib().orc_hh_m2l}[kind]
+    f(p_in, p_out, float(k), float(r_in), np.ascontiguousarray(c_in, dtype=np.float64), float(r_out),
+      np.ascontiguousarray(c_out, dtype=np.float64), _planes(e), out)
+    return _complex(out)
 
 
 def helmholtz_p2p(k, src, q, tgt, gradients=True):
