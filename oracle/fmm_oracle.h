@@ -131,7 +131,6 @@ void orc_helmholtz_p2p(double kre, double kim, size_t ns, const double *src, con
                        const double *tgt, double *potential, double *gradient);
 void orc_helmholtz_direct_sum(double kre, double kim, size_t ns, const double *src, const double *q, size_t nt,
                               const double *tgt, double *potential, double *gradient);
-/* the Helmholtz near field on the plan (fmm.c), with 1/(4 pi) */
 /* Helmholtz expansions for a real k (helmholtz_ops.c): complex expansions are two real
  * planes of (p + 1)^2 (real parts, then imaginary parts) in the layout n^2 + n + m; a box
  * is its centre and half-width r; phi and grad as orc_helmholtz_p2p (e^{ikr}/r sums). */
@@ -151,6 +150,7 @@ void orc_hh_l2l(int p_in, int p_out, double k, double r_in, const double *c_in, 
                 const double *L_in, double *L_out);
 void orc_hh_m2l(int p_in, int p_out, double k, double r_in, const double *c_in, double r_out, const double *c_out,
                 const double *M_in, double *L_out);
+/* the Helmholtz near field on the plan (fmm.c), with 1/(4 pi) */
 int orc_helmholtz_near(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
                        int max_keys, double kre, double kim, int gradients, int threads, double *phi,
                        double *grad);
