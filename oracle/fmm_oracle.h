@@ -150,6 +150,10 @@ void orc_hh_l2l(int p_in, int p_out, double k, double r_in, const double *c_in, 
                 const double *L_in, double *L_out);
 void orc_hh_m2l(int p_in, int p_out, double k, double r_in, const double *c_in, double r_out, const double *c_out,
                 const double *M_in, double *L_out);
+/* the dense M2L of offset (dx, dy, dz) on a level of half-width r: a real 2n x n matrix,
+ * column-major, column j the local (real plane over imaginary plane) of the unit real
+ * multipole e_j (n = (p + 1)^2) */
+void orc_hh_m2l_dense(int p, double k, double r, int dx, int dy, int dz, double *table);
 /* the Helmholtz near field on the plan (fmm.c), with 1/(4 pi) */
 int orc_helmholtz_near(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
                        int max_keys, double kre, double kim, int gradients, int threads, double *phi,

@@ -432,3 +432,104 @@ void orc_hh_m2l(int p_in, int p_out, double k, double r_in, const double *c_in, 
                 const double *M_in, double *L_out) {
     project(p_in, k, r_in, c_in, M_in, 1, p_out, r_out, c_out, 0, L_out);
 }
+
+/* ---- dense M2L tables by projection -------------------------------------------------- */
+
+/* The M2L of one V-list offset on one level as one real 2n x n matrix (n = (p+1)^2),
+ * column-major, the layout of fmm-tables/src/helmholtz/dense.rs:5-14: column j is the
+ * local (real plane in rows 0..n, imaginary plane in rows n..2n) about the box at
+ * 2r (dx, dy, dz) of the unit real multipole e_j about the box at the origin, both of
+ * half-width r.  Each column is orc_hh_m2l of e_j (the same projection and quadrature);
+ * the phi sums of a ring of nodes are taken per order first, so a table costs
+ * O(Q^2 n p) instead of n projections. */
+void orc_hh_m2l_dense(int p, double k, double r, int dx, int dy, int dz, double *table) {
+    const int n = (p + 1) * (p + 1);
+    const double rho = sqrt(3.0) * r, s = level_scale(k, r);
+    const double cout[3] = {2.0 * r * dx, 2.0 * r * dy, 2.0 * r * dz};
+    const int Q = 2 * p + (int)ceil(k * rho) + 40, NP = 2 * Q;
+    double *gx = malloc(sizeof(double) * Q), *gw = malloc(sizeof(double) * Q);
+    gauss_legendre(Q, gx, gw);
+    /* per ring: F[j][m] = sum_l w_l field_j(node l) trig_m(phi_l), m = -p..p (A and B) */
+    const int nm = 2 * p + 1;
+    double *FA = malloc(sizeof(double) * 2 * (size_t)n * nm), *FB = malloc(sizeof(double) * 2 * (size_t)n * nm);
+    double *A = calloc(2 * (size_t)n * n, sizeof(double)), *B = calloc(2 * (size_t)n * n, sizeof(double));
+    double Y[(HMAX + 1) * (HMAX + 1)], Dt[(HMAX + 1) * (HMAX + 1)], Df[(HMAX + 1) * (HMAX + 1)], Yo[(HMAX + 1) * (HMAX + 1)];
+    double jh[HMAX + 1], jhp[HMAX + 1], hh[2 * (HMAX + 1)], hhp[2 * (HMAX + 1)];
+    double *fj = malloc(sizeof(double) * 2 * (size_t)n), *bj = malloc(sizeof(double) * 2 * (size_t)n);
+    for (int i = 0; i < Q; ++i) {
+        const double ct = gx[i], st = sqrt(1.0 - ct * ct);
+        memset(FA, 0, sizeof(double) * 2 * (size_t)n * nm);
+        memset(FB, 0, sizeof(double) * 2 * (size_t)n * nm);
+        for (int l = 0; l < NP; ++l) {
+            const double f = 2.0 * kPi * l / NP, wl = 2.0 * kPi / NP;
+            const double u[3] = {st * cos(f), st * sin(f), ct};
+            const double v[3] = {cout[0] + rho * u[0], cout[1] + rho * u[1], cout[2] + rho * u[2]};
+            const double d = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            orc_hh_harmonics(p, v, Y, Dt, Df);
+            orc_hh_radial(p, k * d, s, jh, jhp, hh, hhp);
+            /* spherical unit vectors of v */
+            const double rr = sqrt(v[0] * v[0] + v[1] * v[1]);
+            const double c2 = v[2] / d, s2 = rr / d, cf = rr > 0.0 ? v[0] / rr : 1.0, sf = rr > 0.0 ? v[1] / rr : 0.0;
+            const double er[3] = {s2 * cf, s2 * sf, c2}, et[3] = {c2 * cf, c2 * sf, -s2}, ef[3] = {-sf, cf, 0.0};
+            const double uer = u[0] * er[0] + u[1] * er[1] + u[2] * er[2];
+            const double uet = u[0] * et[0] + u[1] * et[1] + u[2] * et[2];
+            const double uef = u[0] * ef[0] + u[1] * ef[1] + u[2] * ef[2];
+            /* the unit multipole's field and rho d_rho of it: 4 pi i k times
+             * hh Y and rho (k hh' Y u.er + (hh / d)(Dt u.et + Df u.ef)) */
+            for (int dn = 0; dn <= p; ++dn)
+                for (int m = -dn; m <= dn; ++m) {
+                    const int j = HIDX(dn, m);
+                    const double h0 = hh[2 * dn], h1 = hh[2 * dn + 1];
+                    const double rad = k * uer * Y[j], tan = (uet * Dt[j] + uef * Df[j]) / d;
+                    const double vr = h0 * Y[j], vi = h1 * Y[j];
+                    const double br = rho * (rad * hhp[2 * dn] + tan * h0), bi = rho * (rad * hhp[2 * dn + 1] + tan * h1);
+                    fj[2 * j] = -4.0 * kPi * k * vi; /* times i */
+                    fj[2 * j + 1] = 4.0 * kPi * k * vr;
+                    bj[2 * j] = -4.0 * kPi * k * bi;
+                    bj[2 * j + 1] = 4.0 * kPi * k * br;
+                }
+            for (int m = -p; m <= p; ++m) {
+                const double tr = wl * (m >= 0 ? cos(m * f) : sin(-m * f));
+                double *fa = FA + 2 * (size_t)n * (m + p), *fb = FB + 2 * (size_t)n * (m + p);
+                for (int j = 0; j < 2 * n; ++j) {
+                    fa[j] += tr * fj[j];
+                    fb[j] += tr * bj[j];
+                }
+            }
+        }
+        /* the output harmonics at this ring: Y_t(t_i, phi) = Yo_t(phi = 0 part) trig(m phi) */
+        const double ud[3] = {st, 0.0, ct};
+        orc_hh_harmonics(p, ud, Yo, NULL, NULL); /* at phi = 0: cos part = N Pb, sin part 0 */
+        for (int tn = 0; tn <= p; ++tn)
+            for (int tm = -tn; tm <= tn; ++tm) {
+                const int t = HIDX(tn, tm);
+                const double yt = gw[i] * Yo[HIDX(tn, tm < 0 ? -tm : tm)]; /* N Pb_n^|m| */
+                const double *fa = FA + 2 * (size_t)n * (tm + p), *fb = FB + 2 * (size_t)n * (tm + p);
+                for (int j = 0; j < n; ++j) {
+                    A[2 * ((size_t)j * n + t)] += yt * fa[2 * j];
+                    A[2 * ((size_t)j * n + t) + 1] += yt * fa[2 * j + 1];
+                    B[2 * ((size_t)j * n + t)] += yt * fb[2 * j];
+                    B[2 * ((size_t)j * n + t) + 1] += yt * fb[2 * j + 1];
+                }
+            }
+    }
+    orc_hh_radial(p, k * rho, s, jh, jhp, NULL, NULL);
+    for (int j = 0; j < n; ++j)
+        for (int tn = 0; tn <= p; ++tn) {
+            const double fv = jh[tn], gv = rho * k * jhp[tn], den = fv * fv + gv * gv;
+            for (int tm = -tn; tm <= tn; ++tm) {
+                const int t = HIDX(tn, tm);
+                const size_t a = 2 * ((size_t)j * n + t);
+                table[(size_t)j * 2 * n + t] = (fv * A[a] + gv * B[a]) / den;
+                table[(size_t)j * 2 * n + n + t] = (fv * A[a + 1] + gv * B[a + 1]) / den;
+            }
+        }
+    free(gx);
+    free(gw);
+    free(FA);
+    free(FB);
+    free(A);
+    free(B);
+    free(fj);
+    free(bj);
+}

@@ -77,6 +77,7 @@ def lib():
             "orc_hh_m2m": (None, [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp, _dp, _dp]),
             "orc_hh_l2l": (None, [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp, _dp, _dp]),
             "orc_hh_m2l": (None, [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp, _dp, _dp]),
+            "orc_hh_m2l_dense": (None, [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -232,6 +233,22 @@ def hh_translate(kind, p_in, p_out, k, r_in, c_in, r_out, c_out, e):
     f(p_in, p_out, float(k), float(r_in), np.ascontiguousarray(c_in, dtype=np.float64), float(r_out),
       np.ascontiguousarray(c_out, dtype=np.float64), _planes(e), out)
     return _complex(out)
+
+
+def hh_m2l_dense(p, k, r, offset):
+    """The dense M2L table of one offset (fmm-tables/src/helmholtz/dense.rs layout):
+    a real (2n, n) matrix whose column j is the local of the unit real multipole e_j."""
+    n = (p + 1) ** 2
+    t = np.zeros(2 * n * n)
+    lib().orc_hh_m2l_dense(p, float(k), float(r), int(offset[0]), int(offset[1]), int(offset[2]), t)
+    return t.reshape(n, 2 * n).T  # column-major storage -> (2n, n)
+
+
+def hh_apply_dense(table, m):
+    """A complex multipole through a dense table: (A_r + i A_i)(M_r + i M_i)."""
+    n = table.shape[1]
+    a = table[:n] + 1j * table[n:]
+    return a @ np.asarray(m, dtype=np.complex128)
 
 
 def helmholtz_p2p(k, src, q, tgt, gradients=True):

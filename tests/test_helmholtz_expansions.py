@@ -155,3 +155,25 @@ def test_m2l_between_boxes_of_one_level(k, p, tol):
     phi, g = O.hh_eval(p, k, 0.5, ct, L, tgt, singular=False)
     ex, eg = O.helmholtz_direct_sum(k, src, q, tgt)
     assert rel(phi, ex) < tol and rel(g, eg) < tol
+
+
+def test_dense_m2l_table():
+    """The dense M2L of one offset (fmm-tables/src/helmholtz/dense.rs layout: a real 2n x n
+    matrix, column j the local of the unit real multipole e_j, real plane over imaginary
+    plane) equals the projection M2L column by column, and applied to a complex multipole
+    gives the projection's local of it."""
+    p, k, r = 6, 3.0, 0.5
+    n = (p + 1) ** 2
+    off = (2, 1, -1)
+    ct = 2 * r * np.array(off, dtype=float)
+    T = O.hh_m2l_dense(p, k, r, off)
+    assert T.shape == (2 * n, n)
+    for j in (0, 5, n - 1):
+        e = np.zeros(n, dtype=np.complex128)
+        e[j] = 1.0
+        col = O.hh_translate("m2l", p, p, k, r, CENTRE, r, ct, e)
+        assert np.abs(T[:n, j] + 1j * T[n:, j] - col).max() < 1e-12 * np.abs(col).max()
+    rng, src, q = _problem(16)
+    M = O.hh_p2m(p, k, r, CENTRE, src, q)
+    L = O.hh_translate("m2l", p, p, k, r, CENTRE, r, ct, M)
+    assert np.abs(O.hh_apply_dense(T, M) - L).max() < 1e-12 * np.abs(L).max()
