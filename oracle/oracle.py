@@ -59,6 +59,10 @@ def lib():
             "orc_tree_nleaves": (_sz, [C.c_void_p]),
             "orc_tree_boxes": (None, [C.c_void_p, _u64p, _u8p]),
             "orc_tree_list": (_sz, [C.c_void_p, _sz, C.c_int, _u64p, _sz]),
+            "orc_tree_domain": (None, [C.c_void_p, _dp, C.POINTER(C.c_double)]),
+            "orc_domain": (None, [_sz, _dp, _sz, _dp, _dp, C.POINTER(C.c_double), _dp]),
+            "orc_point_key": (C.c_uint64, [_dp, _dp, C.c_int]),
+            "orc_key_decode": (None, [C.c_uint64, C.POINTER(C.c_int), _u32p]),
             "orc_fmm": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
                                   C.c_int, _dp, C.c_void_p]),
             "orc_fmm_kinds": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
@@ -168,10 +172,6 @@ def _cview(a):
     return np.ascontiguousarray(a, dtype=np.complex128).view(np.float64)
 
 
-def _ptr(a):
-    return a.ctypes.data_as(C.c_void_p) if a is not None else None
-
-
 # ---- Helmholtz expansions for a real k (helmholtz_ops.c) --------------------------------
 # A complex expansion of degree p is returned as a complex array of (p + 1)^2 in the layout
 # n^2 + n + m (the C side's two real planes); a box is its centre and half-width r.
@@ -249,6 +249,121 @@ def hh_apply_dense(table, m):
     n = table.shape[1]
     a = table[:n] + 1j * table[n:]
     return a @ np.asarray(m, dtype=np.complex128)
+
+
+_DEEPEST = 16  # the tree's finest key level (fmm.c DEEPEST)
+
+
+def _decode(key):
+    lvl = C.c_int()
+    idx = np.zeros(3, dtype=np.uint32)
+    lib().orc_key_decode(int(key), C.byref(lvl), idx)
+    return lvl.value, idx.astype(np.int64)
+
+
+def helmholtz_fmm(src, q, tgt, k, p, max_keys):
+    """A Helmholtz FMM for a real k on the oracle's octree and lists (the Laplace plan's
+    tree, U/V/W/X lists and pass order, fmm-plan/src/evaluator.rs:368-440), with the
+    expansions of helmholtz_ops.c in absolute units: P2M; M2M and L2L by projection;
+    M2L from the dense tables of each level and offset (fmm-tables/src/helmholtz/dense.rs
+    layout, built by projection); P2L over X lists; L2P; M2P over W lists; P2P over the
+    near lists.  Degree p on every level.  Returns phi (nt,) and grad (nt, 3), complex, the
+    sums of q e^{ikr}/r (no 1/(4 pi)), in caller order."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    q = np.asarray(q, dtype=np.complex128)
+    T = Tree(src, tgt, _DEEPEST, max_keys)
+    L = lib()
+    lower, side = np.zeros(3), C.c_double()
+    L.orc_tree_domain(T._t, lower, C.byref(side))
+    side = side.value
+    box6, lw, sd = np.zeros(6), np.zeros(3), C.c_double()
+    L.orc_domain(len(src), src, len(tgt), tgt, lw, C.byref(sd), box6)
+    nb = len(T.keys)
+    index = {int(kk): b for b, kk in enumerate(T.keys)}
+    lv = np.zeros(nb, dtype=np.int64)
+    ix = np.zeros((nb, 3), dtype=np.int64)
+    for b, kk in enumerate(T.keys):
+        lv[b], ix[b] = _decode(kk)
+    r = side / 2.0 ** (lv + 1)
+    centre = lower + (2 * ix + 1) * r[:, None]
+
+    def key(level, idx):
+        return int(L.orc_key_from_index(np.ascontiguousarray(idx, dtype=np.uint32), int(level)))
+
+    def leaf_of(x):
+        _, fi = _decode(L.orc_point_key(np.ascontiguousarray(x), box6, _DEEPEST))
+        for level in range(T.nlevels - 1, -1, -1):
+            b = index.get(key(level, fi >> (_DEEPEST - level)))
+            if b is not None and T.is_leaf[b]:
+                return b
+        raise RuntimeError("a point in no leaf")
+
+    s_leaf = np.array([leaf_of(x) for x in src])
+    t_leaf = np.array([leaf_of(x) for x in tgt])
+    members = lambda arr, b: np.nonzero(arr == b)[0]  # noqa: E731
+    boxes = lambda keys: [index[int(kk)] for kk in keys if int(kk) in index]  # noqa: E731
+    n = (p + 1) ** 2
+    M = np.zeros((nb, n), dtype=np.complex128)
+    Lc = np.zeros((nb, n), dtype=np.complex128)
+    parent = np.full(nb, -1)
+    for b in range(nb):
+        if lv[b] > 0:
+            parent[b] = index[key(lv[b] - 1, ix[b] >> 1)]
+    # upward: P2M at the leaves, M2M level by level
+    for b in range(nb):
+        if T.is_leaf[b]:
+            sb = members(s_leaf, b)
+            if len(sb):
+                M[b] = hh_p2m(p, k, r[b], centre[b], src[sb], q[sb])
+    for level in range(T.nlevels - 1, 0, -1):
+        for b in np.nonzero(lv == level)[0]:
+            if np.any(M[b]):
+                P = parent[b]
+                M[P] += hh_translate("m2m", p, p, k, r[b], centre[b], r[P], centre[P], M[b])
+    # downward: M2L (dense tables), P2L (X lists), L2L
+    tables = {}
+    for level in range(2, T.nlevels):
+        for b in np.nonzero(lv == level)[0]:
+            for s in boxes(T.list(b, 1)):
+                if not np.any(M[s]):
+                    continue
+                off = tuple(int(v) for v in ix[b] - ix[s])
+                if (level, off) not in tables:
+                    tables[(level, off)] = hh_m2l_dense(p, k, r[b], off)
+                Lc[b] += hh_apply_dense(tables[(level, off)], M[s])
+            for s in boxes(T.list(b, 3)):
+                sb = members(s_leaf, s)
+                if len(sb):
+                    Lc[b] += hh_p2m(p, k, r[b], centre[b], src[sb], q[sb], singular=True)
+    for level in range(1, T.nlevels):
+        for b in np.nonzero(lv == level)[0]:
+            P = parent[b]
+            if np.any(Lc[P]):
+                Lc[b] += hh_translate("l2l", p, p, k, r[P], centre[P], r[b], centre[b], Lc[P])
+    # leaves: L2P, M2P (W lists), P2P (the near list and the leaf itself)
+    phi = np.zeros(len(tgt), dtype=np.complex128)
+    grad = np.zeros((len(tgt), 3), dtype=np.complex128)
+    for b in range(nb):
+        if not T.is_leaf[b]:
+            continue
+        tb = members(t_leaf, b)
+        if not len(tb):
+            continue
+        x = tgt[tb]
+        f, g = hh_eval(p, k, r[b], centre[b], Lc[b], x, singular=False)
+        for s in boxes(T.list(b, 2)):
+            if np.any(M[s]):
+                f2, g2 = hh_eval(p, k, r[s], centre[s], M[s], x, singular=True)
+                f, g = f + f2, g + g2
+        near = set(boxes(T.list(b, 0))) | {b}
+        sb = np.concatenate([members(s_leaf, s) for s in sorted(near)])
+        if len(sb):
+            f3, g3 = helmholtz_p2p(k, src[sb], q[sb], x)
+            f, g = f + f3, g + g3
+        phi[tb] = f
+        grad[tb] = g
+    return phi, grad
 
 
 def helmholtz_p2p(k, src, q, tgt, gradients=True):
