@@ -83,6 +83,7 @@ def lib():
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_helmholtz_near": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
+            "fmmgpu_helmholtz_m2l_tables": (C.c_int, [C.c_int, C.c_double, C.c_double, dp]),
             "fmmgpu_op_begin_evaluation": (C.c_int, [vp, dp]),
             "fmmgpu_op_p2m": (C.c_int, [vp, C.c_int]),
             "fmmgpu_op_m2m": (C.c_int, [vp, C.c_int]),
@@ -130,6 +131,16 @@ def direct_sum(sources, charges, targets, gradients=True, device=0):
     g = np.zeros((len(tgt), 3)) if gradients else None
     _check(lib().fmmgpu_direct_sum(len(src), _ptr(src), _ptr(q), len(tgt), _ptr(tgt), _ptr(phi), _ptr(g), device))
     return phi, g
+
+
+def helmholtz_m2l_tables(p, k, half_width):
+    """The dense Helmholtz M2L tables of one level (real k; fmm-tables/src/helmholtz/dense.rs
+    layout): an array (316, 2n, n), offset index order, column j the local of e_j with the
+    real plane over the imaginary plane.  Host only."""
+    n = (p + 1) ** 2
+    t = np.zeros(316 * 2 * n * n)
+    _check(lib().fmmgpu_helmholtz_m2l_tables(int(p), float(k), float(half_width), _ptr(t)))
+    return t.reshape(316, n, 2 * n).transpose(0, 2, 1)  # column-major storage
 
 
 def helmholtz_direct_sum(k, sources, charges, targets, gradients=True, device=0):

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfmm_b200.so")
 
-SOURCES = ["evaluator.cu", "direct.cu", "tree.cpp", "tables.cpp", "forest.cpp"]
+SOURCES = ["evaluator.cu", "direct.cu", "tree.cpp", "tables.cpp", "forest.cpp", "helmholtz_tables.cpp"]
 HEADERS = ["plan.hpp", "kernels.cuh", "harmonics.cuh", "m2l_tc.cuh", "m2l_fused.cuh", "p2p_x2.cuh", "helmholtz.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -2023,6 +2023,17 @@ int fmmgpu_fmm_set_p2p_path(fmmgpu_fmm* f, int path) {
     });
 }
 
+int fmmgpu_helmholtz_m2l_tables(int p, double k, double half_width, double* tables) {
+    return guarded([&] {
+        if (!tables || p < 0 || p > 30 || !(k > 0.0) || !std::isfinite(k) || !(half_width > 0.0) ||
+            !std::isfinite(half_width))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "need 0 <= p <= 30, a finite k > 0 and half-width > 0");
+        std::vector<double> t;
+        build_helmholtz_m2l_tables(p, k, half_width, t);
+        std::copy(t.begin(), t.end(), tables);
+    });
+}
+
 int fmmgpu_fmm_set_kinds(fmmgpu_fmm* f, int kinds) {
     return guarded([&] {
         if (!f || !f->eval || kinds < 1 || kinds > 3) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid kinds");

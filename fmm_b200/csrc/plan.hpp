@@ -95,5 +95,8 @@ int offset_index(int dx, int dy, int dz);
 void build_m2l_tables(int p, std::vector<double>& out);  // 316 matrices
 void build_m2m_tables(int p, std::vector<double>& out);  // 8
 void build_l2l_tables(int p, std::vector<double>& out);  // 8
+// Helmholtz (real k): the dense M2L tables of one level of boxes of half-width r, 316 real
+// 2n x n matrices in offset index order (helmholtz_tables.cpp)
+void build_helmholtz_m2l_tables(int p, double k, double r, std::vector<double>& out);
 
 }  // namespace fmmb

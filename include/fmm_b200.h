@@ -287,6 +287,15 @@ int fmmgpu_helmholtz_direct_sum(double k_re, double k_im, size_t nsources, const
  * (caller order), potential[v*nt + i] and gradient[(v*nt + i)*3 + k] complex (caller
  * order; the gradient when the FMM was built with gradients), with 1/(4 pi).  Host
  * buffers; synchronises.  The Helmholtz far field is not offered. */
+/* The dense M2L tables of one level for a real k > 0 (the reference's DenseM2l,
+ * fmm-tables/src/helmholtz/dense.rs:1-30), built on the host in f64 by projection
+ * (fmm-ref/src/helmholtz/direct.rs): boxes of half-width `half_width` (k in the same
+ * units), degree p <= 30; writes 316 * 2 (p + 1)^4 doubles, per V-list offset d in index
+ * order (target box at 2 half_width d from the source box) a real 2n x n matrix,
+ * column-major, column j the local of the unit real multipole e_j (the real plane in rows
+ * 0..n over the imaginary plane), n = (p + 1)^2.  No device needed. */
+int fmmgpu_helmholtz_m2l_tables(int p, double k, double half_width, double* tables);
+
 int fmmgpu_helmholtz_near(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges, double* potential,
                           double* gradient);
 

@@ -1,0 +1,43 @@
+"""The product's dense Helmholtz M2L tables (host code, fmmgpu_helmholtz_m2l_tables; the
+reference's DenseM2l layout, fmm-tables/src/helmholtz/dense.rs) against the oracle's
+projection, offset by offset, and through an M2L against the direct sum.  No device."""
+import numpy as np
+import pytest
+
+import fmm_b200 as F
+from oracle import oracle as O
+
+# the 316 V-list offsets in index order (max |component| 2 or 3 in [-3, 3]^3)
+OFFSETS = [(x, y, z) for x in range(-3, 4) for y in range(-3, 4) for z in range(-3, 4)
+           if max(abs(x), abs(y), abs(z)) >= 2]
+
+
+@pytest.mark.parametrize("p,k,r", [(4, 3.0, 0.5), (6, 0.4, 0.25)])
+def test_tables_equal_the_oracle_projection(p, k, r):
+    T = F.helmholtz_m2l_tables(p, k, r)
+    n = (p + 1) ** 2
+    assert T.shape == (316, 2 * n, n) and len(OFFSETS) == 316
+    for i in (0, 57, 158, 200, 315):
+        ref = O.hh_m2l_dense(p, k, r, OFFSETS[i])
+        assert np.abs(T[i] - ref).max() < 1e-13 * np.abs(ref).max(), OFFSETS[i]
+
+
+def test_table_m2l_against_the_direct_sum():
+    p, k, r = 8, 3.0, 0.5
+    T = F.helmholtz_m2l_tables(p, k, r)
+    i = OFFSETS.index((3, -3, 2))
+    rng = np.random.default_rng(17)
+    src = rng.uniform(-r, r, (10, 3))
+    q = rng.standard_normal(10) + 1j * rng.standard_normal(10)
+    ct = 2 * r * np.array(OFFSETS[i], dtype=float)
+    tgt = ct + rng.uniform(-r, r, (6, 3))
+    L = O.hh_apply_dense(T[i], O.hh_p2m(p, k, r, np.zeros(3), src, q))
+    phi, _ = O.hh_eval(p, k, r, ct, L, tgt, singular=False)
+    ex, _ = O.helmholtz_direct_sum(k, src, q, tgt)
+    assert np.abs(phi - ex).max() / np.abs(ex).max() < 5e-5  # p = 8 at ratio 0.23: ~6e-6 measured
+
+
+def test_invalid_arguments():
+    for args in ((31, 1.0, 0.5), (4, 0.0, 0.5), (4, 1.0, -1.0), (4, float("inf"), 0.5)):
+        with pytest.raises(F.FmmError):
+            F.helmholtz_m2l_tables(*args)
