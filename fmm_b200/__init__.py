@@ -84,6 +84,7 @@ def lib():
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_helmholtz_near": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
             "fmmgpu_helmholtz_m2l_tables": (C.c_int, [C.c_int, C.c_double, C.c_double, dp]),
+            "fmmgpu_helmholtz_octant_tables": (C.c_int, [C.c_int, C.c_double, C.c_double, dp, dp]),
             "fmmgpu_op_begin_evaluation": (C.c_int, [vp, dp]),
             "fmmgpu_op_p2m": (C.c_int, [vp, C.c_int]),
             "fmmgpu_op_m2m": (C.c_int, [vp, C.c_int]),
@@ -141,6 +142,16 @@ def helmholtz_m2l_tables(p, k, half_width):
     t = np.zeros(316 * 2 * n * n)
     _check(lib().fmmgpu_helmholtz_m2l_tables(int(p), float(k), float(half_width), _ptr(t)))
     return t.reshape(316, n, 2 * n).transpose(0, 2, 1)  # column-major storage
+
+
+def helmholtz_octant_tables(p, k, half_width):
+    """The Helmholtz M2M and L2L tables of a parent level (real k): two arrays (8, 2n, n),
+    octant o's child at the parent centre + half_width/2 (+-1, +-1, +-1) (x from bit 2)."""
+    n = (p + 1) ** 2
+    a = np.zeros(8 * 2 * n * n)
+    b = np.zeros(8 * 2 * n * n)
+    _check(lib().fmmgpu_helmholtz_octant_tables(int(p), float(k), float(half_width), _ptr(a), _ptr(b)))
+    return a.reshape(8, n, 2 * n).transpose(0, 2, 1), b.reshape(8, n, 2 * n).transpose(0, 2, 1)
 
 
 def helmholtz_direct_sum(k, sources, charges, targets, gradients=True, device=0):

@@ -2034,6 +2034,18 @@ int fmmgpu_helmholtz_m2l_tables(int p, double k, double half_width, double* tabl
     });
 }
 
+int fmmgpu_helmholtz_octant_tables(int p, double k, double half_width, double* m2m, double* l2l) {
+    return guarded([&] {
+        if (!m2m || !l2l || p < 0 || p > 30 || !(k > 0.0) || !std::isfinite(k) || !(half_width > 0.0) ||
+            !std::isfinite(half_width))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "need 0 <= p <= 30, a finite k > 0 and half-width > 0");
+        std::vector<double> a, b;
+        build_helmholtz_octant_tables(p, k, half_width, a, b);
+        std::copy(a.begin(), a.end(), m2m);
+        std::copy(b.begin(), b.end(), l2l);
+    });
+}
+
 int fmmgpu_fmm_set_kinds(fmmgpu_fmm* f, int kinds) {
     return guarded([&] {
         if (!f || !f->eval || kinds < 1 || kinds > 3) throw Failure(FMMGPU_INVALID_ARGUMENT, "invalid kinds");

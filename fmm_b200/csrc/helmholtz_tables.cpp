@@ -182,11 +182,15 @@ void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w) {
     }
 }
 
-// One offset's table (2n x n, column-major).
-void dense_m2l(int p, double k, double r, const int d[3], double* table) {
+// One table (2n x n, column-major): column j the output expansion of the unit real input
+// expansion e_j.  Input: a multipole (singular) or local about c_in, boxes of half-width
+// r_in; output: a multipole or local about c_out, half-width r_out, projected on the
+// output's sphere (radius the output's circumradius).
+void dense_translation(int p, double k, bool in_singular, double r_in, const double* c_in, bool out_singular,
+                       double r_out, const double* c_out, double* table) {
     const int n = (p + 1) * (p + 1), nm = 2 * p + 1;
-    const double rho = std::sqrt(3.0) * r, a = rho, s = std::min(k * a, 1.0);
-    const double ct3[3] = {2.0 * r * d[0], 2.0 * r * d[1], 2.0 * r * d[2]};
+    const double rho = std::sqrt(3.0) * r_out;
+    const double s_in = std::min(k * std::sqrt(3.0) * r_in, 1.0), s_out = std::min(k * rho, 1.0);
     const int Q = 2 * p + (int)std::ceil(k * rho) + 40, NP = 2 * Q;
     std::vector<double> gx, gw;
     gauss_legendre(Q, gx, gw);
@@ -200,27 +204,54 @@ void dense_m2l(int p, double k, double r, const int d[3], double* table) {
         for (int l = 0; l < NP; ++l) {
             const double f = 2.0 * kPi * l / NP, wl = 2.0 * kPi / NP;
             const double u[3] = {st * std::cos(f), st * std::sin(f), ct};
-            const double v[3] = {ct3[0] + rho * u[0], ct3[1] + rho * u[1], ct3[2] + rho * u[2]};
+            const double v[3] = {c_out[0] + rho * u[0] - c_in[0], c_out[1] + rho * u[1] - c_in[1],
+                                 c_out[2] + rho * u[2] - c_in[2]};
             const double dv = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
             harmonics(p, v, Y.data(), Dt.data(), Df.data());
-            radial(p, k * dv, s, jh.data(), jhp.data(), hh.data(), hhp.data());
+            radial(p, k * dv, s_in, jh.data(), jhp.data(), in_singular ? hh.data() : nullptr,
+                   in_singular ? hhp.data() : nullptr);
             const double rr = std::sqrt(v[0] * v[0] + v[1] * v[1]);
-            const double c2 = v[2] / dv, s2 = rr / dv, cf = rr > 0.0 ? v[0] / rr : 1.0, sf = rr > 0.0 ? v[1] / rr : 0.0;
+            const double c2 = dv > 0.0 ? v[2] / dv : 1.0, s2 = dv > 0.0 ? rr / dv : 0.0;
+            const double cf = rr > 0.0 ? v[0] / rr : 1.0, sf = rr > 0.0 ? v[1] / rr : 0.0;
             const double uer = u[0] * s2 * cf + u[1] * s2 * sf + u[2] * c2;
             const double uet = u[0] * c2 * cf + u[1] * c2 * sf - u[2] * s2;
             const double uef = -u[0] * sf + u[1] * cf;
-            for (int dn = 0; dn <= p; ++dn)
+            for (int dn = 0; dn <= p; ++dn) {
+                // the radial value R, k R' and R / |v| of degree dn (complex for a multipole)
+                double R[2], Rp[2], Rt[2];
+                if (in_singular) {
+                    R[0] = hh[2 * dn];
+                    R[1] = hh[2 * dn + 1];
+                    Rp[0] = k * hhp[2 * dn];
+                    Rp[1] = k * hhp[2 * dn + 1];
+                    Rt[0] = R[0] / dv;
+                    Rt[1] = R[1] / dv;
+                } else {
+                    R[0] = jh[dn];
+                    R[1] = 0.0;
+                    Rp[0] = k * jhp[dn];
+                    Rp[1] = 0.0;
+                    Rt[0] = dv > 0.0 ? jh[dn] / dv : (dn == 1 ? k / (3.0 * s_in) : 0.0);
+                    Rt[1] = 0.0;
+                }
                 for (int m = -dn; m <= dn; ++m) {
                     const int jj = hidx(dn, m);
-                    const double h0 = hh[2 * dn], h1 = hh[2 * dn + 1];
-                    const double rad = k * uer * Y[jj], tan = (uet * Dt[jj] + uef * Df[jj]) / dv;
-                    const double br = rho * (rad * hhp[2 * dn] + tan * h0), bi = rho * (rad * hhp[2 * dn + 1] + tan * h1);
-                    // times 4 pi i k
-                    fj[2 * jj] = -4.0 * kPi * k * h1 * Y[jj];
-                    fj[2 * jj + 1] = 4.0 * kPi * k * h0 * Y[jj];
-                    bj[2 * jj] = -4.0 * kPi * k * bi;
-                    bj[2 * jj + 1] = 4.0 * kPi * k * br;
+                    const double rad = uer * Y[jj], tan = uet * Dt[jj] + uef * Df[jj];
+                    double fv[2] = {R[0] * Y[jj], R[1] * Y[jj]};
+                    double bv[2] = {rho * (Rp[0] * rad + Rt[0] * tan), rho * (Rp[1] * rad + Rt[1] * tan)};
+                    if (in_singular) {  // times 4 pi i k
+                        const double a0 = fv[0], b0 = bv[0];
+                        fv[0] = -4.0 * kPi * k * fv[1];
+                        fv[1] = 4.0 * kPi * k * a0;
+                        bv[0] = -4.0 * kPi * k * bv[1];
+                        bv[1] = 4.0 * kPi * k * b0;
+                    }
+                    fj[2 * jj] = fv[0];
+                    fj[2 * jj + 1] = fv[1];
+                    bj[2 * jj] = bv[0];
+                    bj[2 * jj + 1] = bv[1];
                 }
+            }
             for (int m = -p; m <= p; ++m) {
                 const double tr = wl * (m >= 0 ? std::cos(m * f) : std::sin(-m * f));
                 double* fa = &FA[2 * (size_t)n * (m + p)];
@@ -248,20 +279,57 @@ void dense_m2l(int p, double k, double r, const int d[3], double* table) {
                 }
             }
     }
-    radial(p, k * rho, s, jh.data(), jhp.data(), nullptr, nullptr);
+    radial(p, k * rho, s_out, jh.data(), jhp.data(), out_singular ? hh.data() : nullptr,
+           out_singular ? hhp.data() : nullptr);
     for (int jj = 0; jj < n; ++jj)
         for (int tn = 0; tn <= p; ++tn) {
-            const double fv = jh[tn], gv = rho * k * jhp[tn], den = fv * fv + gv * gv;
             for (int tm = -tn; tm <= tn; ++tm) {
                 const int t = hidx(tn, tm);
                 const size_t o = 2 * ((size_t)jj * n + t);
-                table[(size_t)jj * 2 * n + t] = (fv * A[o] + gv * B[o]) / den;
-                table[(size_t)jj * 2 * n + n + t] = (fv * A[o + 1] + gv * B[o + 1]) / den;
+                double re, im;
+                if (out_singular) {  // A / (4 pi i k hh_n)
+                    const double dr = -4.0 * kPi * k * hh[2 * tn + 1], di = 4.0 * kPi * k * hh[2 * tn];
+                    const double den = dr * dr + di * di;
+                    re = (A[o] * dr + A[o + 1] * di) / den;
+                    im = (A[o + 1] * dr - A[o] * di) / den;
+                } else {  // (f A + g B) / (f^2 + g^2)
+                    const double fv = jh[tn], gv = rho * k * jhp[tn], den = fv * fv + gv * gv;
+                    re = (fv * A[o] + gv * B[o]) / den;
+                    im = (fv * A[o + 1] + gv * B[o + 1]) / den;
+                }
+                table[(size_t)jj * 2 * n + t] = re;
+                table[(size_t)jj * 2 * n + n + t] = im;
             }
         }
 }
 
+// One offset's M2L table: source box at the origin, target at 2 r d.
+void dense_m2l(int p, double k, double r, const int d[3], double* table) {
+    const double c0[3] = {0.0, 0.0, 0.0}, ct[3] = {2.0 * r * d[0], 2.0 * r * d[1], 2.0 * r * d[2]};
+    dense_translation(p, k, true, r, c0, false, r, ct, table);
+}
+
 }  // namespace
+
+// The 8 octants' M2M and L2L tables of a parent level of half-width r (child o at the
+// parent centre + r/2 (+-1, +-1, +-1), the sign of x from bit 2 of o, y bit 1, z bit 0):
+// M2M takes a child's multipole to the parent's, L2L the parent's local to the child's.
+void build_helmholtz_octant_tables(int p, double k, double r, std::vector<double>& m2m, std::vector<double>& l2l) {
+    const int n = (p + 1) * (p + 1);
+    const size_t per = 2 * (size_t)n * n;
+    m2m.assign(8 * per, 0.0);
+    l2l.assign(8 * per, 0.0);
+    std::vector<std::thread> pool;
+    for (int o = 0; o < 8; ++o)
+        pool.emplace_back([&, o] {
+            const double c0[3] = {0.0, 0.0, 0.0};
+            const double cc[3] = {((o >> 2) & 1) ? 0.5 * r : -0.5 * r, ((o >> 1) & 1) ? 0.5 * r : -0.5 * r,
+                                  (o & 1) ? 0.5 * r : -0.5 * r};
+            dense_translation(p, k, true, 0.5 * r, cc, true, r, c0, &m2m[per * o]);
+            dense_translation(p, k, false, r, c0, false, 0.5 * r, cc, &l2l[per * o]);
+        });
+    for (auto& th : pool) th.join();
+}
 
 // The 316 offsets' tables of one level (boxes of half-width r), one after the other in
 // offset index order: 316 * 2 n^2 doubles.

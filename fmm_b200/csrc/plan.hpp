@@ -98,5 +98,8 @@ void build_l2l_tables(int p, std::vector<double>& out);  // 8
 // Helmholtz (real k): the dense M2L tables of one level of boxes of half-width r, 316 real
 // 2n x n matrices in offset index order (helmholtz_tables.cpp)
 void build_helmholtz_m2l_tables(int p, double k, double r, std::vector<double>& out);
+// and the 8 octants' M2M (child multipole -> parent) and L2L (parent local -> child) tables
+// of a parent level of half-width r, real 2n x n matrices each
+void build_helmholtz_octant_tables(int p, double k, double r, std::vector<double>& m2m, std::vector<double>& l2l);
 
 }  // namespace fmmb

@@ -295,6 +295,13 @@ int fmmgpu_helmholtz_direct_sum(double k_re, double k_im, size_t nsources, const
  * column-major, column j the local of the unit real multipole e_j (the real plane in rows
  * 0..n over the imaginary plane), n = (p + 1)^2.  No device needed. */
 int fmmgpu_helmholtz_m2l_tables(int p, double k, double half_width, double* tables);
+/* The M2M and L2L tables between a parent level of half-width `half_width` and its
+ * children (the reference's per-level translation tables, fmm-ref/src/helmholtz/rcr.rs:129-156,
+ * here by projection), 8 octants each in the layout above: child o centred at the parent
+ * centre + half_width/2 (+-1, +-1, +-1), the sign of x from bit 2 of o, y bit 1, z bit 0;
+ * m2m[o] takes the child's multipole to the parent's, l2l[o] the parent's local to the
+ * child's.  Writes 8 * 2 (p + 1)^4 doubles to each.  No device needed. */
+int fmmgpu_helmholtz_octant_tables(int p, double k, double half_width, double* m2m, double* l2l);
 
 int fmmgpu_helmholtz_near(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges, double* potential,
                           double* gradient);

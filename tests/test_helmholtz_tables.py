@@ -41,3 +41,38 @@ def test_invalid_arguments():
     for args in ((31, 1.0, 0.5), (4, 0.0, 0.5), (4, 1.0, -1.0), (4, float("inf"), 0.5)):
         with pytest.raises(F.FmmError):
             F.helmholtz_m2l_tables(*args)
+
+
+def _octant_centre(o, r):
+    return np.array([0.5 * r if (o >> 2) & 1 else -0.5 * r, 0.5 * r if (o >> 1) & 1 else -0.5 * r,
+                     0.5 * r if o & 1 else -0.5 * r])
+
+
+def test_octant_tables_equal_the_oracle_projection_and_translate():
+    p, k, r = 6, 2.0, 0.5
+    m2m, l2l = F.helmholtz_octant_tables(p, k, r)
+    n = (p + 1) ** 2
+    assert m2m.shape == (8, 2 * n, n) and l2l.shape == (8, 2 * n, n)
+    rng = np.random.default_rng(18)
+    for o in (0, 3, 5, 7):
+        cc = _octant_centre(o, r)
+        for j in (0, 7, n - 1):
+            e = np.zeros(n, dtype=np.complex128)
+            e[j] = 1.0
+            up = O.hh_translate("m2m", p, p, k, 0.5 * r, cc, r, np.zeros(3), e)
+            down = O.hh_translate("l2l", p, p, k, r, np.zeros(3), 0.5 * r, cc, e)
+            assert np.abs(m2m[o][:n, j] + 1j * m2m[o][n:, j] - up).max() < 1e-12 * np.abs(up).max()
+            # a local's high degrees carry the quadrature's rounding divided by jh_n(k a)
+            # (fmm-ref/src/helmholtz/direct.rs:27-33): the two orders of summation differ there
+            assert np.abs(l2l[o][:n, j] + 1j * l2l[o][n:, j] - down).max() < 1e-10 * np.abs(down).max()
+    # a child's sources through the M2M table, seen from far away
+    o = 6
+    cc = _octant_centre(o, r)
+    src = cc + rng.uniform(-0.5 * r, 0.5 * r, (6, 3))
+    q = rng.standard_normal(6) + 1j * rng.standard_normal(6)
+    Mp = O.hh_apply_dense(m2m[o], O.hh_p2m(p, k, 0.5 * r, cc, src, q))
+    v = rng.standard_normal((5, 3))
+    tgt = 3.0 * v / np.linalg.norm(v, axis=1)[:, None]
+    phi, _ = O.hh_eval(p, k, r, np.zeros(3), Mp, tgt, singular=True)
+    ex, _ = O.helmholtz_direct_sum(k, src, q, tgt)
+    assert np.abs(phi - ex).max() / np.abs(ex).max() < 1e-4
