@@ -76,3 +76,18 @@ def test_octant_tables_equal_the_oracle_projection_and_translate():
     phi, _ = O.hh_eval(p, k, r, np.zeros(3), Mp, tgt, singular=True)
     ex, _ = O.helmholtz_direct_sum(k, src, q, tgt)
     assert np.abs(phi - ex).max() / np.abs(ex).max() < 1e-4
+
+
+def test_tables_scale_with_the_box():
+    """Only k r and the geometry in units of r enter: an M2L table of boxes of half-width r
+    is 1/r times the table of unit boxes at the wavenumber k r (the 4 pi i k of a
+    multipole's field carries the 1/length), and the M2M/L2L tables are scale free; so a
+    level's tables in leaf-scaled units (half-width 1, k_l = k r_l) serve every box size."""
+    p, k, r = 5, 3.0, 0.125
+    a = F.helmholtz_m2l_tables(p, k, r)
+    b = F.helmholtz_m2l_tables(p, k * r, 1.0)
+    assert np.abs(a - b / r).max() < 1e-11 * np.abs(a).max()
+    m_a, l_a = F.helmholtz_octant_tables(p, k, r)
+    m_b, l_b = F.helmholtz_octant_tables(p, k * r, 1.0)
+    assert np.abs(m_a - m_b).max() < 1e-11 * np.abs(m_a).max()
+    assert np.abs(l_a - l_b).max() < 1e-9 * np.abs(l_a).max()
