@@ -149,3 +149,42 @@ def test_settings_errors():
     bad[3, 1] = np.nan
     with pytest.raises(F.FmmError):
         F.FmmBuilder(4).plan(bad)
+
+
+def _edge_sets():
+    rng = np.random.default_rng(31)
+    line = np.zeros((700, 3))
+    line[:, 0] = rng.uniform(-1, 1, 700)  # collinear
+    plane = np.column_stack([rng.uniform(0, 1, 900), rng.uniform(0, 1, 900), np.full(900, 0.25)])
+    dup = np.repeat(rng.uniform(0, 1, (7, 3)), 150, axis=0)  # 7 sites of 150 coincident points
+    tiny = rng.uniform(0, 1e-9, (500, 3)) + 3.0  # a cloud of width 1e-9 far from the origin
+    huge = rng.uniform(-1e9, 1e9, (500, 3))
+    clumps = np.concatenate([rng.normal(0, 1e-6, (400, 3)), rng.uniform(-1, 1, (400, 3))])  # ragged depth
+    return {"two points": np.array([[0.0, 0, 0], [1.0, 1, 1]]),
+            "collinear": line, "planar": plane, "duplicates": dup, "tiny": tiny, "huge": huge,
+            "clumps": clumps}
+
+
+def test_degenerate_domain_is_an_error():
+    """A domain of no volume (one point, or every point coincident) is refused at build, as
+    the reference's compute_global_bounding_box refuses it (octree/src/lib.rs:67-68)."""
+    for x in (np.array([[0.3, 0.2, 0.1]]), np.repeat([[1.0, 2.0, 3.0]], 50, axis=0)):
+        with pytest.raises(F.FmmError, match="no volume"):
+            F.FmmBuilder(3).plan(x)
+
+
+@pytest.mark.parametrize("name", list(_edge_sets()))
+def test_tree_equals_oracle_on_edge_cases(oracle, name):
+    """Degenerate point sets (two points, collinear and planar clouds, coincident points
+    beyond the leaf limit, extreme scales, deep clumps beside a uniform cloud): the tree
+    equals the oracle's restatement key for key."""
+    x = _edge_sets()[name]
+    for mk in (1, 16):
+        plan = F.FmmBuilder(3).max_points_per_leaf(mk).plan(x)
+        keys, leaf = plan.boxes()
+        tr = oracle.Tree(x, x, 16, mk)
+        assert np.array_equal(keys, tr.keys), (name, mk)
+        assert np.array_equal(leaf, tr.is_leaf), (name, mk)
+        info = plan.info()
+        assert info["nsources"] == len(x) and info["nleaves"] == int(leaf.sum())
+        plan.close()
