@@ -67,7 +67,17 @@ def test_tree_with_distinct_targets(oracle):
 
 def test_lists_equal_brute_force_rule(oracle):
     x, _ = oracle.point_sets("sphere", 5000, 5)
-    mk = 20
+    assert _check_lists(oracle, x, 20) > 1000
+
+
+@pytest.mark.parametrize("name", ["clumps", "planar", "duplicates"])
+def test_lists_equal_brute_force_rule_on_edge_cases(oracle, name):
+    """Ragged depth (clumps 1e-6 wide beside a uniform cloud), a planar cloud and coincident
+    points: every list row equals the brute-force rule in accumulation order."""
+    _check_lists(oracle, _edge_sets()[name], 8)  # duplicates: few sites, no V pair at all
+
+
+def _check_lists(oracle, x, mk):
     plan = F.FmmBuilder(4).max_points_per_leaf(mk).plan(x)
     keys, leaf = plan.boxes()
     tr = oracle.Tree(x, x, 16, mk)
@@ -104,7 +114,7 @@ def test_lists_equal_brute_force_rule(oracle):
             w = plan.list(2, j).tolist()
             want_w = [k for k in tr.list(b, 2).tolist() if occ_of[k]] if occ[b] else []
             assert w == sorted(want_w, key=lambda k: pos[k])
-    assert offsets_checked > 1000
+    return offsets_checked
 
 
 def _index(key):
