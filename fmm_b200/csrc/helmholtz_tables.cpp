@@ -21,6 +21,8 @@
 // all n columns of an offset cost O(Q^2 n p); the offsets run on the host's threads.
 #include <algorithm>
 #include <cmath>
+#include <exception>
+#include <functional>
 #include <thread>
 #include <vector>
 
@@ -309,6 +311,27 @@ void dense_m2l(int p, double k, double r, const int d[3], double* table) {
     dense_translation(p, k, true, r, c0, false, r, ct, table);
 }
 
+// Runs work(t) for t = 0..count-1 on up to `threads` host threads; an exception in any of
+// them (an allocation failure) is rethrown here after all have joined.
+void parallel_for(int count, int threads, const std::function<void(int)>& work) {
+    const int nt = std::max(1, std::min(threads, count));
+    std::vector<std::exception_ptr> err(nt);
+    std::vector<std::thread> pool;
+    for (int w = 0; w < nt; ++w)
+        pool.emplace_back([&, w] {
+            try {
+                for (int t = w; t < count; t += nt) work(t);
+            } catch (...) {
+                err[w] = std::current_exception();
+            }
+        });
+    for (auto& th : pool) th.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
+int host_threads() { return (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 64u)); }
+
 }  // namespace
 
 // The 8 octants' M2M and L2L tables of a parent level of half-width r (child o at the
@@ -319,16 +342,16 @@ void build_helmholtz_octant_tables(int p, double k, double r, std::vector<double
     const size_t per = 2 * (size_t)n * n;
     m2m.assign(8 * per, 0.0);
     l2l.assign(8 * per, 0.0);
-    std::vector<std::thread> pool;
-    for (int o = 0; o < 8; ++o)
-        pool.emplace_back([&, o] {
-            const double c0[3] = {0.0, 0.0, 0.0};
-            const double cc[3] = {((o >> 2) & 1) ? 0.5 * r : -0.5 * r, ((o >> 1) & 1) ? 0.5 * r : -0.5 * r,
-                                  (o & 1) ? 0.5 * r : -0.5 * r};
-            dense_translation(p, k, true, 0.5 * r, cc, true, r, c0, &m2m[per * o]);
+    parallel_for(16, host_threads(), [&](int t) {
+        const int o = t >> 1;
+        const double c0[3] = {0.0, 0.0, 0.0};
+        const double cc[3] = {((o >> 2) & 1) ? 0.5 * r : -0.5 * r, ((o >> 1) & 1) ? 0.5 * r : -0.5 * r,
+                              (o & 1) ? 0.5 * r : -0.5 * r};
+        if (t & 1)
             dense_translation(p, k, false, r, c0, false, 0.5 * r, cc, &l2l[per * o]);
-        });
-    for (auto& th : pool) th.join();
+        else
+            dense_translation(p, k, true, 0.5 * r, cc, true, r, c0, &m2m[per * o]);
+    });
 }
 
 // The 316 offsets' tables of one level (boxes of half-width r), one after the other in
@@ -346,13 +369,7 @@ void build_helmholtz_m2l_tables(int p, double k, double r, std::vector<double>& 
     const int n = (p + 1) * (p + 1), count = (int)off.size() / 3;
     const size_t per = 2 * (size_t)n * n;
     out.assign(per * count, 0.0);
-    const int nthreads = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
-    std::vector<std::thread> pool;
-    for (int w = 0; w < nthreads; ++w)
-        pool.emplace_back([&, w] {
-            for (int t = w; t < count; t += nthreads) dense_m2l(p, k, r, &off[3 * t], &out[per * t]);
-        });
-    for (auto& th : pool) th.join();
+    parallel_for(count, host_threads(), [&](int t) { dense_m2l(p, k, r, &off[3 * t], &out[per * t]); });
 }
 
 }  // namespace fmmb
