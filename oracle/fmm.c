@@ -282,6 +282,11 @@ static void leaf_lists(const plan_t *P, size_t b, vecz *wl, vecz *near) {
     sort_unique(near);
 }
 
+/* seconds of the last orc_fmm_kinds without its plan and table builds (the evaluation the
+ * reference's benchmark times, fmm-bench/src/measure.rs: build and tables excluded) */
+static double g_eval_seconds = 0.0;
+double orc_fmm_last_eval_seconds(void) { return g_eval_seconds; }
+
 int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
             int p, int max_keys, int gradients, int threads, double *phi_out, double *grad_out) {
     return orc_fmm_kinds(ns, src, q, m, nt, tgt, p, max_keys, gradients, threads, 3, phi_out, grad_out);
@@ -298,6 +303,7 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
     int nc = (p + 1) * (p + 1);
     plan_t PL;
     plan_setup(&PL, ns, src, nt, tgt, max_keys);
+    const double t_start = omp_get_wtime();
     boxes_t B = PL.B;
     const double *lower = PL.lower;
     const double side = PL.side;
@@ -315,9 +321,11 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
     double *m2l_t = (double *)malloc((size_t)316 * nc * nc * sizeof(double));
     double *m2m_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
     double *l2l_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
+    const double t_tab0 = omp_get_wtime();
     orc_build_m2l_tables(p, m2l_t);
     orc_build_m2m_tables(p, m2m_t);
     orc_build_l2l_tables(p, l2l_t);
+    const double t_tab1 = omp_get_wtime();
 
     double *M = (double *)calloc(B.nboxes * m * nc, sizeof(double));
     double *Lc = (double *)calloc(B.nboxes * m * nc, sizeof(double));
@@ -471,6 +479,7 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
         }
     }
 
+    g_eval_seconds = (omp_get_wtime() - t_start) - (t_tab1 - t_tab0);
     free(M); free(Lc); free(phi); free(grad);
     free(m2l_t); free(m2m_t); free(l2l_t);
     free(qs);

@@ -81,7 +81,13 @@ void orc_build_l2l_tables(int p, double *tables);
 /* y += A x, k ascending (fmm-tables/src/matrix_set.rs:128) */
 void orc_matvec(int nc, const double *A, const double *x, double *y);
 
-/* ---- P2P (fmm-ref/src/p2p.rs) ---- */
+/* ---- P2P (fmm-ref/src/p2p.rs); orc_p2p_ref is the same sums one target at a time ---- */
+void orc_p2p_ref(size_t ns, const double *src, const double *q, size_t nt, const double *tgt,
+                 double *potential, double *gradient);
+/* the sums of orc_p2p on targets split into coordinate and accumulator arrays */
+void orc_p2p_lanes(size_t ns, const double *src, const double *q, size_t nt, const double *restrict tx,
+                   const double *restrict ty, const double *restrict tz, double *restrict ph,
+                   double *restrict g0, double *restrict g1, double *restrict g2);
 void orc_p2p(size_t ns, const double *src, const double *q, size_t nt, const double *tgt,
              double *potential, double *gradient);
 void orc_direct_sum(size_t ns, const double *src, const double *q, size_t nt, const double *tgt,
@@ -117,6 +123,9 @@ size_t orc_tree_list(const orc_tree *t, size_t box, int kind, uint64_t *out, siz
  * and boxes (bit-identical to serial).  Returns 0 on success. */
 int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
             int p, int max_keys, int gradients, int threads, double *phi, double *grad);
+
+/* seconds of the last orc_fmm / orc_fmm_kinds call without its plan and table builds */
+double orc_fmm_last_eval_seconds(void);
 
 /* the same with a kinds mask: bit 0 the near field (P2P), bit 1 the far field (L2P, M2P
  * and everything upstream of them); 3 is the whole FMM */

@@ -434,19 +434,13 @@ void orc_build_l2l_tables(int p, double *tables) {
     free(unit);
 }
 
-void orc_matvec(int nc, const double *A, const double *x, double *y) {
-    for (int k = 0; k < nc; ++k) {
-        double xk = x[k];
-        const double *col = A + (size_t)k * nc;
-        for (int r = 0; r < nc; ++r) y[r] = y[r] + xk * col[r];
-    }
-}
-
 /* ------------------------------------------------------------------------------------
  * P2P and the direct sum (fmm-ref/src/p2p.rs:90-186, Term at :400-433, Neumaier :436-460)
  * ---------------------------------------------------------------------------------- */
-void orc_p2p(size_t ns, const double *src, const double *q, size_t nt, const double *tgt,
-             double *potential, double *gradient) {
+/* The reference's loop order, one target at a time (kept as the statement of the rule and
+ * to check orc_p2p against). */
+void orc_p2p_ref(size_t ns, const double *src, const double *q, size_t nt, const double *tgt,
+                 double *potential, double *gradient) {
     for (size_t i = 0; i < nt; ++i) {
         const double *x = tgt + 3 * i;
         for (size_t j = 0; j < ns; ++j) {
@@ -463,6 +457,33 @@ void orc_p2p(size_t ns, const double *src, const double *q, size_t nt, const dou
             }
         }
     }
+}
+
+void orc_p2p(size_t ns, const double *src, const double *q, size_t nt, const double *tgt,
+             double *potential, double *gradient) {
+    if (nt == 0) return;
+    double *w = (double *)malloc(7 * nt * sizeof(double));
+    double *tx = w, *ty = w + nt, *tz = w + 2 * nt, *ph = w + 3 * nt, *g0 = w + 4 * nt, *g1 = w + 5 * nt,
+           *g2 = w + 6 * nt;
+    for (size_t i = 0; i < nt; ++i) {
+        tx[i] = tgt[3 * i];
+        ty[i] = tgt[3 * i + 1];
+        tz[i] = tgt[3 * i + 2];
+        ph[i] = potential[i];
+        g0[i] = gradient ? gradient[3 * i] : 0.0;
+        g1[i] = gradient ? gradient[3 * i + 1] : 0.0;
+        g2[i] = gradient ? gradient[3 * i + 2] : 0.0;
+    }
+    orc_p2p_lanes(ns, src, q, nt, tx, ty, tz, ph, g0, g1, g2);  /* the gradient sums are dropped without one */
+    for (size_t i = 0; i < nt; ++i) {
+        potential[i] = ph[i];
+        if (gradient) {
+            gradient[3 * i] = g0[i];
+            gradient[3 * i + 1] = g1[i];
+            gradient[3 * i + 2] = g2[i];
+        }
+    }
+    free(w);
 }
 
 typedef struct { double sum, comp; } neumaier;

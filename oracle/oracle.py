@@ -49,6 +49,7 @@ def lib():
             "orc_build_l2l_tables": (None, [C.c_int, _dp]),
             "orc_offset_index": (C.c_int, [C.c_int64, C.c_int64, C.c_int64]),
             "orc_p2p": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
+            "orc_p2p_ref": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_direct_sum": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_direct_sum_omp": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_key_from_index": (C.c_uint64, [_u32p, C.c_int]),
@@ -67,6 +68,7 @@ def lib():
                                   C.c_int, _dp, C.c_void_p]),
             "orc_fmm_kinds": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
                                         C.c_int, C.c_int, _dp, C.c_void_p]),
+            "orc_fmm_last_eval_seconds": (C.c_double, []),
             "orc_helmholtz_p2p": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_helmholtz_direct_sum": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp,
                                                 C.c_void_p]),
@@ -406,6 +408,11 @@ def helmholtz_near(src, q, tgt, k, max_keys, gradients=True, threads=0):
                              int(gradients), threads, phi.view(np.float64),
                              None if g is None else g.view(np.float64).ctypes.data_as(C.c_void_p))
     return phi.reshape(m, len(tgt)), (None if g is None else g.reshape(m, len(tgt), 3))
+
+
+def fmm_last_eval_seconds():
+    """Seconds of the last fmm() call without its plan and table builds."""
+    return lib().orc_fmm_last_eval_seconds()
 
 
 def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0, kinds=3):

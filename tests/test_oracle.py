@@ -156,3 +156,25 @@ def test_fmm_accuracy_gate(oracle, p, prediction):
         errs.append(np.linalg.norm(phi[k][sample] - d) / np.linalg.norm(d))
     rms = float(np.sqrt(np.mean(np.square(errs))))
     assert rms < 2.0 * prediction, (rms, errs)
+
+
+def test_p2p_in_vector_lanes_equals_the_scalar_loop(oracle):
+    """orc_p2p (targets in vector lanes, oracle/lanes.c) gives the bits of the reference's
+    one-target-at-a-time loop (orc_p2p_ref), coincident pairs included, adding into what
+    the outputs hold."""
+    import ctypes
+
+    L = oracle.lib()
+    rng = np.random.default_rng(41)
+    for ns, nt in ((1, 1), (7, 3), (64, 65), (300, 513)):
+        src = rng.uniform(-1, 1, (ns, 3))
+        tgt = np.concatenate([rng.uniform(-1, 1, (nt, 3)), src[: min(ns, 4)]])
+        q = rng.standard_normal(ns)
+        phi0 = rng.standard_normal(len(tgt))
+        g0 = rng.standard_normal(3 * len(tgt))
+        out = []
+        for f in (L.orc_p2p, L.orc_p2p_ref):
+            phi, g = phi0.copy(), g0.copy()
+            f(ns, src, q, len(tgt), tgt, phi, g.ctypes.data_as(ctypes.c_void_p))
+            out.append((phi, g))
+        assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
