@@ -4,6 +4,7 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 import fmm_b200 as F
 
@@ -47,3 +48,28 @@ def test_level_calls_need_an_evaluator():
     assert lib.fmmgpu_op_p2m(plan._h, 0) == 1
     assert b"plan-only" in lib.fmmgpu_last_error()
     assert lib.fmmgpu_op_begin_evaluation(plan._h, None) == 1
+
+
+def _struct_fields(name):
+    """(type, field) pairs of the header's `typedef struct { ... } name;`, in order."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    body = re.search(r"typedef struct \{([^}]*)\}\s*" + name + r";", text).group(1)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        ctype, names = decl.split(None, 1)
+        out += [(ctype, n.strip()) for n in names.split(",")]
+    return out
+
+
+@pytest.mark.parametrize("cname,pystruct", [("fmmgpu_settings", F.Settings), ("fmmgpu_info", F.Info)])
+def test_python_structs_mirror_the_header(cname, pystruct):
+    """The ctypes mirrors of the header's structs: the same fields in the same order with
+    the same widths, so the library and the binding agree on the layout."""
+    width = {"int": C.c_int, "int64_t": C.c_int64}
+    fields = _struct_fields(cname)
+    assert [n for _, n in fields] == [n for n, _ in pystruct._fields_]
+    for (ctype, n), (pn, pt) in zip(fields, pystruct._fields_):
+        assert C.sizeof(width[ctype]) == C.sizeof(pt), (n, ctype, pt)
