@@ -153,10 +153,23 @@ extern "C" int fmmgpu_direct_sum(size_t ns, const double* src, const double* q, 
     return e == cudaSuccess ? FMMGPU_OK : fail(e);
 }
 
+// Restores the calling thread's current device when a call returns.
+struct CurrentDevice {
+    int saved = -1;
+    CurrentDevice() {
+        if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+    }
+    ~CurrentDevice() {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
+
 // The same sums on device buffers with the scratch in g_noalloc_part: no device or host
 // allocation, no synchronisation.  Its address on each device is looked up once, under a
-// lock, by the first call there.  Every scratch slot the combine reads is written by the
-// partial kernel earlier in the same call, so nothing in it has to start at zero.
+// lock, by the first call there (the cached address assumes the device is not reset
+// while the library is loaded).  Every scratch slot the combine reads is written by the
+// partial kernel earlier in the same call, so nothing in it has to start at zero.  The
+// calling thread's current device is the same on return as on entry.
 extern "C" int fmmgpu_direct_sum_noalloc(size_t ns, const double* src, const double* q, size_t nt,
                                          const double* tgt, double* phi, double* grad, int device,
                                          void* stream) {
@@ -184,8 +197,13 @@ extern "C" int fmmgpu_direct_sum_noalloc(size_t ns, const double* src, const dou
         fmmb::set_last_error(std::string("fmmgpu_direct_sum_noalloc: ") + what + ": " + cudaGetErrorString(e));
         return FMMGPU_DEVICE_ERROR;
     };
+    CurrentDevice keep;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail("cudaSetDevice", e);
+    // an error left by earlier work on this thread is reported as such, not cleared, and
+    // nothing is launched
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return fail("a CUDA error from before this call is pending", e);
     static std::mutex mu;
     static double* scratch[kMaxDevices] = {};
     double* part;

@@ -1,0 +1,1266 @@
+// The device evaluator of one expansion order P and one precision T: plan upload, the
+// level-by-level pass sequence on one stream, the level calls.  Included by
+// evaluator_order.cu, which instantiates it for one order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "evaluator_base.hpp"
+#include "helmholtz.cuh"
+#include "kernels.cuh"
+#include "m2l_fused.cuh"
+#include "m2l_tc.cuh"
+#include "p2p_x2.cuh"
+
+namespace fmmb {
+
+static_assert(kX2Warps == 4, "EvaluatorBase::p2p_warps starts at the mixed P2P's static block");
+
+// ----------------------------------------------------------------------------------
+// The evaluator of one precision T and one degree P.
+// ----------------------------------------------------------------------------------
+template <int P, typename T>
+struct Evaluator final : EvaluatorBase {
+    static constexpr int NC = nc_of(P);
+    using T4 = typename Vec4<T>::type;
+    const Plan& plan;
+    DevPlan dp{};
+    cudaStream_t stream;
+    int m;
+    bool gradients;
+    // plan arrays
+    DevBuf level, idx, parent, child_first, box_leaf, src_below, tgt_below, leaf_box, src_start,
+        tgt_start, tgt_perm, src_perm, near_row, near_col, w_row, w_col, x_row, x_col, v_row, v_col,
+        v_off, box_side;
+    // data
+    DevBuf m2l_tab, m2m_tab, l2l_tab, spos, tpos, sq, M, Lc, far_phi, far_g, Y;
+    // interior boxes per level with a source below (M2M parents), CSR by level
+    DevBuf m2m_par;
+    std::vector<int64_t> m2m_start;
+    // per-level octant batches of the M2M (children with a source) and L2L (children with a
+    // target) products, tiles of kGemmPairs; Yo holds one product row per child box
+    DevBuf oct_tile_d, oct_tile_begin, oct_tile_count, oct_pair_e, oct_pair_src, Yo;
+    std::vector<int64_t> m2m_tiles, l2l_tiles;  // tile ranges per level (nlevels + 1)
+    // M2L batches: pairs of all levels grouped by offset, in tiles
+    DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src, v_pos;
+    int64_t ntiles = 0;
+    // the same pairs in per-level tiles, for the level calls
+    DevBuf ltile_d, ltile_begin, ltile_count;
+    std::vector<int64_t> lvl_tiles;
+    // tensor-core M2L (mixed form, (p+1)^2 <= 128 output slots: p <= 10): tiles of
+    // TcTs<P>::NT columns and the table images; the fused form needs p <= 8 (tensor memory
+    // holds two tables there)
+    static constexpr bool kTensor = sizeof(T) == 4 && P <= 10;
+    static constexpr bool kFusedOk = kTensor && P <= 8;
+    DevBuf tc_tile_d, tc_tile_begin, tc_tile_count, tc_pair_e, tc_pair_src, tc_bimg, tc_error;
+    DevBuf tc_ltile_d, tc_ltile_begin, tc_ltile_count;
+    std::vector<int64_t> tc_lvl_tiles;
+    int64_t tc_ntiles = 0;
+    int num_sms = 148;
+    // fused tensor-core M2L: per level, chunks of consecutive target boxes cut into tiles
+    // of one offset (pairs in (chunk, offset, target) order), CTA c of level l taking the
+    // tiles fu_cta[fu_lvl_cta[l] + c] .. fu_cta[fu_lvl_cta[l] + c + 1]
+    DevBuf fu_tile_d, fu_tile_begin, fu_tile_np, fu_cta, fu_pair_src, fu_pair_tgt, fu_img;
+    std::vector<int64_t> fu_lvl_cta;
+    std::vector<int> fu_lvl_grid;
+    bool product_path_built = false;  // the product paths' tiles and Y (built on first use)
+    // chunked product path: when the products of every V pair and vector do not fit the
+    // product budget (ybudget bytes), each level's boxes are cut into chunks whose products
+    // fit; a chunk's pairs are ordered by (offset, target) at positions local to the chunk
+    // (v_pos), tensor-core tiles (NT / m pairs) and SIMT tiles (kGemmPairs pairs) per chunk
+    struct Chunk {
+        int level;
+        int64_t b0, b1, base, npairs, tc_t0, tc_nt, s_t0, s_nt;
+    };
+    std::vector<Chunk> chunks;
+    int64_t ybudget = 0;
+    DevBuf ck_tc_d, ck_tc_begin, ck_tc_count, ck_s_d, ck_s_begin, ck_s_count, ck_pair_src;
+    std::vector<uint32_t> tc_img;     // host copy of the tensor-memory table images
+    CUtensorMap mmap{};               // the multipoles, for the tensor-core M2L's row gathers
+    CUtensorMap vmap{};               // the same, boxes of m rows (a pair's vectors)
+    // P2P work items (32 targets of one leaf each) and, for the mixed form, the
+    // near-singular pairs evaluated in f64
+    DevBuf item_leaf, item_t0, close_row, close_src, close_leaf, spos64, tpos64, sq64, near_rec, close_y;
+    // the near rows' source streams in the target leaves' frames (mixed form, P2pStream)
+    DevBuf st_rowpair, st_xy, st_zz, st_idx;
+    // the near-singular pairs' weights (per pair) and, per evaluation, their f64 sums per
+    // target and vector (close_weights_kernel, close_sum_kernel)
+    DevBuf close_w, close_acc;
+    // boxes with a nonempty X list, level by level (the P2L launches)
+    DevBuf xbox;
+    std::vector<int64_t> xbox_start;
+    // the near field summed apart on a second, lower-priority stream, joined by output_kernel
+    DevBuf near_phi, near_g;
+    cudaStream_t near_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    P2pItems items{};
+    std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
+    std::vector<int32_t> item_leaf_h;  // the items' leaves (host copy, ascending)
+    ClosePairs close{};
+    int64_t nclose = 0;
+    static constexpr bool kMixed = sizeof(T) == 4;
+    static constexpr bool kBfly = sizeof(T) == 4;  // register P2M/P2L (f32, vectors one after another)
+
+    // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
+    static constexpr float kTheta2 = 0.0625f;
+    static constexpr float kRmax = 4.0f;  // 1 / theta: the mixed P2P's clamp of 1/r
+
+    Evaluator(const Plan& pl, const std::vector<double>& m2l, const std::vector<double>& m2m,
+              const std::vector<double>& l2l, cudaStream_t s, int m_, bool grad, const std::vector<double>& us,
+              const std::vector<double>& ut, bool fused, int64_t ybudget_)
+        : plan(pl), stream(s), m(m_), gradients(grad), ybudget(ybudget_) {
+        timer.stream = s;
+        level.upload(pl.level);
+        idx.upload(pl.idx);
+        parent.upload(pl.parent);
+        child_first.upload(pl.child_first);
+        box_leaf.upload(pl.box_leaf);
+        src_below.upload(pl.src_below);
+        tgt_below.upload(pl.tgt_below);
+        leaf_box.upload(pl.leaf_box);
+        src_start.upload(pl.src_start);
+        tgt_start.upload(pl.tgt_start);
+        tgt_perm.upload(pl.tgt_perm);
+        src_perm.upload(pl.src_perm);
+        near_row.upload(pl.near.row);
+        near_col.upload(pl.near.col);
+        w_row.upload(pl.w.row);
+        w_col.upload(pl.w.col);
+        x_row.upload(pl.x.row);
+        x_col.upload(pl.x.col);
+        v_row.upload(pl.v.row);
+        v_col.upload(pl.v.col);
+        v_off.upload(pl.v.aux);
+        dp.nlevels = pl.nlevels;
+        dp.side = pl.side;
+        dp.level = level.as<int32_t>();
+        dp.idx = idx.as<uint32_t>();
+        dp.parent = parent.as<int32_t>();
+        dp.child_first = child_first.as<int32_t>();
+        dp.box_leaf = box_leaf.as<int32_t>();
+        dp.src_below = src_below.as<int64_t>();
+        dp.tgt_below = tgt_below.as<int64_t>();
+        dp.leaf_box = leaf_box.as<int32_t>();
+        dp.src_start = src_start.as<int64_t>();
+        dp.tgt_start = tgt_start.as<int64_t>();
+        dp.tgt_perm = tgt_perm.as<int64_t>();
+        dp.src_perm = src_perm.as<int64_t>();
+        dp.near_row = near_row.as<int64_t>();
+        dp.near_col = near_col.as<int32_t>();
+        dp.w_row = w_row.as<int64_t>();
+        dp.w_col = w_col.as<int32_t>();
+        dp.x_row = x_row.as<int64_t>();
+        dp.x_col = x_col.as<int32_t>();
+        dp.v_row = v_row.as<int64_t>();
+        dp.v_col = v_col.as<int32_t>();
+        dp.v_off = v_off.as<int32_t>();
+        if (!pl.box_side.empty()) box_side.upload(pl.box_side);
+        dp.box_side = pl.box_side.empty() ? nullptr : box_side.as<double>();
+        dp.nsrc = (int64_t)pl.src_perm.size();
+        dp.ntgt = (int64_t)pl.tgt_perm.size();
+        // tables rounded entry by entry to T (fmm-tables/src/matrix_set.rs:150 cast)
+        auto up_tab = [](DevBuf& b, const std::vector<double>& t) {
+            std::vector<T> c(t.begin(), t.end());
+            b.upload(c);
+        };
+        up_tab(m2l_tab, m2l);
+        up_tab(m2m_tab, m2m);
+        up_tab(l2l_tab, l2l);
+        // leaf-scaled coordinates, rounded once to T
+        auto up_pos = [](DevBuf& b, const std::vector<double>& u) {
+            size_t n = u.size() / 3;
+            std::vector<T4> v(n);
+            for (size_t i = 0; i < n; ++i) {
+                v[i].x = (T)u[3 * i];
+                v[i].y = (T)u[3 * i + 1];
+                v[i].z = (T)u[3 * i + 2];
+                v[i].w = T(0);
+            }
+            b.upload(v);
+        };
+        up_pos(spos, us);
+        up_pos(tpos, ut);
+        const size_t nb = pl.nboxes();
+        sq.alloc(sizeof(T) * (size_t)m * (dp.nsrc + 1));
+        M.alloc(sizeof(T) * (size_t)m * ms_of(P) * nb);
+        Lc.alloc(sizeof(T) * (size_t)m * ms_of(P) * nb);
+        far_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
+        far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
+        CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
+        build_parent_lists();
+        if (kTensor) build_tensor_m2l(m2l);
+        if (kFusedOk && fused && m <= fused_tile_columns(P)) {
+            build_fused_m2l();
+            m2l_path = 2;
+        } else {
+            m2l_path = kTensor ? 1 : 0;
+            ensure_product_path();
+        }
+        build_p2p_items();
+        {
+            std::vector<int32_t> xb;
+            xbox_start.assign(pl.nlevels + 1, 0);
+            for (int l = 0; l < pl.nlevels; ++l) {
+                xbox_start[l] = (int64_t)xb.size();
+                for (int64_t b = pl.level_start[l]; b < pl.level_start[l + 1]; ++b)
+                    if (pl.x.row[b + 1] > pl.x.row[b]) xb.push_back((int32_t)b);
+            }
+            xbox_start[pl.nlevels] = (int64_t)xb.size();
+            xbox.upload(xb);
+        }
+        int least = 0, greatest = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_TRY(cudaStreamCreateWithPriority(&near_stream, cudaStreamNonBlocking, least));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        near_phi.alloc(sizeof(double) * (size_t)m * (dp.ntgt + 1));
+        if (gradients) near_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
+        if (kMixed) {
+            for (size_t j = 0; j < pl.nleaves(); ++j)  // a row fits the kernel's shared memory
+                if (pl.near.row[j + 1] - pl.near.row[j] > kX2Recs)
+                    throw Failure(FMMGPU_INVALID_ARGUMENT, "a near row longer than " + std::to_string(kX2Recs) +
+                                                              " leaves (the tree is not 2:1 balanced)");
+            build_close_pairs(us, ut);
+            near_rec.alloc(sizeof(NearRec) * (pl.near.nnz() + 1));
+            if (pl.nleaves())
+                near_record_kernel<<<(unsigned)((pl.nleaves() + 127) / 128), 128>>>(dp, (int64_t)pl.nleaves(),
+                                                                                   near_rec.as<NearRec>());
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaDeviceSynchronize());
+            build_p2p_stream();
+        }
+        close_pairs = nclose;
+        gemm_smem = GemmShape<P, T>::SMEM;
+        if (gemm_smem > 48 * 1024)
+            CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem));
+        // shared memory opt-in beyond 48 KB where a kernel needs it
+        size_t exp_smem = sizeof(T) * (NC * 32 + (size_t)m * 32);
+        if (exp_smem > 48 * 1024) {
+            CUDA_TRY(cudaFuncSetAttribute(expand_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)exp_smem));
+            CUDA_TRY(cudaFuncSetAttribute(expand_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)exp_smem));
+        }
+    }
+
+    size_t gemm_smem = 0;
+
+    ~Evaluator() override {
+        if (near_stream) {
+            cudaStreamSynchronize(near_stream);
+            cudaStreamDestroy(near_stream);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+    }
+
+    // The product paths (1 and 0): offset-sorted tiles, the position map and the product
+    // array Y, built when a product path is first used.
+    void ensure_product_path() {
+        if (product_path_built) return;
+        const int64_t row_bytes = (int64_t)sizeof(T) * m * ys_of(P);
+        if (ybudget > 0 && ((int64_t)plan.v.nnz() + 1) * row_bytes > ybudget) {
+            build_product_chunks(row_bytes);
+            product_path_built = true;
+            return;
+        }
+        build_m2l_batches(kGemmPairs);
+        if constexpr (kTensor) {
+            Tiles all, lvl;
+            std::vector<int64_t> pe;
+            std::vector<int32_t> ps;
+            batches(TcTs<P>::NT / m, all, lvl, tc_lvl_tiles, pe, ps);
+            tc_ntiles = (int64_t)all.d.size();
+            tc_tile_d.upload(all.d);
+            tc_tile_begin.upload(all.begin);
+            tc_tile_count.upload(all.count);
+            tc_ltile_d.upload(lvl.d);
+            tc_ltile_begin.upload(lvl.begin);
+            tc_ltile_count.upload(lvl.count);
+            tc_pair_src.upload(ps);
+        }
+        Y.alloc(sizeof(T) * (size_t)m * ys_of(P) * (plan.v.nnz() + 1));
+        product_path_built = true;
+    }
+
+    void build_product_chunks(int64_t row_bytes) {
+        const Plan& pl = plan;
+        const int ppt_tc = kTensor ? std::max(1, tc_tile_columns(P) / m) : 1;
+        const int64_t max_pairs = std::max<int64_t>(1, ybudget / row_bytes - 1);
+        std::vector<int32_t> ps, tcd, tcn, sd, sn;
+        std::vector<int64_t> tcb, sb, vp(pl.v.nnz());
+        std::vector<int64_t> cnt(317), fill(316);
+        int64_t ymax = 0;
+        chunks.clear();
+        for (int l = 0; l < pl.nlevels; ++l) {
+            int64_t b = pl.level_start[l];
+            const int64_t bend = pl.level_start[l + 1];
+            while (b < bend) {
+                int64_t e = b, np = 0;
+                for (; e < bend; ++e) {
+                    const int64_t nv = pl.v.row[e + 1] - pl.v.row[e];
+                    if (np > 0 && np + nv > max_pairs) break;
+                    np += nv;
+                }
+                Chunk c{l, b, e, (int64_t)ps.size(), np, (int64_t)tcd.size(), 0, (int64_t)sd.size(), 0};
+                if (np > 0) {
+                    std::fill(cnt.begin(), cnt.end(), 0);
+                    for (int64_t x = b; x < e; ++x)
+                        for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) cnt[pl.v.aux[q] + 1]++;
+                    for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+                    ps.resize(c.base + np);
+                    for (int d = 0; d < 316; ++d) fill[d] = cnt[d];
+                    // boxes in order: each offset's pairs come out ordered by target
+                    for (int64_t x = b; x < e; ++x)
+                        for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) {
+                            const int64_t pos = fill[pl.v.aux[q]]++;
+                            ps[c.base + pos] = pl.v.col[q];
+                            vp[q] = pos;
+                        }
+                    for (int d = 0; d < 316; ++d) {
+                        for (int64_t j = cnt[d]; j < cnt[d + 1]; j += ppt_tc) {
+                            tcd.push_back(d);
+                            tcb.push_back(j);
+                            tcn.push_back((int32_t)std::min<int64_t>(ppt_tc, cnt[d + 1] - j));
+                        }
+                        for (int64_t j = cnt[d]; j < cnt[d + 1]; j += kGemmPairs) {
+                            sd.push_back(d);
+                            sb.push_back(j);
+                            sn.push_back((int32_t)std::min<int64_t>(kGemmPairs, cnt[d + 1] - j));
+                        }
+                    }
+                    c.tc_nt = (int64_t)tcd.size() - c.tc_t0;
+                    c.s_nt = (int64_t)sd.size() - c.s_t0;
+                    ymax = std::max(ymax, np);
+                }
+                chunks.push_back(c);
+                b = e;
+            }
+        }
+        ck_tc_d.upload(tcd);
+        ck_tc_begin.upload(tcb);
+        ck_tc_count.upload(tcn);
+        ck_s_d.upload(sd);
+        ck_s_begin.upload(sb);
+        ck_s_count.upload(sn);
+        ck_pair_src.upload(ps);
+        v_pos.upload(vp);
+        Y.alloc((size_t)row_bytes * (size_t)(ymax + 1));
+    }
+
+    // M2L products of one chunk into the product buffer, then its boxes' locals
+    void m2l_chunk(const Chunk& c) {
+        if (c.npairs == 0) return;
+        if (kTensor && m2l_path == 1) {
+            if constexpr (kTensor) {
+                const unsigned grid = (unsigned)std::min<int64_t>(c.tc_nt, num_sms);
+                m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                    ck_tc_d.as<int32_t>() + c.tc_t0, ck_tc_begin.as<int64_t>() + c.tc_t0,
+                    ck_tc_count.as<int32_t>() + c.tc_t0, c.tc_nt, ck_pair_src.as<int32_t>() + c.base, m,
+                    tc_bimg.as<uint32_t>(), mmap, vmap, reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+            }
+            return;
+        }
+        m2l_gemm_kernel<P, T><<<counted((unsigned)c.s_nt), 256, gemm_smem, stream>>>(
+            ck_s_d.as<int32_t>() + c.s_t0, ck_s_begin.as<int64_t>() + c.s_t0, ck_s_count.as<int32_t>() + c.s_t0,
+            nullptr, ck_pair_src.as<int32_t>() + c.base, m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
+    }
+    void reduce_chunk(const Chunk& c, int with_l2l, int with_v, int accumulate) {
+        reduce_range(c.b0, c.b1, with_l2l, with_v, accumulate);
+    }
+
+    // the local reduce of boxes [b0, b1): f32 a warp per box with 16-byte accesses, f64 a
+    // block per box (the same order of additions either way)
+    void reduce_range(int64_t b0, int64_t b1, int with_l2l, int with_v, int accumulate) {
+        if (b1 <= b0) return;
+        if constexpr (kMixed)
+            local_reduce4_kernel<P><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
+                dp, b0, b1, m, with_l2l, with_v, accumulate, reinterpret_cast<const float*>(Yo.ptr),
+                reinterpret_cast<const float*>(Y.ptr), v_pos.as<int64_t>(), reinterpret_cast<float*>(Lc.ptr));
+        else
+            local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
+                dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
+                Lc.as<T>());
+    }
+
+    // The fused path's tiles (see m2l_fused.cuh).  A chunk closes once it holds about
+    // three full tiles per offset, or a 1 / (2 num_sms) share of its level's columns (so
+    // that every level spreads over the SMs), or before its locals pass kFuChunkBytes (they
+    // stay in L2 while its CTA walks the offsets); each level's chunks are dealt to at most
+    // num_sms CTAs in contiguous runs of about equal tile counts.
+    static constexpr int64_t kFuChunkBytes = 384 * 1024;
+    void build_fused_m2l() {
+        if constexpr (kFusedOk) {
+            using S = FuShape<P>;
+            const Plan& pl = plan;
+            const int ppt = S::NT / m;
+            const int64_t col_full = 3 * 316 * (int64_t)S::NT;
+            const int64_t box_bytes = (int64_t)m * ms_of(P) * (int64_t)sizeof(float);
+            std::vector<int32_t> td, tn, ps, pt;
+            std::vector<int64_t> tb, cta;
+            fu_lvl_cta.assign(pl.nlevels + 1, 0);
+            fu_lvl_grid.assign(pl.nlevels, 0);
+            std::vector<int64_t> cnt(317), fill(316);
+            for (int l = 0; l < pl.nlevels; ++l) {
+                std::vector<int64_t> chunk_tiles{(int64_t)td.size()};
+                int64_t b = pl.level_start[l];
+                const int64_t bend = pl.level_start[l + 1];
+                const int64_t level_cols = (pl.v.row[bend] - pl.v.row[b]) * m;
+                const int64_t col_target =
+                    std::min<int64_t>(col_full, std::max<int64_t>(S::NT, level_cols / (2 * (int64_t)num_sms)));
+                while (b < bend) {
+                    int64_t e = b, cols = 0, nbox = 0;
+                    for (; e < bend; ++e) {
+                        const int64_t nv = pl.v.row[e + 1] - pl.v.row[e];
+                        if (nv == 0) continue;
+                        if (nbox > 0 && (cols >= col_target || (nbox + 1) * box_bytes > kFuChunkBytes)) break;
+                        cols += nv * m;
+                        ++nbox;
+                    }
+                    if (nbox > 0) {
+                        std::fill(cnt.begin(), cnt.end(), 0);
+                        for (int64_t x = b; x < e; ++x)
+                            for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) cnt[pl.v.aux[q] + 1]++;
+                        for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+                        const int64_t base = (int64_t)ps.size();
+                        ps.resize(base + cnt[316]);
+                        pt.resize(base + cnt[316]);
+                        for (int d = 0; d < 316; ++d) fill[d] = cnt[d];
+                        // boxes in order: each offset's pairs come out ordered by target
+                        for (int64_t x = b; x < e; ++x)
+                            for (int64_t q = pl.v.row[x]; q < pl.v.row[x + 1]; ++q) {
+                                const int64_t pos = base + fill[pl.v.aux[q]]++;
+                                ps[pos] = pl.v.col[q];
+                                pt[pos] = (int32_t)x;
+                            }
+                        for (int d = 0; d < 316; ++d)
+                            for (int64_t j = cnt[d]; j < cnt[d + 1]; j += ppt) {
+                                td.push_back(d);
+                                tb.push_back(base + j);
+                                tn.push_back((int32_t)std::min<int64_t>(ppt, cnt[d + 1] - j));
+                            }
+                        chunk_tiles.push_back((int64_t)td.size());
+                    }
+                    b = e;
+                }
+                const int64_t nch = (int64_t)chunk_tiles.size() - 1;
+                const int G = (int)std::min<int64_t>(num_sms, nch);
+                fu_lvl_cta[l] = (int64_t)cta.size();
+                fu_lvl_grid[l] = G;
+                if (G > 0) {
+                    const int64_t t0 = chunk_tiles[0], tt = chunk_tiles[nch] - t0;
+                    int64_t ci = 0;
+                    cta.push_back(t0);
+                    for (int c = 1; c < G; ++c) {
+                        const int64_t want = t0 + tt * c / G;
+                        while (ci < nch && chunk_tiles[ci] < want) ++ci;
+                        cta.push_back(std::max(cta.back(), chunk_tiles[ci]));
+                    }
+                    cta.push_back(chunk_tiles[nch]);
+                }
+            }
+            fu_lvl_cta[pl.nlevels] = (int64_t)cta.size();
+            fu_tile_d.upload(td);
+            fu_tile_begin.upload(tb);
+            fu_tile_np.upload(tn);
+            fu_cta.upload(cta);
+            fu_pair_src.upload(ps);
+            fu_pair_tgt.upload(pt);
+            std::vector<uint32_t> img;
+            build_fused_table_images<P>(tc_img, img);
+            fu_img.upload(img);
+            CUDA_TRY(cudaFuncSetAttribute(m2l_fused_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          FuShape<P>::SMEM));
+        }
+    }
+
+    void build_tensor_m2l(const std::vector<double>& m2l) {
+        if constexpr (kTensor) {
+            build_tc_table_images<P>(m2l, tc_img);
+            tc_bimg.upload(tc_img);
+            encode_multipole_map<P>(&mmap, reinterpret_cast<const float*>(M.ptr), (int64_t)plan.nboxes() * m);
+            encode_multipole_map<P>(&vmap, reinterpret_cast<const float*>(M.ptr), (int64_t)plan.nboxes() * m, m);
+            tc_error.alloc(sizeof(int));
+            CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
+            CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          TcTs<P>::SMEM));
+            int dev = 0;
+            CUDA_TRY(cudaGetDevice(&dev));
+            CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+    }
+
+    // Tile lists over the V pairs grouped by offset index, then by target box (pair
+    // positions pe/ps shared by both lists):
+    //  - the evaluation's list: tiles of up to `tile` pairs of one offset, all levels;
+    //  - the level calls' list: the same pairs cut at level boundaries too, ordered by
+    //    (level, offset), with its tile range per level in lstart.
+    struct Tiles {
+        std::vector<int32_t> d, count;
+        std::vector<int64_t> begin;
+        void add(int dd, int64_t b, int64_t n, int tile) {
+            for (int64_t x = b; x < b + n; x += tile) {
+                d.push_back(dd);
+                begin.push_back(x);
+                count.push_back((int32_t)std::min<int64_t>(tile, b + n - x));
+            }
+        }
+    };
+    void batches(int tile, Tiles& all, Tiles& lvl, std::vector<int64_t>& lstart, std::vector<int64_t>& pe,
+                 std::vector<int32_t>& ps) {
+        const Plan& pl = plan;
+        const size_t nnz = pl.v.nnz();
+        std::vector<int64_t> cnt(317, 0);
+        for (size_t e2 = 0; e2 < nnz; ++e2) cnt[pl.v.aux[e2] + 1]++;
+        for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+        pe.assign(nnz, 0);
+        ps.assign(nnz, 0);
+        std::vector<int64_t> tbox(nnz, 0);
+        std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+        // rows are boxes in order, so pairs of one offset come out ordered by target
+        for (size_t b = 0; b + 1 < pl.v.row.size(); ++b)
+            for (int64_t e2 = pl.v.row[b]; e2 < pl.v.row[b + 1]; ++e2) {
+                int64_t pos = fill[pl.v.aux[e2]]++;
+                pe[pos] = e2;
+                ps[pos] = pl.v.col[e2];
+                tbox[pos] = (int64_t)b;
+            }
+        for (int d = 0; d < 316; ++d) all.add(d, cnt[d], cnt[d + 1] - cnt[d], tile);
+        lstart.assign(pl.nlevels + 1, 0);
+        for (int l = 0; l < pl.nlevels; ++l) {
+            lstart[l] = (int64_t)lvl.d.size();
+            for (int d = 0; d < 316; ++d) {
+                auto b0 = std::lower_bound(tbox.begin() + cnt[d], tbox.begin() + cnt[d + 1], pl.level_start[l]);
+                auto b1 = std::lower_bound(b0, tbox.begin() + cnt[d + 1], pl.level_start[l + 1]);
+                lvl.add(d, b0 - tbox.begin(), b1 - b0, tile);
+            }
+        }
+        lstart[pl.nlevels] = (int64_t)lvl.d.size();
+    }
+
+    void build_m2l_batches(int tile) {
+        Tiles all, lvl;
+        std::vector<int64_t> pe;
+        std::vector<int32_t> ps;
+        batches(tile, all, lvl, lvl_tiles, pe, ps);
+        ntiles = (int64_t)all.d.size();
+        tile_d.upload(all.d);
+        tile_begin.upload(all.begin);
+        tile_count.upload(all.count);
+        ltile_d.upload(lvl.d);
+        ltile_begin.upload(lvl.begin);
+        ltile_count.upload(lvl.count);
+        pair_e.upload(pe);
+        pair_src.upload(ps);
+        // the row of each V entry's product in Y: its position in the offset-sorted list
+        std::vector<int64_t> vp(pe.size());
+        for (size_t pos = 0; pos < pe.size(); ++pos) vp[pe[pos]] = (int64_t)pos;
+        v_pos.upload(vp);
+    }
+
+    void build_parent_lists() {
+        std::vector<int32_t> a;
+        m2m_start.assign(plan.nlevels + 1, 0);
+        for (int l = 0; l < plan.nlevels; ++l) {
+            for (int64_t x = plan.level_start[l]; x < plan.level_start[l + 1]; ++x)
+                if (plan.child_first[x] >= 0 && plan.src_below[x] > 0) a.push_back((int32_t)x);
+            m2m_start[l + 1] = (int64_t)a.size();
+        }
+        m2m_par.upload(a);
+        // octant batches: M2M of level l takes children (level l + 1) with a source, L2L of
+        // level l takes children (level l) with a target; pairs grouped by octant per level
+        std::vector<int32_t> td, tc, ps;
+        std::vector<int64_t> tb, pe;
+        m2m_tiles.assign(plan.nlevels + 1, 0);
+        l2l_tiles.assign(plan.nlevels + 1, 0);
+        auto octant = [&](int64_t c) {
+            return (int)(((plan.idx[3 * c] & 1) << 2) | ((plan.idx[3 * c + 1] & 1) << 1) | (plan.idx[3 * c + 2] & 1));
+        };
+        for (int pass = 0; pass < 2; ++pass) {
+            std::vector<int64_t>& ranges = pass == 0 ? m2m_tiles : l2l_tiles;
+            for (int l = 0; l < plan.nlevels; ++l) {
+                ranges[l] = (int64_t)td.size();
+                const int cl = pass == 0 ? l + 1 : l;  // level of the children
+                if (cl >= plan.nlevels || (pass == 1 && l < 3)) continue;
+                std::vector<std::vector<int64_t>> by(8);
+                for (int64_t c = plan.level_start[cl]; c < plan.level_start[cl + 1]; ++c) {
+                    if (pass == 0 ? plan.src_below[c] == 0 : plan.tgt_below[c] == 0) continue;
+                    by[octant(c)].push_back(c);
+                }
+                for (int o = 0; o < 8; ++o)
+                    for (size_t s0 = 0; s0 < by[o].size(); s0 += kGemmPairs) {
+                        td.push_back(o);
+                        tb.push_back((int64_t)pe.size());
+                        const size_t cnt = std::min<size_t>(kGemmPairs, by[o].size() - s0);
+                        tc.push_back((int32_t)cnt);
+                        for (size_t q = s0; q < s0 + cnt; ++q) {
+                            const int64_t c = by[o][q];
+                            pe.push_back(c);
+                            ps.push_back(pass == 0 ? (int32_t)c : plan.parent[c]);
+                        }
+                    }
+            }
+            ranges[plan.nlevels] = (int64_t)td.size();
+        }
+        oct_tile_d.upload(td);
+        oct_tile_begin.upload(tb);
+        oct_tile_count.upload(tc);
+        oct_pair_e.upload(pe);
+        oct_pair_src.upload(ps);
+        Yo.alloc(sizeof(T) * (size_t)m * ys_of(P) * plan.nboxes());
+    }
+
+    // The near rows' source streams (P2pStream), built when they take at most a quarter of
+    // the free device memory; otherwise the P2P maps its sources per flush (the same floats).
+    void build_p2p_stream() {
+        const size_t nl = plan.nleaves();
+        std::vector<int64_t> rp(nl + 1, 0);
+        for (size_t j = 0; j < nl; ++j) {
+            int64_t S = 0;
+            for (int64_t e = plan.near.row[j]; e < plan.near.row[j + 1]; ++e) {
+                const int sl = plan.near.col[e];
+                S += plan.src_start[sl + 1] - plan.src_start[sl];
+            }
+            rp[j + 1] = rp[j] + (S + 1) / 2;
+        }
+        const size_t pairs = (size_t)rp[nl];
+        const size_t bytes = pairs * (sizeof(float4) + sizeof(float2) + sizeof(int2)) + 8 * (nl + 1);
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        if (dp.nsrc >= ((int64_t)1 << 31) || bytes > free_b / 4) return;
+        st_rowpair.upload(rp);
+        st_xy.alloc(sizeof(float4) * (pairs + 1));
+        st_zz.alloc(sizeof(float2) * (pairs + 1));
+        st_idx.alloc(sizeof(int2) * (pairs + 1));
+        if (nl)
+            near_stream_kernel<<<(unsigned)((nl + 3) / 4), 128>>>(dp, (int64_t)nl, near_rec.as<NearRec>(),
+                                                                  reinterpret_cast<const float4*>(spos.ptr),
+                                                                  st_rowpair.as<int64_t>(), st_xy.as<float4>(),
+                                                                  st_zz.as<float2>(), st_idx.as<int2>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaDeviceSynchronize());
+        p2p_stream_bytes = (int64_t)(st_rowpair.bytes + st_xy.bytes + st_zz.bytes + st_idx.bytes);
+        p2p_path = 1;
+    }
+
+    void set_p2p_path(int path) override {
+        if (path < 0 || path > 1 || (path == 1 && !p2p_stream_bytes))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "P2P path " + std::to_string(path) + " not available");
+        p2p_path = path;
+    }
+
+    void build_p2p_items() {
+        std::vector<int32_t> il;
+        std::vector<int64_t> it;
+        for (size_t j = 0; j < plan.nleaves(); ++j)
+            for (int64_t t = plan.tgt_start[j]; t < plan.tgt_start[j + 1]; t += 32) {
+                il.push_back((int32_t)j);
+                it.push_back(t);
+            }
+        item_lstart.assign(plan.nlevels + 1, (int64_t)il.size());
+        for (int l = plan.nlevels - 1; l >= 0; --l) {
+            int64_t first = plan.leaf_level_start[l];
+            item_lstart[l] = std::lower_bound(il.begin(), il.end(), (int32_t)first) - il.begin();
+        }
+        item_leaf.upload(il);
+        item_t0.upload(it);
+        item_leaf_h = il;
+        items.leaf = item_leaf.as<int32_t>();
+        items.t0 = item_t0.as<int64_t>();
+        items.count = (int64_t)il.size();
+    }
+
+    // The mixed form's f64 pairs: found on the device with the f32 arithmetic of the P2P
+    // kernel itself, then sorted per target (source order) into a CSR.
+    void build_close_pairs(const std::vector<double>& us, const std::vector<double>& ut) {
+        auto up64 = [](DevBuf& b, const std::vector<double>& u) {
+            size_t n = u.size() / 3;
+            std::vector<double4> v(n);
+            for (size_t i = 0; i < n; ++i) v[i] = make_double4(u[3 * i], u[3 * i + 1], u[3 * i + 2], 0.0);
+            b.upload(v);
+        };
+        up64(spos64, us);
+        up64(tpos64, ut);
+        sq64.alloc(sizeof(double) * (size_t)m * (dp.nsrc + 1));
+        int64_t cap = std::max<int64_t>(1 << 20, dp.ntgt * 2);
+        DevBuf cnt, ot, os, ol;
+        cnt.alloc(sizeof(unsigned long long));
+        unsigned long long found = 0;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            ot.alloc(sizeof(int64_t) * cap);
+            os.alloc(sizeof(int64_t) * cap);
+            ol.alloc(sizeof(int32_t) * cap);
+            CUDA_TRY(cudaMemset(cnt.ptr, 0, sizeof(unsigned long long)));
+            if (items.count)
+                close_pairs_kernel<T><<<(unsigned)((items.count + kP2pWarps - 1) / kP2pWarps), 32 * kP2pWarps>>>(
+                    dp, items, (T)kTheta2, spos.as<T4>(), tpos.as<T4>(), cnt.as<unsigned long long>(), cap,
+                    ot.as<int64_t>(), os.as<int64_t>(), ol.as<int32_t>());
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaMemcpy(&found, cnt.ptr, sizeof(found), cudaMemcpyDeviceToHost));
+            if ((int64_t)found <= cap) break;
+            cap = (int64_t)found + 1024;
+        }
+        nclose = (int64_t)found;
+        std::vector<int64_t> ht(nclose), hs(nclose);
+        std::vector<int32_t> hl(nclose);
+        if (nclose) {
+            CUDA_TRY(cudaMemcpy(ht.data(), ot.ptr, sizeof(int64_t) * nclose, cudaMemcpyDeviceToHost));
+            CUDA_TRY(cudaMemcpy(hs.data(), os.ptr, sizeof(int64_t) * nclose, cudaMemcpyDeviceToHost));
+            CUDA_TRY(cudaMemcpy(hl.data(), ol.ptr, sizeof(int32_t) * nclose, cudaMemcpyDeviceToHost));
+        }
+        std::vector<int64_t> order(nclose);
+        for (int64_t i = 0; i < nclose; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+            return ht[a] != ht[b] ? ht[a] < ht[b] : hs[a] < hs[b];
+        });
+        std::vector<int64_t> row(dp.ntgt + 1, 0), src(nclose);
+        std::vector<int32_t> lf(nclose);
+        for (int64_t i = 0; i < nclose; ++i) {
+            row[ht[order[i]] + 1]++;
+            src[i] = hs[order[i]];
+            lf[i] = hl[order[i]];
+        }
+        for (int64_t t = 0; t < dp.ntgt; ++t) row[t + 1] += row[t];
+        close_row.upload(row);
+        close_src.upload(src);
+        close_leaf.upload(lf);
+        close.row = close_row.as<int64_t>();
+        close.src = close_src.as<int64_t>();
+        close.leaf = close_leaf.as<int32_t>();
+        close.spos = spos64.as<double4>();
+        close.tpos = tpos64.as<double4>();
+        close_y.alloc(sizeof(double4) * (size_t)(nclose + 1));
+        close.y = close_y.as<double4>();
+        if (plan.nleaves()) close_map_kernel<<<(unsigned)plan.nleaves(), 64>>>(dp, close, close_y.as<double4>());
+        CUDA_TRY(cudaGetLastError());
+        close.q = sq64.as<double>();
+        const size_t wd = gradients ? 4 : 1;  // doubles a pair / a target and vector
+        close_w.alloc(sizeof(double) * wd * (size_t)(nclose + 1));
+        close_acc.alloc(sizeof(double) * wd * (size_t)m * (dp.ntgt + 1));
+        close.acc = nclose ? close_acc.as<double>() : nullptr;  // no pairs: nothing to add
+        if (plan.nleaves() && nclose) {
+            const auto* s32 = reinterpret_cast<const float4*>(spos.ptr);
+            const auto* t32 = reinterpret_cast<const float4*>(tpos.ptr);
+            if (gradients)
+                close_weights_kernel<true><<<(unsigned)plan.nleaves(), 64>>>(dp, close, s32, t32, kRmax,
+                                                                             close_w.as<double>());
+            else
+                close_weights_kernel<false><<<(unsigned)plan.nleaves(), 64>>>(dp, close, s32, t32, kRmax,
+                                                                              close_w.as<double>());
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    // The near-singular pairs' f64 sums of this pass's charges (mixed form).
+    void close_sums(cudaStream_t s) {
+        if (!kMixed || !nclose || !dp.ntgt) return;
+        const unsigned g = (unsigned)((dp.ntgt + 255) / 256);
+        if (gradients)
+            close_sum_kernel<true><<<counted(g), 256, 0, s>>>(close, close_w.as<double>(), m, dp.nsrc, dp.ntgt,
+                                                             close_acc.as<double>());
+        else
+            close_sum_kernel<false><<<counted(g), 256, 0, s>>>(close, close_w.as<double>(), m, dp.nsrc, dp.ntgt,
+                                                              close_acc.as<double>());
+    }
+
+    int device_status() override {
+        if constexpr (kTensor) {
+            int err = 0;
+            CUDA_TRY(cudaMemcpy(&err, tc_error.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+            return err;
+        }
+        return 0;
+    }
+
+    size_t device_bytes() const {
+        const DevBuf* all[] = {&level, &idx, &parent, &child_first, &box_leaf, &src_below, &tgt_below,
+                               &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
+                               &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
+                               &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
+                               &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e,
+                               &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
+                               &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
+                               &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
+                               &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
+                               &near_phi, &near_g, &box_side, &v_pos, &xbox, &fu_tile_d, &fu_tile_begin,
+                               &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
+                               &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src, &st_rowpair,
+                               &st_xy, &st_zz, &st_idx, &close_w, &close_acc};
+        size_t s = 0;
+        for (auto* b : all) s += b->bytes;
+        return s;
+    }
+
+    // ---- evaluation: every pass, fused where the level structure allows ----
+    void evaluate(const double* d_charges, double* d_phi, double* d_grad) override {
+        if (first_pass) {
+            timer.begin();
+            launches = 0;
+        }
+        // the near-singular sums (mixed) need only the charges: beside the far field on
+        // near_stream, or with the charge load when kinds are timed
+        const bool sums = kMixed && nclose && (kinds & 1) && items.count;
+        // charge load into leaf order
+        timer.run(kLoad, [&] {
+            load_charges(d_charges);
+            if (sums && timer.on) close_sums(stream);
+            // locals of levels 0 and 1 stay zero (no V or L2L reaches them)
+            int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
+            CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, sizeof(T) * (size_t)m * ms_of(P) * top, stream));
+        });
+        if (overlap && !timer.on && kinds == 3 && items.count) {
+            // the near field on near_stream (it needs only the charges) beside the far-field
+            // chain on the evaluator's stream; output_kernel adds them: far + near, the same
+            // addition as the fused P2P epilogue, so the same floats
+            CUDA_TRY(cudaEventRecord(ev_fork, stream));
+            CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
+            close_sums(near_stream);
+            p2p_items(0, items.count, 1, 2, near_phi.as<double>(), gradients ? near_g.as<double>() : nullptr,
+                      near_stream);
+            CUDA_TRY(cudaEventRecord(ev_join, near_stream));
+            run_far();
+            CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
+            output(d_phi, d_grad, true);
+            CUDA_TRY(cudaGetLastError());
+            return;
+        }
+        const bool forked = sums && !timer.on;
+        if (forked) {
+            CUDA_TRY(cudaEventRecord(ev_fork, stream));
+            CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
+            close_sums(near_stream);
+            CUDA_TRY(cudaEventRecord(ev_join, near_stream));
+        }
+        if (!(kinds & 2)) {
+            // far field off: zero partials, then the near field and the output pass only
+            CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
+            CUDA_TRY(cudaMemsetAsync(far_g.ptr, 0, far_g.bytes, stream));
+        } else {
+            run_far();
+        }
+        if (forked) CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
+        if (items.count) timer.run(kP2P, [&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    // Times the launch shapes that change no float (every P2P target and every L2P / M2P
+    // target sums the same terms in the same order whatever the block) on this plan and
+    // device, and keeps the fastest: warps a block of the mixed P2P kernel, threads a block
+    // of the L2P / M2P kernel.  One evaluation first leaves the far partials in place; the
+    // P2P launches with accumulate 0 only read them and rewrite the output, the L2P / M2P
+    // launches rewrite the same partials.  A last evaluation leaves the output and the
+    // launch count as a plain evaluation does.
+    int64_t product_chunks() const override { return (int64_t)chunks.size(); }
+
+    void set_m2l_path(int path) override {
+        if (path < 0 || path > 2 || (path >= 1 && !kTensor) || (path == 2 && !kFusedOk))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "M2L path " + std::to_string(path) + " not available");
+        if (path == 2 && fu_lvl_grid.empty()) {
+            if (m > fused_tile_columns(P))
+                throw Failure(FMMGPU_INVALID_ARGUMENT, "the fused M2L takes at most " +
+                                                           std::to_string(fused_tile_columns(P)) + " vectors a pass");
+            build_fused_m2l();
+        }
+        if (path <= 1) ensure_product_path();
+        m2l_path = path;
+    }
+
+    void autotune(const double* d_charges, double* d_phi, double* d_grad) override {
+        const bool timing = timer.on;
+        timer.on = false;
+        first_pass = true;
+        evaluate(d_charges, d_phi, d_grad);
+        cudaEvent_t e0, e1;
+        CUDA_TRY(cudaEventCreate(&e0));
+        CUDA_TRY(cudaEventCreate(&e1));
+        auto time = [&](auto&& launch) {
+            launch();  // warm-up
+            CUDA_TRY(cudaEventRecord(e0, stream));
+            for (int r = 0; r < 3; ++r) launch();
+            CUDA_TRY(cudaEventRecord(e1, stream));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            return ms;
+        };
+        if (kMixed && items.count) {
+            float best = 0.f;
+            int pick = p2p_warps;
+            for (int w : {1, 2, 4}) {
+                p2p_warps = w;
+                const float ms = time([&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
+                if (w == 1 || ms < best) best = ms, pick = w;
+            }
+            p2p_warps = pick;
+        }
+        if (plan.nleaves() && (kinds & 2)) {
+            float best = 0.f;
+            int pick = leaf_block;
+            for (int b : {32, 64, 128}) {
+                leaf_block = b;
+                const float ms = time([&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+                if (b == 32 || ms < best) best = ms, pick = b;
+            }
+            leaf_block = pick;
+        }
+        CUDA_TRY(cudaEventDestroy(e0));
+        CUDA_TRY(cudaEventDestroy(e1));
+        timer.on = timing;
+        first_pass = true;
+        evaluate(d_charges, d_phi, d_grad);
+    }
+
+    void output(double* d_phi, double* d_grad, bool with_near) {
+        if (plan.nleaves())
+            output_kernel<<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
+                dp, m, far_phi.as<double>(), far_g.as<double>(), with_near ? near_phi.as<double>() : nullptr,
+                with_near && gradients ? near_g.as<double>() : nullptr, d_phi, gradients ? d_grad : nullptr);
+    }
+
+    void run_far() {
+        const int L = plan.nlevels - 1;
+        // upward: P2M of every leaf, then M2M from level L-1 up to 0
+        timer.run(kP2M, [&] { p2m_rows(0, (int64_t)plan.nleaves()); });
+        for (int l = L - 1; l >= 0; --l) timer.run(kM2M, [&] { m2m_level(l); });
+        if (m2l_path == 2) {
+            // downward, fused: per level the L2L part of the locals, then the V products
+            // added into them in row order, then P2L
+            for (int l = 2; l <= L; ++l) {
+                timer.run(kL2L, [&] {
+                    if (l >= 3) l2l_products(l);
+                    reduce_locals(l, l >= 3, 0, 0);
+                });
+                timer.run(kM2L, [&] { m2l_fused(l); });
+                timer.run(kP2L, [&] { p2l_level(l); });
+            }
+            timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+            return;
+        }
+        if (!chunks.empty()) {
+            // downward, chunked: per level the L2L products, then chunk by chunk the M2L
+            // products and the locals (L2L + V in offset order), then P2L
+            for (int l = 2; l <= L; ++l) {
+                timer.run(kL2L, [&] {
+                    if (l >= 3) l2l_products(l);
+                });
+                for (const Chunk& c : chunks) {
+                    if (c.level != l) continue;
+                    timer.run(kM2L, [&] { m2l_chunk(c); });
+                    timer.run(kL2L, [&] { reduce_chunk(c, l >= 3, 1, 0); });
+                }
+                timer.run(kP2L, [&] { p2l_level(l); });
+            }
+            timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+            return;
+        }
+        // M2L products of every level at once (all multipoles are final here)
+        timer.run(kM2L, [&] { m2l_products(-1); });
+        // downward: for l = 2..L: L2L products, the local (L2L + V in offset order), then P2L
+        for (int l = 2; l <= L; ++l) {
+            timer.run(kL2L, [&] {
+                l2l_products(l);
+                reduce_locals(l, l >= 3, 1, 0);
+            });
+            timer.run(kP2L, [&] { p2l_level(l); });
+        }
+        // leaves: L2P + M2P
+        timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
+    }
+
+    // ---- the pieces, shared by the evaluation and the level calls ----
+    void load_charges(const double* d_charges) {
+        const int64_t ns = dp.nsrc;
+        if (ns > 0)
+            charge_load_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
+                d_charges, src_perm.as<int64_t>(), ns, m, qstride, sq.as<T>(), kMixed ? sq64.as<double>() : nullptr);
+    }
+
+    size_t exp_smem() const { return sizeof(T) * (NC * 32 + (size_t)m * 32); }
+
+    void p2m_rows(int64_t r0, int64_t r1) {  // P2M of leaves [r0, r1)
+        if (r1 <= r0) return;
+        if (kBfly && m == 1)
+            expand_bfly_kernel<P, false, false><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
+                dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
+        else if (kBfly)
+            expand_bfly_kernel<P, false, true><<<counted((unsigned)(r1 - r0)), 32, 0, stream>>>(
+                dp, r0, r1, nullptr, reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(M.ptr));
+        else
+            expand_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), 32, exp_smem(), stream>>>(
+                dp, r0, r1, nullptr, m, spos.as<T4>(), sq.as<T>(), M.as<T>());
+    }
+
+    void m2m_level(int l) {  // parents on level l from their children on level l + 1
+        const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
+        const int64_t n = m2m_start[l + 1] - m2m_start[l];
+        if (nt)
+            m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
+                oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0, oct_tile_count.as<int32_t>() + t0,
+                oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m, m2m_tab.as<T>(), M.as<T>(), Yo.as<T>());
+        if (n)
+            m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
+                dp, m2m_par.as<int32_t>() + m2m_start[l], n, m, Yo.as<T>(), M.as<T>());
+    }
+
+    // fused M2L of level l: L += the V products, in row order (after the L2L part)
+    void m2l_fused(int l) {
+        if constexpr (kFusedOk) {
+            const int G = fu_lvl_grid[l];
+            if (G == 0) return;
+            m2l_fused_kernel<P><<<counted((unsigned)G), 32 * kFuWarps, FuShape<P>::SMEM, stream>>>(
+                fu_tile_d.as<int32_t>(), fu_tile_begin.as<int64_t>(), fu_tile_np.as<int32_t>(),
+                fu_cta.as<int64_t>() + fu_lvl_cta[l], fu_pair_src.as<int32_t>(), fu_pair_tgt.as<int32_t>(), m,
+                fu_img.as<uint32_t>(), reinterpret_cast<const float*>(M.ptr), reinterpret_cast<float*>(Lc.ptr),
+                tc_error.as<int>());
+        }
+    }
+
+    // M2L products Y of the V pairs of level l (l < 0: every level in one launch)
+    void m2l_products(int l) {
+        if (kTensor && m2l_path == 1) {
+            if constexpr (kTensor) {
+                const int64_t t0 = l < 0 ? 0 : tc_lvl_tiles[l];
+                const int64_t nt = l < 0 ? tc_ntiles : tc_lvl_tiles[l + 1] - tc_lvl_tiles[l];
+                const DevBuf& td = l < 0 ? tc_tile_d : tc_ltile_d;
+                const DevBuf& tb = l < 0 ? tc_tile_begin : tc_ltile_begin;
+                const DevBuf& tn = l < 0 ? tc_tile_count : tc_ltile_count;
+                if (nt == 0) return;
+                const unsigned grid = (unsigned)std::min<int64_t>(nt, num_sms);
+                m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                    td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt, tc_pair_src.as<int32_t>(),
+                    m, tc_bimg.as<uint32_t>(), mmap, vmap, reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+            }
+            return;
+        }
+        const int64_t t0 = l < 0 ? 0 : lvl_tiles[l];
+        const int64_t nt = l < 0 ? ntiles : lvl_tiles[l + 1] - lvl_tiles[l];
+        const DevBuf& td = l < 0 ? tile_d : ltile_d;
+        const DevBuf& tb = l < 0 ? tile_begin : ltile_begin;
+        const DevBuf& tn = l < 0 ? tile_count : ltile_count;
+        if (nt)
+            m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
+                td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nullptr,
+                pair_src.as<int32_t>(), m, m2l_tab.as<T>(), M.as<T>(), Y.as<T>());
+    }
+
+    void l2l_products(int l) {  // L2L products Yo of the children on level l (l >= 3)
+        const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
+        if (nt)
+            m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
+                oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0, oct_tile_count.as<int32_t>() + t0,
+                oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m, l2l_tab.as<T>(), Lc.as<T>(), Yo.as<T>());
+    }
+
+    void reduce_locals(int l, int with_l2l, int with_v, int accumulate) {
+        reduce_range(plan.level_start[l], plan.level_start[l + 1], with_l2l, with_v, accumulate);
+    }
+
+    void p2l_level(int l) {  // the boxes of level l with an X list
+        const int64_t b0 = xbox_start[l], b1 = xbox_start[l + 1];
+        if (b1 <= b0) return;
+        if (kBfly && m == 1)
+            expand_bfly_kernel<P, true, false><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+                dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
+        else if (kBfly)
+            expand_bfly_kernel<P, true, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+                dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
+        else
+            expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), stream>>>(
+                dp, b0, b1, xbox.as<int32_t>(), m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
+    }
+
+    void leaf_far(int64_t r0, int64_t r1, int mode) {  // L2P / M2P of leaves [r0, r1)
+        if (r1 <= r0) return;
+        const size_t smem = sizeof(T) == 8 ? NC * sizeof(T) : 0;
+        if constexpr (kMixed) {
+            // a warp per P2P work item of these leaves (items are in leaf order); leaf_block
+            // threads a block
+            const int64_t i0 = std::lower_bound(item_leaf_h.begin(), item_leaf_h.end(), (int32_t)r0) - item_leaf_h.begin();
+            const int64_t i1 = std::lower_bound(item_leaf_h.begin(), item_leaf_h.end(), (int32_t)r1) - item_leaf_h.begin();
+            if (i1 <= i0) return;
+            const P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
+            const int wpb = leaf_block / 32;
+            const unsigned g = (unsigned)((it.count + wpb - 1) / wpb);
+            const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
+            const auto* Mf = reinterpret_cast<const float*>(M.ptr);
+            const auto* Lf = reinterpret_cast<const float*>(Lc.ptr);
+            if (!gradients)  // potentials: the harmonics shared by up to 8 vectors (any m: the same floats)
+                leaf_far_mv_items_kernel<P, 8><<<counted(g), leaf_block, 0, stream>>>(dp, it, mode, m, tp, Mf, Lf,
+                                                                                     far_phi.as<double>());
+            else
+                leaf_far_items_kernel<P, true><<<counted(g), leaf_block, 0, stream>>>(
+                    dp, it, mode, m, tp, Mf, Lf, far_phi.as<double>(), far_g.as<double>());
+            return;
+        }
+        if (gradients)
+            leaf_far_kernel<P, T, true><<<counted((unsigned)(r1 - r0)), leaf_block, smem, stream>>>(
+                dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+        else
+            leaf_far_kernel<P, T, false><<<counted((unsigned)(r1 - r0)), leaf_block, smem, stream>>>(
+                dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
+    }
+
+    template <int W>
+    void p2p_x2_launch(const P2pItems& it, int near, int accumulate, double* d_phi, double* fg, double* og,
+                       cudaStream_t s) {
+        const unsigned g = (unsigned)((it.count + W - 1) / W);
+        const auto* sp = reinterpret_cast<const float4*>(spos.ptr);
+        const auto* tp = reinterpret_cast<const float4*>(tpos.ptr);
+        const auto* q = reinterpret_cast<const float*>(sq.ptr);
+        if (p2p_path == 1) {
+            const P2pStream st{st_rowpair.as<int64_t>(), st_xy.as<float4>(), st_zz.as<float2>(), st_idx.as<int2>()};
+            if (!gradients)
+                p2p_st_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, st, q, tp, close,
+                                                                 far_phi.as<double>(), accumulate, d_phi);
+            else
+                p2p_st_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, st, q, tp, close,
+                                                                   far_phi.as<double>(), fg, accumulate, d_phi, og);
+            return;
+        }
+        if (!gradients) {  // potentials: the pair geometry shared by up to kX2Vb vectors (any m)
+            p2p_x2_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, near_rec.as<NearRec>(), sp, q,
+                                                             tp, close, far_phi.as<double>(), accumulate, d_phi);
+            return;
+        }
+        if (gradients)
+            p2p_x2_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, near_rec.as<NearRec>(), sp,
+                                                               q, tp, close, far_phi.as<double>(), fg, accumulate,
+                                                               d_phi, og);
+        else
+            p2p_x2_kernel<false, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, near_rec.as<NearRec>(),
+                                                                sp, q, tp, close, far_phi.as<double>(), fg,
+                                                                accumulate, d_phi, og);
+    }
+
+    // P2P over work items [i0, i1); accumulate = 0 adds the far partial and writes the
+    // scaled output in caller order, 1 adds into the leaf-order store (level calls), 2
+    // writes the near field alone in leaf order into d_phi / d_grad
+    void p2p_items(int64_t i0, int64_t i1, int near, int accumulate, double* d_phi, double* d_grad,
+                   cudaStream_t s = nullptr) {
+        if (i1 <= i0) return;
+        if (!s) s = stream;
+        P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
+        double* fg = gradients ? far_g.as<double>() : nullptr;
+        double* og = gradients ? d_grad : nullptr;
+        if constexpr (kMixed) {
+            if (p2p_warps == 1)
+                p2p_x2_launch<1>(it, near, accumulate, d_phi, fg, og, s);
+            else if (p2p_warps == 2)
+                p2p_x2_launch<2>(it, near, accumulate, d_phi, fg, og, s);
+            else
+                p2p_x2_launch<4>(it, near, accumulate, d_phi, fg, og, s);
+        } else {
+            const unsigned g = (unsigned)((it.count + kP2pWarps - 1) / kP2pWarps);
+            if (gradients)
+                p2p_kernel<T, true><<<counted(g), 32 * kP2pWarps, 0, s>>>(
+                    dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
+                    far_phi.as<double>(), fg, accumulate, d_phi, og);
+            else
+                p2p_kernel<T, false><<<counted(g), 32 * kP2pWarps, 0, s>>>(
+                    dp, it, m, near, (T)kTheta2, spos.as<T4>(), sq.as<T>(), tpos.as<T4>(), close,
+                    far_phi.as<double>(), fg, accumulate, d_phi, og);
+        }
+    }
+
+    // ---- the Helmholtz near field (all leaves' P2P level calls) ----
+    DevBuf hq, hq64;
+    void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) override {
+        if (first_pass) launches = 0;
+        const int64_t ns = dp.nsrc;
+        if (!hq.ptr) {
+            hq.alloc(sizeof(Cplx<T>) * (size_t)m * (ns + 1));
+            if (kMixed) hq64.alloc(sizeof(double2) * (size_t)m * (ns + 1));
+        }
+        if (ns > 0)
+            helm_charge_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
+                d_q, src_perm.as<int64_t>(), ns, m, qstride, hq.as<Cplx<T>>(), kMixed ? hq64.as<double2>() : nullptr);
+        if (items.count) {
+            const unsigned g = (unsigned)((items.count + kHelmWarps - 1) / kHelmWarps);
+            if (gradients)
+                helm_p2p_kernel<T, true, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
+                    dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
+                    hq64.as<double2>(), d_phi, d_grad);
+            else
+                helm_p2p_kernel<T, false, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
+                    dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
+                    hq64.as<double2>(), d_phi, nullptr);
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    // ---- level calls (the FmmOperator trait, fmm-plan/src/operator.rs:434-492) ----
+    void op_begin(const double* d_charges) override {
+        launches = 0;
+        load_charges(d_charges);
+        close_sums(stream);
+        CUDA_TRY(cudaMemsetAsync(Lc.ptr, 0, Lc.bytes, stream));
+        CUDA_TRY(cudaMemsetAsync(far_phi.ptr, 0, far_phi.bytes, stream));
+        CUDA_TRY(cudaMemsetAsync(far_g.ptr, 0, far_g.bytes, stream));
+    }
+
+    void op_level(int kind, int l) override {
+        const int L = plan.nlevels - 1;
+        const int64_t f0 = plan.leaf_level_start[l], f1 = plan.leaf_level_start[l + 1];
+        switch (kind) {
+            case FMMGPU_OP_P2M: p2m_rows(f0, f1); break;
+            case FMMGPU_OP_M2M: if (l < L) m2m_level(l); break;
+            case FMMGPU_OP_L2L:
+                if (l >= 3) {
+                    l2l_products(l);
+                    reduce_locals(l, 1, 0, 1);
+                }
+                break;
+            case FMMGPU_OP_M2L:
+                if (l >= 2 && m2l_path == 2) {
+                    m2l_fused(l);
+                } else if (l >= 2 && !chunks.empty()) {
+                    for (const Chunk& c : chunks)
+                        if (c.level == l) {
+                            m2l_chunk(c);
+                            reduce_chunk(c, 0, 1, 1);
+                        }
+                } else if (l >= 2) {
+                    m2l_products(l);
+                    reduce_locals(l, 0, 1, 1);
+                }
+                break;
+            case FMMGPU_OP_P2L: if (l >= 2) p2l_level(l); break;
+            case FMMGPU_OP_L2P: leaf_far(f0, f1, 5); break;
+            case FMMGPU_OP_M2P: leaf_far(f0, f1, 6); break;
+            case FMMGPU_OP_P2P: p2p_items(item_lstart[l], item_lstart[l + 1], 1, 1, nullptr, nullptr); break;
+            default: throw Failure(FMMGPU_INVALID_ARGUMENT, "unknown operator kind");
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    void op_output(double* d_phi, double* d_grad) override {
+        output(d_phi, d_grad, false);
+        CUDA_TRY(cudaGetLastError());
+    }
+};
+
+template <int P>
+std::unique_ptr<EvaluatorBase> make_evaluator_at(bool mixed, const EvaluatorArgs& a, size_t* bytes) {
+    if (mixed) {
+        auto e = std::make_unique<Evaluator<P, float>>(a.plan, a.m2l, a.m2m, a.l2l, a.stream, a.m, a.gradients, a.us,
+                                                       a.ut, a.fused, a.ybudget);
+        *bytes = e->device_bytes();
+        return e;
+    }
+    auto e = std::make_unique<Evaluator<P, double>>(a.plan, a.m2l, a.m2m, a.l2l, a.stream, a.m, a.gradients, a.us,
+                                                    a.ut, false, a.ybudget);
+    *bytes = e->device_bytes();
+    return e;
+}
+
+}  // namespace fmmb

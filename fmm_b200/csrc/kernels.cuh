@@ -377,11 +377,12 @@ __global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int
                                                             const float* __restrict__ Yo, const float* __restrict__ Yv,
                                                             const int64_t* __restrict__ vpos, float* __restrict__ Lc) {
     constexpr int NC = nc_of(P), YS = ys_of(P), MS = ms_of(P), NQ = (NC + 3) / 4;
-    static_assert(YS % 4 == 0 && MS % 4 == 0 && 4 * NQ <= MS && NQ <= 32, "row layout");
+    static_assert(YS % 4 == 0 && MS % 4 == 0 && 4 * NQ <= MS, "row layout");
     const int64_t b = b0 + (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
-    const int q = threadIdx.x & 31;
-    if (b >= b1 || q >= NQ || plan.tgt_below[b] == 0) return;
+    if (b >= b1 || plan.tgt_below[b] == 0) return;
     const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
+    // lane q holds quads q, q + 32, ... (one pass up to p = 10, two above)
+    for (int q = threadIdx.x & 31; q < NQ; q += 32)
     for (int v = 0; v < m; ++v) {
         float4* out = reinterpret_cast<float4*>(Lc + (b * m + v) * MS) + q;
         float4 s = accumulate ? *out : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -441,6 +442,20 @@ __device__ __forceinline__ void gemm_cp_async(T* smem, const T* gmem, bool valid
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
 }
 
+// Shared memory of the SIMT GEMM: the table (columns as rows, NCP wide) and the tile's
+// source rows, KC input slots at a time.  KC = (p+1)^2 (one staging) where both fit in
+// 200 KB; at higher degree in f64 the input slots are staged in chunks of KC, the
+// accumulators kept in registers across the chunks (the same order of additions).
+template <int P, typename T>
+struct GemmShape {
+    static constexpr int NC = nc_of(P);
+    static constexpr int NCP = 96 > NC ? 96 : ((NC + 15) / 16) * 16;
+    static constexpr int ROW_BYTES = (NCP + kGemmPairs) * (int)sizeof(T);
+    static constexpr int KC_FIT = (200 * 1024) / ROW_BYTES;
+    static constexpr int KC = KC_FIT < NC ? KC_FIT : NC;
+    static constexpr int SMEM = KC * ROW_BYTES;
+};
+
 template <int P, typename T>
 __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict__ tile_d,
                                                        const int64_t* __restrict__ tile_begin,
@@ -449,12 +464,13 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
                                                        const int32_t* __restrict__ pair_src, int m,
                                                        const T* __restrict__ tab, const T* __restrict__ M,
                                                        T* __restrict__ Y) {
-    constexpr int NC = nc_of(P);
-    constexpr int NCP = 96 > NC ? 96 : ((NC + 15) / 16) * 16;
+    using S = GemmShape<P, T>;
+    constexpr int NC = S::NC, NCP = S::NCP, KC = S::KC;
     constexpr int JN = NCP / 16;
+    constexpr bool kOneStage = KC == NC;
     extern __shared__ unsigned char smem_raw[];
-    T* At = reinterpret_cast<T*>(smem_raw);  // [NC][NCP]: At[k][n] = A_d[n][k]
-    T* Xs = At + NC * NCP;                   // [NC][64]:  Xs[k][pair]
+    T* At = reinterpret_cast<T*>(smem_raw);  // [KC][NCP]: At[k][n] = A_d[n][k0 + k]
+    T* Xs = At + KC * NCP;                   // [KC][64]:  Xs[k][pair]
     const int tile = blockIdx.x;
     const int d = tile_d[tile];
     const int64_t p0 = tile_begin[tile];
@@ -463,38 +479,45 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
     // staging by asynchronous copies (every copy of the block in flight at once; padding
     // zero-filled): the table, then each vector's source rows once the tile's sources are
     // known; 256 threads
-    constexpr int SA = NC * NCP, SX = NC * kGemmPairs;
     __shared__ int32_t srcs[kGemmPairs];
     if (threadIdx.x < kGemmPairs) srcs[threadIdx.x] = threadIdx.x < cnt ? pair_src[p0 + threadIdx.x] : 0;
-    for (int t = threadIdx.x; t < SA; t += 256) {
-        const int k = t / NCP, n = t % NCP;
-        gemm_cp_async<T>(At + t, A + (int64_t)k * NC + (n < NC ? n : 0), n < NC);
-    }
+    auto stage_table = [&](int k0, int kc) {
+        for (int t = threadIdx.x; t < kc * NCP; t += 256) {
+            const int k = t / NCP, n = t % NCP;
+            gemm_cp_async<T>(At + t, A + (int64_t)(k0 + k) * NC + (n < NC ? n : 0), n < NC);
+        }
+    };
+    if (kOneStage) stage_table(0, NC);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int v = 0; v < m; ++v) {
-        __syncthreads();  // srcs written; the previous vector's Xs read
-        for (int t = threadIdx.x; t < SX; t += 256) {
-            const int pr = t / NC, k = t % NC;
-            gemm_cp_async<T>(Xs + k * kGemmPairs + pr, M + ((int64_t)srcs[pr] * m + v) * ms_of(P) + k, pr < cnt);
-        }
-        asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
-        __syncthreads();
         T acc[4][JN];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < JN; ++j) acc[i][j] = T(0);
+        for (int k0 = 0; k0 < NC; k0 += KC) {
+            const int kc = NC - k0 < KC ? NC - k0 : KC;
+            __syncthreads();  // srcs written; the previous chunk's or vector's staging read
+            if (!kOneStage) stage_table(k0, kc);
+            for (int t = threadIdx.x; t < kc * kGemmPairs; t += 256) {
+                const int pr = t / kc, k = t % kc;
+                gemm_cp_async<T>(Xs + k * kGemmPairs + pr, M + ((int64_t)srcs[pr] * m + v) * ms_of(P) + k0 + k,
+                                 pr < cnt);
+            }
+            asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
+            __syncthreads();
 #pragma unroll 3
-        for (int k = 0; k < NC; ++k) {
-            T xv[4], av[JN];
+            for (int k = 0; k < kc; ++k) {
+                T xv[4], av[JN];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) xv[i] = Xs[k * kGemmPairs + ty * 4 + i];
+                for (int i = 0; i < 4; ++i) xv[i] = Xs[k * kGemmPairs + ty * 4 + i];
 #pragma unroll
-            for (int j = 0; j < JN; ++j) av[j] = At[k * NCP + tx + 16 * j];
+                for (int j = 0; j < JN; ++j) av[j] = At[k * NCP + tx + 16 * j];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < JN; ++j) acc[i][j] += av[j] * xv[i];
+                    for (int j = 0; j < JN; ++j) acc[i][j] += av[j] * xv[i];
+            }
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -791,9 +814,10 @@ struct P2pItems {
 // block per leaf holds every thread of its block while a leaf of few targets keeps one
 // warp busy, a warp per item leaves no idle warp resident.  leaf_far_mv_items_kernel forms
 // each target's harmonics once for up to VB vectors (l2p_eval_mv / m2p_eval_mv).
-// The gradient form is held to 96 registers (21 warps an SM, no spills).
+// The gradient form is held to 96 registers up to p = 8 (21 warps an SM, no spills), to
+// 168 at p = 9, 10 and 255 above (the harmonic rows and the coefficient loop grow with p).
 template <int P, bool GRAD>
-__global__ void __launch_bounds__(128, 5) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
+__global__ void __launch_bounds__(128, P <= 8 ? 5 : P <= 10 ? 3 : 2) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
                                                              const float4* __restrict__ tpos,
                                                              const float* __restrict__ M, const float* __restrict__ Lc,
                                                              double* __restrict__ far_phi, double* __restrict__ far_g) {
@@ -911,7 +935,7 @@ struct ClosePairs {  // near-singular pairs of the mixed form, CSR by target (le
 // Build time (mixed form): each near-singular pair's source point mapped into its target
 // leaf's frame in f64, y = fma(r, u, c) with the exact relative frame (the identity for the
 // leaf itself), as the evaluation would form it.  Block per leaf.
-__global__ void close_map_kernel(DevPlan plan, ClosePairs close, double4* __restrict__ y) {
+static __global__ void close_map_kernel(DevPlan plan, ClosePairs close, double4* __restrict__ y) {
     const int64_t leaf = blockIdx.x;
     const int box = plan.leaf_box[leaf];
     for (int64_t t = plan.tgt_start[leaf] + threadIdx.x; t < plan.tgt_start[leaf + 1]; t += blockDim.x)
@@ -1045,7 +1069,7 @@ __global__ void __launch_bounds__(128) p2p_kernel(DevPlan plan, P2pItems items, 
 // near field was summed apart (near_phi non-null), else the store as it is (level calls).
 // Block per leaf; the same expressions as the P2P kernels' fused output, so all of them
 // give the same floats.
-__global__ void output_kernel(DevPlan plan, int m, const double* __restrict__ far_phi,
+static __global__ void output_kernel(DevPlan plan, int m, const double* __restrict__ far_phi,
                               const double* __restrict__ far_g, const double* __restrict__ near_phi,
                               const double* __restrict__ near_g, double* __restrict__ out_phi,
                               double* __restrict__ out_g) {

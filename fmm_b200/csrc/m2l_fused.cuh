@@ -86,8 +86,19 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  : "memory");
 }
 
-// tile columns (pairs x charge vectors) of the fused kernel for the compiled degrees
-inline int fused_tile_columns(int p) { return p == 3 ? FuShape<3>::NT : p == 6 ? FuShape<6>::NT : FuShape<8>::NT; }
+// tile columns (pairs x charge vectors) of the fused kernel at degree p; 0 where it does
+// not apply (p > 8: tensor memory holds two tables only up to KP = 96)
+inline int fused_tile_columns(int p) {
+    switch (p) {
+        case 3: return FuShape<3>::NT;
+        case 4: return FuShape<4>::NT;
+        case 5: return FuShape<5>::NT;
+        case 6: return FuShape<6>::NT;
+        case 7: return FuShape<7>::NT;
+        case 8: return FuShape<8>::NT;
+        default: return 0;
+    }
+}
 
 template <int P>
 __global__ void __launch_bounds__(32 * kFuWarps, 1) m2l_fused_kernel(

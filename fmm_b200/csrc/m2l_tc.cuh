@@ -167,9 +167,10 @@ struct TcTs {
     static constexpr int KA = (NC + 31) / 32;
     static constexpr int KP = 32 * KA;             // padded K (input slots)
     static constexpr int KSTEPS = KP / 8;
-    // columns per tile (UMMA N): 96 at p = 8, where shared memory then holds two raw
-    // stages (measured faster than 64 columns with four)
-    static constexpr int NT = KP > 64 ? 96 : 128;
+    // columns per tile (UMMA N): 96 at p = 7, 8 (KP = 96), where shared memory then holds
+    // two raw stages (measured faster than 64 columns with four); 64 at p = 9, 10
+    // (KP = 128), the most beside two X stages and two raw stages
+    static constexpr int NT = KP > 96 ? 64 : KP > 64 ? 96 : 128;
     static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage (also one raw stage)
     // raw stages: as many as shared memory holds beside the two X stages, at most 4 (the
     // copy engine's loads take several tiles' time to land)
@@ -529,8 +530,24 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     }
 }
 
-// columns (pairs x vectors) of a tensor-core M2L tile for the compiled degrees
-inline int tc_tile_columns(int p) { return p == 3 ? TcTs<3>::NT : p == 6 ? TcTs<6>::NT : TcTs<8>::NT; }
+// columns (pairs x vectors) of a tensor-core M2L tile at degree p; 0 where the
+// tensor-core M2L does not apply ((p+1)^2 > 128 output slots)
+inline int tc_tile_columns(int p) {
+    switch (p) {
+        case 0: return TcTs<0>::NT;
+        case 1: return TcTs<1>::NT;
+        case 2: return TcTs<2>::NT;
+        case 3: return TcTs<3>::NT;
+        case 4: return TcTs<4>::NT;
+        case 5: return TcTs<5>::NT;
+        case 6: return TcTs<6>::NT;
+        case 7: return TcTs<7>::NT;
+        case 8: return TcTs<8>::NT;
+        case 9: return TcTs<9>::NT;
+        case 10: return TcTs<10>::NT;
+        default: return 0;
+    }
+}
 
 // Host: the tensor map of the multipoles for the gathers: 2D, rows (box * m + vector) of
 // ms_of(P) f32 (16-byte multiples), the inner extent (p+1)^2 so that a box of KP slots

@@ -35,7 +35,7 @@ struct __align__(16) NearRec {
 };
 
 // Build time: one record per near-list entry (row = target leaf).
-__global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec* __restrict__ rec) {
+static __global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec* __restrict__ rec) {
     const int64_t leaf = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (leaf >= nleaves) return;
     const int box = plan.leaf_box[leaf];
@@ -572,7 +572,7 @@ struct P2pStream {
 };
 
 // Build time: warp per leaf row, writing that row's pairs.
-__global__ void near_stream_kernel(DevPlan plan, int64_t nleaves, const NearRec* __restrict__ recs,
+static __global__ void near_stream_kernel(DevPlan plan, int64_t nleaves, const NearRec* __restrict__ recs,
                                    const float4* __restrict__ spos, const int64_t* __restrict__ row_pair,
                                    float4* __restrict__ xy_out, float2* __restrict__ zz_out,
                                    int2* __restrict__ idx_out) {

@@ -325,8 +325,12 @@ int fmmgpu_helmholtz_near(fmmgpu_fmm* fmm, double k_re, double k_im, const doubl
  * Calls share that one scratch: two calls in flight at once on one device (different
  * streams, or threads without ordering) race on it and give wrong results.  Calls
  * queued one after another on one stream are safe.  The first call on each device does
- * one-time setup (cudaSetDevice and the lookup of the scratch address, which may load
- * the library's module there): make that call before any stream capture begins. */
+ * one-time setup (the lookup of the scratch address, which may load the library's module
+ * there): make that call before any stream capture begins.  The address is cached for the
+ * life of the process, so do not reset a device (cudaDeviceReset) and then call again.
+ * The calling thread's current device is restored before the call returns.  A CUDA
+ * error left pending by earlier work on the thread is reported (FMMGPU_DEVICE_ERROR, not
+ * cleared) and nothing is launched. */
 #define FMMGPU_DIRECT_NOALLOC_SCRATCH_BYTES (16u << 20)
 int fmmgpu_direct_sum_noalloc(size_t nsources, const double* sources, const double* charges, size_t ntargets,
                               const double* targets, double* potential, double* gradient, int device,

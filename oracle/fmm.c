@@ -292,40 +292,68 @@ int orc_fmm(size_t ns, const double *src, const double *q, int m, size_t nt, con
     return orc_fmm_kinds(ns, src, q, m, nt, tgt, p, max_keys, gradients, threads, 3, phi_out, grad_out);
 }
 
-int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
-                  int p, int max_keys, int gradients, int threads, int kinds, double *phi_out,
-                  double *grad_out) {
+/* A built oracle FMM: the plan and the f64 tables, kept for repeated evaluations (the
+ * reference's Fmm, fmm-exec/src/fmm.rs:1853 build then :3691 evaluate). */
+struct orc_fmm_handle {
+    plan_t PL;
+    int p, m, gradients;
+    size_t ns, nt;
+    double *m2l_t, *m2m_t, *l2l_t;
+};
+
+orc_fmm_handle *orc_fmm_new(size_t ns, const double *src, size_t nt, const double *tgt, int p, int max_keys,
+                            int m, int gradients) {
+    orc_fmm_handle *h = (orc_fmm_handle *)calloc(1, sizeof(orc_fmm_handle));
+    int nc = (p + 1) * (p + 1);
+    plan_setup(&h->PL, ns, src, nt, tgt, max_keys);
+    h->p = p;
+    h->m = m;
+    h->gradients = gradients;
+    h->ns = ns;
+    h->nt = nt;
+    h->m2l_t = (double *)malloc((size_t)316 * nc * nc * sizeof(double));
+    h->m2m_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
+    h->l2l_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
+    orc_build_m2l_tables(p, h->m2l_t);
+    orc_build_m2m_tables(p, h->m2m_t);
+    orc_build_l2l_tables(p, h->l2l_t);
+    return h;
+}
+
+void orc_fmm_free(orc_fmm_handle *h) {
+    if (!h) return;
+    free(h->m2l_t);
+    free(h->m2m_t);
+    free(h->l2l_t);
+    plan_free(&h->PL);
+    free(h);
+}
+
+/* One evaluation of a built FMM: charges q[i][v] in caller order, outputs in caller order
+ * (phi[v][nt], grad[v][nt][3]); kinds bit 0 the near field, bit 1 the far field.  Its
+ * wall time is orc_fmm_last_eval_seconds(). */
+int orc_fmm_eval(orc_fmm_handle *h, const double *q, int threads, int kinds, double *phi_out, double *grad_out) {
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #else
     (void)threads;
 #endif
-    int nc = (p + 1) * (p + 1);
-    plan_t PL;
-    plan_setup(&PL, ns, src, nt, tgt, max_keys);
     const double t_start = omp_get_wtime();
+    const int p = h->p, m = h->m, gradients = h->gradients;
+    const size_t ns = h->ns, nt = h->nt;
+    int nc = (p + 1) * (p + 1);
+    const plan_t PL = h->PL;
     boxes_t B = PL.B;
-    const double *lower = PL.lower;
     const double side = PL.side;
-    (void)lower;
     size_t nleaves = PL.nleaves;
     long *leaf_of_box = PL.leaf_of_box;
     size_t *leaf_box = PL.leaf_box, *s_off = PL.s_off, *t_off = PL.t_off, *t_perm = PL.t_perm, *s_perm = PL.s_perm;
     double *us = PL.us, *ut = PL.ut;
+    const double *m2l_t = h->m2l_t, *m2m_t = h->m2m_t, *l2l_t = h->l2l_t;
     /* charges in leaf order */
     double *qs = (double *)malloc((ns * m + 1) * sizeof(double));
     for (size_t a = 0; a < ns; ++a)
         for (int v = 0; v < m; ++v) qs[a * m + v] = q[s_perm[a] * m + v];
-
-    /* tables */
-    double *m2l_t = (double *)malloc((size_t)316 * nc * nc * sizeof(double));
-    double *m2m_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
-    double *l2l_t = (double *)malloc((size_t)8 * nc * nc * sizeof(double));
-    const double t_tab0 = omp_get_wtime();
-    orc_build_m2l_tables(p, m2l_t);
-    orc_build_m2m_tables(p, m2m_t);
-    orc_build_l2l_tables(p, l2l_t);
-    const double t_tab1 = omp_get_wtime();
 
     double *M = (double *)calloc(B.nboxes * m * nc, sizeof(double));
     double *Lc = (double *)calloc(B.nboxes * m * nc, sizeof(double));
@@ -479,12 +507,22 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
         }
     }
 
-    g_eval_seconds = (omp_get_wtime() - t_start) - (t_tab1 - t_tab0);
+    g_eval_seconds = omp_get_wtime() - t_start;
     free(M); free(Lc); free(phi); free(grad);
-    free(m2l_t); free(m2m_t); free(l2l_t);
     free(qs);
-    plan_free(&PL);
     return 0;
+}
+
+int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t nt, const double *tgt,
+                  int p, int max_keys, int gradients, int threads, int kinds, double *phi_out,
+                  double *grad_out) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+    orc_fmm_handle *h = orc_fmm_new(ns, src, nt, tgt, p, max_keys, m, gradients);
+    int rc = orc_fmm_eval(h, q, threads, kinds, phi_out, grad_out);
+    orc_fmm_free(h);
+    return rc;
 }
 
 /* The Helmholtz near field on the plan (see helmholtz.c for the term): charges q[i][v]

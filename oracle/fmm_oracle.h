@@ -133,6 +133,15 @@ int orc_fmm_kinds(size_t ns, const double *src, const double *q, int m, size_t n
                   const double *tgt, int p, int max_keys, int gradients, int threads, int kinds,
                   double *phi, double *grad);
 
+/* A built FMM kept for repeated evaluations (plan and tables once, the reference's
+ * FmmBuilder::build then Fmm::evaluate): orc_fmm_eval takes caller-order charges q[i][v]
+ * and writes caller-order outputs as orc_fmm; its wall time is orc_fmm_last_eval_seconds(). */
+typedef struct orc_fmm_handle orc_fmm_handle;
+orc_fmm_handle *orc_fmm_new(size_t ns, const double *src, size_t nt, const double *tgt, int p, int max_keys,
+                            int m, int gradients);
+int orc_fmm_eval(orc_fmm_handle *h, const double *q, int threads, int kinds, double *phi, double *grad);
+void orc_fmm_free(orc_fmm_handle *h);
+
 /* Helmholtz (helmholtz.c): complex values are (re, im) double pairs.  p2p and the
  * Neumaier direct sum of e^{ikr}/r (no 1/(4 pi)), potential[nt] and gradient[nt][3]
  * complex, += into the outputs */

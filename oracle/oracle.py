@@ -69,6 +69,9 @@ def lib():
             "orc_fmm_kinds": (C.c_int, [_sz, _dp, _dp, C.c_int, _sz, _dp, C.c_int, C.c_int, C.c_int,
                                         C.c_int, C.c_int, _dp, C.c_void_p]),
             "orc_fmm_last_eval_seconds": (C.c_double, []),
+            "orc_fmm_new": (C.c_void_p, [_sz, _dp, _sz, _dp, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "orc_fmm_eval": (C.c_int, [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_void_p]),
+            "orc_fmm_free": (None, [C.c_void_p]),
             "orc_helmholtz_p2p": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_helmholtz_direct_sum": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp,
                                                 C.c_void_p]),
@@ -432,6 +435,33 @@ def fmm(src, q, tgt, p, max_keys, gradients=True, threads=0, kinds=3):
     return phi.reshape(m, len(tgt)), (g.reshape(m, len(tgt), 3) if gradients else None)
 
 
+class Fmm:
+    """A built oracle FMM (plan and tables once) for repeated evaluations, as the
+    reference's FmmBuilder::build then Fmm::evaluate; evaluate() returns what fmm() does."""
+
+    def __init__(self, src, tgt, p, max_keys, gradients=True, vectors=1):
+        self.src = np.ascontiguousarray(src, dtype=np.float64)
+        self.tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+        self.m, self.gradients = vectors, gradients
+        self._h = lib().orc_fmm_new(len(self.src), self.src, len(self.tgt), self.tgt, p, max_keys, vectors,
+                                    int(gradients))
+
+    def evaluate(self, q, threads=0, kinds=3):
+        q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(len(self.src), self.m))
+        nt = len(self.tgt)
+        phi = np.zeros(self.m * nt)
+        g = np.zeros(3 * self.m * nt) if self.gradients else None
+        rc = lib().orc_fmm_eval(self._h, q, threads, kinds, phi, _ptr(g))
+        if rc != 0:
+            raise RuntimeError(f"oracle fmm failed: {rc}")
+        return phi.reshape(self.m, nt), (g.reshape(self.m, nt, 3) if self.gradients else None)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_fmm_free(self._h)
+            self._h = None
+
+
 class Tree:
     """The oracle's octree (refine + 2:1 balance) and its brute-force list rule."""
 
@@ -476,3 +506,28 @@ def point_sets(kind, n, seed):
     L.orc_charges.argtypes = [C.c_void_p, _sz, _dp]
     L.orc_charges(C.byref(st), n, q)
     return xyz.reshape(n, 3), q
+
+
+REFERENCE_BENCH_SEED = 0x00BE9C06
+
+
+def bench_problem(n, sampled=1000, seed=REFERENCE_BENCH_SEED):
+    """The reference's own benchmark problem (fmm-bench/src/measure.rs:34-66, Problem::new):
+    from one SplitMix64 stream, N points uniform in [0, 1)^3 (points::cube about (1/2, 1/2,
+    1/2) with half-width 1/2, fmm-validate/src/points.rs:28-32), then N charges U[-1, 1)
+    (points.rs:138-140), then the sampled targets by a partial Fisher-Yates shuffle
+    (measure.rs:49-56).  Returns (points (n, 3), charges (n,), sample (sampled,) int64)."""
+    L = lib()
+    st = C.c_uint64(seed)
+    xyz = np.zeros(3 * n)
+    f = L.orc_points_cube
+    f.argtypes = [C.c_void_p, _sz, _dp, C.c_double, _dp]
+    f(C.byref(st), n, np.array([0.5, 0.5, 0.5]), 0.5, xyz)
+    q = np.zeros(n)
+    L.orc_charges.argtypes = [C.c_void_p, _sz, _dp]
+    L.orc_charges(C.byref(st), n, q)
+    sampled = min(sampled, n)
+    out = np.zeros(max(sampled, 1), dtype=np.uint32)
+    L.orc_sample.argtypes = [C.c_void_p, _sz, _sz, _u32p]
+    L.orc_sample(C.byref(st), n, sampled, out)
+    return xyz.reshape(n, 3), q, out[:sampled].astype(np.int64)

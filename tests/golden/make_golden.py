@@ -75,6 +75,8 @@ def helmholtz(ref):
 
 
 if __name__ == "__main__":
-    reference = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    reference = sys.argv[1]
     main(reference)
     helmholtz(reference)

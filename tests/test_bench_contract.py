@@ -22,7 +22,9 @@ def test_reference_arm_line():
                 "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
-    assert line["config"] == bench.headline_config(bench.N_DEFAULT, 1)
+    # the config names the N actually timed (the headline's own N by default)
+    assert line["config"] == bench.headline_config(20000, 1) and line["config"]["n_points"] == 20000
+    assert line["ms_per_step"] > 0 and abs(20000 / (line["ms_per_step"] * 1e-3) / 1e6 - line["value"]) < 1e-3 * line["value"] + 1e-3
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and "N=20000" in cb["sample"] and cb["value"] == line["value"]
     e = line["e2e"]
@@ -37,3 +39,14 @@ def test_passes_hbm_figures():
     assert out["m2m"]["bytes"] == 2 * 1000 * nc * 4
     assert abs(out["m2m"]["gbs"] - out["m2m"]["bytes"] / 0.25e-3 / 1e9) < 0.1
     assert out["peak_gbs"] == 6000.0 and 0 < out["l2p_m2p"]["frac"] < 1
+
+
+def test_cpu_baseline_is_a_median_of_five():
+    class A:
+        cpu_n = 20000
+
+    b = bench.cpu_baseline(A())
+    assert len(b["evaluations_s"]) == bench.CPU_REPEATS >= 5 and b["n_points"] == 20000
+    import numpy as np
+
+    assert abs(b["value"] - 20000 / float(np.median(b["evaluations_s"])) / 1e6) < 0.02 * b["value"]

@@ -178,3 +178,16 @@ def test_p2p_in_vector_lanes_equals_the_scalar_loop(oracle):
             f(ns, src, q, len(tgt), tgt, phi, g.ctypes.data_as(ctypes.c_void_p))
             out.append((phi, g))
         assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_reference_bench_problem_error(oracle):
+    """The reference's benchmark problem (fmm-bench/src/measure.rs:34-66: seed 0x00be9c06,
+    N = 1e5 in [0, 1)^3, p = 6, 64 per leaf) gives its published error, 1.42e-4 relative
+    L2 of phi at the 1,000 sampled targets (fmm-bench/results/phase4s-gh200.md:101)."""
+    x, q, sample = oracle.bench_problem(100_000, 1000)
+    assert len(sample) == 1000 and len(set(sample.tolist())) == 1000
+    phi, _ = oracle.fmm(x, q, x, 6, 64, gradients=False, threads=8)
+    d, _ = oracle.direct_sum(x, q, x[sample], gradients=False)
+    d /= 4 * np.pi
+    err = float(np.linalg.norm(phi[0][sample] - d) / np.linalg.norm(d))
+    assert abs(err - 1.42e-4) < 0.005e-4, err
