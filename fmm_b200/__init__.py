@@ -83,6 +83,9 @@ def lib():
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_helmholtz_near": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
+            "fmmgpu_helmholtz_evaluate": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
+            "fmmgpu_helmholtz_evaluate_device": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
+            "fmmgpu_helmholtz_table_seconds": (C.c_double, [vp]),
             "fmmgpu_helmholtz_m2l_tables": (C.c_int, [C.c_int, C.c_double, C.c_double, dp]),
             "fmmgpu_helmholtz_octant_tables": (C.c_int, [C.c_int, C.c_double, C.c_double, dp, dp]),
             "fmmgpu_op_begin_evaluation": (C.c_int, [vp, dp]),
@@ -341,6 +344,28 @@ class Fmm(Plan):
         k = complex(k)
         _check(lib().fmmgpu_helmholtz_near(self._h, k.real, k.imag, _ptr(q), _ptr(phi), _ptr(g)))
         return Output(phi, g)
+
+    def helmholtz_evaluate(self, k, charges):
+        """The whole Helmholtz FMM of e^{ikr}/(4 pi r) for a real k > 0 (near and far field)
+        on this FMM's tree and lists, complex charges (ns, m): Output with complex potential
+        (m, nt) and gradient (m, nt, 3).  The tables of a new k are built on the first call."""
+        m = self.settings.vectors
+        q = np.ascontiguousarray(charges, dtype=np.complex128).reshape(self.nsources, m)
+        phi = np.zeros((m, self.ntargets), dtype=np.complex128)
+        g = np.zeros((m, self.ntargets, 3), dtype=np.complex128) if self.settings.gradients else None
+        k = complex(k)
+        _check(lib().fmmgpu_helmholtz_evaluate(self._h, k.real, k.imag, _ptr(q), _ptr(phi), _ptr(g)))
+        return Output(phi, g)
+
+    def helmholtz_evaluate_device(self, k, charges_ptr, potential_ptr, gradient_ptr=None):
+        """The Helmholtz FMM on device buffers (pointers) on the evaluator's stream; no sync."""
+        k = complex(k)
+        _check(lib().fmmgpu_helmholtz_evaluate_device(self._h, k.real, k.imag, C.c_void_p(charges_ptr),
+                                                      C.c_void_p(potential_ptr),
+                                                      C.c_void_p(gradient_ptr) if gradient_ptr else None))
+
+    def helmholtz_table_seconds(self):
+        return float(lib().fmmgpu_helmholtz_table_seconds(self._h))
 
     def vjp(self, charges, cotangent):
         """Vector-Jacobian product of the potentials for the cotangent w (shape (m, nt)):

@@ -80,6 +80,7 @@ struct fmmgpu_fmm {
     std::vector<double> src_pts, tgt_pts;
     fmmgpu_fmm* transpose = nullptr;
     DevBuf d_vjp_w, d_vjp_tq, d_vjp_dq, d_vjp_dxs, d_vjp_dxt;
+    DevBuf d_hq, d_hphi, d_hg;  // the Helmholtz host call's device buffers
 };
 
 namespace fmmb {
@@ -571,6 +572,57 @@ int fmmgpu_helmholtz_near(fmmgpu_fmm* f, double k_re, double k_im, const double*
         CUDA_TRY(cudaStreamSynchronize(f->stream));
     });
 }
+
+int fmmgpu_helmholtz_evaluate_device(fmmgpu_fmm* f, double k_re, double k_im, const double* charges,
+                                     double* potential, double* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        if (!std::isfinite(k_re) || !std::isfinite(k_im))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "the wavenumber must be finite");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors;
+        const size_t nt = f->plan.tgt_perm.size();
+        for (int v0 = 0; v0 < (int)m; v0 += f->mpass) {
+            f->eval->first_pass = v0 == 0;
+            f->eval->helmholtz_fmm(k_re, k_im, charges + 2 * v0, potential + 2 * (size_t)v0 * nt,
+                                   f->settings.gradients ? gradient + 6 * (size_t)v0 * nt : nullptr);
+        }
+        f->eval->first_pass = true;
+    });
+}
+
+int fmmgpu_helmholtz_evaluate(fmmgpu_fmm* f, double k_re, double k_im, const double* charges, double* potential,
+                              double* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const size_t m = f->settings.vectors;
+        const size_t ns = f->plan.src_perm.size(), nt = f->plan.tgt_perm.size();
+        if (f->d_hq.bytes < sizeof(double) * 2 * m * (ns + 1)) {
+            f->d_hq.alloc(sizeof(double) * 2 * m * (ns + 1));
+            f->d_hphi.alloc(sizeof(double) * 2 * m * (nt + 1));
+            if (f->settings.gradients) f->d_hg.alloc(sizeof(double) * 6 * m * (nt + 1));
+        }
+        CUDA_TRY(cudaMemcpyAsync(f->d_hq.ptr, charges, sizeof(double) * 2 * m * ns, cudaMemcpyHostToDevice,
+                                 f->stream));
+        const int rc = fmmgpu_helmholtz_evaluate_device(f, k_re, k_im, f->d_hq.as<double>(), f->d_hphi.as<double>(),
+                                                        f->settings.gradients ? f->d_hg.as<double>() : nullptr);
+        if (rc != FMMGPU_OK) throw Failure(rc, g_last_error);
+        CUDA_TRY(cudaMemcpyAsync(potential, f->d_hphi.ptr, sizeof(double) * 2 * m * nt, cudaMemcpyDeviceToHost,
+                                 f->stream));
+        if (f->settings.gradients)
+            CUDA_TRY(cudaMemcpyAsync(gradient, f->d_hg.ptr, sizeof(double) * 6 * m * nt, cudaMemcpyDeviceToHost,
+                                     f->stream));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    });
+}
+
+double fmmgpu_helmholtz_table_seconds(const fmmgpu_fmm* f) { return f && f->eval ? f->eval->hh_table_seconds : 0.0; }
 
 int fmmgpu_op_begin_evaluation(fmmgpu_fmm* f, const double* charges) {
     return guarded([&] {

@@ -143,6 +143,11 @@ struct EvaluatorBase {
     virtual void op_level(int kind, int level) = 0;
     virtual void op_output(double* d_phi, double* d_grad) = 0;
     virtual void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
+    // the whole Helmholtz FMM for a real wavenumber (near and far field), device buffers:
+    // complex charges [i][v] (qstride vectors a point), outputs [v][i] and [v][i][3] complex
+    virtual void helmholtz_fmm(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
+    // host seconds spent building the Helmholtz tables of the last new wavenumber
+    double hh_table_seconds = 0.0;
     virtual void autotune(const double* d_charges, double* d_phi, double* d_grad) = 0;
     virtual void set_m2l_path(int path) = 0;
     virtual void set_p2p_path(int path) = 0;

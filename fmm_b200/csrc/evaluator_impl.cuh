@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,7 @@
 
 #include "evaluator_base.hpp"
 #include "helmholtz.cuh"
+#include "helmholtz_far.cuh"
 #include "kernels.cuh"
 #include "m2l_fused.cuh"
 #include "m2l_tc.cuh"
@@ -23,6 +25,15 @@
 namespace fmmb {
 
 static_assert(kX2Warps == 4, "EvaluatorBase::p2p_warps starts at the mixed P2P's static block");
+
+// The Helmholtz FMM's state in an evaluator: complex multipoles and locals (row pairs), the
+// translation products, the per-level tables of one wavenumber, the far partials.
+struct HhState {
+    double k = -1.0;  // the wavenumber of the tables held
+    DevBuf M, L, Y, Yo, m2l, m2m, l2l, far_phi, far_g;
+    HhLevels lv{};
+    bool built = false;
+};
 
 // ----------------------------------------------------------------------------------
 // The evaluator of one precision T and one degree P.
@@ -55,10 +66,11 @@ struct Evaluator final : EvaluatorBase {
     // the same pairs in per-level tiles, for the level calls
     DevBuf ltile_d, ltile_begin, ltile_count;
     std::vector<int64_t> lvl_tiles;
-    // tensor-core M2L (mixed form, (p+1)^2 <= 128 output slots: p <= 10): tiles of
-    // TcTs<P>::NT columns and the table images; the fused form needs p <= 8 (tensor memory
-    // holds two tables there)
-    static constexpr bool kTensor = sizeof(T) == 4 && P <= 10;
+    // tensor-core M2L (mixed form, p <= 12; above p = 10 in two output-slot halves):
+    // tiles of TcTs<P>::NT columns and the table images; the fused form needs p <= 8
+    // (tensor memory holds two tables there)
+    static constexpr bool kTensor = sizeof(T) == 4 && P <= 12;
+    static constexpr int kTcHalves = kTensor ? TcTs<P>::H : 1;
     static constexpr bool kFusedOk = kTensor && P <= 8;
     DevBuf tc_tile_d, tc_tile_begin, tc_tile_count, tc_pair_e, tc_pair_src, tc_bimg, tc_error;
     DevBuf tc_ltile_d, tc_ltile_begin, tc_ltile_count;
@@ -276,6 +288,8 @@ struct Evaluator final : EvaluatorBase {
             std::vector<int64_t> pe;
             std::vector<int32_t> ps;
             batches(TcTs<P>::NT / m, all, lvl, tc_lvl_tiles, pe, ps);
+            tc_halves(all, nullptr);
+            tc_halves(lvl, &tc_lvl_tiles);
             tc_ntiles = (int64_t)all.d.size();
             tc_tile_d.upload(all.d);
             tc_tile_begin.upload(all.begin);
@@ -324,11 +338,12 @@ struct Evaluator final : EvaluatorBase {
                             vp[q] = pos;
                         }
                     for (int d = 0; d < 316; ++d) {
-                        for (int64_t j = cnt[d]; j < cnt[d + 1]; j += ppt_tc) {
-                            tcd.push_back(d);
-                            tcb.push_back(j);
-                            tcn.push_back((int32_t)std::min<int64_t>(ppt_tc, cnt[d + 1] - j));
-                        }
+                        for (int h = 0; h < kTcHalves; ++h)  // table index d * halves + half
+                            for (int64_t j = cnt[d]; j < cnt[d + 1]; j += ppt_tc) {
+                                tcd.push_back(d * kTcHalves + h);
+                                tcb.push_back(j);
+                                tcn.push_back((int32_t)std::min<int64_t>(ppt_tc, cnt[d + 1] - j));
+                            }
                         for (int64_t j = cnt[d]; j < cnt[d + 1]; j += kGemmPairs) {
                             sd.push_back(d);
                             sb.push_back(j);
@@ -512,6 +527,38 @@ struct Evaluator final : EvaluatorBase {
             }
         }
     };
+    // Tensor-core tiles with two output-slot halves (TcTs<P>::H == 2, p = 11, 12): every run
+    // of tiles of one offset d is listed twice, with table index 2d (slots 0..127) and then
+    // 2d + 1 (slots 128..255), so a CTA swaps tables as rarely as with one half; lstart
+    // (per-level tile ranges, when given) is remapped.  With one half the index is d.
+    static void tc_halves(Tiles& t, std::vector<int64_t>* lstart) {
+        if constexpr (TcTs<P>::H == 2) {
+            std::vector<int64_t> seg = lstart ? *lstart : std::vector<int64_t>{0, (int64_t)t.d.size()};
+            Tiles o;
+            std::vector<int64_t> nseg(seg.size(), 0);
+            for (size_t sgi = 0; sgi + 1 < seg.size(); ++sgi) {
+                nseg[sgi] = (int64_t)o.d.size();
+                for (int64_t i = seg[sgi]; i < seg[sgi + 1];) {
+                    int64_t j = i;
+                    while (j < seg[sgi + 1] && t.d[j] == t.d[i]) ++j;
+                    for (int h = 0; h < 2; ++h)
+                        for (int64_t x = i; x < j; ++x) {
+                            o.d.push_back(2 * t.d[x] + h);
+                            o.begin.push_back(t.begin[x]);
+                            o.count.push_back(t.count[x]);
+                        }
+                    i = j;
+                }
+            }
+            nseg.back() = (int64_t)o.d.size();
+            if (lstart) *lstart = nseg;
+            t = std::move(o);
+        } else {
+            (void)t;
+            (void)lstart;
+        }
+    }
+
     void batches(int tile, Tiles& all, Tiles& lvl, std::vector<int64_t>& lstart, std::vector<int64_t>& pe,
                  std::vector<int32_t>& ps) {
         const Plan& pl = plan;
@@ -1172,6 +1219,195 @@ struct Evaluator final : EvaluatorBase {
         }
     }
 
+    // ---- the Helmholtz FMM (real k): complex expansions as row pairs, per-level tables ----
+    static constexpr int NE = 2 * NC;  // order of a complex translation as a real matrix
+    HhState hh;
+
+    // the complex translation of a host table (a real 2n x n matrix per set, column-major,
+    // column j the image of the unit real input e_j, the real plane over the imaginary
+    // plane) as the real 2n x 2n block [[A_r, -A_i], [A_i, A_r]], column-major, in T,
+    // scaled by `scale` (exact: a power of two)
+    static void hh_block(const std::vector<double>& host, int sets, double scale, std::vector<T>& out, size_t at) {
+        const int n = NC;
+        for (int d = 0; d < sets; ++d) {
+            const double* h = host.data() + (size_t)d * 2 * n * n;
+            T* o = out.data() + at + (size_t)d * NE * NE;
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    const double ar = h[(size_t)j * 2 * n + i], ai = h[(size_t)j * 2 * n + n + i];
+                    o[(size_t)j * NE + i] = (T)(scale * ar);
+                    o[(size_t)j * NE + n + i] = (T)(scale * ai);
+                    o[(size_t)(n + j) * NE + i] = (T)(-scale * ai);
+                    o[(size_t)(n + j) * NE + n + i] = (T)(scale * ar);
+                }
+        }
+    }
+
+    // Buffers (first use) and the tables of wavenumber k (when it changed): per level l the
+    // M2L set of boxes of half-width 1 at k_l = k r_l (l >= 2), the M2M set of parent level
+    // l (l < L) and the L2L set of child level l (l >= 3, its parent's octant tables times
+    // 1/2: a local in box units is r_l times the absolute one).
+    void hh_setup(double k) {
+        const int NL = plan.nlevels;
+        if (NL > 32) throw Failure(FMMGPU_UNSUPPORTED, "more than 32 levels");
+        if (!hh.built) {
+            const size_t nb = plan.nboxes();
+            const size_t mv = 2 * (size_t)m;
+            hh.M.alloc(sizeof(T) * mv * ms_of(P) * nb);
+            hh.L.alloc(sizeof(T) * mv * ms_of(P) * nb);
+            hh.Y.alloc(sizeof(T) * mv * ys_of(P) * (plan.v.nnz() + 1));
+            hh.Yo.alloc(sizeof(T) * mv * ys_of(P) * nb);
+            hh.far_phi.alloc(sizeof(double) * 2 * (size_t)m * (dp.ntgt + 1));
+            if (gradients) hh.far_g.alloc(sizeof(double) * 6 * (size_t)m * (dp.ntgt + 1));
+            if (!hq.ptr) {
+                hq.alloc(sizeof(Cplx<T>) * (size_t)m * (dp.nsrc + 1));
+                if (kMixed) hq64.alloc(sizeof(double2) * (size_t)m * (dp.nsrc + 1));
+            }
+            size_t smem = sizeof(double) * (2 * NC * 32 + 2 * (size_t)m * 32);
+            if (smem > 227 * 1024) throw Failure(FMMGPU_UNSUPPORTED, "too many charge vectors a pass for P2L");
+            CUDA_TRY(cudaFuncSetAttribute(hh_expand_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            CUDA_TRY(cudaFuncSetAttribute(hh_expand_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            if (GemmShape<P, T, true>::SMEM > 48 * 1024)
+                CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              GemmShape<P, T, true>::SMEM));
+            hh.built = true;
+        }
+        if (k == hh.k) return;
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int l = 0; l < NL; ++l) hh.lv.kl[l] = k * plan.side * std::ldexp(1.0, -(l + 1));
+        const size_t set = (size_t)NE * NE;
+        std::vector<T> m2l((size_t)std::max(NL - 2, 1) * 316 * set), m2m((size_t)NL * 8 * set), l2l((size_t)NL * 8 * set);
+        std::vector<double> host, hm, hl;
+        for (int l = 2; l < NL; ++l) {
+            bool any = false;
+            for (int64_t b = plan.level_start[l]; b < plan.level_start[l + 1] && !any; ++b)
+                any = plan.v.row[b + 1] > plan.v.row[b];
+            if (!any) continue;  // no V pair on this level: its tables are never read
+            build_helmholtz_m2l_tables(P, hh.lv.kl[l], 1.0, host);
+            hh_block(host, 316, 1.0, m2l, (size_t)(l - 2) * 316 * set);
+        }
+        for (int l = 0; l + 1 < NL; ++l) {
+            build_helmholtz_octant_tables(P, hh.lv.kl[l], 1.0, hm, hl);
+            hh_block(hm, 8, 1.0, m2m, (size_t)l * 8 * set);
+            hh_block(hl, 8, 0.5, l2l, (size_t)(l + 1) * 8 * set);
+        }
+        hh.m2l.upload(m2l);
+        hh.m2m.upload(m2m);
+        hh.l2l.upload(l2l);
+        hh.k = k;
+        hh_table_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    void helmholtz_fmm(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) override {
+        if (kim != 0.0)
+            throw Failure(FMMGPU_UNSUPPORTED, "the Helmholtz far field is built for a real wavenumber (Im k = 0)");
+        if (!(kre > 0.0)) throw Failure(FMMGPU_INVALID_ARGUMENT, "the Helmholtz FMM needs k > 0");
+        if (!plan.box_side.empty())
+            throw Failure(FMMGPU_UNSUPPORTED, "the Helmholtz FMM is not offered for multi-cloud batches");
+        if (!chunks.empty())
+            throw Failure(FMMGPU_UNSUPPORTED,
+                          "the Helmholtz far field needs every M2L product at once (the plan was built chunked)");
+        ensure_product_path();
+        if (!chunks.empty())
+            throw Failure(FMMGPU_UNSUPPORTED, "the Helmholtz far field needs every M2L product at once");
+        hh_setup(kre);
+        if (first_pass) launches = 0;
+        const int64_t ns = dp.nsrc;
+        const int L = plan.nlevels - 1;
+        const int mv = 2 * m;
+        const size_t set = (size_t)NE * NE;
+        T* hM = hh.M.as<T>();
+        T* hL = hh.L.as<T>();
+        if (ns > 0)
+            helm_charge_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
+                d_q, src_perm.as<int64_t>(), ns, m, qstride, hq.as<Cplx<T>>(), kMixed ? hq64.as<double2>() : nullptr);
+        CUDA_TRY(cudaMemsetAsync(hh.M.ptr, 0, hh.M.bytes, stream));
+        const int64_t top = plan.nlevels > 2 ? plan.level_start[2] : (int64_t)plan.nboxes();
+        CUDA_TRY(cudaMemsetAsync(hh.L.ptr, 0, sizeof(T) * (size_t)mv * ms_of(P) * top, stream));
+        const size_t esmem = sizeof(double) * (2 * NC * 32 + 2 * (size_t)m * 32);
+        // upward: P2M of every leaf, then M2M from level L-1 up to 0
+        if (plan.nleaves())
+            hh_expand_kernel<P, T, false><<<counted((unsigned)plan.nleaves()), 32, esmem, stream>>>(
+                dp, hh.lv, 0, (int64_t)plan.nleaves(), nullptr, m, spos.as<T4>(), hq.as<Cplx<T>>(), hM);
+        constexpr int gsm = GemmShape<P, T, true>::SMEM;
+        for (int l = L - 1; l >= 0; --l) {
+            const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
+            const int64_t n = m2m_start[l + 1] - m2m_start[l];
+            if (nt)
+                m2l_gemm_kernel<P, T, true><<<counted((unsigned)nt), 256, gsm, stream>>>(
+                    oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
+                    oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
+                    hh.m2m.as<T>() + (size_t)l * 8 * set, hM, hh.Yo.as<T>());
+            if (n)
+                m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
+                    dp, m2m_par.as<int32_t>() + m2m_start[l], n, mv, hh.Yo.as<T>(), hM);
+        }
+        // M2L products of every level (their tables are per level)
+        for (int l = 2; l <= L; ++l) {
+            const int64_t t0 = lvl_tiles[l], nt = lvl_tiles[l + 1] - lvl_tiles[l];
+            if (nt)
+                m2l_gemm_kernel<P, T, true><<<counted((unsigned)nt), 256, gsm, stream>>>(
+                    ltile_d.as<int32_t>() + t0, ltile_begin.as<int64_t>() + t0, ltile_count.as<int32_t>() + t0,
+                    nullptr, pair_src.as<int32_t>(), m, hh.m2l.as<T>() + (size_t)(l - 2) * 316 * set, hM,
+                    hh.Y.as<T>());
+        }
+        // downward: per level the L2L products, the locals (L2L + V in offset order), P2L
+        for (int l = 2; l <= L; ++l) {
+            if (l >= 3) {
+                const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
+                if (nt)
+                    m2l_gemm_kernel<P, T, true><<<counted((unsigned)nt), 256, gsm, stream>>>(
+                        oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0,
+                        oct_tile_count.as<int32_t>() + t0, oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m,
+                        hh.l2l.as<T>() + (size_t)l * 8 * set, hL, hh.Yo.as<T>());
+            }
+            const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
+            if (b1 > b0) {
+                if constexpr (kMixed)
+                    local_reduce4_kernel<P><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
+                        dp, b0, b1, mv, l >= 3, 1, 0, reinterpret_cast<const float*>(hh.Yo.ptr),
+                        reinterpret_cast<const float*>(hh.Y.ptr), v_pos.as<int64_t>(),
+                        reinterpret_cast<float*>(hh.L.ptr));
+                else
+                    local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
+                        dp, b0, b1, mv, l >= 3, 1, 0, hh.Yo.as<T>(), hh.Y.as<T>(), v_pos.as<int64_t>(), hL);
+            }
+            const int64_t x0 = xbox_start[l], x1 = xbox_start[l + 1];
+            if (x1 > x0)
+                hh_expand_kernel<P, T, true><<<counted((unsigned)(x1 - x0)), 32, esmem, stream>>>(
+                    dp, hh.lv, x0, x1, xbox.as<int32_t>(), m, spos.as<T4>(), hq.as<Cplx<T>>(), hL);
+        }
+        // leaves: L2P + M2P into the far partials, then the near field and the output pass
+        if (plan.nleaves()) {
+            if (gradients)
+                hh_leaf_far_kernel<P, T, true><<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
+                    dp, hh.lv, 0, m, tpos.as<T4>(), hM, hL, hh.far_phi.as<double>(), hh.far_g.as<double>());
+            else
+                hh_leaf_far_kernel<P, T, false><<<counted((unsigned)plan.nleaves()), 128, 0, stream>>>(
+                    dp, hh.lv, 0, m, tpos.as<T4>(), hM, hL, hh.far_phi.as<double>(), nullptr);
+        }
+        helm_near_launch(kre, kim, d_phi, d_grad, hh.far_phi.as<double>(), gradients ? hh.far_g.as<double>() : nullptr);
+        CUDA_TRY(cudaGetLastError());
+    }
+
+    // the Helmholtz P2P of every leaf into the caller-order outputs, after adding the far
+    // partials when given (far_phi [v][t][2], far_g [v][t][6], leaf order)
+    void helm_near_launch(double kre, double kim, double* d_phi, double* d_grad, const double* far_phi,
+                          const double* far_g) {
+        if (!items.count) return;
+        const unsigned g = (unsigned)((items.count + kHelmWarps - 1) / kHelmWarps);
+        if (gradients)
+            helm_p2p_kernel<T, true, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
+                dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
+                hq64.as<double2>(), far_phi, far_g, d_phi, d_grad);
+        else
+            helm_p2p_kernel<T, false, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
+                dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
+                hq64.as<double2>(), far_phi, nullptr, d_phi, nullptr);
+    }
+
     // ---- the Helmholtz near field (all leaves' P2P level calls) ----
     DevBuf hq, hq64;
     void helmholtz_near(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) override {
@@ -1184,17 +1420,7 @@ struct Evaluator final : EvaluatorBase {
         if (ns > 0)
             helm_charge_kernel<T><<<counted((unsigned)((ns + 255) / 256)), 256, 0, stream>>>(
                 d_q, src_perm.as<int64_t>(), ns, m, qstride, hq.as<Cplx<T>>(), kMixed ? hq64.as<double2>() : nullptr);
-        if (items.count) {
-            const unsigned g = (unsigned)((items.count + kHelmWarps - 1) / kHelmWarps);
-            if (gradients)
-                helm_p2p_kernel<T, true, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
-                    dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
-                    hq64.as<double2>(), d_phi, d_grad);
-            else
-                helm_p2p_kernel<T, false, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
-                    dp, items, m, (T)kTheta2, kre, kim, spos.as<T4>(), hq.as<Cplx<T>>(), tpos.as<T4>(), close,
-                    hq64.as<double2>(), d_phi, nullptr);
-        }
+        helm_near_launch(kre, kim, d_phi, d_grad, nullptr, nullptr);
         CUDA_TRY(cudaGetLastError());
     }
 

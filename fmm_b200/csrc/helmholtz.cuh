@@ -116,13 +116,15 @@ constexpr int kHelmWarps = 4;
 constexpr int kHelmStage = 64;
 
 // k the physical wavenumber; out_phi [v][nt] and out_g [v][nt][3], complex as (re, im)
-// doubles, caller order
+// doubles, caller order; far_phi / far_g (when given) the far field's partials of the
+// FMM in leaf order ([v][t] complex, [v][t][3] complex), added to each target's sum
 template <typename T, bool GRAD, bool CLOSE>
 __global__ void __launch_bounds__(32 * kHelmWarps) helm_p2p_kernel(
     DevPlan plan, P2pItems items, int m, T theta2, double k_re, double k_im,
     const typename Vec4<T>::type* __restrict__ spos, const Cplx<T>* __restrict__ sq,
     const typename Vec4<T>::type* __restrict__ tpos, ClosePairs close, const double2* __restrict__ q64,
-    double* __restrict__ out_phi, double* __restrict__ out_g) {
+    const double* __restrict__ far_phi, const double* __restrict__ far_g, double* __restrict__ out_phi,
+    double* __restrict__ out_g) {
     using T4 = typename Vec4<T>::type;
     __shared__ T4 stage[kHelmWarps][kHelmStage];
     __shared__ Cplx<T> qstage[kHelmWarps][kHelmStage];
@@ -196,6 +198,12 @@ __global__ void __launch_bounds__(32 * kHelmWarps) helm_p2p_kernel(
             }
         }
         if (!valid) continue;
+        if (far_phi) {  // the far field's partials (the FMM): added after the near sums
+            aphi[0] += far_phi[2 * ((int64_t)v * nt + t)];
+            aphi[1] += far_phi[2 * ((int64_t)v * nt + t) + 1];
+            if (GRAD)
+                for (int k = 0; k < 6; ++k) ag[k] += far_g[6 * ((int64_t)v * nt + t) + k];
+        }
         if (CLOSE) {
             // near-singular pairs in f64 with the reference's coincidence rule
             const double4 u = close.tpos[t];

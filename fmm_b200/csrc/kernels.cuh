@@ -443,20 +443,27 @@ __device__ __forceinline__ void gemm_cp_async(T* smem, const T* gmem, bool valid
 }
 
 // Shared memory of the SIMT GEMM: the table (columns as rows, NCP wide) and the tile's
-// source rows, KC input slots at a time.  KC = (p+1)^2 (one staging) where both fit in
-// 200 KB; at higher degree in f64 the input slots are staged in chunks of KC, the
-// accumulators kept in registers across the chunks (the same order of additions).
-template <int P, typename T>
+// source rows, KC input slots at a time.  KC = the matrix order (one staging) where both
+// fit in 200 KB; at higher degree in f64 the input slots are staged in chunks of KC, the
+// accumulators kept in registers across the chunks (the same order of additions).  CPLX:
+// the Helmholtz form, a complex expansion as one real vector of 2 (p+1)^2 entries (the
+// real plane, then the imaginary plane) and the table a real 2n x 2n matrix.
+template <int P, typename T, bool CPLX = false>
 struct GemmShape {
     static constexpr int NC = nc_of(P);
-    static constexpr int NCP = 96 > NC ? 96 : ((NC + 15) / 16) * 16;
+    static constexpr int NE = CPLX ? 2 * NC : NC;  // matrix order
+    static constexpr int NCP = 96 > NE ? 96 : ((NE + 15) / 16) * 16;
     static constexpr int ROW_BYTES = (NCP + kGemmPairs) * (int)sizeof(T);
     static constexpr int KC_FIT = (200 * 1024) / ROW_BYTES;
-    static constexpr int KC = KC_FIT < NC ? KC_FIT : NC;
+    static constexpr int KC = KC_FIT < NE ? KC_FIT : NE;
     static constexpr int SMEM = KC * ROW_BYTES;
 };
 
-template <int P, typename T>
+// Y[pair] = A_d X[source] for a tile of pairs of one matrix d (column-major NE x NE).
+// Rows: a box holds MV = m (real) or 2m (CPLX: rows 2v and 2v + 1 the real and imaginary
+// planes of vector v) expansion rows of ms_of(P) slots; a product holds MV rows of
+// ys_of(P) slots.
+template <int P, typename T, bool CPLX = false>
 __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict__ tile_d,
                                                        const int64_t* __restrict__ tile_begin,
                                                        const int32_t* __restrict__ tile_count,
@@ -464,10 +471,11 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
                                                        const int32_t* __restrict__ pair_src, int m,
                                                        const T* __restrict__ tab, const T* __restrict__ M,
                                                        T* __restrict__ Y) {
-    using S = GemmShape<P, T>;
-    constexpr int NC = S::NC, NCP = S::NCP, KC = S::KC;
+    using S = GemmShape<P, T, CPLX>;
+    constexpr int NC = S::NC, NE = S::NE, NCP = S::NCP, KC = S::KC;
     constexpr int JN = NCP / 16;
-    constexpr bool kOneStage = KC == NC;
+    constexpr bool kOneStage = KC == NE;
+    const int mv = CPLX ? 2 * m : m;  // expansion rows a box
     extern __shared__ unsigned char smem_raw[];
     T* At = reinterpret_cast<T*>(smem_raw);  // [KC][NCP]: At[k][n] = A_d[n][k0 + k]
     T* Xs = At + KC * NCP;                   // [KC][64]:  Xs[k][pair]
@@ -475,7 +483,7 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
     const int d = tile_d[tile];
     const int64_t p0 = tile_begin[tile];
     const int cnt = tile_count[tile];
-    const T* A = tab + (int64_t)d * NC * NC;
+    const T* A = tab + (int64_t)d * NE * NE;
     // staging by asynchronous copies (every copy of the block in flight at once; padding
     // zero-filled): the table, then each vector's source rows once the tile's sources are
     // known; 256 threads
@@ -484,25 +492,27 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
     auto stage_table = [&](int k0, int kc) {
         for (int t = threadIdx.x; t < kc * NCP; t += 256) {
             const int k = t / NCP, n = t % NCP;
-            gemm_cp_async<T>(At + t, A + (int64_t)(k0 + k) * NC + (n < NC ? n : 0), n < NC);
+            gemm_cp_async<T>(At + t, A + (int64_t)(k0 + k) * NE + (n < NE ? n : 0), n < NE);
         }
     };
-    if (kOneStage) stage_table(0, NC);
+    if (kOneStage) stage_table(0, NE);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int v = 0; v < m; ++v) {
+        const int vrow = CPLX ? 2 * v : v;
         T acc[4][JN];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < JN; ++j) acc[i][j] = T(0);
-        for (int k0 = 0; k0 < NC; k0 += KC) {
-            const int kc = NC - k0 < KC ? NC - k0 : KC;
+        for (int k0 = 0; k0 < NE; k0 += KC) {
+            const int kc = NE - k0 < KC ? NE - k0 : KC;
             __syncthreads();  // srcs written; the previous chunk's or vector's staging read
             if (!kOneStage) stage_table(k0, kc);
             for (int t = threadIdx.x; t < kc * kGemmPairs; t += 256) {
-                const int pr = t / kc, k = t % kc;
-                gemm_cp_async<T>(Xs + k * kGemmPairs + pr, M + ((int64_t)srcs[pr] * m + v) * ms_of(P) + k0 + k,
-                                 pr < cnt);
+                const int pr = t / kc, kk = k0 + t % kc;
+                const int plane = CPLX ? kk / NC : 0, slot_ = CPLX ? kk % NC : kk;
+                gemm_cp_async<T>(Xs + (t % kc) * kGemmPairs + pr,
+                                 M + ((int64_t)srcs[pr] * mv + vrow + plane) * ms_of(P) + slot_, pr < cnt);
             }
             asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
             __syncthreads();
@@ -523,11 +533,15 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
         for (int i = 0; i < 4; ++i) {
             int pr = ty * 4 + i;
             if (pr >= cnt) continue;
-            T* y = Y + ((pair_e ? pair_e[p0 + pr] : p0 + pr) * m + v) * ys_of(P);
+            const int64_t e = pair_e ? pair_e[p0 + pr] : p0 + pr;
 #pragma unroll
             for (int j = 0; j < JN; ++j) {
-                int n = tx + 16 * j;
-                if (n < NC) __stcs(y + n, acc[i][j]);  // read once by the reduce: stream past L2
+                const int n = tx + 16 * j;
+                if (n < NE) {
+                    const int plane = CPLX ? n / NC : 0, slot_ = CPLX ? n % NC : n;
+                    // read once by the reduce: stream past L2
+                    __stcs(Y + (e * mv + vrow + plane) * ys_of(P) + slot_, acc[i][j]);
+                }
             }
         }
     }

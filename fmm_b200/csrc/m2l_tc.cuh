@@ -167,10 +167,15 @@ struct TcTs {
     static constexpr int KA = (NC + 31) / 32;
     static constexpr int KP = 32 * KA;             // padded K (input slots)
     static constexpr int KSTEPS = KP / 8;
+    // output slot halves: (p+1)^2 > 128 (p = 11, 12) takes two passes over a tile's
+    // columns, each with the table rows of one half (128 slots) in tensor memory
+    static constexpr int H = NC > 128 ? 2 : 1;
     // columns per tile (UMMA N): 96 at p = 7, 8 (KP = 96), where shared memory then holds
     // two raw stages (measured faster than 64 columns with four); 64 at p = 9, 10
-    // (KP = 128), the most beside two X stages and two raw stages
-    static constexpr int NT = KP > 96 ? 64 : KP > 64 ? 96 : 128;
+    // (KP = 128), the most beside two X stages and two raw stages; 48 at p = 11, 12
+    // (KP = 160, 192: tensor memory then holds the table's 2 KP columns and two 48-column
+    // accumulators, shared memory two X stages and two or three raw stages)
+    static constexpr int NT = KP > 128 ? 48 : KP > 96 ? 64 : KP > 64 ? 96 : 128;
     static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage (also one raw stage)
     // raw stages: as many as shared memory holds beside the two X stages, at most 4 (the
     // copy engine's loads take several tiles' time to land)
@@ -179,10 +184,10 @@ struct TcTs {
     static constexpr int SMEM = (4 + RS) * X_BYTES + 1024;  // X [2 stages][hi, lo], raw [RS stages]
     static constexpr int COL_AHI = 0, COL_ALO = KP, COL_D0 = 2 * KP;  // TMEM columns
     static constexpr int TMEM_COLS = 512;
-    static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per offset (hi, lo)
-    static_assert(NC <= 128, "UMMA M = 128 output slots");
+    static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per (offset, half) (hi, lo)
+    static_assert(NC <= 256, "two halves of UMMA M = 128 output slots");
     static_assert(2 * KP + 2 * NT <= TMEM_COLS, "TMEM budget");
-    static_assert(NT % 32 == 0 && NT / 4 <= 32, "gather rows: four per lane");
+    static_assert(NT % 16 == 0 && NT / 4 <= 32, "UMMA N; gather rows: four per lane");
     static_assert(RS >= 2, "raw stages");
     static_assert(SMEM + 256 <= 227 * 1024, "shared memory");
 };
@@ -491,23 +496,24 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         __syncwarp();
     } else if (warp < 8) {
         // ---------------- epilogue ----------------
-        const int q = warp & 3, g = warp >> 2;  // lane quarter, column half (NT / 2 pairs)
-        const int n = 32 * q + lane;
+        const int q = warp & 3, g = warp >> 2;  // lane quarter, column group (16-column chunks g, g + 2, ...)
         for (int64_t k = 0; k < ntile && !warp_aborted(); ++k) {
             const int64_t it = i0 + k;
             const int st = (int)(k & 1);
             const int64_t p0 = tile_begin[it];
             const int ncol = tile_count[it] * m;
+            const int h = S::H == 2 ? (tile_d[it] & 1) : 0;  // slot half of this pass
+            const int n = 128 * h + 32 * q + lane;            // output slot of this lane
             if (!warp_wait(&bar_accf[st], (uint32_t)((k >> 1) & 1))) {
                 if (lane == 0) give_up();
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            if (32 * q < ys_of(P)) {
+            if (128 * h + 32 * q < ys_of(P)) {
                 // products at rows p0 * m + c (a tile's rows are consecutive), whole 128-byte
                 // lines (rows >= NC of the table are zero), 16 columns per TMEM load
 #pragma unroll 1
-                for (int c0 = (NT / 2) * g; c0 < (NT / 2) * (g + 1); c0 += 16) {
+                for (int c0 = 16 * g; c0 < NT; c0 += 32) {
                     if (c0 >= ncol) break;
                     float v0[16];
                     tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * NT + c0), v0);
@@ -530,8 +536,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     }
 }
 
-// columns (pairs x vectors) of a tensor-core M2L tile at degree p; 0 where the
-// tensor-core M2L does not apply ((p+1)^2 > 128 output slots)
+// columns (pairs x vectors) of a tensor-core M2L tile at degree p (0 to 12)
 inline int tc_tile_columns(int p) {
     switch (p) {
         case 0: return TcTs<0>::NT;
@@ -545,6 +550,8 @@ inline int tc_tile_columns(int p) {
         case 8: return TcTs<8>::NT;
         case 9: return TcTs<9>::NT;
         case 10: return TcTs<10>::NT;
+        case 11: return TcTs<11>::NT;
+        case 12: return TcTs<12>::NT;
         default: return 0;
     }
 }
@@ -574,14 +581,14 @@ void encode_multipole_map(CUtensorMap* map, const float* M, int64_t rows, int bo
     if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
-// Host: the table images for tensor memory, per offset a hi and a lo part, each
-// [128 output slots][KP input slots] of tf32 bits (round to nearest, ties away),
-// zero-padded: image[d][part][n][k] = A_d[n][k].
+// Host: the table images for tensor memory, per offset and slot half a hi and a lo part,
+// each [128 output slots][KP input slots] of tf32 bits (round to nearest, ties away),
+// zero-padded: image[d][h][part][n][k] = A_d[128 h + n][k].
 template <int P>
 void build_tc_table_images(const std::vector<double>& m2l, std::vector<uint32_t>& img) {
     using S = TcTs<P>;
     constexpr int NC = S::NC;
-    img.assign((size_t)316 * S::IMG_WORDS, 0u);
+    img.assign((size_t)316 * S::H * S::IMG_WORDS, 0u);
     for (int d = 0; d < 316; ++d)
         for (int n = 0; n < NC; ++n)
             for (int k = 0; k < NC; ++k) {
@@ -595,7 +602,8 @@ void build_tc_table_images(const std::vector<double>& m2l, std::vector<uint32_t>
                 uint32_t rb;
                 std::memcpy(&rb, &rem, 4);
                 uint32_t lo = tf32_round_bits(rb);
-                size_t base = (size_t)d * S::IMG_WORDS + (size_t)n * S::KP + k;
+                // image (d, half n / 128): the table index of a tile is d * H + half
+                size_t base = ((size_t)d * S::H + n / 128) * S::IMG_WORDS + (size_t)(n % 128) * S::KP + k;
                 img[base] = hi;
                 img[base + (size_t)128 * S::KP] = lo;
             }

@@ -286,7 +286,7 @@ int fmmgpu_helmholtz_direct_sum(double k_re, double k_im, size_t nsources, const
  * complex64 with the mixed form's f64 near-singular pairs).  charges[i*m + v] complex
  * (caller order), potential[v*nt + i] and gradient[(v*nt + i)*3 + k] complex (caller
  * order; the gradient when the FMM was built with gradients), with 1/(4 pi).  Host
- * buffers; synchronises.  The Helmholtz far field is not offered. */
+ * buffers; synchronises.  fmmgpu_helmholtz_evaluate adds the far field. */
 /* The dense M2L tables of one level for a real k > 0 (the reference's DenseM2l,
  * fmm-tables/src/helmholtz/dense.rs:1-30), built on the host in f64 by projection
  * (fmm-ref/src/helmholtz/direct.rs): boxes of half-width `half_width` (k in the same
@@ -305,6 +305,28 @@ int fmmgpu_helmholtz_octant_tables(int p, double k, double half_width, double* m
 
 int fmmgpu_helmholtz_near(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges, double* potential,
                           double* gradient);
+
+/* The whole Helmholtz FMM, e^{ikr}/(4 pi r), for a real wavenumber k = k_re > 0 (k_im must
+ * be 0: the far field's tables are built for a real k), on the tree and lists the build
+ * made: the reference's HelmholtzFmm evaluation (fmm-exec/src/helmholtz/fmm.rs; its
+ * operator, fmm-exec/src/helmholtz/operator.rs:16-29, is host-only there).  Complex
+ * expansions of degree p on every level in the real orthonormal harmonics and scaled
+ * radial functions (fmm-ref/src/helmholtz/leaf.rs), the dense M2L tables of every level
+ * (fmm-tables/src/helmholtz/dense.rs) and the M2M / L2L tables of every level built on the
+ * host by projection (fmm-ref/src/helmholtz/direct.rs) when k is new (then kept for the
+ * next calls with the same k), every pass on the GPU in the handle's precision (f64, or
+ * f32 expansions and translations with complex64 near field and f64 near-singular pairs).
+ * charges[i*m + v] complex (caller order), potential[v*nt + i] and gradient[(v*nt + i)*3 +
+ * k] complex, with 1/(4 pi), HOST buffers; synchronises.  Not offered for multi-cloud
+ * batches. */
+int fmmgpu_helmholtz_evaluate(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges, double* potential,
+                              double* gradient);
+/* The same with DEVICE buffers on the evaluator's stream; does not synchronise (the
+ * tables of a new k are built, on the host, before the launches are queued). */
+int fmmgpu_helmholtz_evaluate_device(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges,
+                                     double* potential, double* gradient);
+/* Host seconds the last new wavenumber's Helmholtz tables took to build. */
+double fmmgpu_helmholtz_table_seconds(const fmmgpu_fmm* fmm);
 
 /* The same direct sum on DEVICE buffers, allocating nothing.  No counterpart in the
  * reference (its direct_sum, fmm-ref/src/p2p.rs:147-186, is host code); the results are
