@@ -34,7 +34,8 @@ class FmmError(RuntimeError):
 class Settings(C.Structure):
     _fields_ = [("p", C.c_int), ("precision", C.c_int), ("gradients", C.c_int), ("vectors", C.c_int),
                 ("max_points_per_leaf", C.c_int), ("max_level", C.c_int), ("device", C.c_int),
-                ("vectors_per_pass", C.c_int), ("autotune", C.c_int), ("product_bytes", C.c_int64)]
+                ("vectors_per_pass", C.c_int), ("autotune", C.c_int), ("product_bytes", C.c_int64),
+                ("table_cache", C.c_char_p), ("tuning_cache", C.c_char_p)]
 
 
 class Info(C.Structure):
@@ -43,7 +44,8 @@ class Info(C.Structure):
                 ("v_pairs", C.c_int64), ("w_pairs", C.c_int64), ("x_pairs", C.c_int64),
                 ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64),
                 ("vectors_per_pass", C.c_int64), ("p2p_warps", C.c_int64), ("leaf_block", C.c_int64),
-                ("product_chunks", C.c_int64), ("p2p_stream_bytes", C.c_int64)]
+                ("product_chunks", C.c_int64), ("p2p_stream_bytes", C.c_int64), ("tables_loaded", C.c_int64),
+                ("tuning_loaded", C.c_int64)]
 
 
 def lib():
@@ -212,6 +214,19 @@ class FmmBuilder:
         """M2L product buffer bytes (0: automatic); smaller buffers run the products in
         chunks of target boxes, with the same results."""
         self._s.product_bytes = int(n)
+        return self
+
+    def table_cache(self, directory):
+        """Load the operator tables from `directory` (the reference's TableCache files),
+        building and storing the missing ones (FmmBuilder::table_cache); None: always build."""
+        self._table_cache = None if directory is None else os.fsencode(directory)
+        self._s.table_cache = self._table_cache
+        return self
+
+    def tuning_cache(self, directory):
+        """Keep the autotuner's choices in `directory` and reuse them (FmmBuilder::tuning_cache)."""
+        self._tuning_cache = None if directory is None else os.fsencode(directory)
+        self._s.tuning_cache = self._tuning_cache
         return self
 
     def max_level(self, level):

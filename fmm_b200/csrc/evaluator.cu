@@ -81,6 +81,9 @@ struct fmmgpu_fmm {
     fmmgpu_fmm* transpose = nullptr;
     DevBuf d_vjp_w, d_vjp_tq, d_vjp_dq, d_vjp_dxs, d_vjp_dxt;
     DevBuf d_hq, d_hphi, d_hg;  // the Helmholtz host call's device buffers
+    int64_t tables_loaded = 0;  // tables taken from the table cache (bits: M2L, M2M, L2L)
+    std::string table_cache_dir, tuning_cache_dir;  // the settings' cache directories ("" none)
+    int64_t tuning_loaded = 0;  // launch shapes taken from the tuning cache
 };
 
 namespace fmmb {
@@ -205,6 +208,8 @@ void fmmgpu_default_settings(fmmgpu_settings* s) {
     s->vectors_per_pass = 0;
     s->autotune = 0;
     s->product_bytes = 0;
+    s->table_cache = nullptr;
+    s->tuning_cache = nullptr;
 }
 
 namespace {
@@ -251,6 +256,44 @@ int64_t count_near_pairs(const Plan& P) {
     return n;
 }
 
+// The f64 operator tables of degree p: from the table cache when the settings name one
+// (a file missing or rejected is rebuilt and stored; a failed store leaves the build as it
+// is, as the reference's load_or_build never fails because of its cache), else built.
+// The settings' cache directories are copied (the caller's strings need not outlive the
+// build) and the handle's copy of the settings keeps no pointer to them.
+void keep_cache_dirs(fmmgpu_fmm* f) {
+    f->table_cache_dir = f->settings.table_cache ? f->settings.table_cache : "";
+    f->tuning_cache_dir = f->settings.tuning_cache ? f->settings.tuning_cache : "";
+    f->settings.table_cache = nullptr;
+    f->settings.tuning_cache = nullptr;
+}
+
+void load_or_build_tables(fmmgpu_fmm* f) {
+    const fmmgpu_settings& s = f->settings;
+    const std::string& dir = f->table_cache_dir;
+    const int p = s.p;
+    const size_t n2 = (size_t)(p + 1) * (p + 1) * (p + 1) * (p + 1);
+    struct Kind {
+        int code;
+        size_t sets;
+        std::vector<double>* out;
+        void (*build)(int, std::vector<double>&);
+        int bit;
+    } kinds[3] = {{kTableM2l, 316, &f->m2l, build_m2l_tables, 1},
+                  {kTableM2m, 8, &f->m2m, build_m2m_tables, 2},
+                  {kTableL2l, 8, &f->l2l, build_l2l_tables, 4}};
+    f->tables_loaded = 0;
+    for (const Kind& k : kinds) {
+        std::string why;
+        if (!dir.empty() && table_cache_load(dir, k.code, p, 0.0, k.sets * n2, *k.out, &why)) {
+            f->tables_loaded |= k.bit;
+            continue;
+        }
+        k.build(p, *k.out);
+        if (!dir.empty()) table_cache_store(dir, k.code, p, 0.0, *k.out, &why);
+    }
+}
+
 // Host part of a build: plan, tables, leaf-scaled coordinates (no device work).
 std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
                                        const double* tgt, std::vector<double>& us, std::vector<double>& ut) {
@@ -259,10 +302,9 @@ std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t n
     if ((ns && !src) || (nt && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
     auto f = std::make_unique<fmmgpu_fmm>();
     f->settings = s;
+    keep_cache_dirs(f.get());
     f->plan = build_plan(ns, src, nt, tgt, s.max_level, s.max_points_per_leaf);
-    build_m2l_tables(s.p, f->m2l);
-    build_m2m_tables(s.p, f->m2m);
-    build_l2l_tables(s.p, f->l2l);
+    load_or_build_tables(f.get());
     leaf_scaled(f->plan, src, tgt, us, ut);
     f->near_pairs = count_near_pairs(f->plan);
     return f;
@@ -311,10 +353,9 @@ std::unique_ptr<fmmgpu_fmm> build_host_batch(const fmmgpu_settings* settings, si
         if (!errors[c].empty()) throw Failure(FMMGPU_INVALID_ARGUMENT, "cloud " + std::to_string(c) + ": " + errors[c]);
     auto f = std::make_unique<fmmgpu_fmm>();
     f->settings = s;
+    keep_cache_dirs(f.get());
     f->plan = merge_plans(parts, us, ut);
-    build_m2l_tables(s.p, f->m2l);
-    build_m2m_tables(s.p, f->m2m);
-    build_l2l_tables(s.p, f->l2l);
+    load_or_build_tables(f.get());
     f->near_pairs = count_near_pairs(f->plan);
     return f;
 }
@@ -383,13 +424,48 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
     f->d_phi.alloc(sizeof(double) * (size_t)s.vectors * (nt + 1));
     if (s.gradients) f->d_grad.alloc(sizeof(double) * 3 * (size_t)s.vectors * (nt + 1));
     f->device_bytes = bytes + f->d_charges.bytes + f->d_phi.bytes + f->d_grad.bytes;
+    f->eval->table_cache_dir = f->table_cache_dir;
     if (s.autotune) {
-        // the launch shapes timed on this plan with zero charges: the charges change no
-        // branch and no launch, so they time as any others
-        CUDA_TRY(cudaMemsetAsync(f->d_charges.ptr, 0, f->d_charges.bytes, f->stream));
-        f->eval->autotune(f->d_charges.as<double>(), f->d_phi.as<double>(),
-                          s.gradients ? f->d_grad.as<double>() : nullptr);
-        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+        // a choice kept in the tuning cache for this device, precision, p and gradients
+        // setting is used as it is; otherwise the shapes are timed and the choice stored
+        TuningKey key;
+        std::map<std::string, int> entries;
+        const std::string g = s.gradients ? "gradients:" : "potentials:";
+        bool cached = false;
+        if (!f->tuning_cache_dir.empty()) {
+            cudaDeviceProp prop{};
+            CUDA_TRY(cudaGetDeviceProperties(&prop, s.device));
+            key.device = std::string(prop.name) + " sm_" + std::to_string(prop.major) + std::to_string(prop.minor) +
+                         " " + std::to_string(prop.multiProcessorCount) + " SMs";
+            key.compiler = "nvcc cudart " + std::to_string(CUDART_VERSION) + " sm_100a";
+            key.precision = s.precision == FMMGPU_PRECISION_F64 ? "f64" : "mixed";
+            key.p = s.p;
+            std::string why;
+            if (tuning_cache_load(f->tuning_cache_dir, key, entries, &why) && entries.count(g + "p2p_warps") &&
+                entries.count(g + "leaf_block")) {
+                const int w = entries[g + "p2p_warps"], b = entries[g + "leaf_block"];
+                if ((w == 1 || w == 2 || w == 4) && (b == 32 || b == 64 || b == 128)) {
+                    f->eval->p2p_warps = w;
+                    f->eval->leaf_block = b;
+                    cached = true;
+                }
+            }
+        }
+        if (!cached) {
+            // the launch shapes timed on this plan with zero charges: the charges change no
+            // branch and no launch, so they time as any others
+            CUDA_TRY(cudaMemsetAsync(f->d_charges.ptr, 0, f->d_charges.bytes, f->stream));
+            f->eval->autotune(f->d_charges.as<double>(), f->d_phi.as<double>(),
+                              s.gradients ? f->d_grad.as<double>() : nullptr);
+            if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+            if (!f->tuning_cache_dir.empty()) {
+                entries[g + "p2p_warps"] = f->eval->p2p_warps;
+                entries[g + "leaf_block"] = f->eval->leaf_block;
+                std::string why;
+                tuning_cache_store(f->tuning_cache_dir, key, entries, &why);
+            }
+        }
+        f->tuning_loaded = cached ? 1 : 0;
     }
     CUDA_TRY(cudaDeviceSynchronize());
 }
@@ -836,6 +912,8 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->vectors_per_pass = f->eval ? f->mpass : 0;
         info->p2p_warps = f->eval ? f->eval->p2p_warps : 0;
         info->p2p_stream_bytes = f->eval ? f->eval->p2p_stream_bytes : 0;
+        info->tables_loaded = f->tables_loaded;
+        info->tuning_loaded = f->tuning_loaded;
         info->leaf_block = f->eval ? f->eval->leaf_block : 0;
         info->product_chunks = f->eval ? f->eval->product_chunks() : 0;
     });

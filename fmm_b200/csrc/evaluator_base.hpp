@@ -146,8 +146,11 @@ struct EvaluatorBase {
     // the whole Helmholtz FMM for a real wavenumber (near and far field), device buffers:
     // complex charges [i][v] (qstride vectors a point), outputs [v][i] and [v][i][3] complex
     virtual void helmholtz_fmm(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) = 0;
-    // host seconds spent building the Helmholtz tables of the last new wavenumber
+    // host seconds spent building (or loading) the Helmholtz tables of the last new wavenumber
     double hh_table_seconds = 0.0;
+    // the table cache directory of the build ("" none): the Helmholtz tables of each level
+    // are loaded from it, or built and stored there
+    std::string table_cache_dir;
     virtual void autotune(const double* d_charges, double* d_phi, double* d_grad) = 0;
     virtual void set_m2l_path(int path) = 0;
     virtual void set_p2p_path(int path) = 0;

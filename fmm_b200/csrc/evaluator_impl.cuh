@@ -1285,11 +1285,31 @@ struct Evaluator final : EvaluatorBase {
             for (int64_t b = plan.level_start[l]; b < plan.level_start[l + 1] && !any; ++b)
                 any = plan.v.row[b + 1] > plan.v.row[b];
             if (!any) continue;  // no V pair on this level: its tables are never read
-            build_helmholtz_m2l_tables(P, hh.lv.kl[l], 1.0, host);
+            const size_t cnt = (size_t)316 * 2 * NC * NC;
+            std::string why;
+            if (table_cache_dir.empty() ||
+                !table_cache_load(table_cache_dir, kTableHelmholtzM2l, P, hh.lv.kl[l], cnt, host, &why)) {
+                build_helmholtz_m2l_tables(P, hh.lv.kl[l], 1.0, host);
+                if (!table_cache_dir.empty())
+                    table_cache_store(table_cache_dir, kTableHelmholtzM2l, P, hh.lv.kl[l], host, &why);
+            }
             hh_block(host, 316, 1.0, m2l, (size_t)(l - 2) * 316 * set);
         }
         for (int l = 0; l + 1 < NL; ++l) {
-            build_helmholtz_octant_tables(P, hh.lv.kl[l], 1.0, hm, hl);
+            const size_t half = (size_t)8 * 2 * NC * NC;
+            std::string why;
+            if (!table_cache_dir.empty() &&
+                table_cache_load(table_cache_dir, kTableHelmholtzOctant, P, hh.lv.kl[l], 2 * half, host, &why)) {
+                hm.assign(host.begin(), host.begin() + half);
+                hl.assign(host.begin() + half, host.end());
+            } else {
+                build_helmholtz_octant_tables(P, hh.lv.kl[l], 1.0, hm, hl);
+                if (!table_cache_dir.empty()) {
+                    host = hm;
+                    host.insert(host.end(), hl.begin(), hl.end());
+                    table_cache_store(table_cache_dir, kTableHelmholtzOctant, P, hh.lv.kl[l], host, &why);
+                }
+            }
             hh_block(hm, 8, 1.0, m2m, (size_t)l * 8 * set);
             hh_block(hl, 8, 0.5, l2l, (size_t)(l + 1) * 8 * set);
         }

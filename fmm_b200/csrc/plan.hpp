@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -101,5 +102,26 @@ void build_helmholtz_m2l_tables(int p, double k, double r, std::vector<double>& 
 // and the 8 octants' M2M (child multipole -> parent) and L2L (parent local -> child) tables
 // of a parent level of half-width r, real 2n x n matrices each
 void build_helmholtz_octant_tables(int p, double k, double r, std::vector<double>& m2m, std::vector<double>& l2l);
+
+// On-disk caches (table_cache.cpp): the operator tables in the reference's TableCache
+// format (fmm-tables/src/cache.rs; kind codes 1 M2M, 2 L2L, 3 M2L; the Helmholtz tables of
+// a level under codes 65 and 66 with k_l in the name), f64, and the autotuner's choices in
+// the layout of its TuningCache (fmm-exec/src/tune.rs:118-140).  Loads return false with
+// the reason in *why (missing, or which check rejected the file); stores are atomic.
+enum { kTableM2m = 1, kTableL2l = 2, kTableM2l = 3, kTableHelmholtzM2l = 65, kTableHelmholtzOctant = 66 };
+std::string table_cache_file_name(int kind, int p, double k = 0.0);
+bool table_cache_store(const std::string& dir, int kind, int p, double k, const std::vector<double>& values,
+                       std::string* why);
+bool table_cache_load(const std::string& dir, int kind, int p, double k, size_t count, std::vector<double>& values,
+                      std::string* why);
+struct TuningKey {
+    std::string device, compiler, precision;
+    int p = 0;
+};
+std::string tuning_cache_file_name(const TuningKey& key);
+bool tuning_cache_load(const std::string& dir, const TuningKey& key, std::map<std::string, int>& entries,
+                       std::string* why);
+bool tuning_cache_store(const std::string& dir, const TuningKey& key, const std::map<std::string, int>& entries,
+                        std::string* why);
 
 }  // namespace fmmb

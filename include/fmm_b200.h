@@ -69,6 +69,14 @@ typedef struct {
                                  free memory); > 0 at most this many bytes, the products
                                  then made and reduced level by level in chunks of target
                                  boxes.  The results do not depend on it */
+    const char* table_cache;  /* directory of the operator-table cache (FmmBuilder::table_cache,
+                                 fmm-exec/src/fmm.rs:1410-1425; the reference's TableCache
+                                 files, fmm-tables/src/cache.rs): tables are loaded from it,
+                                 or built and stored there; NULL (default): always built */
+    const char* tuning_cache; /* directory of the autotuner's choices (FmmBuilder::tuning_cache,
+                                 fmm.rs:1655-1669): with autotune on, a choice kept there for
+                                 this device, precision and p is used instead of timing, and
+                                 new timings are stored; NULL (default): no file */
 } fmmgpu_settings;
 
 typedef struct {
@@ -85,6 +93,8 @@ typedef struct {
     int64_t leaf_block;   /* threads a block of the L2P / M2P kernel (static 64, or the tuned one) */
     int64_t product_chunks; /* chunks of the M2L product path (0: every product at once) */
     int64_t p2p_stream_bytes; /* the mixed P2P's near-row source streams (0: mapped per flush) */
+    int64_t tables_loaded;    /* tables the build took from the table cache: bit 0 M2L, 1 M2M, 2 L2L */
+    int64_t tuning_loaded;    /* 1: the launch shapes came from the tuning cache */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;

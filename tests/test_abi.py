@@ -59,7 +59,10 @@ def _struct_fields(name):
         decl = decl.strip()
         if not decl:
             continue
-        ctype, names = decl.split(None, 1)
+        if decl.startswith("const char*"):
+            ctype, names = "const char*", decl[len("const char*"):]
+        else:
+            ctype, names = decl.split(None, 1)
         out += [(ctype, n.strip()) for n in names.split(",")]
     return out
 
@@ -68,7 +71,7 @@ def _struct_fields(name):
 def test_python_structs_mirror_the_header(cname, pystruct):
     """The ctypes mirrors of the header's structs: the same fields in the same order with
     the same widths, so the library and the binding agree on the layout."""
-    width = {"int": C.c_int, "int64_t": C.c_int64}
+    width = {"int": C.c_int, "int64_t": C.c_int64, "const char*": C.c_char_p}
     fields = _struct_fields(cname)
     assert [n for _, n in fields] == [n for n, _ in pystruct._fields_]
     for (ctype, n), (pn, pt) in zip(fields, pystruct._fields_):
