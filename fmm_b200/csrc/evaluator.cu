@@ -83,6 +83,8 @@ struct fmmgpu_fmm {
     DevBuf d_hq, d_hphi, d_hg;  // the Helmholtz host call's device buffers
     int64_t tables_loaded = 0;  // tables taken from the table cache (bits: M2L, M2M, L2L)
     std::string table_cache_dir, tuning_cache_dir;  // the settings' cache directories ("" none)
+    bool uploaded = false;         // the plan came from the caller (fmmgpu_upload_plan)
+    std::vector<uint8_t> is_leaf;  // per box, for fmmgpu_fmm_plan_arrays
     int64_t tuning_loaded = 0;  // launch shapes taken from the tuning cache
 };
 
@@ -483,6 +485,98 @@ int fmmgpu_plan_build(const fmmgpu_settings* settings, size_t ns, const double* 
     });
 }
 
+namespace {
+
+// Host part of a build on a caller's plan: checks, tables, leaf-scaled coordinates (every
+// point inside its leaf, within 2^-20 of the leaf's half-width).
+std::unique_ptr<fmmgpu_fmm> build_host_uploaded(const fmmgpu_settings* settings, const fmmgpu_plan_arrays* pa,
+                                                size_t ns, const double* src, size_t nt, const double* tgt,
+                                                std::vector<double>& us, std::vector<double>& ut) {
+    check_settings(settings);
+    if (!pa) throw Failure(FMMGPU_INVALID_ARGUMENT, "null plan");
+    if ((ns && !src) || (nt && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
+    for (size_t i = 0; i < 3 * ns; ++i)
+        if (!std::isfinite(src[i])) throw Failure(FMMGPU_INVALID_ARGUMENT, "non-finite point coordinate");
+    for (size_t i = 0; i < 3 * nt; ++i)
+        if (!std::isfinite(tgt[i])) throw Failure(FMMGPU_INVALID_ARGUMENT, "non-finite point coordinate");
+    auto f = std::make_unique<fmmgpu_fmm>();
+    f->settings = *settings;
+    keep_cache_dirs(f.get());
+    f->plan = plan_from_arrays(*pa, ns, nt);
+    f->uploaded = true;
+    load_or_build_tables(f.get());
+    leaf_scaled(f->plan, src, tgt, us, ut);
+    const double lim = 1.0 + std::ldexp(1.0, -20);
+    for (const std::vector<double>* u : {&us, &ut})
+        for (size_t i = 0; i < u->size(); ++i)
+            if (!(std::fabs((*u)[i]) <= lim))
+                throw Failure(FMMGPU_INVALID_ARGUMENT, std::string("uploaded plan: a ") + (u == &us ? "source" : "target") +
+                                                           " point lies outside its leaf");
+    f->near_pairs = count_near_pairs(f->plan);
+    return f;
+}
+
+}  // namespace
+
+int fmmgpu_plan_from_arrays(const fmmgpu_settings* settings, const fmmgpu_plan_arrays* plan, size_t ns,
+                            const double* src, size_t nt, const double* tgt, fmmgpu_fmm** out) {
+    return guarded([&] {
+        if (!out) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        std::vector<double> us, ut;
+        auto f = build_host_uploaded(settings, plan, ns, src, nt, tgt, us, ut);
+        *out = f.release();
+    });
+}
+
+int fmmgpu_upload_plan(const fmmgpu_settings* settings, const fmmgpu_plan_arrays* plan, size_t ns,
+                       const double* src, size_t nt, const double* tgt, fmmgpu_fmm** out) {
+    return guarded([&] {
+        if (!out) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            throw Failure(FMMGPU_NO_DEVICE, "no CUDA device is visible");
+        }
+        std::vector<double> us, ut;
+        auto f = build_host_uploaded(settings, plan, ns, src, nt, tgt, us, ut);
+        build_device(f.get(), us, ut);
+        f->symmetric = src == tgt && ns == nt;
+        *out = f.release();
+    });
+}
+
+int fmmgpu_fmm_plan_arrays(const fmmgpu_fmm* f, fmmgpu_plan_arrays* a) {
+    return guarded([&] {
+        if (!f || !a) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        const Plan& P = f->plan;
+        if (!P.box_side.empty()) throw Failure(FMMGPU_UNSUPPORTED, "a multi-cloud forest is not one plan");
+        auto* self = const_cast<fmmgpu_fmm*>(f);
+        self->is_leaf.assign(P.nboxes(), 0);
+        for (size_t j = 0; j < P.nleaves(); ++j) self->is_leaf[P.leaf_box[j]] = 1;
+        a->nlevels = P.nlevels;
+        a->level_start = P.level_start.data();
+        a->keys = P.key.data();
+        a->is_leaf = self->is_leaf.data();
+        for (int k = 0; k < 3; ++k) a->lower[k] = P.lower[k];
+        a->side = P.side;
+        a->source_offsets = P.src_start.data();
+        a->target_offsets = P.tgt_start.data();
+        a->source_order = P.src_perm.data();
+        a->target_order = P.tgt_perm.data();
+        a->near_rows = P.near.row.data();
+        a->near = P.near.col.data();
+        a->w_rows = P.w.row.data();
+        a->w = P.w.col.data();
+        a->x_rows = P.x.row.data();
+        a->x = P.x.col.data();
+        a->v_rows = P.v.row.data();
+        a->v = P.v.col.data();
+        a->v_offsets = P.v.aux.data();
+    });
+}
+
 int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
                      const double* tgt, fmmgpu_fmm** out) {
     return guarded([&] {
@@ -575,6 +669,8 @@ int fmmgpu_fmm_vjp(fmmgpu_fmm* f, const double* charges, const double* cotangent
         const int m = f->settings.vectors;
         const int64_t ns = (int64_t)f->plan.src_perm.size(), nt = (int64_t)f->plan.tgt_perm.size();
         fmmgpu_fmm* T = f;
+        if (!f->symmetric && f->uploaded)
+            throw Failure(FMMGPU_UNSUPPORTED, "a VJP on an uploaded plan needs targets == sources");
         if (!f->symmetric) {
             if (!f->transpose) {  // the swapped problem: charges at the targets, evaluated at the sources
                 std::vector<double> us, ut;

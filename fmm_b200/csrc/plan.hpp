@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include "../../include/fmm_b200.h"
+
 namespace fmmb {
 
 constexpr int kDeepest = 16;
@@ -90,6 +92,16 @@ double leaf_coordinate(double x, double a, double w, int level, uint32_t index);
 
 // M2L offset index of d = index(target) - index(source) (fmm-tables/src/geometry.rs:90)
 int offset_index(int dx, int dy, int dz);
+
+// Morton keys (octree/src/morton.rs): encode the integer coordinates of a box of a level,
+// decode them, read the level
+uint64_t morton_encode(uint32_t i, uint32_t j, uint32_t k, int level);
+void morton_decode(uint64_t key, uint32_t out[3]);
+int morton_level(uint64_t key);
+
+// A plan given in the reference's flattened layout (fmmgpu_plan_arrays), checked
+// (plan_upload.cpp); throws std::runtime_error naming the first failed check.
+Plan plan_from_arrays(const fmmgpu_plan_arrays& a, size_t ns, size_t nt);
 
 // Operator tables (column-major, (p+1)^2 x (p+1)^2 each), built in f64 from the direct
 // translations applied to unit vectors (fmm-tables/src/m2l.rs:67-96, octant.rs:150-174).

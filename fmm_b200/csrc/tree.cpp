@@ -438,4 +438,8 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
     return P;
 }
 
+uint64_t morton_encode(uint32_t i, uint32_t j, uint32_t k, int level) { return encode(i, j, k, level); }
+void morton_decode(uint64_t key, uint32_t out[3]) { decode(key, out); }
+int morton_level(uint64_t key) { return key_level(key); }
+
 }  // namespace fmmb

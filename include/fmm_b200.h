@@ -112,6 +112,64 @@ int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t nsources, const dou
 int fmmgpu_plan_build(const fmmgpu_settings* settings, size_t nsources, const double* sources,
                       size_t ntargets, const double* targets, fmmgpu_fmm** out);
 
+/* A plan made outside the library (the reference's one-rank Plan, fmm-plan/src/plan.rs,
+ * with the views its level calls receive, fmm-plan/src/operator.rs:170-317, and its list
+ * CSRs, fmm-plan/src/lists.rs:172-282), flattened over all levels:
+ *  - boxes level-major, key order within a level (box t of level l is global box
+ *    level_start[l] + t: the reference's BoxIndex per level); keys are the reference's
+ *    Morton keys (octree/src/morton.rs: 3 interleaved index bits a level, x highest,
+ *    shifted left 15, the level in the low 15 bits);
+ *  - leaves are the leaf boxes in box order (the reference's leaf index); leaf j holds the
+ *    leaf-order points source_offsets[j] .. source_offsets[j + 1] (targets likewise), and
+ *    source_order[a] / target_order[a] is the caller index of leaf-order point a;
+ *  - the cubic domain: lower corner and side (fmm-exec/src/geometry.rs:120-147);
+ *  - the lists as CSR (row offsets int64, entries int32), rows in the reference's
+ *    accumulation order (operator.rs:34-45): near (per leaf: leaf indices, the leaf itself
+ *    included, ascending), W (per leaf: box indices on the next level, ascending), X (per
+ *    box: leaf indices, ascending), V (per box: source boxes of the same level with their
+ *    offset indices 0..315, fmm-plan/src/lists.rs:100, by offset index; the batches of the
+ *    reference's GroupedCsr are formed from them).
+ * Every array is read during the call only. */
+typedef struct {
+    int nlevels;
+    const int64_t* level_start;      /* nlevels + 1 */
+    const uint64_t* keys;            /* level_start[nlevels] boxes */
+    const uint8_t* is_leaf;          /* per box */
+    double lower[3];
+    double side;
+    const int64_t* source_offsets;   /* nleaves + 1 */
+    const int64_t* target_offsets;   /* nleaves + 1 */
+    const int64_t* source_order;     /* nsources */
+    const int64_t* target_order;     /* ntargets */
+    const int64_t* near_rows;        /* nleaves + 1 */
+    const int32_t* near;
+    const int64_t* w_rows;           /* nleaves + 1 */
+    const int32_t* w;
+    const int64_t* x_rows;           /* nboxes + 1 */
+    const int32_t* x;
+    const int64_t* v_rows;           /* nboxes + 1 */
+    const int32_t* v;
+    const int32_t* v_offsets;        /* the offset index of each V entry */
+} fmmgpu_plan_arrays;
+
+/* The FmmOperator's device operator created on a caller's plan (the reference's
+ * DeviceOperator::new, fmm-exec/src/device.rs:3032, which uploads the plan's views,
+ * geometry and tables): the plan is checked (a complete octree of consistent keys, every
+ * index in range, rows ordered, each point inside its leaf, near rows 2:1-balanced) and
+ * uploaded with the f64 tables of settings->p and the points' leaf-scaled coordinates;
+ * settings->max_points_per_leaf and max_level are not used.  The handle then answers every
+ * call an fmmgpu_fmm_build handle does, the level calls on this plan.  A vector-Jacobian
+ * product needs targets == sources here.  FMMGPU_INVALID_ARGUMENT names the first check
+ * that failed. */
+int fmmgpu_upload_plan(const fmmgpu_settings* settings, const fmmgpu_plan_arrays* plan, size_t nsources,
+                       const double* sources, size_t ntargets, const double* targets, fmmgpu_fmm** out);
+/* The same without a device (checks, host tables, a plan-only handle as fmmgpu_plan_build's). */
+int fmmgpu_plan_from_arrays(const fmmgpu_settings* settings, const fmmgpu_plan_arrays* plan, size_t nsources,
+                            const double* sources, size_t ntargets, const double* targets, fmmgpu_fmm** out);
+/* The arrays of a handle's plan in that layout (pointers into the handle, valid while it
+ * lives): what fmmgpu_upload_plan takes, so a plan round-trips. */
+int fmmgpu_fmm_plan_arrays(const fmmgpu_fmm* fmm, fmmgpu_plan_arrays* plan);
+
 /* Multi-cloud batch (no reference counterpart: the reference batches charge vectors
  * only, FmmBuilder::vectors, fmm.rs:200-227): `ncloud` independent clouds, cloud c with
  * nsources[c] sources and ntargets[c] targets (ntargets NULL: the targets are the
