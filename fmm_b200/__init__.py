@@ -86,6 +86,9 @@ def lib():
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_helmholtz_near": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
             "fmmgpu_helmholtz_evaluate": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
+            "fmmgpu_upload_plan": (C.c_int, [C.POINTER(Settings), vp, sz, dp, sz, dp, C.POINTER(vp)]),
+            "fmmgpu_plan_from_arrays": (C.c_int, [C.POINTER(Settings), vp, sz, dp, sz, dp, C.POINTER(vp)]),
+            "fmmgpu_fmm_plan_arrays": (C.c_int, [vp, vp]),
             "fmmgpu_helmholtz_evaluate_device": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
             "fmmgpu_helmholtz_table_seconds": (C.c_double, [vp]),
             "fmmgpu_helmholtz_m2l_tables": (C.c_int, [C.c_int, C.c_double, C.c_double, dp]),
@@ -178,6 +181,61 @@ class Output:
     def __init__(self, potential, gradient):
         self.potential = potential
         self.gradient = gradient
+
+
+class PlanArrays(C.Structure):
+    """fmmgpu_plan_arrays: a plan in the reference's flattened layout (include/fmm_b200.h)."""
+    _fields_ = [("nlevels", C.c_int), ("level_start", C.c_void_p), ("keys", C.c_void_p), ("is_leaf", C.c_void_p),
+                ("lower", C.c_double * 3), ("side", C.c_double), ("source_offsets", C.c_void_p),
+                ("target_offsets", C.c_void_p), ("source_order", C.c_void_p), ("target_order", C.c_void_p),
+                ("near_rows", C.c_void_p), ("near", C.c_void_p), ("w_rows", C.c_void_p), ("w", C.c_void_p),
+                ("x_rows", C.c_void_p), ("x", C.c_void_p), ("v_rows", C.c_void_p), ("v", C.c_void_p),
+                ("v_offsets", C.c_void_p)]
+
+    # name -> (dtype, length key): the arrays of a plan dict
+    ARRAYS = {"level_start": np.int64, "keys": np.uint64, "is_leaf": np.uint8, "source_offsets": np.int64,
+              "target_offsets": np.int64, "source_order": np.int64, "target_order": np.int64,
+              "near_rows": np.int64, "near": np.int32, "w_rows": np.int64, "w": np.int32, "x_rows": np.int64,
+              "x": np.int32, "v_rows": np.int64, "v": np.int32, "v_offsets": np.int32}
+
+    @classmethod
+    def from_dict(cls, plan):
+        """A struct pointing into contiguous copies of the dict's arrays (kept on the struct)."""
+        s = cls()
+        keep = {}
+        for name, dt in cls.ARRAYS.items():
+            a = np.ascontiguousarray(plan[name], dtype=dt)
+            keep[name] = a
+            setattr(s, name, a.ctypes.data if a.size else None)
+        s.nlevels = int(plan["nlevels"])
+        for k in range(3):
+            s.lower[k] = float(plan["lower"][k])
+        s.side = float(plan["side"])
+        s._keep = keep
+        return s
+
+    def to_dict(self, nboxes, nleaves, ns, nt):
+        """Copies of the arrays the struct points to."""
+        def arr(name, n):
+            ptr = getattr(self, name)
+            dt = np.dtype(self.ARRAYS[name])
+            if not n or not ptr:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dt))), (n,)).copy()
+        nl = self.nlevels
+        out = {"nlevels": nl, "lower": list(self.lower), "side": self.side}
+        out["level_start"] = arr("level_start", nl + 1)
+        out["keys"] = arr("keys", nboxes)
+        out["is_leaf"] = arr("is_leaf", nboxes)
+        for s in ("source", "target"):
+            out[f"{s}_offsets"] = arr(f"{s}_offsets", nleaves + 1)
+        out["source_order"] = arr("source_order", ns)
+        out["target_order"] = arr("target_order", nt)
+        for name, nrows in (("near", nleaves), ("w", nleaves), ("x", nboxes), ("v", nboxes)):
+            out[f"{name}_rows"] = arr(f"{name}_rows", nrows + 1)
+            out[name] = arr(name, int(out[f"{name}_rows"][-1]))
+        out["v_offsets"] = arr("v_offsets", int(out["v_rows"][-1]))
+        return out
 
 
 class FmmBuilder:
@@ -278,6 +336,27 @@ class FmmBuilder:
         h, ns, nt = self._batch(lib().fmmgpu_batch_plan_build, clouds, targets)
         return Plan(h, self._s, ns, nt)
 
+    def upload(self, plan, sources, targets=None):
+        """An FMM on a caller's plan (a dict of the fmmgpu_plan_arrays fields, the reference's
+        flattened layout): checked, uploaded, then evaluated like any other (fmmgpu_upload_plan)."""
+        src = _points(sources)
+        tgt = src if targets is None else _points(targets)
+        arrays = PlanArrays.from_dict(plan)
+        h = C.c_void_p()
+        _check(lib().fmmgpu_upload_plan(C.byref(self._s), C.byref(arrays), len(src), _ptr(src), len(tgt), _ptr(tgt),
+                                        C.byref(h)))
+        return Fmm(h, self._s, len(src), len(tgt))
+
+    def plan_from(self, plan, sources, targets=None):
+        """The host half of upload(): the checks and a plan-only handle; needs no GPU."""
+        src = _points(sources)
+        tgt = src if targets is None else _points(targets)
+        arrays = PlanArrays.from_dict(plan)
+        h = C.c_void_p()
+        _check(lib().fmmgpu_plan_from_arrays(C.byref(self._s), C.byref(arrays), len(src), _ptr(src), len(tgt),
+                                             _ptr(tgt), C.byref(h)))
+        return Plan(h, self._s, len(src), len(tgt))
+
     def plan(self, sources, targets=None):
         """The host half only (tree, lists, tables); needs no GPU."""
         src = _points(sources)
@@ -314,6 +393,14 @@ class Plan:
         if n < 0:
             raise IndexError(row)
         return out[:n].copy()
+
+    def plan_arrays(self):
+        """The plan in the reference's flattened layout (fmmgpu_fmm_plan_arrays), as a dict of
+        copies: what FmmBuilder.upload takes."""
+        a = PlanArrays()
+        _check(lib().fmmgpu_fmm_plan_arrays(self._h, C.byref(a)))
+        info = self.info()
+        return a.to_dict(info["nboxes"], info["nleaves"], self.nsources, self.ntargets)
 
     def tables(self):
         p = self.settings.p
