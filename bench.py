@@ -777,11 +777,15 @@ def run_helmholtz(F, torch, dev, flush, n=1_000_000, k=20.0, p=10, leaf=96, step
 
 
 CPU_REPEATS = 5
+HOST_PATH = ("restated reference host path (LaplaceOperator with nd-fmm-simd on AVX-512F: P2P with vrsqrt14pd + "
+             "two Newton steps, targets in lanes, 16 a block; batched M2L in blocks of 64 targets, 4 columns a "
+             "pass; lists made at build), OpenMP over the host cores")
+HOST_PATH_SCALAR = "restated reference host path without AVX-512F on this CPU: its scalar P2P, batched M2L"
 
 
 def cpu_baseline(args, n_sample=None, repeats=CPU_REPEATS, warmup=1):
-    """The restated reference host FMM (oracle: OpenMP over all host cores, the P2P and the
-    table products in vector lanes) on the headline workload (the same sphere problem,
+    """The restated reference host path (oracle/hostpath.c: its AVX-512 P2P and batched M2L,
+    OpenMP over all host cores) on the headline workload (the same sphere problem,
     n_sample points), built once (plan and f64 tables, reported beside), then `warmup`
     untimed and `repeats` timed evaluations; the value is N over the median evaluation
     time, as the metric defines it (fmm-bench/src/measure.rs: build and tables excluded)."""
@@ -791,7 +795,7 @@ def cpu_baseline(args, n_sample=None, repeats=CPU_REPEATS, warmup=1):
     x, q = sphere_problem(n, SEED)
     cores = os.cpu_count()
     t0 = time.perf_counter()
-    f = O.Fmm(x, x, P, LEAF, gradients=True)
+    f = O.Fmm(x, x, P, LEAF, gradients=True, host_path=True)
     build_s = time.perf_counter() - t0
     for _ in range(warmup):
         f.evaluate(q, threads=cores)
@@ -801,8 +805,9 @@ def cpu_baseline(args, n_sample=None, repeats=CPU_REPEATS, warmup=1):
         times.append(O.fmm_last_eval_seconds())
     med = float(np.median(times))
     return {"value": round(n / med / 1e6, 4), "unit": "Mpoints/s", "cores": cores, "kind": "port",
+            "path": HOST_PATH if O.lib().orc_hp_has_avx512() else HOST_PATH_SCALAR,
             "sample": f"sphere N={n} p={P} leaf={LEAF} phi+grad f64: median of {repeats} evaluations after "
-                      f"{warmup} warm-up ({med:.2f} s each; plan and tables built once in {build_s:.1f} s)",
+                      f"{warmup} warm-up ({med:.2f} s each; plan, lists and tables built once in {build_s:.1f} s)",
             "evaluations_s": [round(v, 3) for v in times], "n_points": n}
 
 
@@ -815,7 +820,7 @@ def headline_config(n, world):
 
 
 def run_reference(args):
-    """The reference arm: the restated reference host FMM (the oracle) on the host cores, at
+    """The reference arm: the restated reference host path (oracle/hostpath.c) on the host cores, at
     the headline's own N (--ref-n, default the headline's): built once, --warmup untimed
     evaluations, then --steps timed evaluations; the value is N over the median step.
     Under torchrun only rank 0 runs it."""
@@ -828,7 +833,7 @@ def run_reference(args):
     x, q = sphere_problem(n, SEED)
     cores = os.cpu_count()
     t0 = time.perf_counter()
-    f = O.Fmm(x, x, P, LEAF, gradients=True)
+    f = O.Fmm(x, x, P, LEAF, gradients=True, host_path=True)
     build_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         f.evaluate(q, threads=cores)
@@ -847,6 +852,7 @@ def run_reference(args):
         "dtype": "f64", "data": "synthetic (seeded SplitMix64 sphere)",
         "config": cfg,
         "cpu_baseline": {"value": v, "unit": "Mpoints/s", "cores": cores, "kind": "port",
+                         "path": HOST_PATH if O.lib().orc_hp_has_avx512() else HOST_PATH_SCALAR,
                          "sample": f"the whole workload (N={n}) every step: one host evaluation; median of "
                                    f"{args.steps} after {args.warmup} warm-up; plan and tables built once "
                                    f"({build_s:.1f} s, not timed)"},
@@ -855,6 +861,7 @@ def run_reference(args):
 
 
 def main():
+    global P
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
@@ -866,10 +873,25 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (256 clouds) measurement")
     ap.add_argument("--no-iso", action="store_true", help="skip the iso-accuracy (rel-L2 <= 1e-6) measurement")
+    ap.add_argument("--p", type=int, default=P, help="expansion order of the headline workload (profiling runs)")
+    ap.add_argument("--helmholtz-only", action="store_true",
+                    help="run the Helmholtz configuration alone (--hn points) and print its JSON")
+    ap.add_argument("--hn", type=int, default=1_000_000, help="points of the Helmholtz configuration")
     ap.add_argument("--shapes", default=None,
                     help="P2P warps,L2P/M2P threads (e.g. 1,128): set instead of timed at build "
                          "(profiler runs, whose serialised launches would mislead the timing)")
     args = ap.parse_args()
+    P = args.p
+    if args.helmholtz_only:
+        import torch
+
+        import fmm_b200 as F
+
+        dev = torch.device("cuda", 0)
+        flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        print(json.dumps(run_helmholtz(F, torch, dev, flush, n=args.hn, steps=args.steps, warmup=args.warmup)),
+              flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

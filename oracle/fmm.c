@@ -299,7 +299,36 @@ struct orc_fmm_handle {
     int p, m, gradients;
     size_t ns, nt;
     double *m2l_t, *m2m_t, *l2l_t;
+    /* the host path (orc_fmm_set_host_path): lists made once, batched M2L, SIMD P2P */
+    int host_path;
+    size_t *v_row, *v_box, *v_off;     /* V list of every box, by offset index */
+    size_t *near_row, *near_leaf;      /* near list of every leaf (itself included) */
+    size_t *w_row, *w_box;             /* W list of every leaf */
 };
+
+/* the V list of box b: children of its parent's colleagues not adjacent to b, as
+ * (offset index, box) sorted by offset index (fmm-plan/src/interaction_manager.rs:15-27) */
+static int v_list(const boxes_t *B, size_t b, size_t vl[189][2]) {
+    long P = parent_box(B, b);
+    int nv = 0;
+    if (P < 0) return 0;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                if (!dx && !dy && !dz) continue;
+                long C = neighbour(B, (size_t)P, dx, dy, dz);
+                if (C < 0 || B->leaf[C]) continue;
+                for (int co = 0; co < 8; ++co) {
+                    long s = child_box(B, (size_t)C, co);
+                    if (adjacent_boxes(B, (size_t)s, b)) continue;
+                    vl[nv][0] = (size_t)offset_of(B, b, (size_t)s);
+                    vl[nv][1] = (size_t)s;
+                    ++nv;
+                }
+            }
+    qsort(vl, nv, sizeof(vl[0]), cmp_pair);
+    return nv;
+}
 
 orc_fmm_handle *orc_fmm_new(size_t ns, const double *src, size_t nt, const double *tgt, int p, int max_keys,
                             int m, int gradients) {
@@ -320,8 +349,57 @@ orc_fmm_handle *orc_fmm_new(size_t ns, const double *src, size_t nt, const doubl
     return h;
 }
 
+/* The reference's host path instead of its scalar operators (hostpath.c): the lists made
+ * once here (the reference's plan holds them), the batched M2L in blocks of 64 targets and
+ * the AVX-512 P2P; the same FMM to rounding (the P2P terms differ in the last bits). */
+void orc_fmm_set_host_path(orc_fmm_handle *h, int on) {
+    h->host_path = on;
+    if (!on || h->v_row) return;
+    const boxes_t *B = &h->PL.B;
+    const size_t nb = B->nboxes, nl = h->PL.nleaves;
+    h->v_row = (size_t *)calloc(nb + 1, sizeof(size_t));
+    size_t (*vl)[2] = malloc(sizeof(size_t[189][2]));
+    for (size_t b = 0; b < nb; ++b) h->v_row[b + 1] = h->v_row[b] + (size_t)(B->level[b] >= 2 ? v_list(B, b, vl) : 0);
+    h->v_box = (size_t *)malloc((h->v_row[nb] + 1) * sizeof(size_t));
+    h->v_off = (size_t *)malloc((h->v_row[nb] + 1) * sizeof(size_t));
+    for (size_t b = 0; b < nb; ++b) {
+        if (B->level[b] < 2) continue;
+        int nv = v_list(B, b, vl);
+        for (int e = 0; e < nv; ++e) {
+            h->v_off[h->v_row[b] + e] = vl[e][0];
+            h->v_box[h->v_row[b] + e] = vl[e][1];
+        }
+    }
+    free(vl);
+    vecz *nears = calloc(nl, sizeof(vecz)), *ws = calloc(nl, sizeof(vecz));
+    h->near_row = (size_t *)calloc(nl + 1, sizeof(size_t));
+    h->w_row = (size_t *)calloc(nl + 1, sizeof(size_t));
+    for (size_t j = 0; j < nl; ++j) {
+        leaf_lists(&h->PL, h->PL.leaf_box[j], &ws[j], &nears[j]);
+        h->near_row[j + 1] = h->near_row[j] + nears[j].len;
+        h->w_row[j + 1] = h->w_row[j] + ws[j].len;
+    }
+    h->near_leaf = (size_t *)malloc((h->near_row[nl] + 1) * sizeof(size_t));
+    h->w_box = (size_t *)malloc((h->w_row[nl] + 1) * sizeof(size_t));
+    for (size_t j = 0; j < nl; ++j) {
+        if (nears[j].len) memcpy(h->near_leaf + h->near_row[j], nears[j].data, nears[j].len * sizeof(size_t));
+        if (ws[j].len) memcpy(h->w_box + h->w_row[j], ws[j].data, ws[j].len * sizeof(size_t));
+        free(nears[j].data);
+        free(ws[j].data);
+    }
+    free(nears);
+    free(ws);
+}
+
 void orc_fmm_free(orc_fmm_handle *h) {
     if (!h) return;
+    free(h->v_row);
+    free(h->v_box);
+    free(h->v_off);
+    free(h->near_row);
+    free(h->near_leaf);
+    free(h->w_row);
+    free(h->w_box);
     free(h->m2l_t);
     free(h->m2m_t);
     free(h->l2l_t);
@@ -387,6 +465,78 @@ int orc_fmm_eval(orc_fmm_handle *h, const double *q, int threads, int kinds, dou
 
     /* ---- downward: for l = 1..L: l2l, m2l (V by offset), p2l (X by source leaf) ---- */
     for (int l = 1; l <= L; ++l) {
+        if (h->host_path) {
+            /* the reference's batched M2L: L2L of every box, then the V products of blocks of
+             * 64 consecutive targets, offset by offset, four columns at a time (each box's
+             * chain: L2L, then V by offset index, then X, as below) */
+#pragma omp parallel for schedule(dynamic, 4)
+            for (long b = (long)B.level_start[l]; b < (long)B.level_start[l + 1]; ++b) {
+                long P = parent_box(&B, (size_t)b);
+                int o = (int)(((B.idx[b][0] & 1) << 2) | ((B.idx[b][1] & 1) << 1) | (B.idx[b][2] & 1));
+                for (int v = 0; v < m; ++v)
+                    orc_matvec(nc, l2l_t + (size_t)o * nc * nc, Lc + ((size_t)P * m + v) * nc,
+                               Lc + ((size_t)b * m + v) * nc);
+            }
+            const long b0 = (long)B.level_start[l], b1 = (long)B.level_start[l + 1];
+#pragma omp parallel for schedule(dynamic, 1)
+            for (long blk = b0; blk < b1; blk += 64) {
+                const long be = blk + 64 < b1 ? blk + 64 : b1;
+                size_t npair = h->v_row[be] - h->v_row[blk];
+                size_t *ord = (size_t *)malloc((npair + 1) * sizeof(size_t));
+                for (size_t e = 0; e < npair; ++e) ord[e] = h->v_row[blk] + e;
+                /* by offset index, then target (a V row is by offset: a stable merge) */
+                size_t cnt[317] = {0};
+                for (size_t e = 0; e < npair; ++e) cnt[h->v_off[ord[e]] + 1]++;
+                for (int d = 0; d < 316; ++d) cnt[d + 1] += cnt[d];
+                size_t *sorted = (size_t *)malloc((npair + 1) * sizeof(size_t)), fill[316];
+                for (int d = 0; d < 316; ++d) fill[d] = cnt[d];
+                for (size_t e = 0; e < npair; ++e) sorted[fill[h->v_off[ord[e]]]++] = ord[e];
+                const double **bc = (const double **)malloc((npair + 1) * sizeof(double *));
+                double **cc = (double **)malloc((npair + 1) * sizeof(double *));
+                size_t *tbox = (size_t *)malloc((npair + 1) * sizeof(size_t));
+                for (long t2 = blk; t2 < be; ++t2)
+                    for (size_t e = h->v_row[t2]; e < h->v_row[t2 + 1]; ++e) tbox[e - h->v_row[blk]] = (size_t)t2;
+                for (int v = 0; v < m; ++v)
+                    for (int d = 0; d < 316; ++d) {
+                        const int nq = (int)(cnt[d + 1] - cnt[d]);
+                        if (!nq) continue;
+                        for (int i = 0; i < nq; ++i) {
+                            const size_t e = sorted[cnt[d] + i];
+                            bc[i] = M + (h->v_box[e] * m + v) * nc;
+                            cc[i] = Lc + (tbox[e - h->v_row[blk]] * m + v) * nc;
+                        }
+                        orc_hp_columns(nc, m2l_t + (size_t)d * nc * nc, bc, cc, nq);
+                    }
+                free(ord);
+                free(sorted);
+                free(bc);
+                free(cc);
+                free(tbox);
+            }
+#pragma omp parallel for schedule(dynamic, 4)
+            for (long b = b0; b < b1; ++b) {
+                long P = parent_box(&B, (size_t)b);
+                double *Lb = Lc + (size_t)b * m * nc;
+                vecz xl = {0, 0, 0};
+                for (int dx = -1; dx <= 1; ++dx)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dz = -1; dz <= 1; ++dz) {
+                            if (!dx && !dy && !dz) continue;
+                            long C = neighbour(&B, (size_t)P, dx, dy, dz);
+                            if (C < 0 || !B.leaf[C] || adjacent_boxes(&B, (size_t)C, (size_t)b)) continue;
+                            zpush(&xl, (size_t)leaf_of_box[C]);
+                        }
+                sort_unique(&xl);
+                for (size_t e = 0; e < xl.len; ++e) {
+                    size_t j = xl.data[e], s = leaf_box[j];
+                    double c[3], r;
+                    rel_frame(&B, (size_t)b, s, c, &r);
+                    orc_p2l(p, c, r, s_off[j + 1] - s_off[j], us + 3 * s_off[j], qs + m * s_off[j], m, Lb);
+                }
+                free(xl.data);
+            }
+            continue;
+        }
 #pragma omp parallel for schedule(dynamic, 4)
         for (long b = (long)B.level_start[l]; b < (long)B.level_start[l + 1]; ++b) {
             long P = parent_box(&B, (size_t)b);
@@ -450,7 +600,14 @@ int orc_fmm_eval(orc_fmm_handle *h, const double *q, int threads, int kinds, dou
             const double *u = ut + 3 * t_off[j];
             if (kinds & 2) orc_l2p(p, zero3, 1.0, Lc + (size_t)b * m * nc, m, n, u, cphi, cg);
             vecz wl = {0, 0, 0}, near = {0, 0, 0};
-            leaf_lists(&PL, (size_t)b, &wl, &near);
+            if (h->host_path) {  /* the lists the reference's plan holds */
+                wl.data = h->w_box + h->w_row[j];
+                wl.len = h->w_row[j + 1] - h->w_row[j];
+                near.data = h->near_leaf + h->near_row[j];
+                near.len = h->near_row[j + 1] - h->near_row[j];
+            } else {
+                leaf_lists(&PL, (size_t)b, &wl, &near);
+            }
             for (size_t e = 0; e < ((kinds & 2) ? wl.len : 0); ++e) {
                 size_t s = wl.data[e];
                 double c[3], r;
@@ -474,13 +631,18 @@ int orc_fmm_eval(orc_fmm_handle *h, const double *q, int threads, int kinds, dou
                 double *qv = (double *)malloc((nsrc + 1) * sizeof(double));
                 for (int v = 0; v < m; ++v) {
                     for (size_t a = 0; a < nsrc; ++a) qv[a] = qs[(s_off[sj] + a) * m + v];
-                    orc_p2p(nsrc, y, qv, n, u, cphi + v * n, cg ? cg + 3 * v * n : NULL);
+                    if (h->host_path)
+                        orc_hp_p2p(nsrc, y, qv, n, u, cphi + v * n, cg ? cg + 3 * v * n : NULL);
+                    else
+                        orc_p2p(nsrc, y, qv, n, u, cphi + v * n, cg ? cg + 3 * v * n : NULL);
                 }
                 free(qv);
             }
             free(ys);
-            free(wl.data);
-            free(near.data);
+            if (!h->host_path) {
+                free(wl.data);
+                free(near.data);
+            }
             for (int v = 0; v < m; ++v)
                 for (size_t a = 0; a < n; ++a) {
                     phi[v * nt + t_off[j] + a] = cphi[v * n + a];

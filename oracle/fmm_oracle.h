@@ -141,6 +141,15 @@ orc_fmm_handle *orc_fmm_new(size_t ns, const double *src, size_t nt, const doubl
                             int m, int gradients);
 int orc_fmm_eval(orc_fmm_handle *h, const double *q, int threads, int kinds, double *phi, double *grad);
 void orc_fmm_free(orc_fmm_handle *h);
+/* on = 1: the reference's host path (hostpath.c: lists made once, batched M2L, AVX-512 P2P)
+ * in the following evaluations; 0: the scalar operators (the parity oracle) */
+void orc_fmm_set_host_path(orc_fmm_handle *h, int on);
+/* hostpath.c */
+int orc_hp_has_avx512(void);
+void orc_hp_p2p(size_t ns, const double *src, const double *q, size_t nt, const double *tgt, double *potential,
+                double *gradient);
+void orc_hp_columns(int n, const double *A, const double *const *bcols, double *const *ccols, int ncol);
+void orc_matvec(int nc, const double *A, const double *x, double *y);
 
 /* Helmholtz (helmholtz.c): complex values are (re, im) double pairs.  p2p and the
  * Neumaier direct sum of e^{ikr}/r (no 1/(4 pi)), potential[nt] and gradient[nt][3]

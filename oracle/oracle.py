@@ -72,6 +72,9 @@ def lib():
             "orc_fmm_new": (C.c_void_p, [_sz, _dp, _sz, _dp, C.c_int, C.c_int, C.c_int, C.c_int]),
             "orc_fmm_eval": (C.c_int, [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_void_p]),
             "orc_fmm_free": (None, [C.c_void_p]),
+            "orc_fmm_set_host_path": (None, [C.c_void_p, C.c_int]),
+            "orc_hp_has_avx512": (C.c_int, []),
+            "orc_hp_p2p": (None, [_sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_helmholtz_p2p": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp, C.c_void_p]),
             "orc_helmholtz_direct_sum": (None, [C.c_double, C.c_double, _sz, _dp, _dp, _sz, _dp, _dp,
                                                 C.c_void_p]),
@@ -159,6 +162,17 @@ def p2p(src, q, tgt, gradients=True):
     g = np.zeros((len(tgt), 3)) if gradients else None
     lib().orc_p2p(len(src), src, q, len(tgt), tgt, phi, _ptr(g))
     return phi, g
+
+
+def host_p2p(src, q, tgt, gradients=True):
+    """The AVX-512 P2P of the reference's host path (oracle/hostpath.c), no 1/(4 pi)."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    phi = np.zeros(len(tgt))
+    g = np.zeros(3 * len(tgt)) if gradients else None
+    lib().orc_hp_p2p(len(src), src, q, len(tgt), tgt, phi, _ptr(g))
+    return phi, (g.reshape(-1, 3) if gradients else None)
 
 
 def direct_sum(src, q, tgt, gradients=True, threads=True):
@@ -439,12 +453,16 @@ class Fmm:
     """A built oracle FMM (plan and tables once) for repeated evaluations, as the
     reference's FmmBuilder::build then Fmm::evaluate; evaluate() returns what fmm() does."""
 
-    def __init__(self, src, tgt, p, max_keys, gradients=True, vectors=1):
+    def __init__(self, src, tgt, p, max_keys, gradients=True, vectors=1, host_path=False):
+        """host_path: the reference's host path (lists made once, the batched M2L, the
+        AVX-512 P2P of nd-fmm-simd; oracle/hostpath.c) instead of its scalar operators."""
         self.src = np.ascontiguousarray(src, dtype=np.float64)
         self.tgt = np.ascontiguousarray(tgt, dtype=np.float64)
         self.m, self.gradients = vectors, gradients
         self._h = lib().orc_fmm_new(len(self.src), self.src, len(self.tgt), self.tgt, p, max_keys, vectors,
                                     int(gradients))
+        if host_path:
+            lib().orc_fmm_set_host_path(self._h, 1)
 
     def evaluate(self, q, threads=0, kinds=3):
         q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(len(self.src), self.m))

@@ -191,3 +191,35 @@ def test_reference_bench_problem_error(oracle):
     d /= 4 * np.pi
     err = float(np.linalg.norm(phi[0][sample] - d) / np.linalg.norm(d))
     assert abs(err - 1.42e-4) < 0.005e-4, err
+
+
+def test_host_path_p2p_within_the_simd_contract(oracle):
+    """The AVX-512 P2P of the reference's host path (rsqrt14 + two Newton steps, targets in
+    lanes, oracle/hostpath.c) against the scalar loop: every term within 8 u (potential) and
+    16 u (gradient, relative to |q| / r^2) of the scalar term (fmm-simd/src/lib.rs:103-109),
+    so a sum of N terms within N * 16 u of the absolute sum; coincident pairs skipped."""
+    rng = np.random.default_rng(12)
+    for ns, nt in ((1, 1), (9, 17), (200, 333)):
+        src = rng.uniform(-1, 1, (ns, 3))
+        tgt = np.concatenate([rng.uniform(-1, 1, (nt, 3)), src[: min(ns, 5)]])
+        q = rng.standard_normal(ns)
+        a, ga = oracle.host_p2p(src, q, tgt)
+        b, gb = oracle.p2p(src, q, tgt)
+        d = tgt[:, None, :] - src[None, :, :]
+        r = np.sqrt((d * d).sum(-1))
+        with np.errstate(divide="ignore"):
+            absphi = np.where(r > 0, np.abs(q) / r, 0.0).sum(1)
+            absg = np.where(r > 0, np.abs(q) / r ** 2, 0.0).sum(1)
+        u = 2.0 ** -53
+        assert np.all(np.abs(a - b) <= (8 + 2 * ns) * u * absphi + 1e-300)
+        assert np.all(np.abs(ga - gb) <= (16 + 2 * ns) * u * absg[:, None] + 1e-300)
+
+
+def test_host_path_fmm_matches_the_scalar_oracle(oracle):
+    """The reference's host path (lists made once, batched M2L in blocks of 64 targets with
+    four columns a pass, the AVX-512 P2P) gives the scalar oracle's FMM to rounding."""
+    x, q = oracle.point_sets("sphere", 30000, 4)
+    a, ga = oracle.Fmm(x, x, 8, 64).evaluate(q, threads=4)
+    b, gb = oracle.Fmm(x, x, 8, 64, host_path=True).evaluate(q, threads=4)
+    assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-13
+    assert np.linalg.norm(ga - gb) / np.linalg.norm(ga) < 1e-13
