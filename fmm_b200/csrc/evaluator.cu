@@ -298,14 +298,16 @@ void load_or_build_tables(fmmgpu_fmm* f) {
 
 // Host part of a build: plan, tables, leaf-scaled coordinates (no device work).
 std::unique_ptr<fmmgpu_fmm> build_host(const fmmgpu_settings* settings, size_t ns, const double* src, size_t nt,
-                                       const double* tgt, std::vector<double>& us, std::vector<double>& ut) {
+                                       const double* tgt, std::vector<double>& us, std::vector<double>& ut,
+                                       bool device_points = false) {
     check_settings(settings);
     const fmmgpu_settings& s = *settings;
     if ((ns && !src) || (nt && !tgt)) throw Failure(FMMGPU_INVALID_ARGUMENT, "null points");
     auto f = std::make_unique<fmmgpu_fmm>();
     f->settings = s;
     keep_cache_dirs(f.get());
-    f->plan = build_plan(ns, src, nt, tgt, s.max_level, s.max_points_per_leaf);
+    if (device_points) CUDA_TRY(cudaSetDevice(s.device));
+    f->plan = build_plan(ns, src, nt, tgt, s.max_level, s.max_points_per_leaf, device_points);
     load_or_build_tables(f.get());
     leaf_scaled(f->plan, src, tgt, us, ut);
     f->near_pairs = count_near_pairs(f->plan);
@@ -588,7 +590,7 @@ int fmmgpu_fmm_build(const fmmgpu_settings* settings, size_t ns, const double* s
             throw Failure(FMMGPU_NO_DEVICE, "no CUDA device is visible");
         }
         std::vector<double> us, ut;
-        auto f = build_host(settings, ns, src, nt, tgt, us, ut);
+        auto f = build_host(settings, ns, src, nt, tgt, us, ut, true);  // the point stages on the GPU
         build_device(f.get(), us, ut);
         f->symmetric = src == tgt && ns == nt;
         if (!f->symmetric) {
@@ -674,7 +676,8 @@ int fmmgpu_fmm_vjp(fmmgpu_fmm* f, const double* charges, const double* cotangent
         if (!f->symmetric) {
             if (!f->transpose) {  // the swapped problem: charges at the targets, evaluated at the sources
                 std::vector<double> us, ut;
-                auto t = build_host(&f->settings, (size_t)nt, f->tgt_pts.data(), (size_t)ns, f->src_pts.data(), us, ut);
+                auto t = build_host(&f->settings, (size_t)nt, f->tgt_pts.data(), (size_t)ns, f->src_pts.data(), us, ut,
+                                    true);
                 build_device(t.get(), us, ut);
                 t->symmetric = true;  // never asked for its own transpose
                 f->transpose = t.release();

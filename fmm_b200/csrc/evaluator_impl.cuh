@@ -33,6 +33,11 @@ struct HhState {
     DevBuf M, L, Y, Yo, m2l, m2m, l2l, far_phi, far_g;
     HhLevels lv{};
     bool built = false;
+    // the mixed form's tensor-core M2L (p <= 10): tiles over every level, (level, offset,
+    // half) as the table index, the table images, and the multipoles' tensor maps
+    DevBuf tc_d, tc_begin, tc_count, tc_img;
+    int64_t tc_ntiles = 0;
+    CUtensorMap mmap{}, vmap{};
 };
 
 // ----------------------------------------------------------------------------------
@@ -1221,6 +1226,8 @@ struct Evaluator final : EvaluatorBase {
 
     // ---- the Helmholtz FMM (real k): complex expansions as row pairs, per-level tables ----
     static constexpr int NE = 2 * NC;  // order of a complex translation as a real matrix
+    // the mixed form's Helmholtz M2L on the tensor cores ((p+1)^2 <= 128: p <= 10)
+    static constexpr bool kHhTensor = kMixed && P <= 10;
     HhState hh;
 
     // the complex translation of a host table (a real 2n x n matrix per set, column-major,
@@ -1255,7 +1262,7 @@ struct Evaluator final : EvaluatorBase {
             const size_t mv = 2 * (size_t)m;
             hh.M.alloc(sizeof(T) * mv * ms_of(P) * nb);
             hh.L.alloc(sizeof(T) * mv * ms_of(P) * nb);
-            hh.Y.alloc(sizeof(T) * mv * ys_of(P) * (plan.v.nnz() + 1));
+            hh.Y.alloc(sizeof(T) * mv * (kHhTensor ? 256 : ys_of(P)) * (plan.v.nnz() + 1));
             hh.Yo.alloc(sizeof(T) * mv * ys_of(P) * nb);
             hh.far_phi.alloc(sizeof(double) * 2 * (size_t)m * (dp.ntgt + 1));
             if (gradients) hh.far_g.alloc(sizeof(double) * 6 * (size_t)m * (dp.ntgt + 1));
@@ -1272,14 +1279,17 @@ struct Evaluator final : EvaluatorBase {
             if (GemmShape<P, T, true>::SMEM > 48 * 1024)
                 CUDA_TRY(cudaFuncSetAttribute(m2l_gemm_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               GemmShape<P, T, true>::SMEM));
+            if constexpr (kHhTensor) hh_tc_tiles();
             hh.built = true;
         }
         if (k == hh.k) return;
         const auto t0 = std::chrono::steady_clock::now();
         for (int l = 0; l < NL; ++l) hh.lv.kl[l] = k * plan.side * std::ldexp(1.0, -(l + 1));
         const size_t set = (size_t)NE * NE;
-        std::vector<T> m2l((size_t)std::max(NL - 2, 1) * 316 * set), m2m((size_t)NL * 8 * set), l2l((size_t)NL * 8 * set);
+        std::vector<T> m2l(kHhTensor ? 0 : (size_t)std::max(NL - 2, 1) * 316 * set), m2m((size_t)NL * 8 * set),
+            l2l((size_t)NL * 8 * set);
         std::vector<double> host, hm, hl;
+        std::vector<uint32_t> tc_img;
         for (int l = 2; l < NL; ++l) {
             bool any = false;
             for (int64_t b = plan.level_start[l]; b < plan.level_start[l + 1] && !any; ++b)
@@ -1293,7 +1303,12 @@ struct Evaluator final : EvaluatorBase {
                 if (!table_cache_dir.empty())
                     table_cache_store(table_cache_dir, kTableHelmholtzM2l, P, hh.lv.kl[l], host, &why);
             }
-            hh_block(host, 316, 1.0, m2l, (size_t)(l - 2) * 316 * set);
+            if constexpr (kHhTensor) {
+                tc_img.resize((size_t)(l - 2) * 316 * 2 * TcTs<P, true>::IMG_WORDS);
+                append_tc_complex_images<P>(host, tc_img);
+            } else {
+                hh_block(host, 316, 1.0, m2l, (size_t)(l - 2) * 316 * set);
+            }
         }
         for (int l = 0; l + 1 < NL; ++l) {
             const size_t half = (size_t)8 * 2 * NC * NC;
@@ -1313,11 +1328,66 @@ struct Evaluator final : EvaluatorBase {
             hh_block(hm, 8, 1.0, m2m, (size_t)l * 8 * set);
             hh_block(hl, 8, 0.5, l2l, (size_t)(l + 1) * 8 * set);
         }
-        hh.m2l.upload(m2l);
+        if constexpr (kHhTensor) {
+            tc_img.resize((size_t)std::max(NL - 2, 1) * 316 * 2 * TcTs<P, true>::IMG_WORDS);
+            hh.tc_img.upload(tc_img);
+            std::vector<uint32_t>().swap(tc_img);
+        } else {
+            hh.m2l.upload(m2l);
+        }
         hh.m2m.upload(m2m);
         hh.l2l.upload(l2l);
         hh.k = k;
         hh_table_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    // The mixed form's tensor-core Helmholtz M2L: tiles of NT / (2m) pairs (each pair's 2m
+    // columns: the real and imaginary planes of its vectors) over the V pairs of every
+    // level, by (level, offset), each run listed twice (halves A_r and A_i), table index
+    // ((level - 2) * 316 + d) * 2 + half; the multipoles' tensor maps over the complex rows.
+    void hh_tc_tiles() {
+        if constexpr (kHhTensor) {
+            using S = TcTs<P, true>;
+            Tiles all, lvl;
+            std::vector<int64_t> pe, lstart;
+            std::vector<int32_t> ps;
+            batches(std::max(1, S::NT / (2 * m)), all, lvl, lstart, pe, ps);
+            tc_halves_force(lvl, lstart);
+            for (int l = 0; l < plan.nlevels; ++l)
+                for (int64_t i = lstart[l]; i < lstart[l + 1]; ++i) lvl.d[i] += (l - 2) * 316 * 2;
+            hh.tc_ntiles = (int64_t)lvl.d.size();
+            hh.tc_d.upload(lvl.d);
+            hh.tc_begin.upload(lvl.begin);
+            hh.tc_count.upload(lvl.count);
+            const int64_t rows = (int64_t)plan.nboxes() * 2 * m;
+            encode_multipole_map<P>(&hh.mmap, reinterpret_cast<const float*>(hh.M.ptr), rows);
+            encode_multipole_map<P>(&hh.vmap, reinterpret_cast<const float*>(hh.M.ptr), rows, 2 * m);
+            CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          S::SMEM));
+        }
+    }
+
+    // every run of tiles of one table index d listed twice, as 2d then 2d + 1 (per level)
+    static void tc_halves_force(Tiles& t, std::vector<int64_t>& lstart) {
+        Tiles o;
+        std::vector<int64_t> nseg(lstart.size(), 0);
+        for (size_t sgi = 0; sgi + 1 < lstart.size(); ++sgi) {
+            nseg[sgi] = (int64_t)o.d.size();
+            for (int64_t i = lstart[sgi]; i < lstart[sgi + 1];) {
+                int64_t j = i;
+                while (j < lstart[sgi + 1] && t.d[j] == t.d[i]) ++j;
+                for (int h = 0; h < 2; ++h)
+                    for (int64_t x = i; x < j; ++x) {
+                        o.d.push_back(2 * t.d[x] + h);
+                        o.begin.push_back(t.begin[x]);
+                        o.count.push_back(t.count[x]);
+                    }
+                i = j;
+            }
+        }
+        nseg.back() = (int64_t)o.d.size();
+        lstart = nseg;
+        t = std::move(o);
     }
 
     void helmholtz_fmm(double kre, double kim, const double* d_q, double* d_phi, double* d_grad) override {
@@ -1364,14 +1434,25 @@ struct Evaluator final : EvaluatorBase {
                 m2m_reduce_kernel<P, T><<<counted((unsigned)n), round32(NC), 0, stream>>>(
                     dp, m2m_par.as<int32_t>() + m2m_start[l], n, mv, hh.Yo.as<T>(), hM);
         }
-        // M2L products of every level (their tables are per level)
-        for (int l = 2; l <= L; ++l) {
-            const int64_t t0 = lvl_tiles[l], nt = lvl_tiles[l + 1] - lvl_tiles[l];
-            if (nt)
-                m2l_gemm_kernel<P, T, true><<<counted((unsigned)nt), 256, gsm, stream>>>(
-                    ltile_d.as<int32_t>() + t0, ltile_begin.as<int64_t>() + t0, ltile_count.as<int32_t>() + t0,
-                    nullptr, pair_src.as<int32_t>(), m, hh.m2l.as<T>() + (size_t)(l - 2) * 316 * set, hM,
-                    hh.Y.as<T>());
+        // M2L products of every level (their tables are per level): the mixed form on the
+        // tensor cores in one launch over every level, f64 on the SIMT GEMM level by level
+        if constexpr (kHhTensor) {
+            if (hh.tc_ntiles) {
+                const unsigned grid = (unsigned)std::min<int64_t>(hh.tc_ntiles, num_sms);
+                m2l_tc_kernel<P, true><<<counted(grid), 32 * kTcWarps, TcTs<P, true>::SMEM, stream>>>(
+                    hh.tc_d.as<int32_t>(), hh.tc_begin.as<int64_t>(), hh.tc_count.as<int32_t>(), hh.tc_ntiles,
+                    pair_src.as<int32_t>(), 2 * m, hh.tc_img.as<uint32_t>(), hh.mmap, hh.vmap,
+                    reinterpret_cast<float*>(hh.Y.ptr), tc_error.as<int>());
+            }
+        } else {
+            for (int l = 2; l <= L; ++l) {
+                const int64_t t0 = lvl_tiles[l], nt = lvl_tiles[l + 1] - lvl_tiles[l];
+                if (nt)
+                    m2l_gemm_kernel<P, T, true><<<counted((unsigned)nt), 256, gsm, stream>>>(
+                        ltile_d.as<int32_t>() + t0, ltile_begin.as<int64_t>() + t0, ltile_count.as<int32_t>() + t0,
+                        nullptr, pair_src.as<int32_t>(), m, hh.m2l.as<T>() + (size_t)(l - 2) * 316 * set, hM,
+                        hh.Y.as<T>());
+            }
         }
         // downward: per level the L2L products, the locals (L2L + V in offset order), P2L
         for (int l = 2; l <= L; ++l) {
@@ -1385,7 +1466,12 @@ struct Evaluator final : EvaluatorBase {
             }
             const int64_t b0 = plan.level_start[l], b1 = plan.level_start[l + 1];
             if (b1 > b0) {
-                if constexpr (kMixed)
+                if constexpr (kHhTensor)
+                    hh_local_reduce_tc_kernel<P><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
+                        dp, b0, b1, m, l >= 3, reinterpret_cast<const float*>(hh.Yo.ptr),
+                        reinterpret_cast<const float*>(hh.Y.ptr), v_pos.as<int64_t>(),
+                        reinterpret_cast<float*>(hh.L.ptr));
+                else if constexpr (kMixed)
                     local_reduce4_kernel<P><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
                         dp, b0, b1, mv, l >= 3, 1, 0, reinterpret_cast<const float*>(hh.Yo.ptr),
                         reinterpret_cast<const float*>(hh.Y.ptr), v_pos.as<int64_t>(),

@@ -527,4 +527,37 @@ __global__ void __launch_bounds__(128) hh_leaf_far_kernel(DevPlan plan, HhLevels
     }
 }
 
+// The locals of one level from the tensor-core complex M2L's products (f32): for every box
+// with a target below it and every vector v,
+//   L_re = (L2L part) + sum_V (A_r x_re - A_i x_im),  L_im = (L2L part) + sum_V (A_i x_re + A_r x_im)
+// with a pair's products Y[pos][2v + c][0..n) = A_r x_c and [128..128+n) = A_i x_c (row
+// stride 256), V entries in row order; the L2L part (with_l2l) from the SIMT complex GEMM's
+// rows 2v, 2v + 1 of stride ys_of(P).  Block per box, thread per slot.
+template <int P>
+__global__ void hh_local_reduce_tc_kernel(DevPlan plan, int64_t b0, int64_t b1, int m, int with_l2l,
+                                          const float* __restrict__ Yo, const float* __restrict__ Yv,
+                                          const int64_t* __restrict__ vpos, float* __restrict__ L) {
+    constexpr int NC = nc_of(P), YS = ys_of(P), MS = ms_of(P);
+    const int64_t b = b0 + blockIdx.x;
+    if (b >= b1 || plan.tgt_below[b] == 0) return;
+    const int64_t e0 = plan.v_row[b], e1 = plan.v_row[b + 1];
+    for (int v = 0; v < m; ++v)
+        for (int t = threadIdx.x; t < NC; t += blockDim.x) {
+            float sr = 0.0f, si = 0.0f;
+            if (with_l2l) {
+                sr = Yo[((int64_t)b * 2 * m + 2 * v) * YS + t];
+                si = Yo[((int64_t)b * 2 * m + 2 * v + 1) * YS + t];
+            }
+            for (int64_t e = e0; e < e1; ++e) {
+                const float* y = Yv + (vpos[e] * 2 * m + 2 * v) * 256;
+                const float rr = __ldcs(y + t), ir = __ldcs(y + 128 + t);        // A_r x_re, A_i x_re
+                const float ri = __ldcs(y + 256 + t), ii = __ldcs(y + 384 + t);  // A_r x_im, A_i x_im
+                sr += rr - ii;
+                si += ir + ri;
+            }
+            L[((int64_t)b * 2 * m + 2 * v) * MS + t] = sr;
+            L[((int64_t)b * 2 * m + 2 * v + 1) * MS + t] = si;
+        }
+}
+
 }  // namespace fmmb

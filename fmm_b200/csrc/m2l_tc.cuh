@@ -161,7 +161,12 @@ constexpr int kTcMmaWarp = 16;    // the MMA issuer's warp
 constexpr int kTcGatherWarp = 17; // the gather issuer's warp
 constexpr long long kTcWait = 4000000000LL;  // clock cycles (about 2 s)
 
-template <int P>
+// CPLX: the Helmholtz form, a complex table A = A_r + i A_i applied to the real and the
+// imaginary plane of a multipole as two columns (its two expansion rows), with the table's
+// rows [A_r; A_i] as two halves of 128 output slots (the n = (p+1)^2 rows of each padded):
+// the products of a column are A_r x in slots 0..n and A_i x in slots 128..128+n of a
+// 256-slot row, which the complex local reduce combines into the local's two planes.
+template <int P, bool CPLX = false>
 struct TcTs {
     static constexpr int NC = nc_of(P);
     static constexpr int KA = (NC + 31) / 32;
@@ -169,7 +174,8 @@ struct TcTs {
     static constexpr int KSTEPS = KP / 8;
     // output slot halves: (p+1)^2 > 128 (p = 11, 12) takes two passes over a tile's
     // columns, each with the table rows of one half (128 slots) in tensor memory
-    static constexpr int H = NC > 128 ? 2 : 1;
+    static constexpr int H = (CPLX || NC > 128) ? 2 : 1;
+    static constexpr int YS = CPLX ? 256 : ys_of(P);  // product row stride (floats)
     // columns per tile (UMMA N): 96 at p = 7, 8 (KP = 96), where shared memory then holds
     // two raw stages (measured faster than 64 columns with four); 64 at p = 9, 10
     // (KP = 128), the most beside two X stages and two raw stages; 48 at p = 11, 12
@@ -185,7 +191,7 @@ struct TcTs {
     static constexpr int COL_AHI = 0, COL_ALO = KP, COL_D0 = 2 * KP;  // TMEM columns
     static constexpr int TMEM_COLS = 512;
     static constexpr int IMG_WORDS = 2 * 128 * KP;  // table image words per (offset, half) (hi, lo)
-    static_assert(NC <= 256, "two halves of UMMA M = 128 output slots");
+    static_assert(NC <= (CPLX ? 128 : 256), "two halves of UMMA M = 128 output slots");
     static_assert(2 * KP + 2 * NT <= TMEM_COLS, "TMEM budget");
     static_assert(NT % 16 == 0 && NT / 4 <= 32, "UMMA N; gather rows: four per lane");
     static_assert(RS >= 2, "raw stages");
@@ -247,7 +253,7 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-template <int P>
+template <int P, bool CPLX = false>
 __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
                                                                   const int64_t* __restrict__ tile_begin,
                                                                   const int32_t* __restrict__ tile_count,
@@ -257,8 +263,8 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   const __grid_constant__ CUtensorMap mmap,
                                                                   const __grid_constant__ CUtensorMap vmap,
                                                                   float* __restrict__ Y, int* __restrict__ error) {
-    using S = TcTs<P>;
-    constexpr int NT = S::NT, KP = S::KP;
+    using S = TcTs<P, CPLX>;
+    constexpr int NT = S::NT, KP = S::KP, YS = S::YS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 stages][hi, lo]
     unsigned char* rbuf = xbuf + 4 * S::X_BYTES;                                      // raw [RS stages][NT][KP]
@@ -509,7 +515,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            if (128 * h + 32 * q < ys_of(P)) {
+            if (128 * h + 32 * q < YS) {
                 // products at rows p0 * m + c (a tile's rows are consecutive), whole 128-byte
                 // lines (rows >= NC of the table are zero), 16 columns per TMEM load
 #pragma unroll 1
@@ -517,10 +523,10 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                     if (c0 >= ncol) break;
                     float v0[16];
                     tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * NT + c0), v0);
-                    float* yb = Y + (p0 * m + c0) * ys_of(P) + n;
+                    float* yb = Y + (p0 * m + c0) * YS + n;
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
-                        if (c0 + i < ncol) __stcs(yb + (int64_t)i * ys_of(P), v0[i]);
+                        if (c0 + i < ncol) __stcs(yb + (int64_t)i * YS, v0[i]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
@@ -607,6 +613,35 @@ void build_tc_table_images(const std::vector<double>& m2l, std::vector<uint32_t>
                 img[base] = hi;
                 img[base + (size_t)128 * S::KP] = lo;
             }
+}
+
+// Host: the complex form's images of one level's tables (host layout: per offset a real
+// 2n x n matrix, column-major, column j = the local of e_j, real plane over imaginary
+// plane), appended to img: per offset d, half 0 holds A_r (rows 0..n), half 1 A_i, each
+// [part][128][KP] of tf32 bits; table index (level set * 316 + d) * 2 + half.
+template <int P>
+void append_tc_complex_images(const std::vector<double>& host, std::vector<uint32_t>& img) {
+    using S = TcTs<P, true>;
+    constexpr int NC = S::NC;
+    const size_t base0 = img.size();
+    img.resize(base0 + (size_t)316 * 2 * S::IMG_WORDS, 0u);
+    for (int d = 0; d < 316; ++d)
+        for (int h = 0; h < 2; ++h)
+            for (int n = 0; n < NC; ++n)
+                for (int k = 0; k < NC; ++k) {
+                    const float a = (float)host[(size_t)d * 2 * NC * NC + (size_t)k * 2 * NC + h * NC + n];
+                    uint32_t bits;
+                    std::memcpy(&bits, &a, 4);
+                    const uint32_t hi = tf32_round_bits(bits);
+                    float fhi;
+                    std::memcpy(&fhi, &hi, 4);
+                    const float rem = a - fhi;
+                    uint32_t rb;
+                    std::memcpy(&rb, &rem, 4);
+                    const size_t at = base0 + ((size_t)d * 2 + h) * S::IMG_WORDS + (size_t)n * S::KP + k;
+                    img[at] = hi;
+                    img[at + (size_t)128 * S::KP] = tf32_round_bits(rb);
+                }
 }
 
 }  // namespace fmmb

@@ -17,6 +17,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -84,8 +85,22 @@ Plan merge_plans(std::vector<TreePart>& parts, std::vector<double>& us, std::vec
 // Builds the cubic domain, the tree of the distinct level-16 keys of sources ++ targets
 // (refined while a box holds more than max_keys keys, then 2:1 balanced), the box
 // index, the point order and the lists.  Throws std::runtime_error on bad input.
+// device_points: the point stages (keys, sort, each point's leaf, the order by leaf) on the
+// current CUDA device (plan_gpu.cu), with the same results.
 Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
-                int max_keys);
+                int max_keys, bool device_points = false);
+
+// The point stages of a build: the level-16 keys of sources ++ targets sorted and made
+// distinct, then, once the leaves are known (their first level-16 keys ascending and their
+// leaf indices), each point's leaf and the stable order of the points by leaf.
+struct PointSort {
+    virtual ~PointSort() = default;
+    virtual std::vector<uint64_t> distinct_keys() = 0;
+    virtual void leaf_order(const std::vector<uint64_t>& firsts, const std::vector<int32_t>& leaf_index, size_t nl,
+                            Plan& P) = 0;
+};
+std::unique_ptr<PointSort> device_point_sort(size_t ns, const double* src, size_t nt, const double* tgt,
+                                             const double box6[6]);
 
 // Leaf-scaled coordinate of CONVENTIONS 3.13: fl(fl(fl(x - a) * 2^(l+1)) / w) - (2i + 1).
 double leaf_coordinate(double x, double a, double w, int level, uint32_t index);

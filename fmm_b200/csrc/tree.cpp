@@ -1,12 +1,16 @@
 // Host plan build: domain, Morton keys, refinement, 2:1 balance, box index, point
 // order and interaction lists (see plan.hpp for the conventions it follows).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
+#include <string>
+#include <thread>
 #include <unordered_map>
 
+#include "morton.hpp"
 #include "plan.hpp"
 
 namespace fmmb {
@@ -14,16 +18,6 @@ namespace fmmb {
 namespace {
 
 constexpr uint64_t kLevelMask = 0x7FFF;
-
-inline uint64_t spread3(uint64_t x) {
-    x &= 0xFFFF;
-    x = (x | (x << 32)) & 0x1F00000000FFFFULL;
-    x = (x | (x << 16)) & 0x1F0000FF0000FFULL;
-    x = (x | (x << 8)) & 0x100F00F00F00F00FULL;
-    x = (x | (x << 4)) & 0x10C30C30C30C30C3ULL;
-    x = (x | (x << 2)) & 0x1249249249249249ULL;
-    return x;
-}
 
 inline uint64_t compact3(uint64_t x) {
     x &= 0x1249249249249249ULL;
@@ -35,12 +29,7 @@ inline uint64_t compact3(uint64_t x) {
     return x;
 }
 
-inline uint64_t encode(uint32_t i, uint32_t j, uint32_t k, int level) {
-    int d = kDeepest - level;
-    uint64_t m = (spread3((uint64_t)i << d) << 2) | (spread3((uint64_t)j << d) << 1) |
-                 spread3((uint64_t)k << d);
-    return (m << 15) | (uint64_t)level;
-}
+inline uint64_t encode(uint32_t i, uint32_t j, uint32_t k, int level) { return morton_encode_hd(i, j, k, level); }
 
 inline int key_level(uint64_t key) { return (int)(key & kLevelMask); }
 
@@ -178,7 +167,7 @@ int offset_index(int x, int y, int z) {
 }
 
 Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
-                int max_keys) {
+                int max_keys, bool device_points) {
     if (ns + nt == 0) throw std::runtime_error("no points");
     if (max_keys < 1) throw std::runtime_error("max_points_per_leaf must be at least 1");
     if (max_level > kDeepest) max_level = kDeepest;
@@ -229,14 +218,22 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         }
         return encode(id[0], id[1], id[2], kDeepest);
     };
-    std::vector<uint64_t> skey(ns), tkey(nt);
-    for (size_t i = 0; i < ns; ++i) skey[i] = point_key(src + 3 * i);
-    for (size_t i = 0; i < nt; ++i) tkey[i] = point_key(tgt + 3 * i);
-    std::vector<uint64_t> fine;
-    fine.reserve(ns + nt);
-    fine.insert(fine.end(), skey.begin(), skey.end());
-    fine.insert(fine.end(), tkey.begin(), tkey.end());
-    sort_unique(fine);  // distinct keys (route_keys on one rank)
+    // the point stages (keys, their distinct sorted set, later each point's leaf and the
+    // order by leaf) on the device when asked (plan_gpu.cu: the same keys and order), else here
+    std::unique_ptr<PointSort> dev = device_points ? device_point_sort(ns, src, nt, tgt, P.box6) : nullptr;
+    std::vector<uint64_t> skey, tkey, fine;
+    if (dev) {
+        fine = dev->distinct_keys();
+    } else {
+        skey.resize(ns);
+        tkey.resize(nt);
+        for (size_t i = 0; i < ns; ++i) skey[i] = point_key(src + 3 * i);
+        for (size_t i = 0; i < nt; ++i) tkey[i] = point_key(tgt + 3 * i);
+        fine.reserve(ns + nt);
+        fine.insert(fine.end(), skey.begin(), skey.end());
+        fine.insert(fine.end(), tkey.begin(), tkey.end());
+        sort_unique(fine);  // distinct keys (route_keys on one rank)
+    }
 
     std::vector<uint64_t> refined;
     refine(fine.data(), fine.size(), 0ULL, max_level, (size_t)max_keys, refined);
@@ -303,7 +300,8 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         size_t pos = (size_t)(std::upper_bound(firsts.begin(), firsts.end(), fk) - firsts.begin()) - 1;
         return morton_leaf_index[pos];
     };
-    for (int s = 0; s < 2; ++s) {
+    if (dev) dev->leaf_order(firsts, morton_leaf_index, nl, P);
+    for (int s = 0; s < (dev ? 0 : 2); ++s) {
         const std::vector<uint64_t>& keys = s ? tkey : skey;
         size_t n = keys.size();
         std::vector<int32_t> lf(n);
@@ -348,14 +346,53 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         if (a < 0 || c < 0 || e < 0 || a >= size || c >= size || e >= size) return -2;
         return km.find(encode((uint32_t)a, (uint32_t)c, (uint32_t)e, l));
     };
-    P.near.row.assign(nl + 1, 0);
-    P.w.row.assign(nl + 1, 0);
-    P.x.row.assign(nb + 1, 0);
-    P.v.row.assign(nb + 1, 0);
-    std::vector<int32_t> tmp;
-    std::vector<std::pair<int32_t, int32_t>> vtmp;
+    // the rows of two lists at once, in parallel over chunks of rows (each row depends on
+    // the tree only); the chunks' rows are joined in row order, so the lists are the
+    // same whatever the number of threads
+    struct Rows {
+        std::vector<int32_t> a, aux, b;
+        std::vector<int64_t> arow, brow;  // row ends within the chunk
+    };
+    auto two_lists = [](size_t nrows, Csr& A, Csr& B, bool with_aux, auto&& row_fn) {
+        const size_t nth = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+        const size_t nch = std::min(nrows, nth * 4) ? std::min(nrows, nth * 4) : 1;
+        std::vector<Rows> parts(nch);
+        std::vector<std::string> errors(nch);
+        std::atomic<size_t> next{0};
+        auto work = [&] {
+            for (size_t c; (c = next.fetch_add(1)) < nch;) {
+                try {
+                    for (size_t r = nrows * c / nch; r < nrows * (c + 1) / nch; ++r) row_fn(r, parts[c]);
+                } catch (const std::exception& e) {
+                    errors[c] = e.what();
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (size_t i = 1; i < nth; ++i) pool.emplace_back(work);
+        work();
+        for (auto& th : pool) th.join();
+        for (const auto& e : errors)
+            if (!e.empty()) throw std::runtime_error(e);
+        A.row.assign(nrows + 1, 0);
+        B.row.assign(nrows + 1, 0);
+        A.col.clear();
+        B.col.clear();
+        A.aux.clear();
+        size_t r = 0;
+        for (const Rows& pr : parts) {
+            const int64_t a0 = (int64_t)A.col.size(), b0 = (int64_t)B.col.size();
+            A.col.insert(A.col.end(), pr.a.begin(), pr.a.end());
+            if (with_aux) A.aux.insert(A.aux.end(), pr.aux.begin(), pr.aux.end());
+            B.col.insert(B.col.end(), pr.b.begin(), pr.b.end());
+            for (size_t i = 0; i < pr.arow.size(); ++i, ++r) {
+                A.row[r + 1] = a0 + pr.arow[i];
+                B.row[r + 1] = b0 + pr.brow[i];
+            }
+        }
+    };
     // near and W, per leaf
-    for (size_t j = 0; j < nl; ++j) {
+    two_lists(nl, P.near, P.w, false, [&](size_t j, Rows& out) {
         int32_t b = P.leaf_box[j];
         std::vector<int32_t> nearj, wj;
         if (P.tgt_below[b] > 0) {
@@ -392,16 +429,16 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
             nearj.erase(std::unique(nearj.begin(), nearj.end()), nearj.end());
             std::sort(wj.begin(), wj.end());
         }
-        P.near.col.insert(P.near.col.end(), nearj.begin(), nearj.end());
-        P.near.row[j + 1] = (int64_t)P.near.col.size();
-        P.w.col.insert(P.w.col.end(), wj.begin(), wj.end());
-        P.w.row[j + 1] = (int64_t)P.w.col.size();
-    }
+        out.a.insert(out.a.end(), nearj.begin(), nearj.end());
+        out.arow.push_back((int64_t)out.a.size());
+        out.b.insert(out.b.end(), wj.begin(), wj.end());
+        out.brow.push_back((int64_t)out.b.size());
+        });
     // V and X, per box
-    for (size_t bb = 0; bb < nb; ++bb) {
+    two_lists(nb, P.v, P.x, true, [&](size_t bb, Rows& out) {
         int32_t b = (int32_t)bb;
-        vtmp.clear();
-        tmp.clear();
+        std::vector<std::pair<int32_t, int32_t>> vtmp;
+        std::vector<int32_t> tmp;
         if (P.level[b] >= 1 && P.tgt_below[b] > 0) {
             int32_t par = P.parent[b];
             for (int dx = -1; dx <= 1; ++dx)
@@ -428,13 +465,13 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
             std::sort(tmp.begin(), tmp.end());
         }
         for (auto& e : vtmp) {
-            P.v.col.push_back(e.second);
-            P.v.aux.push_back(e.first);
+            out.a.push_back(e.second);
+            out.aux.push_back(e.first);
         }
-        P.v.row[bb + 1] = (int64_t)P.v.col.size();
-        P.x.col.insert(P.x.col.end(), tmp.begin(), tmp.end());
-        P.x.row[bb + 1] = (int64_t)P.x.col.size();
-    }
+        out.arow.push_back((int64_t)out.a.size());
+        out.b.insert(out.b.end(), tmp.begin(), tmp.end());
+        out.brow.push_back((int64_t)out.b.size());
+        });
     return P;
 }
 
