@@ -608,13 +608,17 @@ static __global__ void near_stream_kernel(DevPlan plan, int64_t nleaves, const N
 
 constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
 
+// NB flush buffers (NB - 1 flushes in flight while one is computed).
+constexpr int kStBufs = 3;
+
 template <bool GRAD, int W>
 __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
     DevPlan plan, P2pItems items, int m, int near, float rmax, P2pStream st, const float* __restrict__ sq,
     const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, double* __restrict__ far_g,
     int accumulate, double* __restrict__ out_phi, double* __restrict__ out_g) {
-    __shared__ float4 sxy[W][2][kStPairs];  // (x0, x1, y0, y1), two flushes
-    __shared__ float4 szq[W][2][kStPairs];  // (z0, z1, q0, q1)
+    constexpr int NB = kStBufs;
+    __shared__ float4 sxy[W][NB][kStPairs];  // (x0, x1, y0, y1), NB flushes
+    __shared__ float4 szq[W][NB][kStPairs];  // (z0, z1, q0, q1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t item = (int64_t)blockIdx.x * W + warp;
     if (item >= items.count) return;
@@ -677,14 +681,20 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         if (iv < m) load_idx();  // lands while the flush being computed runs
     };
     load_idx();
-    issue(0);
+    for (int f = 0; f < NB - 1; ++f) {  // the first NB - 1 flushes in flight (empty groups past the end)
+        if (f < total) issue(f);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     double aphi = 0.0, ag0 = 0.0, ag1 = 0.0, ag2 = 0.0;
     int cv = 0, cfl = 0;  // the flush being computed
     for (int f = 0; f < total; ++f) {
-        const int b = f & 1;
-        asm volatile("cp.async.wait_all;" ::: "memory");
+        const int b = f % NB;
+        // flush f has landed once at most NB - 2 younger groups are pending
+        asm volatile("cp.async.wait_group %0;" ::"n"(NB - 2) : "memory");
         __syncwarp();
-        if (f + 1 < total) issue(b ^ 1);  // buffer b ^ 1 was last read by flush f - 1
+        // buffer (f + NB - 1) % NB was last read by flush f - 1; an empty group keeps the count
+        if (f + NB - 1 < total) issue((f + NB - 1) % NB);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
         const int rem = np_row - cfl * kStPairs;
         const int npairs = rem < kStPairs ? rem : kStPairs;
         float2 pphi = f2(0.f, 0.f), pg0 = f2(0.f, 0.f), pg1 = f2(0.f, 0.f), pg2 = f2(0.f, 0.f);
