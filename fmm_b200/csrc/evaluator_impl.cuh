@@ -759,29 +759,14 @@ struct Evaluator final : EvaluatorBase {
             cap = (int64_t)found + 1024;
         }
         nclose = (int64_t)found;
-        std::vector<int64_t> ht(nclose), hs(nclose);
-        std::vector<int32_t> hl(nclose);
-        if (nclose) {
-            CUDA_TRY(cudaMemcpy(ht.data(), ot.ptr, sizeof(int64_t) * nclose, cudaMemcpyDeviceToHost));
-            CUDA_TRY(cudaMemcpy(hs.data(), os.ptr, sizeof(int64_t) * nclose, cudaMemcpyDeviceToHost));
-            CUDA_TRY(cudaMemcpy(hl.data(), ol.ptr, sizeof(int32_t) * nclose, cudaMemcpyDeviceToHost));
-        }
-        std::vector<int64_t> order(nclose);
-        for (int64_t i = 0; i < nclose; ++i) order[i] = i;
-        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
-            return ht[a] != ht[b] ? ht[a] < ht[b] : hs[a] < hs[b];
-        });
-        std::vector<int64_t> row(dp.ntgt + 1, 0), src(nclose);
-        std::vector<int32_t> lf(nclose);
-        for (int64_t i = 0; i < nclose; ++i) {
-            row[ht[order[i]] + 1]++;
-            src[i] = hs[order[i]];
-            lf[i] = hl[order[i]];
-        }
-        for (int64_t t = 0; t < dp.ntgt; ++t) row[t + 1] += row[t];
-        close_row.upload(row);
-        close_src.upload(src);
-        close_leaf.upload(lf);
+        // sorted by (target, source) into a CSR by target, on the device (plan_gpu.cu; the
+        // pair's key packs both indices in 64 bits)
+        if (dp.nsrc >= ((int64_t)1 << 32)) throw Failure(FMMGPU_UNSUPPORTED, "more than 2^32 sources");
+        close_row.alloc(sizeof(int64_t) * (size_t)(dp.ntgt + 2));
+        close_src.alloc(sizeof(int64_t) * (size_t)(nclose + 1));
+        close_leaf.alloc(sizeof(int32_t) * (size_t)(nclose + 1));
+        sort_close_pairs(nclose, ot.as<int64_t>(), os.as<int64_t>(), ol.as<int32_t>(), dp.ntgt, close_row.as<int64_t>(),
+                         close_src.as<int64_t>(), close_leaf.as<int32_t>());
         close.row = close_row.as<int64_t>();
         close.src = close_src.as<int64_t>();
         close.leaf = close_leaf.as<int32_t>();

@@ -101,6 +101,11 @@ struct PointSort {
 };
 std::unique_ptr<PointSort> device_point_sort(size_t ns, const double* src, size_t nt, const double* tgt,
                                              const double box6[6]);
+// The mixed P2P's near-singular pairs (target t[i], source s[i], source leaf l[i], device
+// arrays of n) sorted by (target, source) into a CSR by target: row[ntgt + 1], src[n],
+// leaf[n], device arrays (plan_gpu.cu); synchronises.
+void sort_close_pairs(int64_t n, const int64_t* t, const int64_t* s, const int32_t* l, int64_t ntgt, int64_t* row,
+                      int64_t* src, int32_t* leaf);
 
 // Leaf-scaled coordinate of CONVENTIONS 3.13: fl(fl(fl(x - a) * 2^(l+1)) / w) - (2i + 1).
 double leaf_coordinate(double x, double a, double w, int level, uint32_t index);

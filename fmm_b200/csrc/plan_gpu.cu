@@ -181,7 +181,52 @@ class DevicePointSort final : public PointSort {
     Buf<uint64_t> keys_;
 };
 
+__global__ void pair_keys_kernel(const int64_t* __restrict__ t, const int64_t* __restrict__ s, int64_t n,
+                                 uint64_t* __restrict__ keys) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = ((uint64_t)t[i] << 32) | (uint64_t)s[i];
+}
+
+__global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, int64_t n, int64_t* __restrict__ src) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) src[i] = (int64_t)(keys[i] & 0xFFFFFFFFull);
+}
+
+// row[t] = the first sorted pair whose target is >= t (t = 0..ntgt)
+__global__ void pair_rows_kernel(const uint64_t* __restrict__ keys, int64_t n, int64_t ntgt, int64_t* __restrict__ row) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t > ntgt) return;
+    const uint64_t k = (uint64_t)t << 32;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    row[t] = lo;
+}
+
 }  // namespace
+
+void sort_close_pairs(int64_t n, const int64_t* t, const int64_t* s, const int32_t* l, int64_t ntgt, int64_t* row,
+                      int64_t* src, int32_t* leaf) {
+    if (ntgt >= ((int64_t)1 << 31)) throw std::runtime_error("device plan build: too many targets");
+    if (n > 0) {
+        Buf<uint64_t> keys(n), sorted(n);
+        pair_keys_kernel<<<blocks(n), 256>>>(t, s, n, keys.p);
+        check(cudaGetLastError(), "pair keys");
+        size_t tb = 0;
+        check(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.p, sorted.p, l, leaf, n), "pair sort size");
+        Buf<unsigned char> temp(tb);
+        check(cub::DeviceRadixSort::SortPairs(temp.p, tb, keys.p, sorted.p, l, leaf, n), "pair sort");
+        pair_unpack_kernel<<<blocks(n), 256>>>(sorted.p, n, src);
+        pair_rows_kernel<<<blocks(ntgt + 1), 256>>>(sorted.p, n, ntgt, row);
+        check(cudaGetLastError(), "pair rows");
+        check(cudaDeviceSynchronize(), "pair sort");
+    } else {
+        check(cudaMemset(row, 0, sizeof(int64_t) * (size_t)(ntgt + 1)), "pair rows");
+    }
+}
 
 std::unique_ptr<PointSort> device_point_sort(size_t ns, const double* src, size_t nt, const double* tgt,
                                              const double box6[6]) {
