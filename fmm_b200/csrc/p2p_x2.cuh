@@ -608,8 +608,9 @@ static __global__ void near_stream_kernel(DevPlan plan, int64_t nleaves, const N
 
 constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
 
-// NB flush buffers (NB - 1 flushes in flight while one is computed).
-constexpr int kStBufs = 3;
+// NB flush buffers (NB - 1 flushes in flight while one is computed); three measured no
+// faster than two at the bench size (P2P 2.046 vs 2.042 ms): the flush latency is hidden.
+constexpr int kStBufs = 2;
 
 template <bool GRAD, int W>
 __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
