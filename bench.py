@@ -398,6 +398,17 @@ def run_ours(args):
         if t:
             roof["traffic"] = round(t["dram_bytes_per_unit"] * info["near_pairs"])
             roof["traffic_source"] = t["source"]
+    elif dominant == "m2l" and "bf16_tflops" in pk:
+        # the tensor-core M2L: 2 (p+1)^4 FLOP per V pair (the reference's count), against the
+        # dense TF32 rate, half the measured BF16 one
+        roof["kernel"] = "m2l_tc_kernel"
+        flop = info["v_pairs"] * 2.0 * float((P + 1) ** 4)
+        achieved = flop / (kinds["m2l"] * 1e-3) / 1e12
+        peak = 0.5 * float(pk["bf16_tflops"])
+        roof.update({"bound": "tensor", "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": "derived: dense TF32 = half the measured BF16 burst (MEASURED_PEAKS.json)",
+                     "op_model": "2 (p+1)^4 FLOP per V pair; the 3xTF32 split runs three such products"})
     else:
         roof.update({"bound": "unknown", "achieved": None, "peak": None, "unit": None, "frac": None,
                      "traffic": None})

@@ -124,7 +124,10 @@ struct Evaluator final : EvaluatorBase {
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
-    static constexpr bool kBfly = sizeof(T) == 4;  // register P2M/P2L (f32, vectors one after another)
+    // register P2M/P2L (f32, vectors one after another) up to p = 10; above, its (p+1)^2
+    // accumulators a lane exceed the register file (255 registers at p = 11, 12) and the
+    // shared-memory column sums run instead
+    static constexpr bool kBfly = sizeof(T) == 4 && P <= 10;
 
     // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
     static constexpr float kTheta2 = 0.0625f;

@@ -828,10 +828,10 @@ struct P2pItems {
 // block per leaf holds every thread of its block while a leaf of few targets keeps one
 // warp busy, a warp per item leaves no idle warp resident.  leaf_far_mv_items_kernel forms
 // each target's harmonics once for up to VB vectors (l2p_eval_mv / m2p_eval_mv).
-// The gradient form is held to 96 registers up to p = 8 (21 warps an SM, no spills), to
-// 168 at p = 9, 10 and 255 above (the harmonic rows and the coefficient loop grow with p).
+// The gradient form is held to 96 registers up to p = 8 (21 warps an SM, no spills) and to
+// 168 above (12 warps an SM; no spills to p = 12).
 template <int P, bool GRAD>
-__global__ void __launch_bounds__(128, P <= 8 ? 5 : P <= 10 ? 3 : 2) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
+__global__ void __launch_bounds__(128, P <= 8 ? 5 : 3) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
                                                              const float4* __restrict__ tpos,
                                                              const float* __restrict__ M, const float* __restrict__ Lc,
                                                              double* __restrict__ far_phi, double* __restrict__ far_g) {
