@@ -124,10 +124,13 @@ struct Evaluator final : EvaluatorBase {
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
-    // register P2M/P2L (f32, vectors one after another) up to p = 10; above, its (p+1)^2
+    // register P2M (f32, vectors one after another) up to p = 10; above, its (p+1)^2
     // accumulators a lane exceed the register file (255 registers at p = 11, 12) and the
-    // shared-memory column sums run instead
+    // shared-memory column sums run instead (p = 11, sphere 1e6: 0.19 against 0.24 ms).
+    // P2L keeps the register kernel at every order: its boxes sum many more sources, and
+    // the shared-memory form measured slower there (p = 11: 0.60 against 0.28 ms)
     static constexpr bool kBfly = sizeof(T) == 4 && P <= 10;
+    static constexpr bool kBflyP2L = sizeof(T) == 4;
 
     // near-singular threshold of the mixed form: r2 < 1/16 in target-leaf units (|d| < r_t/4)
     static constexpr float kTheta2 = 0.0625f;
@@ -1106,11 +1109,11 @@ struct Evaluator final : EvaluatorBase {
     void p2l_level(int l) {  // the boxes of level l with an X list
         const int64_t b0 = xbox_start[l], b1 = xbox_start[l + 1];
         if (b1 <= b0) return;
-        if (kBfly && m == 1)
+        if (kBflyP2L && m == 1)
             expand_bfly_kernel<P, true, false><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
                 reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
-        else if (kBfly)
+        else if (kBflyP2L)
             expand_bfly_kernel<P, true, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
                 reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
