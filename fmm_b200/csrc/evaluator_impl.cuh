@@ -121,6 +121,13 @@ struct Evaluator final : EvaluatorBase {
     P2pItems items{};
     std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
     std::vector<int32_t> item_leaf_h;  // the items' leaves (host copy, ascending)
+    // The mixed P2P's own work lists: every item of 32 targets (one target a lane, the
+    // FULL kernel), then the remainders of the leaves cut into items of 16 and 8 targets
+    // and a last one below 8 (K = 32 / n lanes a target split its pair-steps, so no lane
+    // idles but in the last item); each list in leaf order, with explicit target counts.
+    DevBuf pitem_leaf, pitem_t0, pitem_n;
+    P2pItems pfull{}, ppart{};
+    std::vector<int64_t> pfull_lstart, ppart_lstart;  // first item of each level (nlevels + 1)
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
@@ -732,6 +739,47 @@ struct Evaluator final : EvaluatorBase {
         items.leaf = item_leaf.as<int32_t>();
         items.t0 = item_t0.as<int64_t>();
         items.count = (int64_t)il.size();
+        if constexpr (kMixed) build_p2p_lists();
+    }
+
+    void build_p2p_lists() {
+        std::vector<int32_t> fl, pl, fn, pn;
+        std::vector<int64_t> ft, pt;
+        for (size_t j = 0; j < plan.nleaves(); ++j) {
+            int64_t t = plan.tgt_start[j];
+            const int64_t t1 = plan.tgt_start[j + 1];
+            for (; t + 32 <= t1; t += 32) {
+                fl.push_back((int32_t)j);
+                ft.push_back(t);
+                fn.push_back(32);
+            }
+            for (int sz : {16, 8, 0}) {
+                const int64_t r = t1 - t;
+                if (r <= 0) break;
+                const int n = sz ? (r >= sz ? sz : 0) : (int)r;
+                if (!n) continue;
+                pl.push_back((int32_t)j);
+                pt.push_back(t);
+                pn.push_back(n);
+                t += n;
+            }
+        }
+        const int64_t nf = (int64_t)fl.size(), np = (int64_t)pl.size();
+        auto starts = [&](const std::vector<int32_t>& lv, std::vector<int64_t>& out) {
+            out.assign(plan.nlevels + 1, (int64_t)lv.size());
+            for (int l = plan.nlevels - 1; l >= 0; --l)
+                out[l] = std::lower_bound(lv.begin(), lv.end(), (int32_t)plan.leaf_level_start[l]) - lv.begin();
+        };
+        starts(fl, pfull_lstart);
+        starts(pl, ppart_lstart);
+        fl.insert(fl.end(), pl.begin(), pl.end());
+        ft.insert(ft.end(), pt.begin(), pt.end());
+        fn.insert(fn.end(), pn.begin(), pn.end());
+        pitem_leaf.upload(fl);
+        pitem_t0.upload(ft);
+        pitem_n.upload(fn);
+        pfull = P2pItems{pitem_leaf.as<int32_t>(), pitem_t0.as<int64_t>(), nf, pitem_n.as<int32_t>()};
+        ppart = P2pItems{pitem_leaf.as<int32_t>() + nf, pitem_t0.as<int64_t>() + nf, np, pitem_n.as<int32_t>() + nf};
     }
 
     // The mixed form's f64 pairs: found on the device with the f32 arithmetic of the P2P
@@ -864,8 +912,8 @@ struct Evaluator final : EvaluatorBase {
             CUDA_TRY(cudaEventRecord(ev_fork, stream));
             CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
             close_sums(near_stream);
-            p2p_items(0, items.count, 1, 2, near_phi.as<double>(), gradients ? near_g.as<double>() : nullptr,
-                      near_stream);
+            p2p_levels(0, plan.nlevels, 1, 2, near_phi.as<double>(), gradients ? near_g.as<double>() : nullptr,
+                       near_stream);
             CUDA_TRY(cudaEventRecord(ev_join, near_stream));
             run_far();
             CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
@@ -888,7 +936,7 @@ struct Evaluator final : EvaluatorBase {
             run_far();
         }
         if (forked) CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
-        if (items.count) timer.run(kP2P, [&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
+        if (items.count) timer.run(kP2P, [&] { p2p_levels(0, plan.nlevels, kinds & 1, 0, d_phi, d_grad); });
         CUDA_TRY(cudaGetLastError());
     }
 
@@ -937,7 +985,7 @@ struct Evaluator final : EvaluatorBase {
             int pick = p2p_warps;
             for (int w : {1, 2, 4}) {
                 p2p_warps = w;
-                const float ms = time([&] { p2p_items(0, items.count, kinds & 1, 0, d_phi, d_grad); });
+                const float ms = time([&] { p2p_levels(0, plan.nlevels, kinds & 1, 0, d_phi, d_grad); });
                 if (w == 1 || ms < best) best = ms, pick = w;
             }
             p2p_warps = pick;
@@ -1153,7 +1201,7 @@ struct Evaluator final : EvaluatorBase {
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
     }
 
-    template <int W>
+    template <int W, bool FULL>
     void p2p_x2_launch(const P2pItems& it, int near, int accumulate, double* d_phi, double* fg, double* og,
                        cudaStream_t s) {
         const unsigned g = (unsigned)((it.count + W - 1) / W);
@@ -1162,12 +1210,20 @@ struct Evaluator final : EvaluatorBase {
         const auto* q = reinterpret_cast<const float*>(sq.ptr);
         if (p2p_path == 1) {
             const P2pStream st{st_rowpair.as<int64_t>(), st_xy.as<float4>(), st_zz.as<float2>(), st_idx.as<int2>()};
-            if (!gradients)
+            if (!gradients) {
                 p2p_st_mv_kernel<W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, st, q, tp, close,
                                                                  far_phi.as<double>(), accumulate, d_phi);
-            else
-                p2p_st_kernel<true, W><<<counted(g), 32 * W, 0, s>>>(dp, it, m, near, kRmax, st, q, tp, close,
-                                                                   far_phi.as<double>(), fg, accumulate, d_phi, og);
+                return;
+            }
+            if constexpr (FULL) {
+                if (m == 1) {  // the common case: one vector, one target a lane
+                    p2p_st_kernel<true, W, true, true><<<counted(g), 32 * W, 0, s>>>(
+                        dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og);
+                    return;
+                }
+            }
+            p2p_st_kernel<true, W, false, FULL><<<counted(g), 32 * W, 0, s>>>(
+                dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og);
             return;
         }
         if (!gradients) {  // potentials: the pair geometry shared by up to kX2Vb vectors (any m)
@@ -1185,24 +1241,39 @@ struct Evaluator final : EvaluatorBase {
                                                                 accumulate, d_phi, og);
     }
 
-    // P2P over work items [i0, i1); accumulate = 0 adds the far partial and writes the
-    // scaled output in caller order, 1 adds into the leaf-order store (level calls), 2
-    // writes the near field alone in leaf order into d_phi / d_grad
-    void p2p_items(int64_t i0, int64_t i1, int near, int accumulate, double* d_phi, double* d_grad,
-                   cudaStream_t s = nullptr) {
-        if (i1 <= i0) return;
+    template <bool FULL>
+    void p2p_x2_shape(const P2pItems& it, int near, int accumulate, double* d_phi, double* fg, double* og,
+                      cudaStream_t s) {
+        if (!it.count) return;
+        if (p2p_warps == 1)
+            p2p_x2_launch<1, FULL>(it, near, accumulate, d_phi, fg, og, s);
+        else if (p2p_warps == 2)
+            p2p_x2_launch<2, FULL>(it, near, accumulate, d_phi, fg, og, s);
+        else
+            p2p_x2_launch<4, FULL>(it, near, accumulate, d_phi, fg, og, s);
+    }
+    static P2pItems item_range(const P2pItems& a, int64_t i0, int64_t i1) {
+        return P2pItems{a.leaf + i0, a.t0 + i0, i1 - i0, a.n ? a.n + i0 : nullptr};
+    }
+
+    // P2P of the leaves of levels [l0, l1); accumulate = 0 adds the far partial and writes
+    // the scaled output in caller order, 1 adds into the leaf-order store (level calls), 2
+    // writes the near field alone in leaf order into d_phi / d_grad.  The mixed form runs
+    // its two work lists (items of 32 targets, then the split remainders).
+    void p2p_levels(int l0, int l1, int near, int accumulate, double* d_phi, double* d_grad,
+                    cudaStream_t s = nullptr) {
         if (!s) s = stream;
-        P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
         double* fg = gradients ? far_g.as<double>() : nullptr;
         double* og = gradients ? d_grad : nullptr;
         if constexpr (kMixed) {
-            if (p2p_warps == 1)
-                p2p_x2_launch<1>(it, near, accumulate, d_phi, fg, og, s);
-            else if (p2p_warps == 2)
-                p2p_x2_launch<2>(it, near, accumulate, d_phi, fg, og, s);
-            else
-                p2p_x2_launch<4>(it, near, accumulate, d_phi, fg, og, s);
+            p2p_x2_shape<true>(item_range(pfull, pfull_lstart[l0], pfull_lstart[l1]), near, accumulate, d_phi, fg,
+                               og, s);
+            p2p_x2_shape<false>(item_range(ppart, ppart_lstart[l0], ppart_lstart[l1]), near, accumulate, d_phi, fg,
+                                og, s);
         } else {
+            const int64_t i0 = item_lstart[l0], i1 = item_lstart[l1];
+            if (i1 <= i0) return;
+            P2pItems it{items.leaf + i0, items.t0 + i0, i1 - i0};
             const unsigned g = (unsigned)((it.count + kP2pWarps - 1) / kP2pWarps);
             if (gradients)
                 p2p_kernel<T, true><<<counted(g), 32 * kP2pWarps, 0, s>>>(
@@ -1560,7 +1631,7 @@ struct Evaluator final : EvaluatorBase {
             case FMMGPU_OP_P2L: if (l >= 2) p2l_level(l); break;
             case FMMGPU_OP_L2P: leaf_far(f0, f1, 5); break;
             case FMMGPU_OP_M2P: leaf_far(f0, f1, 6); break;
-            case FMMGPU_OP_P2P: p2p_items(item_lstart[l], item_lstart[l + 1], 1, 1, nullptr, nullptr); break;
+            case FMMGPU_OP_P2P: p2p_levels(l, l + 1, 1, 1, nullptr, nullptr); break;
             default: throw Failure(FMMGPU_INVALID_ARGUMENT, "unknown operator kind");
         }
         CUDA_TRY(cudaGetLastError());

@@ -819,7 +819,15 @@ struct P2pItems {
     const int32_t* leaf;  // work item -> target leaf
     const int64_t* t0;    // work item -> first target (leaf order)
     int64_t count;
+    const int32_t* n = nullptr;  // work item -> its targets (1 to 32); null: up to 32, to the leaf's end
 };
+
+// the targets of a work item: its own count, else up to 32 from t0 to the leaf's end t1
+__device__ __forceinline__ int item_targets(const P2pItems& items, int64_t item, int64_t t1) {
+    if (items.n) return items.n[item];
+    const int64_t r = t1 - items.t0[item];
+    return (int)(r < 32 ? r : 32);
+}
 
 // L2P + M2P of the f32 form over P2P work items: a warp per item (up to 32 targets of one
 // leaf, lane = target), any number of warps a block.  Each target sums the terms of

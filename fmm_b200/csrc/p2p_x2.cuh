@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
     // an item of ni < 32 targets splits each flush's pair-steps over K = 32 / ni lanes per
     // target: lane = target + ni * kk takes the pair-steps i = kk (mod K); the K sums of a
     // target are added in kk order at the end
-    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int ni = item_targets(items, item, t1);
     const int K = 32 / ni;
     const int kk = lane < ni * K ? lane / ni : K;  // lanes past ni * K take no pair-steps
     const int ti = lane < ni * K ? lane % ni : 0;
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
-    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int ni = item_targets(items, item, t1);
     const int K = 32 / ni;
     const int kk = lane < ni * K ? lane / ni : K;
     const int ti = lane < ni * K ? lane % ni : 0;
@@ -612,12 +612,15 @@ constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
 // faster than two at the bench size (P2P 2.046 vs 2.042 ms): the flush latency is hidden.
 constexpr int kStBufs = 2;
 
-template <bool GRAD, int W>
+// V1: one charge vector (m = 1), the vector loop compiled out; FULL: items of 32 targets
+// only (one target a lane), the split pair loop compiled out.
+template <bool GRAD, int W, bool V1 = false, bool FULL = false>
 __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
-    DevPlan plan, P2pItems items, int m, int near, float rmax, P2pStream st, const float* __restrict__ sq,
+    DevPlan plan, P2pItems items, int m_, int near, float rmax, P2pStream st, const float* __restrict__ sq,
     const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, double* __restrict__ far_g,
     int accumulate, double* __restrict__ out_phi, double* __restrict__ out_g) {
     constexpr int NB = kStBufs;
+    const int m = V1 ? 1 : m_;
     __shared__ float4 sxy[W][NB][kStPairs];  // (x0, x1, y0, y1), NB flushes
     __shared__ float4 szq[W][NB][kStPairs];  // (z0, z1, q0, q1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -627,15 +630,15 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
     // the lanes of an item of ni < 32 targets split the pair-steps (p2p_x2_kernel)
-    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
-    const int K = 32 / ni;
-    const int kk = lane < ni * K ? lane / ni : K;
-    const int ti = lane < ni * K ? lane % ni : 0;
+    const int ni = FULL ? 32 : item_targets(items, item, t1);
+    const int K = FULL ? 1 : 32 / ni;
+    const int kk = FULL ? 0 : lane < ni * K ? lane / ni : K;
+    const int ti = FULL ? lane : lane < ni * K ? lane % ni : 0;
     const int64_t t = items.t0[item] + ti;
-    const bool valid = lane < ni;
+    const bool valid = FULL || lane < ni;
     const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (kk < K) {
+    if (FULL || kk < K) {
         const float4 p4 = tpos[t];
         tx = p4.x;
         ty = p4.y;
@@ -675,11 +678,15 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
             cp_async4_zf(zq + 4 * (lane + 32) + 3, qv + (ix1.y < 0 ? 0 : ix1.y), ix1.y < 0 ? 0 : 4);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
-        if (++ifl == nfl) {
-            ifl = 0;
-            ++iv;
+        if (V1) {
+            if (++ifl < nfl) load_idx();  // lands while the flush being computed runs
+        } else {
+            if (++ifl == nfl) {
+                ifl = 0;
+                ++iv;
+            }
+            if (iv < m) load_idx();
         }
-        if (iv < m) load_idx();  // lands while the flush being computed runs
     };
     load_idx();
     for (int f = 0; f < NB - 1; ++f) {  // the first NB - 1 flushes in flight (empty groups past the end)
@@ -719,7 +726,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
             }
         };
         if (K == 1) {  // the common item of one target a lane: a unit stride (11 % faster)
-#pragma unroll 8
+#pragma unroll 16
             for (int i = 0; i < npairs; ++i) step(i);
         } else {
 #pragma unroll 2
@@ -813,7 +820,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
-    const int ni = (int)((t1 - items.t0[item]) < 32 ? (t1 - items.t0[item]) : 32);
+    const int ni = item_targets(items, item, t1);
     const int K = 32 / ni;
     const int kk = lane < ni * K ? lane / ni : K;
     const int ti = lane < ni * K ? lane % ni : 0;
