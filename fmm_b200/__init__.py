@@ -45,7 +45,8 @@ class Info(C.Structure):
                 ("device_bytes", C.c_int64), ("close_pairs", C.c_int64), ("launches", C.c_int64),
                 ("vectors_per_pass", C.c_int64), ("p2p_warps", C.c_int64), ("leaf_block", C.c_int64),
                 ("product_chunks", C.c_int64), ("p2p_stream_bytes", C.c_int64), ("tables_loaded", C.c_int64),
-                ("tuning_loaded", C.c_int64)]
+                ("tuning_loaded", C.c_int64), ("m2l_tile_columns", C.c_int64),
+                ("vjp_forward_reused", C.c_int64)]
 
 
 def lib():
@@ -81,6 +82,8 @@ def lib():
             "fmmgpu_fmm_set_p2p_path": (C.c_int, [vp, C.c_int]),
             "fmmgpu_fmm_autotune": (C.c_int, [vp, dp, dp]),
             "fmmgpu_fmm_set_launch_shapes": (C.c_int, [vp, C.c_int, C.c_int]),
+            "fmmgpu_fmm_set_m2l_tile": (C.c_int, [vp, C.c_int]),
+            "fmmgpu_fmm_set_vjp_store": (C.c_int, [vp, C.c_int]),
             "fmmgpu_direct_sum": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_direct_sum_noalloc": (C.c_int, [sz, dp, dp, sz, dp, dp, dp, C.c_int, vp]),
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
@@ -538,6 +541,16 @@ class Fmm(Plan):
     def set_launch_shapes(self, p2p_warps, leaf_block):
         """Sets the shapes autotune chooses (e.g. a stored choice): 1, 2 or 4 and 32, 64 or 128."""
         _check(lib().fmmgpu_fmm_set_launch_shapes(self._h, int(p2p_warps), int(leaf_block)))
+
+    def set_vjp_store(self, on):
+        """Stores each evaluation's charges and target gradients so that a VJP with the same
+        charges skips its forward FMM (on), or recomputes it every time (off, the default)."""
+        _check(lib().fmmgpu_fmm_set_vjp_store(self._h, 1 if on else 0))
+
+    def set_m2l_tile(self, tile):
+        """The tensor-core M2L tile: 0 its default columns, 1 the tuner's alternative (the
+        same floats); info()["m2l_tile_columns"] names the columns in use."""
+        _check(lib().fmmgpu_fmm_set_m2l_tile(self._h, int(tile)))
 
     def set_kinds(self, kinds):
         """Test hook: bit 0 near field, bit 1 far field (3, the default, is the FMM)."""

@@ -80,6 +80,12 @@ struct fmmgpu_fmm {
     std::vector<double> src_pts, tgt_pts;
     fmmgpu_fmm* transpose = nullptr;
     DevBuf d_vjp_w, d_vjp_tq, d_vjp_dq, d_vjp_dxs, d_vjp_dxt;
+    // the stored forward pass (fmmgpu_fmm_set_vjp_store): the charges and target gradients
+    // of the last evaluation, which a VJP with the same charges uses instead of its own
+    // forward FMM; off, every VJP recomputes it
+    bool vjp_store = false, keep_valid = false;
+    DevBuf d_keep_q, d_keep_g, d_keep_flag;
+    int64_t vjp_forward_reused = 0;
     DevBuf d_hq, d_hphi, d_hg;  // the Helmholtz host call's device buffers
     int64_t tables_loaded = 0;  // tables taken from the table cache (bits: M2L, M2M, L2L)
     std::string table_cache_dir, tuning_cache_dir;  // the settings' cache directories ("" none)
@@ -89,6 +95,16 @@ struct fmmgpu_fmm {
 };
 
 namespace fmmb {
+
+// flag = 1 when a[0..n) and b[0..n) differ in any bit (flag starts at 0)
+__global__ void differ_kernel(int64_t n, const unsigned long long* __restrict__ a,
+                              const unsigned long long* __restrict__ b, int* __restrict__ flag) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (a[i] != b[i]) {
+            *flag = 1;
+            return;
+        }
+}
 
 // ---- vector-Jacobian products of phi(q, sources, targets) for a cotangent w on phi ----
 // dx_t[i] = sum_v w[v][i] grad phi_v(t_i)   (w, phi in the output layout [v][nt])
@@ -172,6 +188,15 @@ void run_evaluation(fmmgpu_fmm* f, const double* q, double* phi, double* grad) {
     }
     CUDA_TRY(cudaGraphLaunch(f->graph, f->stream));
     ev.launches = f->graph_launches;
+}
+
+// with the forward pass stored: keep this evaluation's charges and target gradients
+void keep_forward(fmmgpu_fmm* f, const double* q, const double* grad) {
+    if (!f->vjp_store || !grad) return;
+    const size_t m = f->settings.vectors, ns = f->plan.src_perm.size(), nt = f->plan.tgt_perm.size();
+    CUDA_TRY(cudaMemcpyAsync(f->d_keep_q.ptr, q, sizeof(double) * m * ns, cudaMemcpyDeviceToDevice, f->stream));
+    CUDA_TRY(cudaMemcpyAsync(f->d_keep_g.ptr, grad, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToDevice, f->stream));
+    f->keep_valid = true;
 }
 
 }  // namespace
@@ -448,9 +473,11 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
             if (tuning_cache_load(f->tuning_cache_dir, key, entries, &why) && entries.count(g + "p2p_warps") &&
                 entries.count(g + "leaf_block")) {
                 const int w = entries[g + "p2p_warps"], b = entries[g + "leaf_block"];
-                if ((w == 1 || w == 2 || w == 4) && (b == 32 || b == 64 || b == 128)) {
+                const int t = entries.count(g + "m2l_tile") ? entries[g + "m2l_tile"] : 0;
+                if ((w == 1 || w == 2 || w == 4) && (b == 32 || b == 64 || b == 128) && (t == 0 || t == 1)) {
                     f->eval->p2p_warps = w;
                     f->eval->leaf_block = b;
+                    f->eval->m2l_tile = t;
                     cached = true;
                 }
             }
@@ -465,6 +492,7 @@ void build_device(fmmgpu_fmm* f, const std::vector<double>& us, const std::vecto
             if (!f->tuning_cache_dir.empty()) {
                 entries[g + "p2p_warps"] = f->eval->p2p_warps;
                 entries[g + "leaf_block"] = f->eval->leaf_block;
+                entries[g + "m2l_tile"] = f->eval->m2l_tile;
                 std::string why;
                 tuning_cache_store(f->tuning_cache_dir, key, entries, &why);
             }
@@ -636,6 +664,7 @@ int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* f, const double* charges, double* pot
         if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
         CUDA_TRY(cudaSetDevice(f->settings.device));
         run_evaluation(f, charges, potential, f->settings.gradients ? gradient : nullptr);
+        keep_forward(f, charges, f->settings.gradients ? gradient : nullptr);
     });
 }
 
@@ -650,6 +679,7 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
         CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, f->stream));
         run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(),
                        f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        keep_forward(f, f->d_charges.as<double>(), f->settings.gradients ? f->d_grad.as<double>() : nullptr);
         CUDA_TRY(cudaMemcpyAsync(potential, f->d_phi.ptr, sizeof(double) * m * nt, cudaMemcpyDeviceToHost, f->stream));
         if (f->settings.gradients)
             CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
@@ -692,11 +722,31 @@ int fmmgpu_fmm_vjp(fmmgpu_fmm* f, const double* charges, const double* cotangent
         cudaStream_t s = f->stream;
         CUDA_TRY(cudaMemcpyAsync(f->d_charges.ptr, charges, sizeof(double) * m * ns, cudaMemcpyHostToDevice, s));
         CUDA_TRY(cudaMemcpyAsync(f->d_vjp_w.ptr, cotangent, sizeof(double) * m * nt, cudaMemcpyHostToDevice, s));
-        // forward pass (recomputed, nothing kept from earlier evaluations): grad phi at the targets
-        run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(), f->d_grad.as<double>());
+        // forward pass: grad phi at the targets, from the stored forward pass when its
+        // charges are these (bit for bit, checked on the device), else recomputed
+        bool reuse = false;
+        if (f->vjp_store && f->keep_valid) {
+            CUDA_TRY(cudaMemsetAsync(f->d_keep_flag.ptr, 0, sizeof(int), s));
+            const int64_t n = (int64_t)m * ns;
+            if (n)
+                differ_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(
+                    n, f->d_charges.as<unsigned long long>(), f->d_keep_q.as<unsigned long long>(),
+                    f->d_keep_flag.as<int>());
+            int differ = 1;
+            CUDA_TRY(cudaMemcpyAsync(&differ, f->d_keep_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaStreamSynchronize(s));
+            reuse = differ == 0;
+        }
+        if (reuse) {
+            ++f->vjp_forward_reused;
+        } else {
+            run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(), f->d_grad.as<double>());
+            keep_forward(f, f->d_charges.as<double>(), f->d_grad.as<double>());
+        }
+        const double* fwd_grad = reuse ? f->d_keep_g.as<double>() : f->d_grad.as<double>();
         const unsigned bt = (unsigned)((nt + 255) / 256), bs = (unsigned)((ns + 255) / 256);
         if (nt) {
-            vjp_target_kernel<<<bt, 256, 0, s>>>(nt, m, f->d_vjp_w.as<double>(), f->d_grad.as<double>(),
+            vjp_target_kernel<<<bt, 256, 0, s>>>(nt, m, f->d_vjp_w.as<double>(), fwd_grad,
                                                 f->d_vjp_dxt.as<double>());
             vjp_transpose_kernel<<<bt, 256, 0, s>>>(nt, m, f->d_vjp_w.as<double>(), f->d_vjp_tq.as<double>());
         }
@@ -974,6 +1024,47 @@ int fmmgpu_fmm_set_launch_shapes(fmmgpu_fmm* f, int p2p_warps, int leaf_block) {
     });
 }
 
+int fmmgpu_fmm_set_vjp_store(fmmgpu_fmm* f, int on) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        if (on != 0 && on != 1) throw Failure(FMMGPU_INVALID_ARGUMENT, "on must be 0 or 1");
+        if (on && !f->settings.gradients) throw Failure(FMMGPU_INVALID_ARGUMENT, "a VJP needs an FMM built with gradients");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->keep_valid = false;
+        if (!on) {
+            f->vjp_store = false;
+            f->d_keep_q.alloc(0);
+            f->d_keep_g.alloc(0);
+            f->d_keep_flag.alloc(0);
+            return;
+        }
+        const size_t m = f->settings.vectors, ns = f->plan.src_perm.size(), nt = f->plan.tgt_perm.size();
+        const size_t bytes = sizeof(double) * m * (ns + 1) + sizeof(double) * 3 * m * (nt + 1);
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        // memory asks for recomputation: the store may take at most half of what is free
+        if (bytes > free_b / 2) throw Failure(FMMGPU_DEVICE_MEMORY, "no room to store the forward pass");
+        f->d_keep_q.alloc(sizeof(double) * m * (ns + 1));
+        f->d_keep_g.alloc(sizeof(double) * 3 * m * (nt + 1));
+        f->d_keep_flag.alloc(sizeof(int));
+        f->vjp_store = true;
+    });
+}
+
+int fmmgpu_fmm_set_m2l_tile(fmmgpu_fmm* f, int tile) {
+    return guarded([&] {
+        if (!f || !f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
+        if (tile != 0 && tile != 1) throw Failure(FMMGPU_INVALID_ARGUMENT, "the M2L tile must be 0 or 1");
+        if (tile == 1 && !f->eval->m2l_tile_columns(1))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "this evaluator has no tensor-core M2L");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        CUDA_TRY(cudaStreamSynchronize(f->stream));
+        f->eval->m2l_tile = tile;
+        f->drop_graph();
+    });
+}
+
 int fmmgpu_fmm_kind_times(fmmgpu_fmm* f, double* ms) {
     return guarded([&] {
         if (!f || !f->eval || !ms) throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument or plan-only handle");
@@ -1015,6 +1106,8 @@ int fmmgpu_fmm_info(const fmmgpu_fmm* f, fmmgpu_info* info) {
         info->tuning_loaded = f->tuning_loaded;
         info->leaf_block = f->eval ? f->eval->leaf_block : 0;
         info->product_chunks = f->eval ? f->eval->product_chunks() : 0;
+        info->m2l_tile_columns = f->eval ? f->eval->m2l_tile_columns(f->eval->m2l_tile) : 0;
+        info->vjp_forward_reused = f->vjp_forward_reused;
     });
 }
 

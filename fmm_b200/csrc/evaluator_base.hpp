@@ -129,6 +129,9 @@ struct EvaluatorBase {
     // (1, 2 or 4) and threads a block of the L2P / M2P kernel (32, 64 or 128)
     int p2p_warps = 4;  // the static block, kX2Warps of p2p_x2.cuh (checked there)
     int leaf_block = 64;
+    // the tensor-core M2L tile: 0 the default columns, 1 the alternative (tc_alt_columns)
+    int m2l_tile = 0;
+    virtual int m2l_tile_columns(int tile) const = 0;
     // mixed P2P: 1 the sources from the near rows' streams mapped at build time (the
     // default when the streams fit), 0 mapped per flush; the same floats
     int p2p_path = 0;

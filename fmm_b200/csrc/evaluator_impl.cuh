@@ -95,6 +95,11 @@ struct Evaluator final : EvaluatorBase {
     DevBuf tc_ltile_d, tc_ltile_begin, tc_ltile_count;
     std::vector<int64_t> tc_lvl_tiles;
     int64_t tc_ntiles = 0;
+    // the same with the tuner's alternative tile (tc_alt_columns<P>() columns; m2l_tile 1)
+    static constexpr int kTcAlt = kTensor ? tc_alt_columns<(P <= 12 ? P : 12)>() : 0;
+    DevBuf tc2_tile_d, tc2_tile_begin, tc2_tile_count, tc2_ltile_d, tc2_ltile_begin, tc2_ltile_count;
+    std::vector<int64_t> tc2_lvl_tiles;
+    int64_t tc2_ntiles = 0;
     int num_sms = 148;
     // fused tensor-core M2L: per level, chunks of consecutive target boxes cut into tiles
     // of one offset (pairs in (chunk, offset, target) order), CTA c of level l taking the
@@ -333,6 +338,20 @@ struct Evaluator final : EvaluatorBase {
             tc_ltile_begin.upload(lvl.begin);
             tc_ltile_count.upload(lvl.count);
             tc_pair_src.upload(ps);
+            // the alternative tile's lists (the pair order is the same)
+            Tiles all2, lvl2;
+            std::vector<int64_t> pe2;
+            std::vector<int32_t> ps2;
+            batches(std::max(1, kTcAlt / m), all2, lvl2, tc2_lvl_tiles, pe2, ps2);
+            tc_halves(all2, nullptr);
+            tc_halves(lvl2, &tc2_lvl_tiles);
+            tc2_ntiles = (int64_t)all2.d.size();
+            tc2_tile_d.upload(all2.d);
+            tc2_tile_begin.upload(all2.begin);
+            tc2_tile_count.upload(all2.count);
+            tc2_ltile_d.upload(lvl2.d);
+            tc2_ltile_begin.upload(lvl2.begin);
+            tc2_ltile_count.upload(lvl2.count);
         }
         Y.alloc(sizeof(T) * (size_t)m * ys_of(P) * (plan.v.nnz() + 1));
         product_path_built = true;
@@ -540,6 +559,8 @@ struct Evaluator final : EvaluatorBase {
             CUDA_TRY(cudaMemset(tc_error.ptr, 0, sizeof(int)));
             CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           TcTs<P>::SMEM));
+            CUDA_TRY(cudaFuncSetAttribute(m2l_tc_kernel<P, false, kTcAlt>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, TcTs<P, false, kTcAlt>::SMEM));
             int dev = 0;
             CUDA_TRY(cudaGetDevice(&dev));
             CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1020,6 +1041,10 @@ struct Evaluator final : EvaluatorBase {
     // launches rewrite the same partials.  A last evaluation leaves the output and the
     // launch count as a plain evaluation does.
     int64_t product_chunks() const override { return (int64_t)chunks.size(); }
+    int m2l_tile_columns(int tile) const override {
+        if constexpr (kTensor) return tile ? kTcAlt : TcTs<P>::NT;
+        return 0;
+    }
 
     void set_m2l_path(int path) override {
         if (path < 0 || path > 2 || (path >= 1 && !kTensor) || (path == 2 && !kFusedOk))
@@ -1071,6 +1096,18 @@ struct Evaluator final : EvaluatorBase {
                 if (b == 32 || ms < best) best = ms, pick = b;
             }
             leaf_block = pick;
+        }
+        // the tensor-core M2L tile (the products are the same floats for either: every
+        // column is its own MMA column with the same K order)
+        if (kTensor && m2l_path == 1 && chunks.empty() && tc_ntiles && (kinds & 2)) {
+            float best = 0.f;
+            int pick = m2l_tile;
+            for (int t : {0, 1}) {
+                m2l_tile = t;
+                const float ms = time([&] { m2l_products(-1); });
+                if (t == 0 || ms < best) best = ms, pick = t;
+            }
+            m2l_tile = pick;
         }
         CUDA_TRY(cudaEventDestroy(e0));
         CUDA_TRY(cudaEventDestroy(e1));
@@ -1192,16 +1229,26 @@ struct Evaluator final : EvaluatorBase {
     void m2l_products(int l) {
         if (kTensor && m2l_path == 1) {
             if constexpr (kTensor) {
-                const int64_t t0 = l < 0 ? 0 : tc_lvl_tiles[l];
-                const int64_t nt = l < 0 ? tc_ntiles : tc_lvl_tiles[l + 1] - tc_lvl_tiles[l];
-                const DevBuf& td = l < 0 ? tc_tile_d : tc_ltile_d;
-                const DevBuf& tb = l < 0 ? tc_tile_begin : tc_ltile_begin;
-                const DevBuf& tn = l < 0 ? tc_tile_count : tc_ltile_count;
+                const bool alt = m2l_tile == 1;
+                const std::vector<int64_t>& ls = alt ? tc2_lvl_tiles : tc_lvl_tiles;
+                const int64_t t0 = l < 0 ? 0 : ls[l];
+                const int64_t nt = l < 0 ? (alt ? tc2_ntiles : tc_ntiles) : ls[l + 1] - ls[l];
+                const DevBuf& td = l < 0 ? (alt ? tc2_tile_d : tc_tile_d) : (alt ? tc2_ltile_d : tc_ltile_d);
+                const DevBuf& tb = l < 0 ? (alt ? tc2_tile_begin : tc_tile_begin) : (alt ? tc2_ltile_begin : tc_ltile_begin);
+                const DevBuf& tn = l < 0 ? (alt ? tc2_tile_count : tc_tile_count) : (alt ? tc2_ltile_count : tc_ltile_count);
                 if (nt == 0) return;
                 const unsigned grid = (unsigned)std::min<int64_t>(nt, num_sms);
-                m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
-                    td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt, tc_pair_src.as<int32_t>(), nullptr,
-                    m, tc_bimg.as<uint32_t>(), mmap, vmap, reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+                if (alt)
+                    m2l_tc_kernel<P, false, kTcAlt><<<counted(grid), 32 * kTcWarps, TcTs<P, false, kTcAlt>::SMEM,
+                                                      stream>>>(
+                        td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
+                        tc_pair_src.as<int32_t>(), nullptr, m, tc_bimg.as<uint32_t>(), mmap, vmap,
+                        reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
+                else
+                    m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
+                        td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
+                        tc_pair_src.as<int32_t>(), nullptr, m, tc_bimg.as<uint32_t>(), mmap, vmap,
+                        reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
             return;
         }

@@ -166,7 +166,8 @@ constexpr long long kTcWait = 4000000000LL;  // clock cycles (about 2 s)
 // rows [A_r; A_i] as two halves of 128 output slots (the n = (p+1)^2 rows of each padded):
 // the products of a column are A_r x in slots 0..n and A_i x in slots 128..128+n of a
 // 256-slot row, which the complex local reduce combines into the local's two planes.
-template <int P, bool CPLX = false>
+// NTA: the columns of a tile when nonzero (the tuner's alternative), else the default below
+template <int P, bool CPLX = false, int NTA = 0>
 struct TcTs {
     static constexpr int NC = nc_of(P);
     static constexpr int KA = (NC + 31) / 32;
@@ -181,7 +182,7 @@ struct TcTs {
     // (KP = 128), the most beside two X stages and two raw stages; 48 at p = 11, 12
     // (KP = 160, 192: tensor memory then holds the table's 2 KP columns and two 48-column
     // accumulators, shared memory two X stages and two or three raw stages)
-    static constexpr int NT = KP > 128 ? 48 : KP > 96 ? 64 : KP > 64 ? 96 : 128;
+    static constexpr int NT = NTA ? NTA : KP > 128 ? 48 : KP > 96 ? 64 : KP > 64 ? 96 : 128;
     static constexpr int X_BYTES = NT * KP * 4;    // one part of one stage (also one raw stage)
     // raw stages: as many as shared memory holds beside the two X stages, at most 4 (the
     // copy engine's loads take several tiles' time to land)
@@ -253,7 +254,7 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-template <int P, bool CPLX = false>
+template <int P, bool CPLX = false, int NTA = 0>
 __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t* __restrict__ tile_d,
                                                                   const int64_t* __restrict__ tile_begin,
                                                                   const int32_t* __restrict__ tile_count,
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   const __grid_constant__ CUtensorMap mmap,
                                                                   const __grid_constant__ CUtensorMap vmap,
                                                                   float* __restrict__ Y, int* __restrict__ error) {
-    using S = TcTs<P, CPLX>;
+    using S = TcTs<P, CPLX, NTA>;
     constexpr int NT = S::NT, KP = S::KP, YS = S::YS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* xbuf = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // [2 stages][hi, lo]
@@ -555,6 +556,13 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
         asm volatile("tcgen05.fence::after_thread_sync;");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS));
     }
+}
+
+// the autotuner's alternative tile of the real M2L: 64 columns where the default has 96 or
+// 128, 32 where it has 64 or 48 (more raw stages in the shared memory freed)
+template <int P>
+constexpr int tc_alt_columns() {
+    return TcTs<P>::NT >= 96 ? 64 : 32;
 }
 
 // columns (pairs x vectors) of a tensor-core M2L tile at degree p (0 to 12)

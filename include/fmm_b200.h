@@ -95,6 +95,8 @@ typedef struct {
     int64_t p2p_stream_bytes; /* the mixed P2P's near-row source streams (0: mapped per flush) */
     int64_t tables_loaded;    /* tables the build took from the table cache: bit 0 M2L, 1 M2M, 2 L2L */
     int64_t tuning_loaded;    /* 1: the launch shapes came from the tuning cache */
+    int64_t m2l_tile_columns; /* columns of a tensor-core M2L tile (the tuned one; 0: no tensor-core M2L) */
+    int64_t vjp_forward_reused; /* VJPs that took the stored forward pass (fmmgpu_fmm_set_vjp_store) */
 } fmmgpu_info;
 
 typedef struct fmmgpu_fmm fmmgpu_fmm;
@@ -232,8 +234,9 @@ int fmmgpu_fmm_set_overlap(fmmgpu_fmm* fmm, int on);
 
 /* Times the launch shapes that change no result on this handle's plan and device and
  * keeps the fastest (the reference's build-time tuner, fmm-exec/src/tune.rs:1-60, with
- * the P2P layout decision as the block of the mixed P2P kernel, 1, 2 or 4 warps, and the
- * L2P / M2P block, 32, 64 or 128 threads).  `charges` as fmmgpu_fmm_evaluate's (host);
+ * the P2P layout decision as the block of the mixed P2P kernel, 1, 2 or 4 warps, the
+ * L2P / M2P block, 32, 64 or 128 threads, and the tensor-core M2L tile, its default or
+ * its alternative column count: fmmgpu_fmm_set_m2l_tile, info.m2l_tile_columns).  `charges` as fmmgpu_fmm_evaluate's (host);
  * the handle's device outputs then hold their evaluation.  choice (may be NULL) receives
  * {p2p warps, leaf block}.  Every target sums the same terms in the same order whatever
  * the shape, so later evaluations give the same bits as before.  Drops a captured graph.
@@ -245,6 +248,23 @@ int fmmgpu_fmm_autotune(fmmgpu_fmm* fmm, const double* charges, int* choice);
  * p2p_warps 1, 2 or 4; leaf_block 32, 64 or 128.  The results are the same bits for
  * every pair.  Drops a captured graph.  Synchronises. */
 int fmmgpu_fmm_set_launch_shapes(fmmgpu_fmm* fmm, int p2p_warps, int leaf_block);
+
+/* The VJP's forward pass, stored or recomputed.  on = 1: every following evaluation with
+ * gradients (host or device call, and a VJP's own forward pass) keeps a device copy of its
+ * charges and target gradients (8 m (N_s + 3 N_t) bytes), and a VJP whose charges equal the
+ * kept ones bit for bit (checked on the device) takes the kept gradients instead of running
+ * the forward FMM (the same floats: the same evaluation).  on = 0 (the default, and what
+ * memory asks for): every VJP recomputes its forward pass; the store is freed.  Refused with
+ * FMMGPU_DEVICE_MEMORY when the store would take more than half the free device memory.
+ * info.vjp_forward_reused counts the VJPs that used it.  Synchronises. */
+int fmmgpu_fmm_set_vjp_store(fmmgpu_fmm* fmm, int on);
+
+/* The tensor-core M2L tile of the following evaluations (mixed precision): 0 its default
+ * columns (128 at p <= 6, 96 at p = 7, 8, 64 at p = 9, 10, 48 at p = 11, 12), 1 the
+ * alternative (64 where the default has 96 or 128, else 32; more raw stages in flight).
+ * Every product is the same float either way.  The autotuner picks one; a tuning cache
+ * keeps it.  Drops a captured graph.  Synchronises. */
+int fmmgpu_fmm_set_m2l_tile(fmmgpu_fmm* fmm, int tile);
 
 /* Per-kind device timing of the following evaluations (the reference's KindTiming,
  * fmm-exec/src/fmm.rs:150-153): every launch is bracketed by CUDA events. */

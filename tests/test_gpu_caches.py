@@ -22,10 +22,12 @@ def test_tuning_cache_keeps_the_choice(tmp_path):
     assert len(files) == 1 and files[0].startswith("tuning-cuda-") and files[0].endswith("-mixed-p06.txt")
     text = open(os.path.join(d, files[0])).read()
     assert f"gradients:p2p_warps {ia['p2p_warps']}" in text and f"gradients:leaf_block {ia['leaf_block']}" in text
+    assert f"gradients:m2l_tile {0 if ia['m2l_tile_columns'] == 128 else 1}" in text
     b = F.FmmBuilder(6).gradients().max_points_per_leaf(64).precision("mixed").autotune().tuning_cache(d).build(x)
     ib = b.info()
     assert ib["tuning_loaded"] == 1
-    assert (ib["p2p_warps"], ib["leaf_block"]) == (ia["p2p_warps"], ia["leaf_block"])
+    assert (ib["p2p_warps"], ib["leaf_block"], ib["m2l_tile_columns"]) == (
+        ia["p2p_warps"], ia["leaf_block"], ia["m2l_tile_columns"])
     oa, ob = a.evaluate(q), b.evaluate(q)
     assert np.array_equal(oa.potential, ob.potential) and np.array_equal(oa.gradient, ob.gradient)
     # a corrupted file is rejected and the shapes timed again (and stored again)

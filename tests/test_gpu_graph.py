@@ -76,6 +76,20 @@ def test_launch_shapes_change_speed_only(oracle, precision):
             assert np.array_equal(got.gradient, want.gradient), (w, b)
     with pytest.raises(F.FmmError):
         fmm.set_launch_shapes(3, 64)
+    # the tensor-core M2L tile (mixed): the alternative column count gives the same bits
+    if precision == "mixed":
+        assert fmm.info()["m2l_tile_columns"] == 128
+        fmm.set_m2l_tile(1)
+        assert fmm.info()["m2l_tile_columns"] == 64
+        got = fmm.evaluate(q)
+        assert np.array_equal(got.potential, want.potential) and np.array_equal(got.gradient, want.gradient)
+        fmm.set_m2l_tile(0)
+    else:
+        assert fmm.info()["m2l_tile_columns"] == 0
+        with pytest.raises(F.FmmError):
+            fmm.set_m2l_tile(1)
+    with pytest.raises(F.FmmError):
+        fmm.set_m2l_tile(2)
     choice = fmm.autotune(q)
     assert choice["p2p_warps"] in (1, 2, 4) and choice["leaf_block"] in (32, 64, 128)
     assert (fmm.info()["p2p_warps"], fmm.info()["leaf_block"]) == (choice["p2p_warps"], choice["leaf_block"])

@@ -81,3 +81,40 @@ def test_vjp_with_distinct_sources_and_targets(oracle):
     # a second call reuses the transpose FMM built by the first
     dq2, _, _ = fmm.vjp(q, w[None, :])
     assert np.array_equal(dq, dq2)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_stored_forward_pass_gives_the_same_vjp(precision, symmetric):
+    """With the forward pass stored, a VJP whose charges are those of the last evaluation
+    takes the kept target gradients instead of its own forward FMM: the same bits as
+    recomputing it; other charges are recomputed (and then kept)."""
+    x = clusters(12000, 6, 7)
+    y = x if symmetric else clusters(9000, 5, 8)
+    rng = np.random.default_rng(9)
+    q, q2 = rng.normal(size=len(x)), rng.normal(size=len(x))
+    w = rng.normal(size=(1, len(y)))
+    build = lambda: F.FmmBuilder(6).gradients().max_points_per_leaf(64).precision(precision).build(
+        x, None if symmetric else y)
+    ref, st = build(), build()
+    want = ref.vjp(q, w)
+    want2 = ref.vjp(q2, w)
+    st.set_vjp_store(True)
+    st.evaluate(q)
+    got = st.vjp(q, w)
+    assert st.info()["vjp_forward_reused"] == 1
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
+    got2 = st.vjp(q2, w)  # other charges: recomputed
+    assert st.info()["vjp_forward_reused"] == 1
+    for a, b in zip(got2, want2):
+        assert np.array_equal(a, b)
+    got3 = st.vjp(q2, w)  # the VJP's own forward pass was kept
+    assert st.info()["vjp_forward_reused"] == 2
+    for a, b in zip(got3, want2):
+        assert np.array_equal(a, b)
+    st.set_vjp_store(False)
+    st.vjp(q2, w)
+    assert st.info()["vjp_forward_reused"] == 2
+    ref.close()
+    st.close()
