@@ -140,13 +140,15 @@ struct Evaluator final : EvaluatorBase {
     P2pItems items{};
     std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
     std::vector<int32_t> item_leaf_h;  // the items' leaves (host copy, ascending)
-    // The mixed P2P's own work lists: every item of 32 targets (one target a lane, the
-    // FULL kernel), then the remainders of the leaves cut into items of 16 and 8 targets
-    // and a last one below 8 (K = 32 / n lanes a target split its pair-steps, so no lane
-    // idles but in the last item); each list in leaf order, with explicit target counts.
+    // The mixed P2P's own work lists, by item size: every item of 32 targets (one target a
+    // lane), then the remainders of the leaves cut into items of 16 and of 8 targets and a
+    // last one below 8 (K = 32 / n lanes a target split its pair-steps, so no lane idles but
+    // in the last item); each list in leaf order, with explicit target counts; the first
+    // three run kernels with K fixed at compile time.
+    static constexpr int kP2pClasses = 4;
     DevBuf pitem_leaf, pitem_t0, pitem_n;
-    P2pItems pfull{}, ppart{};
-    std::vector<int64_t> pfull_lstart, ppart_lstart;  // first item of each level (nlevels + 1)
+    P2pItems plist[kP2pClasses]{};
+    std::vector<int64_t> plist_lstart[kP2pClasses];  // first item of each level (nlevels + 1)
     ClosePairs close{};
     int64_t nclose = 0;
     static constexpr bool kMixed = sizeof(T) == 4;
@@ -835,43 +837,40 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void build_p2p_lists() {
-        std::vector<int32_t> fl, pl, fn, pn;
-        std::vector<int64_t> ft, pt;
+        std::vector<int32_t> lv[kP2pClasses], nv[kP2pClasses];
+        std::vector<int64_t> tv[kP2pClasses];
+        auto add = [&](int c, size_t j, int64_t t, int n) {
+            lv[c].push_back((int32_t)j);
+            tv[c].push_back(t);
+            nv[c].push_back(n);
+        };
         for (size_t j = 0; j < plan.nleaves(); ++j) {
             int64_t t = plan.tgt_start[j];
             const int64_t t1 = plan.tgt_start[j + 1];
-            for (; t + 32 <= t1; t += 32) {
-                fl.push_back((int32_t)j);
-                ft.push_back(t);
-                fn.push_back(32);
-            }
-            for (int sz : {16, 8, 0}) {
-                const int64_t r = t1 - t;
-                if (r <= 0) break;
-                const int n = sz ? (r >= sz ? sz : 0) : (int)r;
-                if (!n) continue;
-                pl.push_back((int32_t)j);
-                pt.push_back(t);
-                pn.push_back(n);
-                t += n;
-            }
+            for (; t + 32 <= t1; t += 32) add(0, j, t, 32);
+            if (t + 16 <= t1) add(1, j, t, 16), t += 16;
+            if (t + 8 <= t1) add(2, j, t, 8), t += 8;
+            if (t < t1) add(3, j, t, (int)(t1 - t));
         }
-        const int64_t nf = (int64_t)fl.size(), np = (int64_t)pl.size();
-        auto starts = [&](const std::vector<int32_t>& lv, std::vector<int64_t>& out) {
-            out.assign(plan.nlevels + 1, (int64_t)lv.size());
+        std::vector<int32_t> al, an;
+        std::vector<int64_t> at;
+        int64_t base[kP2pClasses];
+        for (int c = 0; c < kP2pClasses; ++c) {
+            plist_lstart[c].assign(plan.nlevels + 1, (int64_t)lv[c].size());
             for (int l = plan.nlevels - 1; l >= 0; --l)
-                out[l] = std::lower_bound(lv.begin(), lv.end(), (int32_t)plan.leaf_level_start[l]) - lv.begin();
-        };
-        starts(fl, pfull_lstart);
-        starts(pl, ppart_lstart);
-        fl.insert(fl.end(), pl.begin(), pl.end());
-        ft.insert(ft.end(), pt.begin(), pt.end());
-        fn.insert(fn.end(), pn.begin(), pn.end());
-        pitem_leaf.upload(fl);
-        pitem_t0.upload(ft);
-        pitem_n.upload(fn);
-        pfull = P2pItems{pitem_leaf.as<int32_t>(), pitem_t0.as<int64_t>(), nf, pitem_n.as<int32_t>()};
-        ppart = P2pItems{pitem_leaf.as<int32_t>() + nf, pitem_t0.as<int64_t>() + nf, np, pitem_n.as<int32_t>() + nf};
+                plist_lstart[c][l] =
+                    std::lower_bound(lv[c].begin(), lv[c].end(), (int32_t)plan.leaf_level_start[l]) - lv[c].begin();
+            base[c] = (int64_t)al.size();
+            al.insert(al.end(), lv[c].begin(), lv[c].end());
+            at.insert(at.end(), tv[c].begin(), tv[c].end());
+            an.insert(an.end(), nv[c].begin(), nv[c].end());
+        }
+        pitem_leaf.upload(al);
+        pitem_t0.upload(at);
+        pitem_n.upload(an);
+        for (int c = 0; c < kP2pClasses; ++c)
+            plist[c] = P2pItems{pitem_leaf.as<int32_t>() + base[c], pitem_t0.as<int64_t>() + base[c],
+                                (int64_t)lv[c].size(), pitem_n.as<int32_t>() + base[c]};
     }
 
     // The mixed form's f64 pairs: found on the device with the f32 arithmetic of the P2P
@@ -1326,7 +1325,7 @@ struct Evaluator final : EvaluatorBase {
                 dp, r0, mode, m, tpos.as<T4>(), M.as<T>(), Lc.as<T>(), far_phi.as<double>(), far_g.as<double>());
     }
 
-    template <int W, bool FULL>
+    template <int W, int KS>
     void p2p_x2_launch(const P2pItems& it, int near, int accumulate, double* d_phi, double* fg, double* og,
                        cudaStream_t s) {
         const unsigned g = (unsigned)((it.count + W - 1) / W);
@@ -1340,14 +1339,14 @@ struct Evaluator final : EvaluatorBase {
                                                                  far_phi.as<double>(), accumulate, d_phi);
                 return;
             }
-            if constexpr (FULL) {
-                if (m == 1) {  // the common case: one vector, one target a lane
-                    p2p_st_kernel<true, W, true, true><<<counted(g), 32 * W, 0, s>>>(
+            if constexpr (KS != 0) {
+                if (m == 1) {  // the common case: one vector
+                    p2p_st_kernel<true, W, true, KS><<<counted(g), 32 * W, 0, s>>>(
                         dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og);
                     return;
                 }
             }
-            p2p_st_kernel<true, W, false, FULL><<<counted(g), 32 * W, 0, s>>>(
+            p2p_st_kernel<true, W, false, KS><<<counted(g), 32 * W, 0, s>>>(
                 dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og);
             return;
         }
@@ -1366,16 +1365,16 @@ struct Evaluator final : EvaluatorBase {
                                                                 accumulate, d_phi, og);
     }
 
-    template <bool FULL>
+    template <int KS>
     void p2p_x2_shape(const P2pItems& it, int near, int accumulate, double* d_phi, double* fg, double* og,
                       cudaStream_t s) {
         if (!it.count) return;
         if (p2p_warps == 1)
-            p2p_x2_launch<1, FULL>(it, near, accumulate, d_phi, fg, og, s);
+            p2p_x2_launch<1, KS>(it, near, accumulate, d_phi, fg, og, s);
         else if (p2p_warps == 2)
-            p2p_x2_launch<2, FULL>(it, near, accumulate, d_phi, fg, og, s);
+            p2p_x2_launch<2, KS>(it, near, accumulate, d_phi, fg, og, s);
         else
-            p2p_x2_launch<4, FULL>(it, near, accumulate, d_phi, fg, og, s);
+            p2p_x2_launch<4, KS>(it, near, accumulate, d_phi, fg, og, s);
     }
     static P2pItems item_range(const P2pItems& a, int64_t i0, int64_t i1) {
         return P2pItems{a.leaf + i0, a.t0 + i0, i1 - i0, a.n ? a.n + i0 : nullptr};
@@ -1391,10 +1390,11 @@ struct Evaluator final : EvaluatorBase {
         double* fg = gradients ? far_g.as<double>() : nullptr;
         double* og = gradients ? d_grad : nullptr;
         if constexpr (kMixed) {
-            p2p_x2_shape<true>(item_range(pfull, pfull_lstart[l0], pfull_lstart[l1]), near, accumulate, d_phi, fg,
-                               og, s);
-            p2p_x2_shape<false>(item_range(ppart, ppart_lstart[l0], ppart_lstart[l1]), near, accumulate, d_phi, fg,
-                                og, s);
+            auto range = [&](int c) { return item_range(plist[c], plist_lstart[c][l0], plist_lstart[c][l1]); };
+            p2p_x2_shape<1>(range(0), near, accumulate, d_phi, fg, og, s);
+            p2p_x2_shape<2>(range(1), near, accumulate, d_phi, fg, og, s);
+            p2p_x2_shape<4>(range(2), near, accumulate, d_phi, fg, og, s);
+            p2p_x2_shape<0>(range(3), near, accumulate, d_phi, fg, og, s);
         } else {
             const int64_t i0 = item_lstart[l0], i1 = item_lstart[l1];
             if (i1 <= i0) return;

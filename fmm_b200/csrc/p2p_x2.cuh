@@ -612,9 +612,10 @@ constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
 // faster than two at the bench size (P2P 2.046 vs 2.042 ms): the flush latency is hidden.
 constexpr int kStBufs = 2;
 
-// V1: one charge vector (m = 1), the vector loop compiled out; FULL: items of 32 targets
-// only (one target a lane), the split pair loop compiled out.
-template <bool GRAD, int W, bool V1 = false, bool FULL = false>
+// V1: one charge vector (m = 1), the vector loop compiled out.  KS: the lanes a target
+// splits its pair-steps over when fixed at compile time (items of 32 / KS targets only:
+// 1 one target a lane, 2 or 4 a strided loop of constant stride), 0 any item.
+template <bool GRAD, int W, bool V1 = false, int KS = 0>
 __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
     DevPlan plan, P2pItems items, int m_, int near, float rmax, P2pStream st, const float* __restrict__ sq,
     const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, double* __restrict__ far_g,
@@ -630,15 +631,16 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
     // the lanes of an item of ni < 32 targets split the pair-steps (p2p_x2_kernel)
-    const int ni = FULL ? 32 : item_targets(items, item, t1);
-    const int K = FULL ? 1 : 32 / ni;
-    const int kk = FULL ? 0 : lane < ni * K ? lane / ni : K;
-    const int ti = FULL ? lane : lane < ni * K ? lane % ni : 0;
+    constexpr int NIS = KS ? 32 / KS : 0;  // targets of an item when KS fixes them
+    const int ni = KS ? NIS : item_targets(items, item, t1);
+    const int K = KS ? KS : 32 / ni;
+    const int kk = KS ? lane / NIS : lane < ni * K ? lane / ni : K;
+    const int ti = KS ? lane % NIS : lane < ni * K ? lane % ni : 0;
     const int64_t t = items.t0[item] + ti;
-    const bool valid = FULL || lane < ni;
+    const bool valid = lane < ni;
     const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (FULL || kk < K) {
+    if (KS || kk < K) {
         const float4 p4 = tpos[t];
         tx = p4.x;
         ty = p4.y;
@@ -728,6 +730,9 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         if (K == 1) {  // the common item of one target a lane: a unit stride (11 % faster)
 #pragma unroll 16
             for (int i = 0; i < npairs; ++i) step(i);
+        } else if (KS) {  // a constant stride
+#pragma unroll 8
+            for (int i = kk; i < npairs; i += KS) step(i);
         } else {
 #pragma unroll 2
             for (int i = kk; i < npairs; i += K) step(i);
