@@ -394,7 +394,14 @@ __global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int
                 s = y;
         }
         int64_t e = e0;
-        for (; e + 8 <= e1; e += 8) {  // eight rows in flight, added in row order
+        for (; e + 16 <= e1; e += 16) {  // sixteen rows in flight, added in row order
+            float4 y[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) add4(s, y[j]);
+        }
+        for (; e + 8 <= e1; e += 8) {
             float4 y[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);

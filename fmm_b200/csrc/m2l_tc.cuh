@@ -148,7 +148,7 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 //     and commits to empty[k&1] and acc_full[k&1];
 //   warps 0-7 (epilogue): wait acc_full[k&1], read the accumulator with tcgen05.ld
 //     and stream the products past L2 into Y at the pairs' positions in the tile list
-//     (a tile's rows consecutive, each padded to ys_of(P) slots: whole 128-byte lines),
+//     (a tile's rows consecutive, each ys_of(P) slots: (p+1)^2 rounded up to 4),
 //     then release acc_empty[k&1].
 // Every wait is bounded; a role that gives up sets the shared abort flag (which ends
 // the other roles' waits) and *error, and the CTA frees its tensor memory and returns.
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (128 * h + 32 * q < YS) {
                 // products at rows p0 * m + c (a tile's rows are consecutive), or, with
-                // pair_row, at rows pair_row[pair] * m + vector; whole 128-byte lines (rows
+                // pair_row, at rows pair_row[pair] * m + vector; the slots below YS (rows
                 // >= NC of the table are zero), 16 columns per TMEM load
 #pragma unroll 1
                 for (int c0 = 16 * g; c0 < NT; c0 += 32) {
@@ -535,13 +535,13 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
 #pragma unroll
                         for (int i = 0; i < 16; ++i) {
                             const int64_t row = __shfl_sync(0xffffffffu, myrow, i);
-                            if (c0 + i < ncol) __stcs(Y + row * YS + n, v0[i]);
+                            if (c0 + i < ncol && n < YS) __stcs(Y + row * YS + n, v0[i]);
                         }
                     } else {
                         float* yb = Y + (p0 * m + c0) * YS + n;
 #pragma unroll
                         for (int i = 0; i < 16; ++i)
-                            if (c0 + i < ncol) __stcs(yb + (int64_t)i * YS, v0[i]);
+                            if (c0 + i < ncol && n < YS) __stcs(yb + (int64_t)i * YS, v0[i]);
                     }
                 }
             }
