@@ -65,20 +65,6 @@ struct Evaluator final : EvaluatorBase {
     // target) products, tiles of kGemmPairs; Yo holds one product row per child box
     DevBuf oct_tile_d, oct_tile_begin, oct_tile_count, oct_pair_e, oct_pair_src, Yo;
     std::vector<int64_t> m2m_tiles, l2l_tiles;  // tile ranges per level (nlevels + 1)
-    // the octant runs of the M2M (0) and L2L (1) pairs: per level and octant, `count`
-    // consecutive pairs of oct_pair_e / oct_pair_src from `begin`
-    struct OctGroup {
-        int level, octant;
-        int64_t begin, count;
-    };
-    std::vector<OctGroup> oct_groups[2];
-    // the mixed form's M2M / L2L products on the tensor-core kernel: tiles of NT / m pairs
-    // of one octant (table index octant + 8 pass, doubled for two slot halves), per pass
-    // and level tile ranges, the tables' images, and maps over the locals for the L2L
-    // gathers (the multipole maps serve M2M)
-    DevBuf oct_tc_d, oct_tc_begin, oct_tc_count, oct_img;
-    std::vector<int64_t> oct_tc_lstart[2];
-    CUtensorMap lmap{}, lvmap{};
     // M2L batches: pairs of all levels grouped by offset, in tiles
     DevBuf tile_d, tile_begin, tile_count, pair_e, pair_src, v_pos;
     int64_t ntiles = 0;
@@ -247,10 +233,7 @@ struct Evaluator final : EvaluatorBase {
         far_g.alloc(sizeof(double) * 3 * (size_t)m * (dp.ntgt + 1));
         CUDA_TRY(cudaMemset(M.ptr, 0, M.bytes));
         build_parent_lists();
-        if (kTensor) {
-            build_tensor_m2l(m2l);
-            build_tensor_octants(m2m, l2l);
-        }
+        if (kTensor) build_tensor_m2l(m2l);
         if (kFusedOk && fused && m <= fused_tile_columns(P)) {
             build_fused_m2l();
             m2l_path = 2;
@@ -433,7 +416,7 @@ struct Evaluator final : EvaluatorBase {
                 const unsigned grid = (unsigned)std::min<int64_t>(c.tc_nt, num_sms);
                 m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
                     ck_tc_d.as<int32_t>() + c.tc_t0, ck_tc_begin.as<int64_t>() + c.tc_t0,
-                    ck_tc_count.as<int32_t>() + c.tc_t0, c.tc_nt, ck_pair_src.as<int32_t>() + c.base, nullptr, m,
+                    ck_tc_count.as<int32_t>() + c.tc_t0, c.tc_nt, ck_pair_src.as<int32_t>() + c.base, m,
                     tc_bimg.as<uint32_t>(), mmap, vmap, reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
             return;
@@ -569,56 +552,6 @@ struct Evaluator final : EvaluatorBase {
         }
     }
 
-    void build_tensor_octants(const std::vector<double>& m2m, const std::vector<double>& l2l) {
-        if constexpr (kTensor) {
-            std::vector<double> both(m2m);
-            both.insert(both.end(), l2l.begin(), l2l.end());
-            std::vector<uint32_t> img;
-            build_tc_table_images<P>(both, img, 16);
-            oct_img.upload(img);
-            encode_multipole_map<P>(&lmap, reinterpret_cast<const float*>(Lc.ptr), (int64_t)plan.nboxes() * m);
-            encode_multipole_map<P>(&lvmap, reinterpret_cast<const float*>(Lc.ptr), (int64_t)plan.nboxes() * m, m);
-            const int ppt = std::max(1, TcTs<P>::NT / m);
-            Tiles all;
-            for (int pass = 0; pass < 2; ++pass) {
-                Tiles t;
-                std::vector<int64_t> ls(plan.nlevels + 1, 0);
-                size_t g = 0;
-                for (int l = 0; l < plan.nlevels; ++l) {
-                    ls[l] = (int64_t)t.d.size();
-                    for (; g < oct_groups[pass].size() && oct_groups[pass][g].level == l; ++g)
-                        t.add(oct_groups[pass][g].octant + 8 * pass, oct_groups[pass][g].begin,
-                              oct_groups[pass][g].count, ppt);
-                }
-                ls[plan.nlevels] = (int64_t)t.d.size();
-                tc_halves(t, &ls);
-                const int64_t base = (int64_t)all.d.size();
-                for (auto& x : ls) x += base;
-                oct_tc_lstart[pass] = ls;
-                all.d.insert(all.d.end(), t.d.begin(), t.d.end());
-                all.begin.insert(all.begin.end(), t.begin.begin(), t.begin.end());
-                all.count.insert(all.count.end(), t.count.begin(), t.count.end());
-            }
-            oct_tc_d.upload(all.d);
-            oct_tc_begin.upload(all.begin);
-            oct_tc_count.upload(all.count);
-        }
-    }
-
-    // M2M (pass 0) or L2L (pass 1) products of level l on the tensor-core kernel, into Yo
-    // at the children's rows
-    void octant_tc(int pass, int l) {
-        if constexpr (kTensor) {
-            const int64_t t0 = oct_tc_lstart[pass][l], nt = oct_tc_lstart[pass][l + 1] - t0;
-            if (nt <= 0) return;
-            const unsigned grid = (unsigned)std::min<int64_t>(nt, num_sms);
-            m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
-                oct_tc_d.as<int32_t>() + t0, oct_tc_begin.as<int64_t>() + t0, oct_tc_count.as<int32_t>() + t0, nt,
-                oct_pair_src.as<int32_t>(), oct_pair_e.as<int64_t>(), m, oct_img.as<uint32_t>(),
-                pass ? lmap : mmap, pass ? lvmap : vmap, reinterpret_cast<float*>(Yo.ptr), tc_error.as<int>());
-        }
-    }
-
     // Tile lists over the V pairs grouped by offset index, then by target box (pair
     // positions pe/ps shared by both lists):
     //  - the evaluation's list: tiles of up to `tile` pairs of one offset, all levels;
@@ -720,8 +653,6 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void build_parent_lists() {
-        oct_groups[0].clear();
-        oct_groups[1].clear();
         std::vector<int32_t> a;
         m2m_start.assign(plan.nlevels + 1, 0);
         for (int l = 0; l < plan.nlevels; ++l) {
@@ -750,8 +681,7 @@ struct Evaluator final : EvaluatorBase {
                     if (pass == 0 ? plan.src_below[c] == 0 : plan.tgt_below[c] == 0) continue;
                     by[octant(c)].push_back(c);
                 }
-                for (int o = 0; o < 8; ++o) {
-                    if (!by[o].empty()) oct_groups[pass].push_back({l, o, (int64_t)pe.size(), (int64_t)by[o].size()});
+                for (int o = 0; o < 8; ++o)
                     for (size_t s0 = 0; s0 < by[o].size(); s0 += kGemmPairs) {
                         td.push_back(o);
                         tb.push_back((int64_t)pe.size());
@@ -763,7 +693,6 @@ struct Evaluator final : EvaluatorBase {
                             ps.push_back(pass == 0 ? (int32_t)c : plan.parent[c]);
                         }
                     }
-                }
             }
             ranges[plan.nlevels] = (int64_t)td.size();
         }
@@ -965,8 +894,7 @@ struct Evaluator final : EvaluatorBase {
                                &leaf_box, &src_start, &tgt_start, &tgt_perm, &src_perm, &near_row,
                                &near_col, &w_row, &w_col, &x_row, &x_col, &v_row, &v_col, &v_off,
                                &m2l_tab, &m2m_tab, &l2l_tab, &spos, &tpos, &sq, &M, &Lc, &far_phi, &far_g,
-                               &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e, &oct_tc_d,
-                               &oct_tc_begin, &oct_tc_count, &oct_img, &pitem_leaf, &pitem_t0, &pitem_n,
+                               &Y, &m2m_par, &oct_tile_d, &oct_tile_begin, &oct_tile_count, &oct_pair_e, &pitem_leaf, &pitem_t0, &pitem_n,
                                &oct_pair_src, &Yo, &tile_d, &tile_begin, &tile_count, &pair_e, &pair_src, &item_leaf, &item_t0,
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
@@ -1200,9 +1128,7 @@ struct Evaluator final : EvaluatorBase {
     void m2m_level(int l) {  // parents on level l from their children on level l + 1
         const int64_t t0 = m2m_tiles[l], nt = m2m_tiles[l + 1] - m2m_tiles[l];
         const int64_t n = m2m_start[l + 1] - m2m_start[l];
-        if (kTensor)
-            octant_tc(0, l);
-        else if (nt)
+        if (nt)
             m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
                 oct_tile_d.as<int32_t>() + t0, oct_tile_begin.as<int64_t>() + t0, oct_tile_count.as<int32_t>() + t0,
                 oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m, m2m_tab.as<T>(), M.as<T>(), Yo.as<T>());
@@ -1241,12 +1167,12 @@ struct Evaluator final : EvaluatorBase {
                     m2l_tc_kernel<P, false, kTcAlt><<<counted(grid), 32 * kTcWarps, TcTs<P, false, kTcAlt>::SMEM,
                                                       stream>>>(
                         td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
-                        tc_pair_src.as<int32_t>(), nullptr, m, tc_bimg.as<uint32_t>(), mmap, vmap,
+                        tc_pair_src.as<int32_t>(), m, tc_bimg.as<uint32_t>(), mmap, vmap,
                         reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
                 else
                     m2l_tc_kernel<P><<<counted(grid), 32 * kTcWarps, TcTs<P>::SMEM, stream>>>(
                         td.as<int32_t>() + t0, tb.as<int64_t>() + t0, tn.as<int32_t>() + t0, nt,
-                        tc_pair_src.as<int32_t>(), nullptr, m, tc_bimg.as<uint32_t>(), mmap, vmap,
+                        tc_pair_src.as<int32_t>(), m, tc_bimg.as<uint32_t>(), mmap, vmap,
                         reinterpret_cast<float*>(Y.ptr), tc_error.as<int>());
             }
             return;
@@ -1263,10 +1189,6 @@ struct Evaluator final : EvaluatorBase {
     }
 
     void l2l_products(int l) {  // L2L products Yo of the children on level l (l >= 3)
-        if (kTensor) {
-            octant_tc(1, l);
-            return;
-        }
         const int64_t t0 = l2l_tiles[l], nt = l2l_tiles[l + 1] - l2l_tiles[l];
         if (nt)
             m2l_gemm_kernel<P, T><<<counted((unsigned)nt), 256, gemm_smem, stream>>>(
@@ -1628,7 +1550,7 @@ struct Evaluator final : EvaluatorBase {
                 const unsigned grid = (unsigned)std::min<int64_t>(hh.tc_ntiles, num_sms);
                 m2l_tc_kernel<P, true><<<counted(grid), 32 * kTcWarps, TcTs<P, true>::SMEM, stream>>>(
                     hh.tc_d.as<int32_t>(), hh.tc_begin.as<int64_t>(), hh.tc_count.as<int32_t>(), hh.tc_ntiles,
-                    pair_src.as<int32_t>(), nullptr, 2 * m, hh.tc_img.as<uint32_t>(), hh.mmap, hh.vmap,
+                    pair_src.as<int32_t>(), 2 * m, hh.tc_img.as<uint32_t>(), hh.mmap, hh.vmap,
                     reinterpret_cast<float*>(hh.Y.ptr), tc_error.as<int>());
             }
         } else {

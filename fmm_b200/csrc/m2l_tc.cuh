@@ -259,8 +259,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
                                                                   const int64_t* __restrict__ tile_begin,
                                                                   const int32_t* __restrict__ tile_count,
                                                                   int64_t ntiles,
-                                                                  const int32_t* __restrict__ pair_src,
-                                                                  const int64_t* __restrict__ pair_row, int m,
+                                                                  const int32_t* __restrict__ pair_src, int m,
                                                                   const uint32_t* __restrict__ timg,
                                                                   const __grid_constant__ CUtensorMap mmap,
                                                                   const __grid_constant__ CUtensorMap vmap,
@@ -518,31 +517,17 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (128 * h + 32 * q < YS) {
-                // products at rows p0 * m + c (a tile's rows are consecutive), or, with
-                // pair_row, at rows pair_row[pair] * m + vector; the slots below YS (rows
-                // >= NC of the table are zero), 16 columns per TMEM load
+                // products at rows p0 * m + c (a tile's rows are consecutive), the slots
+                // below YS (rows >= NC of the table are zero), 16 columns per TMEM load
 #pragma unroll 1
                 for (int c0 = 16 * g; c0 < NT; c0 += 32) {
                     if (c0 >= ncol) break;
                     float v0[16];
                     tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(S::COL_D0 + st * NT + c0), v0);
-                    if (pair_row) {
-                        int64_t myrow = 0;  // lane i < 16: the row of column c0 + i
-                        if (lane < 16 && c0 + lane < ncol) {
-                            const int c = c0 + lane;
-                            myrow = pair_row[p0 + c / m] * m + c % m;
-                        }
+                    float* yb = Y + (p0 * m + c0) * YS + n;
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const int64_t row = __shfl_sync(0xffffffffu, myrow, i);
-                            if (c0 + i < ncol && n < YS) __stcs(Y + row * YS + n, v0[i]);
-                        }
-                    } else {
-                        float* yb = Y + (p0 * m + c0) * YS + n;
-#pragma unroll
-                        for (int i = 0; i < 16; ++i)
-                            if (c0 + i < ncol && n < YS) __stcs(yb + (int64_t)i * YS, v0[i]);
-                    }
+                    for (int i = 0; i < 16; ++i)
+                        if (c0 + i < ncol && n < YS) __stcs(yb + (int64_t)i * YS, v0[i]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
