@@ -209,10 +209,12 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
     int box, nent;
     int64_t ent0;
     if (!IRREG) {
+        // a leaf without sources keeps its zero multipole; the test reads the leaf's source
+        // range, which needs no load of its box first (the box is read beside it)
         box = plan.leaf_box[row];
         nent = 1;
         ent0 = 0;
-        if (plan.src_below[box] == 0) return;
+        if (plan.src_start[row + 1] == plan.src_start[row]) return;
     } else {
         box = (int)row;
         ent0 = plan.x_row[row];
@@ -232,9 +234,21 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
         if (IRREG) rel_frame<float>(plan, box, plan.leaf_box[sleaf], fc, fr);  // (c(t|s), r(t|s))
         const float finv = 1.0f / fr;
         const int64_t s1 = plan.src_start[sleaf + 1];
-        for (int64_t si = plan.src_start[sleaf] + lane; si < s1; si += 32) {
-            const float4 p4 = spos[si];
-            const float q = qv[si];
+        // the lane's next source is loaded before its current one is summed
+        int64_t si = plan.src_start[sleaf] + lane;
+        float4 pn = make_float4(0.f, 0.f, 0.f, 0.f);
+        float qn = 0.f;
+        if (si < s1) {
+            pn = spos[si];
+            qn = qv[si];
+        }
+        for (; si < s1; si += 32) {
+            const float4 p4 = pn;
+            const float q = qn;
+            if (si + 32 < s1) {
+                pn = spos[si + 32];
+                qn = qv[si + 32];
+            }
             const float x = (p4.x - fc[0]) * finv, y = (p4.y - fc[1]) * finv, z = (p4.z - fc[2]) * finv;
             if (!IRREG) {
                 RegularRows<P, float> h;
