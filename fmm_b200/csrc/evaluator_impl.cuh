@@ -126,11 +126,11 @@ struct Evaluator final : EvaluatorBase {
     P2pItems items{};
     std::vector<int64_t> item_lstart;  // first work item of each level's leaves (nlevels + 1)
     std::vector<int32_t> item_leaf_h;  // the items' leaves (host copy, ascending)
-    // The mixed P2P's own work lists, by item size: every item of 32 targets (one target a
+    // The mixed P2P's own work lists, by item slots: every item of 32 targets (one target a
     // lane), then the remainders of the leaves cut into items of 16 and of 8 targets and a
-    // last one below 8 (K = 32 / n lanes a target split its pair-steps, so no lane idles but
-    // in the last item); each list in leaf order, with explicit target counts; the first
-    // three run kernels with K fixed at compile time.
+    // last one of up to 8 in 8 slots or up to 4 in 4 slots (K = 32 / slots lanes a target
+    // split its pair-steps, so lanes idle only in the last item); each list in leaf order,
+    // with explicit targets and slots, on a kernel with K fixed at compile time.
     static constexpr int kP2pClasses = 4;
     DevBuf pitem_leaf, pitem_t0, pitem_n;
     P2pItems plist[kP2pClasses]{};
@@ -776,10 +776,12 @@ struct Evaluator final : EvaluatorBase {
         for (size_t j = 0; j < plan.nleaves(); ++j) {
             int64_t t = plan.tgt_start[j];
             const int64_t t1 = plan.tgt_start[j + 1];
-            for (; t + 32 <= t1; t += 32) add(0, j, t, 32);
-            if (t + 16 <= t1) add(1, j, t, 16), t += 16;
-            if (t + 8 <= t1) add(2, j, t, 8), t += 8;
-            if (t < t1) add(3, j, t, (int)(t1 - t));
+            for (; t + 32 <= t1; t += 32) add(0, j, t, 32 | 32 << 8);
+            if (t + 16 <= t1) add(1, j, t, 16 | 16 << 8), t += 16;
+            if (t + 8 <= t1) add(2, j, t, 8 | 8 << 8), t += 8;
+            const int r = (int)(t1 - t);  // 0 to 7 left
+            if (r > 4) add(2, j, t, r | 8 << 8);
+            else if (r > 0) add(3, j, t, r | 4 << 8);
         }
         std::vector<int32_t> al, an;
         std::vector<int64_t> at;
@@ -1316,7 +1318,7 @@ struct Evaluator final : EvaluatorBase {
             p2p_x2_shape<1>(range(0), near, accumulate, d_phi, fg, og, s);
             p2p_x2_shape<2>(range(1), near, accumulate, d_phi, fg, og, s);
             p2p_x2_shape<4>(range(2), near, accumulate, d_phi, fg, og, s);
-            p2p_x2_shape<0>(range(3), near, accumulate, d_phi, fg, og, s);
+            p2p_x2_shape<8>(range(3), near, accumulate, d_phi, fg, og, s);
         } else {
             const int64_t i0 = item_lstart[l0], i1 = item_lstart[l1];
             if (i1 <= i0) return;

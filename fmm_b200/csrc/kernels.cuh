@@ -840,14 +840,23 @@ struct P2pItems {
     const int32_t* leaf;  // work item -> target leaf
     const int64_t* t0;    // work item -> first target (leaf order)
     int64_t count;
-    const int32_t* n = nullptr;  // work item -> its targets (1 to 32); null: up to 32, to the leaf's end
+    // work item -> its targets (1 to 32) | its lane slots << 8 (a power of two >= the
+    // targets, 0: the targets); null: up to 32 targets, to the leaf's end, in as many slots
+    const int32_t* n = nullptr;
 };
 
-// the targets of a work item: its own count, else up to 32 from t0 to the leaf's end t1
-__device__ __forceinline__ int item_targets(const P2pItems& items, int64_t item, int64_t t1) {
-    if (items.n) return items.n[item];
+// The targets ni of a work item and its slots ns: the lanes are ns targets x K = 32 / ns
+// pair-step splits (lane = kk ns + ti), so an item padded to ns > ni slots splits its
+// pairs as an item of ns targets would, and lanes with ti >= ni hold no target.
+__device__ __forceinline__ void item_shape(const P2pItems& items, int64_t item, int64_t t1, int& ni, int& ns) {
+    if (items.n) {
+        const int v = items.n[item];
+        ni = v & 255;
+        ns = (v >> 8) ? (v >> 8) : ni;
+        return;
+    }
     const int64_t r = t1 - items.t0[item];
-    return (int)(r < 32 ? r : 32);
+    ni = ns = (int)(r < 32 ? r : 32);
 }
 
 // L2P + M2P of the f32 form over P2P work items: a warp per item (up to 32 targets of one

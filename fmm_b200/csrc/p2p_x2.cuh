@@ -210,13 +210,14 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
-    // an item of ni < 32 targets splits each flush's pair-steps over K = 32 / ni lanes per
-    // target: lane = target + ni * kk takes the pair-steps i = kk (mod K); the K sums of a
-    // target are added in kk order at the end
-    const int ni = item_targets(items, item, t1);
-    const int K = 32 / ni;
-    const int kk = lane < ni * K ? lane / ni : K;  // lanes past ni * K take no pair-steps
-    const int ti = lane < ni * K ? lane % ni : 0;
+    // an item of ni targets in ns >= ni slots splits each flush's pair-steps over K = 32 / ns
+    // lanes per target: lane = slot + ns * kk takes the pair-steps i = kk (mod K); the K
+    // sums of a target are added in kk order at the end (slots past ni hold no target)
+    int ni, ns;
+    item_shape(items, item, t1, ni, ns);
+    const int K = 32 / ns;
+    const int kk = lane < ns * K && lane % ns < ni ? lane / ns : K;  // lanes without a target take no pair-steps
+    const int ti = lane < ns * K ? lane % ns : 0;
     const int64_t t = items.t0[item] + ti;
     const bool valid = lane < ni;  // the lanes that finish their target (kk = 0)
     const int64_t n0 = plan.near_row[leaf], n1 = near ? plan.near_row[leaf + 1] : n0;
@@ -334,10 +335,10 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_x2_kernel(
             __syncwarp();
             if (valid)
                 for (int j = 1; j < K; ++j) {
-                    aphi += red[0][ti + ni * j];
-                    ag0 += red[1][ti + ni * j];
-                    ag1 += red[2][ti + ni * j];
-                    ag2 += red[3][ti + ni * j];
+                    aphi += red[0][ti + ns * j];
+                    ag0 += red[1][ti + ns * j];
+                    ag1 += red[2][ti + ns * j];
+                    ag2 += red[3][ti + ns * j];
                 }
             __syncwarp();
         }
@@ -407,10 +408,11 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
-    const int ni = item_targets(items, item, t1);
-    const int K = 32 / ni;
-    const int kk = lane < ni * K ? lane / ni : K;
-    const int ti = lane < ni * K ? lane % ni : 0;
+    int ni, ns;
+    item_shape(items, item, t1, ni, ns);
+    const int K = 32 / ns;
+    const int kk = lane < ns * K && lane % ns < ni ? lane / ns : K;
+    const int ti = lane < ns * K ? lane % ns : 0;
     const int64_t t = items.t0[item] + ti;
     const bool valid = lane < ni;
     const int64_t n0 = plan.near_row[leaf], n1 = near ? plan.near_row[leaf + 1] : n0;
@@ -525,7 +527,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_x2_mv_kernel(
             if (valid)
                 for (int j = 1; j < K; ++j)
 #pragma unroll
-                    for (int b = 0; b < VB; ++b) aphi[b] += red[b][ti + ni * j];
+                    for (int b = 0; b < VB; ++b) aphi[b] += red[b][ti + ns * j];
             __syncwarp();
         }
         if (valid) {
@@ -631,16 +633,19 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
     // the lanes of an item of ni < 32 targets split the pair-steps (p2p_x2_kernel)
-    constexpr int NIS = KS ? 32 / KS : 0;  // targets of an item when KS fixes them
-    const int ni = KS ? NIS : item_targets(items, item, t1);
-    const int K = KS ? KS : 32 / ni;
-    const int kk = KS ? lane / NIS : lane < ni * K ? lane / ni : K;
-    const int ti = KS ? lane % NIS : lane < ni * K ? lane % ni : 0;
+    constexpr int NIS = KS ? 32 / KS : 0;  // slots of an item when KS fixes them
+    int ni, ns;
+    item_shape(items, item, t1, ni, ns);
+    if (KS) ns = NIS;
+    const int K = KS ? KS : 32 / ns;
+    const int kk = KS ? lane / NIS : lane < ns * K ? lane / ns : K;
+    const int ti = KS ? lane % NIS : lane < ns * K ? lane % ns : 0;
     const int64_t t = items.t0[item] + ti;
     const bool valid = lane < ni;
+    const bool has_target = kk < K && ti < ni;  // lanes of padding slots hold no target
     const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (KS || kk < K) {
+    if (has_target) {
         const float4 p4 = tpos[t];
         tx = p4.x;
         ty = p4.y;
@@ -765,10 +770,10 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
             __syncwarp();
             if (valid)
                 for (int j = 1; j < K; ++j) {
-                    aphi += red[0][ti + ni * j];
-                    ag0 += red[1][ti + ni * j];
-                    ag1 += red[2][ti + ni * j];
-                    ag2 += red[3][ti + ni * j];
+                    aphi += red[0][ti + ns * j];
+                    ag0 += red[1][ti + ns * j];
+                    ag1 += red[2][ti + ns * j];
+                    ag2 += red[3][ti + ns * j];
                 }
             __syncwarp();
         }
@@ -825,10 +830,11 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
-    const int ni = item_targets(items, item, t1);
-    const int K = 32 / ni;
-    const int kk = lane < ni * K ? lane / ni : K;
-    const int ti = lane < ni * K ? lane % ni : 0;
+    int ni, ns;
+    item_shape(items, item, t1, ni, ns);
+    const int K = 32 / ns;
+    const int kk = lane < ns * K && lane % ns < ni ? lane / ns : K;
+    const int ti = lane < ns * K ? lane % ns : 0;
     const int64_t t = items.t0[item] + ti;
     const bool valid = lane < ni;
     const int64_t nt = plan.ntgt, nsrc = plan.nsrc;
@@ -940,7 +946,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W) p2p_st_mv_kernel(
             if (valid)
                 for (int j = 1; j < K; ++j)
 #pragma unroll
-                    for (int vb = 0; vb < VB; ++vb) aphi[vb] += red[vb][ti + ni * j];
+                    for (int vb = 0; vb < VB; ++vb) aphi[vb] += red[vb][ti + ns * j];
             __syncwarp();
         }
         if (valid) {
