@@ -19,7 +19,7 @@ OBJ = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libfmm_b200.so")
 
 SOURCES = ["evaluator.cu", "direct.cu", "tree.cpp", "tables.cpp", "forest.cpp", "helmholtz_tables.cpp",
-           "table_cache.cpp", "plan_upload.cpp", "plan_gpu.cu"]
+           "table_cache.cpp", "plan_upload.cpp", "plan_gpu.cu", "p2p_launch.cu"]
 ORDER_SOURCE = "evaluator_order.cu"
 HEADERS = ["plan.hpp", "evaluator_base.hpp", "evaluator_impl.cuh", "kernels.cuh", "harmonics.cuh", "m2l_tc.cuh",
            "m2l_fused.cuh", "p2p_x2.cuh", "helmholtz.cuh", "helmholtz_far.cuh", "morton.hpp"]

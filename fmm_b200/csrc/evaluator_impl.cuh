@@ -1263,15 +1263,8 @@ struct Evaluator final : EvaluatorBase {
                                                                  far_phi.as<double>(), accumulate, d_phi);
                 return;
             }
-            if constexpr (KS != 0) {
-                if (m == 1) {  // the common case: one vector
-                    p2p_st_kernel<true, W, true, KS><<<counted(g), 32 * W, 0, s>>>(
-                        dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og);
-                    return;
-                }
-            }
-            p2p_st_kernel<true, W, false, KS><<<counted(g), 32 * W, 0, s>>>(
-                dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og);
+            const P2pStArgs a{dp, it, m, near, kRmax, st, q, tp, close, far_phi.as<double>(), fg, accumulate, d_phi, og};
+            launch_p2p_st(a, W, KS, counted(g), s);
             return;
         }
         if (!gradients) {  // potentials: the pair geometry shared by up to kX2Vb vectors (any m)

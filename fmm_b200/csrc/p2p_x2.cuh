@@ -614,21 +614,42 @@ constexpr int kStPairs = kX2Stage / 2;  // pairs a flush (64)
 // faster than two at the bench size (P2P 2.046 vs 2.042 ms): the flush latency is hidden.
 constexpr int kStBufs = 2;
 
+// The arguments of the streamed P2P launches.
+struct P2pStArgs {
+    DevPlan plan;
+    P2pItems items;
+    int m, near;
+    float rmax;
+    P2pStream st;
+    const float* sq;
+    const float4* tpos;
+    ClosePairs close;
+    double *far_phi, *far_g;
+    int accumulate;
+    double *out_phi, *out_g;
+};
+
+// One work item of the streamed P2P, by one warp, with its NB flush buffers sxy / szq.
 // V1: one charge vector (m = 1), the vector loop compiled out.  KS: the lanes a target
-// splits its pair-steps over when fixed at compile time (items of 32 / KS targets only:
-// 1 one target a lane, 2 or 4 a strided loop of constant stride), 0 any item.
-template <bool GRAD, int W, bool V1 = false, int KS = 0>
-__global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
-    DevPlan plan, P2pItems items, int m_, int near, float rmax, P2pStream st, const float* __restrict__ sq,
-    const float4* __restrict__ tpos, ClosePairs close, double* __restrict__ far_phi, double* __restrict__ far_g,
-    int accumulate, double* __restrict__ out_phi, double* __restrict__ out_g) {
+// splits its pair-steps over when fixed at compile time (items of 32 / KS slots: 1 one
+// target a lane, 2, 4 or 8 a strided loop of constant stride), 0 any item.
+template <bool GRAD, bool V1, int KS>
+__device__ __forceinline__ void p2p_st_item(const P2pStArgs& a, int64_t item, float4 (*sxy)[kStPairs],
+                                            float4 (*szq)[kStPairs], int lane) {
     constexpr int NB = kStBufs;
-    const int m = V1 ? 1 : m_;
-    __shared__ float4 sxy[W][NB][kStPairs];  // (x0, x1, y0, y1), NB flushes
-    __shared__ float4 szq[W][NB][kStPairs];  // (z0, z1, q0, q1)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t item = (int64_t)blockIdx.x * W + warp;
-    if (item >= items.count) return;
+    const DevPlan& plan = a.plan;
+    const P2pItems& items = a.items;
+    const P2pStream& st = a.st;
+    const ClosePairs& close = a.close;
+    const float* __restrict__ sq = a.sq;
+    const float4* __restrict__ tpos = a.tpos;
+    double* __restrict__ far_phi = a.far_phi;
+    double* __restrict__ far_g = a.far_g;
+    double* __restrict__ out_phi = a.out_phi;
+    double* __restrict__ out_g = a.out_g;
+    const int near = a.near, accumulate = a.accumulate;
+    const float rmax = a.rmax;
+    const int m = V1 ? 1 : a.m;
     const int leaf = items.leaf[item];
     const int box = plan.leaf_box[leaf];
     const int64_t t1 = plan.tgt_start[leaf + 1];
@@ -671,15 +692,15 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         const float* qv = sq + (int64_t)iv * nsrc;
         const int64_t base = pb + (int64_t)ifl * kStPairs;
         const int npf = np_row - ifl * kStPairs;
-        float* zq = reinterpret_cast<float*>(&szq[warp][b][0]);
+        float* zq = reinterpret_cast<float*>(&szq[b][0]);
         if (lane < npf) {
-            cp_async16_cg(&sxy[warp][b][lane], st.xy + base + lane);
+            cp_async16_cg(&sxy[b][lane], st.xy + base + lane);
             cp_async8(zq + 4 * lane, st.zz + base + lane);
             cp_async4_zf(zq + 4 * lane + 2, qv + (ix0.x < 0 ? 0 : ix0.x), ix0.x < 0 ? 0 : 4);
             cp_async4_zf(zq + 4 * lane + 3, qv + (ix0.y < 0 ? 0 : ix0.y), ix0.y < 0 ? 0 : 4);
         }
         if (lane + 32 < npf) {
-            cp_async16_cg(&sxy[warp][b][lane + 32], st.xy + base + lane + 32);
+            cp_async16_cg(&sxy[b][lane + 32], st.xy + base + lane + 32);
             cp_async8(zq + 4 * (lane + 32), st.zz + base + lane + 32);
             cp_async4_zf(zq + 4 * (lane + 32) + 2, qv + (ix1.x < 0 ? 0 : ix1.x), ix1.x < 0 ? 0 : 4);
             cp_async4_zf(zq + 4 * (lane + 32) + 3, qv + (ix1.y < 0 ? 0 : ix1.y), ix1.y < 0 ? 0 : 4);
@@ -714,8 +735,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         const int npairs = rem < kStPairs ? rem : kStPairs;
         float2 pphi = f2(0.f, 0.f), pg0 = f2(0.f, 0.f), pg1 = f2(0.f, 0.f), pg2 = f2(0.f, 0.f);
         auto step = [&](int i) {
-            const float4 a = sxy[warp][b][i];
-            const float4 c = szq[warp][b][i];
+            const float4 a = sxy[b][i];
+            const float4 c = szq[b][i];
             const float2 dx = __fadd2_rn(f2(a.x, a.y), ntx);
             const float2 dy = __fadd2_rn(f2(a.z, a.w), nty);
             const float2 dz = __fadd2_rn(f2(c.x, c.y), ntz);
@@ -762,7 +783,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         if (!last) continue;
         // ---- the last flush of vector v: finish its targets ----
         if (K > 1) {  // the target's K partial sums, in kk order, through buffer b
-            double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[warp][b][0]);
+            double(*red)[32] = reinterpret_cast<double(*)[32]>(&sxy[b][0]);
             red[0][lane] = aphi;
             red[1][lane] = ag0;
             red[2][lane] = ag1;
@@ -811,6 +832,24 @@ __global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(
         aphi = ag0 = ag1 = ag2 = 0.0;
     }
 }
+
+// The streamed P2P over a work list of items of 32 / KS slots: W warps a block, a warp an
+// item.  (One kernel for every split, each item's taken from its slots, measured slower:
+// sphere 4e6 2.32 against 1.94 ms.)
+template <bool GRAD, int W, bool V1, int KS>
+__global__ void __launch_bounds__(32 * W, 32 / W) p2p_st_kernel(P2pStArgs a) {
+    __shared__ float4 sxy[W][kStBufs][kStPairs];  // (x0, x1, y0, y1), NB flushes
+    __shared__ float4 szq[W][kStBufs][kStPairs];  // (z0, z1, q0, q1)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * W + warp;
+    if (item >= a.items.count) return;
+    p2p_st_item<GRAD, V1, KS>(a, item, sxy[warp], szq[warp], lane);
+}
+
+// Host: the streamed P2P with gradients over a work list on stream s (p2p_launch.cu, its
+// own translation unit: these kernels depend on no expansion order): W = warps a block
+// (1, 2 or 4), ks the split of every item (1, 2, 4 or 8; 0 any item).
+void launch_p2p_st(const P2pStArgs& a, int warps, int ks, unsigned grid, cudaStream_t s);
 
 // Potentials of several vectors from the stream: p2p_x2_mv_kernel's pair-steps (the pair
 // geometry once, q rinv added per vector) on flushes copied from the stream.
