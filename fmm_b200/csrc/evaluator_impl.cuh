@@ -433,11 +433,18 @@ struct Evaluator final : EvaluatorBase {
     // block per box (the same order of additions either way)
     void reduce_range(int64_t b0, int64_t b1, int with_l2l, int with_v, int accumulate) {
         if (b1 <= b0) return;
-        if constexpr (kMixed)
-            local_reduce4_kernel<P><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
-                dp, b0, b1, m, with_l2l, with_v, accumulate, reinterpret_cast<const float*>(Yo.ptr),
-                reinterpret_cast<const float*>(Y.ptr), v_pos.as<int64_t>(), reinterpret_cast<float*>(Lc.ptr));
-        else
+        if constexpr (kMixed) {
+            const unsigned g = counted((unsigned)((b1 - b0 + 3) / 4));
+            const auto* yo = reinterpret_cast<const float*>(Yo.ptr);
+            const auto* yv = reinterpret_cast<const float*>(Y.ptr);
+            auto* lc = reinterpret_cast<float*>(Lc.ptr);
+            if (m == 1)
+                local_reduce4_kernel<P, true><<<g, 128, 0, stream>>>(dp, b0, b1, m, with_l2l, with_v, accumulate, yo,
+                                                                     yv, v_pos.as<int64_t>(), lc);
+            else
+                local_reduce4_kernel<P, false><<<g, 128, 0, stream>>>(dp, b0, b1, m, with_l2l, with_v, accumulate,
+                                                                      yo, yv, v_pos.as<int64_t>(), lc);
+        } else
             local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
                 dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
                 Lc.as<T>());
@@ -1576,7 +1583,7 @@ struct Evaluator final : EvaluatorBase {
                         reinterpret_cast<const float*>(hh.Y.ptr), v_pos.as<int64_t>(),
                         reinterpret_cast<float*>(hh.L.ptr));
                 else if constexpr (kMixed)
-                    local_reduce4_kernel<P><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
+                    local_reduce4_kernel<P, false><<<counted((unsigned)((b1 - b0 + 3) / 4)), 128, 0, stream>>>(
                         dp, b0, b1, mv, l >= 3, 1, 0, reinterpret_cast<const float*>(hh.Yo.ptr),
                         reinterpret_cast<const float*>(hh.Y.ptr), v_pos.as<int64_t>(),
                         reinterpret_cast<float*>(hh.L.ptr));

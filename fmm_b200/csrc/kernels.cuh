@@ -372,12 +372,14 @@ __global__ void local_reduce_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
         }
 }
 
-// The same reduce for f32 expansions with 16-byte accesses: a warp per box (4 a block),
-// lane q holding coefficients 4q .. 4q + 3; every coefficient adds the same terms in the
-// same order as local_reduce_kernel, so the floats are that kernel's.  Rows are 16-byte
-// aligned (ys_of and ms_of are multiples of 4 floats); the last quad's padding is read,
-// never written.  Four blocks an SM in the launch bound leave room for the eight 16-byte
-// rows in flight (96 registers; the compiler's own choice, 32-34, spilled or held fewer).
+// The same reduce for f32 expansions with 16-byte accesses: a warp per box (4 a block).
+// A box's m rows (its m vectors) are m NQ consecutive quads in the locals, in Yo and in
+// each of its V entries' products (ys_of = ms_of = 4 NQ), so the lanes take quads f, f + 32,
+// ... of that run: every lane busy for any m (m = 16 at p = 6: 208 quads, 7 passes), 13 of
+// 32 when the lanes held one vector's quads.  Every coefficient adds the same terms in the
+// same order as local_reduce_kernel, so the floats are that kernel's.  The last quad of a
+// row is read with its padding, which is never written.  Four blocks an SM in the launch
+// bound leave room for sixteen 16-byte rows in flight.
 __device__ __forceinline__ void add4(float4& s, const float4 y) {
     s.x += y.x;
     s.y += y.y;
@@ -385,51 +387,53 @@ __device__ __forceinline__ void add4(float4& s, const float4 y) {
     s.w += y.w;
 }
 
-template <int P>
-__global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int64_t b0, int64_t b1, int m,
+template <int P, bool ONE>  // ONE: m = 1 at compile time
+__global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int64_t b0, int64_t b1, int m_,
                                                             int with_l2l, int with_v, int accumulate,
                                                             const float* __restrict__ Yo, const float* __restrict__ Yv,
                                                             const int64_t* __restrict__ vpos, float* __restrict__ Lc) {
     constexpr int NC = nc_of(P), YS = ys_of(P), MS = ms_of(P), NQ = (NC + 3) / 4;
-    static_assert(YS % 4 == 0 && MS % 4 == 0 && 4 * NQ <= MS, "row layout");
+    static_assert(YS == MS && MS == 4 * NQ, "a box's m rows are m NQ consecutive quads");
+    const int m = ONE ? 1 : m_;
     const int64_t b = b0 + (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
     if (b >= b1 || plan.tgt_below[b] == 0) return;
     const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
-    // lane q holds quads q, q + 32, ... (one pass up to p = 10, two above)
-    for (int q = threadIdx.x & 31; q < NQ; q += 32)
-    for (int v = 0; v < m; ++v) {
-        float4* out = reinterpret_cast<float4*>(Lc + (b * m + v) * MS) + q;
+    const int F = m * NQ;  // the box's quads, all vectors
+    for (int f = threadIdx.x & 31; f < F; f += 32) {
+        const int q = f % NQ;  // the quad within its vector's row
+        float4* out = reinterpret_cast<float4*>(Lc + b * m * MS) + f;
         float4 s = accumulate ? *out : make_float4(0.f, 0.f, 0.f, 0.f);
         if (with_l2l) {
-            const float4 y = reinterpret_cast<const float4*>(Yo + (b * m + v) * YS)[q];
+            const float4 y = reinterpret_cast<const float4*>(Yo + b * m * YS)[f];
             if (accumulate)
                 add4(s, y);
             else
                 s = y;
         }
+        auto row = [&](int64_t e) { return __ldcs(reinterpret_cast<const float4*>(Yv + vpos[e] * m * YS) + f); };
         int64_t e = e0;
         for (; e + 16 <= e1; e += 16) {  // sixteen rows in flight, added in row order
             float4 y[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);
+            for (int j = 0; j < 16; ++j) y[j] = row(e + j);
 #pragma unroll
             for (int j = 0; j < 16; ++j) add4(s, y[j]);
         }
         for (; e + 8 <= e1; e += 8) {
             float4 y[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);
+            for (int j = 0; j < 8; ++j) y[j] = row(e + j);
 #pragma unroll
             for (int j = 0; j < 8; ++j) add4(s, y[j]);
         }
         for (; e + 4 <= e1; e += 4) {
             float4 y[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) y[j] = __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e + j] * m + v) * YS) + q);
+            for (int j = 0; j < 4; ++j) y[j] = row(e + j);
 #pragma unroll
             for (int j = 0; j < 4; ++j) add4(s, y[j]);
         }
-        for (; e < e1; ++e) add4(s, __ldcs(reinterpret_cast<const float4*>(Yv + (vpos[e] * m + v) * YS) + q));
+        for (; e < e1; ++e) add4(s, row(e));
         if (4 * q + 3 < NC) {
             *out = s;
         } else {  // the last quad: its coefficients below NC only (NC - 4q of them, 1 to 3)
