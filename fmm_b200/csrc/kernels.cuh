@@ -579,22 +579,34 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
 //   d/dz phi = sum w_mu Re(L_{k+1}^mu R_k^mu)          (L2P; M2P uses M_{k-1}, sign -)
 // Results (phi_hat, g_hat in the leaf's units) go to the f64 far-field partials.
 // ---------------------------------------------------------------------------------
+// The weight 2 of the orders mu > 0 is applied once at the end: their terms add into
+// their own sums (f1, dz1), the mu = 0 terms (real harmonics: no imaginary part) into f0,
+// dz0, so a term costs two fused multiply-adds, not a product, a difference and a scaled add.
 template <int P, typename T, bool GRAD>
 __device__ __forceinline__ void l2p_eval(const T* L, T x, T y, T z, T& phi, T& gx, T& gy, T& gz) {
     RegularRows<P, T> h;
     h.init(x, y, z);
-    T f = T(0), dz = T(0), are = T(0), aim = T(0);
+    T f0 = T(0), f1 = T(0), dz0 = T(0), dz1 = T(0), are = T(0), aim = T(0);
 #pragma unroll
     for (int k = 0; k <= P; ++k) {
         h.step(k);
 #pragma unroll
         for (int mu = 0; mu <= k; ++mu) {
-            T w = mu ? T(2) : T(1);
             Cx<T> c = coef_at(L, k, mu);
-            f += w * (c.re * h.cre[mu] - c.im * h.cim[mu]);
+            if (mu == 0) {
+                f0 += c.re * h.cre[0];
+            } else {
+                f1 += c.re * h.cre[mu];
+                f1 -= c.im * h.cim[mu];
+            }
             if (GRAD && k < P) {
                 Cx<T> c1 = coef_at(L, k + 1, mu);
-                dz += w * (c1.re * h.cre[mu] - c1.im * h.cim[mu]);
+                if (mu == 0) {
+                    dz0 += c1.re * h.cre[0];
+                } else {
+                    dz1 += c1.re * h.cre[mu];
+                    dz1 -= c1.im * h.cim[mu];
+                }
                 Cx<T> up = coef_at(L, k + 1, mu + 1);
                 are += up.re * h.cre[mu] - up.im * h.cim[mu];
                 aim += up.re * h.cim[mu] + up.im * h.cre[mu];
@@ -606,10 +618,10 @@ __device__ __forceinline__ void l2p_eval(const T* L, T x, T y, T z, T& phi, T& g
             }
         }
     }
-    phi = f;
+    phi = f0 + T(2) * f1;
     gx = are;
     gy = -aim;
-    gz = dz;
+    gz = dz0 + T(2) * dz1;
 }
 
 template <int P, typename T, bool GRAD>
@@ -618,20 +630,30 @@ __device__ __forceinline__ void m2p_eval(const T* M, T x, T y, T z, T& phi, T& g
     IrregularRows<P, T> h;
     T r2 = x * x + y * y + z * z;
     h.init(x, y, z, T(1) / sqrt(r2));
-    T f = T(0), dz = T(0), are = T(0), aim = T(0);
+    // the orders mu > 0 into their own sums, weighted 2 at the end (as l2p_eval)
+    T f0 = T(0), f1 = T(0), dz0 = T(0), dz1 = T(0), are = T(0), aim = T(0);
 #pragma unroll
     for (int k = 0; k <= KMAX; ++k) {
         h.step(k);
 #pragma unroll
         for (int mu = 0; mu <= k; ++mu) {
-            T w = mu ? T(2) : T(1);
             if (k <= P) {
                 Cx<T> c = coef_at(M, k, mu);
-                f += w * (c.re * h.cre[mu] - c.im * h.cim[mu]);
+                if (mu == 0) {
+                    f0 += c.re * h.cre[0];
+                } else {
+                    f1 += c.re * h.cre[mu];
+                    f1 -= c.im * h.cim[mu];
+                }
             }
             if (GRAD && k >= 1) {
                 Cx<T> c1 = coef_at(M, k - 1, mu);
-                dz -= w * (c1.re * h.cre[mu] - c1.im * h.cim[mu]);
+                if (mu == 0) {
+                    dz0 -= c1.re * h.cre[0];
+                } else {
+                    dz1 -= c1.re * h.cre[mu];
+                    dz1 += c1.im * h.cim[mu];
+                }
                 if (mu <= k - 2) {
                     Cx<T> up = coef_at(M, k - 1, mu + 1);
                     are += up.re * h.cre[mu] - up.im * h.cim[mu];
@@ -645,10 +667,10 @@ __device__ __forceinline__ void m2p_eval(const T* M, T x, T y, T z, T& phi, T& g
             }
         }
     }
-    phi = f;
+    phi = f0 + T(2) * f1;
     gx = are;
     gy = -aim;
-    gz = dz;
+    gz = dz0 + T(2) * dz1;
 }
 
 // mode: bit 0 L2P, bit 1 M2P, bit 2 add into far_phi / far_g (else overwrite them).
@@ -758,22 +780,29 @@ __device__ __forceinline__ void l2p_eval_mv(const float* L, int nb, float x, flo
     constexpr int MS = ms_of(P);
     RegularRows<P, float> h;
     h.init(x, y, z);
+    float f1[VB];  // the orders mu > 0, weighted 2 at the end (as l2p_eval)
 #pragma unroll
-    for (int b = 0; b < VB; ++b) f[b] = 0.0f;
+    for (int b = 0; b < VB; ++b) f[b] = f1[b] = 0.0f;
 #pragma unroll
     for (int k = 0; k <= P; ++k) {
         h.step(k);
 #pragma unroll
         for (int mu = 0; mu <= k; ++mu) {
-            const float w = mu ? 2.0f : 1.0f;
 #pragma unroll
             for (int b = 0; b < VB; ++b)
                 if (b < nb) {
                     const Cx<float> c = coef_at(L + b * MS, k, mu);
-                    f[b] += w * (c.re * h.cre[mu] - c.im * h.cim[mu]);
+                    if (mu == 0) {
+                        f[b] += c.re * h.cre[0];
+                    } else {
+                        f1[b] += c.re * h.cre[mu];
+                        f1[b] -= c.im * h.cim[mu];
+                    }
                 }
         }
     }
+#pragma unroll
+    for (int b = 0; b < VB; ++b) f[b] += 2.0f * f1[b];
 }
 
 template <int P, int VB>
@@ -782,22 +811,29 @@ __device__ __forceinline__ void m2p_eval_mv(const float* M, int nb, float x, flo
     IrregularRows<P, float> h;
     const float r2 = x * x + y * y + z * z;
     h.init(x, y, z, 1.0f / sqrt(r2));
+    float f1[VB];  // the orders mu > 0, weighted 2 at the end (as l2p_eval)
 #pragma unroll
-    for (int b = 0; b < VB; ++b) f[b] = 0.0f;
+    for (int b = 0; b < VB; ++b) f[b] = f1[b] = 0.0f;
 #pragma unroll
     for (int k = 0; k <= P; ++k) {
         h.step(k);
 #pragma unroll
         for (int mu = 0; mu <= k; ++mu) {
-            const float w = mu ? 2.0f : 1.0f;
 #pragma unroll
             for (int b = 0; b < VB; ++b)
                 if (b < nb) {
                     const Cx<float> c = coef_at(M + b * MS, k, mu);
-                    f[b] += w * (c.re * h.cre[mu] - c.im * h.cim[mu]);
+                    if (mu == 0) {
+                        f[b] += c.re * h.cre[0];
+                    } else {
+                        f1[b] += c.re * h.cre[mu];
+                        f1[b] -= c.im * h.cim[mu];
+                    }
                 }
         }
     }
+#pragma unroll
+    for (int b = 0; b < VB; ++b) f[b] += 2.0f * f1[b];
 }
 
 // ---------------------------------------------------------------------------------
