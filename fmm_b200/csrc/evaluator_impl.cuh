@@ -116,8 +116,9 @@ struct Evaluator final : EvaluatorBase {
     // the near-singular pairs' weights (per pair) and, per evaluation, their f64 sums per
     // target and vector (close_weights_kernel, close_sum_kernel)
     DevBuf close_w, close_acc;
-    // boxes with a nonempty X list, level by level (the P2L launches)
-    DevBuf xbox;
+    // boxes with a nonempty X list, level by level (the P2L launches), and the f32 P2L's
+    // per-entry records (XRec)
+    DevBuf xbox, xrec;
     std::vector<int64_t> xbox_start;
     // the near field summed apart on a second, lower-priority stream, joined by output_kernel
     DevBuf near_phi, near_g;
@@ -252,6 +253,12 @@ struct Evaluator final : EvaluatorBase {
             }
             xbox_start[pl.nlevels] = (int64_t)xb.size();
             xbox.upload(xb);
+            if (kMixed && !xb.empty()) {  // the f32 P2L's entry records
+                xrec.alloc(sizeof(XRec) * (pl.x.nnz() + 1));
+                x_record_kernel<<<(unsigned)((xb.size() + 127) / 128), 128>>>(dp, xbox.as<int32_t>(),
+                                                                              (int64_t)xb.size(), xrec.as<XRec>());
+                CUDA_TRY(cudaGetLastError());
+            }
         }
         int least = 0, greatest = 0;
         CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -908,7 +915,7 @@ struct Evaluator final : EvaluatorBase {
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
-                               &near_phi, &near_g, &box_side, &v_pos, &xbox, &fu_tile_d, &fu_tile_begin,
+                               &near_phi, &near_g, &box_side, &v_pos, &xbox, &xrec, &fu_tile_d, &fu_tile_begin,
                                &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
                                &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src, &st_rowpair,
                                &st_xy, &st_zz, &st_idx, &close_w, &close_acc};
@@ -1215,11 +1222,11 @@ struct Evaluator final : EvaluatorBase {
         if (kBflyP2L && m == 1)
             expand_bfly_kernel<P, true, false><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
-                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr), xrec.as<XRec>());
         else if (kBflyP2L)
             expand_bfly_kernel<P, true, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
-                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr));
+                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr), xrec.as<XRec>());
         else
             expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), stream>>>(
                 dp, b0, b1, xbox.as<int32_t>(), m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());

@@ -195,11 +195,41 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
 // NCP/32 finished slots (NCP = slots padded to a multiple of 32).  The summation order
 // is fixed (per-lane partial sums, then a fixed tree), so results are repeatable.
 // ---------------------------------------------------------------------------------
+// One X-list entry of the f32 P2L, fixed at build (x_record_kernel): the source leaf's
+// frame seen from the target box, (c(t|s), r(t|s)) of rel_frame<float>, and its sources,
+// so that an entry costs one load, issued while the entry before it is summed.
+struct __align__(16) XRec {
+    float4 frame;  // (c0, c1, c2, r)
+    long long s0;  // the source leaf's first source (leaf order)
+    int ns;        // its sources
+    int pad;
+};
+
+// Build time: thread per X entry of the boxes of `rows` (x_row order).
+static __global__ void x_record_kernel(DevPlan plan, const int32_t* __restrict__ rows, int64_t nrows,
+                                       XRec* __restrict__ rec) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    const int box = rows[r];
+    for (int64_t e = plan.x_row[box]; e < plan.x_row[box + 1]; ++e) {
+        const int sleaf = plan.x_col[e];
+        float c[3], fr;
+        rel_frame<float>(plan, box, plan.leaf_box[sleaf], c, fr);
+        XRec x;
+        x.frame = make_float4(c[0], c[1], c[2], fr);
+        x.s0 = plan.src_start[sleaf];
+        x.ns = (int)(plan.src_start[sleaf + 1] - plan.src_start[sleaf]);
+        x.pad = 0;
+        rec[e] = x;
+    }
+}
+
 template <int P, bool IRREG, bool MULTI>
 __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t row_begin, int64_t row_end,
                                                          const int32_t* __restrict__ rows,
                                                          const float4* __restrict__ spos, int m,
-                                                         const float* __restrict__ sq, float* __restrict__ out) {
+                                                         const float* __restrict__ sq, float* __restrict__ out,
+                                                         const XRec* __restrict__ xrec = nullptr) {
     constexpr int NC = nc_of(P);
     constexpr int NCP = ((NC + 31) / 32) * 32;
     const int lane = threadIdx.x;
@@ -228,14 +258,28 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
     float w[NCP];
 #pragma unroll
     for (int c = 0; c < NCP; ++c) w[c] = 0.0f;
+    // P2L: the entries' records, the next one loaded while the current one is summed
+    XRec xn{};
+    if (IRREG) xn = xrec[ent0];
     for (int e = 0; e < nent; ++e) {
-        const int sleaf = IRREG ? plan.x_col[ent0 + e] : (int)row;
-        float fc[3] = {0.0f, 0.0f, 0.0f}, fr = 1.0f;
-        if (IRREG) rel_frame<float>(plan, box, plan.leaf_box[sleaf], fc, fr);  // (c(t|s), r(t|s))
+        float fc[3] = {0.0f, 0.0f, 0.0f}, fr = 1.0f;  // (c(t|s), r(t|s))
+        int64_t s0, s1;
+        if (IRREG) {
+            const XRec xr = xn;
+            if (e + 1 < nent) xn = xrec[ent0 + e + 1];
+            fc[0] = xr.frame.x;
+            fc[1] = xr.frame.y;
+            fc[2] = xr.frame.z;
+            fr = xr.frame.w;
+            s0 = xr.s0;
+            s1 = s0 + xr.ns;
+        } else {
+            s0 = plan.src_start[row];
+            s1 = plan.src_start[row + 1];
+        }
         const float finv = 1.0f / fr;
-        const int64_t s1 = plan.src_start[sleaf + 1];
         // the lane's next source is loaded before its current one is summed
-        int64_t si = plan.src_start[sleaf] + lane;
+        int64_t si = s0 + lane;
         float4 pn = make_float4(0.f, 0.f, 0.f, 0.f);
         float qn = 0.f;
         if (si < s1) {
