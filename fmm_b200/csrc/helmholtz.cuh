@@ -77,8 +77,14 @@ __device__ __forceinline__ void helm_pair_f32(float kre, float kim, float dx, fl
     const float rinv = rsqrtf(r2);
     const float r = r2 * rinv;
     const float damping = -(kim * r), phase = kre * r;
+    // the phase reduced to [-pi, pi] by Cody and Waite's two-step reduction (2 pi as a float
+    // head and its remainder), then the hardware sine and cosine, whose error there is
+    // below 2^-21 absolute: the f32 pair terms' own level
+    const float turns = rintf(phase * 0.159154943091895336f);  // 1 / (2 pi)
+    float pr = fmaf(-turns, 6.28318548202514648f, phase);     // 2 pi rounded to float
+    pr = fmaf(-turns, -1.74845553146951640e-7f, pr);           // 2 pi minus that float
     float s, c;
-    sincosf(phase, &s, &c);
+    __sincosf(pr, &s, &c);
     const float decay = kim == 0.0f ? 1.0f : expf(damping);
     const Cplx<float> e{decay * c, decay * s};
     const Cplx<float> qe = cmul(q, e);
