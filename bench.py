@@ -465,6 +465,8 @@ def run_ours(args):
                 line[key] = {"error": f"{type(e).__name__}: {str(e)[:200]}"}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
+        if isinstance(line.get("helmholtz"), dict) and "mixed" in line["helmholtz"]:
+            line["helmholtz"]["cpu_oracle"] = helmholtz_cpu_oracle()
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -819,6 +821,27 @@ def run_helmholtz(F, torch, dev, flush, n=1_000_000, k=20.0, p=10, leaf=96, step
     del dq, dphi, dg
     torch.cuda.empty_cache()
     return res
+
+
+def helmholtz_cpu_oracle(n=5000, k=20.0, p=10, leaf=96):
+    """The oracle's Helmholtz FMM (oracle/oracle.py helmholtz_fmm: per-box Python loops over the
+    C operators of oracle/helmholtz_ops.c) timed on a bounded sample of the Helmholtz
+    configuration: the test restatement of the reference's host-only Helmholtz path, reported
+    beside the device numbers as the reference arm of this leg; it is not the reference's own
+    host speed (its Rust operator cannot be built here)."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(SEED + 13)
+    x = rng.uniform(0.0, 1.0, (n, 3))
+    q = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    t0 = time.perf_counter()
+    O.helmholtz_fmm(x, q, x, k, p, leaf)
+    s = time.perf_counter() - t0
+    return {"value": round(n / s / 1e6, 6), "unit": "Mpoints/s", "seconds": round(s, 2), "cores": 1,
+            "kind": "oracle", "sample": f"N={n} uniform in the unit cube, k={k}, p={p}, {leaf} per leaf, phi+grad, "
+                                        "one evaluation (tables built inside it)",
+            "note": "the oracle's Python-driven Helmholtz FMM: a checker, far slower than the reference's "
+                    "host operator; the ratio to it says nothing about the kernels"}
 
 
 CPU_REPEATS = 5
