@@ -1,7 +1,8 @@
 """Every compiled expansion order (3 to 12) against the oracle (needs a B200: -m gpu):
 f64 within 1e-12 and the mixed form within 2e-6 relative L2 over all targets, with
-gradients; the mixed M2L runs on the tensor cores up to p = 10 ((p+1)^2 <= 128 output
-slots) and on the f32 SIMT GEMM above; the level calls give the fused evaluation's bits."""
+gradients; the mixed M2L runs on the tensor cores at every order (above p = 10, where
+(p+1)^2 > 128 output slots, each tile once per half of them); the level calls and the
+tuner's alternative M2L tile give the fused evaluation's bits."""
 import numpy as np
 import pytest
 
@@ -32,6 +33,10 @@ def test_order_matches_oracle(oracle, points, p):
         if p in (10, 12):
             lv = fmm.evaluate_levels(q)
             assert np.array_equal(lv.potential, out.potential) and np.array_equal(lv.gradient, out.gradient)
+        if precision == "mixed" and p in (7, 11, 12):
+            fmm.set_m2l_tile(1)
+            alt = fmm.evaluate(q)
+            assert np.array_equal(alt.potential, out.potential) and np.array_equal(alt.gradient, out.gradient)
         fmm.close()
 
 
