@@ -116,9 +116,13 @@ struct Evaluator final : EvaluatorBase {
     // the near-singular pairs' weights (per pair) and, per evaluation, their f64 sums per
     // target and vector (close_weights_kernel, close_sum_kernel)
     DevBuf close_w, close_acc;
-    // boxes with a nonempty X list, level by level (the P2L launches), and the f32 P2L's
-    // per-entry records (XRec)
-    DevBuf xbox, xrec;
+    // boxes with a nonempty X list, level by level (the P2L launches), the f32 P2L's
+    // per-entry records (XRec), and the X-list sums of the f32 P2L when it runs apart (Lx,
+    // a box's rows as in Lc): in the evaluation with the near-singular sums on near_stream,
+    // the P2L of every level runs there too, beside the upward pass, and the local reduce
+    // adds Lx last (the same floats as adding P2L into the stored locals)
+    DevBuf xbox, xrec, Lx;
+    bool p2l_apart = false;  // set for one evaluation of that form
     std::vector<int64_t> xbox_start;
     // the near field summed apart on a second, lower-priority stream, joined by output_kernel
     DevBuf near_phi, near_g;
@@ -253,7 +257,8 @@ struct Evaluator final : EvaluatorBase {
             }
             xbox_start[pl.nlevels] = (int64_t)xb.size();
             xbox.upload(xb);
-            if (kMixed && !xb.empty()) {  // the f32 P2L's entry records
+            if (kMixed && !xb.empty()) {  // the f32 P2L's entry records and its apart sums
+                Lx.alloc(sizeof(float) * (size_t)m * ms_of(P) * pl.nboxes());
                 xrec.alloc(sizeof(XRec) * (pl.x.nnz() + 1));
                 x_record_kernel<<<(unsigned)((xb.size() + 127) / 128), 128>>>(dp, xbox.as<int32_t>(),
                                                                               (int64_t)xb.size(), xrec.as<XRec>());
@@ -438,19 +443,20 @@ struct Evaluator final : EvaluatorBase {
 
     // the local reduce of boxes [b0, b1): f32 a warp per box with 16-byte accesses, f64 a
     // block per box (the same order of additions either way)
-    void reduce_range(int64_t b0, int64_t b1, int with_l2l, int with_v, int accumulate) {
+    void reduce_range(int64_t b0, int64_t b1, int with_l2l, int with_v, int accumulate, bool with_x = false) {
         if (b1 <= b0) return;
         if constexpr (kMixed) {
             const unsigned g = counted((unsigned)((b1 - b0 + 3) / 4));
             const auto* yo = reinterpret_cast<const float*>(Yo.ptr);
             const auto* yv = reinterpret_cast<const float*>(Y.ptr);
             auto* lc = reinterpret_cast<float*>(Lc.ptr);
+            const auto* lx = with_x ? reinterpret_cast<const float*>(Lx.ptr) : nullptr;
             if (m == 1)
                 local_reduce4_kernel<P, true><<<g, 128, 0, stream>>>(dp, b0, b1, m, with_l2l, with_v, accumulate, yo,
-                                                                     yv, v_pos.as<int64_t>(), lc);
+                                                                     yv, v_pos.as<int64_t>(), lc, lx);
             else
                 local_reduce4_kernel<P, false><<<g, 128, 0, stream>>>(dp, b0, b1, m, with_l2l, with_v, accumulate,
-                                                                      yo, yv, v_pos.as<int64_t>(), lc);
+                                                                      yo, yv, v_pos.as<int64_t>(), lc, lx);
         } else
             local_reduce_kernel<P, T><<<counted((unsigned)(b1 - b0)), round32(NC), 0, stream>>>(
                 dp, b0, b1, m, with_l2l, with_v, accumulate, Yo.as<T>(), Y.as<T>(), v_pos.as<int64_t>(),
@@ -915,7 +921,7 @@ struct Evaluator final : EvaluatorBase {
                                &close_row, &close_src, &close_leaf, &spos64, &tpos64, &sq64, &close_y, &tc_tile_d,
                                &tc_tile_begin, &tc_tile_count, &tc_pair_e, &tc_pair_src, &tc_bimg, &tc_error, &near_rec,
                                &ltile_d, &ltile_begin, &ltile_count, &tc_ltile_d, &tc_ltile_begin, &tc_ltile_count,
-                               &near_phi, &near_g, &box_side, &v_pos, &xbox, &xrec, &fu_tile_d, &fu_tile_begin,
+                               &near_phi, &near_g, &box_side, &v_pos, &xbox, &xrec, &Lx, &fu_tile_d, &fu_tile_begin,
                                &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
                                &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src, &st_rowpair,
                                &st_xy, &st_zz, &st_idx, &close_w, &close_acc};
@@ -958,9 +964,13 @@ struct Evaluator final : EvaluatorBase {
             return;
         }
         const bool forked = sums && !timer.on;
+        // P2L apart on near_stream: the product path (all levels' M2L products at once)
+        p2l_apart = forked && (kinds & 2) && m2l_path == 1 && chunks.empty() && Lx.ptr;
         if (forked) {
             CUDA_TRY(cudaEventRecord(ev_fork, stream));
             CUDA_TRY(cudaStreamWaitEvent(near_stream, ev_fork, 0));
+            if (p2l_apart)  // first: the first local reduce waits for it
+                for (int l = 2; l < plan.nlevels; ++l) p2l_level(l, true, near_stream);
             close_sums(near_stream);
             CUDA_TRY(cudaEventRecord(ev_join, near_stream));
         }
@@ -971,7 +981,8 @@ struct Evaluator final : EvaluatorBase {
         } else {
             run_far();
         }
-        if (forked) CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
+        if (forked && !p2l_apart) CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
+        p2l_apart = false;
         if (items.count) timer.run(kP2P, [&] { p2p_levels(0, plan.nlevels, kinds & 1, 0, d_phi, d_grad); });
         CUDA_TRY(cudaGetLastError());
     }
@@ -1104,13 +1115,15 @@ struct Evaluator final : EvaluatorBase {
         }
         // M2L products of every level at once (all multipoles are final here)
         timer.run(kM2L, [&] { m2l_products(-1); });
+        // P2L apart: its sums (on near_stream) are read by the first reduce
+        if (p2l_apart) CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
         // downward: for l = 2..L: L2L products, the local (L2L + V in offset order), then P2L
         for (int l = 2; l <= L; ++l) {
             timer.run(kL2L, [&] {
                 l2l_products(l);
-                reduce_locals(l, l >= 3, 1, 0);
+                reduce_locals(l, l >= 3, 1, 0, p2l_apart);
             });
-            timer.run(kP2L, [&] { p2l_level(l); });
+            if (!p2l_apart) timer.run(kP2L, [&] { p2l_level(l); });
         }
         // leaves: L2P + M2P
         timer.run(kFar, [&] { leaf_far(0, (int64_t)plan.nleaves(), 3); });
@@ -1212,23 +1225,27 @@ struct Evaluator final : EvaluatorBase {
                 oct_pair_e.as<int64_t>(), oct_pair_src.as<int32_t>(), m, l2l_tab.as<T>(), Lc.as<T>(), Yo.as<T>());
     }
 
-    void reduce_locals(int l, int with_l2l, int with_v, int accumulate) {
-        reduce_range(plan.level_start[l], plan.level_start[l + 1], with_l2l, with_v, accumulate);
+    void reduce_locals(int l, int with_l2l, int with_v, int accumulate, bool with_x = false) {
+        reduce_range(plan.level_start[l], plan.level_start[l + 1], with_l2l, with_v, accumulate, with_x);
     }
 
-    void p2l_level(int l) {  // the boxes of level l with an X list
+    // P2L of the boxes of level l with an X list: added into the locals, or (apart, true)
+    // written into Lx on stream s for the local reduce to add (mixed form)
+    void p2l_level(int l, bool apart = false, cudaStream_t s = nullptr) {
         const int64_t b0 = xbox_start[l], b1 = xbox_start[l + 1];
         if (b1 <= b0) return;
+        if (!s) s = stream;
+        float* out = reinterpret_cast<float*>(apart ? Lx.ptr : Lc.ptr);
         if (kBflyP2L && m == 1)
-            expand_bfly_kernel<P, true, false><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+            expand_bfly_kernel<P, true, false><<<counted((unsigned)(b1 - b0)), 32, 0, s>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
-                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr), xrec.as<XRec>());
+                reinterpret_cast<const float*>(sq.ptr), out, xrec.as<XRec>(), apart ? 1 : 0);
         else if (kBflyP2L)
-            expand_bfly_kernel<P, true, true><<<counted((unsigned)(b1 - b0)), 32, 0, stream>>>(
+            expand_bfly_kernel<P, true, true><<<counted((unsigned)(b1 - b0)), 32, 0, s>>>(
                 dp, b0, b1, xbox.as<int32_t>(), reinterpret_cast<const float4*>(spos.ptr), m,
-                reinterpret_cast<const float*>(sq.ptr), reinterpret_cast<float*>(Lc.ptr), xrec.as<XRec>());
-        else
-            expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), stream>>>(
+                reinterpret_cast<const float*>(sq.ptr), out, xrec.as<XRec>(), apart ? 1 : 0);
+        else  // (f64: never apart)
+            expand_kernel<P, T, true><<<counted((unsigned)(b1 - b0)), 32, exp_smem(), s>>>(
                 dp, b0, b1, xbox.as<int32_t>(), m, spos.as<T4>(), sq.as<T>(), Lc.as<T>());
     }
 

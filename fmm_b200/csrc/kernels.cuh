@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
                                                          const int32_t* __restrict__ rows,
                                                          const float4* __restrict__ spos, int m,
                                                          const float* __restrict__ sq, float* __restrict__ out,
-                                                         const XRec* __restrict__ xrec = nullptr) {
+                                                         const XRec* __restrict__ xrec = nullptr, int overwrite = 0) {
     constexpr int NC = nc_of(P);
     constexpr int NCP = ((NC + 31) / 32) * 32;
     const int lane = threadIdx.x;
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
     for (int i = 0; i < NCP / 32; ++i) {
         const int c = base + i;
         if (c < NC) {
-            if (IRREG) o[c] += w[i];
+            if (IRREG && !overwrite) o[c] += w[i];
             else o[c] = w[i];
         }
     }
@@ -435,7 +435,8 @@ template <int P, bool ONE>  // ONE: m = 1 at compile time
 __global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int64_t b0, int64_t b1, int m_,
                                                             int with_l2l, int with_v, int accumulate,
                                                             const float* __restrict__ Yo, const float* __restrict__ Yv,
-                                                            const int64_t* __restrict__ vpos, float* __restrict__ Lc) {
+                                                            const int64_t* __restrict__ vpos, float* __restrict__ Lc,
+                                                            const float* __restrict__ Lx = nullptr) {
     constexpr int NC = nc_of(P), YS = ys_of(P), MS = ms_of(P), NQ = (NC + 3) / 4;
     static_assert(YS == MS && MS == 4 * NQ, "a box's m rows are m NQ consecutive quads");
     const int m = ONE ? 1 : m_;
@@ -443,6 +444,9 @@ __global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int
     if (b >= b1 || plan.tgt_below[b] == 0) return;
     const int64_t e0 = plan.v_row[b], e1 = with_v ? plan.v_row[b + 1] : e0;
     const int F = m * NQ;  // the box's quads, all vectors
+    // P2L computed apart (Lx, the box's X-list sum, written by the P2L kernel beside the
+    // upward pass): added last, as the P2L kernel adds it to the stored locals otherwise
+    const bool with_x = Lx && plan.x_row[b + 1] > plan.x_row[b];
     for (int f = threadIdx.x & 31; f < F; f += 32) {
         const int q = f % NQ;  // the quad within its vector's row
         float4* out = reinterpret_cast<float4*>(Lc + b * m * MS) + f;
@@ -478,6 +482,7 @@ __global__ void __launch_bounds__(128, 4) local_reduce4_kernel(DevPlan plan, int
             for (int j = 0; j < 4; ++j) add4(s, y[j]);
         }
         for (; e < e1; ++e) add4(s, row(e));
+        if (with_x) add4(s, reinterpret_cast<const float4*>(Lx + b * m * MS)[f]);
         if (4 * q + 3 < NC) {
             *out = s;
         } else {  // the last quad: its coefficients below NC only (NC - 4q of them, 1 to 3)
