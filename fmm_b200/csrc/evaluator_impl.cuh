@@ -17,6 +17,7 @@
 #include "evaluator_base.hpp"
 #include "helmholtz.cuh"
 #include "helmholtz_far.cuh"
+#include "helmholtz_st.cuh"
 #include "kernels.cuh"
 #include "m2l_fused.cuh"
 #include "m2l_tc.cuh"
@@ -1638,6 +1639,34 @@ struct Evaluator final : EvaluatorBase {
     void helm_near_launch(double kre, double kim, double* d_phi, double* d_grad, const double* far_phi,
                           const double* far_g) {
         if (!items.count) return;
+        if constexpr (kMixed) {
+            // one vector, a real wavenumber and the near rows' streams built: the streamed
+            // kernel over the P2P work lists (item slots 32, 16, 8, 4)
+            if (m == 1 && kim == 0.0 && p2p_path == 1) {
+                const P2pStream st{st_rowpair.as<int64_t>(), st_xy.as<float4>(), st_zz.as<float2>(),
+                                   st_idx.as<int2>()};
+                for (int c = 0; c < kP2pClasses; ++c) {
+                    const P2pItems it = plist[c];
+                    if (!it.count) continue;
+                    const HelmStArgs a{dp, it, kTheta2, kre, st, hq.as<Cplx<float>>(),
+                                       reinterpret_cast<const float4*>(tpos.ptr), close, hq64.as<double2>(),
+                                       far_phi, far_g, d_phi, gradients ? d_grad : nullptr};
+                    const unsigned g = counted((unsigned)it.count);
+                    if (gradients) {
+                        if (c == 0) helm_st_kernel<true, 1><<<g, 32, 0, stream>>>(a);
+                        else if (c == 1) helm_st_kernel<true, 2><<<g, 32, 0, stream>>>(a);
+                        else if (c == 2) helm_st_kernel<true, 4><<<g, 32, 0, stream>>>(a);
+                        else helm_st_kernel<true, 8><<<g, 32, 0, stream>>>(a);
+                    } else {
+                        if (c == 0) helm_st_kernel<false, 1><<<g, 32, 0, stream>>>(a);
+                        else if (c == 1) helm_st_kernel<false, 2><<<g, 32, 0, stream>>>(a);
+                        else if (c == 2) helm_st_kernel<false, 4><<<g, 32, 0, stream>>>(a);
+                        else helm_st_kernel<false, 8><<<g, 32, 0, stream>>>(a);
+                    }
+                }
+                return;
+            }
+        }
         const unsigned g = (unsigned)((items.count + kHelmWarps - 1) / kHelmWarps);
         if (gradients)
             helm_p2p_kernel<T, true, kMixed><<<counted(g), 32 * kHelmWarps, 0, stream>>>(
