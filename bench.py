@@ -13,8 +13,10 @@ value     : N / (device time of one evaluation) in Mpoints/s, inputs resident in
             L2 flushed (a 512 MiB write) before every timed step, CUDA events on the
             evaluator's stream; the evaluation replayed from one captured CUDA graph of the
             whole sweep (fmmgpu_fmm_set_graph; direct launches reported beside it).
-e2e       : the same through the public host API (fmmgpu_fmm_evaluate) with pinned host
-            buffers, host->device charges and device->host outputs inside the timed call.
+e2e       : the same through the public host API with pinned host buffers, host->device
+            charges and device->host outputs inside the timed call: the f32 call
+            (fmmgpu_fmm_evaluate_f32, the reference's Fmm<f32> value type, as its f32 runs
+            use it) with its error at the sampled targets, the f64 call beside it.
 plain_f64 : the plain f64 evaluator (the drop-in) on the same input, for the mixed/plain
             ratio of the metric.
 error     : relative L2 of phi and grad at 2,000 sampled targets against an f64 direct sum
@@ -343,8 +345,27 @@ def run_ours(args):
     for _ in range(args.steps):
         F._check(F.lib().fmmgpu_fmm_evaluate(fmm._h, hq.data_ptr(), hphi.data_ptr(), hg.data_ptr()))
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    log(f"e2e (f64 host buffers) {e2e_ms:.3f} ms")
+    # the same through the f32 host call, the reference's Fmm<f32> value type (its f32
+    # runs take f32 charges and return f32 potentials and gradients): half the copies
+    q32 = q.astype(np.float32)
+    hq32 = torch.from_numpy(q32).pin_memory()
+    hphi32 = torch.empty(n, dtype=torch.float32).pin_memory()
+    hg32 = torch.empty(n * 3, dtype=torch.float32).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        F._check(F.lib().fmmgpu_fmm_evaluate_f32(fmm._h, hq32.data_ptr(), hphi32.data_ptr(), hg32.data_ptr()))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        F._check(F.lib().fmmgpu_fmm_evaluate_f32(fmm._h, hq32.data_ptr(), hphi32.data_ptr(), hg32.data_ptr()))
+    e2e32_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     fmm.close()
-    log(f"e2e {e2e_ms:.3f} ms")
+    log(f"e2e (f32 host buffers) {e2e32_ms:.3f} ms")
+    # its error against the f64 direct sum of the charges it was given (rounded to f32)
+    ex32_phi, ex32_g = F.direct_sum(x, q32.astype(np.float64), x[sample], device=local)
+    phi32 = hphi32.numpy().astype(np.float64)
+    g32 = hg32.numpy().astype(np.float64).reshape(n, 3)
+    err32_phi = float(np.linalg.norm(phi32[sample] - ex32_phi) / np.linalg.norm(ex32_phi))
+    err32_g = float(np.linalg.norm(g32[sample] - ex32_g) / np.linalg.norm(ex32_g))
     # the plain f64 evaluator on the same input, in the same graph mode
     plain = build("f64")
     plain_info = plain.info()
@@ -442,9 +463,15 @@ def run_ours(args):
         "launch_shapes": {"p2p_warps": info["p2p_warps"], "leaf_block": info["leaf_block"],
                           "plain_f64_leaf_block": plain_info["leaf_block"],
                           "note": "timed at build (autotune); build_s includes it"},
-        "e2e": {"value": round(n / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
-                "ms_per_step": round(e2e_ms, 4),
-                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8 * 4},
+        "e2e": {"value": round(n / (e2e32_ms * 1e-3) / 1e6, 3), "unit": "Mpoints/s",
+                "ms_per_step": round(e2e32_ms, 4),
+                "h2d_bytes_per_step": n * 4, "d2h_bytes_per_step": n * 4 * 4,
+                "call": "fmmgpu_fmm_evaluate_f32 (the reference's Fmm<f32>: f32 charges in, f32 phi and "
+                        "grad phi out, pinned host buffers, graph replay)",
+                "phi_rel_l2": err32_phi, "grad_rel_l2": err32_g,
+                "f64_host": {"value": round(n / (e2e_ms * 1e-3) / 1e6, 3), "ms_per_step": round(e2e_ms, 4),
+                             "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8 * 4,
+                             "call": "fmmgpu_fmm_evaluate (f64 charges in, f64 phi and grad phi out)"}},
         "gpu_launches": None,
         "roofline": roof,
         "clocks": clocks,

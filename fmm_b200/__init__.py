@@ -64,6 +64,7 @@ def lib():
             "fmmgpu_batch_build": (C.c_int, [C.POINTER(Settings), sz, dp, dp, dp, dp, C.POINTER(vp)]),
             "fmmgpu_batch_plan_build": (C.c_int, [C.POINTER(Settings), sz, dp, dp, dp, dp, C.POINTER(vp)]),
             "fmmgpu_fmm_evaluate": (C.c_int, [vp, dp, dp, dp]),
+            "fmmgpu_fmm_evaluate_f32": (C.c_int, [vp, dp, dp, dp]),
             "fmmgpu_fmm_evaluate_device": (C.c_int, [vp, dp, dp, dp]),
             "fmmgpu_fmm_vjp": (C.c_int, [vp, dp, dp, dp, dp, dp]),
             "fmmgpu_fmm_stream": (vp, [vp]),
@@ -432,11 +433,17 @@ class Fmm(Plan):
     """A built FMM on one GPU (nd-fmm-exec's Fmm): evaluate charge vectors."""
 
     def evaluate(self, charges):
+        """Fmm::evaluate (fmm.rs:3691): the value type follows the charges', as the reference's
+        Fmm<T> does: float32 charges give float32 potentials and gradients (the f64 evaluation
+        of the widened charges, rounded), anything else float64."""
         m = self.settings.vectors
-        q = np.ascontiguousarray(charges, dtype=np.float64).reshape(self.nsources, m)
-        phi = np.zeros((m, self.ntargets))
-        g = np.zeros((m, self.ntargets, 3)) if self.settings.gradients else None
-        _check(lib().fmmgpu_fmm_evaluate(self._h, _ptr(q), _ptr(phi), _ptr(g)))
+        f32 = np.asarray(charges).dtype == np.float32
+        dt = np.float32 if f32 else np.float64
+        q = np.ascontiguousarray(charges, dtype=dt).reshape(self.nsources, m)
+        phi = np.zeros((m, self.ntargets), dtype=dt)
+        g = np.zeros((m, self.ntargets, 3), dtype=dt) if self.settings.gradients else None
+        call = lib().fmmgpu_fmm_evaluate_f32 if f32 else lib().fmmgpu_fmm_evaluate
+        _check(call(self._h, _ptr(q), _ptr(phi), _ptr(g)))
         return Output(phi, g)
 
     def helmholtz_near(self, k, charges):

@@ -87,6 +87,7 @@ struct fmmgpu_fmm {
     DevBuf d_keep_q, d_keep_g, d_keep_flag;
     int64_t vjp_forward_reused = 0;
     DevBuf d_hq, d_hphi, d_hg;  // the Helmholtz host call's device buffers
+    DevBuf d_q32, d_out32;      // the f32 host call's charges and (potential, gradient) in f32
     int64_t tables_loaded = 0;  // tables taken from the table cache (bits: M2L, M2M, L2L)
     std::string table_cache_dir, tuning_cache_dir;  // the settings' cache directories ("" none)
     bool uploaded = false;         // the plan came from the caller (fmmgpu_upload_plan)
@@ -105,6 +106,18 @@ __global__ void differ_kernel(int64_t n, const unsigned long long* __restrict__ 
             return;
         }
 }
+
+// the f32 host call's conversions: charges widened to f64 exactly; potentials and
+// gradients rounded to the nearest f32 (ties to even)
+__global__ void widen_kernel(int64_t n, const float* __restrict__ a, double* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+__global__ void narrow_kernel(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = __double2float_rn(a[i]);
+}
+static unsigned grid_of(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
 // ---- vector-Jacobian products of phi(q, sources, targets) for a cotangent w on phi ----
 // dx_t[i] = sum_v w[v][i] grad phi_v(t_i)   (w, phi in the output layout [v][nt])
@@ -685,6 +698,42 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
             CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
                                      f->stream));
         CUDA_TRY(cudaStreamSynchronize(f->stream));
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    });
+}
+
+int fmmgpu_fmm_evaluate_f32(fmmgpu_fmm* f, const float* charges, float* potential, float* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const int64_t m = f->settings.vectors;
+        const int64_t ns = (int64_t)f->plan.src_perm.size(), nt = (int64_t)f->plan.tgt_perm.size();
+        const int64_t nq = m * ns, nout = m * nt * (f->settings.gradients ? 4 : 1);
+        if (f->d_q32.bytes < sizeof(float) * (size_t)(nq + 1)) f->d_q32.alloc(sizeof(float) * (size_t)(nq + 1));
+        if (f->d_out32.bytes < sizeof(float) * (size_t)(nout + 1)) f->d_out32.alloc(sizeof(float) * (size_t)(nout + 1));
+        cudaStream_t s = f->stream;
+        if (nq) {
+            CUDA_TRY(cudaMemcpyAsync(f->d_q32.ptr, charges, sizeof(float) * nq, cudaMemcpyHostToDevice, s));
+            widen_kernel<<<grid_of(nq), 256, 0, s>>>(nq, f->d_q32.as<float>(), f->d_charges.as<double>());
+            CUDA_TRY(cudaGetLastError());
+        }
+        run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(),
+                       f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        keep_forward(f, f->d_charges.as<double>(), f->settings.gradients ? f->d_grad.as<double>() : nullptr);
+        const int64_t np = m * nt;
+        if (np) {
+            float* o = f->d_out32.as<float>();
+            narrow_kernel<<<grid_of(np), 256, 0, s>>>(np, f->d_phi.as<double>(), o);
+            if (f->settings.gradients)
+                narrow_kernel<<<grid_of(3 * np), 256, 0, s>>>(3 * np, f->d_grad.as<double>(), o + np);
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaMemcpyAsync(potential, o, sizeof(float) * np, cudaMemcpyDeviceToHost, s));
+            if (f->settings.gradients)
+                CUDA_TRY(cudaMemcpyAsync(gradient, o + np, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost, s));
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
         if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
     });
 }

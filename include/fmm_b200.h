@@ -194,6 +194,14 @@ int fmmgpu_batch_plan_build(const fmmgpu_settings* settings, size_t ncloud, cons
  * NULL without gradients).  Copies in, evaluates, copies out, synchronises. */
 int fmmgpu_fmm_evaluate(fmmgpu_fmm* fmm, const double* charges, double* potential, double* gradient);
 
+/* Fmm<f32>::evaluate_into (fmm.rs:3719 with T = f32, the value type of the reference's
+ * f32 runs, fmm-bench/src/measure.rs:196) with HOST f32 buffers in the layouts of
+ * fmmgpu_fmm_evaluate: the charges are widened to f64 on the device (exactly), the
+ * evaluation is fmmgpu_fmm_evaluate's, and the potentials and gradients are rounded to
+ * the nearest f32 on the device, so each element is the f64 call's result on the widened
+ * charges, rounded; the copies move half the bytes.  Synchronises. */
+int fmmgpu_fmm_evaluate_f32(fmmgpu_fmm* fmm, const float* charges, float* potential, float* gradient);
+
 /* Vector-Jacobian product of the potentials (no reference counterpart; the reference has
  * no adjoint): for charges q and a cotangent w on the potentials (both HOST buffers, the
  * layouts of fmmgpu_fmm_evaluate: q[i*m + v], w[v*nt + i]) it returns
