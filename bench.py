@@ -671,7 +671,8 @@ def run_published_configs(F, torch, dev, flush):
     leaf; its times are the mean host call with one upload, one download and one sync):
     the same problems here (seeded numpy PCG64 in place of the reference's generator,
     charges U[-1,1)), timed both ways -- device-timed graph replays like the headline, and
-    the mean wall clock of the host call fmmgpu_fmm_evaluate, the published figures' form --
+    the mean wall clock of the host call (fmmgpu_fmm_evaluate_f32 for the f32 row, as the
+    published run's Fmm<f32>; fmmgpu_fmm_evaluate for the f64 rows), the published figures' form --
     with the relative L2 error of phi at 1,000 sampled targets against the GPU f64 direct
     sum."""
     cases = [  # (name, N, p, points per leaf, precision, gradients, published ms, source)
@@ -695,17 +696,21 @@ def run_published_configs(F, torch, dev, flush):
         ms = device_timed(f, torch, flush, dq, dphi, dg)
         phi = dphi.cpu().numpy()
         f.set_graph(True)
+        # the host call in the published run's value type: f32 for its f32 rows (the mixed
+        # form here, fmmgpu_fmm_evaluate_f32), f64 otherwise
+        qh = q.astype(np.float32) if prec == "mixed" else q
         for _ in range(3):
-            f.evaluate(q)
+            f.evaluate(qh)
         t0 = time.perf_counter()
         for _ in range(10):
-            f.evaluate(q)
+            f.evaluate(qh)
         host_ms = (time.perf_counter() - t0) * 100.0
         pick = np.random.default_rng(SEED).choice(n, 1000, replace=False)
         ex, _ = F.direct_sum(x, q, x[pick], gradients=False)
         err = float(np.linalg.norm(phi[pick] - ex) / np.linalg.norm(ex))
         out[name] = {"n": n, "p": p, "leaf": leaf, "precision": prec, "gradients": grad,
                      "device_ms": round(ms, 4), "host_call_ms": round(host_ms, 4),
+                     "host_call_value_type": str(qh.dtype),
                      "mpoints_per_s": round(n / (host_ms * 1e-3) / 1e6, 2), "phi_rel_l2": err,
                      "published_ms": pub_ms, "published_source": src,
                      "host_call_speedup_vs_published": round(pub_ms / host_ms, 2)}
@@ -788,7 +793,8 @@ def run_helmholtz(F, torch, dev, flush, n=1_000_000, k=20.0, p=10, leaf=96, step
     per leaf, potential and gradient of e^{ikr}/(4 pi r).  The whole FMM (near and far
     field) in f64 and in the mixed form: device time per evaluation (graph-free launches on
     the evaluator's stream, L2 flushed before every step, CUDA events), the host call with
-    the copies (best of three), the tables' host build time for the new k, and the relative
+    pinned buffers and the copies (best of four; complex64 for the mixed form, complex128
+    for f64), the tables' host build time for the new k, and the relative
     L2 error of phi and grad at 1,000 sampled targets against the f64 direct sum (GPU,
     Neumaier, complex128); the near field alone (P2P) is timed beside it."""
     rng = np.random.default_rng(SEED + 11)
@@ -803,7 +809,9 @@ def run_helmholtz(F, torch, dev, flush, n=1_000_000, k=20.0, p=10, leaf=96, step
                        "phi+grad, complex charges N(0,1)+iN(0,1)",
            "data": "synthetic (numpy PCG64, seeded)", "unit": "Mpoints/s",
            "timing": "device: CUDA events on the evaluator's stream, L2 flushed before each step; "
-                     "host_call: fmmgpu_helmholtz_evaluate with the copies, best of 3"}
+                     "host_call: the host call with pinned buffers and the copies, best of 4 (mixed: "
+                     "fmmgpu_helmholtz_evaluate_f32, complex64 in and out; f64: fmmgpu_helmholtz_evaluate, "
+                     "complex128)"}
     for prec in ("f64", "mixed"):
         t0 = time.perf_counter()
         f = F.FmmBuilder(p).gradients().max_points_per_leaf(leaf).precision(prec).build(x)
@@ -825,11 +833,21 @@ def run_helmholtz(F, torch, dev, flush, n=1_000_000, k=20.0, p=10, leaf=96, step
                 s1.synchronize()
                 total += s0.elapsed_time(s1)
         ms = total / steps
+        # the host call with pinned buffers, in the value type of the form: complex64 for
+        # the mixed one (fmmgpu_helmholtz_evaluate_f32), complex128 for f64
+        ct = torch.complex64 if prec == "mixed" else torch.complex128
+        hq = torch.from_numpy(q.astype(np.complex64 if prec == "mixed" else np.complex128)).pin_memory()
+        hphi = torch.empty(n, dtype=ct).pin_memory()
+        hg = torch.empty(3 * n, dtype=ct).pin_memory()
+        call = F.lib().fmmgpu_helmholtz_evaluate_f32 if prec == "mixed" else F.lib().fmmgpu_helmholtz_evaluate
         best = float("inf")
-        for _ in range(3):
+        for _ in range(4):
             t0 = time.perf_counter()
-            f.helmholtz_evaluate(k, q)
+            F._check(call(f._h, float(k), 0.0, hq.data_ptr(), hphi.data_ptr(), hg.data_ptr()))
             best = min(best, time.perf_counter() - t0)
+        hbytes = (hq.numel() + hphi.numel() + hg.numel()) * hq.element_size()
+        ephi_h = float(np.linalg.norm(hphi.numpy().astype(np.complex128)[pick] - ex) / np.linalg.norm(ex))
+        del hq, hphi, hg
         near = float("inf")
         for _ in range(2):
             t0 = time.perf_counter()
@@ -839,6 +857,8 @@ def run_helmholtz(F, torch, dev, flush, n=1_000_000, k=20.0, p=10, leaf=96, step
         egr = float(np.linalg.norm(out.gradient[0][pick] - eg) / np.linalg.norm(eg))
         res[prec] = {"ms_per_step": round(ms, 3), "value": round(n / (ms * 1e-3) / 1e6, 3),
                      "host_call_ms": round(best * 1e3, 3), "e2e_value": round(n / best / 1e6, 3),
+                     "host_call": {"value_type": str(ct).replace("torch.", ""), "copied_bytes": hbytes,
+                                   "phi_rel_l2": ephi_h},
                      "phi_rel_l2": ep, "grad_rel_l2": egr, "build_s": round(build_s, 2),
                      "tables_s": round(table_s, 2), "nlevels": info["nlevels"], "v_pairs": info["v_pairs"],
                      "near_field_host_call_ms": round(near * 1e3, 3), "near_pairs": info["near_pairs"]}

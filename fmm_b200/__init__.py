@@ -90,6 +90,7 @@ def lib():
             "fmmgpu_helmholtz_direct_sum": (C.c_int, [C.c_double, C.c_double, sz, dp, dp, sz, dp, dp, dp, C.c_int]),
             "fmmgpu_helmholtz_near": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
             "fmmgpu_helmholtz_evaluate": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
+            "fmmgpu_helmholtz_evaluate_f32": (C.c_int, [vp, C.c_double, C.c_double, dp, dp, dp]),
             "fmmgpu_upload_plan": (C.c_int, [C.POINTER(Settings), vp, sz, dp, sz, dp, C.POINTER(vp)]),
             "fmmgpu_plan_from_arrays": (C.c_int, [C.POINTER(Settings), vp, sz, dp, sz, dp, C.POINTER(vp)]),
             "fmmgpu_fmm_plan_arrays": (C.c_int, [vp, vp]),
@@ -460,13 +461,18 @@ class Fmm(Plan):
     def helmholtz_evaluate(self, k, charges):
         """The whole Helmholtz FMM of e^{ikr}/(4 pi r) for a real k > 0 (near and far field)
         on this FMM's tree and lists, complex charges (ns, m): Output with complex potential
-        (m, nt) and gradient (m, nt, 3).  The tables of a new k are built on the first call."""
+        (m, nt) and gradient (m, nt, 3).  The tables of a new k are built on the first call.
+        complex64 charges give complex64 outputs (fmmgpu_helmholtz_evaluate_f32), anything
+        else complex128."""
         m = self.settings.vectors
-        q = np.ascontiguousarray(charges, dtype=np.complex128).reshape(self.nsources, m)
-        phi = np.zeros((m, self.ntargets), dtype=np.complex128)
-        g = np.zeros((m, self.ntargets, 3), dtype=np.complex128) if self.settings.gradients else None
+        c64 = np.asarray(charges).dtype == np.complex64
+        dt = np.complex64 if c64 else np.complex128
+        q = np.ascontiguousarray(charges, dtype=dt).reshape(self.nsources, m)
+        phi = np.zeros((m, self.ntargets), dtype=dt)
+        g = np.zeros((m, self.ntargets, 3), dtype=dt) if self.settings.gradients else None
         k = complex(k)
-        _check(lib().fmmgpu_helmholtz_evaluate(self._h, k.real, k.imag, _ptr(q), _ptr(phi), _ptr(g)))
+        call = lib().fmmgpu_helmholtz_evaluate_f32 if c64 else lib().fmmgpu_helmholtz_evaluate
+        _check(call(self._h, k.real, k.imag, _ptr(q), _ptr(phi), _ptr(g)))
         return Output(phi, g)
 
     def helmholtz_evaluate_device(self, k, charges_ptr, potential_ptr, gradient_ptr=None):

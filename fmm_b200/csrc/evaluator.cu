@@ -896,6 +896,47 @@ int fmmgpu_helmholtz_evaluate(fmmgpu_fmm* f, double k_re, double k_im, const dou
     });
 }
 
+int fmmgpu_helmholtz_evaluate_f32(fmmgpu_fmm* f, double k_re, double k_im, const float* charges, float* potential,
+                                  float* gradient) {
+    return guarded([&] {
+        if (!f || !charges || !potential || (f->settings.gradients && !gradient))
+            throw Failure(FMMGPU_INVALID_ARGUMENT, "null argument");
+        if (!f->eval) throw Failure(FMMGPU_INVALID_ARGUMENT, "a plan-only handle cannot evaluate");
+        CUDA_TRY(cudaSetDevice(f->settings.device));
+        const int64_t m = f->settings.vectors;
+        const int64_t ns = (int64_t)f->plan.src_perm.size(), nt = (int64_t)f->plan.tgt_perm.size();
+        if (f->d_hq.bytes < sizeof(double) * 2 * m * (ns + 1)) {
+            f->d_hq.alloc(sizeof(double) * 2 * m * (ns + 1));
+            f->d_hphi.alloc(sizeof(double) * 2 * m * (nt + 1));
+            if (f->settings.gradients) f->d_hg.alloc(sizeof(double) * 6 * m * (nt + 1));
+        }
+        // complex numbers as (re, im) pairs: the conversions act on the 2n reals
+        const int64_t nq = 2 * m * ns, np = 2 * m * nt, ng = f->settings.gradients ? 3 * np : 0;
+        if (f->d_q32.bytes < sizeof(float) * (size_t)(nq + 1)) f->d_q32.alloc(sizeof(float) * (size_t)(nq + 1));
+        if (f->d_out32.bytes < sizeof(float) * (size_t)(np + ng + 1))
+            f->d_out32.alloc(sizeof(float) * (size_t)(np + ng + 1));
+        cudaStream_t s = f->stream;
+        if (nq) {
+            CUDA_TRY(cudaMemcpyAsync(f->d_q32.ptr, charges, sizeof(float) * nq, cudaMemcpyHostToDevice, s));
+            widen_kernel<<<grid_of(nq), 256, 0, s>>>(nq, f->d_q32.as<float>(), f->d_hq.as<double>());
+            CUDA_TRY(cudaGetLastError());
+        }
+        const int rc = fmmgpu_helmholtz_evaluate_device(f, k_re, k_im, f->d_hq.as<double>(), f->d_hphi.as<double>(),
+                                                        f->settings.gradients ? f->d_hg.as<double>() : nullptr);
+        if (rc != FMMGPU_OK) throw Failure(rc, g_last_error);
+        if (np) {
+            float* o = f->d_out32.as<float>();
+            narrow_kernel<<<grid_of(np), 256, 0, s>>>(np, f->d_hphi.as<double>(), o);
+            if (ng) narrow_kernel<<<grid_of(ng), 256, 0, s>>>(ng, f->d_hg.as<double>(), o + np);
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaMemcpyAsync(potential, o, sizeof(float) * np, cudaMemcpyDeviceToHost, s));
+            if (ng) CUDA_TRY(cudaMemcpyAsync(gradient, o + np, sizeof(float) * ng, cudaMemcpyDeviceToHost, s));
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
+        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+    });
+}
+
 double fmmgpu_helmholtz_table_seconds(const fmmgpu_fmm* f) { return f && f->eval ? f->eval->hh_table_seconds : 0.0; }
 
 int fmmgpu_op_begin_evaluation(fmmgpu_fmm* f, const double* charges) {

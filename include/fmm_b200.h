@@ -417,6 +417,13 @@ int fmmgpu_helmholtz_near(fmmgpu_fmm* fmm, double k_re, double k_im, const doubl
  * batches. */
 int fmmgpu_helmholtz_evaluate(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges, double* potential,
                               double* gradient);
+/* The same with complex64 HOST buffers (each complex number two floats, re then im; the
+ * value type of a Helmholtz FMM of T = f32, fmm-exec/src/helmholtz/fmm.rs:2277): the
+ * charges are widened to complex128 on the device, the evaluation is
+ * fmmgpu_helmholtz_evaluate's, and the potentials and gradients are rounded to complex64
+ * on the device, so the copies move half the bytes.  Synchronises. */
+int fmmgpu_helmholtz_evaluate_f32(fmmgpu_fmm* fmm, double k_re, double k_im, const float* charges, float* potential,
+                                  float* gradient);
 /* The same with DEVICE buffers on the evaluator's stream; does not synchronise (the
  * tables of a new k are built, on the host, before the launches are queued). */
 int fmmgpu_helmholtz_evaluate_device(fmmgpu_fmm* fmm, double k_re, double k_im, const double* charges,

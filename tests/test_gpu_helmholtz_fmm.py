@@ -87,3 +87,18 @@ def test_complex_wavenumber_is_refused(cloud):
         fmm.helmholtz_evaluate(5.0 + 0.5j, q)
     assert e.value.status == 2
     fmm.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "f64"])
+def test_complex64_call_is_the_complex128_call_rounded(cloud, precision):
+    """fmmgpu_helmholtz_evaluate_f32: complex64 charges in, every complex64 output the
+    complex128 call's result on the widened charges, rounded (real and imaginary parts)."""
+    x, q = cloud
+    q64 = q.astype(np.complex64)
+    fmm = F.FmmBuilder(6).gradients().max_points_per_leaf(24).precision(precision).build(x)
+    want = fmm.helmholtz_evaluate(5.0, q64.astype(np.complex128))
+    got = fmm.helmholtz_evaluate(5.0, q64)
+    assert got.potential.dtype == np.complex64 and got.gradient.dtype == np.complex64
+    assert np.array_equal(got.potential, want.potential.astype(np.complex64))
+    assert np.array_equal(got.gradient, want.gradient.astype(np.complex64))
+    fmm.close()
