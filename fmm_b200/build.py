@@ -22,7 +22,7 @@ SOURCES = ["evaluator.cu", "direct.cu", "tree.cpp", "tables.cpp", "forest.cpp", 
            "table_cache.cpp", "plan_upload.cpp", "plan_gpu.cu", "p2p_launch.cu"]
 ORDER_SOURCE = "evaluator_order.cu"
 HEADERS = ["plan.hpp", "evaluator_base.hpp", "evaluator_impl.cuh", "kernels.cuh", "harmonics.cuh", "m2l_tc.cuh",
-           "m2l_fused.cuh", "p2p_x2.cuh", "helmholtz.cuh", "helmholtz_far.cuh", "helmholtz_st.cuh", "morton.hpp"]
+           "m2l_fused.cuh", "p2p_x2.cuh", "helmholtz.cuh", "helmholtz_far.cuh", "helmholtz_st.cuh", "leaf_far_x2.cuh", "morton.hpp"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -13,6 +13,7 @@
 #include <cstdint>
 
 #include "harmonics.cuh"
+#include "leaf_far_x2.cuh"
 
 namespace fmmb {
 
@@ -957,11 +958,14 @@ __device__ __forceinline__ void item_shape(const P2pItems& items, int64_t item, 
 // each target's harmonics once for up to VB vectors (l2p_eval_mv / m2p_eval_mv).
 // The gradient form is held to 96 registers up to p = 8 (21 warps an SM, no spills) and to
 // 168 above (12 warps an SM; no spills to p = 12).
+// With gradients (the mixed form's only use of this kernel) the terms run on the packed
+// f32x2 pipe, coefficient by coefficient (l2p_x2 / m2p_x2, leaf_far_x2.cuh).
 template <int P, bool GRAD>
 __global__ void __launch_bounds__(128, P <= 8 ? 5 : 3) leaf_far_items_kernel(DevPlan plan, P2pItems items, int mode, int m,
                                                              const float4* __restrict__ tpos,
                                                              const float* __restrict__ M, const float* __restrict__ Lc,
                                                              double* __restrict__ far_phi, double* __restrict__ far_g) {
+    static_assert(GRAD, "potentials: leaf_far_mv_items_kernel");
     const int64_t item = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (item >= items.count) return;
     const int leaf = items.leaf[item];
@@ -971,23 +975,24 @@ __global__ void __launch_bounds__(128, P <= 8 ? 5 : 3) leaf_far_items_kernel(Dev
     const int64_t w0 = plan.w_row[leaf], w1 = (mode & 2) ? plan.w_row[leaf + 1] : plan.w_row[leaf];
     const int64_t nt = plan.ntgt;
     const float4 p4 = tpos[t];
-    const float ux = p4.x, uy = p4.y, uz = p4.z;
     for (int v = 0; v < m; ++v) {
+        // an opaque copy of the position each vector: the harmonics are formed per
+        // evaluation in registers, never hoisted out of this loop as invariants (which held
+        // every row of them live across it and spilled)
+        float ux = p4.x, uy = p4.y, uz = p4.z;
+        asm volatile("" : "+f"(ux), "+f"(uy), "+f"(uz));
         double fphi = 0.0, fg[3] = {0.0, 0.0, 0.0};
         if (mode & 4) {
             fphi = far_phi[(int64_t)v * nt + t];
-            if (GRAD)
-                for (int k = 0; k < 3; ++k) fg[k] = far_g[((int64_t)v * nt + t) * 3 + k];
+            for (int k = 0; k < 3; ++k) fg[k] = far_g[((int64_t)v * nt + t) * 3 + k];
         }
         if (mode & 1) {
             float ph, gx, gy, gz;
-            l2p_eval<P, float, GRAD>(Lc + ((int64_t)box * m + v) * ms_of(P), ux, uy, uz, ph, gx, gy, gz);
+            l2p_x2<P>(Lc + ((int64_t)box * m + v) * ms_of(P), ux, uy, uz, ph, gx, gy, gz);
             fphi = (mode & 4) ? fphi + (double)ph : (double)ph;
-            if (GRAD) {
-                fg[0] = (mode & 4) ? fg[0] + (double)gx : (double)gx;
-                fg[1] = (mode & 4) ? fg[1] + (double)gy : (double)gy;
-                fg[2] = (mode & 4) ? fg[2] + (double)gz : (double)gz;
-            }
+            fg[0] = (mode & 4) ? fg[0] + (double)gx : (double)gx;
+            fg[1] = (mode & 4) ? fg[1] + (double)gy : (double)gy;
+            fg[2] = (mode & 4) ? fg[2] + (double)gz : (double)gz;
         }
         for (int64_t e = w0; e < w1; ++e) {
             const int s = plan.w_col[e];
@@ -995,23 +1000,19 @@ __global__ void __launch_bounds__(128, P <= 8 ? 5 : 3) leaf_far_items_kernel(Dev
             rel_frame<float>(plan, s, box, c, r);
             const float rinv = 1.0f / r;
             float ph, gx, gy, gz;
-            m2p_eval<P, float, GRAD>(M + ((int64_t)s * m + v) * ms_of(P), (ux - c[0]) * rinv, (uy - c[1]) * rinv,
-                                     (uz - c[2]) * rinv, ph, gx, gy, gz);
+            m2p_x2<P>(M + ((int64_t)s * m + v) * ms_of(P), (ux - c[0]) * rinv, (uy - c[1]) * rinv,
+                      (uz - c[2]) * rinv, ph, gx, gy, gz);
             fphi += (double)(ph * rinv);
-            if (GRAD) {
-                const float r2inv = rinv * rinv;
-                fg[0] += (double)(gx * r2inv);
-                fg[1] += (double)(gy * r2inv);
-                fg[2] += (double)(gz * r2inv);
-            }
+            const float r2inv = rinv * rinv;
+            fg[0] += (double)(gx * r2inv);
+            fg[1] += (double)(gy * r2inv);
+            fg[2] += (double)(gz * r2inv);
         }
         far_phi[(int64_t)v * nt + t] = fphi;
-        if (GRAD) {
-            double* g = far_g + ((int64_t)v * nt + t) * 3;
-            g[0] = fg[0];
-            g[1] = fg[1];
-            g[2] = fg[2];
-        }
+        double* g = far_g + ((int64_t)v * nt + t) * 3;
+        g[0] = fg[0];
+        g[1] = fg[1];
+        g[2] = fg[2];
     }
 }
 
