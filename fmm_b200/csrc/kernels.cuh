@@ -295,29 +295,37 @@ __global__ void __launch_bounds__(32) expand_bfly_kernel(DevPlan plan, int64_t r
                 qn = qv[si + 32];
             }
             const float x = (p4.x - fc[0]) * finv, y = (p4.y - fc[1]) * finv, z = (p4.z - fc[2]) * finv;
+            // conj(X) q into the slots: (w[slot(n, mm)], w[slot(n, -mm)]) += (q, -q) * X_n^mm,
+            // one packed fused multiply-add an order mm > 0 (the rows on the packed pipe,
+            // leaf_far_x2.cuh)
+            const float2 qq = make_float2(q, -q);
+            auto scatter = [&](int n, const float2* cr) {
+#pragma unroll
+                for (int mm = 0; mm <= n; ++mm) {
+                    if (mm == 0) {
+                        w[slot(n, 0)] = fmaf(q, cr[0].x, w[slot(n, 0)]);
+                    } else {
+                        const float2 acc = __ffma2_rn(qq, cr[mm], make_float2(w[slot(n, mm)], w[slot(n, -mm)]));
+                        w[slot(n, mm)] = acc.x;
+                        w[slot(n, -mm)] = acc.y;
+                    }
+                }
+            };
             if (!IRREG) {
-                RegularRows<P, float> h;
+                RegularRows2<P> h;
                 h.init(x, y, z);
 #pragma unroll
                 for (int n = 0; n <= P; ++n) {
                     h.step(n);
-#pragma unroll
-                    for (int mm = 0; mm <= n; ++mm) {
-                        w[slot(n, mm)] += q * h.cre[mm];
-                        if (mm) w[slot(n, -mm)] -= q * h.cim[mm];
-                    }
+                    scatter(n, h.c);
                 }
             } else {
-                IrregularRows<P, float> h;
+                IrregularRows2<P> h;
                 h.init(x, y, z, rsqrtf(x * x + y * y + z * z));
 #pragma unroll
                 for (int n = 0; n <= P; ++n) {
                     h.step(n);
-#pragma unroll
-                    for (int mm = 0; mm <= n; ++mm) {
-                        w[slot(n, mm)] += q * h.cre[mm];
-                        if (mm) w[slot(n, -mm)] -= q * h.cim[mm];
-                    }
+                    scatter(n, h.c);
                 }
             }
         }
@@ -823,16 +831,20 @@ __global__ void __launch_bounds__(128) leaf_far_kernel(DevPlan plan, int64_t lea
 // ---------------------------------------------------------------------------------
 // L2P + M2P of the potentials for several charge vectors (f32, m > 1): the harmonics of a
 // target are formed once per W entry (and once for L2P) and dotted with VB vectors'
-// expansions, which are consecutive rows of ms_of(P) floats.  Per vector the sums are
-// those of l2p_eval / m2p_eval and leaf_far_kernel<P, float, false>, in the same order.
+// expansions, which are consecutive rows of ms_of(P) floats.  Per vector the terms are
+// those of l2p_eval / m2p_eval, with the harmonic rows on the packed f32x2 pipe and each
+// order mu > 0 one packed fused multiply-add (real and imaginary products summed apart).
 template <int P, int VB>
 __device__ __forceinline__ void l2p_eval_mv(const float* L, int nb, float x, float y, float z, float (&f)[VB]) {
     constexpr int MS = ms_of(P);
-    RegularRows<P, float> h;
+    RegularRows2<P> h;  // the rows on the packed pipe (leaf_far_x2.cuh)
     h.init(x, y, z);
-    float f1[VB];  // the orders mu > 0, weighted 2 at the end (as l2p_eval)
+    float2 f1[VB];  // the orders mu > 0, real and imaginary products apart, weighted 2 at the end
 #pragma unroll
-    for (int b = 0; b < VB; ++b) f[b] = f1[b] = 0.0f;
+    for (int b = 0; b < VB; ++b) {
+        f[b] = 0.0f;
+        f1[b] = make_float2(0.0f, 0.0f);
+    }
 #pragma unroll
     for (int k = 0; k <= P; ++k) {
         h.step(k);
@@ -842,28 +854,29 @@ __device__ __forceinline__ void l2p_eval_mv(const float* L, int nb, float x, flo
             for (int b = 0; b < VB; ++b)
                 if (b < nb) {
                     const Cx<float> c = coef_at(L + b * MS, k, mu);
-                    if (mu == 0) {
-                        f[b] += c.re * h.cre[0];
-                    } else {
-                        f1[b] += c.re * h.cre[mu];
-                        f1[b] -= c.im * h.cim[mu];
-                    }
+                    if (mu == 0)
+                        f[b] = fmaf(c.re, h.c[0].x, f[b]);
+                    else
+                        f1[b] = __ffma2_rn(make_float2(c.re, c.im), h.c[mu], f1[b]);
                 }
         }
     }
 #pragma unroll
-    for (int b = 0; b < VB; ++b) f[b] += 2.0f * f1[b];
+    for (int b = 0; b < VB; ++b) f[b] += 2.0f * (f1[b].x - f1[b].y);
 }
 
 template <int P, int VB>
 __device__ __forceinline__ void m2p_eval_mv(const float* M, int nb, float x, float y, float z, float (&f)[VB]) {
     constexpr int MS = ms_of(P);
-    IrregularRows<P, float> h;
+    IrregularRows2<P> h;
     const float r2 = x * x + y * y + z * z;
     h.init(x, y, z, 1.0f / sqrt(r2));
-    float f1[VB];  // the orders mu > 0, weighted 2 at the end (as l2p_eval)
+    float2 f1[VB];
 #pragma unroll
-    for (int b = 0; b < VB; ++b) f[b] = f1[b] = 0.0f;
+    for (int b = 0; b < VB; ++b) {
+        f[b] = 0.0f;
+        f1[b] = make_float2(0.0f, 0.0f);
+    }
 #pragma unroll
     for (int k = 0; k <= P; ++k) {
         h.step(k);
@@ -873,17 +886,15 @@ __device__ __forceinline__ void m2p_eval_mv(const float* M, int nb, float x, flo
             for (int b = 0; b < VB; ++b)
                 if (b < nb) {
                     const Cx<float> c = coef_at(M + b * MS, k, mu);
-                    if (mu == 0) {
-                        f[b] += c.re * h.cre[0];
-                    } else {
-                        f1[b] += c.re * h.cre[mu];
-                        f1[b] -= c.im * h.cim[mu];
-                    }
+                    if (mu == 0)
+                        f[b] = fmaf(c.re, h.c[0].x, f[b]);
+                    else
+                        f1[b] = __ffma2_rn(make_float2(c.re, c.im), h.c[mu], f1[b]);
                 }
         }
     }
 #pragma unroll
-    for (int b = 0; b < VB; ++b) f[b] += 2.0f * f1[b];
+    for (int b = 0; b < VB; ++b) f[b] += 2.0f * (f1[b].x - f1[b].y);
 }
 
 // ---------------------------------------------------------------------------------

@@ -28,6 +28,90 @@ namespace fmmb {
 
 __device__ __forceinline__ float2 x2(float a) { return make_float2(a, a); }
 
+// The row recursions of RegularRows / IrregularRows (harmonics.cuh) in f32 with both parts
+// of a harmonic in one packed instruction and the recursion's constants folded at compile
+// time (a multiplication by 1 / ((n + m)(n - m)), no division): step(n) forms row n into
+// c (m = 0..n), keeping rows n - 1 (pr) and n - 2 (pp); rows in order n = 0, 1, 2, ...
+template <int PMAX>
+struct RegularRows2 {
+    float x, y, z;
+    float2 nr2;
+    float2 pp[PMAX + 2], pr[PMAX + 2], c[PMAX + 2];  // one spare slot
+    __device__ __forceinline__ void init(float x_, float y_, float z_) {
+        x = x_;
+        y = y_;
+        z = z_;
+        nr2 = x2(-(x * x + y * y + z * z));
+    }
+    __device__ __forceinline__ void step(int n) {
+#pragma unroll
+        for (int m = 0; m < n; ++m) {
+            pp[m] = pr[m];
+            pr[m] = c[m];
+        }
+        if (n == 0) {
+            c[0] = make_float2(1.0f, 0.0f);
+            return;
+        }
+        const float2 zn = x2((float)(2 * n - 1) * z);
+#pragma unroll
+        for (int m = 0; m <= n; ++m) {
+            if (m + 2 <= n) {
+                // R_n^m = ((2n - 1) z R_{n-1}^m - r^2 R_{n-2}^m) / ((n + m)(n - m))
+                const float inv_den = 1.0f / (float)((n + m) * (n - m));
+                c[m] = __fmul2_rn(x2(inv_den), __ffma2_rn(zn, pr[m], __fmul2_rn(nr2, pp[m])));
+            } else if (m + 1 == n) {
+                c[m] = __fmul2_rn(x2(z), pr[m]);
+            } else {
+                const float sc = 1.0f / (float)(2 * n);
+                const float a = pr[n - 1].x, b = pr[n - 1].y;
+                c[m] = make_float2((x * a - y * b) * sc, (x * b + y * a) * sc);
+            }
+        }
+    }
+};
+
+template <int PMAX>
+struct IrregularRows2 {
+    float x, y, z, inv_r, inv_r2;
+    float2 ir2;
+    float2 pp[PMAX + 2], pr[PMAX + 2], c[PMAX + 2];
+    __device__ __forceinline__ void init(float x_, float y_, float z_, float inv_r_) {
+        x = x_;
+        y = y_;
+        z = z_;
+        inv_r = inv_r_;
+        inv_r2 = inv_r * inv_r;
+        ir2 = x2(inv_r2);
+    }
+    __device__ __forceinline__ void step(int n) {
+#pragma unroll
+        for (int m = 0; m < n; ++m) {
+            pp[m] = pr[m];
+            pr[m] = c[m];
+        }
+        if (n == 0) {
+            c[0] = make_float2(inv_r, 0.0f);
+            return;
+        }
+        // I_n^m = ((2n - 1) z I_{n-1}^m - (n - 1 - m)(n - 1 + m) I_{n-2}^m) / r^2
+        const float2 zn = x2((float)(2 * n - 1) * z);
+#pragma unroll
+        for (int m = 0; m <= n; ++m) {
+            if (m + 2 <= n) {
+                const float2 k2 = x2(-(float)((n - 1 - m) * (n - 1 + m)));
+                c[m] = __fmul2_rn(ir2, __ffma2_rn(zn, pr[m], __fmul2_rn(k2, pp[m])));
+            } else if (m + 1 == n) {
+                c[m] = __fmul2_rn(ir2, __fmul2_rn(zn, pr[m]));
+            } else {
+                const float sc = (float)(2 * n - 1) * inv_r2;
+                const float a = pr[n - 1].x, b = pr[n - 1].y;
+                c[m] = make_float2((x * a - y * b) * sc, (x * b + y * a) * sc);
+            }
+        }
+    }
+};
+
 // The sums of one evaluation; the orders mu > 0 weighted 2 at the end.
 struct LadderSums {
     float f0 = 0.0f, d0 = 0.0f, gxs = 0.0f, gys = 0.0f;  // mu = 0 (b = 0, H and W real)
@@ -78,57 +162,34 @@ struct LadderSums {
 template <int P>
 __device__ __forceinline__ void l2p_x2(const float* __restrict__ L, float x, float y, float z, float& phi,
                                        float& gx, float& gy, float& gz) {
-    const float2 nr2 = x2(-(x * x + y * y + z * z));
     const float2 zero = make_float2(0.0f, 0.0f);
-    float2 pp[P + 2], pr[P + 2], c[P + 2];  // rows n - 2, n - 1, n (one spare slot)
+    RegularRows2<P> h;
+    h.init(x, y, z);
     LadderSums s;
 #pragma unroll
     for (int n = 0; n <= P; ++n) {
-#pragma unroll
-        for (int m = 0; m < n; ++m) {
-            pp[m] = pr[m];
-            pr[m] = c[m];
-        }
-        if (n == 0) {
-            c[0] = make_float2(1.0f, 0.0f);
-        } else {
-            const float2 zn = x2((float)(2 * n - 1) * z);
-#pragma unroll
-            for (int m = 0; m <= n; ++m) {
-                if (m + 2 <= n) {
-                    // R_n^m = ((2n - 1) z R_{n-1}^m - r^2 R_{n-2}^m) / ((n + m)(n - m))
-                    const float inv_den = 1.0f / (float)((n + m) * (n - m));
-                    c[m] = __fmul2_rn(x2(inv_den), __ffma2_rn(zn, pr[m], __fmul2_rn(nr2, pp[m])));
-                } else if (m + 1 == n) {
-                    c[m] = __fmul2_rn(x2(z), pr[m]);
-                } else {
-                    const float sc = 1.0f / (float)(2 * n);
-                    const float a = pr[n - 1].x, b = pr[n - 1].y;
-                    c[m] = make_float2((x * a - y * b) * sc, (x * b + y * a) * sc);
-                }
-            }
-        }
+        h.step(n);
         // the coefficients of degree n: H = R_n^mu, W = R_{n-1}^mu, U = R_{n-1}^{mu-1},
         // V = R_{n-1}^{mu+1}
 #pragma unroll
         for (int mu = 0; mu <= n; ++mu) {
             const float a = L[slot(n, mu)], b = mu ? L[slot(n, -mu)] : 0.0f;
-            const float2 W = mu <= n - 1 ? pr[mu] : zero;
-            const float2 U = mu >= 1 ? pr[mu >= 1 ? mu - 1 : 0] : zero;
-            const float2 V = mu + 1 <= n - 1 ? pr[mu + 1] : zero;
+            const float2 W = mu <= n - 1 ? h.pr[mu] : zero;
+            const float2 U = mu >= 1 ? h.pr[mu >= 1 ? mu - 1 : 0] : zero;
+            const float2 V = mu + 1 <= n - 1 ? h.pr[mu + 1] : zero;
             if (mu == 0) {
                 if (n >= 2)
-                    s.add<true, true, false, true>(a, b, c[0], W, U, V);
+                    s.add<true, true, false, true>(a, b, h.c[0], W, U, V);
                 else if (n == 1)
-                    s.add<true, true, false, false>(a, b, c[0], W, U, V);
+                    s.add<true, true, false, false>(a, b, h.c[0], W, U, V);
                 else
-                    s.add<true, false, false, false>(a, b, c[0], W, U, V);
+                    s.add<true, false, false, false>(a, b, h.c[0], W, U, V);
             } else if (mu + 1 <= n - 1) {
-                s.add<false, true, true, true>(a, b, c[mu], W, U, V);
+                s.add<false, true, true, true>(a, b, h.c[mu], W, U, V);
             } else if (mu <= n - 1) {
-                s.add<false, true, true, false>(a, b, c[mu], W, U, V);
+                s.add<false, true, true, false>(a, b, h.c[mu], W, U, V);
             } else {
-                s.add<false, false, true, false>(a, b, c[mu], W, U, V);
+                s.add<false, false, true, false>(a, b, h.c[mu], W, U, V);
             }
         }
     }
@@ -140,38 +201,14 @@ template <int P>
 __device__ __forceinline__ void m2p_x2(const float* __restrict__ M, float x, float y, float z, float& phi,
                                        float& gx, float& gy, float& gz) {
     constexpr int K = P + 1;
-    const float inv_r = 1.0f / sqrtf(x * x + y * y + z * z);
-    const float inv_r2 = inv_r * inv_r;
-    const float2 ir2 = x2(inv_r2);
     const float2 zero = make_float2(0.0f, 0.0f);
-    float2 pp[K + 2], pr[K + 2], c[K + 2];
+    IrregularRows2<K> h;
+    h.init(x, y, z, 1.0f / sqrtf(x * x + y * y + z * z));
     LadderSums s;
 #pragma unroll
     for (int n = 0; n <= K; ++n) {
-#pragma unroll
-        for (int m = 0; m < n; ++m) {
-            pp[m] = pr[m];
-            pr[m] = c[m];
-        }
-        if (n == 0) {
-            c[0] = make_float2(inv_r, 0.0f);
-            continue;
-        }
-        // I_n^m = ((2n - 1) z I_{n-1}^m - (n - 1 - m)(n - 1 + m) I_{n-2}^m) / r^2
-        const float2 zn = x2((float)(2 * n - 1) * z);
-#pragma unroll
-        for (int m = 0; m <= n; ++m) {
-            if (m + 2 <= n) {
-                const float2 k2 = x2(-(float)((n - 1 - m) * (n - 1 + m)));
-                c[m] = __fmul2_rn(ir2, __ffma2_rn(zn, pr[m], __fmul2_rn(k2, pp[m])));
-            } else if (m + 1 == n) {
-                c[m] = __fmul2_rn(ir2, __fmul2_rn(zn, pr[m]));
-            } else {
-                const float sc = (float)(2 * n - 1) * inv_r2;
-                const float a = pr[n - 1].x, b = pr[n - 1].y;
-                c[m] = make_float2((x * a - y * b) * sc, (x * b + y * a) * sc);
-            }
-        }
+        h.step(n);
+        if (n == 0) continue;
         // the coefficients of degree d = n - 1: H = I_d^mu, W = I_n^mu, U = I_n^{mu-1},
         // V = I_n^{mu+1}
         const int d = n - 1;
@@ -179,9 +216,9 @@ __device__ __forceinline__ void m2p_x2(const float* __restrict__ M, float x, flo
         for (int mu = 0; mu <= d; ++mu) {
             const float a = M[slot(d, mu)], b = mu ? M[slot(d, -mu)] : 0.0f;
             if (mu == 0)
-                s.add<true, true, false, true>(a, b, pr[0], c[0], zero, c[1]);
+                s.add<true, true, false, true>(a, b, h.pr[0], h.c[0], zero, h.c[1]);
             else
-                s.add<false, true, true, true>(a, b, pr[mu], c[mu], c[mu - 1], c[mu + 1]);
+                s.add<false, true, true, true>(a, b, h.pr[mu], h.c[mu], h.c[mu - 1], h.c[mu + 1]);
         }
     }
     s.finish(-1.0f, phi, gx, gy, gz);
