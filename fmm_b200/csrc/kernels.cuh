@@ -147,7 +147,19 @@ __global__ void __launch_bounds__(32) expand_kernel(DevPlan plan, int64_t row_be
                 z = (p4.z - fc[2]) * finv;
             }
             for (int v = 0; v < m; ++v) Q[v * 32 + lane] = valid ? sq[(int64_t)v * plan.nsrc + si] : T(0);
-            if (!IRREG) {
+            if constexpr (!IRREG && sizeof(T) == 4) {  // f32: the rows on the packed pipe (leaf_far_x2.cuh)
+                RegularRows2<P> h;
+                h.init((float)x, (float)y, (float)z);
+#pragma unroll
+                for (int n = 0; n <= P; ++n) {
+                    h.step(n);
+#pragma unroll
+                    for (int mm = 0; mm <= n; ++mm) {
+                        S[slot(n, mm) * 32 + lane] = valid ? (T)h.c[mm].x : T(0);
+                        if (mm) S[slot(n, -mm) * 32 + lane] = valid ? (T)-h.c[mm].y : T(0);
+                    }
+                }
+            } else if (!IRREG) {
                 RegularRows<P, T> h;
                 h.init(x, y, z);
 #pragma unroll
@@ -599,17 +611,46 @@ __global__ void __launch_bounds__(256) m2l_gemm_kernel(const int32_t* __restrict
             }
             asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
             __syncthreads();
+            if constexpr (sizeof(T) == 4) {
+                // f32: two pairs' sums of one slot in one packed fused multiply-add (the
+                // same fma a sum as the scalar loop below)
+                float2 acc2[2][JN];
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < JN; ++j) acc2[i][j] = make_float2(acc[2 * i][j], acc[2 * i + 1][j]);
 #pragma unroll 3
-            for (int k = 0; k < kc; ++k) {
-                T xv[4], av[JN];
+                for (int k = 0; k < kc; ++k) {
+                    const float4 xv = *reinterpret_cast<const float4*>(Xs + k * kGemmPairs + ty * 4);
+                    float av[JN];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) xv[i] = Xs[k * kGemmPairs + ty * 4 + i];
+                    for (int j = 0; j < JN; ++j) av[j] = At[k * NCP + tx + 16 * j];
 #pragma unroll
-                for (int j = 0; j < JN; ++j) av[j] = At[k * NCP + tx + 16 * j];
+                    for (int j = 0; j < JN; ++j) {
+                        acc2[0][j] = __ffma2_rn(make_float2(av[j], av[j]), make_float2(xv.x, xv.y), acc2[0][j]);
+                        acc2[1][j] = __ffma2_rn(make_float2(av[j], av[j]), make_float2(xv.z, xv.w), acc2[1][j]);
+                    }
+                }
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 2; ++i)
 #pragma unroll
-                    for (int j = 0; j < JN; ++j) acc[i][j] += av[j] * xv[i];
+                    for (int j = 0; j < JN; ++j) {
+                        acc[2 * i][j] = acc2[i][j].x;
+                        acc[2 * i + 1][j] = acc2[i][j].y;
+                    }
+            } else {
+#pragma unroll 3
+                for (int k = 0; k < kc; ++k) {
+                    T xv[4], av[JN];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) xv[i] = Xs[k * kGemmPairs + ty * 4 + i];
+#pragma unroll
+                    for (int j = 0; j < JN; ++j) av[j] = At[k * NCP + tx + 16 * j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < JN; ++j) acc[i][j] += av[j] * xv[i];
+                }
             }
         }
 #pragma unroll
