@@ -116,7 +116,7 @@ struct Evaluator final : EvaluatorBase {
     DevBuf st_rowpair, st_xy, st_zz, st_idx;
     // the near-singular pairs' weights (per pair) and, per evaluation, their f64 sums per
     // target and vector (close_weights_kernel, close_sum_kernel)
-    DevBuf close_w, close_acc;
+    DevBuf close_w, close_acc, close_src32;
     // boxes with a nonempty X list, level by level (the P2L launches), the f32 P2L's
     // per-entry records (XRec), and the X-list sums of the f32 P2L when it runs apart (Lx,
     // a box's rows as in Lc): in the evaluation with the near-singular sums on near_stream,
@@ -874,19 +874,23 @@ struct Evaluator final : EvaluatorBase {
         if (plan.nleaves()) close_map_kernel<<<(unsigned)plan.nleaves(), 64>>>(dp, close, close_y.as<double4>());
         CUDA_TRY(cudaGetLastError());
         close.q = sq64.as<double>();
-        const size_t wd = gradients ? 4 : 1;  // doubles a pair / a target and vector
-        close_w.alloc(sizeof(double) * wd * (size_t)(nclose + 1));
+        const size_t wd = gradients ? 4 : 1;  // floats a pair, doubles a target and vector
+        close_w.alloc(sizeof(float) * wd * (size_t)(nclose + 1));
         close_acc.alloc(sizeof(double) * wd * (size_t)m * (dp.ntgt + 1));
+        close_src32.alloc(sizeof(uint32_t) * (size_t)(nclose + 1));
+        if (nclose)
+            close_src32_kernel<<<(unsigned)((nclose + 255) / 256), 256>>>(close_src.as<int64_t>(), nclose,
+                                                                          close_src32.as<uint32_t>());
         close.acc = nclose ? close_acc.as<double>() : nullptr;  // no pairs: nothing to add
         if (plan.nleaves() && nclose) {
             const auto* s32 = reinterpret_cast<const float4*>(spos.ptr);
             const auto* t32 = reinterpret_cast<const float4*>(tpos.ptr);
             if (gradients)
                 close_weights_kernel<true><<<(unsigned)plan.nleaves(), 64>>>(dp, close, s32, t32, kRmax,
-                                                                             close_w.as<double>());
+                                                                             close_w.as<float>());
             else
                 close_weights_kernel<false><<<(unsigned)plan.nleaves(), 64>>>(dp, close, s32, t32, kRmax,
-                                                                              close_w.as<double>());
+                                                                              close_w.as<float>());
         }
         CUDA_TRY(cudaGetLastError());
     }
@@ -896,10 +900,12 @@ struct Evaluator final : EvaluatorBase {
         if (!kMixed || !nclose || !dp.ntgt) return;
         const unsigned g = (unsigned)((dp.ntgt + 255) / 256);
         if (gradients)
-            close_sum_kernel<true><<<counted(g), 256, 0, s>>>(close, close_w.as<double>(), m, dp.nsrc, dp.ntgt,
+            close_sum_kernel<true><<<counted(g), 256, 0, s>>>(close, close_w.as<float>(), close_src32.as<uint32_t>(),
+                                                             m, dp.nsrc, dp.ntgt,
                                                              close_acc.as<double>());
         else
-            close_sum_kernel<false><<<counted(g), 256, 0, s>>>(close, close_w.as<double>(), m, dp.nsrc, dp.ntgt,
+            close_sum_kernel<false><<<counted(g), 256, 0, s>>>(close, close_w.as<float>(), close_src32.as<uint32_t>(),
+                                                              m, dp.nsrc, dp.ntgt,
                                                               close_acc.as<double>());
     }
 
@@ -925,7 +931,7 @@ struct Evaluator final : EvaluatorBase {
                                &near_phi, &near_g, &box_side, &v_pos, &xbox, &xrec, &Lx, &fu_tile_d, &fu_tile_begin,
                                &fu_tile_np, &fu_cta, &fu_pair_src, &fu_pair_tgt, &fu_img, &ck_tc_d, &ck_tc_begin,
                                &ck_tc_count, &ck_s_d, &ck_s_begin, &ck_s_count, &ck_pair_src, &st_rowpair,
-                               &st_xy, &st_zz, &st_idx, &close_w, &close_acc};
+                               &st_xy, &st_zz, &st_idx, &close_w, &close_acc, &close_src32};
         size_t s = 0;
         for (auto* b : all) s += b->bytes;
         return s;

@@ -65,11 +65,15 @@ static __global__ void near_record_kernel(DevPlan plan, int64_t nleaves, NearRec
 // target's near-singular pairs in CSR order (close_sum_kernel, q the f64 charges) and the
 // P2P epilogue adds it once, after the f32 partials.  The clamp terms carry the f32
 // charge and the weights the f64 one: the difference is 4 |q32 - q64| <= 2^-22 |q| a pair.
+// A weight is formed in f64 and stored rounded to f32 (relative 2^-24 of that pair's
+// term; in range for any two distinct f64 points, whose leaf-unit distance is far above
+// the 1e-19 where 1/r^2 would leave f32), and the sums stay f64: the sparse operator reads
+// 20 bytes a pair (weights and a 32-bit source index) where f64 weights took 40.
 
-// Build time: block per leaf, thread per target; w is 4 doubles a pair (GRAD) or 1.
+// Build time: block per leaf, thread per target; w is 4 floats a pair (GRAD) or 1.
 template <bool GRAD>
 __global__ void close_weights_kernel(DevPlan plan, ClosePairs close, const float4* __restrict__ spos32,
-                                     const float4* __restrict__ tpos32, float rmax, double* __restrict__ w) {
+                                     const float4* __restrict__ tpos32, float rmax, float* __restrict__ w) {
     const int64_t leaf = blockIdx.x;
     const int box = plan.leaf_box[leaf];
     const double R = rmax, R3 = (double)rmax * rmax * rmax;
@@ -94,18 +98,26 @@ __global__ void close_weights_kernel(DevPlan plan, ClosePairs close, const float
             }
             const double r3 = rinv * rinv * rinv;
             if (GRAD)
-                reinterpret_cast<double4*>(w)[c2] =
-                    make_double4(rinv - R, r3 * dx - R3 * d32x, r3 * dy - R3 * d32y, r3 * dz - R3 * d32z);
+                reinterpret_cast<float4*>(w)[c2] =
+                    make_float4(__double2float_rn(rinv - R), __double2float_rn(r3 * dx - R3 * d32x),
+                                __double2float_rn(r3 * dy - R3 * d32y), __double2float_rn(r3 * dz - R3 * d32z));
             else
-                w[c2] = rinv - R;
+                w[c2] = __double2float_rn(rinv - R);
         }
     }
 }
 
+// Build time: each pair's source index as 32 bits.
+static __global__ void close_src32_kernel(const int64_t* __restrict__ src, int64_t n, uint32_t* __restrict__ src32) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) src32[i] = (uint32_t)src[i];
+}
+
 // Evaluation: thread per target, every vector of the pass; acc [vector][target].
+// src32: each pair's source as 32 bits (the plan has fewer than 2^32 sources).
 template <bool GRAD>
-__global__ void close_sum_kernel(ClosePairs close, const double* __restrict__ w, int m, int64_t nsrc, int64_t nt,
-                                 double* __restrict__ acc) {
+__global__ void close_sum_kernel(ClosePairs close, const float* __restrict__ w, const uint32_t* __restrict__ src32,
+                                 int m, int64_t nsrc, int64_t nt, double* __restrict__ acc) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= nt) return;
     const int64_t c0 = close.row[t], c1 = close.row[t + 1];
@@ -114,15 +126,15 @@ __global__ void close_sum_kernel(ClosePairs close, const double* __restrict__ w,
         double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll 4
         for (int64_t c = c0; c < c1; ++c) {
-            const double q = qv[close.src[c]];
+            const double q = qv[src32[c]];
             if (GRAD) {
-                const double4 wc = reinterpret_cast<const double4*>(w)[c];
-                a0 = __fma_rn(q, wc.x, a0);
-                a1 = __fma_rn(q, wc.y, a1);
-                a2 = __fma_rn(q, wc.z, a2);
-                a3 = __fma_rn(q, wc.w, a3);
+                const float4 wc = reinterpret_cast<const float4*>(w)[c];
+                a0 = __fma_rn(q, (double)wc.x, a0);
+                a1 = __fma_rn(q, (double)wc.y, a1);
+                a2 = __fma_rn(q, (double)wc.z, a2);
+                a3 = __fma_rn(q, (double)wc.w, a3);
             } else {
-                a0 = __fma_rn(q, w[c], a0);
+                a0 = __fma_rn(q, (double)w[c], a0);
             }
         }
         if (GRAD)
