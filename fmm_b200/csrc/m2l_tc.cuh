@@ -543,12 +543,14 @@ __global__ void __launch_bounds__(32 * kTcWarps, 1) m2l_tc_kernel(const int32_t*
     }
 }
 
-// the autotuner's alternative tile of the real M2L: 64 columns where the default has 96 or
-// 128, 32 where it has 64 or 48 (more raw stages in the shared memory freed)
+// the autotuner's alternative tile of the real M2L: 80 columns where the default has 96
+// (p = 8: three raw stages instead of two), 64 where it has 128, 32 where it has 64 or 48
+// (more raw stages in the shared memory freed)
 template <int P>
 constexpr int tc_alt_columns() {
-    return TcTs<P>::NT >= 96 ? 64 : 32;
+    return TcTs<P>::NT == 96 ? 80 : TcTs<P>::NT >= 96 ? 64 : 32;
 }
+static_assert(TcTs<8, false, 80>::RS == 3, "p = 8's alternative tile holds three raw stages");
 
 // columns (pairs x vectors) of a tensor-core M2L tile at degree p (0 to 12)
 inline int tc_tile_columns(int p) {

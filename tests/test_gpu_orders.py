@@ -45,3 +45,17 @@ def test_order_outside_the_compiled_range_is_refused(points):
     with pytest.raises(F.FmmError) as e:
         F.FmmBuilder(13).build(x[:100])
     assert e.value.status == 2  # FMMGPU_UNSUPPORTED
+
+
+def test_p8_alternative_tile_same_bits(oracle):
+    """p = 8's alternative tensor-core M2L tile (80 columns, three raw stages, where the
+    default has 96 and two) gives the default tile's bits."""
+    x, q = oracle.point_sets("sphere", 20000, 29)
+    fmm = F.FmmBuilder(8).gradients().max_points_per_leaf(32).precision("mixed").build(x)
+    assert fmm.info()["m2l_tile_columns"] == 96
+    out = fmm.evaluate(q)
+    fmm.set_m2l_tile(1)
+    assert fmm.info()["m2l_tile_columns"] == 80
+    alt = fmm.evaluate(q)
+    assert np.array_equal(alt.potential, out.potential) and np.array_equal(alt.gradient, out.gradient)
+    fmm.close()
