@@ -88,6 +88,7 @@ struct fmmgpu_fmm {
     int64_t vjp_forward_reused = 0;
     DevBuf d_hq, d_hphi, d_hg;  // the Helmholtz host call's device buffers
     DevBuf d_q32, d_out32;      // the f32 host call's charges and (potential, gradient) in f32
+    int* h_status = nullptr;    // pinned: the device status word, copied on the stream by the host calls
     int64_t tables_loaded = 0;  // tables taken from the table cache (bits: M2L, M2M, L2L)
     std::string table_cache_dir, tuning_cache_dir;  // the settings' cache directories ("" none)
     bool uploaded = false;         // the plan came from the caller (fmmgpu_upload_plan)
@@ -118,6 +119,12 @@ __global__ void narrow_kernel(int64_t n, const double* __restrict__ a, float* __
         b[i] = __double2float_rn(a[i]);
 }
 static unsigned grid_of(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+// potentials [0, np) then gradients [np, np + ng) rounded to f32 in one launch
+__global__ void narrow2_kernel(int64_t np, int64_t ng, const double* __restrict__ a, const double* __restrict__ g,
+                               float* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np + ng; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = __double2float_rn(i < np ? a[i] : g[i - np]);
+}
 
 // ---- vector-Jacobian products of phi(q, sources, targets) for a cotangent w on phi ----
 // dx_t[i] = sum_v w[v][i] grad phi_v(t_i)   (w, phi in the output layout [v][nt])
@@ -681,6 +688,18 @@ int fmmgpu_fmm_evaluate_device(fmmgpu_fmm* f, const double* charges, double* pot
     });
 }
 
+// The end of a host call: the device status word is copied on the evaluator's stream
+// into a pinned word, then one synchronisation covers the copies and the check.
+static void finish_host_call(fmmgpu_fmm* f) {
+    const int* w = f->eval->device_status_word();
+    if (w) {
+        if (!f->h_status) CUDA_TRY(cudaMallocHost(&f->h_status, sizeof(int)));
+        CUDA_TRY(cudaMemcpyAsync(f->h_status, w, sizeof(int), cudaMemcpyDeviceToHost, f->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(f->stream));
+    if (w && *f->h_status) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+}
+
 int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential, double* gradient) {
     return guarded([&] {
         if (!f || !charges || !potential || (f->settings.gradients && !gradient))
@@ -697,8 +716,7 @@ int fmmgpu_fmm_evaluate(fmmgpu_fmm* f, const double* charges, double* potential,
         if (f->settings.gradients)
             CUDA_TRY(cudaMemcpyAsync(gradient, f->d_grad.ptr, sizeof(double) * 3 * m * nt, cudaMemcpyDeviceToHost,
                                      f->stream));
-        CUDA_TRY(cudaStreamSynchronize(f->stream));
-        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+        finish_host_call(f);
     });
 }
 
@@ -722,19 +740,16 @@ int fmmgpu_fmm_evaluate_f32(fmmgpu_fmm* f, const float* charges, float* potentia
         run_evaluation(f, f->d_charges.as<double>(), f->d_phi.as<double>(),
                        f->settings.gradients ? f->d_grad.as<double>() : nullptr);
         keep_forward(f, f->d_charges.as<double>(), f->settings.gradients ? f->d_grad.as<double>() : nullptr);
-        const int64_t np = m * nt;
+        const int64_t np = m * nt, ng = f->settings.gradients ? 3 * np : 0;
         if (np) {
             float* o = f->d_out32.as<float>();
-            narrow_kernel<<<grid_of(np), 256, 0, s>>>(np, f->d_phi.as<double>(), o);
-            if (f->settings.gradients)
-                narrow_kernel<<<grid_of(3 * np), 256, 0, s>>>(3 * np, f->d_grad.as<double>(), o + np);
+            narrow2_kernel<<<grid_of(np + ng), 256, 0, s>>>(np, ng, f->d_phi.as<double>(),
+                                                            ng ? f->d_grad.as<double>() : nullptr, o);
             CUDA_TRY(cudaGetLastError());
             CUDA_TRY(cudaMemcpyAsync(potential, o, sizeof(float) * np, cudaMemcpyDeviceToHost, s));
-            if (f->settings.gradients)
-                CUDA_TRY(cudaMemcpyAsync(gradient, o + np, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost, s));
+            if (ng) CUDA_TRY(cudaMemcpyAsync(gradient, o + np, sizeof(float) * ng, cudaMemcpyDeviceToHost, s));
         }
-        CUDA_TRY(cudaStreamSynchronize(s));
-        if (f->eval->device_status()) throw Failure(FMMGPU_DEVICE_ERROR, "a tensor-core wait timed out");
+        finish_host_call(f);
     });
 }
 
@@ -1211,6 +1226,7 @@ void fmmgpu_fmm_destroy(fmmgpu_fmm* f) {
     f->d_charges.alloc(0);
     f->d_phi.alloc(0);
     f->d_grad.alloc(0);
+    if (f->h_status) cudaFreeHost(f->h_status);
     if (f->stream) cudaStreamDestroy(f->stream);
     delete f;
 }

@@ -119,6 +119,9 @@ struct EvaluatorBase {
     // 2 tensor cores fused with the local reduce (an option), 0 SIMT products then the reduce
     int m2l_path = 0;
     virtual int device_status() { return 0; }
+    // the device word device_status() reads (nullptr: none), for a copy queued on the
+    // evaluator's stream instead of a synchronous read after it
+    virtual const int* device_status_word() const { return nullptr; }
     int64_t close_pairs = 0;  // near-singular pairs the mixed form evaluates in f64
     int kinds = 3;  // bit 0 near field (P2P), bit 1 far field; a test hook, 3 in use
     int64_t launches = 0;  // kernels launched by the last evaluation

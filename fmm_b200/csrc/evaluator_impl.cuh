@@ -909,6 +909,11 @@ struct Evaluator final : EvaluatorBase {
                                                               close_acc.as<double>());
     }
 
+    const int* device_status_word() const override {
+        if constexpr (kTensor) return tc_error.as<int>();
+        return nullptr;
+    }
+
     int device_status() override {
         if constexpr (kTensor) {
             int err = 0;
