@@ -798,6 +798,10 @@ struct Evaluator final : EvaluatorBase {
             int64_t t = plan.tgt_start[j];
             const int64_t t1 = plan.tgt_start[j + 1];
             for (; t + 32 <= t1; t += 32) add(0, j, t, 32 | 32 << 8);
+            // a remainder of 25 to 31 targets as one item of 32 slots (a lane a target, the
+            // rest idle): cheaper than the three partial items it would split into, each of
+            // which reads the near row and pays an item's fixed cost
+            if (t1 - t >= 25) add(0, j, t, (int)(t1 - t) | 32 << 8), t = t1;
             if (t + 16 <= t1) add(1, j, t, 16 | 16 << 8), t += 16;
             if (t + 8 <= t1) add(2, j, t, 8 | 8 << 8), t += 8;
             const int r = (int)(t1 - t);  // 0 to 7 left
