@@ -82,3 +82,51 @@ def test_two_ranks_gloo():
         nsrc, ncl, slowest, local = out[r]
         assert nsrc == total and ncl == 5 and slowest == 2.0
     assert out[0][3] + out[1][3] == total and out[0][3] > 0 and out[1][3] > 0
+
+
+def _failing_rank_main(rank, world, port, out):
+    """The batched leg's error path: a rank whose build fails still takes the collective,
+    with an infinite time, so that every rank sees the failure and none waits forever."""
+    import math
+
+    import torch.distributed as dist
+
+    import fmm_b200 as F
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(5)
+        cloud = rng.uniform(-1, 1, (800, 3))
+        if rank == 1:
+            cloud[17, 2] = np.nan  # this rank's build fails on the host
+        try:
+            F.FmmBuilder(3).max_points_per_leaf(32).plan_batch([cloud])
+            t, err = 1.0, ""
+        except F.FmmError as e:
+            t, err = math.inf, str(e)
+        slowest = max_over_ranks(t)
+        out[rank] = (slowest, err)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failed_rank_is_seen_by_every_rank():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    assert out[0] == (float("inf"), "")
+    assert out[1][0] == float("inf") and "non-finite" in out[1][1]
