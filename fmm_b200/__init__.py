@@ -393,10 +393,14 @@ class Plan:
         return keys, leaf
 
     def list(self, kind, row):
-        out = np.zeros(4096, dtype=np.uint64)
+        """One row of a list (kind 0 near, 1 V, 2 W, 3 X) as box keys."""
+        out = np.zeros(64, dtype=np.uint64)  # near rows fit; longer V rows take the second call
         n = lib().fmmgpu_fmm_list(self._h, kind, row, _ptr(out), len(out))
         if n < 0:
             raise IndexError(row)
+        if n > len(out):  # the call returns the row's full length: fetch it whole
+            out = np.zeros(n, dtype=np.uint64)
+            lib().fmmgpu_fmm_list(self._h, kind, row, _ptr(out), len(out))
         return out[:n].copy()
 
     def plan_arrays(self):
