@@ -376,7 +376,12 @@ class Plan:
 
     def __init__(self, handle, settings, ns, nt):
         self._h = handle
-        self.settings = settings
+        # a copy of the settings the handle was built with: the output buffers are sized from
+        # it, so a builder changed and reused afterwards must not change them (the handle keeps
+        # its own copy, cache directories included, so the copy's pointers are dropped)
+        self.settings = Settings.from_buffer_copy(settings)
+        self.settings.table_cache = None
+        self.settings.tuning_cache = None
         self.nsources = ns
         self.ntargets = nt
 

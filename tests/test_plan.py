@@ -161,6 +161,20 @@ def test_settings_errors():
         F.FmmBuilder(4).plan(bad)
 
 
+def test_a_reused_builder_leaves_earlier_handles_alone(tmp_path):
+    """Output buffers are sized from the handle's own settings: changing the builder after a
+    build (more vectors, no gradients) must not change what the earlier handle expects."""
+    x = np.random.default_rng(2).uniform(size=(300, 3))
+    b = F.FmmBuilder(4).vectors(3).gradients().table_cache(tmp_path)
+    first = b.plan(x)
+    second = b.vectors(1).gradients(False).max_points_per_leaf(16).plan(x)
+    assert (first.settings.vectors, first.settings.gradients) == (3, 1)
+    assert (second.settings.vectors, second.settings.gradients) == (1, 0)
+    assert first.settings.table_cache is None and second.settings.table_cache is None
+    first.close()
+    second.close()
+
+
 def _edge_sets():
     rng = np.random.default_rng(31)
     line = np.zeros((700, 3))
