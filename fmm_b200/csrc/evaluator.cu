@@ -386,7 +386,8 @@ std::unique_ptr<fmmgpu_fmm> build_host_batch(const fmmgpu_settings* settings, si
                 const double* cs = src + 3 * tp.src_offset;
                 const double* ct = same ? cs : tgt + 3 * tp.tgt_offset;
                 const size_t cnt = same ? ns[c] : nt[c];
-                tp.plan = build_plan(ns[c], cs, cnt, ct, s.max_level, s.max_points_per_leaf);
+                // one host thread a cloud: the clouds already run on all of them
+                tp.plan = build_plan(ns[c], cs, cnt, ct, s.max_level, s.max_points_per_leaf, false, 1);
                 leaf_scaled(tp.plan, cs, ct, tp.us, tp.ut);
             } catch (const std::exception& e) {
                 errors[c] = e.what();

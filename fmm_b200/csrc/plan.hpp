@@ -86,9 +86,11 @@ Plan merge_plans(std::vector<TreePart>& parts, std::vector<double>& us, std::vec
 // (refined while a box holds more than max_keys keys, then 2:1 balanced), the box
 // index, the point order and the lists.  Throws std::runtime_error on bad input.
 // device_points: the point stages (keys, sort, each point's leaf, the order by leaf) on the
-// current CUDA device (plan_gpu.cu), with the same results.
+// current CUDA device (plan_gpu.cu), with the same results.  Otherwise they run on up to
+// host_threads host threads (0: the host's cores, at most 16; 1: this thread only), with
+// the same results for every thread count.
 Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
-                int max_keys, bool device_points = false);
+                int max_keys, bool device_points = false, int host_threads = 0);
 
 // The point stages of a build: the level-16 keys of sources ++ targets sorted and made
 // distinct, then, once the leaves are known (their first level-16 keys ascending and their

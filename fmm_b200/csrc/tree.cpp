@@ -59,6 +59,47 @@ void sort_unique(std::vector<uint64_t>& v) {
     v.erase(std::unique(v.begin(), v.end()), v.end());
 }
 
+// Host threads for a point stage over n items: one below 2^16 items, else up to `limit`
+// (0: the host's cores, at most 16).
+size_t stage_threads(size_t n, int limit) {
+    if (n < ((size_t)1 << 16)) return 1;
+    size_t cap = limit > 0 ? (size_t)limit : 16;
+    return std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), cap));
+}
+
+// fn(t, begin, end) for the chunks t = 0..nth-1 of [0, n), chunk t on its own thread (chunk
+// 0 on this one).  fn must not throw.  If a thread cannot be started, its chunk and the
+// ones after it run here, so every chunk runs exactly once whatever happens.
+template <class Fn>
+void for_chunks(size_t n, size_t nth, Fn&& fn) {
+    std::vector<std::thread> pool;
+    size_t t = 1;
+    try {
+        for (; t < nth; ++t) pool.emplace_back([&fn, n, nth, t] { fn(t, n * t / nth, n * (t + 1) / nth); });
+    } catch (...) {
+    }
+    fn((size_t)0, (size_t)0, n / nth);
+    for (; t < nth; ++t) fn(t, n * t / nth, n * (t + 1) / nth);
+    for (auto& th : pool) th.join();
+}
+
+// sort_unique with the chunks sorted on nth threads and merged pairwise (the same values)
+void sort_unique_threads(std::vector<uint64_t>& v, size_t nth) {
+    if (nth <= 1) return sort_unique(v);
+    const size_t n = v.size();
+    std::vector<size_t> edge(nth + 1);
+    for (size_t t = 0; t <= nth; ++t) edge[t] = n * t / nth;
+    for_chunks(nth, nth, [&](size_t t, size_t, size_t) { std::sort(v.begin() + edge[t], v.begin() + edge[t + 1]); });
+    for (size_t w = 1; w < nth; w *= 2) {
+        const size_t pairs = (nth + 2 * w - 1) / (2 * w);
+        for_chunks(pairs, pairs, [&](size_t i, size_t, size_t) {
+            const size_t a = 2 * w * i, b = std::min(a + w, nth), c = std::min(a + 2 * w, nth);
+            if (b < c) std::inplace_merge(v.begin() + edge[a], v.begin() + edge[b], v.begin() + edge[c]);
+        });
+    }
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+}
+
 // create_local_tree of octree/src/octree/implementation.rs:682-730 from the root:
 // a box splits while it holds more than max_keys distinct keys and lies above max_level.
 void refine(const uint64_t* fine, size_t n, uint64_t box, int max_level, size_t max_keys,
@@ -167,7 +208,7 @@ int offset_index(int x, int y, int z) {
 }
 
 Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
-                int max_keys, bool device_points) {
+                int max_keys, bool device_points, int host_threads) {
     if (ns + nt == 0) throw std::runtime_error("no points");
     if (max_keys < 1) throw std::runtime_error("max_points_per_leaf must be at least 1");
     if (max_level > kDeepest) max_level = kDeepest;
@@ -221,18 +262,26 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
     // the point stages (keys, their distinct sorted set, later each point's leaf and the
     // order by leaf) on the device when asked (plan_gpu.cu: the same keys and order), else here
     std::unique_ptr<PointSort> dev = device_points ? device_point_sort(ns, src, nt, tgt, P.box6) : nullptr;
+    const bool same_points = src == tgt && ns == nt;  // one point set: the targets' stages are the sources'
     std::vector<uint64_t> skey, tkey, fine;
     if (dev) {
         fine = dev->distinct_keys();
     } else {
         skey.resize(ns);
-        tkey.resize(nt);
-        for (size_t i = 0; i < ns; ++i) skey[i] = point_key(src + 3 * i);
-        for (size_t i = 0; i < nt; ++i) tkey[i] = point_key(tgt + 3 * i);
-        fine.reserve(ns + nt);
+        for_chunks(ns, stage_threads(ns, host_threads), [&](size_t, size_t i0, size_t i1) {
+            for (size_t i = i0; i < i1; ++i) skey[i] = point_key(src + 3 * i);
+        });
+        if (!same_points) {
+            tkey.resize(nt);
+            for_chunks(nt, stage_threads(nt, host_threads), [&](size_t, size_t i0, size_t i1) {
+                for (size_t i = i0; i < i1; ++i) tkey[i] = point_key(tgt + 3 * i);
+            });
+        }
+        // targets that are the sources add no key of their own
+        fine.reserve(ns + (same_points ? 0 : nt));
         fine.insert(fine.end(), skey.begin(), skey.end());
         fine.insert(fine.end(), tkey.begin(), tkey.end());
-        sort_unique(fine);  // distinct keys (route_keys on one rank)
+        sort_unique_threads(fine, stage_threads(fine.size(), host_threads));  // distinct keys (route_keys on one rank)
     }
 
     std::vector<uint64_t> refined;
@@ -301,20 +350,40 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         return morton_leaf_index[pos];
     };
     if (dev) dev->leaf_order(firsts, morton_leaf_index, nl, P);
-    for (int s = 0; s < (dev ? 0 : 2); ++s) {
+    for (int s = 0; s < (dev ? 0 : same_points ? 1 : 2); ++s) {
         const std::vector<uint64_t>& keys = s ? tkey : skey;
         size_t n = keys.size();
+        const size_t nth = stage_threads(n, host_threads);
         std::vector<int32_t> lf(n);
-        for (size_t i = 0; i < n; ++i) lf[i] = leaf_of(keys[i]);
+        // each chunk counts its points per leaf; a chunk's points of leaf j then go after
+        // those of the chunks before it (a stable counting sort: the order of the points'
+        // indices within a leaf, for every thread count)
+        std::vector<std::vector<int64_t>> next(nth, std::vector<int64_t>(nl, 0));
+        for_chunks(n, nth, [&](size_t t, size_t i0, size_t i1) {
+            for (size_t i = i0; i < i1; ++i) {
+                lf[i] = leaf_of(keys[i]);
+                next[t][lf[i]]++;
+            }
+        });
         std::vector<int64_t> start(nl + 1, 0);
-        for (size_t i = 0; i < n; ++i) start[lf[i] + 1]++;
-        for (size_t j = 0; j < nl; ++j) start[j + 1] += start[j];
-        std::vector<int64_t> perm(n), pos_of(n), fill(start.begin(), start.end() - 1);
-        for (size_t i = 0; i < n; ++i) {
-            int64_t pos = fill[lf[i]]++;
-            perm[pos] = (int64_t)i;
-            pos_of[i] = pos;
+        int64_t run = 0;
+        for (size_t j = 0; j < nl; ++j) {
+            start[j] = run;
+            for (size_t t = 0; t < nth; ++t) {
+                const int64_t c = next[t][j];
+                next[t][j] = run;
+                run += c;
+            }
         }
+        start[nl] = run;
+        std::vector<int64_t> perm(n), pos_of(n);
+        for_chunks(n, nth, [&](size_t t, size_t i0, size_t i1) {
+            for (size_t i = i0; i < i1; ++i) {
+                const int64_t pos = next[t][lf[i]]++;
+                perm[pos] = (int64_t)i;
+                pos_of[i] = pos;
+            }
+        });
         if (s) {
             P.tgt_start.swap(start);
             P.tgt_perm.swap(perm);
@@ -324,6 +393,11 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
             P.src_perm.swap(perm);
             P.src_pos_of.swap(pos_of);
         }
+    }
+    if (!dev && same_points) {
+        P.tgt_start = P.src_start;
+        P.tgt_perm = P.src_perm;
+        P.tgt_pos_of = P.src_pos_of;
     }
     // counts below every box (children come after parents, level-major)
     P.src_below.assign(nb, 0);

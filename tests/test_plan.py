@@ -55,6 +55,34 @@ def test_tree_equals_oracle(oracle, kind, n, mk):
     assert np.array_equal(leaf, tr.is_leaf)
 
 
+def test_large_plan_on_host_threads(oracle):
+    """Above 65,536 points the host point stages (keys, distinct sort, each point's leaf, the
+    stable order by leaf) run on several threads: the tree is still the oracle's, the points
+    of a leaf keep their index order, the plan passes every check of an uploaded plan, and
+    targets given as a separate array of the same values give the same plan as targets
+    that are the sources."""
+    x, _ = oracle.point_sets("cube", 200000, 17)
+    mk = 64
+    a = F.FmmBuilder(4).max_points_per_leaf(mk).plan(x)
+    b = F.FmmBuilder(4).max_points_per_leaf(mk).plan(x, x.copy())
+    keys, leaf = a.boxes()
+    tr = oracle.Tree(x, x, 16, mk)
+    assert np.array_equal(keys, tr.keys) and np.array_equal(leaf, tr.is_leaf)
+    pa, pb = a.plan_arrays(), b.plan_arrays()
+    for name in F.PlanArrays.ARRAYS:
+        assert np.array_equal(pa[name], pb[name]), name
+    for s in ("source", "target"):
+        off, order = pa[f"{s}_offsets"], pa[f"{s}_order"]
+        assert off[0] == 0 and off[-1] == len(x) and np.array_equal(np.sort(order), np.arange(len(x)))
+        step = np.diff(order)
+        inside = np.ones(len(step), dtype=bool)
+        inside[off[1:-1] - 1] = False  # the last point of a leaf and the first of the next
+        assert np.all(step[inside] > 0)
+    F.FmmBuilder(4).max_points_per_leaf(mk).plan_from(pa, x).close()
+    a.close()
+    b.close()
+
+
 def test_tree_with_distinct_targets(oracle):
     rng = np.random.default_rng(3)
     src = rng.uniform(0, 1, (2500, 3))
