@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -77,6 +78,14 @@ struct TreePart {
     std::vector<double> us, ut;
     int64_t src_offset = 0, tgt_offset = 0;
 };
+
+// Host threads for a stage over n independent items: one below 2^16 items, else up to
+// `limit` (0: the host's cores, at most 16).
+size_t stage_threads(size_t n, int limit = 0);
+// fn(t, begin, end) for the chunks t = 0..nth-1 of [0, n), chunk t on its own thread (chunk
+// 0 on the calling one).  fn must not throw.  A thread that cannot be started has its chunk
+// run on the calling thread, so every chunk runs exactly once.
+void for_chunks(size_t n, size_t nth, const std::function<void(size_t, size_t, size_t)>& fn);
 
 // The forest of several clouds' plans (forest.cpp): level-major over all trees, with the
 // merged leaf-scaled coordinates in us / ut.

@@ -59,30 +59,6 @@ void sort_unique(std::vector<uint64_t>& v) {
     v.erase(std::unique(v.begin(), v.end()), v.end());
 }
 
-// Host threads for a point stage over n items: one below 2^16 items, else up to `limit`
-// (0: the host's cores, at most 16).
-size_t stage_threads(size_t n, int limit) {
-    if (n < ((size_t)1 << 16)) return 1;
-    size_t cap = limit > 0 ? (size_t)limit : 16;
-    return std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), cap));
-}
-
-// fn(t, begin, end) for the chunks t = 0..nth-1 of [0, n), chunk t on its own thread (chunk
-// 0 on this one).  fn must not throw.  If a thread cannot be started, its chunk and the
-// ones after it run here, so every chunk runs exactly once whatever happens.
-template <class Fn>
-void for_chunks(size_t n, size_t nth, Fn&& fn) {
-    std::vector<std::thread> pool;
-    size_t t = 1;
-    try {
-        for (; t < nth; ++t) pool.emplace_back([&fn, n, nth, t] { fn(t, n * t / nth, n * (t + 1) / nth); });
-    } catch (...) {
-    }
-    fn((size_t)0, (size_t)0, n / nth);
-    for (; t < nth; ++t) fn(t, n * t / nth, n * (t + 1) / nth);
-    for (auto& th : pool) th.join();
-}
-
 // sort_unique with the chunks sorted on nth threads and merged pairwise (the same values)
 void sort_unique_threads(std::vector<uint64_t>& v, size_t nth) {
     if (nth <= 1) return sort_unique(v);
@@ -205,6 +181,24 @@ int offset_index(int x, int y, int z) {
     if (adj(x) && adj(y) && adj(z)) return -1;
     return 49 * (x + 3) + 7 * (y + 3) + (z + 3) - 9 * kappa(x) -
            (adj(x) ? 1 : 0) * (3 * kappa(y) + (adj(y) ? 1 : 0) * kappa(z));
+}
+
+size_t stage_threads(size_t n, int limit) {
+    if (n < ((size_t)1 << 16)) return 1;
+    const size_t cap = limit > 0 ? (size_t)limit : 16;
+    return std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), cap));
+}
+
+void for_chunks(size_t n, size_t nth, const std::function<void(size_t, size_t, size_t)>& fn) {
+    std::vector<std::thread> pool;
+    size_t t = 1;
+    try {
+        for (; t < nth; ++t) pool.emplace_back([&fn, n, nth, t] { fn(t, n * t / nth, n * (t + 1) / nth); });
+    } catch (...) {
+    }
+    fn(0, 0, n / nth);
+    for (; t < nth; ++t) fn(t, n * t / nth, n * (t + 1) / nth);
+    for (auto& th : pool) th.join();
 }
 
 Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
@@ -427,8 +421,9 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         std::vector<int32_t> a, aux, b;
         std::vector<int64_t> arow, brow;  // row ends within the chunk
     };
-    auto two_lists = [](size_t nrows, Csr& A, Csr& B, bool with_aux, auto&& row_fn) {
-        const size_t nth = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+    auto two_lists = [host_threads](size_t nrows, Csr& A, Csr& B, bool with_aux, auto&& row_fn) {
+        const size_t cap = host_threads > 0 ? (size_t)host_threads : 16;
+        const size_t nth = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), cap));
         const size_t nch = std::min(nrows, nth * 4) ? std::min(nrows, nth * 4) : 1;
         std::vector<Rows> parts(nch);
         std::vector<std::string> errors(nch);

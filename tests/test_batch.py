@@ -67,3 +67,35 @@ def test_batch_errors_name_the_cloud():
         assert "cloud 1" in str(e)
     else:
         raise AssertionError("a non-finite cloud must be rejected")
+
+
+
+def test_large_forest_on_host_threads():
+    """A batch large enough for the merge to run on several host threads (more than 65,536
+    boxes, leaves and points): the forest's boxes are the clouds' boxes level by level, its
+    pair counts are their sums, and list rows spread over the whole forest (so over every
+    thread's chunk) are the clouds' rows."""
+    rng = np.random.default_rng(8)
+    cs = [rng.uniform(0, 1, (150000, 3)), rng.normal(0, 1, (120000, 3))]
+    b = F.FmmBuilder(4).max_points_per_leaf(4)
+    forest = b.plan_batch(cs)
+    singles = [b.plan(c) for c in cs]
+    info = forest.info()
+    assert info["nboxes"] > 65536 and info["nleaves"] > 65536 and info["nsources"] > 65536
+    for k in ("nboxes", "nleaves", "near_pairs", "v_pairs", "w_pairs", "x_pairs"):
+        assert info[k] == sum(s.info()[k] for s in singles), k
+    fk, fl = forest.boxes()
+    box_of, leaf_of = [], []  # forest box / leaf -> (cloud, local box / leaf), level by level
+    local = [s.boxes() for s in singles]
+    for lev in range(info["nlevels"]):
+        for c, (k, leaf) in enumerate(local):
+            for bx in np.nonzero(level_of(k) == lev)[0]:
+                box_of.append((c, int(bx)))
+    for n, (c, bx) in enumerate(box_of):
+        assert fk[n] == local[c][0][bx] and fl[n] == local[c][1][bx]
+    leaf_index = [np.cumsum(leaf) - 1 for _, leaf in local]
+    leaf_of = [(c, int(leaf_index[c][bx])) for c, bx in box_of if local[c][1][bx]]
+    for kind, rows in ((1, box_of), (3, box_of), (0, leaf_of), (2, leaf_of)):
+        for r in np.linspace(0, len(rows) - 1, 1500).astype(np.int64):
+            c, lr = rows[r]
+            assert np.array_equal(forest.list(kind, int(r)), singles[c].list(kind, lr)), (kind, int(r))
