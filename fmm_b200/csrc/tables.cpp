@@ -5,7 +5,9 @@
 // as fmm-tables/src/m2l.rs:67-96 and octant.rs:150-174 define them.  The translations
 // are evaluated with the real-storage order sums of CONVENTIONS 3.11 "Real storage"
 // (stored orders m >= 0 of the input only), in complex arithmetic on (re, im) pairs.
+#include <algorithm>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "plan.hpp"
@@ -160,17 +162,22 @@ void m2l(int p, const double b[3], double sigma, const double* in, double* out) 
         }
 }
 
+// The tables are independent (each writes its own nc x nc slice), so they are built in
+// chunks on host threads: the same values for any number of threads.
 template <class F>
 void build(int p, int count, std::vector<double>& out, F&& apply) {
     int nc = (p + 1) * (p + 1);
     out.assign((size_t)count * nc * nc, 0.0);
-    std::vector<double> unit(nc, 0.0);
-    for (int t = 0; t < count; ++t)
-        for (int k = 0; k < nc; ++k) {
-            unit[k] = 1.0;
-            apply(t, unit.data(), out.data() + ((size_t)t * nc + k) * nc);
-            unit[k] = 0.0;
-        }
+    const size_t nth = std::max<size_t>(1, std::min<size_t>({std::thread::hardware_concurrency(), 16, (size_t)count}));
+    for_chunks((size_t)count, nth, [&](size_t, size_t t0, size_t t1) {
+        std::vector<double> unit(nc, 0.0);
+        for (size_t t = t0; t < t1; ++t)
+            for (int k = 0; k < nc; ++k) {
+                unit[k] = 1.0;
+                apply((int)t, unit.data(), out.data() + (t * nc + k) * nc);
+                unit[k] = 0.0;
+            }
+    });
 }
 
 inline void octant_half(int o, double c[3]) {
