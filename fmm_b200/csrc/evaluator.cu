@@ -276,19 +276,22 @@ void leaf_scaled(const Plan& P, const double* src, const double* tgt, std::vecto
                  std::vector<double>& ut) {
     us.assign(3 * P.src_perm.size(), 0.0);
     ut.assign(3 * P.tgt_perm.size(), 0.0);
-    for (size_t j = 0; j < P.nleaves(); ++j) {
-        int b = P.leaf_box[j];
-        for (int64_t a = P.src_start[j]; a < P.src_start[j + 1]; ++a) {
-            int64_t i = P.src_perm[a];
-            for (int k = 0; k < 3; ++k)
-                us[3 * a + k] = leaf_coordinate(src[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
+    // leaves in chunks on host threads (each point written once: the same coordinates)
+    for_chunks(P.nleaves(), stage_threads(P.nleaves()), [&](size_t, size_t j0, size_t j1) {
+        for (size_t j = j0; j < j1; ++j) {
+            int b = P.leaf_box[j];
+            for (int64_t a = P.src_start[j]; a < P.src_start[j + 1]; ++a) {
+                int64_t i = P.src_perm[a];
+                for (int k = 0; k < 3; ++k)
+                    us[3 * a + k] = leaf_coordinate(src[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
+            }
+            for (int64_t a = P.tgt_start[j]; a < P.tgt_start[j + 1]; ++a) {
+                int64_t i = P.tgt_perm[a];
+                for (int k = 0; k < 3; ++k)
+                    ut[3 * a + k] = leaf_coordinate(tgt[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
+            }
         }
-        for (int64_t a = P.tgt_start[j]; a < P.tgt_start[j + 1]; ++a) {
-            int64_t i = P.tgt_perm[a];
-            for (int k = 0; k < 3; ++k)
-                ut[3 * a + k] = leaf_coordinate(tgt[3 * i + k], P.lower[k], P.side, P.level[b], P.idx[3 * b + k]);
-        }
-    }
+    });
 }
 
 int64_t count_near_pairs(const Plan& P) {

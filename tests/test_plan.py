@@ -81,6 +81,12 @@ def test_large_plan_on_host_threads(oracle):
     F.FmmBuilder(4).max_points_per_leaf(mk).plan_from(pa, x).close()
     a.close()
     b.close()
+    # more than 65,536 leaves: the leaf-scaled coordinates are formed on host threads too,
+    # and the upload's check puts every point inside its own leaf
+    small = F.FmmBuilder(4).max_points_per_leaf(2).plan(x)
+    assert small.info()["nleaves"] > 65536
+    F.FmmBuilder(4).max_points_per_leaf(2).plan_from(small.plan_arrays(), x).close()
+    small.close()
 
 
 def test_tree_with_distinct_targets(oracle):
