@@ -83,8 +83,9 @@ struct TreePart {
 // `limit` (0: the host's cores, at most 16).
 size_t stage_threads(size_t n, int limit = 0);
 // fn(t, begin, end) for the chunks t = 0..nth-1 of [0, n), chunk t on its own thread (chunk
-// 0 on the calling one).  fn must not throw.  A thread that cannot be started has its chunk
-// run on the calling thread, so every chunk runs exactly once.
+// 0 on the calling one).  A thread that cannot be started has its chunk run on the calling
+// thread, so every chunk runs exactly once; an exception from a chunk is rethrown here once
+// every chunk has ended (the first chunk's that threw).
 void for_chunks(size_t n, size_t nth, const std::function<void(size_t, size_t, size_t)>& fn);
 
 // The forest of several clouds' plans (forest.cpp): level-major over all trees, with the

@@ -169,8 +169,9 @@ void build(int p, int count, std::vector<double>& out, F&& apply) {
     int nc = (p + 1) * (p + 1);
     out.assign((size_t)count * nc * nc, 0.0);
     const size_t nth = std::max<size_t>(1, std::min<size_t>({std::thread::hardware_concurrency(), 16, (size_t)count}));
-    for_chunks((size_t)count, nth, [&](size_t, size_t t0, size_t t1) {
-        std::vector<double> unit(nc, 0.0);
+    std::vector<std::vector<double>> units(nth, std::vector<double>(nc, 0.0));  // allocated here, not in a thread
+    for_chunks((size_t)count, nth, [&](size_t c, size_t t0, size_t t1) {
+        std::vector<double>& unit = units[c];
         for (size_t t = t0; t < t1; ++t)
             for (int k = 0; k < nc; ++k) {
                 unit[k] = 1.0;

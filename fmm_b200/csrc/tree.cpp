@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -190,15 +191,25 @@ size_t stage_threads(size_t n, int limit) {
 }
 
 void for_chunks(size_t n, size_t nth, const std::function<void(size_t, size_t, size_t)>& fn) {
+    std::vector<std::exception_ptr> failed(nth);
+    auto chunk = [&fn, &failed, n, nth](size_t t) {
+        try {
+            fn(t, n * t / nth, n * (t + 1) / nth);
+        } catch (...) {
+            failed[t] = std::current_exception();
+        }
+    };
     std::vector<std::thread> pool;
     size_t t = 1;
     try {
-        for (; t < nth; ++t) pool.emplace_back([&fn, n, nth, t] { fn(t, n * t / nth, n * (t + 1) / nth); });
+        for (; t < nth; ++t) pool.emplace_back(chunk, t);
     } catch (...) {
     }
-    fn(0, 0, n / nth);
-    for (; t < nth; ++t) fn(t, n * t / nth, n * (t + 1) / nth);
+    chunk(0);
+    for (; t < nth; ++t) chunk(t);
     for (auto& th : pool) th.join();
+    for (const auto& e : failed)
+        if (e) std::rethrow_exception(e);
 }
 
 Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int max_level,
