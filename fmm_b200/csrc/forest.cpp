@@ -28,6 +28,7 @@ Plan merge_plans(std::vector<TreePart>& parts, std::vector<double>& us, std::vec
         nsrc += p.plan.src_perm.size();
         ntgt += p.plan.tgt_perm.size();
     }
+    if (nbox >= ((size_t)1 << 31)) throw std::runtime_error("too many boxes for 32-bit box indices");
     M.nlevels = L;
     M.side = parts[0].plan.side;
     for (int k = 0; k < 3; ++k) M.lower[k] = parts[0].plan.lower[k];

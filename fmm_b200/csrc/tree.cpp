@@ -304,6 +304,7 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
     std::stable_sort(all.begin(), all.end(),
                      [](uint64_t a, uint64_t b) { return key_level(a) < key_level(b); });
     const size_t nb = all.size();
+    if (nb >= ((size_t)1 << 31)) throw std::runtime_error("too many boxes for 32-bit box indices");
     P.key = all;
     P.nlevels = key_level(all.back()) + 1;
     P.level.resize(nb);
