@@ -77,6 +77,30 @@ void sort_unique_threads(std::vector<uint64_t>& v, size_t nth) {
     v.erase(std::unique(v.begin(), v.end()), v.end());
 }
 
+// LSD radix sort of level-16 keys with their point numbers, 8 bits a pass over bits 15..62
+// (the Morton code; the level bits are the same in every key): stable, so equal keys keep
+// their points' order.  A pass whose byte is the same in every key is skipped.
+void radix_sort_keys(std::vector<uint64_t>& key, std::vector<uint32_t>& id) {
+    const size_t n = key.size();
+    std::vector<uint64_t> k2(n);
+    std::vector<uint32_t> i2(n);
+    for (int shift = 15; shift < 63; shift += 8) {
+        size_t start[257] = {0};
+        for (size_t i = 0; i < n; ++i) start[((key[i] >> shift) & 0xFF) + 1]++;
+        bool one_bucket = false;
+        for (int b = 0; b < 256; ++b) one_bucket |= start[b + 1] == n;
+        if (one_bucket) continue;
+        for (int b = 0; b < 256; ++b) start[b + 1] += start[b];
+        for (size_t i = 0; i < n; ++i) {
+            const size_t d = start[(key[i] >> shift) & 0xFF]++;
+            k2[d] = key[i];
+            i2[d] = id[i];
+        }
+        key.swap(k2);
+        id.swap(i2);
+    }
+}
+
 // create_local_tree of octree/src/octree/implementation.rs:682-730 from the root:
 // a box splits while it holds more than max_keys distinct keys and lies above max_level.
 void refine(const uint64_t* fine, size_t n, uint64_t box, int max_level, size_t max_keys,
@@ -269,6 +293,11 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
     std::unique_ptr<PointSort> dev = device_points ? device_point_sort(ns, src, nt, tgt, P.box6) : nullptr;
     const bool same_points = src == tgt && ns == nt;  // one point set: the targets' stages are the sources'
     std::vector<uint64_t> skey, tkey, fine;
+    // on one host thread the keys are radix-sorted with their point numbers (sources, then
+    // targets after ns) once: that gives the distinct keys here and each point's leaf below
+    // by one sweep against the leaves' first keys (the leaf a binary search would find)
+    const bool sweep = !dev && stage_threads(ns + nt, host_threads) == 1 && ns + nt < ((size_t)1 << 32);
+    std::vector<uint32_t> sorted_id;
     if (dev) {
         fine = dev->distinct_keys();
     } else {
@@ -286,7 +315,14 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         fine.reserve(ns + (same_points ? 0 : nt));
         fine.insert(fine.end(), skey.begin(), skey.end());
         fine.insert(fine.end(), tkey.begin(), tkey.end());
-        sort_unique_threads(fine, stage_threads(fine.size(), host_threads));  // distinct keys (route_keys on one rank)
+        if (sweep) {
+            sorted_id.resize(fine.size());
+            for (size_t i = 0; i < sorted_id.size(); ++i) sorted_id[i] = (uint32_t)i;
+            radix_sort_keys(fine, sorted_id);
+            fine.erase(std::unique(fine.begin(), fine.end()), fine.end());
+        } else {
+            sort_unique_threads(fine, stage_threads(fine.size(), host_threads));  // distinct keys (route_keys on one rank)
+        }
     }
 
     std::vector<uint64_t> refined;
@@ -356,6 +392,16 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         return morton_leaf_index[pos];
     };
     if (dev) dev->leaf_order(firsts, morton_leaf_index, nl, P);
+    std::vector<int32_t> swept;  // each point's leaf, sources then targets
+    if (sweep) {
+        swept.resize(sorted_id.size());
+        size_t at = 0;
+        for (uint32_t id : sorted_id) {
+            const uint64_t k = id < ns ? skey[id] : tkey[id - ns];
+            while (at + 1 < firsts.size() && firsts[at + 1] <= k) ++at;
+            swept[id] = morton_leaf_index[at];
+        }
+    }
     for (int s = 0; s < (dev ? 0 : same_points ? 1 : 2); ++s) {
         const std::vector<uint64_t>& keys = s ? tkey : skey;
         size_t n = keys.size();
@@ -367,7 +413,7 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         std::vector<std::vector<int64_t>> next(nth, std::vector<int64_t>(nl, 0));
         for_chunks(n, nth, [&](size_t t, size_t i0, size_t i1) {
             for (size_t i = i0; i < i1; ++i) {
-                lf[i] = leaf_of(keys[i]);
+                lf[i] = sweep ? swept[(s ? ns : 0) + i] : leaf_of(keys[i]);
                 next[t][lf[i]]++;
             }
         });
