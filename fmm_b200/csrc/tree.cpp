@@ -248,15 +248,35 @@ Plan build_plan(size_t ns, const double* src, size_t nt, const double* tgt, int 
         mn[k] = std::numeric_limits<double>::max();
         mx[k] = std::numeric_limits<double>::lowest();
     }
+    // per-chunk bounds on host threads, then combined (min and max are exact in any order)
     for (int s = 0; s < 2; ++s) {
-        size_t n = s ? nt : ns;
+        const size_t n = s ? nt : ns;
         const double* x = s ? tgt : src;
-        for (size_t i = 0; i < n; ++i)
+        const size_t nth = stage_threads(n, host_threads);
+        std::vector<double> lo(3 * nth, std::numeric_limits<double>::max()),
+            hi(3 * nth, std::numeric_limits<double>::lowest());
+        for_chunks(n, nth, [&](size_t t, size_t i0, size_t i1) {
+            double l[3], h[3];  // this chunk's bounds, stored once at its end
             for (int k = 0; k < 3; ++k) {
-                double v = x[3 * i + k];
-                if (!std::isfinite(v)) throw std::runtime_error("non-finite point coordinate");
-                mn[k] = std::fmin(mn[k], v);
-                mx[k] = std::fmax(mx[k], v);
+                l[k] = std::numeric_limits<double>::max();
+                h[k] = std::numeric_limits<double>::lowest();
+            }
+            for (size_t i = i0; i < i1; ++i)
+                for (int k = 0; k < 3; ++k) {
+                    double v = x[3 * i + k];
+                    if (!std::isfinite(v)) throw std::runtime_error("non-finite point coordinate");
+                    l[k] = std::fmin(l[k], v);
+                    h[k] = std::fmax(h[k], v);
+                }
+            for (int k = 0; k < 3; ++k) {
+                lo[3 * t + k] = l[k];
+                hi[3 * t + k] = h[k];
+            }
+        });
+        for (size_t t = 0; t < nth; ++t)
+            for (int k = 0; k < 3; ++k) {
+                mn[k] = std::fmin(mn[k], lo[3 * t + k]);
+                mx[k] = std::fmax(mx[k], hi[3 * t + k]);
             }
     }
     double diam[3], mean[3];
