@@ -246,3 +246,22 @@ def test_tree_equals_oracle_on_edge_cases(oracle, name):
         info = plan.info()
         assert info["nsources"] == len(x) and info["nleaves"] == int(leaf.sum())
         plan.close()
+
+
+@pytest.mark.parametrize("n", [20000, 150000])  # one host thread (sweep) and several
+def test_plan_is_invariant_to_the_point_order(oracle, n):
+    """Permuting the input points leaves the boxes and every list unchanged, and each leaf
+    holds the same points (its order is the caller order, so the permuted indices sorted)."""
+    x, _ = oracle.point_sets("sphere", n, 29)
+    perm = np.random.default_rng(n).permutation(n)
+    b = F.FmmBuilder(4).max_points_per_leaf(32)
+    pa, pb = b.plan(x).plan_arrays(), b.plan(x[perm]).plan_arrays()
+    for name in ("keys", "is_leaf", "level_start", "source_offsets", "near_rows", "near", "w_rows", "w",
+                 "x_rows", "x", "v_rows", "v", "v_offsets"):
+        assert np.array_equal(pa[name], pb[name]), name
+    off = pa["source_offsets"]
+    inv = np.empty(n, dtype=np.int64)
+    inv[perm] = np.arange(n)  # original index -> index in the permuted input
+    for j in np.linspace(0, len(off) - 2, 400).astype(np.int64):
+        want = np.sort(inv[pa["source_order"][off[j]:off[j + 1]]])
+        assert np.array_equal(pb["source_order"][off[j]:off[j + 1]], want), j
